@@ -1,0 +1,310 @@
+#!/usr/bin/env python
+"""Benchmark of the free-wake induced-velocity hot path on B200.
+
+Workload: a 3,744-row rotor-ring + wing-sheet wake (819,890 straight segments, Lamb-Oseen core 0.05 m, circulation
+~ U(0, 8)) induced at 20,570 targets; seeded synthetic data of the shapes of the reference's README wakes.  One step
+is one call of the mixed-precision tree path (Morton-key tree build + FP64 moments + traversal with FP32 far field and
+pairs, FP64 near field and per-target sums) with inputs resident in HBM.  Reported beside it: the plain FP64 GPU
+direct sum on the same inputs (the reference's 'cuda' fp64 backend's job), the relative L2 and max error of the
+tree against that FP64 direct sum, the end-to-end time of the drop-in ``cuda_tree_sum`` from host NumPy arrays, and
+the reference's CPU tree code (its CPU restatement in oracle/) on the host's cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "ms/call at 102k-820k segs, mixed vs FP64 at <=1e-6 rel err; adjoint/fwd ratio"
+ROWS, TARGETS, SEED = 3744, 20570, 3744
+THETA, ORDER, LEAF, CLEARANCE = 0.05, 2, 32, 3.0
+L2_FLUSH_BYTES = 512 << 20  # larger than the 126 MB L2
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    p.add_argument("--rows", type=int, default=ROWS)
+    p.add_argument("--theta", type=float, default=THETA)
+    p.add_argument("--kind", default="morton", choices=("morton", "median"))
+    p.add_argument("--cpu-sample", type=int, default=1024, help="targets in the CPU-baseline sample")
+    return p.parse_args()
+
+
+def workload(rows):
+    from openfawe_b200 import wakes
+    return wakes.rotor_sheet(rows, seed=SEED, targets=TARGETS)
+
+
+def config(case, args, extra=None):
+    c = {"workload": f"rotor-sheet wake {args.rows} rows, {len(case['starts'])} segments x {len(case['points'])} "
+                     f"targets, Lamb-Oseen rc 0.05 m",
+         "segments": len(case["starts"]), "targets": len(case["points"]), "theta": args.theta, "order": ORDER,
+         "leaf_size": LEAF, "tree": args.kind, "precision": "mixed", "l2": "flushed between timed steps (512 MB write)",
+         "parallelism": f"replicas x{args.gpus}"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (SM clock, max clock, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self):
+        self.file.flush()
+        self.file.seek(0)
+        rows = [line.split(",") for line in self.file.read().strip().splitlines() if line.count(",") >= 8]
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = [name for k, name in enumerate(names) if any(r[5 + k].strip() == "Active" for r in rows)]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(path, encoding="utf-8") as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def cpu_baseline(case, args, threads=0):
+    """The reference's CPU tree code (vortex_tree.tree_sum, restated in oracle/) on the host cores: the full tree
+    build + moments, and the traversal for a sample of targets, scaled to the whole call."""
+    from oracle import oracle as O
+    n = len(case["points"])
+    sample = min(args.cpu_sample, n)
+    pick = np.linspace(0, n - 1, sample).astype(np.int64)
+    points = case["points"][pick]
+    a = (case["starts"], case["directions"], case["lengths"], case["gamma"], case["radius"])
+    tick = time.perf_counter()
+    lv, ends, alpha, mid = O.segment_geometry(*a[:4])
+    tree = O.build_tree(mid, LEAF)[:5]
+    q = O.node_moments(tree[0], tree[1], tree[2], a[0], ends, alpha, lv, a[4], a[3], threads)
+    w = O.node_contractions(q[4], q[5])
+    build_s = time.perf_counter() - tick
+    tick = time.perf_counter()
+    O.tree_velocity(points, *a, case["model"], "raise", tree, (*q, *w), args.theta, ORDER, CLEARANCE,
+                    np.zeros(sample + 1, dtype=np.int64), np.zeros(0, dtype=np.int64), threads)
+    eval_s = time.perf_counter() - tick
+    cores = threads if threads > 0 else (os.cpu_count() or 1)
+    try:
+        cores = len(os.sched_getaffinity(0)) if threads <= 0 else threads
+    except AttributeError:
+        pass
+    ms = 1e3 * (build_s + eval_s * n / sample)
+    return {"value": ms, "unit": "ms/call", "cores": cores, "kind": "port",
+            "sample": f"full median-split build + moments ({1e3 * build_s:.0f} ms) and the traversal of {sample} of "
+                      f"{n} targets ({1e3 * eval_s:.0f} ms) scaled to all targets; theta {args.theta}, order {ORDER}, "
+                      f"leaf {LEAF}"}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    case = workload(args.rows)
+    times = []
+    base = None
+    for step in range(args.warmup + args.steps):
+        base = cpu_baseline(case, args)
+        if step >= args.warmup:
+            times.append(base["value"])
+    value = statistics.median(times)
+    base["value"] = value
+    line = {"metric": METRIC, "value": value, "unit": "ms/call", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config(case, args, {"precision": "fp64 (CPU tree code)", "tree": "median"}),
+            "cpu_baseline": base, "e2e": {"value": value, "unit": "ms/call", "h2d_bytes_per_step": 0,
+                                          "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+    from openfawe_b200 import engine, vortex_cuda_tree
+    from openfawe_b200.settings import CudaSettings, TreeSettings
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    device = local
+
+    case = workload(args.rows)
+    model = case["model"]
+    src = engine.Sources(case["starts"], case["directions"], case["lengths"], case["gamma"], case["radius"], device)
+    tgt = engine.Targets(case["points"], None, device)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+
+    def step():
+        return engine.tree_sum(src, tgt, model, "raise", "mixed", 128, 3.0, args.theta, ORDER, LEAF, CLEARANCE,
+                               args.kind, far_counts=False)
+
+    # plain FP64 GPU direct sum: the accuracy oracle of this run and the time to beat by 10x
+    direct, _ = engine.direct(src, tgt, model, "raise", "fp64")
+    torch.cuda.synchronize()
+    fp64_times = []
+    for _ in range(2):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        direct, _ = engine.direct(src, tgt, model, "raise", "fp64")
+        e1.record()
+        torch.cuda.synchronize()
+        fp64_times.append(e0.elapsed_time(e1))
+    fp64_ms = min(fp64_times)
+    direct_host = direct.cpu().numpy()
+
+    for _ in range(args.warmup):
+        out, flags, _ = step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    times, eval_ms, counters = [], [], []
+    with Clocks(torch.cuda.current_device()) as clk:
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            out, flags, _ = step()
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+            s = engine.last_stats(device)
+            eval_ms.append(s["evaluate_ms"])
+            counters.append(s)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = clk.summary()
+    ms = float(np.mean(times))
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    u = out.cpu().numpy()
+    rel_l2 = float(np.linalg.norm(u - direct_host) / np.linalg.norm(direct_host))
+    max_err = float(np.max(np.linalg.norm(u - direct_host, axis=1)) / np.max(np.linalg.norm(direct_host, axis=1)))
+    s = counters[-1]
+
+    # roofline of the dominant kernel (the traversal): algorithmic FLOPs of SURVEY conventions per launch
+    flops = 62.0 * s["near_pairs"] + 180.0 * s["far_evaluations"] + 12.0 * s["visits"]
+    kernel_ms = float(np.mean(eval_ms))
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+    peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None, "kernel": "tree_eval_kernel<mixed>", "kernel_ms": kernel_ms,
+                "peak_note": "nominal FP32 FMA rate of 148 SMs x 128 lanes at 1965 MHz (neither HBM nor tensor "
+                             "bound: FP32 pipe)"}
+
+    # end to end through the drop-in: host NumPy in, host NumPy out
+    tree = TreeSettings(args.theta, ORDER, LEAF, CLEARANCE)
+    cuda = CudaSettings("mixed", 128, "gpu64", tree=args.kind)
+    csr = (np.zeros(len(case["points"]) + 1, dtype=np.int64), np.zeros(0, dtype=np.int64))
+    a = (case["points"], case["starts"], case["directions"], case["lengths"], case["gamma"], case["radius"], model,
+         csr, "raise", tree, cuda)
+    vortex_cuda_tree.cuda_tree_sum(*a)
+    e2e = []
+    for _ in range(max(3, min(args.steps, 5))):
+        torch.cuda.synchronize()
+        tick = time.perf_counter()
+        vortex_cuda_tree.cuda_tree_sum(*a)
+        e2e.append(1e3 * (time.perf_counter() - tick))
+    h2d = sum(np.asarray(x).nbytes for x in (case["points"], case["starts"], case["directions"], case["lengths"],
+                                              case["gamma"], case["radius"]))
+    d2h = len(case["points"]) * (24 + 1 + 8)
+
+    # launches of this library's kernels inside one step (CUPTI through the torch profiler)
+    gpu_launches = None
+    try:
+        from torch.profiler import ProfilerActivity, profile
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            step()
+            torch.cuda.synchronize()
+        gpu_launches = sum(1 for e in prof.events() if e.device_type.name == "CUDA" and "bs::" in e.name)
+    except Exception:  # noqa: BLE001 - profiler unavailable: leave the count out rather than guess
+        gpu_launches = None
+
+    line = {"metric": METRIC, "value": ms / world, "unit": "ms/call", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": config(case, args),
+            "accuracy": {"rel_l2_vs_fp64_direct": rel_l2, "max_err_over_max_speed": max_err},
+            "fp64_direct_ms": fp64_ms, "speedup_vs_fp64_direct": fp64_ms / ms,
+            "stages": {"build_ms": s["build_ms"], "moments_ms": s["moments_ms"], "evaluate_ms": kernel_ms,
+                       "nodes": s["nodes"], "near_pairs": s["near_pairs"], "far_evaluations": s["far_evaluations"],
+                       "fp64_pairs": s["fp64_pairs"], "visits": s["visits"]},
+            "interactions_per_s": {"executed": (s["near_pairs"] + s["far_evaluations"]) / (ms * 1e-3),
+                                   "direct_equivalent": len(case["points"]) * len(case["starts"]) / (ms * 1e-3)},
+            "roofline": roofline,
+            "e2e": {"value": float(np.median(e2e)), "unit": "ms/call", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": gpu_launches, "clocks": clocks}
+    if rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_baseline(case, args)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

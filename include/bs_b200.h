@@ -1,0 +1,135 @@
+/*
+ * bs_b200.h -- C ABI of the B200-native Biot-Savart hot path (libbs_b200.so, sm_100a).
+ *
+ * Replaces the numba.cuda backends of the reference's vortex-batch API (paths inside the reference project):
+ *   cuda_sum        src/openfawe/aero/vortex_cuda.py:381-467        -> bs_direct
+ *   cuda_tree_sum   src/openfawe/aero/vortex_cuda_tree.py:439-595   -> bs_tree_build + bs_tree_eval (bs_tree_sum)
+ *   device_build_tree  src/openfawe/aero/vortex_cuda_build.py:234-275  -> bs_tree_build (kind BS_TREE_MEDIAN)
+ *   device_node_quantities  src/openfawe/aero/vortex_cuda_moments.py:206-230 -> moments inside bs_tree_build /
+ *                   bs_tree_from_arrays, read back with bs_tree_export
+ *   available / probe_error  src/openfawe/aero/vortex_cuda.py:58-82 -> bs_init / bs_last_error
+ *   Statistics.last  src/openfawe/aero/vortex_cuda_tree.py:429-436 -> bs_last_stats
+ *
+ * Conventions.  Every array argument is a DEVICE pointer owned by the caller, float64 unless stated, C-contiguous:
+ * points [n,3], starts [m,3], directions [m,3] (unit), lengths [m] (> 0), gamma [m], radius [m] (>= 0);
+ * exclusions as the reference's CSR (vortex_numba.exclusion_csr, vortex_numba.py:228-243): ex_ptr int64 [n+1],
+ * ex_seg int64 [e], sorted and unique per target (ex_ptr may be NULL for no exclusions).  Outputs: out [n,3] float64,
+ * flags int8 [n] with the reference's codes (0 ok, 1 singular, 2 non-finite; vortex_numba.py:32-34).  Flags are not
+ * errors: the caller re-runs its own reference to raise, as vortex.py:488-492 does.
+ * Scratch memory is taken from a per-context stream-ordered pool (cudaMallocAsync) on the call's stream.
+ * Every entry point returns a bs_status and never aborts or traps; work is enqueued on `stream` and the host blocks only
+ * where stated (tree builds read node counts back).
+ */
+#ifndef BS_B200_H
+#define BS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bs_ctx bs_ctx;
+typedef struct bs_tree bs_tree;
+typedef void *bs_stream; /* cudaStream_t */
+
+typedef enum {
+    BS_OK = 0,
+    BS_ERR_ARG = 1,      /* invalid argument (the reference raises ValueError) */
+    BS_ERR_CUDA = 2,     /* a CUDA runtime call failed; bs_last_error has the text */
+    BS_ERR_STACK = 3,    /* tree traversal stack overflow (the reference raises RuntimeError, vortex_cuda_tree.py:548) */
+    BS_ERR_TIMEOUT = 4,  /* a bounded device-side wait gave up */
+    BS_ERR_OOM = 5       /* the memory pool could not satisfy an allocation */
+} bs_status;
+
+typedef enum { BS_FP64 = 0, BS_MIXED = 1, BS_FP32 = 2 } bs_precision;
+typedef enum { BS_TREE_MEDIAN = 0, BS_TREE_MORTON = 1 } bs_tree_kind;
+
+typedef struct {
+    int64_t m;
+    const double *starts, *directions, *lengths, *gamma, *radius;
+} bs_sources;
+
+typedef struct {
+    int64_t n;
+    const double *points;
+    const int64_t *ex_ptr; /* NULL: no exclusions */
+    const int64_t *ex_seg;
+    int64_t e;
+} bs_targets;
+
+typedef struct {
+    int model;          /* CoreModel 0..5 (vortex.py:21-27) */
+    int raise_singular; /* 1 for singularity='raise' */
+    int precision;      /* bs_precision */
+    int block;          /* threads per block: 32, 64, 128 or 256 (CudaSettings.block) */
+    double near_cores;  /* single precisions: pairs within near_cores core radii of a segment are done in FP64 */
+} bs_kernel_params;
+
+typedef struct {
+    double theta;      /* opening ratio, 0 < theta < 1 (TreeSettings.theta) */
+    int order;         /* expansion order 0, 1 or 2 */
+    int64_t leaf_size; /* maximum segments per leaf */
+    double clearance;  /* core clearance in largest core radii */
+    int kind;          /* bs_tree_kind */
+    int stack_limit;   /* traversal stack entries per warp, 0 = the maximum (128); overflow returns BS_ERR_STACK */
+} bs_tree_params;
+
+typedef struct {
+    int64_t points, segments, nodes, launches;
+    int64_t far_evaluations, near_pairs, fp64_pairs, visits; /* counters of the last tree evaluation */
+    double build_ms, moments_ms, evaluate_ms;                /* device time of the last build / evaluation */
+    int tree_depth;
+} bs_stats;
+
+/* Context: one per device.  bs_init makes `device` current, probes it with a one-thread kernel (the reference's
+ * available(), vortex_cuda.py:58-77) and creates the memory pool. */
+int bs_init(int device, bs_ctx **ctx);
+void bs_destroy(bs_ctx *ctx);
+/* Text of the last error on this thread (never NULL). */
+const char *bs_last_error(void);
+int bs_last_stats(const bs_ctx *ctx, bs_stats *stats);
+/* Library version and the compute capability it was built for (100 for sm_100a). */
+int bs_version(int *major, int *minor, int *arch);
+
+/* Exact direct sum (vortex_numba._sum_point semantics, vortex_numba.py:112-147): every non-excluded (target, segment)
+ * pair, segment order preserved inside each thread's range; BS_FP64 sums in FP64, BS_MIXED/BS_FP32 use FP32 pair
+ * arithmetic on two-float coordinates with FP64 re-evaluation near segments (reference: vortex_cuda.py:179-351). */
+int bs_direct(bs_ctx *ctx, const bs_sources *src, const bs_targets *tgt, const bs_kernel_params *kp, double *out,
+              int8_t *flags, bs_stream stream);
+
+/* Tree build on the device (Morton keys + radix sort + binary radix tree, or the reference's median split element for
+ * element).  Node moments and contractions about cell centres in FP64 (vortex_tree.node_moments semantics).  Blocks
+ * the host while reading node counts back. */
+int bs_tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_tree **tree, bs_stream stream);
+/* A tree from caller arrays (device int64 order [m], lo/hi/left/right [count]); moments computed on the device.
+ * Evaluates the reference's own tree (vortex_tree.build_tree output) with these kernels. */
+int bs_tree_from_arrays(bs_ctx *ctx, const bs_sources *src, const int64_t *order, const int64_t *lo,
+                        const int64_t *hi, const int64_t *left, const int64_t *right, int64_t count,
+                        bs_tree **tree, bs_stream stream);
+void bs_tree_free(bs_tree *tree);
+int64_t bs_tree_count(const bs_tree *tree);
+/* Copy the tree arrays to caller DEVICE buffers (any pointer may be NULL): order [m], lo/hi/left/right [count] int64,
+ * centre [count,3], bound, core [count], m0 [count,3], m1 [count,3,3], m2 [count,3,3,3], w1 [count,3], t2 [count,3],
+ * w2 [count,3,3] float64. */
+int bs_tree_export(const bs_tree *tree, int64_t *order, int64_t *lo, int64_t *hi, int64_t *left, int64_t *right,
+                   double *centre, double *bound, double *core, double *m0, double *m1, double *m2, double *w1,
+                   double *t2, double *w2, bs_stream stream);
+/* Morton keys of the segment midpoints (uint64 [m]) and their stable sort permutation (int64 [m]); either may be NULL.
+ * The bit-exact CPU recomputation is oracle/morton_oracle.c. */
+int bs_tree_keys(const bs_tree *tree, uint64_t *keys, int64_t *sorted_order, bs_stream stream);
+
+/* Tree evaluation (vortex_tree.tree_velocity semantics, vortex_tree.py:508-568): per-target acceptance, DFS order,
+ * exclusions force nodes open, leaves use the exact pair kernel.  far_counts (int64 [n]) may be NULL. */
+int bs_tree_eval(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const bs_targets *tgt,
+                 const bs_kernel_params *kp, double *out, int8_t *flags, int64_t *far_counts, bs_stream stream);
+
+/* Build + evaluate + free (cuda_tree_sum in one call). */
+int bs_tree_sum(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, const bs_targets *tgt,
+                const bs_kernel_params *kp, double *out, int8_t *flags, int64_t *far_counts, bs_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BS_B200_H */

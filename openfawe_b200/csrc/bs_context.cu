@@ -1,0 +1,109 @@
+// Context, error text, memory pool and device probe of libbs_b200.
+// The probe mirrors the reference's available() (src/openfawe/aero/vortex_cuda.py:58-77): a one-thread kernel writes
+// 1.0 and the host reads it back, so a missing or broken device is reported instead of failing later.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "bs_internal.cuh"
+
+namespace bs {
+
+static thread_local char g_error[512] = "no error";
+
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_error, sizeof g_error, fmt, ap);
+    va_end(ap);
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    set_error("%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+    return e == cudaErrorMemoryAllocation ? BS_ERR_OOM : BS_ERR_CUDA;
+}
+
+__global__ void probe_kernel(double *out) { out[0] = 1.0; }
+
+}  // namespace bs
+
+using namespace bs;
+
+extern "C" const char *bs_last_error(void) { return g_error; }
+
+extern "C" int bs_version(int *major, int *minor, int *arch) {
+    if (major) *major = 1;
+    if (minor) *minor = 0;
+    if (arch) *arch = 100;
+    return BS_OK;
+}
+
+extern "C" int bs_init(int device, bs_ctx **out) {
+    if (!out) {
+        set_error("bs_init: null output pointer");
+        return BS_ERR_ARG;
+    }
+    *out = nullptr;
+    int count = 0;
+    BS_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) {
+        set_error("bs_init: device %d out of range (%d devices)", device, count);
+        return BS_ERR_ARG;
+    }
+    BS_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    BS_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) {
+        set_error("bs_init: device %d is sm_%d%d; this library is built for sm_100a", device, prop.major, prop.minor);
+        return BS_ERR_ARG;
+    }
+    double *probe = nullptr;
+    BS_CUDA(cudaMalloc(&probe, sizeof(double)));
+    BS_CUDA(cudaMemset(probe, 0, sizeof(double)));
+    probe_kernel<<<1, 1>>>(probe);
+    cudaError_t e = cudaGetLastError();
+    double value = 0.0;
+    if (e == cudaSuccess) e = cudaMemcpy(&value, probe, sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(probe);
+    if (e != cudaSuccess) return cuda_fail(e, "bs_init probe kernel");
+    if (value != 1.0) {
+        set_error("bs_init: the probe kernel wrote %g instead of 1", value);
+        return BS_ERR_CUDA;
+    }
+    bs_ctx *ctx = new bs_ctx();
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    memset(&ctx->stats, 0, sizeof ctx->stats);
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof props);
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    e = cudaMemPoolCreate(&ctx->pool, &props);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return cuda_fail(e, "cudaMemPoolCreate");
+    }
+    uint64_t keep = UINT64_MAX;  // keep freed blocks cached in the pool between calls
+    cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    *out = ctx;
+    return BS_OK;
+}
+
+extern "C" void bs_destroy(bs_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    cudaMemPoolDestroy(ctx->pool);
+    delete ctx;
+}
+
+extern "C" int bs_last_stats(const bs_ctx *ctx, bs_stats *stats) {
+    if (!ctx || !stats) {
+        set_error("bs_last_stats: null argument");
+        return BS_ERR_ARG;
+    }
+    *stats = ctx->stats;
+    return BS_OK;
+}

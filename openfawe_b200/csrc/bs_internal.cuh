@@ -1,0 +1,346 @@
+// Internal definitions of libbs_b200: device records, the pair and far-field arithmetic, status plumbing.
+//
+// Pair arithmetic follows the reference's vortex_numba.pair_velocity (src/openfawe/aero/vortex_numba.py:42-109)
+// branch for branch: scaled offsets a = (p - s)/L, t = a.d, c = d x a, h = |c|, na = |a|, nb = |a - d|, the roundoff
+// axis guard h <= 8 eps max(1, na, nb), the rationalised denominator when h^2 + t(t - 1) < 0, and the six core models.
+// Per-segment constants (1/L, Gamma/(4 pi L), rc/L) are formed once when the segment records are packed.
+// The far field follows vortex_tree.far_velocity (src/openfawe/aero/vortex_tree.py:450-497).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "../../include/bs_b200.h"
+
+#define BS_FLAG_OK 0
+#define BS_FLAG_SINGULAR 1
+#define BS_FLAG_NONFINITE 2
+
+namespace bs {
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Error plumbing (host).
+// ---------------------------------------------------------------------------------------------------------------------
+void set_error(const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what);
+#define BS_CUDA(call)                                                  \
+    do {                                                               \
+        cudaError_t _e = (call);                                       \
+        if (_e != cudaSuccess) return ::bs::cuda_fail(_e, #call);      \
+    } while (0)
+#define BS_CHECK_LAUNCH(what)                                          \
+    do {                                                               \
+        cudaError_t _e = cudaGetLastError();                           \
+        if (_e != cudaSuccess) return ::bs::cuda_fail(_e, what);       \
+    } while (0)
+
+// Stream-ordered scratch from the context's pool, released (stream-ordered) when the object goes out of scope.
+struct Scratch {
+    cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;
+    std::vector<void *> ptrs;
+    int status = BS_OK;
+    Scratch(cudaMemPool_t p, cudaStream_t s) : stream(s), pool(p) {}
+    Scratch(const Scratch &) = delete;
+    Scratch &operator=(const Scratch &) = delete;
+    template <class T> T *get(size_t elems) {
+        if (status != BS_OK) return nullptr;
+        if (elems == 0) elems = 1;
+        void *p = nullptr;
+        cudaError_t e = cudaMallocFromPoolAsync(&p, elems * sizeof(T), pool, stream);
+        if (e != cudaSuccess) {
+            status = e == cudaErrorMemoryAllocation ? BS_ERR_OOM : BS_ERR_CUDA;
+            cuda_fail(e, "scratch allocation");
+            return nullptr;
+        }
+        ptrs.push_back(p);
+        return static_cast<T *>(p);
+    }
+    void release() {
+        for (void *p : ptrs) cudaFreeAsync(p, stream);
+        ptrs.clear();
+    }
+    ~Scratch() { release(); }
+};
+
+}  // namespace bs
+
+struct bs_ctx {
+    int device;
+    int sm_count;
+    cudaMemPool_t pool;
+    bs_stats stats;
+};
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Device records.
+// ---------------------------------------------------------------------------------------------------------------------
+namespace bs {
+
+// One segment, FP64 (80 bytes; 16-byte multiple for bulk copies).
+struct __align__(16) Seg64 {
+    double sx, sy, sz, inv_len;  // start, 1/L
+    double dx, dy, dz, gfac;     // unit direction, (Gamma/L)/(4 pi)
+    double rcl, radius;          // rc/L, rc (rc > 0 && model != 0 enables the core)
+};
+
+// One segment for the single-precision paths (48 bytes): start as a two-float (hi + lo) pair.
+struct __align__(16) Seg32 {
+    float4 hi;   // sx_hi, sy_hi, sz_hi, 1/L
+    float4 lo;   // sx_lo, sy_lo, sz_lo, (Gamma/L)/(4 pi)
+    float4 dir;  // dx, dy, dz, rc/L
+};
+
+// Traversal record of one node (64 bytes).
+struct __align__(16) NodeRec {
+    double cx, cy, cz, bound;
+    double clear_core;  // clearance * largest core radius
+    int lo, hi, left, right;
+    double pad;
+};
+
+// Far-field coefficients: m0[3], m1[9] (row i, column j), w1[3], t2[3], w2[9], m2 symmetric [3][6] (00,01,02,11,12,22).
+#define BS_FAR_N 45
+struct __align__(16) Far64 { double v[BS_FAR_N + 1]; };
+struct __align__(16) Far32 { float v[BS_FAR_N + 3]; };
+
+enum { F_M0 = 0, F_M1 = 3, F_W1 = 12, F_T2 = 15, F_W2 = 18, F_M2 = 27 };
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Arithmetic helpers.
+// ---------------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ double norm3d(double x, double y, double z) {
+    double q = fma(x, x, fma(y, y, z * z));
+    // Outside [1e-290, 1e290] squares lose range: fall back to the scaled form the reference uses.
+    if (q > 1e-290 && q < 1e290) return sqrt(q);
+    return hypot(hypot(x, y), z);
+}
+
+static constexpr double AXIS_EPS64 = 8.0 * 2.220446049250313e-16;
+static constexpr float AXIS_EPS32 = 8.0f * 1.1920929e-07f;
+static constexpr double LAMB_A = 1.25643;
+static constexpr double LAMB_CUT = 2.821180356260211;   // sqrt(10 / 1.25643), OLAF's exponent cut-off
+static constexpr double LAMB_CUT2 = 7.959058602548491;  // 10 / 1.25643
+static constexpr double INV_FOUR_PI = 0.07957747154594767;  // 1 / (4 pi)
+
+// The reference pair (vortex_numba.pair_velocity) on an FP64 record; a = (p - s)/L given as the scaled offset.
+// Returns the flag; adds the velocity to (ux, uy, uz) only when the flag is ok.
+__device__ __forceinline__ int pair64(double ax, double ay, double az, const Seg64 &s, int model, int raise_singular,
+                                      double &ux, double &uy, double &uz) {
+    const double dx = s.dx, dy = s.dy, dz = s.dz;
+    double t = fma(az, dz, fma(ay, dy, ax * dx));
+    double cx = fma(dy, az, -dz * ay);
+    double cy = fma(dz, ax, -dx * az);
+    double cz = fma(dx, ay, -dy * ax);
+    double h = norm3d(cx, cy, cz);
+    double na = norm3d(ax, ay, az);
+    double nb = norm3d(ax - dx, ay - dy, az - dz);
+    if (!(isfinite(h) && isfinite(na) && isfinite(nb) && isfinite(t))) return BS_FLAG_NONFINITE;
+    double scale = fmax(1.0, fmax(na, nb));
+    if (h <= AXIS_EPS64 * scale) {
+        if (raise_singular && t >= 0.0 && t <= 1.0) return BS_FLAG_SINGULAR;
+        return BS_FLAG_OK;
+    }
+    if (s.gfac == 0.0) return BS_FLAG_OK;
+    double h2 = h * h;
+    double product = na * nb;
+    double dot = fma(t, t - 1.0, h2);
+    double plus = dot < 0.0 ? h2 / (product - dot) : product + dot;
+    double denominator = product * plus;
+    double factor = 1.0;
+    if (s.radius > 0.0 && model != 0) {
+        const double rc = s.rcl;
+        if (model == 5) {  // Rosenhead-Moore
+            na = hypot(na, rc);
+            nb = hypot(nb, rc);
+            product = na * nb;
+            double tr2 = fma(rc, rc, h2);
+            dot = fma(t, t - 1.0, tr2);
+            plus = dot < 0.0 ? tr2 / (product - dot) : product + dot;
+            denominator = product * plus;
+        } else if (model == 4) {  // offset
+            denominator = fma(rc, rc, denominator);
+        } else {
+            double ratio = h / rc;
+            if (!isfinite(ratio)) return BS_FLAG_NONFINITE;
+            if (model == 1) {
+                double l = fmin(ratio, 1.0);
+                factor = l * l;
+            } else if (model == 2) {
+                double r2 = ratio * ratio;
+                if (ratio <= LAMB_CUT) factor = -expm1(-LAMB_A * r2);
+            } else if (model == 3) {
+                if (ratio < 1.0) {
+                    double q = ratio * ratio;
+                    factor = q / hypot(1.0, q);
+                } else {
+                    double inv = 1.0 / ratio;
+                    factor = 1.0 / hypot(1.0, inv * inv);
+                }
+            }
+        }
+    }
+    double coefficient = s.gfac * factor * (na + nb) / denominator;
+    if (!(isfinite(denominator) && isfinite(coefficient) && isfinite(product) && isfinite(dot)))
+        return BS_FLAG_NONFINITE;
+    ux = fma(coefficient, cx, ux);
+    uy = fma(coefficient, cy, uy);
+    uz = fma(coefficient, cz, uz);
+    return BS_FLAG_OK;
+}
+
+// Convenience: the FP64 pair from an FP64 target position.
+__device__ __forceinline__ int pair64_at(double px, double py, double pz, const Seg64 &s, int model,
+                                         int raise_singular, double &ux, double &uy, double &uz) {
+    double ax = (px - s.sx) * s.inv_len, ay = (py - s.sy) * s.inv_len, az = (pz - s.sz) * s.inv_len;
+    return pair64(ax, ay, az, s, model, raise_singular, ux, uy, uz);
+}
+
+// Result of the single-precision pair: 0 = value added, 1 = needs the FP64 pair (near a segment within near_cores core
+// radii, near its axis within 1e-4 L (the reference's "suspect" rule, vortex_cuda.py:123-124), or any non-finite
+// intermediate, so that the FP64 pair decides flags exactly).
+__device__ __forceinline__ int pair32(float rx, float ry, float rz, const float4 &hi, const float4 &lo,
+                                      const float4 &dir, int model, float near2, float &ux, float &uy, float &uz) {
+    if (dir.w < 0.0f) return 1;  // core radius too small for FP32: FP64 decides (and flags, as the reference)
+    const float il = hi.w;
+    float ax = rx * il, ay = ry * il, az = rz * il;
+    const float dx = dir.x, dy = dir.y, dz = dir.z;
+    float t = fmaf(az, dz, fmaf(ay, dy, ax * dx));
+    float cx = fmaf(dy, az, -dz * ay);
+    float cy = fmaf(dz, ax, -dx * az);
+    float cz = fmaf(dx, ay, -dy * ax);
+    float h2 = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
+    float na2 = fmaf(ax, ax, fmaf(ay, ay, az * az));
+    float bx = ax - dx, by = ay - dy, bz = az - dz;
+    float nb2 = fmaf(bx, bx, fmaf(by, by, bz * bz));
+    float big2 = fmaxf(1.0f, fmaxf(na2, nb2));
+    const float rc = dir.w;
+    // distance^2 to the finite segment, in units of L^2
+    float seg2 = t < 0.0f ? na2 : (t > 1.0f ? nb2 : h2);
+    bool cored = rc > 0.0f && model != 0;
+    if (!(h2 > 1e-8f * big2) || (cored && seg2 < near2 * rc * rc) || !(na2 < 1e18f) || !(nb2 < 1e18f)) return 1;
+    float rna = rsqrtf(na2), rnb = rsqrtf(nb2);
+    float na = na2 * rna, nb = nb2 * rnb;
+    float product = na * nb;
+    float dot = fmaf(t, t - 1.0f, h2);
+    float plus = dot < 0.0f ? __fdividef(h2, product - dot) : product + dot;
+    float denominator = product * plus;
+    float factor = 1.0f;
+    if (cored) {
+        if (model == 5) {
+            float rc2 = rc * rc;
+            na = sqrtf(na2 + rc2);
+            nb = sqrtf(nb2 + rc2);
+            product = na * nb;
+            float tr2 = h2 + rc2;
+            dot = fmaf(t, t - 1.0f, tr2);
+            plus = dot < 0.0f ? __fdividef(tr2, product - dot) : product + dot;
+            denominator = product * plus;
+        } else if (model == 4) {
+            denominator = fmaf(rc, rc, denominator);
+        } else {
+            float r2 = __fdividef(h2, rc * rc);
+            if (model == 1) {
+                factor = fminf(r2, 1.0f);
+            } else if (model == 2) {
+                if (r2 <= (float)LAMB_CUT2) factor = -expm1f(-(float)LAMB_A * r2);
+            } else if (model == 3) {
+                factor = r2 < 1.0f ? r2 * rsqrtf(fmaf(r2, r2, 1.0f)) : rsqrtf(fmaf(__frcp_rn(r2), __frcp_rn(r2), 1.0f));
+            }
+        }
+    }
+    float coefficient = lo.w * factor * __fdividef(na + nb, denominator);
+    ux = fmaf(coefficient, cx, ux);
+    uy = fmaf(coefficient, cy, uy);
+    uz = fmaf(coefficient, cz, uz);
+    return 0;
+}
+
+// vortex_tree.far_velocity with the symmetric second moment; R = x - c.
+template <class T>
+__device__ __forceinline__ void far_eval(T rx, T ry, T rz, const T *f, int order, T &ux, T &uy, T &uz) {
+    T r2 = rx * rx + ry * ry + rz * rz;
+    T inv3 = T(1) / (r2 * sqrt(r2));
+    T inv5 = inv3 / r2;
+    T u0 = inv3 * (f[F_M0 + 1] * rz - f[F_M0 + 2] * ry);
+    T u1 = inv3 * (f[F_M0 + 2] * rx - f[F_M0 + 0] * rz);
+    T u2 = inv3 * (f[F_M0 + 0] * ry - f[F_M0 + 1] * rx);
+    if (order >= 1) {
+        T v0 = f[F_M1 + 0] * rx + f[F_M1 + 1] * ry + f[F_M1 + 2] * rz;
+        T v1 = f[F_M1 + 3] * rx + f[F_M1 + 4] * ry + f[F_M1 + 5] * rz;
+        T v2 = f[F_M1 + 6] * rx + f[F_M1 + 7] * ry + f[F_M1 + 8] * rz;
+        T k = T(3) * inv5;
+        u0 += k * (v1 * rz - v2 * ry) - inv3 * f[F_W1 + 0];
+        u1 += k * (v2 * rx - v0 * rz) - inv3 * f[F_W1 + 1];
+        u2 += k * (v0 * ry - v1 * rx) - inv3 * f[F_W1 + 2];
+    }
+    if (order >= 2) {
+        T inv7 = inv5 / r2;
+        T xx = rx * rx, xy = rx * ry, xz = rx * rz, yy = ry * ry, yz = ry * rz, zz = rz * rz;
+        T q[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const T *s = f + F_M2 + 6 * i;
+            q[i] = s[0] * xx + s[3] * yy + s[5] * zz + T(2) * (s[1] * xy + s[2] * xz + s[4] * yz);
+        }
+        T a = T(7.5) * inv7, b = T(1.5) * inv5, k = T(3) * inv5;
+        T b0 = a * q[0] - b * f[F_T2 + 0];
+        T b1 = a * q[1] - b * f[F_T2 + 1];
+        T b2 = a * q[2] - b * f[F_T2 + 2];
+        T s0 = f[F_W2 + 0] * rx + f[F_W2 + 1] * ry + f[F_W2 + 2] * rz;
+        T s1 = f[F_W2 + 3] * rx + f[F_W2 + 4] * ry + f[F_W2 + 5] * rz;
+        T s2 = f[F_W2 + 6] * rx + f[F_W2 + 7] * ry + f[F_W2 + 8] * rz;
+        u0 += (b1 * rz - b2 * ry) - k * s0;
+        u1 += (b2 * rx - b0 * rz) - k * s1;
+        u2 += (b0 * ry - b1 * rx) - k * s2;
+    }
+    ux += T(INV_FOUR_PI) * u0;
+    uy += T(INV_FOUR_PI) * u1;
+    uz += T(INV_FOUR_PI) * u2;
+}
+
+// Two-float split of an FP64 value: hi = round(x), lo = round(x - hi).
+__device__ __forceinline__ void split2(double x, float &hi, float &lo) {
+    hi = __double2float_rn(x);
+    lo = __double2float_rn(x - (double)hi);
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Bulk copies (TMA) with bounded mbarrier waits.
+// ---------------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// Global -> shared bulk copy completing on `bar`; dst/src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+// Waits for `phase` of `bar`; gives up after `limit` polls and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase, uint32_t limit = (1u << 26)) {
+    for (uint32_t i = 0; i < limit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+}  // namespace bs

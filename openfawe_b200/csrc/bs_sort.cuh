@@ -1,0 +1,14 @@
+// Device-wide exclusive scan and stable LSD radix sort (project-written; used by the tree builds).
+#pragma once
+#include "bs_internal.cuh"
+
+namespace bs {
+
+// out[i] = sum(in[0..i)); *total (device, may be null) = sum(in[0..n)).  in and out may alias.
+int scan_exclusive(const int64_t *in, int64_t *out, int64_t n, int64_t *total, Scratch &scratch, cudaStream_t s);
+
+// Stable sort of (keys, vals) by key bits [begin_bit, end_bit); results back in keys/vals.
+int radix_sort(uint64_t *keys, int32_t *vals, int64_t n, int begin_bit, int end_bit, Scratch &scratch,
+               cudaStream_t s);
+
+}  // namespace bs

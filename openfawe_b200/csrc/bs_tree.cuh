@@ -1,0 +1,45 @@
+// Internal tree object shared by the build, moments and evaluation translation units.
+#pragma once
+#include "bs_internal.cuh"
+
+namespace bs {
+
+// Per-segment geometry in input order, formed as vortex_tree.tree_sum forms it (vortex_tree.py:608-611):
+// lv = d * L, end = start + lv, alpha = gamma * lv (IEEE multiply then add, no contraction).
+struct __align__(16) SegGeo {
+    double sx, sy, sz, ex, ey, ez;
+    double lx, ly, lz, gamma, radius, pad;
+};
+
+int pack_segments(const bs_sources *src, const int32_t *order, Seg64 *seg64, Seg32 *seg32, SegGeo *geo,
+                  cudaStream_t s);
+int compute_moments(bs_tree *tree, const SegGeo *geo, Scratch &scratch, cudaStream_t s);
+
+}  // namespace bs
+
+struct bs_tree {
+    int device = 0;
+    int kind = 0;
+    cudaMemPool_t pool = nullptr;
+    int64_t m = 0, count = 0, leaf_size = 0;
+    int64_t *order = nullptr, *lo = nullptr, *hi = nullptr, *left = nullptr, *right = nullptr;  // export layout
+    int32_t *order32 = nullptr, *inverse = nullptr;                                              // position <-> id
+    double *centre = nullptr, *bound = nullptr, *core = nullptr, *m0 = nullptr, *m1 = nullptr, *m2 = nullptr;
+    double *w1 = nullptr, *t2 = nullptr, *w2 = nullptr;
+    bs::NodeRec *nodes = nullptr;
+    bs::Far64 *far64 = nullptr;
+    bs::Far32 *far32 = nullptr;
+    bs::Seg64 *seg64 = nullptr;  // tree order
+    bs::Seg32 *seg32 = nullptr;  // tree order
+    uint64_t *keys = nullptr;    // Morton keys (input order), Morton trees only
+    float build_ms = 0.f, moments_ms = 0.f;
+    void *blocks[32];
+    int nblocks = 0;
+    template <class T> T *alloc(size_t elems, cudaStream_t s) {
+        if (nblocks >= 32) return nullptr;
+        void *p = nullptr;
+        if (cudaMallocFromPoolAsync(&p, (elems ? elems : 1) * sizeof(T), pool, s) != cudaSuccess) return nullptr;
+        blocks[nblocks++] = p;
+        return static_cast<T *>(p);
+    }
+};

@@ -1,0 +1,1004 @@
+// Tree construction on the device: segment packing, Morton-key tree, the reference's median-split tree, node moments.
+//
+// Median tree: the rule of vortex_tree.build_tree (src/openfawe/aero/vortex_tree.py:51-115, 208-306): split a node of
+// more than leaf_size segments with a positive midpoint extent at the middle of its range after a stable sort along the
+// longest axis of the midpoint box (lower axis on a tie); depth-first numbering.  The sort is a radix sort by
+// (node, dense rank of the coordinate on its axis): LSD radix sorting is stable, so equal coordinates keep their current
+// order exactly as numpy's mergesort does.  The host walks the levels (reading one flag per node per level back), as the
+// reference's own GPU build does (src/openfawe/aero/vortex_cuda_build.py:234-275).
+//
+// Morton tree: 21-bit quantisation per axis in IEEE FP64 (no contraction), 63-bit interleaved keys, stable radix sort,
+// Karras's binary radix tree (ties broken by position), and a traversal tree made of the internal nodes holding more
+// than leaf_size segments plus their small children as leaves.  oracle/morton_oracle.c restates it on the CPU.
+//
+// Moments: vortex_tree.node_moments (vortex_tree.py:309-376) per node, split into chunks of CHUNK positions so that big
+// nodes use many blocks; partial sums are combined in chunk order (run-to-run repeatable).
+#include <algorithm>
+#include <vector>
+
+#include "bs_sort.cuh"
+#include "bs_tree.cuh"
+
+namespace bs {
+
+constexpr int CHUNK = 2048;
+constexpr int MOM_THREADS = 256;
+constexpr int MOM_PARTS = 31;  // r2 + m0 (3) + m1 (9) + m2 symmetric (18)
+
+__device__ __forceinline__ uint64_t ordered_bits(double x) {
+    uint64_t b = (uint64_t)__double_as_longlong(x + 0.0);  // -0.0 -> +0.0 (equal keys compare equal)
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double from_ordered(uint64_t k) {
+    uint64_t b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double((long long)b);
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Packing.
+// ---------------------------------------------------------------------------------------------------------------------
+__global__ void pack_kernel(int64_t m, const double *starts, const double *directions, const double *lengths,
+                            const double *gamma, const double *radius, const int32_t *order, Seg64 *seg64,
+                            Seg32 *seg32, SegGeo *geo) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    int64_t s = order ? order[k] : k;
+    double sx = starts[3 * s], sy = starts[3 * s + 1], sz = starts[3 * s + 2];
+    double dx = directions[3 * s], dy = directions[3 * s + 1], dz = directions[3 * s + 2];
+    double L = lengths[s], g = gamma[s], r = radius[s];
+    if (seg64) {
+        Seg64 q;
+        q.sx = sx; q.sy = sy; q.sz = sz;
+        q.inv_len = 1.0 / L;
+        q.dx = dx; q.dy = dy; q.dz = dz;
+        q.gfac = (g / L) / 12.566370614359172;  // (gamma / length) / (4 pi), vortex_numba.py:105
+        q.rcl = r / L;
+        q.radius = r;
+        seg64[k] = q;
+    }
+    if (seg32) {
+        Seg32 q;
+        split2(sx, q.hi.x, q.lo.x);
+        split2(sy, q.hi.y, q.lo.y);
+        split2(sz, q.hi.z, q.lo.z);
+        q.hi.w = (float)(1.0 / L);
+        q.lo.w = (float)((g / L) / 12.566370614359172);
+        // rc/L below FP32's comfortable range: mark the segment (-1) so that its pairs are always done in FP64
+        double rcl = r / L;
+        q.dir = make_float4((float)dx, (float)dy, (float)dz, r > 0.0 ? (rcl >= 1e-15 ? (float)rcl : -1.0f) : 0.0f);
+        seg32[k] = q;
+    }
+    if (geo) {
+        SegGeo q;
+        double lx = __dmul_rn(dx, L), ly = __dmul_rn(dy, L), lz = __dmul_rn(dz, L);
+        q.sx = sx; q.sy = sy; q.sz = sz;
+        q.ex = __dadd_rn(sx, lx); q.ey = __dadd_rn(sy, ly); q.ez = __dadd_rn(sz, lz);
+        q.lx = lx; q.ly = ly; q.lz = lz;
+        q.gamma = g;
+        q.radius = r;
+        q.pad = 0.0;
+        geo[k] = q;
+    }
+}
+
+int pack_segments(const bs_sources *src, const int32_t *order, Seg64 *seg64, Seg32 *seg32, SegGeo *geo,
+                  cudaStream_t s) {
+    if (src->m == 0) return BS_OK;
+    pack_kernel<<<(unsigned)((src->m + 255) / 256), 256, 0, s>>>(src->m, src->starts, src->directions, src->lengths,
+                                                                 src->gamma, src->radius, order, seg64, seg32, geo);
+    BS_CHECK_LAUNCH("pack_kernel");
+    return BS_OK;
+}
+
+// mid = 0.5 * (start + end) exactly as numpy forms it.
+__device__ __forceinline__ void midpoint(const SegGeo &g, double &x, double &y, double &z) {
+    x = __dmul_rn(0.5, __dadd_rn(g.sx, g.ex));
+    y = __dmul_rn(0.5, __dadd_rn(g.sy, g.ey));
+    z = __dmul_rn(0.5, __dadd_rn(g.sz, g.ez));
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Morton tree.
+// ---------------------------------------------------------------------------------------------------------------------
+__global__ void box_init_kernel(unsigned long long *box) {
+    if (threadIdx.x < 3) box[threadIdx.x] = ordered_bits(INFINITY);
+    else if (threadIdx.x < 6) box[threadIdx.x] = ordered_bits(-INFINITY);
+}
+
+__global__ void mid_box_kernel(int64_t m, const SegGeo *geo, unsigned long long *box) {
+    __shared__ unsigned long long sb[6];
+    if (threadIdx.x < 6) sb[threadIdx.x] = threadIdx.x < 3 ? ordered_bits(INFINITY) : ordered_bits(-INFINITY);
+    __syncthreads();
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < m; s += (int64_t)gridDim.x * blockDim.x) {
+        double v[3];
+        midpoint(geo[s], v[0], v[1], v[2]);
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(&sb[a], ordered_bits(v[a]));
+            atomicMax(&sb[3 + a], ordered_bits(v[a]));
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) atomicMin(&box[threadIdx.x], sb[threadIdx.x]);
+    else if (threadIdx.x < 6) atomicMax(&box[threadIdx.x], sb[threadIdx.x]);
+}
+
+__device__ __forceinline__ uint64_t spread3(uint32_t v) {
+    uint64_t x = v & 0x1fffffu;
+    x = (x | x << 32) & 0x1f00000000ffffull;
+    x = (x | x << 16) & 0x1f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+}
+
+// Keys of the spec in morton_oracle.c: q = min(2^21 - 1, trunc((mid - lo) * inv)), inv = 2^21 / max extent.
+__global__ void morton_keys_kernel(int64_t m, const SegGeo *geo, const unsigned long long *box, uint64_t *keys,
+                                   int32_t *vals) {
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= m) return;
+    double lo[3], ext = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = from_ordered(box[a]);
+        double e = __dsub_rn(from_ordered(box[3 + a]), lo[a]);
+        if (e > ext) ext = e;
+    }
+    double inv = ext > 0.0 ? __ddiv_rn(2097152.0, ext) : 0.0;
+    double v[3];
+    midpoint(geo[s], v[0], v[1], v[2]);
+    uint32_t q[3];
+    for (int a = 0; a < 3; ++a) {
+        uint32_t u = __double2uint_rz(__dmul_rn(__dsub_rn(v[a], lo[a]), inv));
+        q[a] = u > 2097151u ? 2097151u : u;
+    }
+    keys[s] = (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
+    vals[s] = (int32_t)s;
+}
+
+__device__ __forceinline__ int kdelta(const uint64_t *k, int64_t n, int64_t i, int64_t j) {
+    if (j < 0 || j >= n) return -1;
+    uint64_t a = k[i], b = k[j];
+    if (a == b) return 64 + __clzll((long long)(i ^ j));
+    return __clzll((long long)(a ^ b));
+}
+
+__global__ void karras_kernel(int64_t n, const uint64_t *k, int32_t *first, int32_t *last, int32_t *split) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int d = kdelta(k, n, i, i + 1) - kdelta(k, n, i, i - 1) > 0 ? 1 : -1;
+    int dmin = kdelta(k, n, i, i - d);
+    int64_t lmax = 2;
+    while (kdelta(k, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    int64_t l = 0;
+    for (int64_t t = lmax >> 1; t >= 1; t >>= 1)
+        if (kdelta(k, n, i, i + (l + t) * d) > dmin) l += t;
+    int64_t j = i + l * d;
+    int dnode = kdelta(k, n, i, j);
+    int64_t s = 0, t = l;
+    do {
+        t = (t + 1) >> 1;
+        if (kdelta(k, n, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    split[i] = (int32_t)(i + s * d + (d < 0 ? -1 : 0));
+    first[i] = (int32_t)(i < j ? i : j);
+    last[i] = (int32_t)(i < j ? j : i);
+}
+
+__device__ __forceinline__ bool big_internal(const int32_t *first, const int32_t *last, int64_t leaf, int64_t c,
+                                             bool is_leaf_segment) {
+    return !is_leaf_segment && (int64_t)(last[c] - first[c] + 1) > leaf;
+}
+
+__global__ void slot_count_kernel(int64_t n, const int32_t *first, const int32_t *last, const int32_t *split,
+                                  int64_t leaf, int64_t *count) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int64_t c = 0;
+    if ((int64_t)(last[i] - first[i] + 1) > leaf) {
+        int32_t g = split[i];
+        c = 1 + !big_internal(first, last, leaf, g, g == first[i]) + !big_internal(first, last, leaf, g + 1,
+                                                                                   g + 1 == last[i]);
+    }
+    count[i] = c;
+}
+
+__global__ void slot_fill_kernel(int64_t n, const int32_t *first, const int32_t *last, const int32_t *split,
+                                 int64_t leaf, const int64_t *slot, int64_t *lo, int64_t *hi, int64_t *left,
+                                 int64_t *right) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    if ((int64_t)(last[i] - first[i] + 1) <= leaf) return;
+    int64_t me = slot[i], next = me + 1;
+    int32_t g = split[i];
+    lo[me] = first[i];
+    hi[me] = (int64_t)last[i] + 1;
+    if (big_internal(first, last, leaf, g, g == first[i])) {
+        left[me] = slot[g];
+    } else {
+        left[me] = next;
+        lo[next] = first[i];
+        hi[next] = (int64_t)g + 1;
+        left[next] = right[next] = -1;
+        ++next;
+    }
+    if (big_internal(first, last, leaf, g + 1, g + 1 == last[i])) {
+        right[me] = slot[g + 1];
+    } else {
+        right[me] = next;
+        lo[next] = (int64_t)g + 1;
+        hi[next] = (int64_t)last[i] + 1;
+        left[next] = right[next] = -1;
+    }
+}
+
+__global__ void single_leaf_kernel(int64_t m, int64_t *lo, int64_t *hi, int64_t *left, int64_t *right) {
+    lo[0] = 0;
+    hi[0] = m;
+    left[0] = -1;
+    right[0] = -1;
+}
+
+__global__ void widen_order_kernel(int64_t m, const int32_t *order32, int64_t *order, int32_t *inverse) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    int32_t s = order32[k];
+    order[k] = s;
+    inverse[s] = (int32_t)k;
+}
+
+__global__ void iota_kernel(int64_t m, int32_t *v) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) v[k] = (int32_t)k;
+}
+
+static inline unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+static int build_morton(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_t s) {
+    const int64_t m = t->m;
+    unsigned long long *box = scratch.get<unsigned long long>(6);
+    uint64_t *keys = scratch.get<uint64_t>(m);
+    t->keys = t->alloc<uint64_t>(m, s);
+    t->order32 = t->alloc<int32_t>(m, s);
+    if (!box || !keys || !t->keys || !t->order32) return scratch.status != BS_OK ? scratch.status : BS_ERR_OOM;
+    box_init_kernel<<<1, 32, 0, s>>>(box);
+    mid_box_kernel<<<std::min<unsigned>(blocks_for(m, 256), 1184), 256, 0, s>>>(m, geo, box);
+    morton_keys_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, geo, box, keys, t->order32);
+    BS_CHECK_LAUNCH("morton keys");
+    BS_CUDA(cudaMemcpyAsync(t->keys, keys, m * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+    int rc = radix_sort(keys, t->order32, m, 0, 63, scratch, s);
+    if (rc != BS_OK) return rc;
+    if (m <= t->leaf_size || m == 1) {
+        t->count = 1;
+    } else {
+        int32_t *first = scratch.get<int32_t>(m - 1), *last = scratch.get<int32_t>(m - 1);
+        int32_t *split = scratch.get<int32_t>(m - 1);
+        int64_t *slot = scratch.get<int64_t>(m - 1), *total = scratch.get<int64_t>(1);
+        if (!first || !last || !split || !slot || !total) return scratch.status;
+        karras_kernel<<<blocks_for(m - 1, 256), 256, 0, s>>>(m, keys, first, last, split);
+        slot_count_kernel<<<blocks_for(m - 1, 256), 256, 0, s>>>(m, first, last, split, t->leaf_size, slot);
+        BS_CHECK_LAUNCH("karras");
+        rc = scan_exclusive(slot, slot, m - 1, total, scratch, s);
+        if (rc != BS_OK) return rc;
+        int64_t count = 0;
+        BS_CUDA(cudaMemcpyAsync(&count, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        BS_CUDA(cudaStreamSynchronize(s));
+        t->count = count;
+        t->lo = t->alloc<int64_t>(count, s);
+        t->hi = t->alloc<int64_t>(count, s);
+        t->left = t->alloc<int64_t>(count, s);
+        t->right = t->alloc<int64_t>(count, s);
+        if (!t->lo || !t->hi || !t->left || !t->right) return BS_ERR_OOM;
+        slot_fill_kernel<<<blocks_for(m - 1, 256), 256, 0, s>>>(m, first, last, split, t->leaf_size, slot, t->lo,
+                                                                t->hi, t->left, t->right);
+        BS_CHECK_LAUNCH("slot_fill_kernel");
+    }
+    if (t->count == 1) {
+        t->lo = t->alloc<int64_t>(1, s);
+        t->hi = t->alloc<int64_t>(1, s);
+        t->left = t->alloc<int64_t>(1, s);
+        t->right = t->alloc<int64_t>(1, s);
+        if (!t->lo || !t->hi || !t->left || !t->right) return BS_ERR_OOM;
+        single_leaf_kernel<<<1, 1, 0, s>>>(m, t->lo, t->hi, t->left, t->right);
+        BS_CHECK_LAUNCH("single_leaf_kernel");
+    }
+    return BS_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Median tree (the reference's rule).
+// ---------------------------------------------------------------------------------------------------------------------
+__global__ void axis_keys_kernel(int64_t m, const SegGeo *geo, int axis, uint64_t *keys, int32_t *vals) {
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= m) return;
+    double v[3];
+    midpoint(geo[s], v[0], v[1], v[2]);
+    keys[s] = ordered_bits(v[axis]);
+    vals[s] = (int32_t)s;
+}
+
+__global__ void distinct_kernel(int64_t m, const uint64_t *keys, int64_t *flag) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    flag[k] = (k == 0 || keys[k] != keys[k - 1]) ? 1 : 0;
+}
+
+__global__ void dense_rank_kernel(int64_t m, const int64_t *flag_scan, const int64_t *flag, const int32_t *vals,
+                                  uint32_t *rank) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    rank[vals[k]] = (uint32_t)(flag_scan[k] + flag[k] - 1);  // inclusive count - 1
+}
+
+struct Item {
+    int32_t node, start, end, pad;
+};
+
+// Midpoint box of one chunk of a level node's range.
+__global__ void level_box_kernel(const Item *items, int64_t nitems, const int32_t *order, const SegGeo *geo,
+                                 double *partial) {
+    __shared__ double red[6][MOM_THREADS / 32];
+    for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+        Item item = items[it];
+        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int k = item.start + threadIdx.x; k < item.end; k += blockDim.x) {
+            double v[3];
+            midpoint(geo[order[k]], v[0], v[1], v[2]);
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = fmin(lo[a], v[a]);
+                hi[a] = fmax(hi[a], v[a]);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1)
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = fmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+                hi[a] = fmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+            }
+        int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (lane == 0)
+            for (int a = 0; a < 3; ++a) { red[a][warp] = lo[a]; red[3 + a][warp] = hi[a]; }
+        __syncthreads();
+        if (threadIdx.x < 6) {
+            double v = red[threadIdx.x][0];
+            for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+                v = threadIdx.x < 3 ? fmin(v, red[threadIdx.x][w]) : fmax(v, red[threadIdx.x][w]);
+            partial[6 * it + threadIdx.x] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// Per level node: combine its chunks, longest axis (lowest on ties), split flag.
+__global__ void level_split_kernel(int64_t nodes, const int64_t *first_item, const int64_t *item_count,
+                                   const double *partial, int8_t *split, int8_t *axis_of) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nodes) return;
+    if (item_count[j] == 0) {
+        split[j] = 0;
+        axis_of[j] = 0;
+        return;
+    }
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t it = first_item[j]; it < first_item[j] + item_count[j]; ++it)
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = fmin(lo[a], partial[6 * it + a]);
+            hi[a] = fmax(hi[a], partial[6 * it + 3 + a]);
+        }
+    int axis = 0;
+    double extent = hi[0] - lo[0];
+    for (int c = 1; c < 3; ++c)
+        if (hi[c] - lo[c] > extent) { extent = hi[c] - lo[c]; axis = c; }
+    split[j] = extent > 0.0 ? 1 : 0;
+    axis_of[j] = (int8_t)axis;
+}
+
+// Keys (node rank in the sort list, dense coordinate rank on its axis) for the elements of splitting nodes.
+__global__ void level_gather_kernel(const Item *items, int64_t nitems, const int64_t *dest_offset,
+                                    const int8_t *axis_of, const int32_t *order, const uint32_t *rank_x,
+                                    const uint32_t *rank_y, const uint32_t *rank_z, int rank_bits, uint64_t *keys,
+                                    int32_t *vals) {
+    for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+        Item item = items[it];  // node = index in the sort list; start/end: positions; pad: node's range start
+        const uint32_t *rank = axis_of[item.node] == 0 ? rank_x : (axis_of[item.node] == 1 ? rank_y : rank_z);
+        for (int k = item.start + threadIdx.x; k < item.end; k += blockDim.x) {
+            int32_t s = order[k];
+            int64_t d = dest_offset[item.node] + (k - item.pad);
+            keys[d] = ((uint64_t)item.node << rank_bits) | rank[s];
+            vals[d] = s;
+        }
+    }
+}
+
+__global__ void level_scatter_kernel(const Item *items, int64_t nitems, const int64_t *dest_offset,
+                                     const int32_t *vals, int32_t *order) {
+    for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+        Item item = items[it];
+        for (int k = item.start + threadIdx.x; k < item.end; k += blockDim.x)
+            order[k] = vals[dest_offset[item.node] + (k - item.pad)];
+    }
+}
+
+static int bits_for(int64_t v) {
+    int b = 0;
+    while ((int64_t(1) << b) <= v) ++b;
+    return b;
+}
+
+template <class T> static int upload(Scratch &scratch, const std::vector<T> &v, T **dev, cudaStream_t s) {
+    *dev = scratch.get<T>(v.size());
+    if (!*dev) return scratch.status;
+    if (!v.empty()) BS_CUDA(cudaMemcpyAsync(*dev, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    return BS_OK;
+}
+
+static int build_median(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_t s) {
+    const int64_t m = t->m, leaf = t->leaf_size;
+    t->order32 = t->alloc<int32_t>(m, s);
+    if (!t->order32) return BS_ERR_OOM;
+    iota_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, t->order32);
+    BS_CHECK_LAUNCH("iota_kernel");
+    // Dense coordinate ranks per axis (equal coordinates share a rank).
+    uint32_t *rank[3];
+    uint64_t *keys = scratch.get<uint64_t>(m);
+    int32_t *vals = scratch.get<int32_t>(m);
+    int64_t *flag = scratch.get<int64_t>(m), *flag_scan = scratch.get<int64_t>(m);
+    if (!keys || !vals || !flag || !flag_scan) return scratch.status;
+    bool needs_sort = m > leaf;
+    for (int a = 0; a < 3 && needs_sort; ++a) {
+        rank[a] = scratch.get<uint32_t>(m);
+        if (!rank[a]) return scratch.status;
+        axis_keys_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, geo, a, keys, vals);
+        BS_CHECK_LAUNCH("axis_keys_kernel");
+        int rc = radix_sort(keys, vals, m, 0, 64, scratch, s);
+        if (rc != BS_OK) return rc;
+        distinct_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, keys, flag);
+        rc = scan_exclusive(flag, flag_scan, m, nullptr, scratch, s);
+        if (rc != BS_OK) return rc;
+        dense_rank_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, flag_scan, flag, vals, rank[a]);
+        BS_CHECK_LAUNCH("dense_rank_kernel");
+    }
+    const int rank_bits = bits_for(m);
+    int64_t capacity = 4 * (m / std::max<int64_t>(leaf, 1) + 1) + 1;
+    std::vector<int64_t> lo(capacity), hi(capacity), left(capacity, -1), right(capacity, -1);
+    lo[0] = 0;
+    hi[0] = m;
+    int64_t count = 1;
+    std::vector<int64_t> level{0};
+    while (!level.empty() && needs_sort) {
+        Scratch scratch(t->pool, s);  // this level's temporaries (shadows the call's scratch)
+        // chunks of every node that may split
+        std::vector<Item> items;
+        std::vector<int64_t> first_item(level.size()), item_count(level.size());
+        for (size_t j = 0; j < level.size(); ++j) {
+            int64_t a = lo[level[j]], b = hi[level[j]];
+            first_item[j] = (int64_t)items.size();
+            if (b - a > leaf)
+                for (int64_t c = a; c < b; c += CHUNK) items.push_back({(int32_t)j, (int32_t)c, (int32_t)std::min(b, c + CHUNK), 0});
+            item_count[j] = (int64_t)items.size() - first_item[j];
+        }
+        std::vector<int8_t> split(level.size(), 0), axis_of(level.size(), 0);
+        if (!items.empty()) {
+            Item *d_items;
+            int64_t *d_first, *d_count;
+            double *partial = scratch.get<double>(6 * items.size());
+            int8_t *d_split = scratch.get<int8_t>(level.size()), *d_axis = scratch.get<int8_t>(level.size());
+            int rc = upload(scratch, items, &d_items, s);
+            if (rc == BS_OK) rc = upload(scratch, first_item, &d_first, s);
+            if (rc == BS_OK) rc = upload(scratch, item_count, &d_count, s);
+            if (rc != BS_OK || !partial || !d_split || !d_axis) return rc != BS_OK ? rc : scratch.status;
+            level_box_kernel<<<(unsigned)std::min<size_t>(items.size(), 4096), MOM_THREADS, 0, s>>>(
+                d_items, (int64_t)items.size(), t->order32, geo, partial);
+            level_split_kernel<<<blocks_for((int64_t)level.size(), 128), 128, 0, s>>>(
+                (int64_t)level.size(), d_first, d_count, partial, d_split, d_axis);
+            BS_CHECK_LAUNCH("level box/split");
+            BS_CUDA(cudaMemcpyAsync(split.data(), d_split, level.size(), cudaMemcpyDeviceToHost, s));
+            BS_CUDA(cudaMemcpyAsync(axis_of.data(), d_axis, level.size(), cudaMemcpyDeviceToHost, s));
+            BS_CUDA(cudaStreamSynchronize(s));
+        }
+        // children (vortex_tree._next_level) and the sort list
+        std::vector<int64_t> following;
+        std::vector<Item> sort_items;
+        std::vector<int64_t> dest;
+        std::vector<int8_t> sort_axis;
+        int64_t total = 0;
+        for (size_t j = 0; j < level.size(); ++j) {
+            if (!split[j]) continue;
+            int64_t node = level[j], a = lo[node], b = hi[node], middle = (a + b) / 2;
+            int64_t f = count, g = count + 1;
+            count += 2;
+            lo[f] = a; hi[f] = middle; lo[g] = middle; hi[g] = b;
+            left[node] = f; right[node] = g;
+            following.push_back(f);
+            following.push_back(g);
+            int32_t r = (int32_t)dest.size();
+            dest.push_back(total);
+            sort_axis.push_back(axis_of[j]);
+            for (int64_t c = a; c < b; c += CHUNK) sort_items.push_back({r, (int32_t)c, (int32_t)std::min(b, c + CHUNK), (int32_t)a});
+            total += b - a;
+        }
+        if (total > 0) {
+            Item *d_items;
+            int64_t *d_dest;
+            int8_t *d_axis;
+            int rc = upload(scratch, sort_items, &d_items, s);
+            if (rc == BS_OK) rc = upload(scratch, dest, &d_dest, s);
+            if (rc == BS_OK) rc = upload(scratch, sort_axis, &d_axis, s);
+            if (rc != BS_OK) return rc;
+            unsigned grid = (unsigned)std::min<size_t>(sort_items.size(), 4096);
+            level_gather_kernel<<<grid, 256, 0, s>>>(d_items, (int64_t)sort_items.size(), d_dest, d_axis, t->order32,
+                                                     rank[0], rank[1], rank[2], rank_bits, keys, vals);
+            BS_CHECK_LAUNCH("level_gather_kernel");
+            rc = radix_sort(keys, vals, total, 0, rank_bits + bits_for((int64_t)dest.size() - 1), scratch, s);
+            if (rc != BS_OK) return rc;
+            level_scatter_kernel<<<grid, 256, 0, s>>>(d_items, (int64_t)sort_items.size(), d_dest, vals, t->order32);
+            BS_CHECK_LAUNCH("level_scatter_kernel");
+        }
+        level.swap(following);
+    }
+    // depth-first numbering (vortex_tree._renumber)
+    std::vector<int64_t> number(count), olo(count), ohi(count), oleft(count, -1), oright(count, -1), stack;
+    number[0] = 0;
+    olo[0] = lo[0];
+    ohi[0] = hi[0];
+    int64_t assigned = 1;
+    stack.push_back(0);
+    while (!stack.empty()) {
+        int64_t node = stack.back();
+        stack.pop_back();
+        if (left[node] < 0) continue;
+        int64_t f = assigned, g = assigned + 1;
+        assigned += 2;
+        number[left[node]] = f;
+        number[right[node]] = g;
+        oleft[number[node]] = f;
+        oright[number[node]] = g;
+        olo[f] = lo[left[node]]; ohi[f] = hi[left[node]];
+        olo[g] = lo[right[node]]; ohi[g] = hi[right[node]];
+        stack.push_back(right[node]);
+        stack.push_back(left[node]);
+    }
+    t->count = count;
+    t->lo = t->alloc<int64_t>(count, s);
+    t->hi = t->alloc<int64_t>(count, s);
+    t->left = t->alloc<int64_t>(count, s);
+    t->right = t->alloc<int64_t>(count, s);
+    if (!t->lo || !t->hi || !t->left || !t->right) return BS_ERR_OOM;
+    BS_CUDA(cudaMemcpyAsync(t->lo, olo.data(), count * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    BS_CUDA(cudaMemcpyAsync(t->hi, ohi.data(), count * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    BS_CUDA(cudaMemcpyAsync(t->left, oleft.data(), count * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    BS_CUDA(cudaMemcpyAsync(t->right, oright.data(), count * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    BS_CUDA(cudaStreamSynchronize(s));  // the host vectors above go out of scope
+    return BS_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Moments.
+// ---------------------------------------------------------------------------------------------------------------------
+__global__ void item_count_kernel(int64_t count, const int64_t *lo, const int64_t *hi, int64_t *n) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    int64_t size = hi[j] - lo[j];
+    n[j] = size > 0 ? (size + CHUNK - 1) / CHUNK : 0;
+}
+
+__global__ void item_fill_kernel(int64_t count, const int64_t *lo, const int64_t *hi, const int64_t *first,
+                                 Item *items) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    int64_t k = first[j];
+    for (int64_t c = lo[j]; c < hi[j]; c += CHUNK, ++k)
+        items[k] = {(int32_t)j, (int32_t)c, (int32_t)min(hi[j], c + CHUNK), 0};
+}
+
+// Endpoint box and largest core of one chunk.
+__global__ void __launch_bounds__(MOM_THREADS) moment_box_kernel(const Item *items, int64_t nitems,
+                                                                 const int32_t *order, const SegGeo *geo,
+                                                                 double *partial) {
+    __shared__ double red[7][MOM_THREADS / 32];
+    for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+        Item item = items[it];
+        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY}, core = 0.0;
+        for (int k = item.start + threadIdx.x; k < item.end; k += blockDim.x) {
+            SegGeo g = geo[order[k]];
+            double a[3] = {g.sx, g.sy, g.sz}, b[3] = {g.ex, g.ey, g.ez};
+            for (int x = 0; x < 3; ++x) {
+                lo[x] = fmin(lo[x], fmin(a[x], b[x]));
+                hi[x] = fmax(hi[x], fmax(a[x], b[x]));
+            }
+            core = fmax(core, g.radius);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            for (int x = 0; x < 3; ++x) {
+                lo[x] = fmin(lo[x], __shfl_xor_sync(0xffffffffu, lo[x], o));
+                hi[x] = fmax(hi[x], __shfl_xor_sync(0xffffffffu, hi[x], o));
+            }
+            core = fmax(core, __shfl_xor_sync(0xffffffffu, core, o));
+        }
+        int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (lane == 0) {
+            for (int x = 0; x < 3; ++x) { red[x][warp] = lo[x]; red[3 + x][warp] = hi[x]; }
+            red[6][warp] = core;
+        }
+        __syncthreads();
+        if (threadIdx.x < 7) {
+            double v = red[threadIdx.x][0];
+            for (int w = 1; w < MOM_THREADS / 32; ++w)
+                v = threadIdx.x < 3 ? fmin(v, red[threadIdx.x][w]) : fmax(v, red[threadIdx.x][w]);
+            partial[7 * it + threadIdx.x] = v;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void moment_centre_kernel(int64_t count, const int64_t *first, const int64_t *nitems,
+                                     const double *partial, double *centre, double *core) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY}, c = 0.0;
+    for (int64_t it = first[j]; it < first[j] + nitems[j]; ++it) {
+        for (int x = 0; x < 3; ++x) {
+            lo[x] = fmin(lo[x], partial[7 * it + x]);
+            hi[x] = fmax(hi[x], partial[7 * it + 3 + x]);
+        }
+        c = fmax(c, partial[7 * it + 6]);
+    }
+    for (int x = 0; x < 3; ++x) centre[3 * j + x] = 0.5 * (lo[x] + hi[x]);
+    core[j] = c;
+}
+
+// Bounding radius^2 and moments (m0, m1, symmetric m2) of one chunk about its node's centre.
+__global__ void __launch_bounds__(MOM_THREADS) moment_sum_kernel(const Item *items, int64_t nitems,
+                                                                 const int32_t *order, const SegGeo *geo,
+                                                                 const double *centre, double *partial) {
+    __shared__ double red[MOM_PARTS][MOM_THREADS / 32];
+    for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+        Item item = items[it];
+        const double c0 = centre[3 * item.node], c1 = centre[3 * item.node + 1], c2 = centre[3 * item.node + 2];
+        double acc[MOM_PARTS];
+#pragma unroll
+        for (int q = 0; q < MOM_PARTS; ++q) acc[q] = 0.0;
+        for (int k = item.start + threadIdx.x; k < item.end; k += blockDim.x) {
+            SegGeo g = geo[order[k]];
+            double a0 = g.sx - c0, a1 = g.sy - c1, a2 = g.sz - c2;
+            double b0 = g.ex - c0, b1 = g.ey - c1, b2 = g.ez - c2;
+            // the reference's ((x^2 + y^2) + z^2) without contraction: the bound is then bit-identical to the CPU's
+            double ra = __dadd_rn(__dadd_rn(__dmul_rn(a0, a0), __dmul_rn(a1, a1)), __dmul_rn(a2, a2));
+            double rb = __dadd_rn(__dadd_rn(__dmul_rn(b0, b0), __dmul_rn(b1, b1)), __dmul_rn(b2, b2));
+            acc[0] = fmax(acc[0], fmax(ra, rb));
+            if (g.gamma == 0.0) continue;
+            double d[3] = {0.5 * (g.sx + g.ex) - c0, 0.5 * (g.sy + g.ey) - c1, 0.5 * (g.sz + g.ez) - c2};
+            double l[3] = {g.lx, g.ly, g.lz};
+            double al[3] = {g.gamma * g.lx, g.gamma * g.ly, g.gamma * g.lz};
+            double sym[6];
+            int q = 0;
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+#pragma unroll
+                for (int k2 = j; k2 < 3; ++k2) sym[q++] = d[j] * d[k2] + l[j] * l[k2] * (1.0 / 12.0);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                acc[1 + i] += al[i];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) acc[4 + 3 * i + j] += al[i] * d[j];
+#pragma unroll
+                for (int p = 0; p < 6; ++p) acc[13 + 6 * i + p] += al[i] * sym[p];
+            }
+        }
+        int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+        for (int q = 0; q < MOM_PARTS; ++q) {
+            double v = acc[q];
+            for (int o = 16; o > 0; o >>= 1) {
+                double w = __shfl_xor_sync(0xffffffffu, v, o);
+                v = q == 0 ? fmax(v, w) : v + w;
+            }
+            if (lane == 0) red[q][warp] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < MOM_PARTS) {
+            double v = red[threadIdx.x][0];
+            for (int w = 1; w < MOM_THREADS / 32; ++w)
+                v = threadIdx.x == 0 ? fmax(v, red[0][w]) : v + red[threadIdx.x][w];
+            partial[(int64_t)MOM_PARTS * it + threadIdx.x] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// Combine chunks in order; write the export arrays, the contractions and the packed traversal/far records.
+__global__ void moment_final_kernel(int64_t count, const int64_t *first, const int64_t *nitems,
+                                    const double *partial, const int64_t *lo, const int64_t *hi,
+                                    const int64_t *left, const int64_t *right, const double *centre,
+                                    const double *core, double *bound, double *m0, double *m1, double *m2,
+                                    double *w1, double *t2, double *w2, NodeRec *nodes, Far64 *far64,
+                                    Far32 *far32) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    double v[MOM_PARTS];
+    for (int q = 0; q < MOM_PARTS; ++q) v[q] = 0.0;
+    for (int64_t it = first[j]; it < first[j] + nitems[j]; ++it)
+        for (int q = 0; q < MOM_PARTS; ++q) {
+            double p = partial[(int64_t)MOM_PARTS * it + q];
+            v[q] = q == 0 ? fmax(v[q], p) : v[q] + p;
+        }
+    double b = sqrt(v[0]) * (1.0 + 1e-12);
+    bound[j] = b;
+    const double *M0 = v + 1, *M1 = v + 4, *S = v + 13;  // S[6 i + p], p over (00,01,02,11,12,22)
+    auto M2 = [&](int i, int a, int c) -> double {
+        int lo_ = a < c ? a : c, hi_ = a < c ? c : a;
+        int p = lo_ == 0 ? hi_ : (lo_ == 1 ? 2 + hi_ : 5);
+        return S[6 * i + p];
+    };
+    for (int i = 0; i < 3; ++i) {
+        m0[3 * j + i] = M0[i];
+        for (int a = 0; a < 3; ++a) {
+            m1[9 * j + 3 * i + a] = M1[3 * i + a];
+            for (int c = 0; c < 3; ++c) m2[27 * j + 9 * i + 3 * a + c] = M2(i, a, c);
+        }
+    }
+    double W1[3] = {M1[5] - M1[7], M1[6] - M1[2], M1[1] - M1[3]};
+    double T2[3], W2[9];
+    for (int i = 0; i < 3; ++i) T2[i] = M2(i, 0, 0) + M2(i, 1, 1) + M2(i, 2, 2);
+    for (int k = 0; k < 3; ++k) {
+        W2[0 + k] = M2(1, 2, k) - M2(2, 1, k);
+        W2[3 + k] = M2(2, 0, k) - M2(0, 2, k);
+        W2[6 + k] = M2(0, 1, k) - M2(1, 0, k);
+    }
+    for (int i = 0; i < 3; ++i) { w1[3 * j + i] = W1[i]; t2[3 * j + i] = T2[i]; }
+    for (int q = 0; q < 9; ++q) w2[9 * j + q] = W2[q];
+    double f[BS_FAR_N];
+    for (int i = 0; i < 3; ++i) f[F_M0 + i] = M0[i];
+    for (int q = 0; q < 9; ++q) f[F_M1 + q] = M1[q];
+    for (int i = 0; i < 3; ++i) { f[F_W1 + i] = W1[i]; f[F_T2 + i] = T2[i]; }
+    for (int q = 0; q < 9; ++q) f[F_W2 + q] = W2[q];
+    for (int q = 0; q < 18; ++q) f[F_M2 + q] = S[q];
+    for (int q = 0; q < BS_FAR_N; ++q) {
+        far64[j].v[q] = f[q];
+        far32[j].v[q] = (float)f[q];
+    }
+    NodeRec r;
+    r.cx = centre[3 * j]; r.cy = centre[3 * j + 1]; r.cz = centre[3 * j + 2];
+    r.bound = b;
+    r.clear_core = core[j];
+    r.lo = (int)lo[j]; r.hi = (int)hi[j]; r.left = (int)left[j]; r.right = (int)right[j];
+    r.pad = 0.0;
+    nodes[j] = r;
+}
+
+int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_t s) {
+    const int64_t count = t->count;
+    t->centre = t->alloc<double>(3 * count, s);
+    t->bound = t->alloc<double>(count, s);
+    t->core = t->alloc<double>(count, s);
+    t->m0 = t->alloc<double>(3 * count, s);
+    t->m1 = t->alloc<double>(9 * count, s);
+    t->m2 = t->alloc<double>(27 * count, s);
+    t->w1 = t->alloc<double>(3 * count, s);
+    t->t2 = t->alloc<double>(3 * count, s);
+    t->w2 = t->alloc<double>(9 * count, s);
+    t->nodes = t->alloc<NodeRec>(count, s);
+    t->far64 = t->alloc<Far64>(count, s);
+    t->far32 = t->alloc<Far32>(count, s);
+    if (!t->centre || !t->bound || !t->core || !t->m0 || !t->m1 || !t->m2 || !t->w1 || !t->t2 || !t->w2 ||
+        !t->nodes || !t->far64 || !t->far32)
+        return BS_ERR_OOM;
+    int64_t *nitems = scratch.get<int64_t>(count), *first = scratch.get<int64_t>(count);
+    int64_t *total = scratch.get<int64_t>(1);
+    if (!nitems || !first || !total) return scratch.status;
+    item_count_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->lo, t->hi, nitems);
+    BS_CHECK_LAUNCH("item_count_kernel");
+    int rc = scan_exclusive(nitems, first, count, total, scratch, s);
+    if (rc != BS_OK) return rc;
+    int64_t n_items = 0;
+    BS_CUDA(cudaMemcpyAsync(&n_items, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    BS_CUDA(cudaStreamSynchronize(s));
+    Item *items = scratch.get<Item>(n_items);
+    double *box = scratch.get<double>(7 * n_items), *sums = scratch.get<double>(MOM_PARTS * n_items);
+    if (!items || !box || !sums) return scratch.status;
+    item_fill_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->lo, t->hi, first, items);
+    unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(n_items, 8192));
+    moment_box_kernel<<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, box);
+    moment_centre_kernel<<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, box, t->centre, t->core);
+    moment_sum_kernel<<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, t->centre, sums);
+    moment_final_kernel<<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, sums, t->lo, t->hi, t->left,
+                                                               t->right, t->centre, t->core, t->bound, t->m0, t->m1,
+                                                               t->m2, t->w1, t->t2, t->w2, t->nodes, t->far64,
+                                                               t->far32);
+    BS_CHECK_LAUNCH("moments");
+    return BS_OK;
+}
+
+}  // namespace bs
+
+using namespace bs;
+
+// Shared tail of both constructors: inverse permutation, int64 order, tree-ordered segment records, moments.
+static int finish_tree(bs_tree *t, const bs_sources *src, const SegGeo *geo, Scratch &scratch, cudaStream_t s) {
+    const int64_t m = t->m;
+    if (!t->order) t->order = t->alloc<int64_t>(m, s);
+    t->inverse = t->alloc<int32_t>(m, s);
+    t->seg64 = t->alloc<Seg64>(m, s);
+    t->seg32 = t->alloc<Seg32>(m, s);
+    if (!t->order || !t->inverse || !t->seg64 || !t->seg32) return BS_ERR_OOM;
+    widen_order_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, t->order32, t->order, t->inverse);
+    BS_CHECK_LAUNCH("widen_order_kernel");
+    int rc = pack_segments(src, t->order32, t->seg64, t->seg32, nullptr, s);
+    if (rc != BS_OK) return rc;
+    return compute_moments(t, geo, scratch, s);
+}
+
+static int check_sources(const bs_sources *src) {
+    if (!src || src->m < 0 || (src->m > 0 && (!src->starts || !src->directions || !src->lengths || !src->gamma ||
+                                               !src->radius))) {
+        set_error("invalid segment arrays");
+        return BS_ERR_ARG;
+    }
+    if (src->m >= (int64_t(1) << 31) - 1) {
+        set_error("at most 2^31 - 2 segments are supported (got %lld)", (long long)src->m);
+        return BS_ERR_ARG;
+    }
+    return BS_OK;
+}
+
+extern "C" void bs_tree_free(bs_tree *tree) {
+    if (!tree) return;
+    cudaSetDevice(tree->device);
+    cudaDeviceSynchronize();
+    for (int i = 0; i < tree->nblocks; ++i) cudaFreeAsync(tree->blocks[i], 0);
+    cudaStreamSynchronize(0);
+    delete tree;
+}
+
+extern "C" int64_t bs_tree_count(const bs_tree *tree) { return tree ? tree->count : -1; }
+
+extern "C" int bs_tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_tree **out,
+                             bs_stream stream) {
+    if (!ctx || !tp || !out) {
+        set_error("bs_tree_build: null argument");
+        return BS_ERR_ARG;
+    }
+    *out = nullptr;
+    int rc = check_sources(src);
+    if (rc != BS_OK) return rc;
+    if (src->m == 0) {
+        set_error("bs_tree_build: no segments");
+        return BS_ERR_ARG;
+    }
+    if (tp->leaf_size < 1 || (tp->kind != BS_TREE_MEDIAN && tp->kind != BS_TREE_MORTON)) {
+        set_error("bs_tree_build: leaf size must be positive and kind median or morton");
+        return BS_ERR_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    BS_CUDA(cudaSetDevice(ctx->device));
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&e2);
+    cudaEventRecord(e0, s);
+    bs_tree *t = new bs_tree();
+    t->device = ctx->device;
+    t->pool = ctx->pool;
+    t->kind = tp->kind;
+    t->m = src->m;
+    t->leaf_size = tp->leaf_size;
+    {
+        Scratch scratch(ctx->pool, s);
+        SegGeo *geo = scratch.get<SegGeo>(src->m);
+        rc = geo ? pack_segments(src, nullptr, nullptr, nullptr, geo, s) : scratch.status;
+        if (rc == BS_OK) rc = tp->kind == BS_TREE_MORTON ? build_morton(t, geo, scratch, s) : build_median(t, geo, scratch, s);
+        if (rc == BS_OK) {
+            cudaEventRecord(e1, s);
+            rc = finish_tree(t, src, geo, scratch, s);
+        }
+        cudaEventRecord(e2, s);
+        if (rc == BS_OK) {
+            cudaError_t e = cudaEventSynchronize(e2);
+            if (e != cudaSuccess) rc = cuda_fail(e, "tree build");
+        }
+    }
+    if (rc == BS_OK) {
+        cudaEventElapsedTime(&t->build_ms, e0, e1);
+        cudaEventElapsedTime(&t->moments_ms, e1, e2);
+        ctx->stats.build_ms = t->build_ms;
+        ctx->stats.moments_ms = t->moments_ms;
+        ctx->stats.nodes = t->count;
+        ctx->stats.segments = t->m;
+        *out = t;
+    } else {
+        bs_tree_free(t);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    return rc;
+}
+
+__global__ void narrow_order_kernel(int64_t m, const int64_t *order, int32_t *order32) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) order32[k] = (int32_t)order[k];
+}
+
+extern "C" int bs_tree_from_arrays(bs_ctx *ctx, const bs_sources *src, const int64_t *order, const int64_t *lo,
+                                   const int64_t *hi, const int64_t *left, const int64_t *right, int64_t count,
+                                   bs_tree **out, bs_stream stream) {
+    if (!ctx || !out || !order || !lo || !hi || !left || !right || count < 1) {
+        set_error("bs_tree_from_arrays: null argument or empty tree");
+        return BS_ERR_ARG;
+    }
+    *out = nullptr;
+    int rc = check_sources(src);
+    if (rc != BS_OK) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    BS_CUDA(cudaSetDevice(ctx->device));
+    bs_tree *t = new bs_tree();
+    t->device = ctx->device;
+    t->pool = ctx->pool;
+    t->kind = -1;
+    t->m = src->m;
+    t->count = count;
+    {
+        Scratch scratch(ctx->pool, s);
+        SegGeo *geo = scratch.get<SegGeo>(src->m);
+        t->order = t->alloc<int64_t>(t->m, s);
+        t->order32 = t->alloc<int32_t>(t->m, s);
+        t->lo = t->alloc<int64_t>(count, s);
+        t->hi = t->alloc<int64_t>(count, s);
+        t->left = t->alloc<int64_t>(count, s);
+        t->right = t->alloc<int64_t>(count, s);
+        if (!geo || !t->order || !t->order32 || !t->lo || !t->hi || !t->left || !t->right) rc = BS_ERR_OOM;
+        if (rc == BS_OK) {
+            cudaMemcpyAsync(t->order, order, t->m * sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(t->lo, lo, count * sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(t->hi, hi, count * sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(t->left, left, count * sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(t->right, right, count * sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
+            narrow_order_kernel<<<blocks_for(t->m, 256), 256, 0, s>>>(t->m, order, t->order32);
+            rc = pack_segments(src, nullptr, nullptr, nullptr, geo, s);
+        }
+        if (rc == BS_OK) rc = finish_tree(t, src, geo, scratch, s);
+        if (rc == BS_OK) {
+            cudaError_t e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) rc = cuda_fail(e, "tree from arrays");
+        }
+    }
+    if (rc == BS_OK) *out = t;
+    else bs_tree_free(t);
+    return rc;
+}
+
+extern "C" int bs_tree_export(const bs_tree *t, int64_t *order, int64_t *lo, int64_t *hi, int64_t *left,
+                              int64_t *right, double *centre, double *bound, double *core, double *m0, double *m1,
+                              double *m2, double *w1, double *t2, double *w2, bs_stream stream) {
+    if (!t) {
+        set_error("bs_tree_export: null tree");
+        return BS_ERR_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t c = t->count;
+    const size_t m8 = (size_t)t->m * 8, c8 = (size_t)c * 8;
+    struct { void *dst; const void *src; size_t bytes; } copies[] = {
+        {order, t->order, m8}, {lo, t->lo, c8}, {hi, t->hi, c8}, {left, t->left, c8}, {right, t->right, c8},
+        {centre, t->centre, 3 * c8}, {bound, t->bound, c8}, {core, t->core, c8}, {m0, t->m0, 3 * c8},
+        {m1, t->m1, 9 * c8}, {m2, t->m2, 27 * c8}, {w1, t->w1, 3 * c8}, {t2, t->t2, 3 * c8}, {w2, t->w2, 9 * c8}};
+    for (auto &cp : copies)
+        if (cp.dst) BS_CUDA(cudaMemcpyAsync(cp.dst, cp.src, cp.bytes, cudaMemcpyDeviceToDevice, s));
+    return BS_OK;
+}
+
+__global__ void widen_keys_order_kernel(int64_t m, const int32_t *order32, int64_t *out) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) out[k] = order32[k];
+}
+
+extern "C" int bs_tree_keys(const bs_tree *t, uint64_t *keys, int64_t *sorted_order, bs_stream stream) {
+    if (!t || t->kind != BS_TREE_MORTON) {
+        set_error("bs_tree_keys: not a Morton tree");
+        return BS_ERR_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    if (keys) BS_CUDA(cudaMemcpyAsync(keys, t->keys, t->m * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+    if (sorted_order) {
+        widen_keys_order_kernel<<<blocks_for(t->m, 256), 256, 0, s>>>(t->m, t->order32, sorted_order);
+        BS_CHECK_LAUNCH("widen_keys_order_kernel");
+    }
+    return BS_OK;
+}

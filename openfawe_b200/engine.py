@@ -1,0 +1,205 @@
+"""Device-resident interface of the B200 library: PyTorch CUDA tensors in, PyTorch CUDA tensors out.
+
+The drop-in backends (``vortex_cuda.cuda_sum``, ``vortex_cuda_tree.cuda_tree_sum``) take NumPy arrays like the
+reference's; this module is the layer below them, for callers that keep wakes in HBM across calls (build a tree once,
+evaluate it at several target sets, or time the kernels without host copies).  All work is enqueued on the current
+PyTorch stream of the tensors' device.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .settings import PRECISION_CODES
+
+_BLOCKS = (32, 64, 128, 256)
+
+
+def _device_of(device):
+    if device is None:
+        return torch.device("cuda", torch.cuda.current_device())
+    if isinstance(device, int):
+        return torch.device("cuda", device)
+    return torch.device(device)
+
+
+def f64(a, device):
+    """A C-contiguous float64 tensor on `device` (copies only when needed)."""
+    t = a if isinstance(a, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64))
+    return t.to(device=device, dtype=torch.float64).contiguous()
+
+
+def i64(a, device):
+    t = a if isinstance(a, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(a, dtype=np.int64))
+    return t.to(device=device, dtype=torch.int64).contiguous()
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() else ctypes.c_void_p(0)
+
+
+def _stream(device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+class Sources:
+    """Directed segments resident on one device: starts [m,3], directions [m,3], lengths, gamma, radius [m]."""
+
+    def __init__(self, starts, directions, lengths, gamma, radius, device=None):
+        self.device = _device_of(device)
+        self.starts = f64(starts, self.device).reshape(-1, 3)
+        self.directions = f64(directions, self.device).reshape(-1, 3)
+        self.lengths = f64(lengths, self.device).reshape(-1)
+        self.gamma = f64(gamma, self.device).reshape(-1)
+        self.radius = f64(radius, self.device).reshape(-1)
+        self.m = int(self.starts.shape[0])
+
+    def struct(self):
+        return L.Sources(self.m, _ptr(self.starts), _ptr(self.directions), _ptr(self.lengths), _ptr(self.gamma),
+                         _ptr(self.radius))
+
+
+class Targets:
+    """Target points [n,3] and optional exclusion CSR (ptr [n+1], seg [e], per-target sorted unique)."""
+
+    def __init__(self, points, csr=None, device=None):
+        self.device = _device_of(device)
+        self.points = f64(points, self.device).reshape(-1, 3)
+        self.n = int(self.points.shape[0])
+        self.ex_ptr = self.ex_seg = None
+        self.e = 0
+        if csr is not None and len(csr[1]):
+            self.ex_ptr = i64(csr[0], self.device)
+            self.ex_seg = i64(csr[1], self.device)
+            self.e = int(self.ex_seg.numel())
+
+    def struct(self):
+        return L.Targets(self.n, _ptr(self.points), _ptr(self.ex_ptr), _ptr(self.ex_seg), self.e)
+
+
+def kernel_params(model, singularity="raise", precision="fp64", block=128, near=3.0):
+    if int(block) not in _BLOCKS:
+        raise ValueError("cuda block must be 32, 64, 128 or 256")
+    code = PRECISION_CODES[precision] if isinstance(precision, str) else int(precision)
+    return L.KernelParams(int(model), int(singularity == "raise"), code, int(block), float(near))
+
+
+def tree_params(theta=0.5, order=2, leaf_size=32, clearance=3.0, kind="median", stack_limit=0):
+    code = {"median": L.BS_TREE_MEDIAN, "morton": L.BS_TREE_MORTON}[kind] if isinstance(kind, str) else int(kind)
+    return L.TreeParams(float(theta), int(order), int(leaf_size), float(clearance), code, int(stack_limit))
+
+
+def direct(sources, targets, model, singularity="raise", precision="fp64", block=128, near=3.0):
+    """Exact direct sum: returns (velocity [n,3] float64, flags [n] int8) device tensors."""
+    dev = sources.device
+    out = torch.empty((targets.n, 3), dtype=torch.float64, device=dev)
+    flags = torch.empty(targets.n, dtype=torch.int8, device=dev)
+    src, tgt = sources.struct(), targets.struct()
+    kp = kernel_params(model, singularity, precision, block, near)
+    L.check(L.library().bs_direct(L.context(dev.index), ctypes.byref(src), ctypes.byref(tgt), ctypes.byref(kp),
+                                  _ptr(out), _ptr(flags), _stream(dev)), "bs_direct")
+    return out, flags
+
+
+class Tree:
+    """A tree on the device (freed with the object)."""
+
+    def __init__(self, handle, sources, params):
+        self._handle = handle
+        self.sources = sources
+        self.params = params
+        self.count = int(L.library().bs_tree_count(handle))
+
+    def __del__(self):
+        handle, self._handle = getattr(self, "_handle", None), None
+        if handle:
+            try:
+                L.library().bs_tree_free(handle)
+            except Exception:  # noqa: BLE001 - interpreter shutdown
+                pass
+
+    @property
+    def handle(self):
+        return self._handle
+
+    def export(self):
+        """The tree arrays in the reference's layout (vortex_tree.build_tree / node_moments / node_contractions) as
+        NumPy arrays: order, lo, hi, left, right, centre, bound, core, m0, m1, m2, w1, t2, w2."""
+        dev, c, m = self.sources.device, self.count, self.sources.m
+        shapes = dict(order=(m,), lo=(c,), hi=(c,), left=(c,), right=(c,), centre=(c, 3), bound=(c,), core=(c,),
+                      m0=(c, 3), m1=(c, 3, 3), m2=(c, 3, 3, 3), w1=(c, 3), t2=(c, 3), w2=(c, 3, 3))
+        ints = ("order", "lo", "hi", "left", "right")
+        t = {k: torch.empty(v, dtype=torch.int64 if k in ints else torch.float64, device=dev)
+             for k, v in shapes.items()}
+        L.check(L.library().bs_tree_export(self._handle, *[_ptr(t[k]) for k in shapes], _stream(dev)),
+                "bs_tree_export")
+        return {k: v.cpu().numpy() for k, v in t.items()}
+
+    def keys(self):
+        """Morton keys (input order, uint64) and their stable sort permutation (Morton trees only)."""
+        dev, m = self.sources.device, self.sources.m
+        keys = torch.empty(m, dtype=torch.int64, device=dev)
+        order = torch.empty(m, dtype=torch.int64, device=dev)
+        L.check(L.library().bs_tree_keys(self._handle, _ptr(keys), _ptr(order), _stream(dev)), "bs_tree_keys")
+        return keys.cpu().numpy().view(np.uint64), order.cpu().numpy()
+
+
+def build_tree(sources, theta=0.5, order=2, leaf_size=32, clearance=3.0, kind="median"):
+    """Build a tree (median or Morton) with FP64 node moments on the device."""
+    dev = sources.device
+    params = tree_params(theta, order, leaf_size, clearance, kind)
+    handle = ctypes.c_void_p()
+    src = sources.struct()
+    L.check(L.library().bs_tree_build(L.context(dev.index), ctypes.byref(src), ctypes.byref(params),
+                                      ctypes.byref(handle), _stream(dev)), "bs_tree_build")
+    return Tree(handle, sources, params)
+
+
+def tree_from_arrays(sources, order, lo, hi, left, right):
+    """A tree given as the reference's arrays (vortex_tree.build_tree output); moments computed on the device."""
+    dev = sources.device
+    arrays = [i64(a, dev) for a in (order, lo, hi, left, right)]
+    handle = ctypes.c_void_p()
+    src = sources.struct()
+    L.check(L.library().bs_tree_from_arrays(L.context(dev.index), ctypes.byref(src), *[_ptr(a) for a in arrays],
+                                            int(arrays[1].numel()), ctypes.byref(handle), _stream(dev)),
+            "bs_tree_from_arrays")
+    return Tree(handle, sources, tree_params())
+
+
+def tree_eval(tree, targets, model, singularity="raise", precision="fp64", block=128, near=3.0, theta=0.5,
+              order=2, clearance=3.0, stack_limit=0, far_counts=True):
+    """Evaluate a tree at the targets: (velocity [n,3] float64, flags [n] int8, far counts [n] int64 or None)."""
+    dev = tree.sources.device
+    out = torch.empty((targets.n, 3), dtype=torch.float64, device=dev)
+    flags = torch.empty(targets.n, dtype=torch.int8, device=dev)
+    far = torch.empty(targets.n, dtype=torch.int64, device=dev) if far_counts else None
+    tp = tree_params(theta, order, tree.params.leaf_size, clearance, tree.params.kind, stack_limit)
+    kp = kernel_params(model, singularity, precision, block, near)
+    tgt = targets.struct()
+    L.check(L.library().bs_tree_eval(L.context(dev.index), tree.handle, ctypes.byref(tp), ctypes.byref(tgt),
+                                     ctypes.byref(kp), _ptr(out), _ptr(flags), _ptr(far), _stream(dev)),
+            "bs_tree_eval")
+    return out, flags, far
+
+
+def tree_sum(sources, targets, model, singularity="raise", precision="mixed", block=128, near=3.0, theta=0.5,
+             order=2, leaf_size=32, clearance=3.0, kind="median", stack_limit=0, far_counts=True):
+    """Build, evaluate and free in one library call."""
+    dev = sources.device
+    out = torch.empty((targets.n, 3), dtype=torch.float64, device=dev)
+    flags = torch.empty(targets.n, dtype=torch.int8, device=dev)
+    far = torch.empty(targets.n, dtype=torch.int64, device=dev) if far_counts else None
+    tp = tree_params(theta, order, leaf_size, clearance, kind, stack_limit)
+    kp = kernel_params(model, singularity, precision, block, near)
+    src, tgt = sources.struct(), targets.struct()
+    L.check(L.library().bs_tree_sum(L.context(dev.index), ctypes.byref(src), ctypes.byref(tp), ctypes.byref(tgt),
+                                    ctypes.byref(kp), _ptr(out), _ptr(flags), _ptr(far), _stream(dev)),
+            "bs_tree_sum")
+    return out, flags, far
+
+
+def last_stats(device=0):
+    """Counters and device times of the last call on `device` (bs_last_stats)."""
+    return L.stats(device)

@@ -1,0 +1,108 @@
+"""Drop-in for the reference's GPU tree backend ``openfawe.aero.vortex_cuda_tree`` (src/openfawe/aero/vortex_cuda_tree.py).
+
+Same public names and call signature: ``Statistics`` and ``cuda_tree_sum(points, starts, directions, lengths, gamma,
+radius, model, csr, singularity, tree, settings, *, targets_per_launch=None, stack_size=512, block=None) ->
+(out, any_flag)`` (vortex_cuda_tree.py:439-595).  Everything runs on the device in libbs_b200:
+
+* the tree: by default the reference's median-split tree (vortex_tree.build_tree), element for element, built on the
+  GPU; with ``settings.tree == 'morton'`` this library's Morton-key tree;
+* node centres, bounding radii, largest cores, moments and contractions in FP64 (vortex_tree.node_moments);
+* the traversal of vortex_tree.tree_velocity with the FP64 acceptance test of the reference's GPU kernels, so the
+  accepted nodes are those of the CPU tree code; ``fp64`` evaluates pairs and expansions in FP64, ``mixed``/``fp32``
+  in FP32 on two-float coordinates with FP64 re-evaluation near segments (no target goes to the CPU, whatever
+  ``settings.suspect`` says).
+
+Errors as in the reference: ValueError for unsupported core models, theta >= 1, fp64 with suspect='gpu64' and a missing
+device; RuntimeError for a traversal stack overflow.  ``targets_per_launch`` is accepted and ignored; ``stack_size``
+caps the traversal stack (its maximum here is 128 entries per warp, enough for trees of depth 127).
+"""
+import time
+
+import numpy as np
+
+from . import vortex_cuda as VC
+
+STACK = 512
+TARGETS_PER_LAUNCH = 65536
+PRECISIONS = ("fp64", "mixed", "fp32")
+SUPPORTED_MODELS = (0, 1, 2)  # NONE, RANKINE, LAMB_OSEEN (vortex_tree.py:46)
+DEVICE_STACK = 128
+
+
+class Statistics:
+    last = {}
+    last_far_counts = None
+    totals = dict(calls=0, suspect=0, launches=0)
+
+    @classmethod
+    def reset_totals(cls):
+        cls.totals = dict(calls=0, suspect=0, launches=0)
+
+
+def cuda_tree_sum(points, starts, directions, lengths, gamma, radius, model, csr, singularity, tree, settings, *,
+                  targets_per_launch=None, stack_size=STACK, block=None):
+    """Return (velocity, any_flag) like ``vortex_tree.tree_sum`` for the same inputs, evaluated on the GPU."""
+    if not VC.available():
+        raise ValueError(f"the cuda tree evaluation needs a CUDA device ({VC.probe_error()})")
+    if int(model) not in SUPPORTED_MODELS and np.any(np.asarray(radius) > 0):
+        raise ValueError("tree backend supports core models NONE, RANKINE and LAMB_OSEEN only")
+    if tree.theta >= 1.0:
+        raise ValueError("tree theta must be below one")
+    precision = settings.precision
+    gpu64 = getattr(settings, "suspect", "cpu") == "gpu64"
+    if gpu64 and precision == "fp64":
+        raise ValueError("suspect='gpu64' is for the single precisions only")
+    block = int(settings.block if block is None else block)
+    _, _, near = VC._check_settings(settings)
+    kind = getattr(settings, "tree", "median")
+    points = np.ascontiguousarray(points, dtype=np.float64)
+    n, m = len(points), len(starts)
+    if n == 0 or m == 0:
+        Statistics.last = dict(points=n, segments=m, launches=0, suspect=0)
+        if gpu64:
+            Statistics.last.update(suspect_mode="gpu64", suspect_targets=0, suspect_pairs=0)
+        return np.zeros((n, 3)), False
+    import torch
+    from . import _lib, engine
+    device = torch.cuda.current_device()
+    tick = time.perf_counter()
+    sources = engine.Sources(starts, directions, lengths, gamma, radius, device)
+    targets = engine.Targets(points, csr, device)
+    torch.cuda.current_stream(device).synchronize()
+    upload_s = time.perf_counter() - tick
+    tick = time.perf_counter()
+    built = engine.build_tree(sources, tree.theta, tree.order, tree.leaf_size, tree.core_clearance, kind)
+    build_s = time.perf_counter() - tick
+    build_stats = engine.last_stats(device)
+    limit = int(stack_size) if 0 < int(stack_size) < DEVICE_STACK else 0
+    tick = time.perf_counter()
+    try:
+        d_out, d_flags, d_far = engine.tree_eval(built, targets, int(model), singularity, precision, block, near,
+                                                 tree.theta, tree.order, tree.core_clearance, stack_limit=limit)
+    except _lib.StackOverflow as error:
+        raise RuntimeError(f"tree traversal stack overflow on the GPU (depth {min(int(stack_size), DEVICE_STACK)})") \
+            from error
+    evaluate_s = time.perf_counter() - tick
+    tick = time.perf_counter()
+    out = VC.to_host(d_out, (n, 3), np.float64)
+    flags = VC.to_host(d_flags, (n,), np.int8)
+    far = VC.to_host(d_far, (n,), np.int64)
+    download_s = time.perf_counter() - tick
+    stats = engine.last_stats(device)
+    Statistics.last = dict(points=n, segments=m, nodes=built.count, precision=precision, launches=1,
+                           targets_per_launch=n, longest_launch_s=stats["evaluate_ms"] * 1e-3, suspect=0,
+                           mean_far_nodes=float(far.mean()), build_s=build_s, moments_s=0.0, upload_s=upload_s,
+                           evaluate_s=evaluate_s, download_s=download_s, recompute_s=0.0, tree=kind,
+                           build_ms=build_stats["build_ms"], moments_ms=build_stats["moments_ms"],
+                           evaluate_ms=stats["evaluate_ms"], near_pairs=int(stats["near_pairs"]),
+                           far_evaluations=int(stats["far_evaluations"]), fp64_pairs=int(stats["fp64_pairs"]),
+                           visits=int(stats["visits"]),
+                           **({"moments": "gpu"} if getattr(settings, "moments", "cpu") == "gpu" else {}),
+                           **({"build": "gpu"} if getattr(settings, "build", "cpu") == "gpu" else {}))
+    if gpu64:
+        Statistics.last.update(suspect_mode="gpu64", suspect_targets=0, suspect_pairs=int(stats["fp64_pairs"]))
+    Statistics.last_far_counts = far
+    Statistics.totals["calls"] += 1
+    Statistics.totals["launches"] += 1
+    del built
+    return out, bool(np.any(flags))

@@ -1,0 +1,260 @@
+"""Generate the golden fixtures of tests/golden/ by running the reference's own code.
+
+Run in a container that holds the reference project (read-only) at REFERENCE (default /root/reference):
+
+    python tests/golden/make_golden.py [--reference /root/reference]
+
+It imports the reference's numba backends (src/openfawe/aero/vortex_numba.py, vortex_tree.py) with the numba cache
+redirected outside the reference tree, evaluates them on small seeded cases and writes compressed ``.npz`` files beside
+this script.  The GPU box does not have the reference; the tests only read these files.
+"""
+import argparse
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+
+def save(name, **arrays):
+    path = os.path.join(HERE, name)
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {name}: {os.path.getsize(path)} bytes")
+
+
+def random_network(seed, nodes=60, segments=90, points=70):
+    """Random directed network with near-axis, collinear-exterior and off-line targets (the kind of case that
+    tests/test_vortex_numba.py:38-54 of the reference uses)."""
+    rng = np.random.default_rng(seed)
+    xyz = rng.normal(size=(nodes, 3))
+    edges = rng.integers(0, nodes, size=(segments, 2))
+    edges = edges[edges[:, 0] != edges[:, 1]]
+    gamma = rng.normal(size=len(edges))
+    gamma[::7] = 0.0
+    radius = rng.uniform(0.01, 0.6, size=len(edges))
+    targets = rng.normal(size=(points, 3))
+    a, b = xyz[edges[:5, 0]], xyz[edges[:5, 1]]
+    normal = np.cross(b - a, [0.3, -0.2, 0.9])
+    normal /= np.linalg.norm(normal, axis=1)[:, None]
+    near = [a + 0.4 * (b - a) + 1e-9 * normal, a + 0.4 * (b - a) + 1e-13 * normal, a + 1.7 * (b - a),
+            a - 0.5 * (b - a), a + 0.5 * (b - a) + 0.05 * normal]
+    return xyz, edges, gamma, radius, np.vstack([targets, *near])
+
+
+def segment_arrays(nodes, edges):
+    """starts, directions, lengths exactly as segments_velocity forms them (vortex.py:460-465)."""
+    starts = nodes[edges[:, 0]]
+    delta = nodes[edges[:, 1]] - starts
+    lengths = np.hypot(np.hypot(delta[..., 0], delta[..., 1]), delta[..., 2])
+    return starts, delta / lengths[:, None], lengths
+
+
+def ring_lattice(seed=11, rows=24, span=17):
+    """A wavy ring lattice with shed circulation differences (the case family of tests/test_vortex_tree.py:25-40)."""
+    rng = np.random.default_rng(seed)
+    x = np.linspace(0.0, 12.0, rows)[:, None] * np.ones((1, span))
+    y = np.ones((rows, 1)) * np.linspace(-4.0, 4.0, span)[None, :]
+    z = 0.3 * np.sin(0.7 * x) * np.cos(0.5 * y) + 0.05 * rng.normal(size=x.shape)
+    nodes = np.column_stack((x.ravel(), y.ravel(), z.ravel()))
+    edges, gamma = [], []
+    strength = np.cos(np.linspace(-1.3, 1.3, span - 1))[None, :] * np.exp(-0.05 * np.arange(rows - 1))[:, None]
+    for i in range(rows - 1):
+        for j in range(span - 1):
+            a, b, c, d = i * span + j, i * span + j + 1, (i + 1) * span + j + 1, (i + 1) * span + j
+            for p, q in ((a, b), (b, c), (c, d), (d, a)):
+                edges.append((p, q))
+                gamma.append(strength[i, j])
+    return nodes, np.asarray(edges, dtype=np.int64), np.asarray(gamma)
+
+
+def main():
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--reference", default="/root/reference")
+    args = parser.parse_args()
+    os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(tempfile.gettempdir(), "numba_reference_cache"))
+    sys.path.insert(0, os.path.join(args.reference, "src"))
+    sys.path.insert(0, REPO)
+    from openfawe.aero import vortex_numba as vn, vortex_tree as vt
+    from openfawe_b200 import wakes
+
+    # 1. welib per-core velocities (tests/fixtures/upstream-kernel-check.json of the reference), as arrays.
+    with open(os.path.join(args.reference, "tests/fixtures/upstream-kernel-check.json"), encoding="utf-8") as f:
+        data = json.load(f)
+    rows = data["direct_reference_results"]
+    save("upstream_kernel.npz", point=np.array([r["point"] for r in rows], dtype=np.float64),
+         model=np.array([r["core_model_id"] for r in rows], dtype=np.int64),
+         radius=np.array([r["core_radius_m"] for r in rows], dtype=np.float64),
+         velocity=np.array([r["velocity_m_per_s"] for r in rows], dtype=np.float64),
+         start=np.array(data["segment_start"], dtype=np.float64), end=np.array(data["segment_end"], dtype=np.float64))
+
+    # 2. numba direct_sum on random networks, every core model, scalar and per-segment cores.
+    out = {}
+    for seed in (3, 4):
+        nodes, edges, gamma, radius, points = random_network(seed)
+        starts, directions, lengths = segment_arrays(nodes, edges)
+        csr = vn.exclusion_csr(len(points), np.zeros((0, 2), dtype=np.int64))
+        out[f"s{seed}_points"], out[f"s{seed}_starts"] = points, starts
+        out[f"s{seed}_directions"], out[f"s{seed}_lengths"], out[f"s{seed}_gamma"] = directions, lengths, gamma
+        out[f"s{seed}_radius"] = radius
+        for model in range(6):
+            for ci, core in enumerate((0.0, 0.2, radius)):
+                r = np.broadcast_to(np.asarray(core, dtype=np.float64), (len(edges),)).copy()
+                for sing in ("zero", "raise"):
+                    u, flagged = vn.direct_sum(points, starts, directions, lengths, gamma, r, model, csr, sing)
+                    key = f"s{seed}_m{model}_c{ci}_{sing}"
+                    out[key] = u
+                    out[key + "_flag"] = np.array(flagged)
+    save("direct_random.npz", **out)
+
+    # 3. exclusions at the network's own nodes, incident segments + random extras + duplicates.
+    nodes, edges, gamma, radius, _ = random_network(5)
+    starts, directions, lengths = segment_arrays(nodes, edges)
+    incident = [(n, s) for s, (a, b) in enumerate(edges) for n in (a, b)]
+    rng = np.random.default_rng(9)
+    extra = [(int(p), int(s)) for p, s in zip(rng.integers(0, len(nodes), 30), rng.integers(0, len(edges), 30))]
+    pairs = np.asarray(incident + extra + incident[:5], dtype=np.int64)
+    ptr, seg = vn.exclusion_csr(len(nodes), pairs)
+    out = dict(points=nodes, starts=starts, directions=directions, lengths=lengths, gamma=gamma, radius=radius,
+               pairs=pairs, ptr=ptr, seg=seg)
+    for model in (0, 2, 5):
+        u, flagged = vn.direct_sum(nodes, starts, directions, lengths, gamma, radius, model, (ptr, seg), "raise")
+        out[f"m{model}"], out[f"m{model}_flag"] = u, np.array(flagged)
+    save("direct_exclusions.npz", **out)
+
+    # 4. flag cases: on-segment point (both circulations), float-range overflow, subnormal cores.
+    out = {}
+    seg_nodes = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0]])
+    st, di, le = segment_arrays(seg_nodes, np.array([[0, 1]]))
+    cases = [("singular_g1", np.array([[0.3, 0.0, 0.0]]), st, di, le, 1.0, 0, 0.0),
+             ("singular_g0", np.array([[0.3, 0.0, 0.0]]), st, di, le, 0.0, 0, 0.0)]
+    tiny_nodes = np.array([[0.0, 0.0, 0.0], [1e-160, 0.0, 0.0]])
+    ts, td, tl = segment_arrays(tiny_nodes, np.array([[0, 1]]))
+    cases.append(("overflow", np.array([[0.0, 1e160, 0.0]]), ts, td, tl, 1.0, 0, 0.0))
+    for model in (1, 2, 3):
+        cases.append((f"subnormal_core_m{model}", np.array([[0.5, 1.0, 0.0]]), st, di, le, 1.0, model, 1e-310))
+    for name, p, s, d, length, g, model, core in cases:
+        for sing in ("raise", "zero"):
+            u, flags = None, None
+            u = np.zeros((1, 3))
+            flags = np.zeros(1, dtype=np.int8)
+            vn.sum_segments_serial(p, s, d, length, np.array([g]), np.array([core]), model, sing == "raise",
+                                   np.zeros(2, dtype=np.int64), np.zeros(1, dtype=np.int64), u, flags)
+            out[f"{name}_{sing}_u"], out[f"{name}_{sing}_flags"] = u, flags
+            out[f"{name}_points"], out[f"{name}_starts"], out[f"{name}_directions"] = p, s, d
+            out[f"{name}_lengths"], out[f"{name}_gamma"] = length, np.array([g])
+            out[f"{name}_radius"], out[f"{name}_model"] = np.array([core]), np.array(model)
+    save("direct_flags.npz", **out)
+
+    # 5. config-1 lattice (16 x 128, Rosenhead-Moore) direct sum.
+    case = wakes.lattice()
+    csr = vn.exclusion_csr(len(case["points"]), np.zeros((0, 2), dtype=np.int64))
+    u, flagged = vn.direct_sum(*wakes.backend_args(case), csr, "raise")
+    save("direct_lattice.npz", u=u, flag=np.array(flagged), points_sum=np.array(case["points"].sum()),
+         starts_sum=np.array(case["starts"].sum()), gamma_sum=np.array(case["gamma"].sum()))
+
+    # 6. tree sums on the ring lattice: theta x order sweep, plus the tree and node quantities of one setting.
+    nodes, edges, gamma = ring_lattice()
+    rng = np.random.default_rng(2)
+    points = nodes + 0.07 * rng.normal(size=nodes.shape)
+    starts, directions, lengths = segment_arrays(nodes, edges)
+    radius = np.full(len(edges), 0.1)
+    csr = vn.exclusion_csr(len(points), np.zeros((0, 2), dtype=np.int64))
+    out = dict(points=points, starts=starts, directions=directions, lengths=lengths, gamma=gamma, radius=radius)
+    out["direct"], _ = vn.direct_sum(points, starts, directions, lengths, gamma, radius, 2, csr, "raise")
+    for order in (0, 1, 2):
+        for theta in (0.6, 0.4, 0.25, 0.15):
+            settings = type("S", (), dict(theta=theta, order=order, leaf_size=8, core_clearance=3.0))()
+            u, flagged = vt.tree_sum(points, starts, directions, lengths, gamma, radius, 2, csr, "raise", settings)
+            out[f"o{order}_t{int(theta * 100)}"] = u
+            out[f"o{order}_t{int(theta * 100)}_far"] = np.array(vt.TreeStatistics.last["mean_far_nodes"])
+    lv = directions * lengths[:, None]
+    ends = starts + lv
+    alpha = gamma[:, None] * lv
+    mid = 0.5 * (starts + ends)
+    order_, lo, hi, left, right, count = vt.build_tree(mid, 8)
+    centre, bound, core, m0, m1, m2 = vt.node_moments(order_, lo, hi, starts, ends, alpha, lv, radius, gamma)
+    w1, t2, w2 = vt.node_contractions(m1, m2)
+    out.update(order=order_, lo=lo, hi=hi, left=left, right=right, centre=centre, bound=bound, core=core, m0=m0, m1=m1,
+               m2=m2, w1=w1, t2=t2, w2=w2)
+    save("tree_lattice.npz", **out)
+
+    # 7. the self-test sheet (40 rows) through tree_sum at theta 0.2 and 0.5 with exclusions, and the direct sum.
+    case = wakes.selftest_sheet(40, seed=40)
+    p = case["points"]
+    rng = np.random.default_rng(40)
+    ex = np.column_stack((rng.integers(0, len(p), 300), rng.integers(0, len(case["starts"]), 300))).astype(np.int64)
+    ex = np.vstack([ex, [[0, 0], [0, 1], [5, 200]]])
+    csr = vn.exclusion_csr(len(p), ex)
+    out = dict(points=p, starts=case["starts"], directions=case["directions"], lengths=case["lengths"],
+               gamma=case["gamma"], radius=case["radius"], pairs=ex, ptr=csr[0], seg=csr[1])
+    args_ = wakes.backend_args(case)
+    out["direct"], _ = vn.direct_sum(*args_, csr, "raise")
+    for theta in (0.2, 0.5):
+        settings = type("S", (), dict(theta=theta, order=2, leaf_size=32, core_clearance=3.0))()
+        u, flagged = vt.tree_sum(*args_, csr, "raise", settings)
+        out[f"t{int(theta * 100)}"] = u
+        out[f"t{int(theta * 100)}_flag"] = np.array(flagged)
+    save("tree_selftest.npz", **out)
+
+    # 8. build_tree arrays on the midpoint cases of the reference's GPU-build test (tests/test_cuda_build.py:20-28).
+    rng = np.random.default_rng(11)
+    grid = np.array([[i * 0.5, j * 0.25, 0.0] for i in range(30) for j in range(20)])
+    mids = [("random", rng.random((600, 3)) * [20.0, 5.0, 2.0], 8), ("grid", grid, 32), ("grid_leaf1", grid[:200], 1),
+            ("coincident", np.ones((40, 3)), 4), ("fewer", rng.random((5, 3)), 32),
+            ("long", rng.random((2100, 3)) * [30.0, 3.0, 1.0], 16)]
+    out = {}
+    for name, mid_, leaf in mids:
+        order_, lo, hi, left, right, count = vt.build_tree(mid_, leaf)
+        out.update({f"{name}_mid": mid_, f"{name}_leaf": np.array(leaf), f"{name}_order": order_, f"{name}_lo": lo,
+                    f"{name}_hi": hi, f"{name}_left": left, f"{name}_right": right})
+    save("tree_build.npz", **out)
+
+    # 9. far-field forms on random symmetric moments (tests/test_vortex_tree.py:170-187 of the reference).
+    rng = np.random.default_rng(5)
+    count = 7
+    m0 = rng.normal(size=(count, 3))
+    m1 = rng.normal(size=(count, 3, 3))
+    m2 = rng.normal(size=(count, 3, 3, 3))
+    m2 = 0.5 * (m2 + m2.transpose(0, 1, 3, 2))
+    w1, t2, w2 = vt.node_contractions(m1, m2)
+    r = rng.normal(size=(count, 3, 3)) * 3.0
+    far = np.zeros((count, 3, 3))
+    explicit = np.zeros((count, 3, 3))
+    for node in range(count):
+        for order in range(3):
+            far[node, order] = vt.far_velocity(*r[node, order], node, m0, m1, m2, w1, t2, w2, order)
+            vt.multipole_velocity_explicit(*r[node, order], node, m0, m1, m2, order, explicit[node, order])
+    save("far_field.npz", m0=m0, m1=m1, m2=m2, w1=w1, t2=t2, w2=w2, r=r, far=far, explicit=explicit)
+
+    # 10. node moments of random segments (tests/test_cuda_moments.py:22-46 of the reference) for leaves 8, 32, 1.
+    out = {}
+    for seed, leaf, count in ((1, 8, 300), (2, 32, 300), (3, 1, 120)):
+        rng = np.random.default_rng(seed)
+        starts = rng.random((count, 3)) * [20.0, 5.0, 2.0]
+        d = rng.normal(size=(count, 3))
+        directions = d / np.linalg.norm(d, axis=1)[:, None]
+        lengths = 0.2 + 0.3 * rng.random(count)
+        gamma = rng.normal(size=count)
+        gamma[::7] = 0.0
+        radius = rng.uniform(0.0, 0.08, count)
+        lv = directions * lengths[:, None]
+        ends = starts + lv
+        alpha = gamma[:, None] * lv
+        order_, lo, hi, left, right, _ = vt.build_tree(0.5 * (starts + ends), leaf)
+        q = vt.node_moments(order_, lo, hi, starts, ends, alpha, lv, radius, gamma)
+        c = vt.node_contractions(q[4], q[5])
+        pre = f"s{seed}_"
+        out.update({pre + "starts": starts, pre + "directions": directions, pre + "lengths": lengths,
+                    pre + "gamma": gamma, pre + "radius": radius, pre + "leaf": np.array(leaf), pre + "order": order_,
+                    pre + "lo": lo, pre + "hi": hi, pre + "left": left, pre + "right": right})
+        for name, value in zip(("centre", "bound", "core", "m0", "m1", "m2", "w1", "t2", "w2"), (*q, *c)):
+            out[pre + name] = value
+    save("moments.npz", **out)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,110 @@
+"""The drop-in boundary without a GPU: the C-ABI library loads and exports every declared entry point, the Python
+mirrors of the reference's settings validate like the reference's, and the modules register under the reference's
+names.  No compute call is made here."""
+import ctypes
+import os
+import re
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import REPO
+
+HEADER = os.path.join(REPO, "include", "bs_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER, encoding="utf-8").read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(bs_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from openfawe_b200 import build
+    path = build.build()
+    lib = ctypes.CDLL(path)
+    names = declared_functions()
+    assert "bs_direct" in names and "bs_tree_eval" in names and len(names) >= 12
+    for name in names:
+        assert hasattr(lib, name), name
+    from openfawe_b200 import _lib
+    assert set(_lib.SIGNATURES) <= set(names)
+    major, minor, arch = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    assert lib.bs_version(ctypes.byref(major), ctypes.byref(minor), ctypes.byref(arch)) == 0
+    assert arch.value == 100
+
+
+def test_struct_layouts_match_header():
+    from openfawe_b200 import _lib
+    assert ctypes.sizeof(_lib.Sources) == 48
+    assert ctypes.sizeof(_lib.Targets) == 40
+    assert ctypes.sizeof(_lib.KernelParams) == 24
+    assert ctypes.sizeof(_lib.TreeParams) == 40
+    assert _lib.TreeParams.stack_limit.offset == 36
+
+
+def test_settings_mirror_reference_validation():
+    from openfawe_b200.settings import CudaSettings, TreeSettings
+    for bad in (dict(theta=1.0), dict(theta=0.0), dict(order=3), dict(leaf_size=0), dict(core_clearance=-1.0),
+                dict(theta=True)):
+        with pytest.raises(ValueError):
+            TreeSettings(**bad)
+    for bad in (dict(precision="fp16"), dict(block=48), dict(block=True), dict(suspect="gpu"),
+                dict(precision="fp64", suspect="gpu64"), dict(moments="device"), dict(build="device"),
+                dict(tree="octree"), dict(near=-1.0)):
+        with pytest.raises(ValueError):
+            CudaSettings(**bad)
+    assert CudaSettings().precision == "mixed" and CudaSettings().tree == "median"
+
+
+def test_install_registers_reference_module_names():
+    import openfawe_b200
+    vc, vct = openfawe_b200.install("fakepkg.aero")
+    try:
+        assert sys.modules["fakepkg.aero.vortex_cuda"] is vc
+        assert sys.modules["fakepkg.aero.vortex_cuda_tree"] is vct
+        for name in ("cuda_sum", "available", "probe_error", "Statistics"):
+            assert hasattr(vc, name)
+        assert hasattr(vct, "cuda_tree_sum") and hasattr(vct, "Statistics")
+    finally:
+        openfawe_b200.uninstall("fakepkg.aero")
+    assert "fakepkg.aero.vortex_cuda" not in sys.modules
+
+
+def test_no_device_means_value_error_not_fallback(monkeypatch):
+    """Without a usable device the backends refuse, like the reference's (vortex_cuda.py:384-385)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    from openfawe_b200 import vortex_cuda, vortex_cuda_tree
+    from openfawe_b200.settings import CudaSettings, TreeSettings
+    monkeypatch.setattr(vortex_cuda, "_AVAILABLE", [])
+    monkeypatch.setattr(vortex_cuda, "_PROBE_ERROR", [])
+    args = (np.zeros((1, 3)), np.zeros((1, 3)), np.array([[1.0, 0, 0]]), np.ones(1), np.ones(1), np.zeros(1), 0,
+            (np.zeros(2, dtype=np.int64), np.zeros(0, dtype=np.int64)), "raise")
+    with pytest.raises(ValueError, match="needs a CUDA device"):
+        vortex_cuda.cuda_sum(*args, CudaSettings("fp64"))
+    with pytest.raises(ValueError, match="needs a CUDA device"):
+        vortex_cuda_tree.cuda_tree_sum(*args, TreeSettings(), CudaSettings("fp64"))
+    assert vortex_cuda.probe_error()
+
+
+def test_product_never_imports_the_oracle():
+    """The oracle is the checker only: no module of the package imports it."""
+    pkg = os.path.join(REPO, "openfawe_b200")
+    for root, _, files in os.walk(pkg):
+        for f in files:
+            if f.endswith(".py"):
+                text = open(os.path.join(root, f), encoding="utf-8").read()
+                assert "import oracle" not in text and "from oracle" not in text, f
+
+
+def test_wake_generators_shapes():
+    from openfawe_b200 import wakes
+    c1 = wakes.lattice()
+    assert len(c1["starts"]) == 4207 and len(c1["points"]) == 1024 and c1["model"] == 5
+    c2 = wakes.rotor_sheet(468)
+    assert len(c2["starts"]) == 219 * 468 - 46 and len(c2["points"]) == 20570 and c2["model"] == 2
+    s = wakes.selftest_sheet(468, seed=468)
+    assert len(s["starts"]) == 102382 and len(s["points"]) == 20570

@@ -1,0 +1,241 @@
+"""GPU tree code (libbs_b200 build + moments + traversal) against the reference's tree code and the oracle.
+
+* Median tree: the arrays of vortex_tree.build_tree element for element; node centres, cores and bounding radii bit
+  for bit, moments within 1e-12 node-relative (the reference's GPU-moment bound, tests/test_cuda_moments.py:90-105).
+* FP64 evaluation: the accepted nodes equal the CPU's (far counts identical per target) and velocities within
+  1e-12 * max|u| of the reference's tree_sum (its GPU self-test allows 1e-10, selftest.py:413).
+* Mixed: max and rms error against the CPU tree within 0.1 x the CPU tree's own error against the direct sum (the
+  self-test's mixed bound, selftest.py:415-417).
+* Morton tree: keys, sort permutation and tree arrays bit-exact against the CPU recomputation (oracle/morton_oracle.c).
+"""
+import numpy as np
+import pytest
+
+from conftest import golden, no_exclusions
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def cuda_settings(precision="fp64", tree="median", block=128, suspect="cpu"):
+    from openfawe_b200.settings import CudaSettings
+    return CudaSettings(precision, block, suspect, tree=tree)
+
+
+def tree_settings(theta=0.5, order=2, leaf=32):
+    from openfawe_b200.settings import TreeSettings
+    return TreeSettings(theta, order, leaf)
+
+
+def node_relative(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    scale = np.abs(a).reshape(len(a), -1).max(axis=1)
+    diff = np.abs(a - b).reshape(len(a), -1).max(axis=1)
+    return np.where(scale > 0, diff / np.where(scale > 0, scale, 1.0), diff)
+
+
+def grid_segments(nx=30, ny=20, length=0.125):
+    """Axis-aligned segments on a grid: exactly representable midpoints with many equal coordinates (ties)."""
+    starts = np.array([[i * 0.5, j * 0.25, 0.0] for i in range(nx) for j in range(ny)])
+    directions = np.tile([1.0, 0.0, 0.0], (len(starts), 1))
+    lengths = np.full(len(starts), length)
+    return starts, directions, lengths
+
+
+def random_segments(seed, count):
+    rng = np.random.default_rng(seed)
+    starts = rng.random((count, 3)) * [20.0, 5.0, 2.0]
+    d = rng.normal(size=(count, 3))
+    directions = d / np.linalg.norm(d, axis=1)[:, None]
+    lengths = 0.2 + 0.3 * rng.random(count)
+    gamma = rng.normal(size=count)
+    gamma[::7] = 0.0
+    radius = rng.uniform(0.0, 0.08, count)
+    return starts, directions, lengths, gamma, radius
+
+
+def test_median_build_element_for_element(device):
+    from openfawe_b200 import engine
+    cases = [("random", *random_segments(11, 600)[:3], 8), ("grid", *grid_segments(), 32),
+             ("grid-leaf-1", *[a[:200] for a in grid_segments()], 1),
+             ("coincident", np.ones((40, 3)), np.tile([0.0, 1.0, 0.0], (40, 1)), np.full(40, 0.5), 4),
+             ("fewer-than-a-leaf", *[a[:5] for a in random_segments(3, 5)[:3]], 32),
+             ("longer-than-a-chunk", *random_segments(4, 5000)[:3], 16)]
+    for name, starts, directions, lengths, leaf in cases:
+        m = len(starts)
+        src = engine.Sources(starts, directions, lengths, np.ones(m), np.zeros(m), device)
+        tree = engine.build_tree(src, leaf_size=leaf, kind="median")
+        got = tree.export()
+        _, _, _, mid = O.segment_geometry(starts, directions, lengths, np.ones(m))
+        ref = O.build_tree(mid, leaf)
+        for key, value in zip(("order", "lo", "hi", "left", "right"), ref[:5]):
+            assert np.array_equal(got[key], value), (name, key)
+        assert tree.count == ref[5]
+
+
+def test_moments_against_reference(device):
+    from openfawe_b200 import engine
+    g = golden("moments.npz")
+    for seed in (1, 2, 3):
+        p = lambda k: g[f"s{seed}_{k}"]  # noqa: E731
+        src = engine.Sources(p("starts"), p("directions"), p("lengths"), p("gamma"), p("radius"), device)
+        for tree in (engine.build_tree(src, leaf_size=int(p("leaf")), kind="median"),
+                     engine.tree_from_arrays(src, p("order"), p("lo"), p("hi"), p("left"), p("right"))):
+            got = tree.export()
+            for key in ("order", "lo", "hi", "left", "right", "centre", "core", "bound"):
+                assert np.array_equal(got[key], p(key)), (seed, key)
+            for key in ("m0", "m1", "m2"):
+                assert node_relative(p(key), got[key]).max() <= 1e-12, (seed, key)
+            for key, made_of in (("w1", "m1"), ("t2", "m2"), ("w2", "m2")):
+                scale = np.abs(p(made_of)).reshape(len(p(made_of)), -1).max(axis=1)
+                diff = np.abs(p(key) - got[key]).reshape(len(got[key]), -1).max(axis=1)
+                assert np.all(diff <= 1e-12 * scale), (seed, key)
+            again = tree.export()
+            assert all(np.array_equal(got[k], again[k]) for k in got)
+
+
+def test_fp64_theta_order_sweep_matches_reference_tree(device):
+    from openfawe_b200 import engine
+    g = golden("tree_lattice.npz")
+    args = (g["points"], g["starts"], g["directions"], g["lengths"], g["gamma"], g["radius"], 2)
+    src = engine.Sources(*args[1:6], device)
+    tgt = engine.Targets(g["points"], None, device)
+    tree = engine.build_tree(src, leaf_size=8, kind="median")
+    for order in (0, 1, 2):
+        for theta in (0.6, 0.4, 0.25, 0.15):
+            key = f"o{order}_t{int(theta * 100)}"
+            u, flags, far = engine.tree_eval(tree, tgt, 2, "raise", "fp64", theta=theta, order=order)
+            u, far = u.cpu().numpy(), far.cpu().numpy()
+            _, _, d = O.tree_sum(*args, no_exclusions(len(g["points"])), "raise", theta=theta, order=order,
+                                 leaf_size=8, details=True)
+            assert np.array_equal(far, d["far"]), key
+            assert far.mean() == float(g[key + "_far"])
+            scale = np.max(np.linalg.norm(g[key], axis=1))
+            assert np.max(np.linalg.norm(u - g[key], axis=1)) <= 1e-12 * scale, key
+            assert not flags.cpu().numpy().any()
+
+
+def test_selftest_sheet_fp64_and_mixed_bounds(device):
+    from openfawe_b200.vortex_cuda_tree import cuda_tree_sum, Statistics
+    g = golden("tree_selftest.npz")
+    args = (g["points"], g["starts"], g["directions"], g["lengths"], g["gamma"], g["radius"], 2,
+            (g["ptr"], g["seg"]), "raise")
+    norm = lambda v: np.linalg.norm(v, axis=1)  # noqa: E731
+    for theta in (0.2, 0.5):
+        cpu = g[f"t{int(theta * 100)}"]
+        scale = norm(cpu).max()
+        tree_error = norm(cpu - g["direct"])
+        u, flag = cuda_tree_sum(*args, tree_settings(theta), cuda_settings("fp64"))
+        assert flag == bool(g[f"t{int(theta * 100)}_flag"])
+        assert norm(u - cpu).max() <= 1e-12 * scale
+        assert Statistics.last["nodes"] > 0 and Statistics.last_far_counts.shape == (len(g["points"]),)
+        for precision in ("mixed", "fp32"):
+            u, flag = cuda_tree_sum(*args, tree_settings(theta), cuda_settings(precision, suspect="gpu64"))
+            error = norm(u - cpu)
+            assert error.max() <= 0.1 * tree_error.max(), (theta, precision)
+            assert np.sqrt(np.mean(error ** 2)) <= 0.1 * np.sqrt(np.mean(tree_error ** 2)), (theta, precision)
+
+
+def test_morton_keys_order_and_tree_bit_exact(device):
+    from openfawe_b200 import engine, wakes
+    for case in (wakes.selftest_sheet(30, seed=30), wakes.rotor_sheet(40, seed=7, targets=500)):
+        m = len(case["starts"])
+        src = engine.Sources(case["starts"], case["directions"], case["lengths"], case["gamma"], case["radius"],
+                             device)
+        for leaf in (1, 8, 32):
+            tree = engine.build_tree(src, leaf_size=leaf, kind="morton")
+            keys, order = tree.keys()
+            ref = O.morton_tree(case["starts"], case["directions"], case["lengths"], leaf)
+            assert np.array_equal(keys, ref["keys"])
+            assert np.array_equal(order, ref["order"])
+            got = tree.export()
+            for key in ("order", "lo", "hi", "left", "right"):
+                assert np.array_equal(got[key], ref[key]), (leaf, key)
+            assert m == len(got["order"])
+
+
+def test_morton_tree_evaluation_matches_oracle_on_same_tree(device):
+    from openfawe_b200 import engine, wakes
+    case = wakes.rotor_sheet(60, seed=5, targets=3000)
+    args = wakes.backend_args(case)
+    src = engine.Sources(*args[1:6], device)
+    tgt = engine.Targets(case["points"], None, device)
+    tree = engine.build_tree(src, leaf_size=16, kind="morton")
+    ex = tree.export()
+    _, ends, _, _ = O.segment_geometry(*args[1:5])
+    quantities = tuple(ex[k] for k in ("centre", "bound", "core", "m0", "m1", "m2", "w1", "t2", "w2"))
+    tree_arrays = tuple(ex[k] for k in ("order", "lo", "hi", "left", "right"))
+    n = len(case["points"])
+    for theta in (0.3, 0.1):
+        ref, flags, far, _ = O.tree_velocity(*args[:7], "raise", tree_arrays, quantities, theta, 2, 3.0,
+                                             no_exclusions(n)[0], np.zeros(0, dtype=np.int64))
+        u, gflags, gfar = engine.tree_eval(tree, tgt, 2, "raise", "fp64", theta=theta)
+        assert np.array_equal(gfar.cpu().numpy(), far)
+        scale = np.linalg.norm(ref, axis=1).max()
+        assert np.max(np.linalg.norm(u.cpu().numpy() - ref, axis=1)) <= 1e-12 * scale
+
+
+def test_excluded_segment_never_leaks_through_a_far_node(device):
+    from openfawe_b200.vortex_cuda_tree import cuda_tree_sum
+    g = golden("tree_lattice.npz")
+    starts, directions, lengths, gamma = g["starts"], g["directions"], g["lengths"], g["gamma"]
+    radius = np.zeros(len(gamma))
+    points = starts[:1] + 0.0
+    loud, silent = gamma.copy(), gamma.copy()
+    loud[-1], silent[-1] = 1e6, 0.0
+    ex = O.exclusion_csr(1, np.array([[0, len(gamma) - 1]]))
+    for kind in ("median", "morton"):
+        for precision in ("fp64", "mixed"):
+            s = cuda_settings(precision, kind)
+            t = tree_settings(0.6, 2, 4)
+            a, _ = cuda_tree_sum(points, starts, directions, lengths, loud, radius, 0, ex, "zero", t, s)
+            b, _ = cuda_tree_sum(points, starts, directions, lengths, silent, radius, 0, ex, "zero", t, s)
+            assert np.array_equal(a, b), (kind, precision)
+            c, _ = cuda_tree_sum(points, starts, directions, lengths, loud, radius, 0, no_exclusions(1), "zero", t, s)
+            assert np.linalg.norm(c - b) > 1e3 * np.linalg.norm(b)
+
+
+def test_errors_like_the_reference(device):
+    from openfawe_b200.vortex_cuda_tree import cuda_tree_sum
+    g = golden("tree_lattice.npz")
+    args = (g["points"], g["starts"], g["directions"], g["lengths"], g["gamma"], g["radius"])
+    csr = no_exclusions(len(g["points"]))
+    for model in (3, 4, 5):
+        with pytest.raises(ValueError):
+            cuda_tree_sum(*args, model, csr, "raise", tree_settings(), cuda_settings())
+    fp64_gpu64 = type("S", (), dict(precision="fp64", block=128, suspect="gpu64"))()  # refused by CudaSettings too
+    with pytest.raises(ValueError, match="single precisions"):
+        cuda_tree_sum(*args, 2, csr, "raise", tree_settings(), fp64_gpu64)
+    with pytest.raises(RuntimeError, match="stack overflow"):
+        cuda_tree_sum(*args, 2, csr, "raise", tree_settings(0.05, 2, 1), cuda_settings(), stack_size=4)
+    u, _ = cuda_tree_sum(*args, 2, csr, "raise", tree_settings(0.05, 2, 1), cuda_settings())
+    assert np.all(np.isfinite(u))
+
+
+def test_singular_target_flags(device):
+    from openfawe_b200.vortex_cuda_tree import cuda_tree_sum
+    g = golden("tree_lattice.npz")
+    starts, directions, lengths = g["starts"], g["directions"], g["lengths"]
+    point = (starts[3] + 0.5 * lengths[3] * directions[3])[None]
+    args = (point, starts, directions, lengths, g["gamma"], np.zeros(len(lengths)), 0, no_exclusions(1))
+    for kind in ("median", "morton"):
+        for precision in ("fp64", "mixed"):
+            _, flag = cuda_tree_sum(*args, "raise", tree_settings(0.4, 2, 2), cuda_settings(precision, kind))
+            assert flag
+            _, flag = cuda_tree_sum(*args, "zero", tree_settings(0.4, 2, 2), cuda_settings(precision, kind))
+            assert not flag
+
+
+def test_rotor_sheet_mixed_tree_against_fp64_direct(device):
+    from openfawe_b200 import engine, wakes
+    case = wakes.rotor_sheet(120, seed=11, targets=4000)
+    args = wakes.backend_args(case)
+    src = engine.Sources(*args[1:6], device)
+    tgt = engine.Targets(case["points"], None, device)
+    direct, _ = engine.direct(src, tgt, 2, "raise", "fp64")
+    direct = direct.cpu().numpy()
+    for kind in ("median", "morton"):
+        tree = engine.build_tree(src, leaf_size=32, kind=kind)
+        u, flags, _ = engine.tree_eval(tree, tgt, 2, "raise", "mixed", theta=0.05)
+        rel = np.linalg.norm(u.cpu().numpy() - direct) / np.linalg.norm(direct)
+        assert rel < 1e-6, (kind, rel)
