@@ -80,7 +80,7 @@ typedef struct {
     int64_t points, segments, nodes, launches;
     int64_t far_evaluations, near_pairs, fp64_pairs, visits; /* counters of the last tree evaluation */
     double build_ms, moments_ms, evaluate_ms;                /* device time of the last build / evaluation */
-    int tree_depth;
+    int64_t pair_slots;  /* lane slots spent in leaf walks (32 per warp-pair); near_pairs / pair_slots = SIMT use */
 } bs_stats;
 
 /* Context: one per device.  bs_init makes `device` current, probes it with a one-thread kernel (the reference's

@@ -40,7 +40,7 @@ class Stats(ctypes.Structure):
     _fields_ = [("points", _i64), ("segments", _i64), ("nodes", _i64), ("launches", _i64),
                 ("far_evaluations", _i64), ("near_pairs", _i64), ("fp64_pairs", _i64), ("visits", _i64),
                 ("build_ms", ctypes.c_double), ("moments_ms", ctypes.c_double), ("evaluate_ms", ctypes.c_double),
-                ("tree_depth", ctypes.c_int)]
+                ("pair_slots", _i64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -68,7 +68,7 @@ SIGNATURES = {
                                    ctypes.POINTER(KernelParams), _p, _p, _p, _p]),
 }
 
-_LOCK = threading.Lock()
+_LOCK = threading.RLock()
 _LIB = []
 _CONTEXTS = {}
 

@@ -32,7 +32,7 @@ struct DirectArgs {
     unsigned long long *fp64_pairs;
 };
 
-template <int PREC>
+template <int PREC, int MODEL>
 __global__ void __launch_bounds__(256) direct_kernel(DirectArgs a) {
     using Rec = typename TileOf<PREC>::T;
     constexpr int TILE = TileOf<PREC>::N;
@@ -92,39 +92,57 @@ __global__ void __launch_bounds__(256) direct_kernel(DirectArgs a) {
         const int64_t base = c0 + (int64_t)t * TILE;
         const int cnt = (int)min((int64_t)TILE, c1 - base);
         if (valid && !failed) {
-            float t0 = 0.f, t1 = 0.f, t2 = 0.f;
-            for (int j = 0; j < cnt; ++j) {
-                const int64_t sidx = base + j;
-                if (sidx == next_ex) {
+            for (int sub = 0; sub < cnt; sub += 32) {
+                const int sc = min(32, cnt - sub);
+                const int64_t s0 = base + sub;
+                unsigned excl = 0;  // this target's excluded segments inside the sub-tile
+                while (next_ex < s0 + sc) {
+                    excl |= 1u << (int)(next_ex - s0);
                     ++k;
                     next_ex = k < stop ? a.ex_seg[k] : INT64_MAX;
-                    continue;
                 }
                 if (PREC == 0) {
-                    const Seg64 &r = reinterpret_cast<const Seg64 &>(tile[b][j]);
-                    int fl = pair64_at(x0, x1, x2, r, a.model, a.raise_singular, u0, u1, u2);
-                    if (fl != BS_FLAG_OK && flag == BS_FLAG_OK) flag = fl;
-                } else {
-                    const Seg32 &r = reinterpret_cast<const Seg32 &>(tile[b][j]);
-                    float q0 = (xh0 - r.hi.x) + (xl0 - r.lo.x);
-                    float q1 = (xh1 - r.hi.y) + (xl1 - r.lo.y);
-                    float q2 = (xh2 - r.hi.z) + (xl2 - r.lo.z);
-                    if (pair32(q0, q1, q2, r.hi, r.lo, r.dir, a.model, a.near2, t0, t1, t2)) {
-                        ++fp64_pairs;
-                        double v0 = 0.0, v1 = 0.0, v2 = 0.0;
-                        int fl = pair64_at(x0, x1, x2, a.seg64[sidx], a.model, a.raise_singular, v0, v1, v2);
-                        if (fl != BS_FLAG_OK) {
-                            if (flag == BS_FLAG_OK) flag = fl;
-                        } else if (PREC == 1) {
-                            u0 += v0; u1 += v1; u2 += v2;
-                        } else {
-                            f0 += (float)v0; f1 += (float)v1; f2 += (float)v2;
-                        }
+                    for (int j = 0; j < sc; ++j) {
+                        if ((excl >> j) & 1u) continue;
+                        const Seg64 &r = reinterpret_cast<const Seg64 &>(tile[b][sub + j]);
+                        int fl = pair64_at(x0, x1, x2, r, a.model, a.raise_singular, u0, u1, u2);
+                        if (fl != BS_FLAG_OK && flag == BS_FLAG_OK) flag = fl;
+                    }
+                    continue;
+                }
+                float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+                unsigned need = 0;
+#pragma unroll 4
+                for (int j = 0; j < sc; ++j) {
+                    const Seg32 &r = reinterpret_cast<const Seg32 &>(tile[b][sub + j]);
+                    const float q0 = (xh0 - r.hi.x) + (xl0 - r.lo.x);
+                    const float q1 = (xh1 - r.hi.y) + (xl1 - r.lo.y);
+                    const float q2 = (xh2 - r.hi.z) + (xl2 - r.lo.z);
+                    float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+                    const bool n64 = pair32<MODEL>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, v0, v1, v2);
+                    const bool skip = (excl >> j) & 1u;
+                    t0 += skip ? 0.f : v0;
+                    t1 += skip ? 0.f : v1;
+                    t2 += skip ? 0.f : v2;
+                    need |= (n64 && !skip ? 1u : 0u) << j;
+                }
+                fp64_pairs += __popc(need);
+                while (need) {
+                    const int j = __ffs(need) - 1;
+                    need &= need - 1;
+                    double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+                    int fl = pair64_at(x0, x1, x2, a.seg64[s0 + j], MODEL, a.raise_singular, v0, v1, v2);
+                    if (fl != BS_FLAG_OK) {
+                        if (flag == BS_FLAG_OK) flag = fl;
+                    } else if (PREC == 1) {
+                        u0 += v0; u1 += v1; u2 += v2;
+                    } else {
+                        f0 += (float)v0; f1 += (float)v1; f2 += (float)v2;
                     }
                 }
+                if (PREC == 1) { u0 += t0; u1 += t1; u2 += t2; }
+                else { f0 += t0; f1 += t1; f2 += t2; }
             }
-            if (PREC == 1) { u0 += t0; u1 += t1; u2 += t2; }
-            else if (PREC == 2) { f0 += t0; f1 += t1; f2 += t2; }
         }
         __syncthreads();  // every thread is done with tile[b]
         if (tid == 0 && t + 2 < ntiles && !failed) {
@@ -180,10 +198,29 @@ __global__ void direct_reduce_kernel(int64_t n, int chunks, const double *partia
 
 using namespace bs;
 
+template <int PREC>
+static void launch_model(int model, dim3 grid, int block, cudaStream_t s, const DirectArgs &args) {
+    switch (model) {
+        case 0: direct_kernel<PREC, 0><<<grid, block, 0, s>>>(args); break;
+        case 1: direct_kernel<PREC, 1><<<grid, block, 0, s>>>(args); break;
+        case 2: direct_kernel<PREC, 2><<<grid, block, 0, s>>>(args); break;
+        case 3: direct_kernel<PREC, 3><<<grid, block, 0, s>>>(args); break;
+        case 4: direct_kernel<PREC, 4><<<grid, block, 0, s>>>(args); break;
+        default: direct_kernel<PREC, 5><<<grid, block, 0, s>>>(args); break;
+    }
+}
+
+// FP64 evaluates the core model at run time; the single precisions are specialised per model.
+static void launch_direct(int precision, int model, dim3 grid, int block, cudaStream_t s, const DirectArgs &args) {
+    if (precision == BS_FP64) direct_kernel<0, 0><<<grid, block, 0, s>>>(args);
+    else if (precision == BS_MIXED) launch_model<1>(model, grid, block, s, args);
+    else launch_model<2>(model, grid, block, s, args);
+}
+
 // Chunks so that (target blocks) x (chunks) covers the SMs several times, each chunk a whole number of tiles.
 static int choose_chunks(int64_t n, int64_t m, int block, int tile, int sm_count) {
     int64_t target_blocks = (n + block - 1) / block;
-    int64_t want = (int64_t)sm_count * 4;
+    int64_t want = (int64_t)sm_count * 8;
     int64_t chunks = (want + target_blocks - 1) / target_blocks;
     int64_t max_chunks = std::max<int64_t>(1, (m + tile - 1) / tile);
     chunks = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(chunks, max_chunks), 4096));
@@ -260,9 +297,7 @@ extern "C" int bs_direct(bs_ctx *ctx, const bs_sources *src, const bs_targets *t
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s);
-    if (prec == BS_FP64) direct_kernel<0><<<grid, block, 0, s>>>(args);
-    else if (prec == BS_MIXED) direct_kernel<1><<<grid, block, 0, s>>>(args);
-    else direct_kernel<2><<<grid, block, 0, s>>>(args);
+    launch_direct(prec, kp->model, grid, block, s, args);
     cudaError_t le = cudaGetLastError();
     if (le == cudaSuccess && chunks > 1) {
         direct_reduce_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, chunks, partial, pflags, out, flags);

@@ -78,11 +78,12 @@ struct bs_ctx {
 // ---------------------------------------------------------------------------------------------------------------------
 namespace bs {
 
-// One segment, FP64 (80 bytes; 16-byte multiple for bulk copies).
+// One segment, FP64 (96 bytes; 16-byte multiple for bulk copies).
 struct __align__(16) Seg64 {
-    double sx, sy, sz, inv_len;  // start, 1/L
-    double dx, dy, dz, gfac;     // unit direction, (Gamma/L)/(4 pi)
-    double rcl, radius;          // rc/L, rc (rc > 0 && model != 0 enables the core)
+    double sx, sy, sz, len;       // start, L
+    double dx, dy, dz, gfac;      // unit direction, (Gamma/L)/(4 pi)
+    double rcl, radius, inv_len;  // rc/L, rc (rc > 0 && model != 0 enables the core), 1/L
+    double pad;
 };
 
 // One segment for the single-precision paths (48 bytes): start as a two-float (hi + lo) pair.
@@ -124,15 +125,12 @@ static constexpr double LAMB_CUT = 2.821180356260211;   // sqrt(10 / 1.25643), O
 static constexpr double LAMB_CUT2 = 7.959058602548491;  // 10 / 1.25643
 static constexpr double INV_FOUR_PI = 0.07957747154594767;  // 1 / (4 pi)
 
-// The reference pair (vortex_numba.pair_velocity) on an FP64 record; a = (p - s)/L given as the scaled offset.
-// Returns the flag; adds the velocity to (ux, uy, uz) only when the flag is ok.
-__device__ __forceinline__ int pair64(double ax, double ay, double az, const Seg64 &s, int model, int raise_singular,
-                                      double &ux, double &uy, double &uz) {
+// The reference pair (vortex_numba.pair_velocity) on an FP64 record from the scaled offset a = (p - s)/L, t = a.d and
+// c = d x a.  Returns the flag; adds the velocity to (ux, uy, uz) only when the flag is ok.
+__device__ __forceinline__ int pair64_core(double ax, double ay, double az, double t, double cx, double cy, double cz,
+                                           const Seg64 &s, int model, int raise_singular, double &ux, double &uy,
+                                           double &uz) {
     const double dx = s.dx, dy = s.dy, dz = s.dz;
-    double t = fma(az, dz, fma(ay, dy, ax * dx));
-    double cx = fma(dy, az, -dz * ay);
-    double cy = fma(dz, ax, -dx * az);
-    double cz = fma(dx, ay, -dy * ax);
     double h = norm3d(cx, cy, cz);
     double na = norm3d(ax, ay, az);
     double nb = norm3d(ax - dx, ay - dy, az - dz);
@@ -190,71 +188,99 @@ __device__ __forceinline__ int pair64(double ax, double ay, double az, const Seg
     return BS_FLAG_OK;
 }
 
-// Convenience: the FP64 pair from an FP64 target position.
+// The FP64 pair from an FP64 target position.  Fast form: a = (p - s) * (1/L) and fused t, c.  Where the target lies
+// within 1% (in angle) of the segment's line, c = d x a cancels and its rounding decides the result, so a, t and c are
+// formed again exactly as the reference forms them (IEEE division, separately rounded products and sums); the two
+// forms then agree to a few units in the last place of c.
 __device__ __forceinline__ int pair64_at(double px, double py, double pz, const Seg64 &s, int model,
                                          int raise_singular, double &ux, double &uy, double &uz) {
-    double ax = (px - s.sx) * s.inv_len, ay = (py - s.sy) * s.inv_len, az = (pz - s.sz) * s.inv_len;
-    return pair64(ax, ay, az, s, model, raise_singular, ux, uy, uz);
+    const double dx = s.dx, dy = s.dy, dz = s.dz;
+    const double rx = px - s.sx, ry = py - s.sy, rz = pz - s.sz;
+    double ax = rx * s.inv_len, ay = ry * s.inv_len, az = rz * s.inv_len;
+    double t = fma(az, dz, fma(ay, dy, ax * dx));
+    double cx = fma(dy, az, -dz * ay);
+    double cy = fma(dz, ax, -dx * az);
+    double cz = fma(dx, ay, -dy * ax);
+    const double h2 = fma(cx, cx, fma(cy, cy, cz * cz));
+    const double a2 = fma(ax, ax, fma(ay, ay, az * az));
+    if (!(h2 >= 1e-4 * a2)) {
+        const double L = s.len;
+        ax = __ddiv_rn(rx, L);
+        ay = __ddiv_rn(ry, L);
+        az = __ddiv_rn(rz, L);
+        t = __dadd_rn(__dadd_rn(__dmul_rn(ax, dx), __dmul_rn(ay, dy)), __dmul_rn(az, dz));
+        cx = __dsub_rn(__dmul_rn(dy, az), __dmul_rn(dz, ay));
+        cy = __dsub_rn(__dmul_rn(dz, ax), __dmul_rn(dx, az));
+        cz = __dsub_rn(__dmul_rn(dx, ay), __dmul_rn(dy, ax));
+    }
+    return pair64_core(ax, ay, az, t, cx, cy, cz, s, model, raise_singular, ux, uy, uz);
 }
 
-// Result of the single-precision pair: 0 = value added, 1 = needs the FP64 pair (near a segment within near_cores core
-// radii, near its axis within 1e-4 L (the reference's "suspect" rule, vortex_cuda.py:123-124), or any non-finite
-// intermediate, so that the FP64 pair decides flags exactly).
-__device__ __forceinline__ int pair32(float rx, float ry, float rz, const float4 &hi, const float4 &lo,
-                                      const float4 &dir, int model, float near2, float &ux, float &uy, float &uz) {
-    if (dir.w < 0.0f) return 1;  // core radius too small for FP32: FP64 decides (and flags, as the reference)
+// The single-precision pair, branch-free so that unrolled loops interleave independent pairs.  `rx, ry, rz` is
+// p - s (formed from two-float coordinates).  Adds the velocity to (ux, uy, uz) unless the pair needs FP64, which is
+// returned as true: within near_cores core radii of the segment (near2 = near_cores^2), within 1e-4 L of its axis (the
+// reference's "suspect" rule, vortex_cuda.py:123-124), a core too small for FP32 (rc/L marked -1), or out of FP32's
+// comfortable range -- the FP64 pair then decides value and flags exactly.  MODEL is the core model (0..5).
+template <int MODEL>
+__device__ __forceinline__ bool pair32(float rx, float ry, float rz, const float4 &hi, const float4 &lo,
+                                       const float4 &dir, float near2, float &ux, float &uy, float &uz) {
     const float il = hi.w;
-    float ax = rx * il, ay = ry * il, az = rz * il;
-    const float dx = dir.x, dy = dir.y, dz = dir.z;
-    float t = fmaf(az, dz, fmaf(ay, dy, ax * dx));
-    float cx = fmaf(dy, az, -dz * ay);
-    float cy = fmaf(dz, ax, -dx * az);
-    float cz = fmaf(dx, ay, -dy * ax);
-    float h2 = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
-    float na2 = fmaf(ax, ax, fmaf(ay, ay, az * az));
-    float bx = ax - dx, by = ay - dy, bz = az - dz;
-    float nb2 = fmaf(bx, bx, fmaf(by, by, bz * bz));
-    float big2 = fmaxf(1.0f, fmaxf(na2, nb2));
-    const float rc = dir.w;
-    // distance^2 to the finite segment, in units of L^2
-    float seg2 = t < 0.0f ? na2 : (t > 1.0f ? nb2 : h2);
-    bool cored = rc > 0.0f && model != 0;
-    if (!(h2 > 1e-8f * big2) || (cored && seg2 < near2 * rc * rc) || !(na2 < 1e18f) || !(nb2 < 1e18f)) return 1;
-    float rna = rsqrtf(na2), rnb = rsqrtf(nb2);
-    float na = na2 * rna, nb = nb2 * rnb;
+    const float ax = rx * il, ay = ry * il, az = rz * il;
+    const float dx = dir.x, dy = dir.y, dz = dir.z, rc = dir.w;
+    const float t = fmaf(az, dz, fmaf(ay, dy, ax * dx));
+    const float cx = fmaf(dy, az, -dz * ay);
+    const float cy = fmaf(dz, ax, -dx * az);
+    const float cz = fmaf(dx, ay, -dy * ax);
+    const float h2 = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
+    const float na2 = fmaf(ax, ax, fmaf(ay, ay, az * az));
+    const float bx = ax - dx, by = ay - dy, bz = az - dz;
+    const float nb2 = fmaf(bx, bx, fmaf(by, by, bz * bz));
+    const float big2 = fmaxf(1.0f, fmaxf(na2, nb2));
+    const float seg2 = t < 0.0f ? na2 : (t > 1.0f ? nb2 : h2);  // distance^2 to the finite segment (units of L^2)
+    const bool cored = MODEL != 0 && rc > 0.0f;
+    const bool need64 = !(h2 > 1e-8f * big2) || !(big2 < 1e18f) || rc < 0.0f || (cored && seg2 < near2 * rc * rc);
+    const float na = na2 * rsqrtf(na2), nb = nb2 * rsqrtf(nb2);
     float product = na * nb;
     float dot = fmaf(t, t - 1.0f, h2);
-    float plus = dot < 0.0f ? __fdividef(h2, product - dot) : product + dot;
-    float denominator = product * plus;
+    float sum = na + nb;
+    // coefficient = (Gamma/L)/(4 pi) * factor * (na + nb) / (product * plus) with plus = product + dot, or, when
+    // dot < 0, the rationalised h^2 / (product - dot); one reciprocal either way.
+    float num = dot < 0.0f ? sum * (product - dot) : sum;
+    float den = product * (dot < 0.0f ? h2 : product + dot);
     float factor = 1.0f;
-    if (cored) {
-        if (model == 5) {
-            float rc2 = rc * rc;
-            na = sqrtf(na2 + rc2);
-            nb = sqrtf(nb2 + rc2);
-            product = na * nb;
-            float tr2 = h2 + rc2;
-            dot = fmaf(t, t - 1.0f, tr2);
-            plus = dot < 0.0f ? __fdividef(tr2, product - dot) : product + dot;
-            denominator = product * plus;
-        } else if (model == 4) {
-            denominator = fmaf(rc, rc, denominator);
-        } else {
-            float r2 = __fdividef(h2, rc * rc);
-            if (model == 1) {
-                factor = fminf(r2, 1.0f);
-            } else if (model == 2) {
-                if (r2 <= (float)LAMB_CUT2) factor = -expm1f(-(float)LAMB_A * r2);
-            } else if (model == 3) {
-                factor = r2 < 1.0f ? r2 * rsqrtf(fmaf(r2, r2, 1.0f)) : rsqrtf(fmaf(__frcp_rn(r2), __frcp_rn(r2), 1.0f));
-            }
+    if (MODEL == 5) {  // Rosenhead-Moore: augmented distances
+        const float rc2 = cored ? rc * rc : 0.0f;
+        const float pa = sqrtf(na2 + rc2), pb = sqrtf(nb2 + rc2);
+        const float pr = pa * pb, tr2 = h2 + rc2;
+        const float dt = fmaf(t, t - 1.0f, tr2);
+        const float ps = pa + pb;
+        num = dt < 0.0f ? ps * (pr - dt) : ps;
+        den = pr * (dt < 0.0f ? tr2 : pr + dt);
+    } else if (MODEL == 4) {  // offset core: denominator + rc^2
+        const float plus = dot < 0.0f ? __fdividef(h2, product - dot) : product + dot;
+        num = sum;
+        den = fmaf(rc, cored ? rc : 0.0f, product * plus);
+    } else if (MODEL != 0) {
+        const float r2 = cored ? __fdividef(h2, rc * rc) : 1e30f;
+        if (MODEL == 1) {
+            factor = fminf(r2, 1.0f);
+        } else if (MODEL == 2) {
+            // 1 - exp(-x), x = 1.25643 r^2, with a series where the exponential form loses digits; 1 past the cut-off
+            const float x = (float)LAMB_A * r2;
+            const float series = x * (1.0f - x * (0.5f - x * (1.0f / 6.0f - x * (1.0f / 24.0f - x * (1.0f / 120.0f)))));
+            factor = r2 > (float)LAMB_CUT2 ? 1.0f : (x < 0.0625f ? series : 1.0f - __expf(-x));
+        } else if (MODEL == 3) {
+            const float q = fminf(r2, 1e18f);
+            factor = q < 1.0f ? q * rsqrtf(fmaf(q, q, 1.0f)) : rsqrtf(fmaf(__frcp_rn(q), __frcp_rn(q), 1.0f));
         }
     }
-    float coefficient = lo.w * factor * __fdividef(na + nb, denominator);
-    ux = fmaf(coefficient, cx, ux);
-    uy = fmaf(coefficient, cy, uy);
-    uz = fmaf(coefficient, cz, uz);
-    return 0;
+    const float coefficient = lo.w * factor * __fdividef(num, den);
+    if (!need64) {
+        ux = fmaf(coefficient, cx, ux);
+        uy = fmaf(coefficient, cy, uy);
+        uz = fmaf(coefficient, cz, uz);
+    }
+    return need64;
 }
 
 // vortex_tree.far_velocity with the symmetric second moment; R = x - c.

@@ -49,11 +49,13 @@ __global__ void pack_kernel(int64_t m, const double *starts, const double *direc
     if (seg64) {
         Seg64 q;
         q.sx = sx; q.sy = sy; q.sz = sz;
-        q.inv_len = 1.0 / L;
+        q.len = L;
         q.dx = dx; q.dy = dy; q.dz = dz;
         q.gfac = (g / L) / 12.566370614359172;  // (gamma / length) / (4 pi), vortex_numba.py:105
         q.rcl = r / L;
         q.radius = r;
+        q.inv_len = 1.0 / L;
+        q.pad = 0.0;
         seg64[k] = q;
     }
     if (seg32) {

@@ -7,12 +7,26 @@
 // Morton key of their positions so that a warp's targets are neighbours and their node sets overlap.
 // Exclusions: the target's excluded segments as sorted tree positions (vortex_tree._positions, :571-580) and a cursor
 // that only moves forward, because depth-first visits see non-decreasing range starts.
+#include <algorithm>
+
 #include "bs_sort.cuh"
 #include "bs_tree.cuh"
 
 namespace bs {
 
 constexpr int STACK_DEPTH = 128;
+constexpr int LIST_CAP = 4096;            // list entries per warp of targets
+constexpr int FAR_BIT = int(0x80000000u);
+constexpr int FAR_COST = 3;               // list cost units: one far evaluation ~ three pairs
+constexpr int LIST_WARPS = 4;             // warps per block of the list kernel
+
+struct TreeView {
+    const NodeRec *nodes;
+    const Far64 *far64;
+    const Far32 *far32;
+    const Seg64 *seg64;
+    const Seg32 *seg32;
+};
 
 struct EvalArgs {
     int64_t n;
@@ -20,42 +34,163 @@ struct EvalArgs {
     const int32_t *perm;
     const int64_t *ex_ptr;
     const int32_t *ex_pos;
-    const NodeRec *nodes;
-    const Far64 *far64;
-    const Far32 *far32;
-    const Seg64 *seg64;
-    const Seg32 *seg32;
+    TreeView tv;
     double theta, clearance;
     int order, model, raise_singular, stack_limit;
     float near2;
-    double *out;
-    int8_t *flags;
+    // interaction lists, one region of LIST_CAP entries per warp of targets
+    int2 *list;          // (node, lane mask); far entries carry FAR_BIT in the node
+    int *list_cost;      // cost before each entry
+    int *list_len;       // entries per warp
+    int *list_total;     // total cost per warp
+    // what the walk evaluates itself (list overflow) and per-target results
+    double *walk_u;
+    int8_t *walk_flag;
     int64_t *far_counts;
     int *overflow;
-    unsigned long long *counters;  // far evaluations, near pairs, fp64 pairs, visits
+    unsigned long long *counters;  // far evaluations, near pairs, fp64 pairs, visits, lane slots of leaf walks
+    // list kernel outputs
+    double *partial;     // [chunks][n][3]
+    int8_t *pflag;       // [chunks][n]
+    int chunks;
+};
+
+// Per-lane state of a target.
+struct Target {
+    double x0, x1, x2;
+    float xh0, xl0, xh1, xl1, xh2, xl2;
+    int64_t p;
+    bool valid;
+    __device__ void load(const EvalArgs &a, int64_t i) {
+        valid = i < a.n;
+        p = valid ? a.perm[i] : 0;
+        x0 = x1 = x2 = 0.0;
+        if (valid) { x0 = a.points[3 * p]; x1 = a.points[3 * p + 1]; x2 = a.points[3 * p + 2]; }
+        split2(x0, xh0, xl0);
+        split2(x1, xh1, xl1);
+        split2(x2, xh2, xl2);
+    }
+};
+
+// Sums of one target in its precision: FP64 for fp64/mixed, FP32 for fp32.
+template <int PREC> struct Acc {
+    double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+    float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+    __device__ void add64(double a, double b, double c) {
+        if (PREC == 2) { f0 += (float)a; f1 += (float)b; f2 += (float)c; }
+        else { u0 += a; u1 += b; u2 += c; }
+    }
+    __device__ void add32(float a, float b, float c) {
+        if (PREC == 2) { f0 += a; f1 += b; f2 += c; }
+        else { u0 += a; u1 += b; u2 += c; }
+    }
+    __device__ double x() const { return PREC == 2 ? (double)f0 : u0; }
+    __device__ double y() const { return PREC == 2 ? (double)f1 : u1; }
+    __device__ double z() const { return PREC == 2 ? (double)f2 : u2; }
 };
 
 template <int PREC>
-__global__ void __launch_bounds__(256) tree_eval_kernel(EvalArgs a) {
-    extern __shared__ int2 stack_mem[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int2 *stack = stack_mem + warp * STACK_DEPTH;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < a.n;
-    const int64_t p = valid ? a.perm[i] : 0;
-    double x0 = 0.0, x1 = 0.0, x2 = 0.0;
-    if (valid) { x0 = a.points[3 * p]; x1 = a.points[3 * p + 1]; x2 = a.points[3 * p + 2]; }
-    float xh0, xl0, xh1, xl1, xh2, xl2;
-    split2(x0, xh0, xl0);
-    split2(x1, xh1, xl1);
-    split2(x2, xh2, xl2);
+__device__ __forceinline__ void far_node(const EvalArgs &a, const Target &t, int node, Acc<PREC> &acc) {
+    const NodeRec nr = a.tv.nodes[node];
+    const double rx = t.x0 - nr.cx, ry = t.x1 - nr.cy, rz = t.x2 - nr.cz;
+    if (PREC == 0) {
+        double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+        far_eval<double>(rx, ry, rz, a.tv.far64[node].v, a.order, g0, g1, g2);
+        acc.add64(g0, g1, g2);
+    } else {
+        float g0 = 0.f, g1 = 0.f, g2 = 0.f;
+        far_eval<float>((float)rx, (float)ry, (float)rz, a.tv.far32[node].v, a.order, g0, g1, g2);
+        acc.add32(g0, g1, g2);
+    }
+}
+
+// One leaf for the lanes in `walk`: the warp stages the leaf's records in shared memory 32 at a time, then every
+// walking lane evaluates its pairs (exclusions skipped through the lane's forward cursor e).
+template <int PREC, int MODEL>
+__device__ __forceinline__ void leaf_pairs(const EvalArgs &a, const Target &t, int lo, int hi, bool walk,
+                                           int64_t &e, int64_t e1, Seg64 *seg64_tile, Seg32 *seg32_tile,
+                                           Acc<PREC> &acc, int &flag, long long &near_pairs,
+                                           long long &fp64_pairs) {
+    const int lane = threadIdx.x & 31;
+    if (walk) while (e < e1 && a.ex_pos[e] < lo) ++e;
+    float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+    for (int base = lo; base < hi; base += 32) {
+        const int cnt = min(32, hi - base);
+        __syncwarp();
+        if (lane < cnt) {
+            if (PREC == 0) seg64_tile[lane] = a.tv.seg64[base + lane];
+            else seg32_tile[lane] = a.tv.seg32[base + lane];
+        }
+        __syncwarp();
+        if (!walk) continue;
+        unsigned excl = 0;
+        while (e < e1 && a.ex_pos[e] < base + cnt) excl |= 1u << (a.ex_pos[e++] - base);
+        near_pairs += cnt - __popc(excl);
+        if (PREC == 0) {
+            double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+            for (int j = 0; j < cnt; ++j) {
+                if ((excl >> j) & 1u) continue;
+                int fl = pair64_at(t.x0, t.x1, t.x2, seg64_tile[j], a.model, a.raise_singular, u0, u1, u2);
+                if (fl != BS_FLAG_OK && flag == BS_FLAG_OK) flag = fl;
+            }
+            acc.add64(u0, u1, u2);
+            continue;
+        }
+        unsigned need = 0;
+#pragma unroll 4
+        for (int j = 0; j < cnt; ++j) {
+            const Seg32 &r = seg32_tile[j];
+            const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
+            const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
+            const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
+            float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+            const bool n64 = pair32<MODEL>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, v0, v1, v2);
+            const bool skip = (excl >> j) & 1u;
+            t0 += skip ? 0.f : v0;
+            t1 += skip ? 0.f : v1;
+            t2 += skip ? 0.f : v2;
+            need |= (n64 && !skip ? 1u : 0u) << j;
+        }
+        // pairs near a segment, its axis or out of FP32 range: FP64 from FP64 inputs
+        fp64_pairs += __popc(need);
+        while (need) {
+            const int j = __ffs(need) - 1;
+            need &= need - 1;
+            double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+            int fl = pair64_at(t.x0, t.x1, t.x2, a.tv.seg64[base + j], MODEL, a.raise_singular, v0, v1, v2);
+            if (fl != BS_FLAG_OK) {
+                if (flag == BS_FLAG_OK) flag = fl;
+            } else {
+                acc.add64(v0, v1, v2);
+            }
+        }
+    }
+    if (walk && PREC != 0) acc.add32(t0, t1, t2);
+}
+
+// Phase 1: the traversal.  Each warp walks the tree once for its 32 targets and writes an interaction list: far
+// nodes and near leaves with the mask of lanes concerned, in depth-first order, and the cost before each entry.  What
+// does not fit in the list is evaluated here.
+template <int PREC, int MODEL>
+__global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
+    extern __shared__ __align__(16) unsigned char eval_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    int2 *stack = reinterpret_cast<int2 *>(eval_smem) + warp * STACK_DEPTH;
+    unsigned char *tiles = eval_smem + (size_t)warps * STACK_DEPTH * sizeof(int2);
+    Seg64 *seg64_tile = reinterpret_cast<Seg64 *>(tiles) + warp * 32;
+    Seg32 *seg32_tile = reinterpret_cast<Seg32 *>(tiles) + warp * 32;
+    const int64_t gw = (int64_t)blockIdx.x * warps + warp;  // warp of targets
+    Target t;
+    t.load(a, gw * 32 + lane);
     int64_t e = 0, e1 = 0;
-    if (valid && a.ex_ptr) { e = a.ex_ptr[p]; e1 = a.ex_ptr[p + 1]; }
-    double u0 = 0.0, u1 = 0.0, u2 = 0.0;      // FP64 accumulator (fp64, mixed)
-    float f0 = 0.0f, f1 = 0.0f, f2 = 0.0f;    // FP32 accumulator (fp32)
+    if (t.valid && a.ex_ptr) { e = a.ex_ptr[t.p]; e1 = a.ex_ptr[t.p + 1]; }
+    Acc<PREC> acc;
     int flag = BS_FLAG_OK;
-    long long far = 0, near_pairs = 0, fp64_pairs = 0, visits = 0;
-    const unsigned active = __ballot_sync(0xffffffffu, valid);
+    long long far = 0, far_total = 0, near_pairs = 0, fp64_pairs = 0, visits = 0, pair_slots = 0;
+    int2 *list = a.list + gw * LIST_CAP;
+    int *cost = a.list_cost + gw * LIST_CAP;
+    int len = 0, running = 0;
+    const unsigned active = __ballot_sync(0xffffffffu, t.valid);
     if (active == 0) return;
     if (lane == 0) stack[0] = make_int2(0, (int)active);
     int top = 1;
@@ -66,14 +201,11 @@ __global__ void __launch_bounds__(256) tree_eval_kernel(EvalArgs a) {
         const int node = entry.x;
         const unsigned mask = (unsigned)entry.y;
         const bool mine = (mask >> lane) & 1u;
-        const NodeRec nr = a.nodes[node];
+        const NodeRec nr = a.tv.nodes[node];
         bool accept = false;
-        double rx = 0.0, ry = 0.0, rz = 0.0;
         if (mine) {
             ++visits;
-            rx = x0 - nr.cx;
-            ry = x1 - nr.cy;
-            rz = x2 - nr.cz;
+            const double rx = t.x0 - nr.cx, ry = t.x1 - nr.cy, rz = t.x2 - nr.cz;
             // the reference's expression, without contraction, so that decisions equal the CPU's
             double dist = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz)));
             accept = nr.bound < __dmul_rn(a.theta, dist) &&
@@ -85,49 +217,27 @@ __global__ void __launch_bounds__(256) tree_eval_kernel(EvalArgs a) {
         }
         const unsigned farm = __ballot_sync(0xffffffffu, mine && accept);
         const unsigned openm = mask & ~farm;
-        if (mine && accept) {
-            ++far;
-            if (PREC == 0) {
-                far_eval<double>(rx, ry, rz, a.far64[node].v, a.order, u0, u1, u2);
-            } else {
-                float g0 = 0.f, g1 = 0.f, g2 = 0.f;
-                far_eval<float>((float)rx, (float)ry, (float)rz, a.far32[node].v, a.order, g0, g1, g2);
-                if (PREC == 1) { u0 += g0; u1 += g1; u2 += g2; }
-                else { f0 += g0; f1 += g1; f2 += g2; }
+        if (farm) {
+            if (mine && accept) ++far;
+            far_total += __popc(farm);
+            if (len < LIST_CAP) {
+                if (lane == 0) { list[len] = make_int2(node | FAR_BIT, (int)farm); cost[len] = running; }
+                ++len;
+                running += FAR_COST;
+            } else if (mine && accept) {
+                far_node<PREC>(a, t, node, acc);
             }
         }
         if (openm) {
             if (nr.left < 0) {
-                if (mine && !accept) {
-                    while (e < e1 && a.ex_pos[e] < nr.lo) ++e;
-                    float t0 = 0.f, t1 = 0.f, t2 = 0.f;
-                    for (int k = nr.lo; k < nr.hi; ++k) {
-                        if (e < e1 && a.ex_pos[e] == k) { ++e; continue; }
-                        ++near_pairs;
-                        if (PREC == 0) {
-                            int fl = pair64_at(x0, x1, x2, a.seg64[k], a.model, a.raise_singular, u0, u1, u2);
-                            if (fl != BS_FLAG_OK && flag == BS_FLAG_OK) flag = fl;
-                        } else {
-                            const Seg32 r = a.seg32[k];
-                            float q0 = (xh0 - r.hi.x) + (xl0 - r.lo.x);
-                            float q1 = (xh1 - r.hi.y) + (xl1 - r.lo.y);
-                            float q2 = (xh2 - r.hi.z) + (xl2 - r.lo.z);
-                            if (pair32(q0, q1, q2, r.hi, r.lo, r.dir, a.model, a.near2, t0, t1, t2)) {
-                                ++fp64_pairs;
-                                double v0 = 0.0, v1 = 0.0, v2 = 0.0;
-                                int fl = pair64_at(x0, x1, x2, a.seg64[k], a.model, a.raise_singular, v0, v1, v2);
-                                if (fl != BS_FLAG_OK) {
-                                    if (flag == BS_FLAG_OK) flag = fl;
-                                } else if (PREC == 1) {
-                                    u0 += v0; u1 += v1; u2 += v2;
-                                } else {
-                                    f0 += (float)v0; f1 += (float)v1; f2 += (float)v2;
-                                }
-                            }
-                        }
-                    }
-                    if (PREC == 1) { u0 += t0; u1 += t1; u2 += t2; }
-                    else if (PREC == 2) { f0 += t0; f1 += t1; f2 += t2; }
+                pair_slots += (long long)(nr.hi - nr.lo);
+                if (len < LIST_CAP) {
+                    if (lane == 0) { list[len] = make_int2(node, (int)openm); cost[len] = running; }
+                    ++len;
+                    running += (nr.hi - nr.lo) + 2;
+                } else {
+                    leaf_pairs<PREC, MODEL>(a, t, nr.lo, nr.hi, mine && !accept, e, e1, seg64_tile, seg32_tile, acc,
+                                            flag, near_pairs, fp64_pairs);
                 }
             } else {
                 if (top + 2 > a.stack_limit) {
@@ -143,27 +253,110 @@ __global__ void __launch_bounds__(256) tree_eval_kernel(EvalArgs a) {
         }
         __syncwarp();
     }
-    if (PREC == 2) { u0 = f0; u1 = f1; u2 = f2; }
-    if (valid) {
-        if (!(isfinite(u0) && isfinite(u1) && isfinite(u2)) && flag == BS_FLAG_OK) flag = BS_FLAG_NONFINITE;
-        a.out[3 * p] = u0;
-        a.out[3 * p + 1] = u1;
-        a.out[3 * p + 2] = u2;
-        a.flags[p] = (int8_t)flag;
-        if (a.far_counts) a.far_counts[p] = far;
+    if (lane == 0) {
+        a.list_len[gw] = len;
+        a.list_total[gw] = running;
+    }
+    if (t.valid) {
+        a.walk_u[3 * t.p] = acc.x();
+        a.walk_u[3 * t.p + 1] = acc.y();
+        a.walk_u[3 * t.p + 2] = acc.z();
+        a.walk_flag[t.p] = (int8_t)flag;
+        if (a.far_counts) a.far_counts[t.p] = far;
     }
     for (int o = 16; o > 0; o >>= 1) {
-        far += __shfl_xor_sync(0xffffffffu, far, o);
         near_pairs += __shfl_xor_sync(0xffffffffu, near_pairs, o);
         fp64_pairs += __shfl_xor_sync(0xffffffffu, fp64_pairs, o);
         visits += __shfl_xor_sync(0xffffffffu, visits, o);
     }
     if (lane == 0) {
-        atomicAdd(&a.counters[0], (unsigned long long)far);
+        atomicAdd(&a.counters[0], (unsigned long long)far_total);
         atomicAdd(&a.counters[1], (unsigned long long)near_pairs);
         atomicAdd(&a.counters[2], (unsigned long long)fp64_pairs);
         atomicAdd(&a.counters[3], (unsigned long long)visits);
+        atomicAdd(&a.counters[4], (unsigned long long)(32 * pair_slots));
     }
+}
+
+// Phase 2: each warp takes one chunk (by cost) of the list of one warp of targets and evaluates its far nodes and
+// near leaves; partial sums per (chunk, target) are combined in chunk order by the reduce kernel.
+template <int PREC, int MODEL>
+__global__ void __launch_bounds__(LIST_WARPS * 32) tree_list_kernel(EvalArgs a, int64_t target_warps) {
+    __shared__ __align__(16) unsigned char tile_mem[LIST_WARPS * 32 * sizeof(Seg64)];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t gw = (int64_t)blockIdx.x * LIST_WARPS + warp;
+    if (gw >= target_warps) return;
+    Seg64 *seg64_tile = reinterpret_cast<Seg64 *>(tile_mem) + warp * 32;
+    Seg32 *seg32_tile = reinterpret_cast<Seg32 *>(tile_mem) + warp * 32;
+    const int c = blockIdx.y, chunks = gridDim.y;
+    const int len = a.list_len[gw];
+    const int64_t total = a.list_total[gw];
+    const int *cost = a.list_cost + gw * LIST_CAP;
+    const int2 *list = a.list + gw * LIST_CAP;
+    auto lower = [&](int64_t v) {  // first entry whose cost start is >= v
+        int l = 0, h = len;
+        while (l < h) {
+            int m = (l + h) >> 1;
+            if (cost[m] < v) l = m + 1; else h = m;
+        }
+        return l;
+    };
+    const int first = lower(total * c / chunks), last = lower(total * (c + 1) / chunks);
+    Target t;
+    t.load(a, gw * 32 + lane);
+    int64_t e = 0, e1 = 0;
+    if (t.valid && a.ex_ptr) { e = a.ex_ptr[t.p]; e1 = a.ex_ptr[t.p + 1]; }
+    Acc<PREC> acc;
+    int flag = BS_FLAG_OK;
+    long long near_pairs = 0, fp64_pairs = 0;
+    for (int k = first; k < last; ++k) {
+        const int2 entry = list[k];
+        const bool mine = ((unsigned)entry.y >> lane) & 1u;
+        if (entry.x & FAR_BIT) {
+            if (mine) far_node<PREC>(a, t, entry.x & ~FAR_BIT, acc);
+        } else {
+            const NodeRec nr = a.tv.nodes[entry.x];
+            leaf_pairs<PREC, MODEL>(a, t, nr.lo, nr.hi, mine, e, e1, seg64_tile, seg32_tile, acc, flag, near_pairs,
+                                    fp64_pairs);
+        }
+    }
+    if (t.valid) {
+        const int64_t o = (int64_t)c * a.n + t.p;
+        a.partial[3 * o] = acc.x();
+        a.partial[3 * o + 1] = acc.y();
+        a.partial[3 * o + 2] = acc.z();
+        a.pflag[o] = (int8_t)flag;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        near_pairs += __shfl_xor_sync(0xffffffffu, near_pairs, o);
+        fp64_pairs += __shfl_xor_sync(0xffffffffu, fp64_pairs, o);
+    }
+    if (lane == 0) {
+        atomicAdd(&a.counters[1], (unsigned long long)near_pairs);
+        atomicAdd(&a.counters[2], (unsigned long long)fp64_pairs);
+    }
+}
+
+// Chunks in order, then what the walk evaluated itself (later in depth-first order); first flag wins.
+template <int PREC>
+__global__ void tree_reduce_kernel(EvalArgs a, double *out, int8_t *flags) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n) return;
+    Acc<PREC> acc;
+    int flag = BS_FLAG_OK;
+    for (int c = 0; c < a.chunks; ++c) {
+        const int64_t o = (int64_t)c * a.n + p;
+        acc.add64(a.partial[3 * o], a.partial[3 * o + 1], a.partial[3 * o + 2]);
+        if (flag == BS_FLAG_OK) flag = a.pflag[o];
+    }
+    acc.add64(a.walk_u[3 * p], a.walk_u[3 * p + 1], a.walk_u[3 * p + 2]);
+    if (flag == BS_FLAG_OK) flag = a.walk_flag[p];
+    const double u0 = acc.x(), u1 = acc.y(), u2 = acc.z();
+    if (!(isfinite(u0) && isfinite(u1) && isfinite(u2)) && flag == BS_FLAG_OK) flag = BS_FLAG_NONFINITE;
+    out[3 * p] = u0;
+    out[3 * p + 1] = u1;
+    out[3 * p + 2] = u2;
+    flags[p] = (int8_t)flag;
 }
 
 // Morton keys of the targets inside their own box (for locality only; any order gives the same per-target result).
@@ -241,6 +434,36 @@ __global__ void exclusion_positions_kernel(int64_t n, const int64_t *ex_ptr, con
 
 static inline unsigned nblocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
+template <int PREC, int MODEL>
+static void launch_pair(unsigned walk_grid, int block, size_t smem, dim3 list_grid, int64_t target_warps,
+                        unsigned reduce_grid, cudaStream_t s, const EvalArgs &args, double *out, int8_t *flags) {
+    tree_walk_kernel<PREC, MODEL><<<walk_grid, block, smem, s>>>(args);
+    tree_list_kernel<PREC, MODEL><<<list_grid, LIST_WARPS * 32, 0, s>>>(args, target_warps);
+    tree_reduce_kernel<PREC><<<reduce_grid, 256, 0, s>>>(args, out, flags);
+}
+
+template <int PREC>
+static void launch_model(int model, unsigned walk_grid, int block, size_t smem, dim3 list_grid, int64_t tw,
+                         unsigned reduce_grid, cudaStream_t s, const EvalArgs &args, double *out, int8_t *flags) {
+    switch (model) {
+        case 0: launch_pair<PREC, 0>(walk_grid, block, smem, list_grid, tw, reduce_grid, s, args, out, flags); break;
+        case 1: launch_pair<PREC, 1>(walk_grid, block, smem, list_grid, tw, reduce_grid, s, args, out, flags); break;
+        case 2: launch_pair<PREC, 2>(walk_grid, block, smem, list_grid, tw, reduce_grid, s, args, out, flags); break;
+        case 3: launch_pair<PREC, 3>(walk_grid, block, smem, list_grid, tw, reduce_grid, s, args, out, flags); break;
+        case 4: launch_pair<PREC, 4>(walk_grid, block, smem, list_grid, tw, reduce_grid, s, args, out, flags); break;
+        default: launch_pair<PREC, 5>(walk_grid, block, smem, list_grid, tw, reduce_grid, s, args, out, flags); break;
+    }
+}
+
+// FP64 evaluates the core model at run time (one instantiation); the single precisions are specialised per model.
+static void launch_eval(int precision, int model, unsigned walk_grid, int block, size_t smem, dim3 list_grid,
+                        int64_t tw, unsigned reduce_grid, cudaStream_t s, const EvalArgs &args, double *out,
+                        int8_t *flags) {
+    if (precision == BS_FP64) launch_pair<0, 0>(walk_grid, block, smem, list_grid, tw, reduce_grid, s, args, out, flags);
+    else if (precision == BS_MIXED) launch_model<1>(model, walk_grid, block, smem, list_grid, tw, reduce_grid, s, args, out, flags);
+    else launch_model<2>(model, walk_grid, block, smem, list_grid, tw, reduce_grid, s, args, out, flags);
+}
+
 int target_order(int64_t n, const double *points, int32_t *perm, Scratch &scratch, cudaStream_t s) {
     unsigned long long *box = scratch.get<unsigned long long>(6);
     uint64_t *keys = scratch.get<uint64_t>(n);
@@ -283,7 +506,7 @@ extern "C" int bs_tree_eval(bs_ctx *ctx, const bs_tree *tree, const bs_tree_para
     const int64_t n = tgt->n;
     int32_t *perm = scratch.get<int32_t>(n);
     int *overflow = scratch.get<int>(1);
-    unsigned long long *counters = scratch.get<unsigned long long>(4);
+    unsigned long long *counters = scratch.get<unsigned long long>(5);
     int32_t *ex_pos = nullptr;
     if (!perm || !overflow || !counters) return scratch.status;
     int rc = target_order(n, tgt->points, perm, scratch, s);
@@ -296,18 +519,25 @@ extern "C" int bs_tree_eval(bs_ctx *ctx, const bs_tree *tree, const bs_tree_para
         BS_CHECK_LAUNCH("exclusion_positions_kernel");
     }
     BS_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int), s));
-    BS_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), s));
+    BS_CUDA(cudaMemsetAsync(counters, 0, 5 * sizeof(unsigned long long), s));
+    const int block = std::min(kp->block, 128);
+    const int64_t target_warps = (n + 31) / 32;
+    const int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(64, ((int64_t)ctx->sm_count * 32 + target_warps - 1)
+                                                                       / target_warps));
+    int2 *list = scratch.get<int2>((size_t)target_warps * LIST_CAP);
+    int *list_cost = scratch.get<int>((size_t)target_warps * LIST_CAP);
+    int *list_len = scratch.get<int>(target_warps), *list_total = scratch.get<int>(target_warps);
+    double *walk_u = scratch.get<double>(3 * n), *partial = scratch.get<double>((size_t)3 * n * chunks);
+    int8_t *walk_flag = scratch.get<int8_t>(n), *pflag = scratch.get<int8_t>((size_t)n * chunks);
+    if (!list || !list_cost || !list_len || !list_total || !walk_u || !partial || !walk_flag || !pflag)
+        return scratch.status;
     EvalArgs args;
     args.n = n;
     args.points = tgt->points;
     args.perm = perm;
     args.ex_ptr = ex_pos ? tgt->ex_ptr : nullptr;
     args.ex_pos = ex_pos;
-    args.nodes = tree->nodes;
-    args.far64 = tree->far64;
-    args.far32 = tree->far32;
-    args.seg64 = tree->seg64;
-    args.seg32 = tree->seg32;
+    args.tv = TreeView{tree->nodes, tree->far64, tree->far32, tree->seg64, tree->seg32};
     args.theta = tp->theta;
     args.clearance = tp->clearance;
     args.order = tp->order;
@@ -315,24 +545,31 @@ extern "C" int bs_tree_eval(bs_ctx *ctx, const bs_tree *tree, const bs_tree_para
     args.raise_singular = kp->raise_singular ? 1 : 0;
     args.near2 = (float)(kp->near_cores * kp->near_cores);
     args.stack_limit = (tp->stack_limit > 0 && tp->stack_limit < STACK_DEPTH) ? tp->stack_limit : STACK_DEPTH;
-    args.out = out;
-    args.flags = flags;
+    args.list = list;
+    args.list_cost = list_cost;
+    args.list_len = list_len;
+    args.list_total = list_total;
+    args.walk_u = walk_u;
+    args.walk_flag = walk_flag;
     args.far_counts = far_counts;
     args.overflow = overflow;
     args.counters = counters;
-    const int block = kp->block;
-    const size_t smem = (size_t)(block / 32) * STACK_DEPTH * sizeof(int2);
+    args.partial = partial;
+    args.pflag = pflag;
+    args.chunks = chunks;
+    const size_t smem = (size_t)(block / 32) * (STACK_DEPTH * sizeof(int2) + 32 * sizeof(Seg64));
+    const unsigned walk_grid = (unsigned)((target_warps + block / 32 - 1) / (block / 32));
+    const dim3 list_grid((unsigned)((target_warps + LIST_WARPS - 1) / LIST_WARPS), (unsigned)chunks);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s);
-    if (kp->precision == BS_FP64) tree_eval_kernel<0><<<nblocks(n, block), block, smem, s>>>(args);
-    else if (kp->precision == BS_MIXED) tree_eval_kernel<1><<<nblocks(n, block), block, smem, s>>>(args);
-    else tree_eval_kernel<2><<<nblocks(n, block), block, smem, s>>>(args);
+    launch_eval(kp->precision, kp->model, walk_grid, block, smem, list_grid, target_warps, nblocks(n, 256), s, args,
+                out, flags);
     cudaError_t le = cudaGetLastError();
     cudaEventRecord(e1, s);
     int host_overflow = 0;
-    unsigned long long host_counters[4] = {0, 0, 0, 0};
+    unsigned long long host_counters[5] = {0, 0, 0, 0, 0};
     if (le == cudaSuccess) le = cudaMemcpyAsync(&host_overflow, overflow, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (le == cudaSuccess)
         le = cudaMemcpyAsync(host_counters, counters, sizeof host_counters, cudaMemcpyDeviceToHost, s);
@@ -345,11 +582,12 @@ extern "C" int bs_tree_eval(bs_ctx *ctx, const bs_tree *tree, const bs_tree_para
     ctx->stats.points = n;
     ctx->stats.segments = tree->m;
     ctx->stats.nodes = tree->count;
-    ctx->stats.launches = 1;
+    ctx->stats.launches = 3;
     ctx->stats.far_evaluations = (int64_t)host_counters[0];
     ctx->stats.near_pairs = (int64_t)host_counters[1];
     ctx->stats.fp64_pairs = (int64_t)host_counters[2];
     ctx->stats.visits = (int64_t)host_counters[3];
+    ctx->stats.pair_slots = (int64_t)host_counters[4];
     ctx->stats.evaluate_ms = ms;
     if (host_overflow) {
         set_error("tree traversal stack overflow on the GPU (depth %d)", args.stack_limit);
