@@ -99,6 +99,24 @@ int bs_version(int *major, int *minor, int *arch);
 int bs_direct(bs_ctx *ctx, const bs_sources *src, const bs_targets *tgt, const bs_kernel_params *kp, double *out,
               int8_t *flags, bs_stream stream);
 
+/* Allocation-free direct sum.  No counterpart in the reference: for callers that must not allocate GPU memory while
+ * they run (a control or flight loop with a hard per-step deadline, where an allocation can stall or fail once another
+ * framework's allocator has reserved the device, or a plugin inside a host that owns all device memory).  Same
+ * semantics and arguments as bs_direct without the context (it runs on the current device, in one segment chunk), but
+ * its scratch is one fixed array compiled into the library, so it calls no cudaMalloc/cudaFree and no allocating
+ * library routine.  Limits and caveats:
+ *   - at most BS_NOALLOC_MAX_SEGMENTS segments (BS_ERR_ARG beyond); targets are not limited;
+ *   - every GPU that loads the library holds the BS_NOALLOC_SCRATCH_BYTES array until the process exits;
+ *   - the first call on a device looks up the array's device address (cudaGetSymbolAddress) with that device current;
+ *     make that first call before any stream capture;
+ *   - all calls share the one array: calls that overlap on the GPU (other streams, other host threads) race and must
+ *     be serialised by the caller;
+ *   - blocks the host until the result is ready, like bs_direct. */
+#define BS_NOALLOC_MAX_SEGMENTS 65536
+#define BS_NOALLOC_SCRATCH_BYTES (65536 * 144 + 256) /* 9 MiB of FP64 + FP32 segment records, 256 B of flags */
+int bs_direct_noalloc(const bs_sources *src, const bs_targets *tgt, const bs_kernel_params *kp, double *out,
+                      int8_t *flags, bs_stream stream);
+
 /* Tree build on the device (Morton keys + radix sort + binary radix tree, or the reference's median split element for
  * element).  Node moments and contractions about cell centres in FP64 (vortex_tree.node_moments semantics).  Blocks
  * the host while reading node counts back. */

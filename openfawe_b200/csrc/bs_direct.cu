@@ -329,3 +329,118 @@ extern "C" int bs_direct(bs_ctx *ctx, const bs_sources *src, const bs_targets *t
     }
     return BS_OK;
 }
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Allocation-free variant of bs_direct.
+//
+// For hosts that must not allocate GPU memory while they run -- a flight or control loop with a hard per-step
+// deadline (an allocation can stall on the driver or fail once a framework's caching allocator has reserved the device),
+// or a plugin loaded into a host program that owns all device memory -- the segment records live in one fixed array
+// inside this library instead of the context's memory pool.  The array is a file-scope __device__ variable, so every
+// GPU that loads the library holds it (BS_NOALLOC_SCRATCH_BYTES) until the process exits; host code must not use its
+// name as a device address and asks the runtime for the address instead (cudaGetSymbolAddress, once per device).
+// ---------------------------------------------------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+
+constexpr size_t kNoAllocSeg64 = (size_t)BS_NOALLOC_MAX_SEGMENTS * sizeof(bs::Seg64);
+constexpr size_t kNoAllocSeg32 = (size_t)BS_NOALLOC_MAX_SEGMENTS * sizeof(bs::Seg32);
+static_assert(kNoAllocSeg64 + kNoAllocSeg32 + 256 == BS_NOALLOC_SCRATCH_BYTES, "scratch layout");
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[BS_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_lock;
+void *g_noalloc_base[kMaxDevices];  // device address of g_noalloc_scratch on each device, set on first use
+
+}  // namespace
+
+extern "C" int bs_direct_noalloc(const bs_sources *src, const bs_targets *tgt, const bs_kernel_params *kp,
+                                 double *out, int8_t *flags, bs_stream stream) {
+    if (!src || !tgt || !kp || (tgt->n > 0 && (!tgt->points || !out || !flags))) {
+        set_error("bs_direct_noalloc: null argument");
+        return BS_ERR_ARG;
+    }
+    if (kp->model < 0 || kp->model > 5 || kp->precision < 0 || kp->precision > 2 ||
+        (kp->block != 32 && kp->block != 64 && kp->block != 128 && kp->block != 256)) {
+        set_error("bs_direct_noalloc: model 0..5, precision 0..2, block 32/64/128/256");
+        return BS_ERR_ARG;
+    }
+    if (src->m < 0 || (src->m > 0 && (!src->starts || !src->directions || !src->lengths || !src->gamma ||
+                                       !src->radius))) {
+        set_error("bs_direct_noalloc: invalid segment arrays");
+        return BS_ERR_ARG;
+    }
+    if (src->m > BS_NOALLOC_MAX_SEGMENTS) {
+        set_error("bs_direct_noalloc: %lld segments exceed the fixed scratch of %d segments; use bs_direct",
+                  (long long)src->m, BS_NOALLOC_MAX_SEGMENTS);
+        return BS_ERR_ARG;
+    }
+    int device = 0;
+    BS_CUDA(cudaGetDevice(&device));
+    if (device < 0 || device >= kMaxDevices) {
+        set_error("bs_direct_noalloc: device %d out of range", device);
+        return BS_ERR_ARG;
+    }
+    void *base = nullptr;
+    {
+        std::lock_guard<std::mutex> guard(g_noalloc_lock);
+        if (!g_noalloc_base[device]) {
+            // once per device, with that device current: the array's device address
+            cudaError_t e = cudaGetSymbolAddress(&g_noalloc_base[device], g_noalloc_scratch);
+            if (e != cudaSuccess) {
+                g_noalloc_base[device] = nullptr;
+                return cuda_fail(e, "bs_direct_noalloc: cudaGetSymbolAddress");
+            }
+        }
+        base = g_noalloc_base[device];
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t n = tgt->n, m = src->m;
+    if (n == 0) return BS_OK;
+    if (m == 0) {
+        BS_CUDA(cudaMemsetAsync(out, 0, n * 3 * sizeof(double), s));
+        BS_CUDA(cudaMemsetAsync(flags, 0, n, s));
+        return BS_OK;
+    }
+    unsigned char *bytes = static_cast<unsigned char *>(base);
+    Seg64 *seg64 = reinterpret_cast<Seg64 *>(bytes);
+    Seg32 *seg32 = reinterpret_cast<Seg32 *>(bytes + kNoAllocSeg64);
+    int *error = reinterpret_cast<int *>(bytes + kNoAllocSeg64 + kNoAllocSeg32);
+    unsigned long long *fp64_pairs = reinterpret_cast<unsigned long long *>(bytes + kNoAllocSeg64 + kNoAllocSeg32 + 64);
+    // the array keeps the previous call's contents: clear the error flag and the counter
+    BS_CUDA(cudaMemsetAsync(error, 0, sizeof(int), s));
+    BS_CUDA(cudaMemsetAsync(fp64_pairs, 0, sizeof(unsigned long long), s));
+    const int prec = kp->precision;
+    int rc = pack_segments(src, nullptr, seg64, prec != BS_FP64 ? seg32 : nullptr, nullptr, s);
+    if (rc != BS_OK) return rc;
+    DirectArgs args;
+    args.n = n;
+    args.m = m;
+    args.chunk_len = m;  // one chunk: no partial sums, hence no further scratch
+    args.points = tgt->points;
+    args.ex_ptr = (tgt->ex_ptr && tgt->e > 0) ? tgt->ex_ptr : nullptr;
+    args.ex_seg = tgt->ex_seg;
+    args.seg64 = seg64;
+    args.seg32 = seg32;
+    args.model = kp->model;
+    args.raise_singular = kp->raise_singular ? 1 : 0;
+    args.near2 = (float)(kp->near_cores * kp->near_cores);
+    args.out = out;
+    args.flags = flags;
+    args.error = error;
+    args.fp64_pairs = fp64_pairs;
+    dim3 grid((unsigned)((n + kp->block - 1) / kp->block), 1);
+    launch_direct(prec, kp->model, grid, kp->block, s, args);
+    cudaError_t le = cudaGetLastError();
+    int host_error = 0;
+    if (le == cudaSuccess) le = cudaMemcpyAsync(&host_error, error, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (le == cudaSuccess) le = cudaStreamSynchronize(s);
+    if (le != cudaSuccess) return cuda_fail(le, "bs_direct_noalloc");
+    if (host_error) {
+        set_error("bs_direct_noalloc: a bounded wait for a segment tile gave up");
+        return BS_ERR_TIMEOUT;
+    }
+    return BS_OK;
+}
