@@ -27,7 +27,7 @@ sys.path.insert(0, HERE)
 
 METRIC = "ms/call at 102k-820k segs, mixed vs FP64 at <=1e-6 rel err; adjoint/fwd ratio"
 ROWS, TARGETS, SEED = 3744, 20570, 3744
-THETA, ORDER, LEAF, CLEARANCE = 0.05, 2, 32, 3.0
+THETA, ORDER, LEAF, CLEARANCE = 0.04, 2, 32, 3.0
 L2_FLUSH_BYTES = 512 << 20  # larger than the 126 MB L2
 
 

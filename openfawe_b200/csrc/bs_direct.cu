@@ -112,19 +112,24 @@ __global__ void __launch_bounds__(256) direct_kernel(DirectArgs a) {
                 }
                 float t0 = 0.f, t1 = 0.f, t2 = 0.f;
                 unsigned need = 0;
+                if (excl == 0) {  // the common case: every pair of the sub-tile counts
 #pragma unroll 4
-                for (int j = 0; j < sc; ++j) {
-                    const Seg32 &r = reinterpret_cast<const Seg32 &>(tile[b][sub + j]);
-                    const float q0 = (xh0 - r.hi.x) + (xl0 - r.lo.x);
-                    const float q1 = (xh1 - r.hi.y) + (xl1 - r.lo.y);
-                    const float q2 = (xh2 - r.hi.z) + (xl2 - r.lo.z);
-                    float v0 = 0.f, v1 = 0.f, v2 = 0.f;
-                    const bool n64 = pair32<MODEL>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, v0, v1, v2);
-                    const bool skip = (excl >> j) & 1u;
-                    t0 += skip ? 0.f : v0;
-                    t1 += skip ? 0.f : v1;
-                    t2 += skip ? 0.f : v2;
-                    need |= (n64 && !skip ? 1u : 0u) << j;
+                    for (int j = 0; j < sc; ++j) {
+                        const Seg32 &r = reinterpret_cast<const Seg32 &>(tile[b][sub + j]);
+                        const float q0 = (xh0 - r.hi.x) + (xl0 - r.lo.x);
+                        const float q1 = (xh1 - r.hi.y) + (xl1 - r.lo.y);
+                        const float q2 = (xh2 - r.hi.z) + (xl2 - r.lo.z);
+                        if (pair32<MODEL>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1u << j;
+                    }
+                } else {
+                    for (int j = 0; j < sc; ++j) {
+                        if ((excl >> j) & 1u) continue;
+                        const Seg32 &r = reinterpret_cast<const Seg32 &>(tile[b][sub + j]);
+                        const float q0 = (xh0 - r.hi.x) + (xl0 - r.lo.x);
+                        const float q1 = (xh1 - r.hi.y) + (xl1 - r.lo.y);
+                        const float q2 = (xh2 - r.hi.z) + (xl2 - r.lo.z);
+                        if (pair32<MODEL>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1u << j;
+                    }
                 }
                 fp64_pairs += __popc(need);
                 while (need) {

@@ -216,17 +216,18 @@ __device__ __forceinline__ int pair64_at(double px, double py, double pz, const 
     return pair64_core(ax, ay, az, t, cx, cy, cz, s, model, raise_singular, ux, uy, uz);
 }
 
-// The single-precision pair, branch-free so that unrolled loops interleave independent pairs.  `rx, ry, rz` is
-// p - s (formed from two-float coordinates).  Adds the velocity to (ux, uy, uz) unless the pair needs FP64, which is
-// returned as true: within near_cores core radii of the segment (near2 = near_cores^2), within 1e-4 L of its axis (the
-// reference's "suspect" rule, vortex_cuda.py:123-124), a core too small for FP32 (rc/L marked -1), or out of FP32's
-// comfortable range -- the FP64 pair then decides value and flags exactly.  MODEL is the core model (0..5).
+// The single-precision pair.  `rx, ry, rz` is p - s (formed from two-float coordinates); dir.w holds (L/rc)^2, 0 for
+// no core, -1 for a core too small for FP32.  Adds the velocity to (ux, uy, uz) unless the pair needs FP64, which is
+// returned as true: within sqrt(near2) core radii of the finite segment, within 1e-4 L of its axis (the reference's
+// "suspect" rule, vortex_cuda.py:123-124), a tiny core, or out of FP32's comfortable range -- the FP64 pair then
+// decides value and flags exactly.  The common path has no data-dependent branch; the core factor is computed only
+// where it differs from 1 (Lamb-Oseen past its cut-off, Rankine and Vatistas outside one core radius).  MODEL: 0..5.
 template <int MODEL>
 __device__ __forceinline__ bool pair32(float rx, float ry, float rz, const float4 &hi, const float4 &lo,
                                        const float4 &dir, float near2, float &ux, float &uy, float &uz) {
     const float il = hi.w;
     const float ax = rx * il, ay = ry * il, az = rz * il;
-    const float dx = dir.x, dy = dir.y, dz = dir.z, rc = dir.w;
+    const float dx = dir.x, dy = dir.y, dz = dir.z, irc2 = dir.w;
     const float t = fmaf(az, dz, fmaf(ay, dy, ax * dx));
     const float cx = fmaf(dy, az, -dz * ay);
     const float cy = fmaf(dz, ax, -dx * az);
@@ -236,45 +237,53 @@ __device__ __forceinline__ bool pair32(float rx, float ry, float rz, const float
     const float bx = ax - dx, by = ay - dy, bz = az - dz;
     const float nb2 = fmaf(bx, bx, fmaf(by, by, bz * bz));
     const float big2 = fmaxf(1.0f, fmaxf(na2, nb2));
-    const float seg2 = t < 0.0f ? na2 : (t > 1.0f ? nb2 : h2);  // distance^2 to the finite segment (units of L^2)
-    const bool cored = MODEL != 0 && rc > 0.0f;
-    const bool need64 = !(h2 > 1e-8f * big2) || !(big2 < 1e18f) || rc < 0.0f || (cored && seg2 < near2 * rc * rc);
+    bool need64 = !(h2 > 1e-8f * big2) || !(big2 < 1e18f) || irc2 < 0.0f;
+    if (MODEL != 0) {
+        const float seg2 = t < 0.0f ? na2 : (t > 1.0f ? nb2 : h2);  // distance^2 to the finite segment, units of L^2
+        need64 = need64 || (irc2 > 0.0f && seg2 * irc2 < near2);
+    }
     const float na = na2 * rsqrtf(na2), nb = nb2 * rsqrtf(nb2);
     float product = na * nb;
     float dot = fmaf(t, t - 1.0f, h2);
-    float sum = na + nb;
     // coefficient = (Gamma/L)/(4 pi) * factor * (na + nb) / (product * plus) with plus = product + dot, or, when
     // dot < 0, the rationalised h^2 / (product - dot); one reciprocal either way.
-    float num = dot < 0.0f ? sum * (product - dot) : sum;
+    float num = na + nb;
+    num = dot < 0.0f ? num * (product - dot) : num;
     float den = product * (dot < 0.0f ? h2 : product + dot);
     float factor = 1.0f;
-    if (MODEL == 5) {  // Rosenhead-Moore: augmented distances
-        const float rc2 = cored ? rc * rc : 0.0f;
-        const float pa = sqrtf(na2 + rc2), pb = sqrtf(nb2 + rc2);
-        const float pr = pa * pb, tr2 = h2 + rc2;
-        const float dt = fmaf(t, t - 1.0f, tr2);
-        const float ps = pa + pb;
-        num = dt < 0.0f ? ps * (pr - dt) : ps;
-        den = pr * (dt < 0.0f ? tr2 : pr + dt);
-    } else if (MODEL == 4) {  // offset core: denominator + rc^2
-        const float plus = dot < 0.0f ? __fdividef(h2, product - dot) : product + dot;
-        num = sum;
-        den = fmaf(rc, cored ? rc : 0.0f, product * plus);
+    if (MODEL == 5 || MODEL == 4) {
+        if (irc2 > 0.0f) {
+            const float rc2 = __fdividef(1.0f, irc2);
+            if (MODEL == 5) {  // Rosenhead-Moore: augmented distances
+                const float pa = sqrtf(na2 + rc2), pb = sqrtf(nb2 + rc2);
+                const float pr = pa * pb, tr2 = h2 + rc2;
+                const float dt = fmaf(t, t - 1.0f, tr2);
+                num = dt < 0.0f ? (pa + pb) * (pr - dt) : pa + pb;
+                den = pr * (dt < 0.0f ? tr2 : pr + dt);
+            } else {  // offset core: denominator + rc^2
+                const float plus = dot < 0.0f ? __fdividef(h2, product - dot) : product + dot;
+                num = na + nb;
+                den = fmaf(product, plus, rc2);
+            }
+        }
     } else if (MODEL != 0) {
-        const float r2 = cored ? __fdividef(h2, rc * rc) : 1e30f;
-        if (MODEL == 1) {
-            factor = fminf(r2, 1.0f);
-        } else if (MODEL == 2) {
-            // 1 - exp(-x), x = 1.25643 r^2, with a series where the exponential form loses digits; 1 past the cut-off
-            const float x = (float)LAMB_A * r2;
-            const float series = x * (1.0f - x * (0.5f - x * (1.0f / 6.0f - x * (1.0f / 24.0f - x * (1.0f / 120.0f)))));
-            factor = r2 > (float)LAMB_CUT2 ? 1.0f : (x < 0.0625f ? series : 1.0f - __expf(-x));
-        } else if (MODEL == 3) {
-            const float q = fminf(r2, 1e18f);
-            factor = q < 1.0f ? q * rsqrtf(fmaf(q, q, 1.0f)) : rsqrtf(fmaf(__frcp_rn(q), __frcp_rn(q), 1.0f));
+        const float r2 = h2 * irc2;  // (h / rc)^2, 0 when there is no core
+        if (irc2 > 0.0f && r2 < (MODEL == 2 ? (float)LAMB_CUT2 : 1e30f)) {
+            if (MODEL == 1) {
+                factor = fminf(r2, 1.0f);
+            } else if (MODEL == 2) {
+                // 1 - exp(-x), x = 1.25643 r^2, by its series where the exponential form loses digits
+                const float x = (float)LAMB_A * r2;
+                factor = x < 0.0625f
+                             ? x * (1.0f - x * (0.5f - x * (1.0f / 6.0f - x * (1.0f / 24.0f - x * (1.0f / 120.0f)))))
+                             : 1.0f - __expf(-x);
+            } else {  // Vatistas n = 2
+                factor = r2 < 1.0f ? r2 * rsqrtf(fmaf(r2, r2, 1.0f))
+                                   : rsqrtf(fmaf(__fdividef(1.0f, r2), __fdividef(1.0f, r2), 1.0f));
+            }
         }
     }
-    const float coefficient = lo.w * factor * __fdividef(num, den);
+    const float coefficient = lo.w * factor * num * __fdividef(1.0f, den);
     if (!need64) {
         ux = fmaf(coefficient, cx, ux);
         uy = fmaf(coefficient, cy, uy);

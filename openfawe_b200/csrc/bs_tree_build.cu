@@ -65,9 +65,10 @@ __global__ void pack_kernel(int64_t m, const double *starts, const double *direc
         split2(sz, q.hi.z, q.lo.z);
         q.hi.w = (float)(1.0 / L);
         q.lo.w = (float)((g / L) / 12.566370614359172);
-        // rc/L below FP32's comfortable range: mark the segment (-1) so that its pairs are always done in FP64
+        // (L/rc)^2; 0 without a core; -1 marks rc/L below FP32's comfortable range (its pairs are done in FP64)
         double rcl = r / L;
-        q.dir = make_float4((float)dx, (float)dy, (float)dz, r > 0.0 ? (rcl >= 1e-15 ? (float)rcl : -1.0f) : 0.0f);
+        q.dir = make_float4((float)dx, (float)dy, (float)dz,
+                            r > 0.0 ? (rcl >= 1e-15 ? (float)(1.0 / (rcl * rcl)) : -1.0f) : 0.0f);
         seg32[k] = q;
     }
     if (geo) {

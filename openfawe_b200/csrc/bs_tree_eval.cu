@@ -35,7 +35,7 @@ struct EvalArgs {
     const int64_t *ex_ptr;
     const int32_t *ex_pos;
     TreeView tv;
-    double theta, clearance;
+    double theta, theta2, clearance;
     int order, model, raise_singular, stack_limit;
     float near2;
     // interaction lists, one region of LIST_CAP entries per warp of targets
@@ -137,19 +137,24 @@ __device__ __forceinline__ void leaf_pairs(const EvalArgs &a, const Target &t, i
             continue;
         }
         unsigned need = 0;
+        if (excl == 0) {  // the common case: every pair of the tile counts
 #pragma unroll 4
-        for (int j = 0; j < cnt; ++j) {
-            const Seg32 &r = seg32_tile[j];
-            const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
-            const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
-            const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
-            float v0 = 0.f, v1 = 0.f, v2 = 0.f;
-            const bool n64 = pair32<MODEL>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, v0, v1, v2);
-            const bool skip = (excl >> j) & 1u;
-            t0 += skip ? 0.f : v0;
-            t1 += skip ? 0.f : v1;
-            t2 += skip ? 0.f : v2;
-            need |= (n64 && !skip ? 1u : 0u) << j;
+            for (int j = 0; j < cnt; ++j) {
+                const Seg32 &r = seg32_tile[j];
+                const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
+                const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
+                const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
+                if (pair32<MODEL>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1u << j;
+            }
+        } else {
+            for (int j = 0; j < cnt; ++j) {
+                if ((excl >> j) & 1u) continue;
+                const Seg32 &r = seg32_tile[j];
+                const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
+                const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
+                const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
+                if (pair32<MODEL>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1u << j;
+            }
         }
         // pairs near a segment, its axis or out of FP32 range: FP64 from FP64 inputs
         fp64_pairs += __popc(need);
@@ -206,10 +211,21 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
         if (mine) {
             ++visits;
             const double rx = t.x0 - nr.cx, ry = t.x1 - nr.cy, rz = t.x2 - nr.cz;
-            // the reference's expression, without contraction, so that decisions equal the CPU's
-            double dist = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz)));
-            accept = nr.bound < __dmul_rn(a.theta, dist) &&
-                     __dsub_rn(dist, nr.bound) >= __dmul_rn(a.clearance, nr.clear_core);
+            // |R|^2 as the reference forms it, without contraction
+            const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz));
+            // The reference's test, bound < theta |R| and |R| - bound >= clearance * core, in squared form (no square
+            // root); only within 1e-12 (relative) of either boundary are the two forms allowed to round differently,
+            // and there the reference's own expression decides, so the decisions equal the CPU's.
+            const double cc = __dmul_rn(a.clearance, nr.clear_core);
+            const double b2 = nr.bound * nr.bound, lhs1 = a.theta2 * r2;
+            const double reach = nr.bound + cc, rhs2 = reach * reach;
+            const double q1 = lhs1 - b2, q2 = r2 - rhs2;
+            if (fabs(q1) > 1e-12 * fmax(lhs1, b2) && fabs(q2) > 1e-12 * fmax(r2, rhs2)) {
+                accept = q1 > 0.0 && q2 > 0.0;
+            } else {
+                const double dist = sqrt(r2);
+                accept = nr.bound < __dmul_rn(a.theta, dist) && __dsub_rn(dist, nr.bound) >= cc;
+            }
             if (accept && e < e1) {
                 while (e < e1 && a.ex_pos[e] < nr.lo) ++e;
                 if (e < e1 && a.ex_pos[e] < nr.hi) accept = false;
@@ -539,6 +555,7 @@ extern "C" int bs_tree_eval(bs_ctx *ctx, const bs_tree *tree, const bs_tree_para
     args.ex_pos = ex_pos;
     args.tv = TreeView{tree->nodes, tree->far64, tree->far32, tree->seg64, tree->seg32};
     args.theta = tp->theta;
+    args.theta2 = tp->theta * tp->theta;
     args.clearance = tp->clearance;
     args.order = tp->order;
     args.model = kp->model;
