@@ -143,6 +143,15 @@ int bs_tree_keys(const bs_tree *tree, uint64_t *keys, int64_t *sorted_order, bs_
 int bs_tree_eval(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const bs_targets *tgt,
                  const bs_kernel_params *kp, double *out, int8_t *flags, int64_t *far_counts, bs_stream stream);
 
+/* Adjoint of the exact direct sum (no counterpart in the reference, which has no adjoint): given the cotangent w
+ * [n,3] of the induced velocity, writes d(sum_p w_p . u_p) with respect to the targets [n,3], the segment starts A and
+ * ends B [m,3] and the circulations [m]; any output may be NULL.  Segments are given by their endpoints; core models
+ * NONE, RANKINE and LAMB_OSEEN; excluded and on-axis pairs contribute nothing.  FP64, pair terms recomputed. */
+int bs_adjoint_direct(bs_ctx *ctx, int64_t n, const double *points, int64_t m, const double *A, const double *B,
+                      const double *gamma, const double *radius, const int64_t *ex_ptr, const int64_t *ex_seg,
+                      int64_t e, int model, const double *cotangent, double *grad_points, double *grad_A,
+                      double *grad_B, double *grad_gamma, bs_stream stream);
+
 /* Build + evaluate + free (cuda_tree_sum in one call). */
 int bs_tree_sum(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, const bs_targets *tgt,
                 const bs_kernel_params *kp, double *out, int8_t *flags, int64_t *far_counts, bs_stream stream);
