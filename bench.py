@@ -41,6 +41,7 @@ def parse():
     p.add_argument("--theta", type=float, default=THETA)
     p.add_argument("--kind", default="morton", choices=("morton", "median"))
     p.add_argument("--cpu-sample", type=int, default=1024, help="targets in the CPU-baseline sample")
+    p.add_argument("--no-extras", action="store_true", help="skip the batched-wakes and adjoint measurements")
     return p.parse_args()
 
 
@@ -163,6 +164,76 @@ def reference_arm(args):
                                           "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _event_ms(fn):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def batch_measure(device, theta):
+    """48 rotor-sheet wakes of 5k-410k segments (a wind sweep) in one forest: autotuned build + evaluation, the
+    evaluation alone, its CUDA-graph replay, and the same wakes one tree_sum call each (the reference's pattern)."""
+    import torch
+    from openfawe_b200 import batch, wakes
+    cases = wakes.wake_batch(48, seed=48)
+    b = batch.WakeBatch(cases, device)
+    tuned = batch.autotune(b, theta=theta, leaves=(16, 32), blocks=(64, 128))
+    leaf, block = tuned["choice"]
+    total = min(_event_ms(lambda: (b.build(leaf), b.evaluate(theta, block=block))) for _ in range(3))
+    evaluate = min(_event_ms(lambda: b.evaluate(theta, block=block)) for _ in range(3))
+    graph = b.capture(theta, block=block)
+    graph.launch()
+    torch.cuda.synchronize()
+    replay = min(_event_ms(graph.launch) for _ in range(3))
+    batch.sequential(cases[:4], device, theta=theta, leaf_size=leaf, block=block)   # warm the pool
+    seq = min((batch.sequential(cases, device, theta=theta, leaf_size=leaf, block=block)[0] for _ in range(2)),
+              key=lambda t: t.sum())
+    return {"wakes": len(cases), "segments": int(b.sources.m), "targets": int(b.targets.n),
+            "segments_per_wake": [int(min(len(c["starts"]) for c in cases)), int(max(len(c["starts"]) for c in cases))],
+            "autotune": {"leaf_size": leaf, "block": block, "table_ms": tuned["table"]},
+            "batched_total_ms": total, "batched_eval_ms": evaluate, "graph_replay_ms": replay,
+            "sequential_total_ms": float(seq.sum()), "sequential_p50_ms": float(np.percentile(seq, 50)),
+            "sequential_p99_ms": float(np.percentile(seq, 99)),
+            "batched_per_wake_ms": total / len(cases), "speedup_vs_sequential": float(seq.sum()) / total}
+
+
+def adjoint_measure(device, theta):
+    """The hand-written adjoint (grads w.r.t. targets, both endpoints and circulations) on a 468-row rotor sheet
+    against the forward it differentiates (FP64 direct) and the mixed tree forward."""
+    import torch
+    from openfawe_b200 import adjoint, engine, wakes
+    case = wakes.rotor_sheet(468, seed=468, targets=20570)
+    ends = case["nodes"][case["edges"][:, 1]]
+    pts = torch.as_tensor(case["points"], device=device)
+    a = torch.as_tensor(case["starts"], device=device)
+    bb = torch.as_tensor(ends, device=device)
+    gam = torch.as_tensor(case["gamma"], device=device)
+    rad = torch.as_tensor(case["radius"], device=device)
+    rng = np.random.default_rng(5)
+    w = torch.as_tensor(rng.standard_normal((len(case["points"]), 3)).astype(np.float32).astype(np.float64),
+                        device=device)
+    src = engine.Sources(case["starts"], case["directions"], case["lengths"], case["gamma"], case["radius"], device)
+    tgt = engine.Targets(case["points"], None, device)
+    model = case["model"]
+    run_adj = lambda: adjoint.adjoint_direct(pts, a, bb, gam, rad, model, w)  # noqa: E731
+    run_direct = lambda: engine.direct(src, tgt, model, "raise", "fp64")  # noqa: E731
+    run_tree = lambda: engine.tree_sum(src, tgt, model, "raise", "mixed", 128, 3.0, theta, ORDER, LEAF,  # noqa: E731
+                                       CLEARANCE, "morton", far_counts=False)
+    for fn in (run_adj, run_direct, run_tree):
+        fn()
+    torch.cuda.synchronize()
+    adj = min(_event_ms(run_adj) for _ in range(3))
+    fwd = min(_event_ms(run_direct) for _ in range(3))
+    tree = min(_event_ms(run_tree) for _ in range(3))
+    return {"workload": f"rotor-sheet wake 468 rows, {src.m} segments x {tgt.n} targets, cotangent N(0,1) seed 5",
+            "adjoint_ms": adj, "fp64_direct_forward_ms": fwd, "mixed_tree_forward_ms": tree,
+            "ratio_to_fp64_direct": adj / fwd, "ratio_to_tree_forward": adj / tree}
 
 
 def main():
@@ -298,6 +369,10 @@ def main():
             "gpu_launches": gpu_launches, "clocks": clocks}
     if rank == 0 and world == 1:
         line["cpu_baseline"] = cpu_baseline(case, args)
+        if not args.no_extras:
+            line["batch"] = batch_measure(device, args.theta)
+            line["adjoint"] = adjoint_measure(device, args.theta)
+            line["adjoint_fwd_ratio"] = line["adjoint"]["ratio_to_fp64_direct"]
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -143,6 +143,32 @@ int bs_tree_keys(const bs_tree *tree, uint64_t *keys, int64_t *sorted_order, bs_
 int bs_tree_eval(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const bs_targets *tgt,
                  const bs_kernel_params *kp, double *out, int8_t *flags, int64_t *far_counts, bs_stream stream);
 
+/* Forests: many wakes in one tree, for batched evaluation (no counterpart in the reference, which evaluates one wake
+ * per call).  The segments of all wakes are concatenated; wake w holds segments [wake_ptr[w], wake_ptr[w+1]) (device
+ * int64 [nwakes+1]).  Keys carry the wake number above a Morton key in the wake's own box, so every wake's segment
+ * range is one node of the traversal tree, its root; wakes never see each other. */
+typedef struct bs_graph bs_graph;
+int bs_forest_build(bs_ctx *ctx, const bs_sources *src, int nwakes, const int64_t *wake_ptr, const bs_tree_params *tp,
+                    bs_tree **forest, bs_stream stream);
+/* Root node of each wake (device int32 [nwakes]; -1 for a wake without segments). */
+int bs_forest_roots(const bs_tree *forest, int32_t *roots, bs_stream stream);
+/* Evaluate every wake at its own targets: targets of wake w are [target_wake_ptr[w], target_wake_ptr[w+1]) of the
+ * concatenated target array (device int64 [nwakes+1]).  One traversal launch and one persistent list kernel for all
+ * wakes; exclusion CSR segment ids are global (offset by the wake's first segment). */
+int bs_forest_eval(bs_ctx *ctx, const bs_tree *forest, const bs_tree_params *tp, const bs_targets *tgt,
+                   const int64_t *target_wake_ptr, const bs_kernel_params *kp, double *out, int8_t *flags,
+                   int64_t *far_counts, bs_stream stream);
+/* Capture the evaluation of bs_forest_eval (target_wake_ptr may be NULL for a plain tree) into a CUDA graph with its
+ * scratch pre-allocated; bs_graph_launch replays it on any stream (same tree, same buffers; new target positions may
+ * be written into the same target buffer between launches).  bs_graph_status reads the counters of the last launch
+ * (blocking) and returns BS_ERR_STACK after a traversal stack overflow. */
+int bs_forest_graph(bs_ctx *ctx, const bs_tree *forest, const bs_tree_params *tp, const bs_targets *tgt,
+                    const int64_t *target_wake_ptr, const bs_kernel_params *kp, double *out, int8_t *flags,
+                    int64_t *far_counts, bs_graph **graph);
+int bs_graph_launch(bs_graph *graph, bs_stream stream);
+int bs_graph_status(bs_graph *graph, bs_stats *stats);
+void bs_graph_free(bs_graph *graph);
+
 /* Adjoint of the exact direct sum (no counterpart in the reference, which has no adjoint): given the cotangent w
  * [n,3] of the induced velocity, writes d(sum_p w_p . u_p) with respect to the targets [n,3], the segment starts A and
  * ends B [m,3] and the circulations [m]; any output may be NULL.  Segments are given by their endpoints; core models

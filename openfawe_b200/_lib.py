@@ -66,6 +66,16 @@ SIGNATURES = {
                                     ctypes.POINTER(KernelParams), _p, _p, _p, _p]),
     "bs_tree_sum": (ctypes.c_int, [_p, ctypes.POINTER(Sources), ctypes.POINTER(TreeParams), ctypes.POINTER(Targets),
                                    ctypes.POINTER(KernelParams), _p, _p, _p, _p]),
+    "bs_forest_build": (ctypes.c_int, [_p, ctypes.POINTER(Sources), ctypes.c_int, _p, ctypes.POINTER(TreeParams),
+                                       ctypes.POINTER(_p), _p]),
+    "bs_forest_roots": (ctypes.c_int, [_p, _p, _p]),
+    "bs_forest_eval": (ctypes.c_int, [_p, _p, ctypes.POINTER(TreeParams), ctypes.POINTER(Targets), _p,
+                                      ctypes.POINTER(KernelParams), _p, _p, _p, _p]),
+    "bs_forest_graph": (ctypes.c_int, [_p, _p, ctypes.POINTER(TreeParams), ctypes.POINTER(Targets), _p,
+                                       ctypes.POINTER(KernelParams), _p, _p, _p, ctypes.POINTER(_p)]),
+    "bs_graph_launch": (ctypes.c_int, [_p, _p]),
+    "bs_graph_status": (ctypes.c_int, [_p, ctypes.POINTER(Stats)]),
+    "bs_graph_free": (None, [_p]),
 }
 
 _LOCK = threading.RLock()

@@ -35,20 +35,38 @@ int cuda_fail(cudaError_t e, const char *what);
         if (_e != cudaSuccess) return ::bs::cuda_fail(_e, what);       \
     } while (0)
 
-// Stream-ordered scratch from the context's pool, released (stream-ordered) when the object goes out of scope.
+// Stream-ordered scratch from the context's pool, released (stream-ordered) when the object goes out of scope.  In
+// arena mode (a pre-allocated buffer, used while a CUDA graph is captured) requests are carved from the arena and
+// nothing is allocated or freed.  `requested` counts the bytes asked for (256-byte granules), so a first, ordinary
+// run can size the arena of a later capture.
 struct Scratch {
     cudaStream_t stream = nullptr;
     cudaMemPool_t pool = nullptr;
     std::vector<void *> ptrs;
     int status = BS_OK;
+    char *arena = nullptr;
+    size_t arena_size = 0, arena_used = 0, requested = 0;
     Scratch(cudaMemPool_t p, cudaStream_t s) : stream(s), pool(p) {}
+    Scratch(void *a, size_t bytes, cudaStream_t s) : stream(s), arena(static_cast<char *>(a)), arena_size(bytes) {}
     Scratch(const Scratch &) = delete;
     Scratch &operator=(const Scratch &) = delete;
     template <class T> T *get(size_t elems) {
         if (status != BS_OK) return nullptr;
         if (elems == 0) elems = 1;
+        const size_t bytes = (elems * sizeof(T) + 255) / 256 * 256;
+        requested += bytes;
+        if (arena) {
+            if (arena_used + bytes > arena_size) {
+                status = BS_ERR_OOM;
+                set_error("scratch arena of %zu bytes exhausted", arena_size);
+                return nullptr;
+            }
+            void *p = arena + arena_used;
+            arena_used += bytes;
+            return static_cast<T *>(p);
+        }
         void *p = nullptr;
-        cudaError_t e = cudaMallocFromPoolAsync(&p, elems * sizeof(T), pool, stream);
+        cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool, stream);
         if (e != cudaSuccess) {
             status = e == cudaErrorMemoryAllocation ? BS_ERR_OOM : BS_ERR_CUDA;
             cuda_fail(e, "scratch allocation");

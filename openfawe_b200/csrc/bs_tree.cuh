@@ -32,6 +32,8 @@ struct bs_tree {
     bs::Seg64 *seg64 = nullptr;  // tree order
     bs::Seg32 *seg32 = nullptr;  // tree order
     uint64_t *keys = nullptr;    // Morton keys (input order), Morton trees only
+    int32_t *wake_root = nullptr;  // forests: root node of each wake (-1 for a wake without segments)
+    int nwakes = 0;
     float build_ms = 0.f, moments_ms = 0.f;
     void *blocks[32];
     int nblocks = 0;

@@ -187,35 +187,41 @@ __global__ void karras_kernel(int64_t n, const uint64_t *k, int32_t *first, int3
     last[i] = (int32_t)(i < j ? j : i);
 }
 
-__device__ __forceinline__ bool big_internal(const int32_t *first, const int32_t *last, int64_t leaf, int64_t c,
-                                             bool is_leaf_segment) {
-    return !is_leaf_segment && (int64_t)(last[c] - first[c] + 1) > leaf;
+// An internal node is "big" (a traversal node with children) when it holds more than leaf segments or, in a forest,
+// when its keys span more than one wake (wake_shift > 0: the bit position of the wake number in the keys).
+__device__ __forceinline__ bool big_range(const uint64_t *keys, int wake_shift, int64_t leaf, int64_t f, int64_t l) {
+    return (l - f + 1) > leaf || (wake_shift > 0 && (keys[f] >> wake_shift) != (keys[l] >> wake_shift));
 }
 
-__global__ void slot_count_kernel(int64_t n, const int32_t *first, const int32_t *last, const int32_t *split,
-                                  int64_t leaf, int64_t *count) {
+__device__ __forceinline__ bool big_internal(const uint64_t *keys, int wake_shift, const int32_t *first,
+                                             const int32_t *last, int64_t leaf, int64_t c, bool is_leaf_segment) {
+    return !is_leaf_segment && big_range(keys, wake_shift, leaf, first[c], last[c]);
+}
+
+__global__ void slot_count_kernel(int64_t n, const uint64_t *keys, int wake_shift, const int32_t *first,
+                                  const int32_t *last, const int32_t *split, int64_t leaf, int64_t *count) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
     int64_t c = 0;
-    if ((int64_t)(last[i] - first[i] + 1) > leaf) {
+    if (big_range(keys, wake_shift, leaf, first[i], last[i])) {
         int32_t g = split[i];
-        c = 1 + !big_internal(first, last, leaf, g, g == first[i]) + !big_internal(first, last, leaf, g + 1,
-                                                                                   g + 1 == last[i]);
+        c = 1 + !big_internal(keys, wake_shift, first, last, leaf, g, g == first[i]) +
+            !big_internal(keys, wake_shift, first, last, leaf, g + 1, g + 1 == last[i]);
     }
     count[i] = c;
 }
 
-__global__ void slot_fill_kernel(int64_t n, const int32_t *first, const int32_t *last, const int32_t *split,
-                                 int64_t leaf, const int64_t *slot, int64_t *lo, int64_t *hi, int64_t *left,
-                                 int64_t *right) {
+__global__ void slot_fill_kernel(int64_t n, const uint64_t *keys, int wake_shift, const int32_t *first,
+                                 const int32_t *last, const int32_t *split, int64_t leaf, const int64_t *slot,
+                                 int64_t *lo, int64_t *hi, int64_t *left, int64_t *right) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
-    if ((int64_t)(last[i] - first[i] + 1) <= leaf) return;
+    if (!big_range(keys, wake_shift, leaf, first[i], last[i])) return;
     int64_t me = slot[i], next = me + 1;
     int32_t g = split[i];
     lo[me] = first[i];
     hi[me] = (int64_t)last[i] + 1;
-    if (big_internal(first, last, leaf, g, g == first[i])) {
+    if (big_internal(keys, wake_shift, first, last, leaf, g, g == first[i])) {
         left[me] = slot[g];
     } else {
         left[me] = next;
@@ -224,7 +230,7 @@ __global__ void slot_fill_kernel(int64_t n, const int32_t *first, const int32_t 
         left[next] = right[next] = -1;
         ++next;
     }
-    if (big_internal(first, last, leaf, g + 1, g + 1 == last[i])) {
+    if (big_internal(keys, wake_shift, first, last, leaf, g + 1, g + 1 == last[i])) {
         right[me] = slot[g + 1];
     } else {
         right[me] = next;
@@ -256,6 +262,47 @@ __global__ void iota_kernel(int64_t m, int32_t *v) {
 
 static inline unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
+// Traversal tree from stably sorted keys (t->order32 holds the sorted segment ids): Karras's binary radix tree, then
+// the big internal nodes and their small children numbered by an exclusive scan.
+static int topology_from_sorted(bs_tree *t, const uint64_t *keys, int wake_shift, Scratch &scratch,
+                                cudaStream_t s) {
+    const int64_t m = t->m;
+    if ((m <= t->leaf_size && wake_shift == 0) || m == 1) {
+        t->count = 1;
+        t->lo = t->alloc<int64_t>(1, s);
+        t->hi = t->alloc<int64_t>(1, s);
+        t->left = t->alloc<int64_t>(1, s);
+        t->right = t->alloc<int64_t>(1, s);
+        if (!t->lo || !t->hi || !t->left || !t->right) return BS_ERR_OOM;
+        single_leaf_kernel<<<1, 1, 0, s>>>(m, t->lo, t->hi, t->left, t->right);
+        BS_CHECK_LAUNCH("single_leaf_kernel");
+        return BS_OK;
+    }
+    int32_t *first = scratch.get<int32_t>(m - 1), *last = scratch.get<int32_t>(m - 1);
+    int32_t *split = scratch.get<int32_t>(m - 1);
+    int64_t *slot = scratch.get<int64_t>(m - 1), *total = scratch.get<int64_t>(1);
+    if (!first || !last || !split || !slot || !total) return scratch.status;
+    karras_kernel<<<blocks_for(m - 1, 256), 256, 0, s>>>(m, keys, first, last, split);
+    slot_count_kernel<<<blocks_for(m - 1, 256), 256, 0, s>>>(m, keys, wake_shift, first, last, split, t->leaf_size,
+                                                             slot);
+    BS_CHECK_LAUNCH("karras");
+    int rc = scan_exclusive(slot, slot, m - 1, total, scratch, s);
+    if (rc != BS_OK) return rc;
+    int64_t count = 0;
+    BS_CUDA(cudaMemcpyAsync(&count, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    BS_CUDA(cudaStreamSynchronize(s));
+    t->count = count;
+    t->lo = t->alloc<int64_t>(count, s);
+    t->hi = t->alloc<int64_t>(count, s);
+    t->left = t->alloc<int64_t>(count, s);
+    t->right = t->alloc<int64_t>(count, s);
+    if (!t->lo || !t->hi || !t->left || !t->right) return BS_ERR_OOM;
+    slot_fill_kernel<<<blocks_for(m - 1, 256), 256, 0, s>>>(m, keys, wake_shift, first, last, split, t->leaf_size,
+                                                            slot, t->lo, t->hi, t->left, t->right);
+    BS_CHECK_LAUNCH("slot_fill_kernel");
+    return BS_OK;
+}
+
 static int build_morton(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_t s) {
     const int64_t m = t->m;
     unsigned long long *box = scratch.get<unsigned long long>(6);
@@ -270,40 +317,106 @@ static int build_morton(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStr
     BS_CUDA(cudaMemcpyAsync(t->keys, keys, m * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
     int rc = radix_sort(keys, t->order32, m, 0, 63, scratch, s);
     if (rc != BS_OK) return rc;
-    if (m <= t->leaf_size || m == 1) {
-        t->count = 1;
-    } else {
-        int32_t *first = scratch.get<int32_t>(m - 1), *last = scratch.get<int32_t>(m - 1);
-        int32_t *split = scratch.get<int32_t>(m - 1);
-        int64_t *slot = scratch.get<int64_t>(m - 1), *total = scratch.get<int64_t>(1);
-        if (!first || !last || !split || !slot || !total) return scratch.status;
-        karras_kernel<<<blocks_for(m - 1, 256), 256, 0, s>>>(m, keys, first, last, split);
-        slot_count_kernel<<<blocks_for(m - 1, 256), 256, 0, s>>>(m, first, last, split, t->leaf_size, slot);
-        BS_CHECK_LAUNCH("karras");
-        rc = scan_exclusive(slot, slot, m - 1, total, scratch, s);
-        if (rc != BS_OK) return rc;
-        int64_t count = 0;
-        BS_CUDA(cudaMemcpyAsync(&count, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-        BS_CUDA(cudaStreamSynchronize(s));
-        t->count = count;
-        t->lo = t->alloc<int64_t>(count, s);
-        t->hi = t->alloc<int64_t>(count, s);
-        t->left = t->alloc<int64_t>(count, s);
-        t->right = t->alloc<int64_t>(count, s);
-        if (!t->lo || !t->hi || !t->left || !t->right) return BS_ERR_OOM;
-        slot_fill_kernel<<<blocks_for(m - 1, 256), 256, 0, s>>>(m, first, last, split, t->leaf_size, slot, t->lo,
-                                                                t->hi, t->left, t->right);
-        BS_CHECK_LAUNCH("slot_fill_kernel");
+    return topology_from_sorted(t, keys, 0, scratch, s);
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Forest: many wakes in one Morton tree.  Keys carry the wake number above a per-wake Morton key (each wake quantised
+// in its own box), so the radix tree's upper splits fall exactly on wake boundaries, nodes spanning two wakes are
+// always split, and every wake's segment range is one node of the traversal tree: its root.
+// ---------------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ int wake_of(const int64_t *ptr, int nw, int64_t i) {
+    int lo = 0, hi = nw;  // largest w with ptr[w] <= i
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (ptr[mid] <= i) lo = mid; else hi = mid;
     }
-    if (t->count == 1) {
-        t->lo = t->alloc<int64_t>(1, s);
-        t->hi = t->alloc<int64_t>(1, s);
-        t->left = t->alloc<int64_t>(1, s);
-        t->right = t->alloc<int64_t>(1, s);
-        if (!t->lo || !t->hi || !t->left || !t->right) return BS_ERR_OOM;
-        single_leaf_kernel<<<1, 1, 0, s>>>(m, t->lo, t->hi, t->left, t->right);
-        BS_CHECK_LAUNCH("single_leaf_kernel");
+    return lo;
+}
+
+__global__ void forest_box_init_kernel(int nw, unsigned long long *box) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 6 * nw) box[i] = (i % 6) < 3 ? ordered_bits(INFINITY) : ordered_bits(-INFINITY);
+}
+
+__global__ void forest_box_kernel(int64_t m, const SegGeo *geo, const int64_t *wake_ptr, int nw,
+                                  unsigned long long *box) {
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= m) return;
+    const int w = wake_of(wake_ptr, nw, s);
+    double v[3];
+    midpoint(geo[s], v[0], v[1], v[2]);
+    for (int a = 0; a < 3; ++a) {
+        atomicMin(&box[6 * w + a], ordered_bits(v[a]));
+        atomicMax(&box[6 * w + 3 + a], ordered_bits(v[a]));
     }
+}
+
+__device__ __forceinline__ uint64_t spread_bits(uint32_t v, int bits) {
+    uint64_t out = 0;
+    for (int i = 0; i < bits; ++i) out |= (uint64_t)((v >> i) & 1u) << (3 * i);
+    return out;
+}
+
+__global__ void forest_keys_kernel(int64_t m, const SegGeo *geo, const int64_t *wake_ptr, int nw,
+                                   const unsigned long long *box, int bits, uint64_t *keys, int32_t *vals) {
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= m) return;
+    const int w = wake_of(wake_ptr, nw, s);
+    double lo[3], ext = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = from_ordered(box[6 * w + a]);
+        ext = fmax(ext, __dsub_rn(from_ordered(box[6 * w + 3 + a]), lo[a]));
+    }
+    const double scale = (double)(1u << bits);
+    const double inv = ext > 0.0 ? __ddiv_rn(scale, ext) : 0.0;
+    double v[3];
+    midpoint(geo[s], v[0], v[1], v[2]);
+    uint32_t q[3];
+    for (int a = 0; a < 3; ++a) {
+        uint32_t u = __double2uint_rz(__dmul_rn(__dsub_rn(v[a], lo[a]), inv));
+        q[a] = min(u, (1u << bits) - 1u);
+    }
+    keys[s] = ((uint64_t)w << (3 * bits)) | (spread_bits(q[0], bits) << 2) | (spread_bits(q[1], bits) << 1) |
+              spread_bits(q[2], bits);
+    vals[s] = (int32_t)s;
+}
+
+// The traversal node whose range is exactly a wake's segment range is that wake's root.
+__global__ void forest_roots_kernel(int64_t count, const int64_t *lo, const int64_t *hi, const int64_t *wake_ptr,
+                                    int nw, int32_t *roots) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    const int w = wake_of(wake_ptr, nw, lo[j]);
+    if (lo[j] == wake_ptr[w] && hi[j] == wake_ptr[w + 1]) roots[w] = (int32_t)j;
+}
+
+static int build_forest(bs_tree *t, const SegGeo *geo, const int64_t *wake_ptr, int nw, Scratch &scratch,
+                        cudaStream_t s) {
+    const int64_t m = t->m;
+    int wbits = 0;
+    while ((1 << wbits) < nw) ++wbits;
+    const int bits = (63 - wbits) / 3;
+    unsigned long long *box = scratch.get<unsigned long long>(6 * (size_t)nw);
+    uint64_t *keys = scratch.get<uint64_t>(m);
+    t->keys = t->alloc<uint64_t>(m, s);
+    t->order32 = t->alloc<int32_t>(m, s);
+    t->wake_root = t->alloc<int32_t>(nw, s);
+    if (!box || !keys || !t->keys || !t->order32 || !t->wake_root)
+        return scratch.status != BS_OK ? scratch.status : BS_ERR_OOM;
+    t->nwakes = nw;
+    forest_box_init_kernel<<<blocks_for(6 * (int64_t)nw, 256), 256, 0, s>>>(nw, box);
+    forest_box_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, geo, wake_ptr, nw, box);
+    forest_keys_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, geo, wake_ptr, nw, box, bits, keys, t->order32);
+    BS_CHECK_LAUNCH("forest keys");
+    BS_CUDA(cudaMemcpyAsync(t->keys, keys, m * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+    int rc = radix_sort(keys, t->order32, m, 0, 64, scratch, s);
+    if (rc != BS_OK) return rc;
+    rc = topology_from_sorted(t, keys, nw > 1 ? 3 * bits : 0, scratch, s);
+    if (rc != BS_OK) return rc;
+    BS_CUDA(cudaMemsetAsync(t->wake_root, 0xff, nw * sizeof(int32_t), s));  // -1: a wake without segments
+    forest_roots_kernel<<<blocks_for(t->count, 256), 256, 0, s>>>(t->count, t->lo, t->hi, wake_ptr, nw, t->wake_root);
+    BS_CHECK_LAUNCH("forest_roots_kernel");
     return BS_OK;
 }
 
@@ -913,6 +1026,74 @@ extern "C" int bs_tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_p
     cudaEventDestroy(e1);
     cudaEventDestroy(e2);
     return rc;
+}
+
+extern "C" int bs_forest_build(bs_ctx *ctx, const bs_sources *src, int nwakes, const int64_t *wake_ptr,
+                               const bs_tree_params *tp, bs_tree **out, bs_stream stream) {
+    if (!ctx || !tp || !out || nwakes < 1 || !wake_ptr) {
+        set_error("bs_forest_build: null argument or no wakes");
+        return BS_ERR_ARG;
+    }
+    *out = nullptr;
+    int rc = check_sources(src);
+    if (rc != BS_OK) return rc;
+    if (src->m == 0 || tp->leaf_size < 1 || nwakes > (1 << 20)) {
+        set_error("bs_forest_build: no segments, a non-positive leaf size or more than 2^20 wakes");
+        return BS_ERR_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    BS_CUDA(cudaSetDevice(ctx->device));
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&e2);
+    cudaEventRecord(e0, s);
+    bs_tree *t = new bs_tree();
+    t->device = ctx->device;
+    t->pool = ctx->pool;
+    t->kind = BS_TREE_MORTON;
+    t->m = src->m;
+    t->leaf_size = tp->leaf_size;
+    {
+        Scratch scratch(ctx->pool, s);
+        SegGeo *geo = scratch.get<SegGeo>(src->m);
+        rc = geo ? pack_segments(src, nullptr, nullptr, nullptr, geo, s) : scratch.status;
+        if (rc == BS_OK) rc = build_forest(t, geo, wake_ptr, nwakes, scratch, s);
+        if (rc == BS_OK) {
+            cudaEventRecord(e1, s);
+            rc = finish_tree(t, src, geo, scratch, s);
+        }
+        cudaEventRecord(e2, s);
+        if (rc == BS_OK) {
+            cudaError_t e = cudaEventSynchronize(e2);
+            if (e != cudaSuccess) rc = cuda_fail(e, "forest build");
+        }
+    }
+    if (rc == BS_OK) {
+        cudaEventElapsedTime(&t->build_ms, e0, e1);
+        cudaEventElapsedTime(&t->moments_ms, e1, e2);
+        ctx->stats.build_ms = t->build_ms;
+        ctx->stats.moments_ms = t->moments_ms;
+        ctx->stats.nodes = t->count;
+        ctx->stats.segments = t->m;
+        *out = t;
+    } else {
+        bs_tree_free(t);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    return rc;
+}
+
+extern "C" int bs_forest_roots(const bs_tree *t, int32_t *roots, bs_stream stream) {
+    if (!t || !t->wake_root || !roots) {
+        set_error("bs_forest_roots: not a forest");
+        return BS_ERR_ARG;
+    }
+    BS_CUDA(cudaMemcpyAsync(roots, t->wake_root, t->nwakes * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                            (cudaStream_t)stream));
+    return BS_OK;
 }
 
 __global__ void narrow_order_kernel(int64_t m, const int64_t *order, int32_t *order32) {

@@ -7,6 +7,8 @@
 // Morton key of their positions so that a warp's targets are neighbours and their node sets overlap.
 // Exclusions: the target's excluded segments as sorted tree positions (vortex_tree._positions, :571-580) and a cursor
 // that only moves forward, because depth-first visits see non-decreasing range starts.
+#include <string.h>
+
 #include <algorithm>
 
 #include "bs_sort.cuh"
@@ -53,6 +55,8 @@ struct EvalArgs {
     double *partial;     // [chunks][n][3]
     int8_t *pflag;       // [chunks][n]
     int chunks;
+    const int32_t *root_of;       // forests: root node of each (sorted) target's wake, -1 for none; null: node 0
+    unsigned long long *queue;    // work counter of the persistent list kernel
 };
 
 // Per-lane state of a target.
@@ -195,10 +199,14 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
     int2 *list = a.list + gw * LIST_CAP;
     int *cost = a.list_cost + gw * LIST_CAP;
     int len = 0, running = 0;
-    const unsigned active = __ballot_sync(0xffffffffu, t.valid);
-    if (active == 0) return;
-    if (lane == 0) stack[0] = make_int2(0, (int)active);
-    int top = 1;
+    // Roots: node 0, or in a forest the root of each lane's wake; one stack entry per distinct root.
+    const int root = a.root_of ? (t.valid ? a.root_of[gw * 32 + lane] : -1) : 0;
+    const bool live = t.valid && root >= 0;
+    const unsigned peers = __match_any_sync(0xffffffffu, live ? root : -1);
+    const bool leader = live && (__ffs(peers) - 1) == lane;
+    const unsigned leaders = __ballot_sync(0xffffffffu, leader);
+    if (leader) stack[__popc(leaders & ((1u << lane) - 1u))] = make_int2(root, (int)peers);
+    int top = __popc(leaders);
     __syncwarp();
     while (top > 0) {
         --top;
@@ -269,7 +277,7 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
         }
         __syncwarp();
     }
-    if (lane == 0) {
+    if (lane == 0 && gw * 32 < a.n) {  // warps past the last target (in the grid's last block) own no list
         a.list_len[gw] = len;
         a.list_total[gw] = running;
     }
@@ -294,17 +302,15 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
     }
 }
 
-// Phase 2: each warp takes one chunk (by cost) of the list of one warp of targets and evaluates its far nodes and
-// near leaves; partial sums per (chunk, target) are combined in chunk order by the reduce kernel.
+// Phase 2: a persistent kernel.  Work items are (warp of targets, chunk) pairs, chunk c holding the c-th slice (by
+// cost) of that warp's list; each warp of the kernel takes items from a device counter until none is left and
+// evaluates the item's far nodes and near leaves.  Partial sums per (chunk, target) are combined in chunk order by the
+// reduce kernel.
 template <int PREC, int MODEL>
-__global__ void __launch_bounds__(LIST_WARPS * 32) tree_list_kernel(EvalArgs a, int64_t target_warps) {
-    __shared__ __align__(16) unsigned char tile_mem[LIST_WARPS * 32 * sizeof(Seg64)];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t gw = (int64_t)blockIdx.x * LIST_WARPS + warp;
-    if (gw >= target_warps) return;
-    Seg64 *seg64_tile = reinterpret_cast<Seg64 *>(tile_mem) + warp * 32;
-    Seg32 *seg32_tile = reinterpret_cast<Seg32 *>(tile_mem) + warp * 32;
-    const int c = blockIdx.y, chunks = gridDim.y;
+__device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, Seg64 *seg64_tile, Seg32 *seg32_tile,
+                                          long long &near_pairs, long long &fp64_pairs) {
+    const int lane = threadIdx.x & 31;
+    const int chunks = a.chunks;
     const int len = a.list_len[gw];
     const int64_t total = a.list_total[gw];
     const int *cost = a.list_cost + gw * LIST_CAP;
@@ -324,7 +330,6 @@ __global__ void __launch_bounds__(LIST_WARPS * 32) tree_list_kernel(EvalArgs a, 
     if (t.valid && a.ex_ptr) { e = a.ex_ptr[t.p]; e1 = a.ex_ptr[t.p + 1]; }
     Acc<PREC> acc;
     int flag = BS_FLAG_OK;
-    long long near_pairs = 0, fp64_pairs = 0;
     for (int k = first; k < last; ++k) {
         const int2 entry = list[k];
         const bool mine = ((unsigned)entry.y >> lane) & 1u;
@@ -342,6 +347,24 @@ __global__ void __launch_bounds__(LIST_WARPS * 32) tree_list_kernel(EvalArgs a, 
         a.partial[3 * o + 1] = acc.y();
         a.partial[3 * o + 2] = acc.z();
         a.pflag[o] = (int8_t)flag;
+    }
+}
+
+template <int PREC, int MODEL>
+__global__ void __launch_bounds__(LIST_WARPS * 32) tree_list_kernel(EvalArgs a, int64_t target_warps) {
+    __shared__ __align__(16) unsigned char tile_mem[LIST_WARPS * 32 * sizeof(Seg64)];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    Seg64 *seg64_tile = reinterpret_cast<Seg64 *>(tile_mem) + warp * 32;
+    Seg32 *seg32_tile = reinterpret_cast<Seg32 *>(tile_mem) + warp * 32;
+    const unsigned long long items = (unsigned long long)target_warps * a.chunks;
+    long long near_pairs = 0, fp64_pairs = 0;
+    for (;;) {
+        unsigned long long item = 0;
+        if (lane == 0) item = atomicAdd(a.queue, 1ull);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= items) break;
+        list_item<PREC, MODEL>(a, (int64_t)(item / a.chunks), (int)(item % a.chunks), seg64_tile, seg32_tile,
+                               near_pairs, fp64_pairs);
     }
     for (int o = 16; o > 0; o >>= 1) {
         near_pairs += __shfl_xor_sync(0xffffffffu, near_pairs, o);
@@ -451,7 +474,7 @@ __global__ void exclusion_positions_kernel(int64_t n, const int64_t *ex_ptr, con
 static inline unsigned nblocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 template <int PREC, int MODEL>
-static void launch_pair(unsigned walk_grid, int block, size_t smem, dim3 list_grid, int64_t target_warps,
+static void launch_pair(unsigned walk_grid, int block, size_t smem, unsigned list_grid, int64_t target_warps,
                         unsigned reduce_grid, cudaStream_t s, const EvalArgs &args, double *out, int8_t *flags) {
     tree_walk_kernel<PREC, MODEL><<<walk_grid, block, smem, s>>>(args);
     tree_list_kernel<PREC, MODEL><<<list_grid, LIST_WARPS * 32, 0, s>>>(args, target_warps);
@@ -459,7 +482,7 @@ static void launch_pair(unsigned walk_grid, int block, size_t smem, dim3 list_gr
 }
 
 template <int PREC>
-static void launch_model(int model, unsigned walk_grid, int block, size_t smem, dim3 list_grid, int64_t tw,
+static void launch_model(int model, unsigned walk_grid, int block, size_t smem, unsigned list_grid, int64_t tw,
                          unsigned reduce_grid, cudaStream_t s, const EvalArgs &args, double *out, int8_t *flags) {
     switch (model) {
         case 0: launch_pair<PREC, 0>(walk_grid, block, smem, list_grid, tw, reduce_grid, s, args, out, flags); break;
@@ -472,7 +495,7 @@ static void launch_model(int model, unsigned walk_grid, int block, size_t smem, 
 }
 
 // FP64 evaluates the core model at run time (one instantiation); the single precisions are specialised per model.
-static void launch_eval(int precision, int model, unsigned walk_grid, int block, size_t smem, dim3 list_grid,
+static void launch_eval(int precision, int model, unsigned walk_grid, int block, size_t smem, unsigned list_grid,
                         int64_t tw, unsigned reduce_grid, cudaStream_t s, const EvalArgs &args, double *out,
                         int8_t *flags) {
     if (precision == BS_FP64) launch_pair<0, 0>(walk_grid, block, smem, list_grid, tw, reduce_grid, s, args, out, flags);
@@ -491,42 +514,125 @@ int target_order(int64_t n, const double *points, int32_t *perm, Scratch &scratc
     return radix_sort(keys, perm, n, 0, 63, scratch, s);
 }
 
+// Forest targets: sorted by (wake, Morton key in the wake's own target box); each sorted target learns its root.
+__device__ __forceinline__ int target_wake(const int64_t *ptr, int nw, int64_t i) {
+    int lo = 0, hi = nw;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (ptr[mid] <= i) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ unsigned long long ordered64(double x) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(x + 0.0);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+__global__ void forest_target_box_kernel(int64_t n, const double *points, const int64_t *ptr, int nw,
+                                         unsigned long long *box) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int w = target_wake(ptr, nw, p);
+    for (int a = 0; a < 3; ++a) {
+        atomicMin(&box[6 * w + a], ordered64(points[3 * p + a]));
+        atomicMax(&box[6 * w + 3 + a], ordered64(points[3 * p + a]));
+    }
+}
+
+__global__ void forest_target_box_init_kernel(int nw, unsigned long long *box) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 6 * nw) box[i] = (i % 6) < 3 ? ordered64(INFINITY) : ordered64(-INFINITY);
+}
+
+__global__ void forest_target_keys_kernel(int64_t n, const double *points, const int64_t *ptr, int nw,
+                                          const unsigned long long *box, int bits, uint64_t *keys, int32_t *vals) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int w = target_wake(ptr, nw, p);
+    double ext = 0.0, lo[3];
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = unordered(box[6 * w + a]);
+        ext = fmax(ext, unordered(box[6 * w + 3 + a]) - lo[a]);
+    }
+    const double inv = ext > 0.0 ? (double)(1u << bits) / ext : 0.0;
+    uint64_t key = 0;
+    for (int a = 0; a < 3; ++a) {
+        uint32_t q = min((1u << bits) - 1u, (uint32_t)((points[3 * p + a] - lo[a]) * inv));
+        for (int b = 0; b < bits; ++b) key |= (uint64_t)((q >> b) & 1u) << (3 * b + 2 - a);
+    }
+    keys[p] = ((uint64_t)w << (3 * bits)) | key;
+    vals[p] = (int32_t)p;
+}
+
+__global__ void forest_roots_of_kernel(int64_t n, const int32_t *perm, const int64_t *ptr, int nw,
+                                       const int32_t *wake_root, int32_t *root_of) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    root_of[i] = wake_root[target_wake(ptr, nw, perm[i])];
+}
+
 }  // namespace bs
 
 using namespace bs;
 
-extern "C" int bs_tree_eval(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const bs_targets *tgt,
-                            const bs_kernel_params *kp, double *out, int8_t *flags, int64_t *far_counts,
-                            bs_stream stream) {
+namespace {
+
+int check_eval_args(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const bs_targets *tgt,
+                    const bs_kernel_params *kp, const double *out, const int8_t *flags) {
     if (!ctx || !tree || !tp || !tgt || !kp || (tgt->n > 0 && (!tgt->points || !out || !flags))) {
-        set_error("bs_tree_eval: null argument");
+        set_error("tree evaluation: null argument");
         return BS_ERR_ARG;
     }
     if (!(tp->theta > 0.0 && tp->theta < 1.0) || tp->order < 0 || tp->order > 2 || !(tp->clearance >= 0.0)) {
-        set_error("bs_tree_eval: theta must lie in (0, 1), order in 0..2, clearance >= 0");
+        set_error("tree evaluation: theta must lie in (0, 1), order in 0..2, clearance >= 0");
         return BS_ERR_ARG;
     }
     if (kp->model < 0 || kp->model > 5 || kp->precision < 0 || kp->precision > 2 ||
         (kp->block != 32 && kp->block != 64 && kp->block != 128 && kp->block != 256)) {
-        set_error("bs_tree_eval: model 0..5, precision 0..2, block 32/64/128/256");
+        set_error("tree evaluation: model 0..5, precision 0..2, block 32/64/128/256");
         return BS_ERR_ARG;
     }
     if (tgt->n >= (int64_t(1) << 31)) {
-        set_error("bs_tree_eval: at most 2^31 - 1 targets");
+        set_error("tree evaluation: at most 2^31 - 1 targets");
         return BS_ERR_ARG;
     }
-    if (tgt->n == 0) return BS_OK;
-    cudaStream_t s = (cudaStream_t)stream;
-    BS_CUDA(cudaSetDevice(ctx->device));
-    Scratch scratch(ctx->pool, s);
+    return BS_OK;
+}
+
+// Everything the evaluation launches, on stream s, with scratch from `scratch` (pool or arena).  No host
+// synchronisation: the counters and the overflow flag stay in `state` (device, 6 words: overflow + 5 counters).
+int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const bs_targets *tgt,
+                 const int64_t *target_wake_ptr, int nw, const bs_kernel_params *kp, double *out, int8_t *flags,
+                 int64_t *far_counts, unsigned long long *state, Scratch &scratch, cudaStream_t s) {
     const int64_t n = tgt->n;
     int32_t *perm = scratch.get<int32_t>(n);
-    int *overflow = scratch.get<int>(1);
-    unsigned long long *counters = scratch.get<unsigned long long>(5);
-    int32_t *ex_pos = nullptr;
-    if (!perm || !overflow || !counters) return scratch.status;
-    int rc = target_order(n, tgt->points, perm, scratch, s);
-    if (rc != BS_OK) return rc;
+    unsigned long long *queue = scratch.get<unsigned long long>(1);
+    int32_t *ex_pos = nullptr, *root_of = nullptr;
+    if (!perm || !queue) return scratch.status;
+    int rc;
+    if (target_wake_ptr) {
+        int wbits = 0;
+        while ((1 << wbits) < nw) ++wbits;
+        const int bits = (63 - wbits) / 3;
+        unsigned long long *box = scratch.get<unsigned long long>(6 * (size_t)nw);
+        uint64_t *keys = scratch.get<uint64_t>(n);
+        root_of = scratch.get<int32_t>(n);
+        if (!box || !keys || !root_of) return scratch.status;
+        forest_target_box_init_kernel<<<nblocks(6 * (int64_t)nw, 256), 256, 0, s>>>(nw, box);
+        forest_target_box_kernel<<<nblocks(n, 256), 256, 0, s>>>(n, tgt->points, target_wake_ptr, nw, box);
+        forest_target_keys_kernel<<<nblocks(n, 256), 256, 0, s>>>(n, tgt->points, target_wake_ptr, nw, box, bits,
+                                                                  keys, perm);
+        BS_CHECK_LAUNCH("forest target keys");
+        rc = radix_sort(keys, perm, n, 0, 64, scratch, s);
+        if (rc != BS_OK) return rc;
+        forest_roots_of_kernel<<<nblocks(n, 256), 256, 0, s>>>(n, perm, target_wake_ptr, nw, tree->wake_root,
+                                                               root_of);
+        BS_CHECK_LAUNCH("forest_roots_of_kernel");
+    } else {
+        rc = target_order(n, tgt->points, perm, scratch, s);
+        if (rc != BS_OK) return rc;
+    }
     if (tgt->ex_ptr && tgt->e > 0) {
         ex_pos = scratch.get<int32_t>(tgt->e);
         if (!ex_pos) return scratch.status;
@@ -534,8 +640,8 @@ extern "C" int bs_tree_eval(bs_ctx *ctx, const bs_tree *tree, const bs_tree_para
                                                                     ex_pos);
         BS_CHECK_LAUNCH("exclusion_positions_kernel");
     }
-    BS_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int), s));
-    BS_CUDA(cudaMemsetAsync(counters, 0, 5 * sizeof(unsigned long long), s));
+    BS_CUDA(cudaMemsetAsync(state, 0, 6 * sizeof(unsigned long long), s));
+    BS_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s));
     const int block = std::min(kp->block, 128);
     const int64_t target_warps = (n + 31) / 32;
     const int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(64, ((int64_t)ctx->sm_count * 32 + target_warps - 1)
@@ -569,48 +675,197 @@ extern "C" int bs_tree_eval(bs_ctx *ctx, const bs_tree *tree, const bs_tree_para
     args.walk_u = walk_u;
     args.walk_flag = walk_flag;
     args.far_counts = far_counts;
-    args.overflow = overflow;
-    args.counters = counters;
+    args.overflow = reinterpret_cast<int *>(state);
+    args.counters = state + 1;
     args.partial = partial;
     args.pflag = pflag;
     args.chunks = chunks;
+    args.root_of = root_of;
+    args.queue = queue;
     const size_t smem = (size_t)(block / 32) * (STACK_DEPTH * sizeof(int2) + 32 * sizeof(Seg64));
     const unsigned walk_grid = (unsigned)((target_warps + block / 32 - 1) / (block / 32));
-    const dim3 list_grid((unsigned)((target_warps + LIST_WARPS - 1) / LIST_WARPS), (unsigned)chunks);
+    const int64_t items = target_warps * chunks;
+    const unsigned list_grid = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>((items + LIST_WARPS - 1) / LIST_WARPS, (int64_t)ctx->sm_count * 4));
+    launch_eval(kp->precision, kp->model, walk_grid, block, smem, list_grid, target_warps, nblocks(n, 256), s, args,
+                out, flags);
+    BS_CHECK_LAUNCH("tree evaluation");
+    return BS_OK;
+}
+
+// Runs the evaluation, waits for it and reads counters and the overflow flag into the context's statistics.
+int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const bs_targets *tgt,
+             const int64_t *target_wake_ptr, int nw, const bs_kernel_params *kp, double *out, int8_t *flags,
+             int64_t *far_counts, cudaStream_t s) {
+    Scratch scratch(ctx->pool, s);
+    unsigned long long *state = scratch.get<unsigned long long>(6);
+    if (!state) return scratch.status;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s);
-    launch_eval(kp->precision, kp->model, walk_grid, block, smem, list_grid, target_warps, nblocks(n, 256), s, args,
-                out, flags);
-    cudaError_t le = cudaGetLastError();
+    int rc = eval_enqueue(ctx, tree, tp, tgt, target_wake_ptr, nw, kp, out, flags, far_counts, state, scratch, s);
     cudaEventRecord(e1, s);
-    int host_overflow = 0;
-    unsigned long long host_counters[5] = {0, 0, 0, 0, 0};
-    if (le == cudaSuccess) le = cudaMemcpyAsync(&host_overflow, overflow, sizeof(int), cudaMemcpyDeviceToHost, s);
-    if (le == cudaSuccess)
-        le = cudaMemcpyAsync(host_counters, counters, sizeof host_counters, cudaMemcpyDeviceToHost, s);
+    unsigned long long host[6] = {0, 0, 0, 0, 0, 0};
+    cudaError_t le = cudaSuccess;
+    if (rc == BS_OK) le = cudaMemcpyAsync(host, state, sizeof host, cudaMemcpyDeviceToHost, s);
     if (le == cudaSuccess) le = cudaStreamSynchronize(s);
     float ms = 0.f;
-    if (le == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    if (rc == BS_OK && le == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (le != cudaSuccess) return cuda_fail(le, "tree_eval_kernel");
-    ctx->stats.points = n;
+    if (rc != BS_OK) return rc;
+    if (le != cudaSuccess) return cuda_fail(le, "tree evaluation");
+    ctx->stats.points = tgt->n;
     ctx->stats.segments = tree->m;
     ctx->stats.nodes = tree->count;
     ctx->stats.launches = 3;
-    ctx->stats.far_evaluations = (int64_t)host_counters[0];
-    ctx->stats.near_pairs = (int64_t)host_counters[1];
-    ctx->stats.fp64_pairs = (int64_t)host_counters[2];
-    ctx->stats.visits = (int64_t)host_counters[3];
-    ctx->stats.pair_slots = (int64_t)host_counters[4];
+    ctx->stats.far_evaluations = (int64_t)host[1];
+    ctx->stats.near_pairs = (int64_t)host[2];
+    ctx->stats.fp64_pairs = (int64_t)host[3];
+    ctx->stats.visits = (int64_t)host[4];
+    ctx->stats.pair_slots = (int64_t)host[5];
     ctx->stats.evaluate_ms = ms;
-    if (host_overflow) {
-        set_error("tree traversal stack overflow on the GPU (depth %d)", args.stack_limit);
+    if (host[0] & 0xffffffffull) {
+        set_error("tree traversal stack overflow on the GPU (depth %d)",
+                  (tp->stack_limit > 0 && tp->stack_limit < STACK_DEPTH) ? tp->stack_limit : STACK_DEPTH);
         return BS_ERR_STACK;
     }
     return BS_OK;
+}
+
+}  // namespace
+
+extern "C" int bs_tree_eval(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const bs_targets *tgt,
+                            const bs_kernel_params *kp, double *out, int8_t *flags, int64_t *far_counts,
+                            bs_stream stream) {
+    int rc = check_eval_args(ctx, tree, tp, tgt, kp, out, flags);
+    if (rc != BS_OK || tgt->n == 0) return rc;
+    BS_CUDA(cudaSetDevice(ctx->device));
+    return eval_run(ctx, tree, tp, tgt, nullptr, 1, kp, out, flags, far_counts, (cudaStream_t)stream);
+}
+
+extern "C" int bs_forest_eval(bs_ctx *ctx, const bs_tree *forest, const bs_tree_params *tp, const bs_targets *tgt,
+                              const int64_t *target_wake_ptr, const bs_kernel_params *kp, double *out, int8_t *flags,
+                              int64_t *far_counts, bs_stream stream) {
+    int rc = check_eval_args(ctx, forest, tp, tgt, kp, out, flags);
+    if (rc != BS_OK || tgt->n == 0) return rc;
+    if (!forest->wake_root || !target_wake_ptr) {
+        set_error("bs_forest_eval: not a forest, or no target ranges");
+        return BS_ERR_ARG;
+    }
+    BS_CUDA(cudaSetDevice(ctx->device));
+    return eval_run(ctx, forest, tp, tgt, target_wake_ptr, forest->nwakes, kp, out, flags, far_counts,
+                    (cudaStream_t)stream);
+}
+
+struct bs_graph {
+    int device;
+    cudaGraphExec_t exec = nullptr;
+    void *arena = nullptr;
+    unsigned long long *state = nullptr;
+};
+
+extern "C" int bs_forest_graph(bs_ctx *ctx, const bs_tree *forest, const bs_tree_params *tp, const bs_targets *tgt,
+                               const int64_t *target_wake_ptr, const bs_kernel_params *kp, double *out,
+                               int8_t *flags, int64_t *far_counts, bs_graph **graph) {
+    if (!graph) {
+        set_error("bs_forest_graph: null output");
+        return BS_ERR_ARG;
+    }
+    *graph = nullptr;
+    int rc = check_eval_args(ctx, forest, tp, tgt, kp, out, flags);
+    if (rc != BS_OK) return rc;
+    if (tgt->n == 0 || (target_wake_ptr && !forest->wake_root)) {
+        set_error("bs_forest_graph: no targets, or target ranges for a tree that is not a forest");
+        return BS_ERR_ARG;
+    }
+    BS_CUDA(cudaSetDevice(ctx->device));
+    const int nw = target_wake_ptr ? forest->nwakes : 1;
+    cudaStream_t s = nullptr;
+    BS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    // 1. an ordinary run sizes the arena (and checks that the evaluation succeeds)
+    size_t need = 0;
+    {
+        Scratch probe(ctx->pool, s);
+        unsigned long long *state = probe.get<unsigned long long>(6);
+        rc = state ? eval_enqueue(ctx, forest, tp, tgt, target_wake_ptr, nw, kp, out, flags, far_counts, state, probe,
+                                  s)
+                   : probe.status;
+        need = probe.requested;
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (rc == BS_OK && e != cudaSuccess) rc = cuda_fail(e, "bs_forest_graph sizing run");
+    }
+    bs_graph *g = new bs_graph();
+    g->device = ctx->device;
+    cudaError_t e = rc == BS_OK ? cudaMalloc(&g->arena, need + 4096) : cudaSuccess;
+    if (rc == BS_OK && e == cudaSuccess) e = cudaMalloc((void **)&g->state, 6 * sizeof(unsigned long long));
+    if (rc == BS_OK && e != cudaSuccess) rc = cuda_fail(e, "bs_forest_graph buffers");
+    // 2. capture the same launches with scratch carved from the arena
+    cudaGraph_t cg = nullptr;
+    if (rc == BS_OK) {
+        e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamBeginCapture");
+    }
+    if (rc == BS_OK) {
+        Scratch arena(g->arena, need + 4096, s);
+        int rc2 = eval_enqueue(ctx, forest, tp, tgt, target_wake_ptr, nw, kp, out, flags, far_counts, g->state,
+                               arena, s);
+        e = cudaStreamEndCapture(s, &cg);
+        if (rc2 != BS_OK) rc = rc2;
+        else if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamEndCapture");
+    }
+    if (rc == BS_OK) {
+        e = cudaGraphInstantiate(&g->exec, cg, 0);
+        if (e != cudaSuccess) rc = cuda_fail(e, "cudaGraphInstantiate");
+    }
+    if (cg) cudaGraphDestroy(cg);
+    cudaStreamDestroy(s);
+    if (rc != BS_OK) {
+        bs_graph_free(g);
+        return rc;
+    }
+    *graph = g;
+    return BS_OK;
+}
+
+extern "C" int bs_graph_launch(bs_graph *g, bs_stream stream) {
+    if (!g || !g->exec) {
+        set_error("bs_graph_launch: null graph");
+        return BS_ERR_ARG;
+    }
+    BS_CUDA(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+    return BS_OK;
+}
+
+extern "C" int bs_graph_status(bs_graph *g, bs_stats *stats) {
+    if (!g || !stats) {
+        set_error("bs_graph_status: null argument");
+        return BS_ERR_ARG;
+    }
+    unsigned long long host[6];
+    BS_CUDA(cudaMemcpy(host, g->state, sizeof host, cudaMemcpyDeviceToHost));
+    memset(stats, 0, sizeof *stats);
+    stats->far_evaluations = (int64_t)host[1];
+    stats->near_pairs = (int64_t)host[2];
+    stats->fp64_pairs = (int64_t)host[3];
+    stats->visits = (int64_t)host[4];
+    stats->pair_slots = (int64_t)host[5];
+    if (host[0] & 0xffffffffull) {
+        set_error("tree traversal stack overflow on the GPU");
+        return BS_ERR_STACK;
+    }
+    return BS_OK;
+}
+
+extern "C" void bs_graph_free(bs_graph *g) {
+    if (!g) return;
+    cudaSetDevice(g->device);
+    cudaDeviceSynchronize();
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->arena) cudaFree(g->arena);
+    if (g->state) cudaFree(g->state);
+    delete g;
 }
 
 extern "C" int bs_tree_sum(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, const bs_targets *tgt,

@@ -203,3 +203,83 @@ def tree_sum(sources, targets, model, singularity="raise", precision="mixed", bl
 def last_stats(device=0):
     """Counters and device times of the last call on `device` (bs_last_stats)."""
     return L.stats(device)
+
+
+# ---------------------------------------------------------------------------------------------------------------------
+# Forests: many wakes in one tree (batched evaluation).
+# ---------------------------------------------------------------------------------------------------------------------
+def build_forest(sources, wake_ptr, leaf_size=32):
+    """One Morton tree over concatenated wakes; wake w owns segments [wake_ptr[w], wake_ptr[w+1])."""
+    dev = sources.device
+    ptr = i64(wake_ptr, dev)
+    params = tree_params(0.5, 2, leaf_size, 3.0, "morton")
+    handle = ctypes.c_void_p()
+    src = sources.struct()
+    L.check(L.library().bs_forest_build(L.context(dev.index), ctypes.byref(src), int(ptr.numel() - 1), _ptr(ptr),
+                                        ctypes.byref(params), ctypes.byref(handle), _stream(dev)), "bs_forest_build")
+    tree = Tree(handle, sources, params)
+    tree.wake_ptr = ptr
+    tree.nwakes = int(ptr.numel() - 1)
+    return tree
+
+
+def forest_roots(tree):
+    roots = torch.empty(tree.nwakes, dtype=torch.int32, device=tree.sources.device)
+    L.check(L.library().bs_forest_roots(tree.handle, _ptr(roots), _stream(tree.sources.device)), "bs_forest_roots")
+    return roots.cpu().numpy()
+
+
+def forest_eval(tree, targets, target_wake_ptr, model, singularity="raise", precision="mixed", block=128, near=3.0,
+                theta=0.5, order=2, clearance=3.0, stack_limit=0, far_counts=True):
+    """Evaluate every wake of a forest at its own targets (targets of wake w: [target_wake_ptr[w], ...[w+1]))."""
+    dev = tree.sources.device
+    ptr = i64(target_wake_ptr, dev)
+    out = torch.empty((targets.n, 3), dtype=torch.float64, device=dev)
+    flags = torch.empty(targets.n, dtype=torch.int8, device=dev)
+    far = torch.empty(targets.n, dtype=torch.int64, device=dev) if far_counts else None
+    tp = tree_params(theta, order, tree.params.leaf_size, clearance, "morton", stack_limit)
+    kp = kernel_params(model, singularity, precision, block, near)
+    tgt = targets.struct()
+    L.check(L.library().bs_forest_eval(L.context(dev.index), tree.handle, ctypes.byref(tp), ctypes.byref(tgt),
+                                       _ptr(ptr), ctypes.byref(kp), _ptr(out), _ptr(flags), _ptr(far), _stream(dev)),
+            "bs_forest_eval")
+    return out, flags, far
+
+
+class Graph:
+    """A captured forest (or tree) evaluation; ``launch()`` replays it on the current stream."""
+
+    def __init__(self, tree, targets, target_wake_ptr, model, singularity="raise", precision="mixed", block=128,
+                 near=3.0, theta=0.5, order=2, clearance=3.0):
+        dev = tree.sources.device
+        self.tree, self.targets, self.device = tree, targets, dev
+        self.ptr = None if target_wake_ptr is None else i64(target_wake_ptr, dev)
+        self.out = torch.empty((targets.n, 3), dtype=torch.float64, device=dev)
+        self.flags = torch.empty(targets.n, dtype=torch.int8, device=dev)
+        self.far = torch.empty(targets.n, dtype=torch.int64, device=dev)
+        tp = tree_params(theta, order, tree.params.leaf_size, clearance, "morton")
+        kp = kernel_params(model, singularity, precision, block, near)
+        tgt = targets.struct()
+        handle = ctypes.c_void_p()
+        torch.cuda.current_stream(dev).synchronize()
+        L.check(L.library().bs_forest_graph(L.context(dev.index), tree.handle, ctypes.byref(tp), ctypes.byref(tgt),
+                                            _ptr(self.ptr), ctypes.byref(kp), _ptr(self.out), _ptr(self.flags),
+                                            _ptr(self.far), ctypes.byref(handle)), "bs_forest_graph")
+        self._handle = handle
+
+    def launch(self):
+        L.check(L.library().bs_graph_launch(self._handle, _stream(self.device)), "bs_graph_launch")
+        return self.out, self.flags, self.far
+
+    def status(self):
+        s = L.Stats()
+        L.check(L.library().bs_graph_status(self._handle, ctypes.byref(s)), "bs_graph_status")
+        return s.as_dict()
+
+    def __del__(self):
+        handle, self._handle = getattr(self, "_handle", None), None
+        if handle:
+            try:
+                L.library().bs_graph_free(handle)
+            except Exception:  # noqa: BLE001 - interpreter shutdown
+                pass
