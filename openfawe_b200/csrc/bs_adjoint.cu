@@ -9,35 +9,42 @@
 // differentiation of that expression by hand.  Pairs on a segment's axis (the reference's roundoff guard) contribute
 // nothing, as in the forward sum.
 //
-// Two kernels, each deterministic: target-major (thread per target, segments streamed through shared memory) for the
-// target gradients, segment-major (thread per segment, targets streamed) for the endpoint and circulation gradients.
-// Both are split into chunks along their inner loop and the chunk partials are added in chunk order.
+// One pass evaluates each pair's adjoint once (adjoint_fused_kernel): blocks tile the (target x segment) plane, target
+// gradients add up over a block's segments, segment gradients over its targets, and a reduce kernel adds the block
+// partials in chunk order.  Deterministic.
 #include <algorithm>
 
 #include "bs_internal.cuh"
 
 namespace bs {
 
+// A segment as the adjoint reads it: endpoints, circulation and the per-segment invariants of the pair.
 struct AdjSeg {
-    double ax, ay, az, bx, by, bz, gamma, radius;
+    double ax, ay, az, bx, by, bz, gamma;
+    double irc2L2;  // 1 / (L^2 rc^2) for a cored model with rc > 0, else 0 (no core factor)
+    double invL2;   // 1 / L^2
+    double pad;
 };
 struct AdjTgt {
     double x, y, z, wx, wy, wz;
 };
 
-// Adds d(w . u)/dx, d/dA, d/dB, d/dGamma of one pair.
-__device__ __forceinline__ void pair_vjp64(double x0, double x1, double x2, const AdjSeg &s, int model, double w0,
-                                           double w1, double w2, double *gx, double *ga, double *gb, double &gg) {
+static constexpr double AXIS_EPS64_SQ = AXIS_EPS64 * AXIS_EPS64;
+
+// d(w . u)/dr1 and d(w . u)/dr2 of one pair (r1 = x - A, r2 = x - B) and d(w . u)/dGamma; false for a pair that
+// contributes nothing (the roundoff axis guard).  Then d/dx = g1 + g2, d/dA = -g1, d/dB = -g2.
+__device__ __forceinline__ bool pair_vjp64(double x0, double x1, double x2, const AdjSeg &s, int model, double w0,
+                                           double w1, double w2, double *g1, double *g2, double &gg) {
     const double r10 = x0 - s.ax, r11 = x1 - s.ay, r12 = x2 - s.az;
     const double r20 = x0 - s.bx, r21 = x1 - s.by, r22 = x2 - s.bz;
-    const double l0 = s.bx - s.ax, l1 = s.by - s.ay, l2 = s.bz - s.az;
-    const double L2 = l0 * l0 + l1 * l1 + l2 * l2;
-    const double L = sqrt(L2);
     const double c0 = r11 * r22 - r12 * r21, c1 = r12 * r20 - r10 * r22, c2v = r10 * r21 - r11 * r20;
     const double cc = c0 * c0 + c1 * c1 + c2v * c2v;
-    const double n1 = sqrt(r10 * r10 + r11 * r11 + r12 * r12), n2 = sqrt(r20 * r20 + r21 * r21 + r22 * r22);
-    // the reference's roundoff axis guard, in its scaled units (h = |c|/L^2, na = n1/L, nb = n2/L)
-    if (sqrt(cc) / L2 <= AXIS_EPS64 * fmax(1.0, fmax(n1, n2) / L)) return;
+    const double q1 = r10 * r10 + r11 * r11 + r12 * r12, q2 = r20 * r20 + r21 * r21 + r22 * r22;
+    // the reference's roundoff axis guard h <= eps max(1, na, nb) in its scaled units (h = |c|/L^2,
+    // na = |r1|/L, nb = |r2|/L), squared
+    if (cc * s.invL2 * s.invL2 <= AXIS_EPS64_SQ * fmax(1.0, fmax(q1, q2) * s.invL2)) return false;
+    const double in1 = rsqrt(q1), in2 = rsqrt(q2);
+    const double n1 = q1 * in1, n2 = q2 * in2;
     const double d = r10 * r20 + r11 * r21 + r12 * r22;
     const double P = n1 * n2;
     double D, dD_dP, dD_dd, dD_dcc;
@@ -46,58 +53,50 @@ __device__ __forceinline__ void pair_vjp64(double x0, double x1, double x2, cons
         dD_dP = 2.0 * P + d;
         dD_dd = P;
         dD_dcc = 0.0;
-    } else {
-        const double q = P - d, iq = 1.0 / q;
+    } else {  // the rationalised denominator P (P + d) = P |c|^2 / (P - d)
+        const double iq = 1.0 / (P - d);
         D = P * cc * iq;
         dD_dP = -cc * d * iq * iq;
         dD_dd = P * cc * iq * iq;
         dD_dcc = P * iq;
     }
-    double f = 1.0, df = 0.0, irc2L2 = 0.0;  // f(rho2), df/drho2, 1/(L2 rc^2)
-    if (s.radius > 0.0 && model != 0) {
-        irc2L2 = 1.0 / (L2 * s.radius * s.radius);
-        const double rho2 = cc * irc2L2;
+    double f = 1.0, df = 0.0, rho2 = 0.0;  // core factor f(rho2), df/drho2 with rho2 = |c|^2 / (L^2 rc^2)
+    if (s.irc2L2 > 0.0) {
+        rho2 = cc * s.irc2L2;
         if (model == 1) {
             if (rho2 < 1.0) { f = rho2; df = 1.0; }
-        } else if (model == 2) {
-            if (rho2 <= LAMB_CUT2) {
-                const double e = exp(-LAMB_A * rho2);
-                f = -expm1(-LAMB_A * rho2);
-                df = LAMB_A * e;
-            }
+        } else if (rho2 <= LAMB_CUT2) {
+            const double em1 = expm1(-LAMB_A * rho2);
+            f = -em1;
+            df = LAMB_A * (1.0 + em1);
         }
     }
     const double S = n1 + n2;
     const double iD = 1.0 / D;
     const double coefG = INV_FOUR_PI * f * S * iD;  // u = Gamma * coefG * c
     const double wc = w0 * c0 + w1 * c1 + w2 * c2v;
-    gg += coefG * wc;
+    gg = coefG * wc;
     const double G = s.gamma;
-    const double gcoef = G * wc;
-    const double g_f = gcoef * INV_FOUR_PI * S * iD;
-    const double g_S = gcoef * INV_FOUR_PI * f * iD;
-    const double g_D = -gcoef * INV_FOUR_PI * f * S * iD * iD;
+    const double h = G * wc * INV_FOUR_PI * iD;  // common factor of the scalar adjoints
+    const double g_f = h * S;
+    const double g_S = h * f;
+    const double g_D = -h * f * S * iD;
     const double g_rho2 = g_f * df;
-    const double g_cc = g_rho2 * irc2L2 + g_D * dD_dcc;
-    const double g_L2 = -g_rho2 * cc * irc2L2 / L2;
+    const double g_cc = g_rho2 * s.irc2L2 + g_D * dD_dcc;
+    const double g_L2 = -g_rho2 * rho2 * s.invL2;
     const double g_P = g_D * dD_dP, g_d = g_D * dD_dd;
-    const double g_n1 = g_S + g_P * n2, g_n2 = g_S + g_P * n1;
     const double k = G * coefG;
     const double gc0 = k * w0 + 2.0 * c0 * g_cc, gc1 = k * w1 + 2.0 * c1 * g_cc, gc2 = k * w2 + 2.0 * c2v * g_cc;
-    // c = r1 x r2: dL/dr1 += r2 x g_c, dL/dr2 += g_c x r1
-    const double a1 = g_n1 / n1, a2 = g_n2 / n2, b = 2.0 * g_L2;
-    const double g10 = a1 * r10 + g_d * r20 + (r21 * gc2 - r22 * gc1) + b * l0;
-    const double g11 = a1 * r11 + g_d * r21 + (r22 * gc0 - r20 * gc2) + b * l1;
-    const double g12 = a1 * r12 + g_d * r22 + (r20 * gc1 - r21 * gc0) + b * l2;
-    const double g20 = a2 * r20 + g_d * r10 + (gc1 * r12 - gc2 * r11) - b * l0;
-    const double g21 = a2 * r21 + g_d * r11 + (gc2 * r10 - gc0 * r12) - b * l1;
-    const double g22 = a2 * r22 + g_d * r12 + (gc0 * r11 - gc1 * r10) - b * l2;
-    // L2 = |B - A|^2 = |r1 - r2|^2 with r1 - r2 = l: dL2/dr1 = 2 l, dL2/dr2 = -2 l (folded in above)
-    gx[0] += g10 + g20;
-    gx[1] += g11 + g21;
-    gx[2] += g12 + g22;
-    ga[0] -= g10; ga[1] -= g11; ga[2] -= g12;
-    gb[0] -= g20; gb[1] -= g21; gb[2] -= g22;
+    // c = r1 x r2: dL/dr1 += r2 x g_c, dL/dr2 += g_c x r1; |B - A|^2 = |r1 - r2|^2: dL2/dr1 = 2 l = -dL2/dr2
+    const double a1 = (g_S + g_P * n2) * in1, a2 = (g_S + g_P * n1) * in2, b = 2.0 * g_L2;
+    const double l0 = s.bx - s.ax, l1 = s.by - s.ay, l2 = s.bz - s.az;
+    g1[0] = a1 * r10 + g_d * r20 + (r21 * gc2 - r22 * gc1) + b * l0;
+    g1[1] = a1 * r11 + g_d * r21 + (r22 * gc0 - r20 * gc2) + b * l1;
+    g1[2] = a1 * r12 + g_d * r22 + (r20 * gc1 - r21 * gc0) + b * l2;
+    g2[0] = a2 * r20 + g_d * r10 + (gc1 * r12 - gc2 * r11) - b * l0;
+    g2[1] = a2 * r21 + g_d * r11 + (gc2 * r10 - gc0 * r12) - b * l1;
+    g2[2] = a2 * r22 + g_d * r12 + (gc0 * r11 - gc1 * r10) - b * l2;
+    return true;
 }
 
 __device__ __forceinline__ bool excluded(const int64_t *ex_ptr, const int64_t *ex_seg, int64_t p, int64_t s) {
@@ -107,80 +106,102 @@ __device__ __forceinline__ bool excluded(const int64_t *ex_ptr, const int64_t *e
     return false;
 }
 
-constexpr int ADJ_TILE = 128;
+constexpr int ADJ_WARPS = 8;
+constexpr int ADJ_THREADS = ADJ_WARPS * 32;
+constexpr int ADJ_MAX_TCHUNK = 1024;  // targets per block: their gradients live in shared memory
 
 struct AdjArgs {
-    int64_t n, m, chunk;
+    int64_t n, m, tchunk, schunk;
     const AdjTgt *tgt;
     const AdjSeg *seg;
     const int64_t *ex_ptr, *ex_seg;
     int model;
-    double *part_x;    // [chunks][n][3]
-    double *part_seg;  // [chunks][m][7]: gA, gB, gGamma
+    double *part_x;    // [segment chunks][n][3]
+    double *part_seg;  // [target chunks][m][7]: gA, gB, gGamma
 };
 
-__global__ void __launch_bounds__(ADJ_TILE) adjoint_target_kernel(AdjArgs a) {
-    __shared__ AdjSeg tile[ADJ_TILE];
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = p < a.n;
-    const int64_t s0 = (int64_t)blockIdx.y * a.chunk, s1 = min(a.m, s0 + a.chunk);
-    AdjTgt t = valid ? a.tgt[p] : AdjTgt{0, 0, 0, 0, 0, 0};
-    double gx[3] = {0, 0, 0}, ga[3] = {0, 0, 0}, gb[3] = {0, 0, 0}, gg = 0.0;
-    for (int64_t base = s0; base < s1; base += ADJ_TILE) {
-        const int cnt = (int)min((int64_t)ADJ_TILE, s1 - base);
+// One pass over the (target chunk x segment chunk) block of pairs computing every gradient.  Each lane owns one target
+// of its warp's current group of 32 and, for the current tile of 32 segments, the accumulators of one segment: at step
+// j lane l evaluates segment (l + j) mod 32 and hands that pair's segment adjoint to the segment's owner lane with
+// shuffles, so no two lanes write one accumulator and no atomics are needed.  Target gradients accumulate in shared
+// memory (a warp owns its groups' slots); segment accumulators of the warps are added in warp order at the end of each
+// tile.  Every sum runs in a fixed order, so the result is deterministic.
+__global__ void __launch_bounds__(ADJ_THREADS) adjoint_fused_kernel(AdjArgs a) {
+    __shared__ double gx_acc[ADJ_MAX_TCHUNK * 3];
+    __shared__ AdjSeg tile[32];
+    __shared__ double red[ADJ_WARPS][7][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t t0 = (int64_t)blockIdx.x * a.tchunk, t1 = min(a.n, t0 + a.tchunk);
+    const int64_t s0 = (int64_t)blockIdx.y * a.schunk, s1 = min(a.m, s0 + a.schunk);
+    const int tn = (int)(t1 - t0), groups = (tn + 31) >> 5;
+    for (int i = threadIdx.x; i < 3 * tn; i += ADJ_THREADS) gx_acc[i] = 0.0;
+    for (int64_t base = s0; base < s1; base += 32) {
+        const int cnt = (int)min((int64_t)32, s1 - base);
         __syncthreads();
         if (threadIdx.x < cnt) tile[threadIdx.x] = a.seg[base + threadIdx.x];
         __syncthreads();
-        if (!valid) continue;
-        for (int j = 0; j < cnt; ++j) {
-            if (a.ex_ptr && excluded(a.ex_ptr, a.ex_seg, p, base + j)) continue;
-            pair_vjp64(t.x, t.y, t.z, tile[j], a.model, t.wx, t.wy, t.wz, gx, ga, gb, gg);
+        double sacc[7] = {0, 0, 0, 0, 0, 0, 0};
+        for (int g = warp; g < groups; g += ADJ_WARPS) {
+            const int local = g * 32 + lane;
+            const bool valid = local < tn;
+            const int64_t p = t0 + local;
+            AdjTgt t = valid ? a.tgt[p] : AdjTgt{0, 0, 0, 0, 0, 0};
+            double gx0 = 0.0, gx1 = 0.0, gx2 = 0.0;
+            for (int j = 0; j < 32; ++j) {
+                const int si = (lane + j) & 31;
+                double g1[3] = {0, 0, 0}, g2[3] = {0, 0, 0}, gg = 0.0;
+                if (valid && si < cnt && !(a.ex_ptr && excluded(a.ex_ptr, a.ex_seg, p, base + si))) {
+                    if (pair_vjp64(t.x, t.y, t.z, tile[si], a.model, t.wx, t.wy, t.wz, g1, g2, gg)) {
+                        gx0 += g1[0] + g2[0];
+                        gx1 += g1[1] + g2[1];
+                        gx2 += g1[2] + g2[2];
+                    }
+                }
+                // lane r owns segment r of the tile and receives from lane (r - j) mod 32
+                const int src = (lane - j) & 31;
+                sacc[0] -= __shfl_sync(0xffffffffu, g1[0], src);
+                sacc[1] -= __shfl_sync(0xffffffffu, g1[1], src);
+                sacc[2] -= __shfl_sync(0xffffffffu, g1[2], src);
+                sacc[3] -= __shfl_sync(0xffffffffu, g2[0], src);
+                sacc[4] -= __shfl_sync(0xffffffffu, g2[1], src);
+                sacc[5] -= __shfl_sync(0xffffffffu, g2[2], src);
+                sacc[6] += __shfl_sync(0xffffffffu, gg, src);
+            }
+            if (valid) {
+                gx_acc[3 * local] += gx0;
+                gx_acc[3 * local + 1] += gx1;
+                gx_acc[3 * local + 2] += gx2;
+            }
+        }
+        for (int k = 0; k < 7; ++k) red[warp][k][lane] = sacc[k];
+        __syncthreads();
+        if (threadIdx.x < cnt) {
+            double *q = a.part_seg + 7 * ((int64_t)blockIdx.x * a.m + base + threadIdx.x);
+            for (int k = 0; k < 7; ++k) {
+                double v = 0.0;
+                for (int w = 0; w < ADJ_WARPS; ++w) v += red[w][k][threadIdx.x];
+                q[k] = v;
+            }
         }
     }
-    if (valid) {
-        const int64_t o = (int64_t)blockIdx.y * a.n + p;
-        a.part_x[3 * o] = gx[0];
-        a.part_x[3 * o + 1] = gx[1];
-        a.part_x[3 * o + 2] = gx[2];
-    }
+    __syncthreads();
+    double *q = a.part_x + 3 * ((int64_t)blockIdx.y * a.n + t0);
+    for (int i = threadIdx.x; i < 3 * tn; i += ADJ_THREADS) q[i] = gx_acc[i];
 }
 
-__global__ void __launch_bounds__(ADJ_TILE) adjoint_segment_kernel(AdjArgs a) {
-    __shared__ AdjTgt tile[ADJ_TILE];
-    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = s < a.m;
-    const int64_t p0 = (int64_t)blockIdx.y * a.chunk, p1 = min(a.n, p0 + a.chunk);
-    AdjSeg g = valid ? a.seg[s] : AdjSeg{0, 0, 0, 1, 0, 0, 0, 0};
-    double gx[3] = {0, 0, 0}, ga[3] = {0, 0, 0}, gb[3] = {0, 0, 0}, gg = 0.0;
-    for (int64_t base = p0; base < p1; base += ADJ_TILE) {
-        const int cnt = (int)min((int64_t)ADJ_TILE, p1 - base);
-        __syncthreads();
-        if (threadIdx.x < cnt) tile[threadIdx.x] = a.tgt[base + threadIdx.x];
-        __syncthreads();
-        if (!valid) continue;
-        for (int j = 0; j < cnt; ++j) {
-            if (a.ex_ptr && excluded(a.ex_ptr, a.ex_seg, base + j, s)) continue;
-            const AdjTgt &t = tile[j];
-            pair_vjp64(t.x, t.y, t.z, g, a.model, t.wx, t.wy, t.wz, gx, ga, gb, gg);
-        }
-    }
-    if (valid) {
-        const int64_t o = (int64_t)blockIdx.y * a.m + s;
-        double *q = a.part_seg + 7 * o;
-        q[0] = ga[0]; q[1] = ga[1]; q[2] = ga[2];
-        q[3] = gb[0]; q[4] = gb[1]; q[5] = gb[2];
-        q[6] = gg;
-    }
-}
-
-__global__ void adjoint_pack_kernel(int64_t n, int64_t m, const double *points, const double *cot, const double *A,
-                                    const double *B, const double *gamma, const double *radius, AdjTgt *tgt,
-                                    AdjSeg *seg) {
+__global__ void adjoint_pack_kernel(int64_t n, int64_t m, int model, const double *points, const double *cot,
+                                    const double *A, const double *B, const double *gamma, const double *radius,
+                                    AdjTgt *tgt, AdjSeg *seg) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) tgt[i] = AdjTgt{points[3 * i], points[3 * i + 1], points[3 * i + 2], cot[3 * i], cot[3 * i + 1],
                                cot[3 * i + 2]};
-    if (i < m) seg[i] = AdjSeg{A[3 * i], A[3 * i + 1], A[3 * i + 2], B[3 * i], B[3 * i + 1], B[3 * i + 2], gamma[i],
-                               radius[i]};
+    if (i < m) {
+        const double l0 = B[3 * i] - A[3 * i], l1 = B[3 * i + 1] - A[3 * i + 1], l2 = B[3 * i + 2] - A[3 * i + 2];
+        const double L2 = l0 * l0 + l1 * l1 + l2 * l2, rc = radius[i];
+        const double irc2L2 = (model != 0 && rc > 0.0) ? 1.0 / (L2 * rc * rc) : 0.0;
+        seg[i] = AdjSeg{A[3 * i], A[3 * i + 1], A[3 * i + 2], B[3 * i], B[3 * i + 1], B[3 * i + 2], gamma[i], irc2L2,
+                        1.0 / L2, 0.0};
+    }
 }
 
 __global__ void adjoint_reduce_kernel(int64_t n, int64_t m, int cx, int cs, const double *part_x,
@@ -206,12 +227,14 @@ __global__ void adjoint_reduce_kernel(int64_t n, int64_t m, int cx, int cs, cons
 
 using namespace bs;
 
-static int chunks_for(int64_t rows, int64_t inner, int sm_count) {
-    int64_t blocks = (rows + ADJ_TILE - 1) / ADJ_TILE;
-    int64_t want = (int64_t)sm_count * 8;
-    int64_t c = (want + blocks - 1) / blocks;
-    c = std::min<int64_t>(c, std::max<int64_t>(1, (inner + ADJ_TILE - 1) / ADJ_TILE));
-    return (int)std::max<int64_t>(1, std::min<int64_t>(c, 1024));
+// Target chunk: at most ADJ_MAX_TCHUNK targets (their gradients sit in shared memory); segment chunks: enough blocks
+// for about eight per SM in total, each at least a few tiles long.
+static void adjoint_chunks(int64_t n, int64_t m, int sm_count, int64_t &tchunk, int64_t &schunk) {
+    const int64_t tc = (n + ADJ_MAX_TCHUNK - 1) / ADJ_MAX_TCHUNK;
+    tchunk = (n + tc - 1) / tc;
+    const int64_t want = std::max<int64_t>(1, (int64_t)sm_count * 8 / tc);
+    schunk = std::max<int64_t>(128, (m + want - 1) / want);
+    schunk = (schunk + 31) / 32 * 32;
 }
 
 extern "C" int bs_adjoint_direct(bs_ctx *ctx, int64_t n, const double *points, int64_t m, const double *A,
@@ -238,15 +261,19 @@ extern "C" int bs_adjoint_direct(bs_ctx *ctx, int64_t n, const double *points, i
     Scratch scratch(ctx->pool, s);
     AdjTgt *tgt = scratch.get<AdjTgt>(n);
     AdjSeg *seg = scratch.get<AdjSeg>(m);
-    const int cx = chunks_for(n, m, ctx->sm_count), cs = chunks_for(m, n, ctx->sm_count);
-    double *part_x = scratch.get<double>((size_t)3 * n * cx), *part_seg = scratch.get<double>((size_t)7 * m * cs);
+    int64_t tchunk, schunk;
+    adjoint_chunks(n, m, ctx->sm_count, tchunk, schunk);
+    const int tc = (int)((n + tchunk - 1) / tchunk), sc = (int)((m + schunk - 1) / schunk);
+    double *part_x = scratch.get<double>((size_t)3 * n * sc), *part_seg = scratch.get<double>((size_t)7 * m * tc);
     if (!tgt || !seg || !part_x || !part_seg) return scratch.status;
     const int64_t big = std::max(n, m);
-    adjoint_pack_kernel<<<(unsigned)((big + 255) / 256), 256, 0, s>>>(n, m, points, cotangent, A, B, gamma, radius, tgt,
-                                                                      seg);
+    adjoint_pack_kernel<<<(unsigned)((big + 255) / 256), 256, 0, s>>>(n, m, model, points, cotangent, A, B, gamma,
+                                                                      radius, tgt, seg);
     AdjArgs args;
     args.n = n;
     args.m = m;
+    args.tchunk = tchunk;
+    args.schunk = schunk;
     args.tgt = tgt;
     args.seg = seg;
     args.ex_ptr = (ex_ptr && e > 0) ? ex_ptr : nullptr;
@@ -258,22 +285,9 @@ extern "C" int bs_adjoint_direct(bs_ctx *ctx, int64_t n, const double *points, i
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s);
-    if (grad_points) {
-        args.chunk = ((m + cx - 1) / cx + ADJ_TILE - 1) / ADJ_TILE * ADJ_TILE;
-        dim3 grid((unsigned)((n + ADJ_TILE - 1) / ADJ_TILE), (unsigned)((m + args.chunk - 1) / args.chunk));
-        adjoint_target_kernel<<<grid, ADJ_TILE, 0, s>>>(args);
-    }
-    int cx_used = (int)((m + args.chunk - 1) / std::max<int64_t>(1, args.chunk));
-    if (!grad_points) cx_used = 0;
-    int cs_used = 0;
-    if (grad_A || grad_B || grad_gamma) {
-        args.chunk = ((n + cs - 1) / cs + ADJ_TILE - 1) / ADJ_TILE * ADJ_TILE;
-        dim3 grid((unsigned)((m + ADJ_TILE - 1) / ADJ_TILE), (unsigned)((n + args.chunk - 1) / args.chunk));
-        cs_used = (int)grid.y;
-        adjoint_segment_kernel<<<grid, ADJ_TILE, 0, s>>>(args);
-    }
-    adjoint_reduce_kernel<<<(unsigned)((big + 255) / 256), 256, 0, s>>>(n, m, cx_used, cs_used, part_x, part_seg,
-                                                                         grad_points, grad_A, grad_B, grad_gamma);
+    adjoint_fused_kernel<<<dim3((unsigned)tc, (unsigned)sc), ADJ_THREADS, 0, s>>>(args);
+    adjoint_reduce_kernel<<<(unsigned)((big + 255) / 256), 256, 0, s>>>(n, m, sc, tc, part_x, part_seg, grad_points,
+                                                                         grad_A, grad_B, grad_gamma);
     cudaError_t le = cudaGetLastError();
     cudaEventRecord(e1, s);
     if (le == cudaSuccess) le = cudaEventSynchronize(e1);
@@ -285,6 +299,6 @@ extern "C" int bs_adjoint_direct(bs_ctx *ctx, int64_t n, const double *points, i
     ctx->stats.points = n;
     ctx->stats.segments = m;
     ctx->stats.evaluate_ms = ms;
-    ctx->stats.launches = 4;
+    ctx->stats.launches = 3;
     return BS_OK;
 }
