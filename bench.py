@@ -236,6 +236,29 @@ def adjoint_measure(device, theta):
             "ratio_to_fp64_direct": adj / fwd, "ratio_to_tree_forward": adj / tree}
 
 
+def sharded_measure(src, case, rank, world, device, args, dist):
+    """One wake split over the ranks by Morton ranges of its targets (segments replicated, no collective on the data
+    path): device ms per call as the max over ranks, after warm-up; every rank takes the same collective steps."""
+    import torch
+    from openfawe_b200 import shard
+    model = case["model"]
+
+    def run():
+        return shard.sharded_tree_sum(src, case["points"], rank, world, model, "mixed", args.theta, ORDER, LEAF)
+
+    for _ in range(2):
+        run()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(3):
+        dist.barrier()
+        times.append(_event_ms(run))
+    t = torch.tensor([min(times)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return {"mode": "targets split by Morton range over ranks, segments replicated", "ms_per_call": float(t.item()),
+            "targets_per_rank": len(case["points"]) // world}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -374,6 +397,7 @@ def main():
             line["adjoint"] = adjoint_measure(device, args.theta)
             line["adjoint_fwd_ratio"] = line["adjoint"]["ratio_to_fp64_direct"]
     if dist:
+        line["sharded"] = sharded_measure(src, case, rank, world, device, args, dist)
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:

@@ -178,6 +178,41 @@ int bs_adjoint_direct(bs_ctx *ctx, int64_t n, const double *points, int64_t m, c
                       int64_t e, int model, const double *cotangent, double *grad_points, double *grad_A,
                       double *grad_B, double *grad_gamma, bs_stream stream);
 
+/* Incident-endpoint exclusion pairs of a wake network (replaces network_numba.incident_pairs,
+ * src/openfawe/aero/network_numba.py:242-256): for every segment s of edges [segments][2] in order and each of its two
+ * ends, the pairs (i, s) of every free point i (node first + i, first in [0, n]) whose three coordinates equal that
+ * end node's bit for bit (NaN never matches), i increasing.  nodes [n][3] float64, edges, pairs [capacity][2] int64,
+ * all device.  *count (host) receives the number of pairs; they are written only if it is <= capacity (call again
+ * with a larger buffer otherwise).  An edge index outside [0, n) is BS_ERR_ARG.  Synchronises the stream. */
+int bs_incident_pairs(bs_ctx *ctx, const double *nodes, int64_t n, const int64_t *edges, int64_t segments,
+                      int64_t first, int64_t *pairs, int64_t capacity, int64_t *count, bs_stream stream);
+
+/* Per-point sorted unique excluded segments from (point, segment) pairs [e][2] (replaces vortex_numba.exclusion_csr,
+ * src/openfawe/aero/vortex_numba.py:228-243, and its np.unique reference :179-190): ptr [n+1] and seg [>= e] device
+ * int64; *unique_count (host) receives the length of seg.  A point outside [0, n) is BS_ERR_ARG.  Synchronises. */
+int bs_exclusion_csr(bs_ctx *ctx, int64_t n, const int64_t *pairs, int64_t e, int64_t *ptr, int64_t *seg,
+                     int64_t *unique_count, bs_stream stream);
+
+/* Unit-circulation pair matrix (replaces vortex_numba.pair_matrix, src/openfawe/aero/vortex_numba.py:271-287):
+ * out [n][m][3] = the FP64 velocity of segment s with circulation 1 at point p (zero for a flagged pair), flags [n] =
+ * the flag of the point's first flagged segment.  src->gamma is not read. */
+int bs_pair_matrix(bs_ctx *ctx, int64_t n, const double *points, const bs_sources *src, int model, int raise_singular,
+                   double *out, int8_t *flags, bs_stream stream);
+
+/* Panel columns from a pair matrix (replaces vortex_numba.assemble_columns, vortex_numba.py:290-308): out [n][columns]
+ * [3][j] = sum over k in [column_ptr[j], column_ptr[j+1]), in order from 0.0, of column_sign[k] * pairs[p]
+ * [column_segment[k]].  column_ptr must not decrease and every column_segment must lie in [0, m) (BS_ERR_ARG). */
+int bs_assemble_columns(bs_ctx *ctx, int64_t n, int64_t m, const double *pairs, int64_t columns,
+                        const int64_t *column_ptr, const int64_t *column_segment, const double *column_sign,
+                        double *out, bs_stream stream);
+
+/* bs_pair_matrix followed by bs_assemble_columns without storing the pair matrix (the VSM ring operators of
+ * vsm_wake._batched_ring_operator, src/openfawe/aero/vsm_wake.py:224-252); flags as bs_pair_matrix's over the
+ * segments the columns use. */
+int bs_ring_columns(bs_ctx *ctx, int64_t n, const double *points, const bs_sources *src, int model, int raise_singular,
+                    int64_t columns, const int64_t *column_ptr, const int64_t *column_segment,
+                    const double *column_sign, double *out, int8_t *flags, bs_stream stream);
+
 /* Build + evaluate + free (cuda_tree_sum in one call). */
 int bs_tree_sum(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, const bs_targets *tgt,
                 const bs_kernel_params *kp, double *out, int8_t *flags, int64_t *far_counts, bs_stream stream);

@@ -76,6 +76,16 @@ SIGNATURES = {
     "bs_graph_launch": (ctypes.c_int, [_p, _p]),
     "bs_graph_status": (ctypes.c_int, [_p, ctypes.POINTER(Stats)]),
     "bs_graph_free": (None, [_p]),
+    "bs_incident_pairs": (ctypes.c_int, [_p, _p, ctypes.c_int64, _p, ctypes.c_int64, ctypes.c_int64, _p, ctypes.c_int64,
+                                         ctypes.POINTER(ctypes.c_int64), _p]),
+    "bs_exclusion_csr": (ctypes.c_int, [_p, ctypes.c_int64, _p, ctypes.c_int64, _p, _p, ctypes.POINTER(ctypes.c_int64),
+                                        _p]),
+    "bs_pair_matrix": (ctypes.c_int, [_p, ctypes.c_int64, _p, ctypes.POINTER(Sources), ctypes.c_int, ctypes.c_int, _p,
+                                      _p, _p]),
+    "bs_assemble_columns": (ctypes.c_int, [_p, ctypes.c_int64, ctypes.c_int64, _p, ctypes.c_int64, _p, _p, _p, _p,
+                                           _p]),
+    "bs_ring_columns": (ctypes.c_int, [_p, ctypes.c_int64, _p, ctypes.POINTER(Sources), ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int64, _p, _p, _p, _p, _p, _p]),
 }
 
 _LOCK = threading.RLock()

@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBRARY = os.path.join(HERE, "libbs_b200.so")
-SOURCES = ["bs_context.cu", "bs_sort.cu", "bs_tree_build.cu", "bs_tree_eval.cu", "bs_direct.cu", "bs_adjoint.cu"]
+SOURCES = ["bs_context.cu", "bs_sort.cu", "bs_tree_build.cu", "bs_tree_eval.cu", "bs_direct.cu", "bs_adjoint.cu", "bs_network.cu", "bs_operators.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 

@@ -13,6 +13,7 @@ signature (``points, starts, directions, lengths, gamma, radius, model``) plus t
   circulation ~ U(0, 8), Lamb-Oseen core 0.05 m, 20,570 targets on the youngest rows' nodes lifted 0.011 m.
 * ``lattice``: 16 spanwise panels x 128 shed rows (4,207 segments), Rosenhead-Moore core 0.05 m, 1,024 targets at the
   three-quarter-chord points of a 1,024-panel wing line over a 26 m span.
+* ``ring_wing``: a 64-panel elliptic wing's attached rings with the per-panel column layout of the VSM operators.
 * ``wake_batch``: 48 rotor-sheet wakes with log-uniform sizes in [5k, 410k] segments, wind 6-14 m/s setting the row
   spacing, log-uniform target counts in [2,000, 20,570].
 """
@@ -150,6 +151,51 @@ def wake_batch(count=48, seed=48, low=5_000, high=410_000, targets_low=2_000, ta
         rows = max(2, int(round(sizes[k] / 219)))
         cases.append(rotor_sheet(rows, seed=seed * 1000 + k, targets=int(target_counts[k]), wind=float(winds[k])))
     return cases
+
+
+def ring_wing(panels=64, rows=4, span=26.0, chord=2.0, spacing=0.4, seed=64, core=0.05):
+    """An elliptic wing's attached vortex rings as the VSM operators use them: (rows+1) x (panels+1) lattice nodes
+    (quarter-chord bound line, then rows shed 0.4 m apart), unique undirected segments in first-appearance order, and
+    one column per panel listing its rings' segments with the sign of their direction in the ring; edges shared by
+    consecutive rings of a panel cancel and are left out (the layout vsm_wake._ring_layout builds,
+    src/openfawe/aero/vsm_wake.py:176-221).  Control points at the three-quarter chord lifted 0.01 m."""
+    rng = np.random.default_rng(seed)
+    y = np.linspace(-span / 2, span / 2, panels + 1)
+    c = chord * np.sqrt(np.maximum(1 - (2 * y / span) ** 2, 0.05))
+    nodes = np.zeros((rows + 1, panels + 1, 3))
+    for r in range(rows + 1):
+        nodes[r, :, 0] = 0.25 * c + r * spacing
+        nodes[r, :, 1] = y
+        nodes[r, :, 2] = 0.02 * r * np.sin(y / 5.0)
+    nodes[1:] += 0.01 * rng.standard_normal(nodes[1:].shape)
+    flat = nodes.reshape(-1, 3)
+    width = panels + 1
+    appearance, per_panel = {}, [dict() for _ in range(panels)]
+    for i in range(rows):
+        for j in range(panels):
+            ring = [i * width + j, i * width + j + 1, (i + 1) * width + j + 1, (i + 1) * width + j]
+            for a, b in zip(ring, ring[1:] + ring[:1]):
+                key = (min(a, b), max(a, b))
+                appearance.setdefault(key, len(appearance))
+                per_panel[j][key] = per_panel[j].get(key, 0.0) + (1.0 if a < b else -1.0)
+    unique, columns = {}, []
+    for edges in per_panel:
+        column = []
+        for key in sorted(edges, key=appearance.__getitem__):
+            if edges[key] != 0.0:
+                column.append((unique.setdefault(key, len(unique)), edges[key]))
+        columns.append(column)
+    segments = np.asarray(list(unique), dtype=np.int64).reshape(-1, 2)
+    pointer = np.zeros(panels + 1, dtype=np.int64)
+    pointer[1:] = np.cumsum([len(col) for col in columns])
+    column_segment = np.asarray([k for col in columns for k, _ in col], dtype=np.int64)
+    column_sign = np.asarray([v for col in columns for _, v in col], dtype=np.float64)
+    yc = 0.5 * (y[:-1] + y[1:])
+    cc = chord * np.sqrt(np.maximum(1 - (2 * yc / span) ** 2, 0.05))
+    control = np.column_stack((0.75 * cc, yc, np.full(panels, 0.01)))
+    case = _case(control, flat, segments, np.ones(len(segments)), np.full(len(segments), core), LAMB_OSEEN)
+    case.update(column_ptr=pointer, column_segment=column_segment, column_sign=column_sign)
+    return case
 
 
 def backend_args(case):

@@ -13,6 +13,7 @@
  *   pair_velocity        src/openfawe/aero/vortex_numba.py:42-109
  *   _sum_point           src/openfawe/aero/vortex_numba.py:112-147   (direct sum, ordered per target)
  *   exclusion_csr        src/openfawe/aero/vortex_numba.py:193-243
+ *   incident_pairs       src/openfawe/aero/network_numba.py:176-256
  *   pair_matrix          src/openfawe/aero/vortex_numba.py:271-287
  *   build_tree_serial    src/openfawe/aero/vortex_tree.py:51-115     (== build_tree element for element, :208-241)
  *   node_moments         src/openfawe/aero/vortex_tree.py:118-167, 320-376
@@ -206,6 +207,90 @@ int64_t orc_exclusion_csr(int64_t point_count, int64_t e, const int64_t *pairs, 
     free(start);
     free(cursor);
     return mcount;
+}
+
+/* network_numba.incident_pairs / _incident_pairs_sorted (src/openfawe/aero/network_numba.py:176-256): the exclusion
+ * pairs (free point i, segment s) of every free node first + i whose coordinates equal an end node of segment s bit
+ * for bit (NaN never matches), in segment order, end order, then member order (increasing i).  Nodes are ordered as
+ * np.lexsort((bits z, bits y, bits x)) orders them (signed 64-bit patterns, stable), equal patterns form runs, groups
+ * are numbered by first appearance among the free points.  Returns the number of pairs; writes them if it fits. */
+static const int64_t *orc_bits_base;
+
+static int orc_bits_cmp(const void *pa, const void *pb)
+{
+    int64_t a = *(const int64_t *)pa, b = *(const int64_t *)pb;
+    for (int c = 0; c < 3; ++c) {
+        int64_t x = orc_bits_base[3 * a + c], y = orc_bits_base[3 * b + c];
+        if (x != y) return x < y ? -1 : 1;
+    }
+    return a < b ? -1 : (a > b);
+}
+
+int64_t orc_incident_pairs(int64_t n, const double *nodes, int64_t segments, const int64_t *edges, int64_t first,
+                           int64_t *pairs, int64_t capacity)
+{
+    int64_t *bits = (int64_t *)malloc(sizeof(int64_t) * (size_t)(3 * n + 1));
+    int64_t *order = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n + 1));
+    int64_t *run_of = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n + 1));
+    unsigned char *no_nan = (unsigned char *)malloc((size_t)n + 1);
+    memcpy(bits, nodes, sizeof(double) * (size_t)(3 * n));
+    for (int64_t i = 0; i < n; ++i) {
+        order[i] = i;
+        no_nan[i] = !(isnan(nodes[3 * i]) || isnan(nodes[3 * i + 1]) || isnan(nodes[3 * i + 2]));
+    }
+    orc_bits_base = bits;
+    qsort(order, (size_t)n, sizeof(int64_t), orc_bits_cmp);
+    int64_t runs = 0, previous = -1;
+    for (int64_t position = 0; position < n; ++position) {
+        int64_t node = order[position];
+        int same = previous >= 0 && no_nan[node] && no_nan[previous] && bits[3 * node] == bits[3 * previous] &&
+                   bits[3 * node + 1] == bits[3 * previous + 1] && bits[3 * node + 2] == bits[3 * previous + 2];
+        if (!same) runs += 1;
+        run_of[node] = runs - 1;
+        previous = node;
+    }
+    int64_t count = n - first;
+    int64_t *group_of_run = (int64_t *)malloc(sizeof(int64_t) * (size_t)(runs + 1));
+    int64_t *point_group = (int64_t *)malloc(sizeof(int64_t) * (size_t)(count + 1));
+    for (int64_t r = 0; r < runs; ++r) group_of_run[r] = -1;
+    int64_t groups = 0;
+    for (int64_t index = 0; index < count; ++index) {
+        int64_t run = run_of[first + index];
+        if (group_of_run[run] < 0) group_of_run[run] = groups++;
+        point_group[index] = group_of_run[run];
+    }
+    int64_t *sizes = (int64_t *)calloc((size_t)groups + 1, sizeof(int64_t));
+    int64_t *cursor = (int64_t *)malloc(sizeof(int64_t) * (size_t)(groups + 1));
+    int64_t *members = (int64_t *)malloc(sizeof(int64_t) * (size_t)(count + 1));
+    for (int64_t index = 0; index < count; ++index) sizes[point_group[index] + 1] += 1;
+    for (int64_t g = 0; g < groups; ++g) sizes[g + 1] += sizes[g];
+    for (int64_t g = 0; g < groups; ++g) cursor[g] = sizes[g];
+    for (int64_t index = 0; index < count; ++index) members[cursor[point_group[index]]++] = index;
+    int64_t total = 0;
+    for (int64_t segment = 0; segment < segments; ++segment)
+        for (int end = 0; end < 2; ++end) {
+            int64_t node = edges[2 * segment + end];
+            if (!no_nan[node]) continue;
+            int64_t g = group_of_run[run_of[node]];
+            if (g >= 0) total += sizes[g + 1] - sizes[g];
+        }
+    if (pairs && total <= capacity) {
+        int64_t m = 0;
+        for (int64_t segment = 0; segment < segments; ++segment)
+            for (int end = 0; end < 2; ++end) {
+                int64_t node = edges[2 * segment + end];
+                if (!no_nan[node]) continue;
+                int64_t g = group_of_run[run_of[node]];
+                if (g < 0) continue;
+                for (int64_t k = sizes[g]; k < sizes[g + 1]; ++k, ++m) {
+                    pairs[2 * m] = members[k];
+                    pairs[2 * m + 1] = segment;
+                }
+            }
+    }
+    free(bits); free(order); free(run_of); free(no_nan); free(group_of_run); free(point_group); free(sizes);
+    free(cursor); free(members);
+    return total;
 }
 
 /* ---------------------------------------------------------------------------------------------------------------- */

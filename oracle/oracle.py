@@ -43,6 +43,7 @@ def lib():
                                       ctypes.c_int]),
             "orc_pair_matrix": (None, [_I, _d, _I, _d, _d, _d, _d, ctypes.c_int, ctypes.c_int, _d, _i8]),
             "orc_exclusion_csr": (_I, [_I, _I, _i64, _i64, _i64]),
+            "orc_incident_pairs": (_I, [_I, _d, _I, _i64, _I, _i64, _I]),
             "orc_tree_capacity": (_I, [_I, _I]),
             "orc_build_tree": (_I, [_I, _d, _I, _i64, _i64, _i64, _i64, _i64]),
             "orc_node_moments": (None, [_I, _i64, _i64, _i64, _d, _d, _d, _d, _d, _d, _d, _d, _d, _d, _d, _d,
@@ -104,6 +105,18 @@ def exclusion_csr(point_count, pair_array):
     return ptr, seg[:count].copy()
 
 
+def incident_pairs(nodes, edges, first):
+    """network_numba.incident_pairs (network_numba.py:242-256) for (n,3) nodes and in-range (e,2) edges."""
+    nodes = _f64(np.asarray(nodes, dtype=np.float64).reshape(-1, 3))
+    edges = _i64a(np.asarray(edges, dtype=np.int64).reshape(-1, 2))
+    n, e = len(nodes), len(edges)
+    total = lib().orc_incident_pairs(n, _p(nodes), e, _p(edges, _i64), int(first), None, 0)
+    pairs = np.zeros((total, 2), dtype=np.int64)
+    if total:
+        lib().orc_incident_pairs(n, _p(nodes), e, _p(edges, _i64), int(first), _p(pairs, _i64), total)
+    return pairs
+
+
 def direct_sum(points, starts, directions, lengths, gamma, radius, model, csr, singularity, threads=0,
                return_flags=False):
     """vortex_numba.direct_sum (vortex_numba.py:246-260): (velocity, any_flag)."""
@@ -133,6 +146,19 @@ def pair_matrix(points, starts, directions, lengths, radius, model, raise_singul
     lib().orc_pair_matrix(n, _p(points), m, _p(starts), _p(directions), _p(lengths), _p(radius), int(model),
                           int(bool(raise_singular)), _p(out), _p(flags, _i8))
     return out, flags
+
+
+def assemble_columns(pairs, column_ptr, column_segment, column_sign):
+    """vortex_numba.assemble_columns (vortex_numba.py:290-308): out[p, j] = sum_k sign_k * pairs[p, segment_k],
+    sequential in k from 0.0 (element-wise NumPy, the same IEEE operations per element)."""
+    pairs = np.asarray(pairs, dtype=np.float64)
+    out = np.zeros((pairs.shape[0], len(column_ptr) - 1, 3))
+    for j in range(len(column_ptr) - 1):
+        acc = np.zeros((pairs.shape[0], 3))
+        for k in range(column_ptr[j], column_ptr[j + 1]):
+            acc = acc + column_sign[k] * pairs[:, column_segment[k], :]
+        out[:, j] = acc
+    return out
 
 
 def segment_geometry(starts, directions, lengths, gamma):

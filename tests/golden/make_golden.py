@@ -71,15 +71,92 @@ def ring_lattice(seed=11, rows=24, span=17):
     return nodes, np.asarray(edges, dtype=np.int64), np.asarray(gamma)
 
 
+def network_cases(seed):
+    """Wake networks whose free nodes (index >= first) coincide bit for bit with bound nodes and with each other, plus
+    -0.0 / 0.0 twins, NaN and infinite coordinates (the cases network_numba.py:13-22 of the reference describes)."""
+    rng = np.random.default_rng(seed)
+    bound = np.round(rng.normal(size=(40, 3)), 2)
+    bound[3] = [0.0, 1.0, 2.0]
+    free = np.round(rng.normal(size=(120, 3)), 2)
+    pick = rng.integers(0, 40, 50)
+    free[:50] = bound[pick]                      # shed nodes sitting on bound nodes
+    free[50:80] = free[rng.integers(0, 50, 30)]  # repeated free nodes
+    free[80] = [-0.0, 1.0, 2.0]                  # differs from bound[3] only in the sign of zero
+    free[81] = [0.0, 1.0, 2.0]
+    free[82] = [np.nan, 0.5, 0.5]
+    free[83] = [np.nan, 0.5, 0.5]
+    free[84] = [np.inf, -1.0, 0.0]
+    free[85] = [np.inf, -1.0, 0.0]
+    nodes = np.vstack([bound, free])
+    edges = rng.integers(0, len(nodes), size=(300, 2))
+    edges[:6] = [[3, 120], [122, 123], [124, 125], [40 + 84, 40 + 85], [0, 40], [40 + 81, 3]]
+    return nodes, edges.astype(np.int64), len(bound)
+
+
+def exclusion_cases(seed):
+    rng = np.random.default_rng(seed)
+    points = rng.integers(0, 50, 400)
+    segments = rng.integers(0, 30, 400)
+    out = {"a": (60, np.column_stack((points, segments)))}
+    # repeats, negative and very large segment ids, unused trailing points
+    b = np.column_stack((rng.integers(0, 7, 90), rng.choice([-5, -1, 0, 3, 2**40, 2**62, 17], 90)))
+    out["b"] = (12, b)
+    out["c"] = (5, np.zeros((0, 2), dtype=np.int64))
+    out["d"] = (3, np.array([[2, 9], [2, 9], [0, 4], [2, 1]]))
+    return out
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--only", default=None, help="write only this fixture (e.g. network.npz)")
     args = parser.parse_args()
     os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(tempfile.gettempdir(), "numba_reference_cache"))
     sys.path.insert(0, os.path.join(args.reference, "src"))
     sys.path.insert(0, REPO)
     from openfawe.aero import vortex_numba as vn, vortex_tree as vt
     from openfawe_b200 import wakes
+
+    if args.only == "operators.npz" or args.only is None:
+        out = {}
+        wing = wakes.ring_wing(panels=16, rows=3)
+        rng = np.random.default_rng(8)
+        # control points, points on the bound line and on a trailing segment (flagged pairs), off-wing points
+        a, b = wing["nodes"][wing["edges"][:3, 0]], wing["nodes"][wing["edges"][:3, 1]]
+        points = np.vstack([wing["points"], a + 0.5 * (b - a), a, rng.normal(scale=5.0, size=(8, 3))])
+        for model in (0, 2, 5):
+            for raise_singular in (True, False):
+                radius = wing["radius"] if model else np.zeros(len(wing["radius"]))
+                pairs = np.zeros((len(points), len(wing["starts"]), 3))
+                flags = np.zeros(len(points), dtype=np.int8)
+                vn.pair_matrix(points, wing["starts"], wing["directions"], wing["lengths"], radius, model,
+                               raise_singular, pairs, flags)
+                cols = np.zeros((len(points), len(wing["column_ptr"]) - 1, 3))
+                vn.assemble_columns(pairs, wing["column_ptr"], wing["column_segment"], wing["column_sign"], cols)
+                key = f"m{model}_{'raise' if raise_singular else 'zero'}"
+                out[key + "_pairs"], out[key + "_flags"], out[key + "_columns"] = pairs, flags, cols
+        out["points"] = points
+        save("operators.npz", **out)
+        if args.only:
+            return
+
+    if args.only == "network.npz" or args.only is None:
+        from openfawe.aero import network_numba as nn
+        out = {}
+        for seed in (1, 2):
+            nodes, edges, first = network_cases(seed)
+            for f in (first, 0, len(nodes)):
+                got = nn.incident_pairs(nodes, edges, f)
+                assert np.array_equal(got, nn.incident_pairs_reference(nodes, edges, f))
+                out[f"n{seed}_f{f}_pairs"] = got
+            out[f"n{seed}_nodes"], out[f"n{seed}_edges"], out[f"n{seed}_first"] = nodes, edges, np.array(first)
+        for name, (count, pairs) in exclusion_cases(3).items():
+            ptr, seg = vn.exclusion_csr(count, pairs)
+            out[f"x{name}_count"], out[f"x{name}_pairs"] = np.array(count), np.asarray(pairs, dtype=np.int64)
+            out[f"x{name}_ptr"], out[f"x{name}_seg"] = ptr, seg
+        save("network.npz", **out)
+        if args.only:
+            return
 
     # 1. welib per-core velocities (tests/fixtures/upstream-kernel-check.json of the reference), as arrays.
     with open(os.path.join(args.reference, "tests/fixtures/upstream-kernel-check.json"), encoding="utf-8") as f:

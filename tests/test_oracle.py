@@ -267,3 +267,34 @@ class TestMortonRecomputation:
             previous = error
         u, _ = O.tree_sum(*args, theta=1e-9, leaf_size=4, kind="morton")
         np.testing.assert_allclose(u, g["direct"], rtol=0, atol=1e-13 * scale)
+
+
+def test_incident_pairs_and_exclusion_csr_match_reference():
+    """network_numba.incident_pairs (sorted-bits version, equal to its dictionary reference) and
+    vortex_numba.exclusion_csr: bound/free coincidences, repeated free nodes, -0.0 vs 0.0, NaN, inf; first = bound
+    count, 0 and n; exclusion pairs with repeats, negative and 2**62 segment ids, empty input."""
+    g = golden("network.npz")
+    for seed in (1, 2):
+        nodes, edges, first = g[f"n{seed}_nodes"], g[f"n{seed}_edges"], int(g[f"n{seed}_first"])
+        for f in (first, 0, len(nodes)):
+            assert np.array_equal(O.incident_pairs(nodes, edges, f), g[f"n{seed}_f{f}_pairs"]), (seed, f)
+    for name in "abcd":
+        ptr, seg_ = O.exclusion_csr(int(g[f"x{name}_count"]), g[f"x{name}_pairs"])
+        assert np.array_equal(ptr, g[f"x{name}_ptr"]) and np.array_equal(seg_, g[f"x{name}_seg"]), name
+
+
+def test_pair_matrix_and_assemble_columns_match_reference():
+    """vortex_numba.pair_matrix and assemble_columns on a 16-panel ring wing's column layout (bound line, trailing
+    legs, shed rings; points on segments for the flags), models 0, 2, 5, both singularity modes: bit for bit."""
+    from openfawe_b200 import wakes
+    g = golden("operators.npz")
+    wing = wakes.ring_wing(panels=16, rows=3)
+    for model in (0, 2, 5):
+        radius = wing["radius"] if model else np.zeros(len(wing["radius"]))
+        for mode in ("raise", "zero"):
+            key = f"m{model}_{mode}"
+            pairs, flags = O.pair_matrix(g["points"], wing["starts"], wing["directions"], wing["lengths"], radius,
+                                         model, mode == "raise")
+            assert bits_equal(pairs, g[key + "_pairs"]) and np.array_equal(flags, g[key + "_flags"]), key
+            cols = O.assemble_columns(pairs, wing["column_ptr"], wing["column_segment"], wing["column_sign"])
+            assert bits_equal(cols, g[key + "_columns"]), key
