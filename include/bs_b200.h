@@ -69,7 +69,8 @@ typedef struct {
 
 typedef struct {
     double theta;      /* opening ratio, 0 < theta < 1 (TreeSettings.theta) */
-    int order;         /* expansion order 0, 1 or 2 */
+    int order;         /* expansion order 0, 1 or 2 (the reference's); 3 adds the third-order term (a tree evaluated
+                          at order 3 must be built with order 3, which computes its third moments) */
     int64_t leaf_size; /* maximum segments per leaf */
     double clearance;  /* core clearance in largest core radii */
     int kind;          /* bs_tree_kind */
@@ -177,6 +178,23 @@ int bs_adjoint_direct(bs_ctx *ctx, int64_t n, const double *points, int64_t m, c
                       const double *gamma, const double *radius, const int64_t *ex_ptr, const int64_t *ex_seg,
                       int64_t e, int model, const double *cotangent, double *grad_points, double *grad_A,
                       double *grad_B, double *grad_gamma, bs_stream stream);
+
+/* The reference's median-split tree from midpoints alone (replaces vortex_cuda_build.device_build_tree,
+ * src/openfawe/aero/vortex_cuda_build.py:234-275, and vortex_tree.build_tree, vortex_tree.py:208-241): order [m] and,
+ * when *count <= capacity, lo/hi/left/right [count] in depth-first numbering, element for element equal to
+ * build_tree's.  mid [m][3] float64; all device.  Synchronises the stream. */
+int bs_median_topology(bs_ctx *ctx, int64_t m, const double *mid, int leaf_size, int64_t *order, int64_t *lo,
+                       int64_t *hi, int64_t *left, int64_t *right, int64_t capacity, int64_t *count, bs_stream stream);
+
+/* Node quantities of a given tree (replaces vortex_cuda_moments.device_node_quantities,
+ * src/openfawe/aero/vortex_cuda_moments.py:206-230, i.e. vortex_tree.node_moments + node_contractions): for the
+ * tree (order [m], lo, hi [count]) over segments with starts, ends, length vectors [m][3], gamma, radius [m], writes
+ * centre [count][3], bound, core [count], m0 [count][3], m1 [count][3][3], m2 [count][3][3][3], w1, t2 [count][3],
+ * w2 [count][3][3] (any may be NULL).  The vortex vectors are gamma * length_vectors.  Synchronises. */
+int bs_node_quantities(bs_ctx *ctx, int64_t m, const double *starts, const double *ends, const double *length_vectors,
+                       const double *gamma, const double *radius, int64_t count, const int64_t *order,
+                       const int64_t *lo, const int64_t *hi, double *centre, double *bound, double *core, double *m0,
+                       double *m1, double *m2, double *w1, double *t2, double *w2, bs_stream stream);
 
 /* Incident-endpoint exclusion pairs of a wake network (replaces network_numba.incident_pairs,
  * src/openfawe/aero/network_numba.py:242-256): for every segment s of edges [segments][2] in order and each of its two

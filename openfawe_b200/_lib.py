@@ -80,6 +80,10 @@ SIGNATURES = {
                                          ctypes.POINTER(ctypes.c_int64), _p]),
     "bs_exclusion_csr": (ctypes.c_int, [_p, ctypes.c_int64, _p, ctypes.c_int64, _p, _p, ctypes.POINTER(ctypes.c_int64),
                                         _p]),
+    "bs_median_topology": (ctypes.c_int, [_p, ctypes.c_int64, _p, ctypes.c_int, _p, _p, _p, _p, _p, ctypes.c_int64,
+                                          ctypes.POINTER(ctypes.c_int64), _p]),
+    "bs_node_quantities": (ctypes.c_int, [_p, ctypes.c_int64, _p, _p, _p, _p, _p, ctypes.c_int64, _p, _p, _p]
+                           + [_p] * 9 + [_p]),
     "bs_pair_matrix": (ctypes.c_int, [_p, ctypes.c_int64, _p, ctypes.POINTER(Sources), ctypes.c_int, ctypes.c_int, _p,
                                       _p, _p]),
     "bs_assemble_columns": (ctypes.c_int, [_p, ctypes.c_int64, ctypes.c_int64, _p, ctypes.c_int64, _p, _p, _p, _p,

@@ -36,6 +36,7 @@ class WakeBatch:
                                       self.device)
         self.targets = engine.Targets(cat("points"), None, self.device)
         self.leaf_size = leaf_size
+        self.order = 2
         self.forest = None
         self.graph = None
 
@@ -43,10 +44,12 @@ class WakeBatch:
     def count(self):
         return len(self.wake_ptr) - 1
 
-    def build(self, leaf_size=None):
+    def build(self, leaf_size=None, order=None):
         if leaf_size is not None:
             self.leaf_size = leaf_size
-        self.forest = engine.build_forest(self.sources, self.wake_ptr, self.leaf_size)
+        if order is not None:
+            self.order = order
+        self.forest = engine.build_forest(self.sources, self.wake_ptr, self.leaf_size, self.order)
         self.graph = None
         return self.forest
 

@@ -126,6 +126,14 @@ struct __align__(16) Far32 { float v[BS_FAR_N + 3]; };
 
 enum { F_M0 = 0, F_M1 = 3, F_W1 = 12, F_T2 = 15, F_W2 = 18, F_M2 = 27 };
 
+// Third-order far-field coefficients (an extension of the reference's orders 0-2): m3 symmetric in its last three
+// indices [3][10] (000,001,002,011,012,022,111,112,122,222), its trace T3[b][l] = m3[b][j][j][l] [3][3],
+// W3[a][k][l] = eps_abc m3[b][c][k][l] symmetric [3][6], w3[a] = eps_abc T3[b][c] [3].
+#define BS_FAR3_N 60
+struct __align__(16) Far64x { double v[64]; };
+struct __align__(16) Far32x { float v[64]; };
+enum { G_M3 = 0, G_T3 = 30, G_W3 = 39, G_W3V = 57 };
+
 // ---------------------------------------------------------------------------------------------------------------------
 // Arithmetic helpers.
 // ---------------------------------------------------------------------------------------------------------------------
@@ -310,9 +318,12 @@ __device__ __forceinline__ bool pair32(float rx, float ry, float rz, const float
     return need64;
 }
 
-// vortex_tree.far_velocity with the symmetric second moment; R = x - c.
+// vortex_tree.far_velocity with the symmetric second moment; R = x - c.  Order 3 (g: the third-order record) adds
+//   (17.5 S3 / r^9 - 7.5 T3 R / r^7) x R - 7.5 (W3 : R R) / r^7 + 1.5 w3 / r^5,  S3_b = m3[b] : R R R,
+// the next term of the same Taylor series of the segments' line integrals about the node centre.
 template <class T>
-__device__ __forceinline__ void far_eval(T rx, T ry, T rz, const T *f, int order, T &ux, T &uy, T &uz) {
+__device__ __forceinline__ void far_eval(T rx, T ry, T rz, const T *f, int order, T &ux, T &uy, T &uz,
+                                         const T *g = nullptr) {
     T r2 = rx * rx + ry * ry + rz * rz;
     T inv3 = T(1) / (r2 * sqrt(r2));
     T inv5 = inv3 / r2;
@@ -347,6 +358,33 @@ __device__ __forceinline__ void far_eval(T rx, T ry, T rz, const T *f, int order
         u0 += (b1 * rz - b2 * ry) - k * s0;
         u1 += (b2 * rx - b0 * rz) - k * s1;
         u2 += (b0 * ry - b1 * rx) - k * s2;
+        if (order >= 3) {
+            const T inv9 = inv7 / r2;
+            // cubic monomials with their multiplicities in the symmetric contraction
+            const T c000 = xx * rx, c001 = T(3) * xx * ry, c002 = T(3) * xx * rz, c011 = T(3) * xy * ry;
+            const T c012 = T(6) * xy * rz, c022 = T(3) * xz * rz, c111 = yy * ry, c112 = T(3) * yy * rz;
+            const T c122 = T(3) * yz * rz, c222 = zz * rz;
+            T x3[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const T *m = g + G_M3 + 10 * i;
+                const T s3 = m[0] * c000 + m[1] * c001 + m[2] * c002 + m[3] * c011 + m[4] * c012 + m[5] * c022 +
+                             m[6] * c111 + m[7] * c112 + m[8] * c122 + m[9] * c222;
+                const T *t3 = g + G_T3 + 3 * i;
+                const T tr = t3[0] * rx + t3[1] * ry + t3[2] * rz;
+                x3[i] = T(17.5) * inv9 * s3 - T(7.5) * inv7 * tr;
+            }
+            T w[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const T *s = g + G_W3 + 6 * i;
+                w[i] = s[0] * xx + s[3] * yy + s[5] * zz + T(2) * (s[1] * xy + s[2] * xz + s[4] * yz);
+            }
+            const T c7 = T(7.5) * inv7, c5 = T(1.5) * inv5;
+            u0 += (x3[1] * rz - x3[2] * ry) - c7 * w[0] + c5 * g[G_W3V + 0];
+            u1 += (x3[2] * rx - x3[0] * rz) - c7 * w[1] + c5 * g[G_W3V + 1];
+            u2 += (x3[0] * ry - x3[1] * rx) - c7 * w[2] + c5 * g[G_W3V + 2];
+        }
     }
     ux += T(INV_FOUR_PI) * u0;
     uy += T(INV_FOUR_PI) * u1;

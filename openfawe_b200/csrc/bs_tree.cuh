@@ -29,6 +29,9 @@ struct bs_tree {
     bs::NodeRec *nodes = nullptr;
     bs::Far64 *far64 = nullptr;
     bs::Far32 *far32 = nullptr;
+    bs::Far64x *far64x = nullptr;  // third-order records (trees built for order 3 only)
+    bs::Far32x *far32x = nullptr;
+    int order3 = 0;
     bs::Seg64 *seg64 = nullptr;  // tree order
     bs::Seg32 *seg32 = nullptr;  // tree order
     uint64_t *keys = nullptr;    // Morton keys (input order), Morton trees only

@@ -23,7 +23,8 @@ namespace bs {
 
 constexpr int CHUNK = 2048;
 constexpr int MOM_THREADS = 256;
-constexpr int MOM_PARTS = 31;  // r2 + m0 (3) + m1 (9) + m2 symmetric (18)
+constexpr int MOM_PARTS = 31;   // r2 + m0 (3) + m1 (9) + m2 symmetric (18)
+constexpr int MOM_PARTS3 = 61;  // ... + m3 symmetric (30), for third-order trees
 
 __device__ __forceinline__ uint64_t ordered_bits(double x) {
     uint64_t b = (uint64_t)__double_as_longlong(x + 0.0);  // -0.0 -> +0.0 (equal keys compare equal)
@@ -761,17 +762,19 @@ __global__ void moment_centre_kernel(int64_t count, const int64_t *first, const 
     core[j] = c;
 }
 
-// Bounding radius^2 and moments (m0, m1, symmetric m2) of one chunk about its node's centre.
+// Bounding radius^2 and moments (m0, m1, symmetric m2, and for PARTS == MOM_PARTS3 symmetric m3) of one chunk about
+// its node's centre.
+template <int PARTS>
 __global__ void __launch_bounds__(MOM_THREADS) moment_sum_kernel(const Item *items, int64_t nitems,
                                                                  const int32_t *order, const SegGeo *geo,
                                                                  const double *centre, double *partial) {
-    __shared__ double red[MOM_PARTS][MOM_THREADS / 32];
+    __shared__ double red[PARTS][MOM_THREADS / 32];
     for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x) {
         Item item = items[it];
         const double c0 = centre[3 * item.node], c1 = centre[3 * item.node + 1], c2 = centre[3 * item.node + 2];
-        double acc[MOM_PARTS];
+        double acc[PARTS];
 #pragma unroll
-        for (int q = 0; q < MOM_PARTS; ++q) acc[q] = 0.0;
+        for (int q = 0; q < PARTS; ++q) acc[q] = 0.0;
         for (int k = item.start + threadIdx.x; k < item.end; k += blockDim.x) {
             SegGeo g = geo[order[k]];
             double a0 = g.sx - c0, a1 = g.sy - c1, a2 = g.sz - c2;
@@ -798,10 +801,28 @@ __global__ void __launch_bounds__(MOM_THREADS) moment_sum_kernel(const Item *ite
 #pragma unroll
                 for (int p = 0; p < 6; ++p) acc[13 + 6 * i + p] += al[i] * sym[p];
             }
+            if (PARTS == MOM_PARTS3) {
+                // <rho_j rho_k rho_l> over the segment: d_j d_k d_l + (d_j l_k l_l + l_j d_k l_l + l_j l_k d_l) / 12
+                double cub[10];
+                int q3 = 0;
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+#pragma unroll
+                    for (int k2 = j; k2 < 3; ++k2)
+#pragma unroll
+                        for (int l2 = k2; l2 < 3; ++l2)
+                            cub[q3++] = d[j] * d[k2] * d[l2] +
+                                        (d[j] * l[k2] * l[l2] + l[j] * d[k2] * l[l2] + l[j] * l[k2] * d[l2]) *
+                                            (1.0 / 12.0);
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int p = 0; p < 10; ++p) acc[31 + 10 * i + p] += al[i] * cub[p];
+            }
         }
         int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
-        for (int q = 0; q < MOM_PARTS; ++q) {
+        for (int q = 0; q < PARTS; ++q) {
             double v = acc[q];
             for (int o = 16; o > 0; o >>= 1) {
                 double w = __shfl_xor_sync(0xffffffffu, v, o);
@@ -810,30 +831,40 @@ __global__ void __launch_bounds__(MOM_THREADS) moment_sum_kernel(const Item *ite
             if (lane == 0) red[q][warp] = v;
         }
         __syncthreads();
-        if (threadIdx.x < MOM_PARTS) {
+        if (threadIdx.x < PARTS) {
             double v = red[threadIdx.x][0];
             for (int w = 1; w < MOM_THREADS / 32; ++w)
                 v = threadIdx.x == 0 ? fmax(v, red[0][w]) : v + red[threadIdx.x][w];
-            partial[(int64_t)MOM_PARTS * it + threadIdx.x] = v;
+            partial[(int64_t)PARTS * it + threadIdx.x] = v;
         }
         __syncthreads();
     }
 }
 
+// Index of the symmetric third-order component (j, k, l) in 000,001,002,011,012,022,111,112,122,222.
+__device__ __forceinline__ int sym3(int j, int k, int l) {
+    int a = j, b = k, c = l, t;
+    if (a > b) { t = a; a = b; b = t; }
+    if (b > c) { t = b; b = c; c = t; }
+    if (a > b) { t = a; a = b; b = t; }
+    return a == 0 ? (b == 0 ? c : (b == 1 ? 2 + c : 5)) : (a == 1 ? (b == 1 ? 5 + c : 8) : 9);
+}
+
 // Combine chunks in order; write the export arrays, the contractions and the packed traversal/far records.
+template <int PARTS>
 __global__ void moment_final_kernel(int64_t count, const int64_t *first, const int64_t *nitems,
                                     const double *partial, const int64_t *lo, const int64_t *hi,
                                     const int64_t *left, const int64_t *right, const double *centre,
                                     const double *core, double *bound, double *m0, double *m1, double *m2,
                                     double *w1, double *t2, double *w2, NodeRec *nodes, Far64 *far64,
-                                    Far32 *far32) {
+                                    Far32 *far32, Far64x *far64x, Far32x *far32x) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= count) return;
-    double v[MOM_PARTS];
-    for (int q = 0; q < MOM_PARTS; ++q) v[q] = 0.0;
+    double v[PARTS];
+    for (int q = 0; q < PARTS; ++q) v[q] = 0.0;
     for (int64_t it = first[j]; it < first[j] + nitems[j]; ++it)
-        for (int q = 0; q < MOM_PARTS; ++q) {
-            double p = partial[(int64_t)MOM_PARTS * it + q];
+        for (int q = 0; q < PARTS; ++q) {
+            double p = partial[(int64_t)PARTS * it + q];
             v[q] = q == 0 ? fmax(v[q], p) : v[q] + p;
         }
     double b = sqrt(v[0]) * (1.0 + 1e-12);
@@ -871,6 +902,30 @@ __global__ void moment_final_kernel(int64_t count, const int64_t *first, const i
         far64[j].v[q] = f[q];
         far32[j].v[q] = (float)f[q];
     }
+    if (PARTS == MOM_PARTS3) {
+        const double *M3 = v + 31;  // M3[10 b + sym3(j, k, l)]
+        double g[BS_FAR3_N], T3[9];
+        for (int q = 0; q < 30; ++q) g[G_M3 + q] = M3[q];
+        for (int b3 = 0; b3 < 3; ++b3)
+            for (int l3 = 0; l3 < 3; ++l3)
+                T3[3 * b3 + l3] = M3[10 * b3 + sym3(0, 0, l3)] + M3[10 * b3 + sym3(1, 1, l3)] +
+                                  M3[10 * b3 + sym3(2, 2, l3)];
+        for (int q = 0; q < 9; ++q) g[G_T3 + q] = T3[q];
+        const int kl[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+        for (int p = 0; p < 6; ++p) {
+            const int k3 = kl[p][0], l3 = kl[p][1];
+            g[G_W3 + 0 * 6 + p] = M3[10 * 1 + sym3(2, k3, l3)] - M3[10 * 2 + sym3(1, k3, l3)];
+            g[G_W3 + 1 * 6 + p] = M3[10 * 2 + sym3(0, k3, l3)] - M3[10 * 0 + sym3(2, k3, l3)];
+            g[G_W3 + 2 * 6 + p] = M3[10 * 0 + sym3(1, k3, l3)] - M3[10 * 1 + sym3(0, k3, l3)];
+        }
+        g[G_W3V + 0] = T3[3 * 1 + 2] - T3[3 * 2 + 1];
+        g[G_W3V + 1] = T3[3 * 2 + 0] - T3[3 * 0 + 2];
+        g[G_W3V + 2] = T3[3 * 0 + 1] - T3[3 * 1 + 0];
+        for (int q = 0; q < 64; ++q) {
+            far64x[j].v[q] = q < BS_FAR3_N ? g[q] : 0.0;
+            far32x[j].v[q] = q < BS_FAR3_N ? (float)g[q] : 0.f;
+        }
+    }
     NodeRec r;
     r.cx = centre[3 * j]; r.cy = centre[3 * j + 1]; r.cz = centre[3 * j + 2];
     r.bound = b;
@@ -894,6 +949,11 @@ int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_
     t->nodes = t->alloc<NodeRec>(count, s);
     t->far64 = t->alloc<Far64>(count, s);
     t->far32 = t->alloc<Far32>(count, s);
+    if (t->order3) {
+        t->far64x = t->alloc<Far64x>(count, s);
+        t->far32x = t->alloc<Far32x>(count, s);
+        if (!t->far64x || !t->far32x) return BS_ERR_OOM;
+    }
     if (!t->centre || !t->bound || !t->core || !t->m0 || !t->m1 || !t->m2 || !t->w1 || !t->t2 || !t->w2 ||
         !t->nodes || !t->far64 || !t->far32)
         return BS_ERR_OOM;
@@ -908,17 +968,24 @@ int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_
     BS_CUDA(cudaMemcpyAsync(&n_items, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     BS_CUDA(cudaStreamSynchronize(s));
     Item *items = scratch.get<Item>(n_items);
-    double *box = scratch.get<double>(7 * n_items), *sums = scratch.get<double>(MOM_PARTS * n_items);
+    const int parts = t->order3 ? MOM_PARTS3 : MOM_PARTS;
+    double *box = scratch.get<double>(7 * n_items), *sums = scratch.get<double>((size_t)parts * n_items);
     if (!items || !box || !sums) return scratch.status;
     item_fill_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->lo, t->hi, first, items);
     unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(n_items, 8192));
     moment_box_kernel<<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, box);
     moment_centre_kernel<<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, box, t->centre, t->core);
-    moment_sum_kernel<<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, t->centre, sums);
-    moment_final_kernel<<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, sums, t->lo, t->hi, t->left,
-                                                               t->right, t->centre, t->core, t->bound, t->m0, t->m1,
-                                                               t->m2, t->w1, t->t2, t->w2, t->nodes, t->far64,
-                                                               t->far32);
+    if (t->order3) {
+        moment_sum_kernel<MOM_PARTS3><<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, t->centre, sums);
+        moment_final_kernel<MOM_PARTS3><<<blocks_for(count, 128), 128, 0, s>>>(
+            count, first, nitems, sums, t->lo, t->hi, t->left, t->right, t->centre, t->core, t->bound, t->m0, t->m1,
+            t->m2, t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x);
+    } else {
+        moment_sum_kernel<MOM_PARTS><<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, t->centre, sums);
+        moment_final_kernel<MOM_PARTS><<<blocks_for(count, 128), 128, 0, s>>>(
+            count, first, nitems, sums, t->lo, t->hi, t->left, t->right, t->centre, t->core, t->bound, t->m0, t->m1,
+            t->m2, t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, nullptr, nullptr);
+    }
     BS_CHECK_LAUNCH("moments");
     return BS_OK;
 }
@@ -996,6 +1063,7 @@ extern "C" int bs_tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_p
     t->kind = tp->kind;
     t->m = src->m;
     t->leaf_size = tp->leaf_size;
+    t->order3 = tp->order >= 3;
     {
         Scratch scratch(ctx->pool, s);
         SegGeo *geo = scratch.get<SegGeo>(src->m);
@@ -1054,6 +1122,7 @@ extern "C" int bs_forest_build(bs_ctx *ctx, const bs_sources *src, int nwakes, c
     t->kind = BS_TREE_MORTON;
     t->m = src->m;
     t->leaf_size = tp->leaf_size;
+    t->order3 = tp->order >= 3;
     {
         Scratch scratch(ctx->pool, s);
         SegGeo *geo = scratch.get<SegGeo>(src->m);
@@ -1149,6 +1218,174 @@ extern "C" int bs_tree_from_arrays(bs_ctx *ctx, const bs_sources *src, const int
     return rc;
 }
 
+__global__ void widen_keys_order_kernel(int64_t m, const int32_t *order32, int64_t *out) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) out[k] = order32[k];
+}
+
+// bad[0] = 1 if an order entry lies outside [0, m) or a node range outside 0 <= lo <= hi <= m
+__global__ void topology_check_kernel(int64_t m, int64_t count, const int64_t *order, const int64_t *lo,
+                                      const int64_t *hi, int *bad) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m && (order[k] < 0 || order[k] >= m)) *bad = 1;
+    if (k < count && (lo[k] < 0 || lo[k] > hi[k] || hi[k] > m)) *bad = 1;
+}
+
+__global__ void geo_from_mid_kernel(int64_t m, const double *mid, SegGeo *geo) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    // start = end = mid, so that 0.5 * (start + end) is mid exactly
+    SegGeo q;
+    q.sx = q.ex = mid[3 * k];
+    q.sy = q.ey = mid[3 * k + 1];
+    q.sz = q.ez = mid[3 * k + 2];
+    q.lx = q.ly = q.lz = 0.0;
+    q.gamma = q.radius = q.pad = 0.0;
+    geo[k] = q;
+}
+
+__global__ void geo_from_ends_kernel(int64_t m, const double *starts, const double *ends, const double *lv,
+                                     const double *gamma, const double *radius, SegGeo *geo) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    SegGeo q;
+    q.sx = starts[3 * k]; q.sy = starts[3 * k + 1]; q.sz = starts[3 * k + 2];
+    q.ex = ends[3 * k]; q.ey = ends[3 * k + 1]; q.ez = ends[3 * k + 2];
+    q.lx = lv[3 * k]; q.ly = lv[3 * k + 1]; q.lz = lv[3 * k + 2];
+    q.gamma = gamma[k];
+    q.radius = radius[k];
+    q.pad = 0.0;
+    geo[k] = q;
+}
+
+extern "C" int bs_median_topology(bs_ctx *ctx, int64_t m, const double *mid, int leaf_size, int64_t *order,
+                                  int64_t *lo, int64_t *hi, int64_t *left, int64_t *right, int64_t capacity,
+                                  int64_t *count, bs_stream stream) {
+    if (!ctx || !count || m < 0 || (m > 0 && (!mid || !order)) || leaf_size < 1 || capacity < 0 ||
+        (capacity > 0 && (!lo || !hi || !left || !right))) {
+        set_error("bs_median_topology: null or negative argument");
+        return BS_ERR_ARG;
+    }
+    if (m >= (int64_t(1) << 31) - 1) {
+        set_error("bs_median_topology: at most 2^31 - 2 midpoints");
+        return BS_ERR_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    BS_CUDA(cudaSetDevice(ctx->device));
+    if (m == 0) {  // one empty leaf, as build_tree returns for no segments
+        *count = 1;
+        if (capacity >= 1) {
+            const int64_t row[4] = {0, 0, -1, -1};
+            BS_CUDA(cudaMemcpyAsync(lo, row, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+            BS_CUDA(cudaMemcpyAsync(hi, row + 1, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+            BS_CUDA(cudaMemcpyAsync(left, row + 2, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+            BS_CUDA(cudaMemcpyAsync(right, row + 3, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+            BS_CUDA(cudaStreamSynchronize(s));
+        }
+        return BS_OK;
+    }
+    bs_tree *t = new bs_tree();
+    t->device = ctx->device;
+    t->pool = ctx->pool;
+    t->kind = BS_TREE_MEDIAN;
+    t->m = m;
+    t->leaf_size = leaf_size;
+    int rc = BS_OK;
+    {
+        Scratch scratch(ctx->pool, s);
+        SegGeo *geo = scratch.get<SegGeo>(m);
+        if (!geo) rc = scratch.status;
+        if (rc == BS_OK) {
+            geo_from_mid_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, mid, geo);
+            BS_CHECK_LAUNCH("geo_from_mid_kernel");
+            rc = build_median(t, geo, scratch, s);
+        }
+        if (rc == BS_OK) {
+            *count = t->count;
+            widen_keys_order_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, t->order32, order);
+            BS_CHECK_LAUNCH("widen_keys_order_kernel");
+            if (t->count <= capacity) {
+                const size_t c8 = (size_t)t->count * sizeof(int64_t);
+                cudaMemcpyAsync(lo, t->lo, c8, cudaMemcpyDeviceToDevice, s);
+                cudaMemcpyAsync(hi, t->hi, c8, cudaMemcpyDeviceToDevice, s);
+                cudaMemcpyAsync(left, t->left, c8, cudaMemcpyDeviceToDevice, s);
+                cudaMemcpyAsync(right, t->right, c8, cudaMemcpyDeviceToDevice, s);
+            }
+            cudaError_t e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) rc = cuda_fail(e, "bs_median_topology");
+        }
+    }
+    bs_tree_free(t);
+    return rc;
+}
+
+extern "C" int bs_node_quantities(bs_ctx *ctx, int64_t m, const double *starts, const double *ends,
+                                  const double *length_vectors, const double *gamma, const double *radius,
+                                  int64_t count, const int64_t *order, const int64_t *lo, const int64_t *hi,
+                                  double *centre, double *bound, double *core, double *m0, double *m1, double *m2,
+                                  double *w1, double *t2, double *w2, bs_stream stream) {
+    if (!ctx || m < 1 || count < 1 || !starts || !ends || !length_vectors || !gamma || !radius || !order || !lo ||
+        !hi) {
+        set_error("bs_node_quantities: null argument or empty tree");
+        return BS_ERR_ARG;
+    }
+    if (m >= (int64_t(1) << 31) - 1) {
+        set_error("bs_node_quantities: at most 2^31 - 2 segments");
+        return BS_ERR_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    BS_CUDA(cudaSetDevice(ctx->device));
+    bs_tree *t = new bs_tree();
+    t->device = ctx->device;
+    t->pool = ctx->pool;
+    t->kind = -1;
+    t->m = m;
+    t->count = count;
+    int rc = BS_OK;
+    {
+        Scratch scratch(ctx->pool, s);
+        SegGeo *geo = scratch.get<SegGeo>(m);
+        t->order32 = t->alloc<int32_t>(m, s);
+        t->lo = t->alloc<int64_t>(count, s);
+        t->hi = t->alloc<int64_t>(count, s);
+        t->left = t->alloc<int64_t>(count, s);
+        t->right = t->alloc<int64_t>(count, s);
+        int *bad = scratch.get<int>(1);
+        if (!geo || !bad || !t->order32 || !t->lo || !t->hi || !t->left || !t->right) rc = BS_ERR_OOM;
+        if (rc == BS_OK) {
+            int host_bad = 0;
+            cudaMemsetAsync(bad, 0, sizeof(int), s);
+            topology_check_kernel<<<blocks_for(std::max(m, count), 256), 256, 0, s>>>(m, count, order, lo, hi, bad);
+            cudaMemcpyAsync(&host_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, s);
+            cudaError_t e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) rc = cuda_fail(e, "bs_node_quantities");
+            else if (host_bad) {
+                set_error("bs_node_quantities: order entry outside [0, m) or node range outside 0 <= lo <= hi <= m");
+                rc = BS_ERR_ARG;
+            }
+        }
+        if (rc == BS_OK) {
+            cudaMemcpyAsync(t->lo, lo, count * sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(t->hi, hi, count * sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
+            cudaMemsetAsync(t->left, 0xff, count * sizeof(int64_t), s);
+            cudaMemsetAsync(t->right, 0xff, count * sizeof(int64_t), s);
+            narrow_order_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, order, t->order32);
+            geo_from_ends_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, starts, ends, length_vectors, gamma, radius,
+                                                                    geo);
+            BS_CHECK_LAUNCH("geo_from_ends_kernel");
+            rc = compute_moments(t, geo, scratch, s);
+        }
+        if (rc == BS_OK) {
+            rc = bs_tree_export(t, nullptr, nullptr, nullptr, nullptr, nullptr, centre, bound, core, m0, m1, m2, w1,
+                                t2, w2, stream);
+            cudaError_t e = cudaStreamSynchronize(s);
+            if (rc == BS_OK && e != cudaSuccess) rc = cuda_fail(e, "bs_node_quantities");
+        }
+    }
+    bs_tree_free(t);
+    return rc;
+}
+
 extern "C" int bs_tree_export(const bs_tree *t, int64_t *order, int64_t *lo, int64_t *hi, int64_t *left,
                               int64_t *right, double *centre, double *bound, double *core, double *m0, double *m1,
                               double *m2, double *w1, double *t2, double *w2, bs_stream stream) {
@@ -1166,11 +1403,6 @@ extern "C" int bs_tree_export(const bs_tree *t, int64_t *order, int64_t *lo, int
     for (auto &cp : copies)
         if (cp.dst) BS_CUDA(cudaMemcpyAsync(cp.dst, cp.src, cp.bytes, cudaMemcpyDeviceToDevice, s));
     return BS_OK;
-}
-
-__global__ void widen_keys_order_kernel(int64_t m, const int32_t *order32, int64_t *out) {
-    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < m) out[k] = order32[k];
 }
 
 extern "C" int bs_tree_keys(const bs_tree *t, uint64_t *keys, int64_t *sorted_order, bs_stream stream) {

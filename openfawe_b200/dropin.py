@@ -10,26 +10,62 @@ import sys
 
 
 def install(package="openfawe.aero"):
-    """Register ``openfawe_b200.vortex_cuda`` / ``vortex_cuda_tree`` as ``<package>.vortex_cuda`` / ``..._tree``.
+    """Register ``openfawe_b200.vortex_cuda`` / ``vortex_cuda_tree`` / ``vortex_cuda_moments`` / ``vortex_cuda_build``
+    under ``<package>``.
 
     Returns the two modules.  Call it before the first GPU-backend call of the process (or after, since the reference
     imports them inside each call)."""
-    from . import vortex_cuda, vortex_cuda_tree
-    sys.modules[package + ".vortex_cuda"] = vortex_cuda
-    sys.modules[package + ".vortex_cuda_tree"] = vortex_cuda_tree
+    from . import vortex_cuda, vortex_cuda_build, vortex_cuda_moments, vortex_cuda_tree
+    modules = dict(vortex_cuda=vortex_cuda, vortex_cuda_tree=vortex_cuda_tree, vortex_cuda_moments=vortex_cuda_moments,
+                   vortex_cuda_build=vortex_cuda_build)
     parent = sys.modules.get(package)
-    if parent is not None:
-        setattr(parent, "vortex_cuda", vortex_cuda)
-        setattr(parent, "vortex_cuda_tree", vortex_cuda_tree)
+    for name, module in modules.items():
+        sys.modules[f"{package}.{name}"] = module
+        if parent is not None:
+            setattr(parent, name, module)
     return vortex_cuda, vortex_cuda_tree
 
 
 def uninstall(package="openfawe.aero"):
     """Remove the registrations made by ``install``."""
-    for name in ("vortex_cuda", "vortex_cuda_tree"):
+    for name in ("vortex_cuda", "vortex_cuda_tree", "vortex_cuda_moments", "vortex_cuda_build"):
         module = sys.modules.get(f"{package}.{name}")
         if module is not None and module.__name__.startswith("openfawe_b200."):
             del sys.modules[f"{package}.{name}"]
             parent = sys.modules.get(package)
             if parent is not None and getattr(parent, name, None) is module:
                 delattr(parent, name)
+
+
+# Functions of the reference's compiled bookkeeping modules that this library replaces one for one, with the modules
+# that bind them by name (ring_wake imports incident_pairs at import time, src/openfawe/rotor/ring_wake.py:17).
+FUNCTIONS = {
+    "aero.network_numba": {"incident_pairs": ("network", "incident_pairs")},
+    "aero.vortex_numba": {"exclusion_csr": ("network", "exclusion_csr"),
+                          "pair_matrix": ("operators", "pair_matrix"),
+                          "assemble_columns": ("operators", "assemble_columns")},
+    "rotor.ring_wake": {"incident_pairs": ("network", "incident_pairs")},
+}
+
+
+def patch_functions(root="openfawe"):
+    """Point the already-imported reference modules' ``incident_pairs``, ``exclusion_csr``, ``pair_matrix`` and
+    ``assemble_columns`` at this library's GPU versions (same signatures and results).  Modules not imported yet are
+    skipped (import them first).  Returns the replaced originals for ``unpatch_functions``."""
+    import importlib
+    saved = []
+    for module_name, names in FUNCTIONS.items():
+        module = sys.modules.get(f"{root}.{module_name}")
+        if module is None:
+            continue
+        for name, (ours, attr) in names.items():
+            if hasattr(module, name):
+                saved.append((module, name, getattr(module, name)))
+                setattr(module, name, getattr(importlib.import_module(f"{__package__}.{ours}"), attr))
+    return saved
+
+
+def unpatch_functions(saved):
+    """Restore what ``patch_functions`` replaced."""
+    for module, name, original in reversed(saved):
+        setattr(module, name, original)

@@ -208,11 +208,11 @@ def last_stats(device=0):
 # ---------------------------------------------------------------------------------------------------------------------
 # Forests: many wakes in one tree (batched evaluation).
 # ---------------------------------------------------------------------------------------------------------------------
-def build_forest(sources, wake_ptr, leaf_size=32):
+def build_forest(sources, wake_ptr, leaf_size=32, order=2):
     """One Morton tree over concatenated wakes; wake w owns segments [wake_ptr[w], wake_ptr[w+1])."""
     dev = sources.device
     ptr = i64(wake_ptr, dev)
-    params = tree_params(0.5, 2, leaf_size, 3.0, "morton")
+    params = tree_params(0.5, order, leaf_size, 3.0, "morton")
     handle = ctypes.c_void_p()
     src = sources.struct()
     L.check(L.library().bs_forest_build(L.context(dev.index), ctypes.byref(src), int(ptr.numel() - 1), _ptr(ptr),

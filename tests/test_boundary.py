@@ -108,3 +108,40 @@ def test_wake_generators_shapes():
     assert len(c2["starts"]) == 219 * 468 - 46 and len(c2["points"]) == 20570 and c2["model"] == 2
     s = wakes.selftest_sheet(468, seed=468)
     assert len(s["starts"]) == 102382 and len(s["points"]) == 20570
+
+
+def test_install_registers_build_and_moments_modules_and_patches_functions():
+    import types
+    import openfawe_b200
+    from openfawe_b200 import dropin, network, operators
+    openfawe_b200.install("fakepkg2.aero")
+    try:
+        assert sys.modules["fakepkg2.aero.vortex_cuda_moments"].__name__ == "openfawe_b200.vortex_cuda_moments"
+        assert sys.modules["fakepkg2.aero.vortex_cuda_build"].__name__ == "openfawe_b200.vortex_cuda_build"
+    finally:
+        openfawe_b200.uninstall("fakepkg2.aero")
+    assert "fakepkg2.aero.vortex_cuda_build" not in sys.modules
+    # stand-ins for the reference's compiled modules, already imported
+    fakes = {name: types.ModuleType(name) for name in ("fk.aero.network_numba", "fk.aero.vortex_numba",
+                                                       "fk.rotor.ring_wake")}
+    originals = {}
+    for name, module in fakes.items():
+        for fn in ("incident_pairs", "exclusion_csr", "pair_matrix", "assemble_columns"):
+            original = (lambda *a: None)
+            setattr(module, fn, original)
+            originals[(name, fn)] = original
+        sys.modules[name] = module
+    try:
+        saved = dropin.patch_functions("fk")
+        assert fakes["fk.aero.network_numba"].incident_pairs is network.incident_pairs
+        assert fakes["fk.rotor.ring_wake"].incident_pairs is network.incident_pairs
+        assert fakes["fk.aero.vortex_numba"].exclusion_csr is network.exclusion_csr
+        assert fakes["fk.aero.vortex_numba"].pair_matrix is operators.pair_matrix
+        assert fakes["fk.aero.vortex_numba"].assemble_columns is operators.assemble_columns
+        # names this library does not replace stay as they were
+        assert fakes["fk.aero.network_numba"].exclusion_csr is originals[("fk.aero.network_numba", "exclusion_csr")]
+        dropin.unpatch_functions(saved)
+        assert fakes["fk.aero.vortex_numba"].pair_matrix is originals[("fk.aero.vortex_numba", "pair_matrix")]
+    finally:
+        for name in fakes:
+            del sys.modules[name]
