@@ -697,10 +697,11 @@ __global__ void item_count_kernel(int64_t count, const int64_t *lo, const int64_
     n[j] = size > 0 ? (size + CHUNK - 1) / CHUNK : 0;
 }
 
+// Items (chunks of CHUNK positions) of every node, or with `left` of the internal nodes only.
 __global__ void item_fill_kernel(int64_t count, const int64_t *lo, const int64_t *hi, const int64_t *first,
-                                 Item *items) {
+                                 Item *items, const int64_t *left = nullptr) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= count) return;
+    if (j >= count || (left && left[j] < 0)) return;
     int64_t k = first[j];
     for (int64_t c = lo[j]; c < hi[j]; c += CHUNK, ++k)
         items[k] = {(int32_t)j, (int32_t)c, (int32_t)min(hi[j], c + CHUNK), 0};
@@ -850,23 +851,30 @@ __device__ __forceinline__ int sym3(int j, int k, int l) {
     return a == 0 ? (b == 0 ? c : (b == 1 ? 2 + c : 5)) : (a == 1 ? (b == 1 ? 5 + c : 8) : 9);
 }
 
-// Combine chunks in order; write the export arrays, the contractions and the packed traversal/far records.
+// The outputs of the moment pipelines for one node.
+struct NodeOut {
+    const int64_t *lo, *hi, *left, *right;
+    const double *centre, *core;
+    double *bound, *m0, *m1, *m2, *w1, *t2, *w2;
+    NodeRec *nodes;
+    Far64 *far64;
+    Far32 *far32;
+    Far64x *far64x;
+    Far32x *far32x;
+};
+
+// Node j from its sums v (bound^2, m0, m1, symmetric m2 [, symmetric m3]) about its centre: the export arrays, the
+// contractions and the packed traversal / far records.
 template <int PARTS>
-__global__ void moment_final_kernel(int64_t count, const int64_t *first, const int64_t *nitems,
-                                    const double *partial, const int64_t *lo, const int64_t *hi,
-                                    const int64_t *left, const int64_t *right, const double *centre,
-                                    const double *core, double *bound, double *m0, double *m1, double *m2,
-                                    double *w1, double *t2, double *w2, NodeRec *nodes, Far64 *far64,
-                                    Far32 *far32, Far64x *far64x, Far32x *far32x) {
-    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= count) return;
-    double v[PARTS];
-    for (int q = 0; q < PARTS; ++q) v[q] = 0.0;
-    for (int64_t it = first[j]; it < first[j] + nitems[j]; ++it)
-        for (int q = 0; q < PARTS; ++q) {
-            double p = partial[(int64_t)PARTS * it + q];
-            v[q] = q == 0 ? fmax(v[q], p) : v[q] + p;
-        }
+__device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
+    double *bound = o.bound, *m0 = o.m0, *m1 = o.m1, *m2 = o.m2, *w1 = o.w1, *t2 = o.t2, *w2 = o.w2;
+    Far64 *far64 = o.far64;
+    Far32 *far32 = o.far32;
+    Far64x *far64x = o.far64x;
+    Far32x *far32x = o.far32x;
+    const double *centre = o.centre, *core = o.core;
+    const int64_t *lo = o.lo, *hi = o.hi, *left = o.left, *right = o.right;
+    NodeRec *nodes = o.nodes;
     double b = sqrt(v[0]) * (1.0 + 1e-12);
     bound[j] = b;
     const double *M0 = v + 1, *M1 = v + 4, *S = v + 13;  // S[6 i + p], p over (00,01,02,11,12,22)
@@ -935,6 +943,327 @@ __global__ void moment_final_kernel(int64_t count, const int64_t *first, const i
     nodes[j] = r;
 }
 
+// Combine a node's chunks in order, then finalize it.
+template <int PARTS>
+__global__ void moment_final_kernel(int64_t count, const int64_t *first, const int64_t *nitems,
+                                    const double *partial, NodeOut o) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    double v[PARTS];
+    for (int q = 0; q < PARTS; ++q) v[q] = 0.0;
+    for (int64_t it = first[j]; it < first[j] + nitems[j]; ++it)
+        for (int q = 0; q < PARTS; ++q) {
+            double p = partial[(int64_t)PARTS * it + q];
+            v[q] = q == 0 ? fmax(v[q], p) : v[q] + p;
+        }
+    finalize_node<PARTS>(j, v, o);
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Bottom-up moments (Morton trees and forests).  Leaves sum their own segments; an internal node takes its box and
+// core from its children (exact) and its moments by translating the children's to its centre
+//   m1_ij += m0_i D_j,  m2_ijk += m1_ij D_k + m1_ik D_j + m0_i D_j D_k,
+//   m3_ijkl += D_j m2_ikl + D_k m2_ijl + D_l m2_ijk + D_j D_k m1_il + D_j D_l m1_ik + D_k D_l m1_ij + D_j D_k D_l m0_i
+// (D = child centre - node centre; left child first, then right), which equals the direct sums up to rounding.  The
+// bounding radius stays exact: one pass over the internal nodes' ranges of tree-ordered endpoints.
+// ---------------------------------------------------------------------------------------------------------------------
+struct __align__(16) EndPts {
+    double sx, sy, sz, ex, ey, ez;
+};
+
+__global__ void sorted_ends_kernel(int64_t m, const int32_t *order, const SegGeo *geo, EndPts *ends) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    const SegGeo g = geo[order[k]];
+    ends[k] = EndPts{g.sx, g.sy, g.sz, g.ex, g.ey, g.ez};
+}
+
+__global__ void parent_kernel(int64_t count, const int64_t *left, const int64_t *right, int32_t *parent) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    if (j == 0) parent[0] = -1;
+    if (left[j] >= 0) {
+        parent[left[j]] = (int32_t)j;
+        parent[right[j]] = (int32_t)j;
+    }
+}
+
+// Adds one segment's bound^2 and moments about (c0, c1, c2) to acc (the accumulation of moment_sum_kernel).
+template <int PARTS>
+__device__ __forceinline__ void accumulate_segment(const SegGeo &g, double c0, double c1, double c2, double *acc) {
+    double a0 = g.sx - c0, a1 = g.sy - c1, a2 = g.sz - c2;
+    double b0 = g.ex - c0, b1 = g.ey - c1, b2 = g.ez - c2;
+    double ra = __dadd_rn(__dadd_rn(__dmul_rn(a0, a0), __dmul_rn(a1, a1)), __dmul_rn(a2, a2));
+    double rb = __dadd_rn(__dadd_rn(__dmul_rn(b0, b0), __dmul_rn(b1, b1)), __dmul_rn(b2, b2));
+    acc[0] = fmax(acc[0], fmax(ra, rb));
+    if (g.gamma == 0.0) return;
+    double d[3] = {0.5 * (g.sx + g.ex) - c0, 0.5 * (g.sy + g.ey) - c1, 0.5 * (g.sz + g.ez) - c2};
+    double l[3] = {g.lx, g.ly, g.lz};
+    double al[3] = {g.gamma * g.lx, g.gamma * g.ly, g.gamma * g.lz};
+    double sym[6];
+    int q = 0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int k2 = j; k2 < 3; ++k2) sym[q++] = d[j] * d[k2] + l[j] * l[k2] * (1.0 / 12.0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        acc[1 + i] += al[i];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) acc[4 + 3 * i + j] += al[i] * d[j];
+#pragma unroll
+        for (int p = 0; p < 6; ++p) acc[13 + 6 * i + p] += al[i] * sym[p];
+    }
+    if (PARTS == MOM_PARTS3) {
+        double cub[10];
+        int q3 = 0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k2 = j; k2 < 3; ++k2)
+#pragma unroll
+                for (int l2 = k2; l2 < 3; ++l2)
+                    cub[q3++] = d[j] * d[k2] * d[l2] +
+                                (d[j] * l[k2] * l[l2] + l[j] * d[k2] * l[l2] + l[j] * l[k2] * d[l2]) * (1.0 / 12.0);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int p = 0; p < 10; ++p) acc[31 + 10 * i + p] += al[i] * cub[p];
+    }
+}
+
+// One warp per leaf: box, core and centre, then bound^2 and moments about the centre; sums[j][PARTS].
+template <int PARTS>
+__global__ void __launch_bounds__(128) leaf_moments_kernel(int64_t count, const int64_t *lo, const int64_t *hi,
+                                                           const int64_t *left, const int32_t *order,
+                                                           const SegGeo *geo, double *box, double *centre,
+                                                           double *core, double *sums) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t j = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); j < count; j += warps) {
+        if (left[j] >= 0) continue;
+        const int64_t a = lo[j], b = hi[j];
+        double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY}, c = 0.0;
+        for (int64_t k = a + lane; k < b; k += 32) {
+            const SegGeo g = geo[order[k]];
+            mn[0] = fmin(mn[0], fmin(g.sx, g.ex)); mx[0] = fmax(mx[0], fmax(g.sx, g.ex));
+            mn[1] = fmin(mn[1], fmin(g.sy, g.ey)); mx[1] = fmax(mx[1], fmax(g.sy, g.ey));
+            mn[2] = fmin(mn[2], fmin(g.sz, g.ez)); mx[2] = fmax(mx[2], fmax(g.sz, g.ez));
+            c = fmax(c, g.radius);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            for (int x = 0; x < 3; ++x) {
+                mn[x] = fmin(mn[x], __shfl_xor_sync(0xffffffffu, mn[x], o));
+                mx[x] = fmax(mx[x], __shfl_xor_sync(0xffffffffu, mx[x], o));
+            }
+            c = fmax(c, __shfl_xor_sync(0xffffffffu, c, o));
+        }
+        const double c0 = 0.5 * (mn[0] + mx[0]), c1 = 0.5 * (mn[1] + mx[1]), c2 = 0.5 * (mn[2] + mx[2]);
+        double acc[PARTS];
+#pragma unroll
+        for (int q = 0; q < PARTS; ++q) acc[q] = 0.0;
+        for (int64_t k = a + lane; k < b; k += 32) accumulate_segment<PARTS>(geo[order[k]], c0, c1, c2, acc);
+#pragma unroll
+        for (int q = 0; q < PARTS; ++q) {
+            double v = acc[q];
+            for (int o = 16; o > 0; o >>= 1) {
+                double w = __shfl_xor_sync(0xffffffffu, v, o);
+                v = q == 0 ? fmax(v, w) : v + w;
+            }
+            acc[q] = v;
+        }
+#pragma unroll
+        for (int q = 0; q < PARTS; ++q)
+            if (lane == (q & 31)) sums[(int64_t)PARTS * j + q] = acc[q];
+        if (lane == 0) {
+            for (int x = 0; x < 3; ++x) {
+                box[6 * j + x] = mn[x];
+                box[6 * j + 3 + x] = mx[x];
+            }
+            centre[3 * j] = c0;
+            centre[3 * j + 1] = c1;
+            centre[3 * j + 2] = c2;
+            core[j] = c;
+        }
+    }
+}
+
+// Adds the child's moments (about its centre cc) translated to the centre c into v (v[0], bound^2, untouched).
+template <int PARTS>
+__device__ __forceinline__ void add_translated(const double *w, const double *cc, const double *c, double *v) {
+    const double D[3] = {cc[0] - c[0], cc[1] - c[1], cc[2] - c[2]};
+    const double *M0 = w + 1, *M1 = w + 4, *S = w + 13;
+    auto S2 = [&](int i, int a, int b) -> double {
+        int x = a < b ? a : b, y = a < b ? b : a;
+        return S[6 * i + (x == 0 ? y : (x == 1 ? 2 + y : 5))];
+    };
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        v[1 + i] += M0[i];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) v[4 + 3 * i + j] += M1[3 * i + j] + M0[i] * D[j];
+        int p = 0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = j; k < 3; ++k, ++p)
+                v[13 + 6 * i + p] += S[6 * i + p] + M1[3 * i + j] * D[k] + M1[3 * i + k] * D[j] + M0[i] * D[j] * D[k];
+        if (PARTS == MOM_PARTS3) {
+            const double *M3 = w + 31;
+            int q = 0;
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+#pragma unroll
+                for (int k = j; k < 3; ++k)
+#pragma unroll
+                    for (int l = k; l < 3; ++l, ++q)
+                        v[31 + 10 * i + q] += M3[10 * i + q] + D[j] * S2(i, k, l) + D[k] * S2(i, j, l) +
+                                              D[l] * S2(i, j, k) + D[j] * D[k] * M1[3 * i + l] +
+                                              D[j] * D[l] * M1[3 * i + k] + D[k] * D[l] * M1[3 * i + j] +
+                                              D[j] * D[k] * D[l] * M0[i];
+        }
+    }
+}
+
+// One thread per leaf climbs towards the root; at each parent the second of the two arriving threads combines the
+// children (their results were published before the arrival count moved), so every internal node is combined exactly
+// once, from its left then its right child.  No thread waits for another.
+template <int PARTS>
+__global__ void bottom_up_kernel(int64_t count, const int64_t *left, const int64_t *right, const int32_t *parent,
+                                 unsigned *arrive, double *box, double *centre, double *core, double *sums) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count || left[j] >= 0) return;
+    int64_t node = j;
+    for (int depth = 0; depth < 4096; ++depth) {
+        const int32_t p = parent[node];
+        if (p < 0) return;
+        __threadfence();
+        if (atomicAdd(&arrive[p], 1u) == 0) return;
+        __threadfence();
+        const int64_t l = left[p], r = right[p];
+        double mn[3], mx[3];
+        for (int x = 0; x < 3; ++x) {
+            mn[x] = fmin(__ldcg(box + 6 * l + x), __ldcg(box + 6 * r + x));
+            mx[x] = fmax(__ldcg(box + 6 * l + 3 + x), __ldcg(box + 6 * r + 3 + x));
+        }
+        const double c[3] = {0.5 * (mn[0] + mx[0]), 0.5 * (mn[1] + mx[1]), 0.5 * (mn[2] + mx[2])};
+        double v[PARTS];
+#pragma unroll
+        for (int q = 0; q < PARTS; ++q) v[q] = 0.0;
+        double w[PARTS], cc[3];
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const int64_t ch = side == 0 ? l : r;
+#pragma unroll
+            for (int q = 0; q < PARTS; ++q) w[q] = __ldcg(sums + (int64_t)PARTS * ch + q);
+            for (int x = 0; x < 3; ++x) cc[x] = __ldcg(centre + 3 * ch + x);
+            add_translated<PARTS>(w, cc, c, v);
+        }
+        for (int q = 1; q < PARTS; ++q) sums[(int64_t)PARTS * p + q] = v[q];
+        for (int x = 0; x < 3; ++x) {
+            box[6 * p + x] = mn[x];
+            box[6 * p + 3 + x] = mx[x];
+            centre[3 * p + x] = c[x];
+        }
+        core[p] = fmax(__ldcg(core + l), __ldcg(core + r));
+        node = p;
+    }
+}
+
+// Bound^2 of one chunk of an internal node's range from the tree-ordered endpoints.
+__global__ void __launch_bounds__(MOM_THREADS) bound_chunk_kernel(const Item *items, int64_t nitems,
+                                                                  const EndPts *ends, const double *centre,
+                                                                  double *partial) {
+    __shared__ double red[MOM_THREADS / 32];
+    for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+        Item item = items[it];
+        const double c0 = centre[3 * item.node], c1 = centre[3 * item.node + 1], c2 = centre[3 * item.node + 2];
+        double r2 = 0.0;
+        for (int k = item.start + threadIdx.x; k < item.end; k += blockDim.x) {
+            const EndPts e = ends[k];
+            const double a0 = e.sx - c0, a1 = e.sy - c1, a2 = e.sz - c2;
+            const double b0 = e.ex - c0, b1 = e.ey - c1, b2 = e.ez - c2;
+            const double ra = __dadd_rn(__dadd_rn(__dmul_rn(a0, a0), __dmul_rn(a1, a1)), __dmul_rn(a2, a2));
+            const double rb = __dadd_rn(__dadd_rn(__dmul_rn(b0, b0), __dmul_rn(b1, b1)), __dmul_rn(b2, b2));
+            r2 = fmax(r2, fmax(ra, rb));
+        }
+        for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r2;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double v = red[0];
+            for (int w = 1; w < MOM_THREADS / 32; ++w) v = fmax(v, red[w]);
+            partial[it] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// Internal node: bound^2 = the max of its chunks; then finalize every node from its sums.
+template <int PARTS>
+__global__ void node_final_kernel(int64_t count, const int64_t *first, const int64_t *nitems, const double *partial,
+                                  double *sums, NodeOut o) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    double v[PARTS];
+    for (int q = 0; q < PARTS; ++q) v[q] = sums[(int64_t)PARTS * j + q];
+    if (o.left[j] >= 0) {
+        double r2 = 0.0;
+        for (int64_t it = first[j]; it < first[j] + nitems[j]; ++it) r2 = fmax(r2, partial[it]);
+        v[0] = r2;
+    }
+    finalize_node<PARTS>(j, v, o);
+}
+
+__global__ void internal_item_count_kernel(int64_t count, const int64_t *lo, const int64_t *hi, const int64_t *left,
+                                           int64_t *n) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    int64_t size = hi[j] - lo[j];
+    n[j] = (left[j] >= 0 && size > 0) ? (size + CHUNK - 1) / CHUNK : 0;
+}
+
+// Bottom-up pipeline: leaves, then internal nodes from their children, then the exact bounds, then the records.
+template <int PARTS>
+static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_t s) {
+    const int64_t count = t->count, m = t->m;
+    double *box = scratch.get<double>(6 * count), *sums = scratch.get<double>((size_t)PARTS * count);
+    int32_t *parent = scratch.get<int32_t>(count);
+    unsigned *arrive = scratch.get<unsigned>(count);
+    EndPts *ends = scratch.get<EndPts>(m);
+    int64_t *nitems = scratch.get<int64_t>(count), *first = scratch.get<int64_t>(count);
+    int64_t *total = scratch.get<int64_t>(1);
+    if (!box || !sums || !parent || !arrive || !ends || !nitems || !first || !total) return scratch.status;
+    BS_CUDA(cudaMemsetAsync(arrive, 0, count * sizeof(unsigned), s));
+    parent_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->left, t->right, parent);
+    sorted_ends_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, t->order32, geo, ends);
+    const unsigned leaf_blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((count + 3) / 4, 148 * 16));
+    leaf_moments_kernel<PARTS><<<leaf_blocks, 128, 0, s>>>(count, t->lo, t->hi, t->left, t->order32, geo, box,
+                                                            t->centre, t->core, sums);
+    bottom_up_kernel<PARTS><<<blocks_for(count, 128), 128, 0, s>>>(count, t->left, t->right, parent, arrive, box,
+                                                                    t->centre, t->core, sums);
+    internal_item_count_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->lo, t->hi, t->left, nitems);
+    BS_CHECK_LAUNCH("bottom-up moments");
+    int rc = scan_exclusive(nitems, first, count, total, scratch, s);
+    if (rc != BS_OK) return rc;
+    int64_t n_items = 0;
+    BS_CUDA(cudaMemcpyAsync(&n_items, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    BS_CUDA(cudaStreamSynchronize(s));
+    Item *items = scratch.get<Item>(std::max<int64_t>(n_items, 1));
+    double *partial = scratch.get<double>(std::max<int64_t>(n_items, 1));
+    if (!items || !partial) return scratch.status;
+    if (n_items > 0) {
+        item_fill_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->lo, t->hi, first, items, t->left);
+        unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(n_items, 8192));
+        bound_chunk_kernel<<<grid, MOM_THREADS, 0, s>>>(items, n_items, ends, t->centre, partial);
+    }
+    const NodeOut out{t->lo, t->hi, t->left, t->right, t->centre, t->core, t->bound, t->m0, t->m1, t->m2,
+                      t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x};
+    node_final_kernel<PARTS><<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, partial, sums, out);
+    BS_CHECK_LAUNCH("bottom-up moments");
+    return BS_OK;
+}
+
 int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_t s) {
     const int64_t count = t->count;
     t->centre = t->alloc<double>(3 * count, s);
@@ -957,6 +1286,8 @@ int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_
     if (!t->centre || !t->bound || !t->core || !t->m0 || !t->m1 || !t->m2 || !t->w1 || !t->t2 || !t->w2 ||
         !t->nodes || !t->far64 || !t->far32)
         return BS_ERR_OOM;
+    if (t->kind == BS_TREE_MORTON) return t->order3 ? moments_bottom_up<MOM_PARTS3>(t, geo, scratch, s)
+                                                   : moments_bottom_up<MOM_PARTS>(t, geo, scratch, s);
     int64_t *nitems = scratch.get<int64_t>(count), *first = scratch.get<int64_t>(count);
     int64_t *total = scratch.get<int64_t>(1);
     if (!nitems || !first || !total) return scratch.status;
@@ -975,16 +1306,14 @@ int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_
     unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(n_items, 8192));
     moment_box_kernel<<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, box);
     moment_centre_kernel<<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, box, t->centre, t->core);
+    const NodeOut out{t->lo, t->hi, t->left, t->right, t->centre, t->core, t->bound, t->m0, t->m1, t->m2,
+                      t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x};
     if (t->order3) {
         moment_sum_kernel<MOM_PARTS3><<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, t->centre, sums);
-        moment_final_kernel<MOM_PARTS3><<<blocks_for(count, 128), 128, 0, s>>>(
-            count, first, nitems, sums, t->lo, t->hi, t->left, t->right, t->centre, t->core, t->bound, t->m0, t->m1,
-            t->m2, t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x);
+        moment_final_kernel<MOM_PARTS3><<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, sums, out);
     } else {
         moment_sum_kernel<MOM_PARTS><<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, t->centre, sums);
-        moment_final_kernel<MOM_PARTS><<<blocks_for(count, 128), 128, 0, s>>>(
-            count, first, nitems, sums, t->lo, t->hi, t->left, t->right, t->centre, t->core, t->bound, t->m0, t->m1,
-            t->m2, t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, nullptr, nullptr);
+        moment_final_kernel<MOM_PARTS><<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, sums, out);
     }
     BS_CHECK_LAUNCH("moments");
     return BS_OK;

@@ -265,3 +265,26 @@ def test_third_order_expansion_converges_one_order_faster(device):
     with pytest.raises(ValueError):
         engine.tree_eval(engine.build_tree(src, leaf_size=16, kind="morton", order=2), tgt, 2, "raise", "fp64",
                          theta=0.1, order=3)
+
+
+def test_morton_bottom_up_moments_against_direct_node_sums(device):
+    """Morton trees and forests take their node moments bottom-up (leaves summed, parents translated from their
+    children): box, centre, core and bounding radius equal the direct per-node computation bit for bit, the moments
+    agree to rounding (1e-12 of the node's largest child-moment magnitude)."""
+    from openfawe_b200 import engine, wakes
+    case = wakes.rotor_sheet(80, seed=11, targets=10)
+    args = wakes.backend_args(case)
+    src = engine.Sources(*args[1:6], device)
+    starts = args[1]
+    lv, ends, alpha, _ = O.segment_geometry(*args[1:5])
+    for leaf in (1, 8, 32):
+        tree = engine.build_tree(src, leaf_size=leaf, kind="morton")
+        ex = tree.export()
+        ref = O.node_moments(ex["order"], ex["lo"], ex["hi"], starts, ends, alpha, lv, args[5], args[4])
+        for key, value in zip(("centre", "bound", "core"), ref[:3]):
+            assert np.array_equal(ex[key], value), (leaf, key)
+        # translation rounds like a sum over the node's segments: scale by the segments' own moment magnitudes
+        seg_scale = np.abs(alpha).max() * (1.0 + np.abs(ex["bound"]).max()) ** 2
+        for key, value in zip(("m0", "m1", "m2"), ref[3:]):
+            assert np.abs(ex[key] - value).max() <= 1e-12 * seg_scale * len(starts), (leaf, key)
+            assert node_relative(value, ex[key]).max() <= 1e-9, (leaf, key)
