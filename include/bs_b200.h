@@ -82,6 +82,7 @@ typedef struct {
     int64_t far_evaluations, near_pairs, fp64_pairs, visits; /* counters of the last tree evaluation */
     double build_ms, moments_ms, evaluate_ms;                /* device time of the last build / evaluation */
     int64_t pair_slots;  /* lane slots spent in leaf walks (32 per warp-pair); near_pairs / pair_slots = SIMT use */
+    double walk_ms, list_ms; /* device time of the traversal and interaction-list kernels of the last tree evaluation */
 } bs_stats;
 
 /* Context: one per device.  bs_init makes `device` current, probes it with a one-thread kernel (the reference's
@@ -93,6 +94,9 @@ const char *bs_last_error(void);
 int bs_last_stats(const bs_ctx *ctx, bs_stats *stats);
 /* Library version and the compute capability it was built for (100 for sm_100a). */
 int bs_version(int *major, int *minor, int *arch);
+/* Measures the device's FP32 FMA throughput (TFLOP/s, an FMA counted as 2) with a kernel of independent FMA chains
+ * on every SM: the denominator of the pair kernels' roofline, which run on the FP32 pipe. */
+int bs_fp32_peak(bs_ctx *ctx, double *tflops);
 
 /* Exact direct sum (vortex_numba._sum_point semantics, vortex_numba.py:112-147): every non-excluded (target, segment)
  * pair, segment order preserved inside each thread's range; BS_FP64 sums in FP64, BS_MIXED/BS_FP32 use FP32 pair

@@ -40,7 +40,7 @@ class Stats(ctypes.Structure):
     _fields_ = [("points", _i64), ("segments", _i64), ("nodes", _i64), ("launches", _i64),
                 ("far_evaluations", _i64), ("near_pairs", _i64), ("fp64_pairs", _i64), ("visits", _i64),
                 ("build_ms", ctypes.c_double), ("moments_ms", ctypes.c_double), ("evaluate_ms", ctypes.c_double),
-                ("pair_slots", _i64)]
+                ("pair_slots", _i64), ("walk_ms", ctypes.c_double), ("list_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -52,6 +52,7 @@ SIGNATURES = {
     "bs_last_error": (ctypes.c_char_p, []),
     "bs_last_stats": (ctypes.c_int, [_p, ctypes.POINTER(Stats)]),
     "bs_version": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)] * 3),
+    "bs_fp32_peak": (ctypes.c_int, [_p, ctypes.POINTER(ctypes.c_double)]),
     "bs_direct": (ctypes.c_int, [_p, ctypes.POINTER(Sources), ctypes.POINTER(Targets), ctypes.POINTER(KernelParams),
                                  _p, _p, _p]),
     "bs_tree_build": (ctypes.c_int, [_p, ctypes.POINTER(Sources), ctypes.POINTER(TreeParams), ctypes.POINTER(_p),

@@ -88,25 +88,27 @@ def device_ms(fn, repeats=3):
     return best
 
 
-def autotune(batch, theta=0.04, precision="mixed", leaves=(16, 32, 64), blocks=(64, 128)):
+def autotune(batch, theta=0.04, precision="mixed", leaves=(16, 32, 64), blocks=(64, 128), order=2):
     """Pick (leaf_size, block) for this batch's size class by timing build + evaluation; returns the choice and the
     table of timings.  Results are cached per (segments, targets, wakes) size class within the process."""
-    key = (int(np.log2(max(1, batch.sources.m))), int(np.log2(max(1, batch.targets.n))), batch.count, theta, precision)
+    key = (int(np.log2(max(1, batch.sources.m))), int(np.log2(max(1, batch.targets.n))), batch.count, theta, precision,
+           order)
     if key in _TUNED:
-        batch.build(_TUNED[key]["choice"][0])
+        batch.build(_TUNED[key]["choice"][0], order)
         return _TUNED[key]
     table = {}
     for leaf in leaves:
         for block in blocks:
             table[(leaf, block)] = device_ms(
-                lambda: (batch.build(leaf), batch.evaluate(theta, precision=precision, block=block)), repeats=2)
+                lambda: (batch.build(leaf, order), batch.evaluate(theta, order, precision=precision, block=block)),
+                repeats=2)
     choice = min(table, key=table.get)
-    batch.build(choice[0])
+    batch.build(choice[0], order)
     _TUNED[key] = dict(choice=choice, table={f"leaf{k[0]}_block{k[1]}": v for k, v in table.items()})
     return _TUNED[key]
 
 
-def sequential(cases, device=0, theta=0.04, precision="mixed", leaf_size=32, block=128, kind="morton"):
+def sequential(cases, device=0, theta=0.04, precision="mixed", leaf_size=32, block=128, kind="morton", order=2):
     """One tree_sum call per wake (the reference's pattern), inputs already on the device; per-wake CUDA-event ms."""
     dev = torch.device("cuda", device) if isinstance(device, int) else device
     data = [(engine.Sources(c["starts"], c["directions"], c["lengths"], c["gamma"], c["radius"], dev),
@@ -116,7 +118,7 @@ def sequential(cases, device=0, theta=0.04, precision="mixed", leaf_size=32, blo
     for src, tgt, model in data:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        u, _, _ = engine.tree_sum(src, tgt, model, "raise", precision, block, 3.0, theta, 2, leaf_size, 3.0, kind,
+        u, _, _ = engine.tree_sum(src, tgt, model, "raise", precision, block, 3.0, theta, order, leaf_size, 3.0, kind,
                                   far_counts=False)
         e1.record()
         outs.append(u)

@@ -477,11 +477,17 @@ __global__ void exclusion_positions_kernel(int64_t n, const int64_t *ex_ptr, con
 
 static inline unsigned nblocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
+// Events that eval_run records around the walk and list kernels (null while a graph is being captured).
+static thread_local cudaEvent_t *t_marks = nullptr;
+
 template <int PREC, int MODEL>
 static void launch_pair(unsigned walk_grid, int block, size_t smem, unsigned list_grid, int64_t target_warps,
                         unsigned reduce_grid, cudaStream_t s, const EvalArgs &args, double *out, int8_t *flags) {
+    if (t_marks) cudaEventRecord(t_marks[0], s);
     tree_walk_kernel<PREC, MODEL><<<walk_grid, block, smem, s>>>(args);
+    if (t_marks) cudaEventRecord(t_marks[1], s);
     tree_list_kernel<PREC, MODEL><<<list_grid, LIST_WARPS * 32, 0, s>>>(args, target_warps);
+    if (t_marks) cudaEventRecord(t_marks[2], s);
     tree_reduce_kernel<PREC><<<reduce_grid, 256, 0, s>>>(args, out, flags);
 }
 
@@ -708,20 +714,28 @@ int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const b
     Scratch scratch(ctx->pool, s);
     unsigned long long *state = scratch.get<unsigned long long>(6);
     if (!state) return scratch.status;
-    cudaEvent_t e0, e1;
+    cudaEvent_t e0, e1, marks[3];
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    for (auto &m : marks) cudaEventCreate(&m);
     cudaEventRecord(e0, s);
+    t_marks = marks;
     int rc = eval_enqueue(ctx, tree, tp, tgt, target_wake_ptr, nw, kp, out, flags, far_counts, state, scratch, s);
+    t_marks = nullptr;
     cudaEventRecord(e1, s);
     unsigned long long host[6] = {0, 0, 0, 0, 0, 0};
     cudaError_t le = cudaSuccess;
     if (rc == BS_OK) le = cudaMemcpyAsync(host, state, sizeof host, cudaMemcpyDeviceToHost, s);
     if (le == cudaSuccess) le = cudaStreamSynchronize(s);
-    float ms = 0.f;
-    if (rc == BS_OK && le == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    float ms = 0.f, walk_ms = 0.f, list_ms = 0.f;
+    if (rc == BS_OK && le == cudaSuccess) {
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventElapsedTime(&walk_ms, marks[0], marks[1]);
+        cudaEventElapsedTime(&list_ms, marks[1], marks[2]);
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    for (auto &m : marks) cudaEventDestroy(m);
     if (rc != BS_OK) return rc;
     if (le != cudaSuccess) return cuda_fail(le, "tree evaluation");
     ctx->stats.points = tgt->n;
@@ -734,6 +748,8 @@ int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const b
     ctx->stats.visits = (int64_t)host[4];
     ctx->stats.pair_slots = (int64_t)host[5];
     ctx->stats.evaluate_ms = ms;
+    ctx->stats.walk_ms = walk_ms;
+    ctx->stats.list_ms = list_ms;
     if (host[0] & 0xffffffffull) {
         set_error("tree traversal stack overflow on the GPU (depth %d)",
                   (tp->stack_limit > 0 && tp->stack_limit < STACK_DEPTH) ? tp->stack_limit : STACK_DEPTH);

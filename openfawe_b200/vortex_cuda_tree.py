@@ -40,8 +40,11 @@ class Statistics:
 
 
 def cuda_tree_sum(points, starts, directions, lengths, gamma, radius, model, csr, singularity, tree, settings, *,
-                  targets_per_launch=None, stack_size=STACK, block=None):
-    """Return (velocity, any_flag) like ``vortex_tree.tree_sum`` for the same inputs, evaluated on the GPU."""
+                  targets_per_launch=None, stack_size=STACK, block=None, order=None):
+    """Return (velocity, any_flag) like ``vortex_tree.tree_sum`` for the same inputs, evaluated on the GPU.
+
+    ``order`` (keyword, not in the reference) overrides ``tree.order``; 3 selects the third-order far field, which
+    reaches the accuracy of order 2 at a larger opening angle."""
     if not VC.available():
         raise ValueError(f"the cuda tree evaluation needs a CUDA device ({VC.probe_error()})")
     if int(model) not in SUPPORTED_MODELS and np.any(np.asarray(radius) > 0):
@@ -53,6 +56,9 @@ def cuda_tree_sum(points, starts, directions, lengths, gamma, radius, model, csr
     if gpu64 and precision == "fp64":
         raise ValueError("suspect='gpu64' is for the single precisions only")
     block = int(settings.block if block is None else block)
+    expansion = int(tree.order if order is None else order)
+    if expansion not in (0, 1, 2, 3):
+        raise ValueError("tree order must be 0, 1, 2 or 3")
     _, _, near = VC._check_settings(settings)
     kind = getattr(settings, "tree", "median")
     points = np.ascontiguousarray(points, dtype=np.float64)
@@ -71,14 +77,14 @@ def cuda_tree_sum(points, starts, directions, lengths, gamma, radius, model, csr
     torch.cuda.current_stream(device).synchronize()
     upload_s = time.perf_counter() - tick
     tick = time.perf_counter()
-    built = engine.build_tree(sources, tree.theta, tree.order, tree.leaf_size, tree.core_clearance, kind)
+    built = engine.build_tree(sources, tree.theta, expansion, tree.leaf_size, tree.core_clearance, kind)
     build_s = time.perf_counter() - tick
     build_stats = engine.last_stats(device)
     limit = int(stack_size) if 0 < int(stack_size) < DEVICE_STACK else 0
     tick = time.perf_counter()
     try:
         d_out, d_flags, d_far = engine.tree_eval(built, targets, int(model), singularity, precision, block, near,
-                                                 tree.theta, tree.order, tree.core_clearance, stack_limit=limit)
+                                                 tree.theta, expansion, tree.core_clearance, stack_limit=limit)
     except _lib.StackOverflow as error:
         raise RuntimeError(f"tree traversal stack overflow on the GPU (depth {min(int(stack_size), DEVICE_STACK)})") \
             from error
