@@ -133,6 +133,9 @@ enum { F_M0 = 0, F_M1 = 3, F_W1 = 12, F_T2 = 15, F_W2 = 18, F_M2 = 27 };
 struct __align__(16) Far64x { double v[64]; };
 struct __align__(16) Far32x { float v[64]; };
 enum { G_M3 = 0, G_T3 = 30, G_W3 = 39, G_W3V = 57 };
+// Far32x keeps each component i's coefficients together in five float4: [20 i, 20 i + 10) m3 row, [+10, +13) T3 row,
+// [+13, +19) W3 row, then w3 at [60, 63).
+enum { H_ROW = 20, H_M3 = 0, H_T3 = 10, H_W3 = 13, H_W3V = 60 };
 
 // ---------------------------------------------------------------------------------------------------------------------
 // Arithmetic helpers.
@@ -389,6 +392,83 @@ __device__ __forceinline__ void far_eval(T rx, T ry, T rz, const T *f, int order
     ux += T(INV_FOUR_PI) * u0;
     uy += T(INV_FOUR_PI) * u1;
     uz += T(INV_FOUR_PI) * u2;
+}
+
+// far_eval<float> reading the packed records (Far32: 12 float4, Far32x: 16 float4) in vector loads, one group at a
+// time where it is used, so that only one order's coefficients are live at once.  Same arithmetic as far_eval.
+__device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const float4 *f, int order, float &ux,
+                                            float &uy, float &uz, const float4 *g = nullptr) {
+    const float r2 = rx * rx + ry * ry + rz * rz;
+    const float inv3 = 1.0f / (r2 * sqrtf(r2));
+    const float inv5 = inv3 / r2;
+    const float4 q0 = __ldg(f);  // m0 x y z, m1[0]
+    float u0 = inv3 * (q0.y * rz - q0.z * ry);
+    float u1 = inv3 * (q0.z * rx - q0.x * rz);
+    float u2 = inv3 * (q0.x * ry - q0.y * rx);
+    if (order >= 1) {
+        const float4 q1 = __ldg(f + 1), q2 = __ldg(f + 2), q3 = __ldg(f + 3);  // m1[1..8], w1, t2[0]
+        const float v0 = q0.w * rx + q1.x * ry + q1.y * rz;
+        const float v1 = q1.z * rx + q1.w * ry + q2.x * rz;
+        const float v2 = q2.y * rx + q2.z * ry + q2.w * rz;
+        const float k = 3.0f * inv5;
+        u0 += k * (v1 * rz - v2 * ry) - inv3 * q3.x;
+        u1 += k * (v2 * rx - v0 * rz) - inv3 * q3.y;
+        u2 += k * (v0 * ry - v1 * rx) - inv3 * q3.z;
+        if (order >= 2) {
+            const float inv7 = inv5 / r2;
+            const float xx = rx * rx, xy = rx * ry, xz = rx * rz, yy = ry * ry, yz = ry * rz, zz = rz * rz;
+            const float4 q4 = __ldg(f + 4), q5 = __ldg(f + 5), q6 = __ldg(f + 6);  // t2[1..2], w2[0..8], m2 s[0]
+            const float4 q7 = __ldg(f + 7), q8 = __ldg(f + 8), q9 = __ldg(f + 9), q10 = __ldg(f + 10),
+                         q11 = __ldg(f + 11);  // m2 symmetric s[1..17]
+            // m2 symmetric rows (00,01,02,11,12,22) of i = 0, 1, 2 at floats 27..44
+            const float s0[6] = {q6.w, q7.x, q7.y, q7.z, q7.w, q8.x};
+            const float s1[6] = {q8.y, q8.z, q8.w, q9.x, q9.y, q9.z};
+            const float s2[6] = {q9.w, q10.x, q10.y, q10.z, q10.w, q11.x};
+            auto quad = [&](const float *sv) {
+                return sv[0] * xx + sv[3] * yy + sv[5] * zz + 2.0f * (sv[1] * xy + sv[2] * xz + sv[4] * yz);
+            };
+            const float a = 7.5f * inv7, b = 1.5f * inv5;
+            const float b0 = a * quad(s0) - b * q3.w;
+            const float b1 = a * quad(s1) - b * q4.x;
+            const float b2 = a * quad(s2) - b * q4.y;
+            const float w0 = q4.z * rx + q4.w * ry + q5.x * rz;
+            const float w1 = q5.y * rx + q5.z * ry + q5.w * rz;
+            const float w2 = q6.x * rx + q6.y * ry + q6.z * rz;
+            u0 += (b1 * rz - b2 * ry) - k * w0;
+            u1 += (b2 * rx - b0 * rz) - k * w1;
+            u2 += (b0 * ry - b1 * rx) - k * w2;
+            if (order >= 3) {
+                const float inv9 = inv7 / r2;
+                const float c000 = xx * rx, c001 = 3.0f * xx * ry, c002 = 3.0f * xx * rz, c011 = 3.0f * xy * ry;
+                const float c012 = 6.0f * xy * rz, c022 = 3.0f * xz * rz, c111 = yy * ry, c112 = 3.0f * yy * rz;
+                const float c122 = 3.0f * yz * rz, c222 = zz * rz;
+                float x3[3], w[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    float h[H_ROW];  // component i's row: m3 (10), T3 (3), W3 (6), pad
+#pragma unroll
+                    for (int q = 0; q < H_ROW / 4; ++q) {
+                        const float4 x = __ldg(g + (H_ROW / 4) * i + q);
+                        h[4 * q] = x.x; h[4 * q + 1] = x.y; h[4 * q + 2] = x.z; h[4 * q + 3] = x.w;
+                    }
+                    const float *m = h + H_M3;
+                    const float s3 = m[0] * c000 + m[1] * c001 + m[2] * c002 + m[3] * c011 + m[4] * c012 +
+                                     m[5] * c022 + m[6] * c111 + m[7] * c112 + m[8] * c122 + m[9] * c222;
+                    const float tr = h[H_T3] * rx + h[H_T3 + 1] * ry + h[H_T3 + 2] * rz;
+                    x3[i] = 17.5f * inv9 * s3 - 7.5f * inv7 * tr;
+                    w[i] = quad(h + H_W3);
+                }
+                const float4 wv = __ldg(g + H_W3V / 4);
+                const float c7 = 7.5f * inv7, c5 = 1.5f * inv5;
+                u0 += (x3[1] * rz - x3[2] * ry) - c7 * w[0] + c5 * wv.x;
+                u1 += (x3[2] * rx - x3[0] * rz) - c7 * w[1] + c5 * wv.y;
+                u2 += (x3[0] * ry - x3[1] * rx) - c7 * w[2] + c5 * wv.z;
+            }
+        }
+    }
+    ux += (float)INV_FOUR_PI * u0;
+    uy += (float)INV_FOUR_PI * u1;
+    uz += (float)INV_FOUR_PI * u2;
 }
 
 // Two-float split of an FP64 value: hi = round(x), lo = round(x - hi).

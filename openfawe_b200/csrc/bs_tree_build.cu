@@ -929,10 +929,16 @@ __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
         g[G_W3V + 0] = T3[3 * 1 + 2] - T3[3 * 2 + 1];
         g[G_W3V + 1] = T3[3 * 2 + 0] - T3[3 * 0 + 2];
         g[G_W3V + 2] = T3[3 * 0 + 1] - T3[3 * 1 + 0];
-        for (int q = 0; q < 64; ++q) {
-            far64x[j].v[q] = q < BS_FAR3_N ? g[q] : 0.0;
-            far32x[j].v[q] = q < BS_FAR3_N ? (float)g[q] : 0.f;
+        for (int q = 0; q < 64; ++q) far64x[j].v[q] = q < BS_FAR3_N ? g[q] : 0.0;
+        float h[64];
+        for (int q = 0; q < 64; ++q) h[q] = 0.f;
+        for (int i = 0; i < 3; ++i) {
+            for (int q = 0; q < 10; ++q) h[H_ROW * i + H_M3 + q] = (float)g[G_M3 + 10 * i + q];
+            for (int q = 0; q < 3; ++q) h[H_ROW * i + H_T3 + q] = (float)g[G_T3 + 3 * i + q];
+            for (int q = 0; q < 6; ++q) h[H_ROW * i + H_W3 + q] = (float)g[G_W3 + 6 * i + q];
         }
+        for (int q = 0; q < 3; ++q) h[H_W3V + q] = (float)g[G_W3V + q];
+        for (int q = 0; q < 64; ++q) far32x[j].v[q] = h[q];
     }
     NodeRec r;
     r.cx = centre[3 * j]; r.cy = centre[3 * j + 1]; r.cz = centre[3 * j + 2];

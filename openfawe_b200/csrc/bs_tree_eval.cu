@@ -12,12 +12,16 @@
 #include <algorithm>
 
 #include "bs_sort.cuh"
+#include <cstdlib>
+
 #include "bs_tree.cuh"
 
 namespace bs {
 
 constexpr int STACK_DEPTH = 128;
-constexpr int LIST_CAP = 4096;            // list entries per warp of targets
+constexpr int LIST_CHUNK = 128;           // list entries per chunk of the shared list pool
+constexpr int LIST_CHUNKS = 32;           // chunks a unit's list may hold (4096 entries)
+constexpr int LIST_POOL = 4096;           // pool entries per warp of targets
 constexpr int FAR_BIT = int(0x80000000u);
 constexpr int FAR_COST = 3;               // list cost units: one far evaluation ~ three pairs
 constexpr int LIST_WARPS = 4;             // warps per block of the list kernel
@@ -42,9 +46,13 @@ struct EvalArgs {
     double theta, theta2, clearance;
     int order, model, raise_singular, stack_limit;
     float near2;
-    // interaction lists, one region of LIST_CAP entries per warp of targets
+    // interaction lists: entries live in chunks of LIST_CHUNK taken from a shared pool; warp gw of targets lists its
+    // chunks in unit_chunks[gw][0 .. LIST_CHUNKS)
     int2 *list;          // (node, lane mask); far entries carry FAR_BIT in the node
     int *list_cost;      // cost before each entry
+    int *unit_chunks;
+    unsigned long long *pool_cursor;
+    unsigned long long pool_chunks;
     int *list_len;       // entries per warp
     int *list_total;     // total cost per warp
     // what the walk evaluates itself (list overflow) and per-target results
@@ -106,8 +114,8 @@ __device__ __forceinline__ void far_node(const EvalArgs &a, const Target &t, int
         acc.add64(g0, g1, g2);
     } else {
         float g0 = 0.f, g1 = 0.f, g2 = 0.f;
-        far_eval<float>((float)rx, (float)ry, (float)rz, a.tv.far32[node].v, a.order, g0, g1, g2,
-                        a.order >= 3 ? a.tv.far32x[node].v : nullptr);
+        far_eval32v((float)rx, (float)ry, (float)rz, reinterpret_cast<const float4 *>(a.tv.far32[node].v), a.order,
+                    g0, g1, g2, a.order >= 3 ? reinterpret_cast<const float4 *>(a.tv.far32x[node].v) : nullptr);
         acc.add32(g0, g1, g2);
     }
 }
@@ -184,7 +192,7 @@ __device__ __forceinline__ void leaf_pairs(const EvalArgs &a, const Target &t, i
 // Phase 1: the traversal.  Each warp walks the tree once for its 32 targets and writes an interaction list: far
 // nodes and near leaves with the mask of lanes concerned, in depth-first order, and the cost before each entry.  What
 // does not fit in the list is evaluated here.
-template <int PREC, int MODEL>
+template <int PREC, int MODEL, int POP>
 __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
     extern __shared__ __align__(16) unsigned char eval_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
@@ -193,6 +201,7 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
     Seg64 *seg64_tile = reinterpret_cast<Seg64 *>(tiles) + warp * 32;
     Seg32 *seg32_tile = reinterpret_cast<Seg32 *>(tiles) + warp * 32;
     const int64_t gw = (int64_t)blockIdx.x * warps + warp;  // warp of targets
+    if (gw * 32 >= a.n) return;  // warp-uniform: warps past the last target own no list
     Target t;
     t.load(a, gw * 32 + lane);
     int64_t e = 0, e1 = 0;
@@ -200,9 +209,30 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
     Acc<PREC> acc;
     int flag = BS_FLAG_OK;
     long long far = 0, far_total = 0, near_pairs = 0, fp64_pairs = 0, visits = 0, pair_slots = 0;
-    int2 *list = a.list + gw * LIST_CAP;
-    int *cost = a.list_cost + gw * LIST_CAP;
-    int len = 0, running = 0;
+    int *my_chunks = a.unit_chunks + gw * LIST_CHUNKS;
+    int len = 0, running = 0, chunk = -1;
+    bool full = false;  // the unit's chunk table or the pool ran out: the rest is evaluated here
+    // Room for one more entry (warp-uniform): a new chunk every LIST_CHUNK entries.
+    auto room = [&]() -> bool {
+        if (full) return false;
+        if ((len & (LIST_CHUNK - 1)) == 0) {
+            int c = -1;
+            if (len / LIST_CHUNK < LIST_CHUNKS && lane == 0) {
+                const unsigned long long got = atomicAdd(a.pool_cursor, 1ull);
+                if (got < a.pool_chunks) {
+                    c = (int)got;
+                    my_chunks[len / LIST_CHUNK] = c;
+                }
+            }
+            c = __shfl_sync(0xffffffffu, c, 0);
+            if (c < 0) {
+                full = true;
+                return false;
+            }
+            chunk = c;
+        }
+        return true;
+    };
     // Roots: node 0, or in a forest the root of each lane's wake; one stack entry per distinct root.
     const int root = a.root_of ? (t.valid ? a.root_of[gw * 32 + lane] : -1) : 0;
     const bool live = t.valid && root >= 0;
@@ -212,13 +242,10 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
     if (leader) stack[__popc(leaders & ((1u << lane) - 1u))] = make_int2(root, (int)peers);
     int top = __popc(leaders);
     __syncwarp();
-    while (top > 0) {
-        --top;
-        const int2 entry = stack[top];
-        const int node = entry.x;
-        const unsigned mask = (unsigned)entry.y;
+    // One node for the lanes of `mask`: per-lane acceptance, then a far entry, a near-leaf entry or two pushed
+    // children.  Returns false when the stack would overflow.
+    auto visit = [&](const int node, const unsigned mask, const NodeRec &nr) -> bool {
         const bool mine = (mask >> lane) & 1u;
-        const NodeRec nr = a.tv.nodes[node];
         bool accept = false;
         if (mine) {
             ++visits;
@@ -238,9 +265,10 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
                 const double dist = sqrt(r2);
                 accept = nr.bound < __dmul_rn(a.theta, dist) && __dsub_rn(dist, nr.bound) >= cc;
             }
-            if (accept && e < e1) {
-                while (e < e1 && a.ex_pos[e] < nr.lo) ++e;
-                if (e < e1 && a.ex_pos[e] < nr.hi) accept = false;
+            if (accept && e < e1) {  // an excluded segment inside the node keeps it open
+                int64_t q = e;
+                while (q < e1 && a.ex_pos[q] < nr.lo) ++q;
+                if (q < e1 && a.ex_pos[q] < nr.hi) accept = false;
             }
         }
         const unsigned farm = __ballot_sync(0xffffffffu, mine && accept);
@@ -248,8 +276,12 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
         if (farm) {
             if (mine && accept) ++far;
             far_total += __popc(farm);
-            if (len < LIST_CAP) {
-                if (lane == 0) { list[len] = make_int2(node | FAR_BIT, (int)farm); cost[len] = running; }
+            if (room()) {
+                if (lane == 0) {
+                    const int64_t k = (int64_t)chunk * LIST_CHUNK + (len & (LIST_CHUNK - 1));
+                    a.list[k] = make_int2(node | FAR_BIT, (int)farm);
+                    a.list_cost[k] = running;
+                }
                 ++len;
                 running += FAR_COST;
             } else if (mine && accept) {
@@ -259,18 +291,23 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
         if (openm) {
             if (nr.left < 0) {
                 pair_slots += (long long)(nr.hi - nr.lo);
-                if (len < LIST_CAP) {
-                    if (lane == 0) { list[len] = make_int2(node, (int)openm); cost[len] = running; }
+                if (room()) {
+                    if (lane == 0) {
+                        const int64_t k = (int64_t)chunk * LIST_CHUNK + (len & (LIST_CHUNK - 1));
+                        a.list[k] = make_int2(node, (int)openm);
+                        a.list_cost[k] = running;
+                    }
                     ++len;
                     running += (nr.hi - nr.lo) + 2;
                 } else {
-                    leaf_pairs<PREC, MODEL>(a, t, nr.lo, nr.hi, mine && !accept, e, e1, seg64_tile, seg32_tile, acc,
+                    int64_t ec = e;
+                    leaf_pairs<PREC, MODEL>(a, t, nr.lo, nr.hi, mine && !accept, ec, e1, seg64_tile, seg32_tile, acc,
                                             flag, near_pairs, fp64_pairs);
                 }
             } else {
                 if (top + 2 > a.stack_limit) {
                     if (lane == 0) atomicExch(a.overflow, 1);
-                    break;
+                    return false;
                 }
                 if (lane == 0) {
                     stack[top] = make_int2(nr.right, (int)openm);
@@ -279,9 +316,27 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
                 top += 2;
             }
         }
+        return true;
+    };
+    // POP entries per step: their node records load together, so that with POP = 2 two independent loads are in
+    // flight per step of the (latency-bound) walk.  The set of visited nodes does not depend on the order.
+    while (top > 0) {
+        if (POP == 2 && top >= 2) {
+            const int2 x = stack[top - 1], y = stack[top - 2];
+            top -= 2;
+            const NodeRec nx = a.tv.nodes[x.x], ny = a.tv.nodes[y.x];
+            __syncwarp();
+            if (!visit(x.x, (unsigned)x.y, nx)) break;
+            if (!visit(y.x, (unsigned)y.y, ny)) break;
+        } else {
+            const int2 x = stack[--top];
+            const NodeRec nx = a.tv.nodes[x.x];
+            __syncwarp();
+            if (!visit(x.x, (unsigned)x.y, nx)) break;
+        }
         __syncwarp();
     }
-    if (lane == 0 && gw * 32 < a.n) {  // warps past the last target (in the grid's last block) own no list
+    if (lane == 0) {
         a.list_len[gw] = len;
         a.list_total[gw] = running;
     }
@@ -315,15 +370,18 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
                                           long long &near_pairs, long long &fp64_pairs) {
     const int lane = threadIdx.x & 31;
     const int chunks = a.chunks;
+    // chunk c is the c-th slice of this warp's list by cost
     const int len = a.list_len[gw];
     const int64_t total = a.list_total[gw];
-    const int *cost = a.list_cost + gw * LIST_CAP;
-    const int2 *list = a.list + gw * LIST_CAP;
+    const int *chunks_of = a.unit_chunks + gw * LIST_CHUNKS;
+    auto at = [&](int k) -> int64_t {  // pool index of the list's k-th entry
+        return (int64_t)chunks_of[k / LIST_CHUNK] * LIST_CHUNK + (k & (LIST_CHUNK - 1));
+    };
     auto lower = [&](int64_t v) {  // first entry whose cost start is >= v
         int l = 0, h = len;
         while (l < h) {
             int m = (l + h) >> 1;
-            if (cost[m] < v) l = m + 1; else h = m;
+            if (a.list_cost[at(m)] < v) l = m + 1; else h = m;
         }
         return l;
     };
@@ -335,13 +393,14 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
     Acc<PREC> acc;
     int flag = BS_FLAG_OK;
     for (int k = first; k < last; ++k) {
-        const int2 entry = list[k];
+        const int2 entry = a.list[at(k)];
         const bool mine = ((unsigned)entry.y >> lane) & 1u;
         if (entry.x & FAR_BIT) {
             if (mine) far_node<PREC>(a, t, entry.x & ~FAR_BIT, acc);
         } else {
             const NodeRec nr = a.tv.nodes[entry.x];
-            leaf_pairs<PREC, MODEL>(a, t, nr.lo, nr.hi, mine, e, e1, seg64_tile, seg32_tile, acc, flag, near_pairs,
+            int64_t ec = e;  // list entries are not in position order: each leaf scans the exclusions from the start
+            leaf_pairs<PREC, MODEL>(a, t, nr.lo, nr.hi, mine, ec, e1, seg64_tile, seg32_tile, acc, flag, near_pairs,
                                     fp64_pairs);
         }
     }
@@ -483,8 +542,14 @@ static thread_local cudaEvent_t *t_marks = nullptr;
 template <int PREC, int MODEL>
 static void launch_pair(unsigned walk_grid, int block, size_t smem, unsigned list_grid, int64_t target_warps,
                         unsigned reduce_grid, cudaStream_t s, const EvalArgs &args, double *out, int8_t *flags) {
+    // BS_WALK_POP=1 takes one stack entry per walk step (for comparisons); the default takes two
+    static const int pop = [] {
+        const char *v = getenv("BS_WALK_POP");
+        return (v && v[0] == '1') ? 1 : 2;
+    }();
     if (t_marks) cudaEventRecord(t_marks[0], s);
-    tree_walk_kernel<PREC, MODEL><<<walk_grid, block, smem, s>>>(args);
+    if (pop == 2) tree_walk_kernel<PREC, MODEL, 2><<<walk_grid, block, smem, s>>>(args);
+    else tree_walk_kernel<PREC, MODEL, 1><<<walk_grid, block, smem, s>>>(args);
     if (t_marks) cudaEventRecord(t_marks[1], s);
     tree_list_kernel<PREC, MODEL><<<list_grid, LIST_WARPS * 32, 0, s>>>(args, target_warps);
     if (t_marks) cudaEventRecord(t_marks[2], s);
@@ -621,7 +686,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
                  int64_t *far_counts, unsigned long long *state, Scratch &scratch, cudaStream_t s) {
     const int64_t n = tgt->n;
     int32_t *perm = scratch.get<int32_t>(n);
-    unsigned long long *queue = scratch.get<unsigned long long>(1);
+    unsigned long long *queue = scratch.get<unsigned long long>(2);  // list-kernel work counter, list-pool cursor
     int32_t *ex_pos = nullptr, *root_of = nullptr;
     if (!perm || !queue) return scratch.status;
     int rc;
@@ -655,17 +720,19 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
         BS_CHECK_LAUNCH("exclusion_positions_kernel");
     }
     BS_CUDA(cudaMemsetAsync(state, 0, 6 * sizeof(unsigned long long), s));
-    BS_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s));
+    BS_CUDA(cudaMemsetAsync(queue, 0, 2 * sizeof(unsigned long long), s));
     const int block = std::min(kp->block, 128);
     const int64_t target_warps = (n + 31) / 32;
     const int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(64, ((int64_t)ctx->sm_count * 32 + target_warps - 1)
                                                                        / target_warps));
-    int2 *list = scratch.get<int2>((size_t)target_warps * LIST_CAP);
-    int *list_cost = scratch.get<int>((size_t)target_warps * LIST_CAP);
-    int *list_len = scratch.get<int>(target_warps), *list_total = scratch.get<int>(target_warps);
-    double *walk_u = scratch.get<double>(3 * n), *partial = scratch.get<double>((size_t)3 * n * chunks);
-    int8_t *walk_flag = scratch.get<int8_t>(n), *pflag = scratch.get<int8_t>((size_t)n * chunks);
-    if (!list || !list_cost || !list_len || !list_total || !walk_u || !partial || !walk_flag || !pflag)
+    const size_t slots = (size_t)target_warps, pool = (size_t)target_warps * LIST_POOL;
+    int2 *list = scratch.get<int2>(pool);
+    int *list_cost = scratch.get<int>(pool);
+    int *unit_chunks = scratch.get<int>(slots * LIST_CHUNKS);
+    int *list_len = scratch.get<int>(slots), *list_total = scratch.get<int>(slots);
+    double *walk_u = scratch.get<double>((size_t)3 * n), *partial = scratch.get<double>((size_t)3 * n * chunks);
+    int8_t *walk_flag = scratch.get<int8_t>((size_t)n), *pflag = scratch.get<int8_t>((size_t)n * chunks);
+    if (!list || !list_cost || !unit_chunks || !list_len || !list_total || !walk_u || !partial || !walk_flag || !pflag)
         return scratch.status;
     EvalArgs args;
     args.n = n;
@@ -695,6 +762,9 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     args.pflag = pflag;
     args.chunks = chunks;
     args.root_of = root_of;
+    args.unit_chunks = unit_chunks;
+    args.pool_cursor = queue + 1;
+    args.pool_chunks = pool / LIST_CHUNK;
     args.queue = queue;
     const size_t smem = (size_t)(block / 32) * (STACK_DEPTH * sizeof(int2) + 32 * sizeof(Seg64));
     const unsigned walk_grid = (unsigned)((target_warps + block / 32 - 1) / (block / 32));
