@@ -94,6 +94,10 @@ const char *bs_last_error(void);
 int bs_last_stats(const bs_ctx *ctx, bs_stats *stats);
 /* Library version and the compute capability it was built for (100 for sm_100a). */
 int bs_version(int *major, int *minor, int *arch);
+/* Copies `bytes` from ordinary (pageable) host memory to device memory on `stream` through a pinned staging ring:
+ * several host threads fill 4 MiB pinned chunks while earlier chunks transfer.  Returns once the source has been read
+ * (the last transfers may still be in flight on the stream). */
+int bs_upload(bs_ctx *ctx, void *dst, const void *src, size_t bytes, bs_stream stream);
 /* Measures the device's FP32 FMA throughput (TFLOP/s, an FMA counted as 2) with a kernel of independent FMA chains
  * on every SM: the denominator of the pair kernels' roofline, which run on the FP32 pipe. */
 int bs_fp32_peak(bs_ctx *ctx, double *tflops);

@@ -10,7 +10,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBRARY = os.path.join(HERE, "libbs_b200.so")
-SOURCES = ["bs_context.cu", "bs_sort.cu", "bs_tree_build.cu", "bs_tree_eval.cu", "bs_direct.cu", "bs_adjoint.cu", "bs_network.cu", "bs_operators.cu"]
+SOURCES = ["bs_context.cu", "bs_sort.cu", "bs_tree_build.cu", "bs_tree_eval.cu", "bs_direct.cu", "bs_adjoint.cu", "bs_network.cu", "bs_operators.cu",
+           "bs_upload.cu"]
+OPENMP = {"bs_upload.cu"}  # host-threaded sources
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 
@@ -37,13 +39,14 @@ def build(verbose=False, extra=()):
         if (os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src)
                 and os.path.getmtime(obj) >= newest_header and not extra):
             continue
-        cmd = [nvcc(), *ARCH, *FLAGS, *extra, "-c", src, "-o", obj]
+        omp = ["-Xcompiler", "-fopenmp"] if source in OPENMP else []
+        cmd = [nvcc(), *ARCH, *FLAGS, *omp, *extra, "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
     if (not os.path.exists(LIBRARY) or extra
             or any(os.path.getmtime(o) > os.path.getmtime(LIBRARY) for o in objects)):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", LIBRARY, *objects]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", LIBRARY, *objects, "-Xcompiler", "-fopenmp"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

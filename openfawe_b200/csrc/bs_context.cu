@@ -91,10 +91,13 @@ extern "C" int bs_init(int device, bs_ctx **out) {
     return BS_OK;
 }
 
+void bs_upload_release(bs_ctx *ctx);  // bs_upload.cu
+
 extern "C" void bs_destroy(bs_ctx *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
+    bs_upload_release(ctx);
     cudaMemPoolDestroy(ctx->pool);
     delete ctx;
 }

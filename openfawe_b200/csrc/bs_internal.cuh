@@ -84,11 +84,14 @@ struct Scratch {
 
 }  // namespace bs
 
+struct bs_upload_ring;  // pinned staging of bs_upload (bs_upload.cu)
+
 struct bs_ctx {
     int device;
     int sm_count;
     cudaMemPool_t pool;
     bs_stats stats;
+    bs_upload_ring *upload = nullptr;
 };
 
 // ---------------------------------------------------------------------------------------------------------------------

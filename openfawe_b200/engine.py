@@ -24,15 +24,33 @@ def _device_of(device):
     return torch.device(device)
 
 
+UPLOAD_MIN_BYTES = 1 << 20  # host arrays from this size up travel through bs_upload (threaded pinned staging)
+
+
+def _upload(array, dtype, device):
+    """Host NumPy array -> new device tensor through the library's pinned staging ring (bs_upload)."""
+    out = torch.empty(array.shape, dtype=dtype, device=device)
+    L.check(L.library().bs_upload(L.context(device.index), _ptr(out), array.ctypes.data_as(ctypes.c_void_p),
+                                  array.nbytes, _stream(device)), "bs_upload")
+    return out
+
+
+def _to_device(a, np_dtype, dtype, device):
+    if not isinstance(a, torch.Tensor):
+        array = np.ascontiguousarray(a, dtype=np_dtype)
+        if device.type == "cuda" and array.nbytes >= UPLOAD_MIN_BYTES:
+            return _upload(array, dtype, device)
+        a = torch.from_numpy(array)
+    return a.to(device=device, dtype=dtype).contiguous()
+
+
 def f64(a, device):
     """A C-contiguous float64 tensor on `device` (copies only when needed)."""
-    t = a if isinstance(a, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64))
-    return t.to(device=device, dtype=torch.float64).contiguous()
+    return _to_device(a, np.float64, torch.float64, _device_of(device))
 
 
 def i64(a, device):
-    t = a if isinstance(a, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(a, dtype=np.int64))
-    return t.to(device=device, dtype=torch.int64).contiguous()
+    return _to_device(a, np.int64, torch.int64, _device_of(device))
 
 
 def _ptr(t):
