@@ -40,7 +40,7 @@ def _to_device(a, np_dtype, dtype, device):
         array = np.ascontiguousarray(a, dtype=np_dtype)
         if device.type == "cuda" and array.nbytes >= UPLOAD_MIN_BYTES:
             return _upload(array, dtype, device)
-        a = torch.from_numpy(array)
+        a = torch.from_numpy(array if array.flags.writeable else array.copy())
     return a.to(device=device, dtype=dtype).contiguous()
 
 

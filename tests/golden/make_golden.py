@@ -117,6 +117,61 @@ def main():
     from openfawe.aero import vortex_numba as vn, vortex_tree as vt
     from openfawe_b200 import wakes
 
+    if args.only == "convection.npz" or args.only is None:
+        # one step of the reference's geometry convection stages (wake._network_convection, wake.py:404-491) on a
+        # rotor-sheet network whose first row is the bound row; the integrators combine the stages as
+        # wake.convect_geometry does (wake.py:590-606)
+        import types
+        from openfawe.aero import wake as W
+        from openfawe.aero.vortex import CoreModel
+        case = wakes.rotor_sheet(10, seed=10, targets=1)
+        nodes, edges = case["nodes"], case["edges"]
+        first = 174
+        gamma = np.random.default_rng(10).uniform(0.0, 8.0, len(edges))
+        radii = np.full(len(edges), 0.05)
+        config = types.SimpleNamespace(free_wake=True, velocity_backend="numba", core_model=CoreModel.LAMB_OSEEN)
+        inflow = np.array([10.0, 0.0, 0.5])
+        dt = 0.02
+
+        def rhs(points, t):
+            return W._network_convection(np.concatenate((nodes[:first], points)), edges, gamma, first, radii, config,
+                                         inflow, t)
+        out = dict(nodes=nodes, edges=edges, gamma=gamma, radii=radii, first=np.array(first), inflow=inflow,
+                   dt=np.array(dt))
+        points = nodes[first:].copy()
+        k1 = rhs(points, 0.0)
+        out["k1"] = k1
+        out["euler"] = points + dt * k1
+        k2 = rhs(points + dt * k1, dt)
+        out["heun"] = points + dt * (k1 + k2) / 2
+        k2 = rhs(points + dt * k1 / 2, dt / 2)
+        k3 = rhs(points + dt * k2 / 2, dt / 2)
+        k4 = rhs(points + dt * k3, dt)
+        out["rk4"] = points + dt * (k1 + 2 * k2 + 2 * k3 + k4) / 6
+        save("convection.npz", **out)
+        if args.only:
+            return
+
+    if args.only == "frozen_state.npz" or args.only is None:
+        # a frozen state in the benchmark's format and the reference's own segments_velocity on it (the numba direct
+        # sum the benchmark takes as its reference, local_benchmark.py:56-66)
+        from openfawe.aero.vortex import segments_velocity
+        from openfawe.aero.network_numba import incident_pairs
+        from openfawe_b200 import wakestate
+        case = wakes.rotor_sheet(24, seed=24, targets=1)
+        nodes, edges = case["nodes"], case["edges"]
+        first = 174
+        gamma = np.random.default_rng(24).uniform(0.0, 8.0, len(edges))
+        radii = np.random.default_rng(25).uniform(0.03, 0.08, len(edges))
+        exclusions = incident_pairs(nodes, edges, first)
+        path = os.path.join(HERE, "frozen_state_input.npz")
+        wakestate.save_state(path, nodes, edges, gamma, radii, first, 10.0, 2, exclusions)
+        u = segments_velocity(nodes[first:], nodes, edges, gamma, model=2, core_radius=radii, exclusions=exclusions,
+                              backend="numba")
+        save("frozen_state.npz", u=u)
+        if args.only:
+            return
+
     if args.only == "operators.npz" or args.only is None:
         out = {}
         wing = wakes.ring_wing(panels=16, rows=3)

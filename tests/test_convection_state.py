@@ -1,0 +1,130 @@
+"""Convection stages and frozen wake states.
+
+CPU: the oracle's composition of the reference's stage (incident pairs -> exclusion CSR -> segments formed as
+segments_velocity forms them -> ordered FP64 direct sum, plus the ambient flow) reproduces the reference's
+``_network_convection`` velocities and Euler / Heun / RK4 steps bit for bit (fixtures made by the reference's own code),
+and a saved frozen state reloads to the same arrays and the reference's ``segments_velocity`` result.
+GPU: the device-resident convection and the loaded state on the device, against the same fixtures: FP64 direct within
+the reference's A1 bound (1e-12 * sum_s |u_s| per point, and that bound times dt for a step), the mixed tree within
+1e-5 relative L2 of the step's displacement.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden
+from oracle import oracle as O
+
+
+def oracle_stage(nodes, edges, gamma, radii, first, model, inflow):
+    """wake._network_convection for a network without rings, restated with the oracle (test infrastructure)."""
+    points = nodes[first:]
+    pairs = O.incident_pairs(nodes, edges, first)
+    csr = O.exclusion_csr(len(points), pairs)
+    starts = nodes[edges[:, 0]]
+    delta = nodes[edges[:, 1]] - starts
+    lengths = np.hypot(np.hypot(delta[..., 0], delta[..., 1]), delta[..., 2])
+    u, flag = O.direct_sum(points, starts, delta / lengths[:, None], lengths, gamma, radii, model, csr, "raise")
+    assert not flag
+    velocity = np.broadcast_to(inflow, points.shape).copy()
+    velocity += u
+    return velocity
+
+
+def oracle_step(g, integrator):
+    nodes, edges, gamma, radii, first = g["nodes"], g["edges"], g["gamma"], g["radii"], int(g["first"])
+    inflow, dt = g["inflow"], float(g["dt"])
+
+    def rhs(points):
+        return oracle_stage(np.concatenate((nodes[:first], points)), edges, gamma, radii, first, 2, inflow)
+    points = nodes[first:].copy()
+    k1 = rhs(points)
+    if integrator == "euler":
+        return points + dt * k1
+    if integrator == "heun":
+        return points + dt * (k1 + rhs(points + dt * k1)) / 2
+    k2 = rhs(points + dt * k1 / 2)
+    k3 = rhs(points + dt * k2 / 2)
+    k4 = rhs(points + dt * k3)
+    return points + dt * (k1 + 2 * k2 + 2 * k3 + k4) / 6
+
+
+def test_oracle_convection_stages_match_reference():
+    g = golden("convection.npz")
+    k1 = oracle_stage(g["nodes"], g["edges"], g["gamma"], g["radii"], int(g["first"]), 2, g["inflow"])
+    assert np.array_equal(k1.view(np.uint64), g["k1"].view(np.uint64))
+    for integrator in ("euler", "heun", "rk4"):
+        got = oracle_step(g, integrator)
+        assert np.array_equal(got.view(np.uint64), g[integrator].view(np.uint64)), integrator
+
+
+def test_frozen_state_roundtrip_and_oracle(tmp_path):
+    from openfawe_b200 import wakestate
+    state = wakestate.load_state(os.path.join(GOLDEN, "frozen_state_input.npz"))
+    path = str(tmp_path / "state_0001.npz")
+    wakestate.save_state(path, state["nodes"], state["edges"], state["gamma"], state["radii"], state["first"],
+                         state["speed"], state["core_model"], state["exclusions"])
+    again = wakestate.load_state(path)
+    for key in wakestate.KEYS:
+        assert np.array_equal(np.asarray(again[key]), np.asarray(state[key])), key
+    nodes, edges, first = state["nodes"], state["edges"], state["first"]
+    starts = nodes[edges[:, 0]]
+    delta = nodes[edges[:, 1]] - starts
+    lengths = np.hypot(np.hypot(delta[..., 0], delta[..., 1]), delta[..., 2])
+    csr = O.exclusion_csr(len(nodes) - first, state["exclusions"])
+    u, _ = O.direct_sum(nodes[first:], starts, delta / lengths[:, None], lengths, state["gamma"], state["radii"], 2,
+                        csr, "raise")
+    assert np.array_equal(u.view(np.uint64), golden("frozen_state.npz")["u"].view(np.uint64))
+    with pytest.raises(ValueError):
+        np.savez(str(tmp_path / "bad.npz"), nodes=nodes)
+        wakestate.load_state(str(tmp_path / "bad.npz"))
+
+
+def _a1_scale(nodes, edges, gamma, radii, first):
+    starts = nodes[edges[:, 0]]
+    delta = nodes[edges[:, 1]] - starts
+    lengths = np.hypot(np.hypot(delta[..., 0], delta[..., 1]), delta[..., 2])
+    pairs, _ = O.pair_matrix(nodes[first:], starts, delta / lengths[:, None], lengths, radii, 2, False)
+    return (np.linalg.norm(pairs, axis=2) * np.abs(gamma)[None, :]).sum(axis=1)
+
+
+@pytest.mark.gpu
+def test_device_convection_matches_reference_steps(device):
+    from openfawe_b200 import convection
+    g = golden("convection.npz")
+    nodes, edges, gamma, radii, first = g["nodes"], g["edges"], g["gamma"], g["radii"], int(g["first"])
+    dt = float(g["dt"])
+    scale = _a1_scale(nodes, edges, gamma, radii, first)
+    import torch
+    dnodes = torch.as_tensor(nodes, device=device)
+    v = convection.network_velocity(dnodes, torch.as_tensor(edges, device=device), torch.as_tensor(gamma, device=device),
+                                    torch.as_tensor(radii, device=device), first, 2, g["inflow"], method="direct",
+                                    precision="fp64")
+    err = np.linalg.norm(v.cpu().numpy() - g["k1"], axis=1)
+    assert np.all(err <= 1e-12 * scale), float((err / scale).max())
+    for integrator in ("euler", "heun", "rk4"):
+        got = convection.convect(nodes, edges, gamma, radii, first, 2, dt, g["inflow"], integrator, method="direct",
+                                 precision="fp64", device=device).cpu().numpy()
+        err = np.linalg.norm(got - g[integrator], axis=1)
+        assert np.all(err <= 4e-12 * scale * dt + 1e-15), integrator
+        step = g[integrator] - nodes[first:]
+        tree = convection.convect(nodes, edges, gamma, radii, first, 2, dt, g["inflow"], integrator, method="tree",
+                                  precision="mixed", theta=0.1, order=3, device=device).cpu().numpy()
+        assert np.linalg.norm(tree - g[integrator]) / np.linalg.norm(step) < 1e-5, integrator
+
+
+@pytest.mark.gpu
+def test_frozen_state_on_device(device):
+    from openfawe_b200 import wakestate
+    wake = wakestate.FrozenWake(os.path.join(GOLDEN, "frozen_state_input.npz"), device)
+    ref = golden("frozen_state.npz")["u"]
+    s = wake.state
+    scale = _a1_scale(s["nodes"], s["edges"], s["gamma"], s["radii"], s["first"])
+    # excluded pairs are left out of the reference's sum, so the bound uses the full scale (larger, still tight)
+    u, flags = wake.velocity("direct", "fp64")
+    assert not flags.any()
+    assert np.all(np.linalg.norm(u.cpu().numpy() - ref, axis=1) <= 1e-12 * scale)
+    ut, _ = wake.velocity("tree", "mixed", theta=0.1, order=3)
+    assert np.linalg.norm(ut.cpu().numpy() - ref) / np.linalg.norm(ref) < 1e-5
+    assert wake.error_over_speed(ut, ref) < 1e-4
