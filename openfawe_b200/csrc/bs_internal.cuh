@@ -402,8 +402,13 @@ __device__ __forceinline__ void far_eval(T rx, T ry, T rz, const T *f, int order
 __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const float4 *f, int order, float &ux,
                                             float &uy, float &uz, const float4 *g = nullptr) {
     const float r2 = rx * rx + ry * ry + rz * rz;
-    const float inv3 = 1.0f / (r2 * sqrtf(r2));
-    const float inv5 = inv3 / r2;
+    // 1/r from the hardware estimate and one Newton-Raphson step for x^(-1/2) (y <- y (3 - x y^2) / 2), then the odd
+    // inverse powers by products: no IEEE division or square root on this path
+    float ir = rsqrtf(r2);
+    ir = ir * fmaf(-0.5f * r2, ir * ir, 1.5f);
+    const float ir2 = ir * ir;
+    const float inv3 = ir * ir2;
+    const float inv5 = inv3 * ir2;
     const float4 q0 = __ldg(f);  // m0 x y z, m1[0]
     float u0 = inv3 * (q0.y * rz - q0.z * ry);
     float u1 = inv3 * (q0.z * rx - q0.x * rz);
@@ -418,7 +423,7 @@ __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const 
         u1 += k * (v2 * rx - v0 * rz) - inv3 * q3.y;
         u2 += k * (v0 * ry - v1 * rx) - inv3 * q3.z;
         if (order >= 2) {
-            const float inv7 = inv5 / r2;
+            const float inv7 = inv5 * ir2;
             const float xx = rx * rx, xy = rx * ry, xz = rx * rz, yy = ry * ry, yz = ry * rz, zz = rz * rz;
             const float4 q4 = __ldg(f + 4), q5 = __ldg(f + 5), q6 = __ldg(f + 6);  // t2[1..2], w2[0..8], m2 s[0]
             const float4 q7 = __ldg(f + 7), q8 = __ldg(f + 8), q9 = __ldg(f + 9), q10 = __ldg(f + 10),
@@ -441,7 +446,7 @@ __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const 
             u1 += (b2 * rx - b0 * rz) - k * w1;
             u2 += (b0 * ry - b1 * rx) - k * w2;
             if (order >= 3) {
-                const float inv9 = inv7 / r2;
+                const float inv9 = inv7 * ir2;
                 const float c000 = xx * rx, c001 = 3.0f * xx * ry, c002 = 3.0f * xx * rz, c011 = 3.0f * xy * ry;
                 const float c012 = 6.0f * xy * rz, c022 = 3.0f * xz * rz, c111 = yy * ry, c112 = 3.0f * yy * rz;
                 const float c122 = 3.0f * yz * rz, c222 = zz * rz;

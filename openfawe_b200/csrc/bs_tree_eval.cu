@@ -23,7 +23,7 @@ constexpr int LIST_CHUNK = 128;           // list entries per chunk of the share
 constexpr int LIST_CHUNKS = 32;           // chunks a unit's list may hold (4096 entries)
 constexpr int LIST_POOL = 4096;           // pool entries per warp of targets
 constexpr int FAR_BIT = int(0x80000000u);
-constexpr int FAR_COST = 3;               // list cost units: one far evaluation ~ three pairs
+constexpr int FAR_COST = 16;              // list cost units: one far evaluation ~ sixteen near pairs (measured)
 constexpr int LIST_WARPS = 4;             // warps per block of the list kernel
 
 struct TreeView {
