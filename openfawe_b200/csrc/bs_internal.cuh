@@ -254,7 +254,9 @@ __device__ __forceinline__ int pair64_at(double px, double py, double pz, const 
 // "suspect" rule, vortex_cuda.py:123-124), a tiny core, or out of FP32's comfortable range -- the FP64 pair then
 // decides value and flags exactly.  The common path has no data-dependent branch; the core factor is computed only
 // where it differs from 1 (Lamb-Oseen past its cut-off, Rankine and Vatistas outside one core radius).  MODEL: 0..5.
-template <int MODEL>
+// NEAR = false leaves out the "within sqrt(near2) core radii" test, for callers that know every pair of the batch lies
+// farther than that from its segment.
+template <int MODEL, bool NEAR = true>
 __device__ __forceinline__ bool pair32(float rx, float ry, float rz, const float4 &hi, const float4 &lo,
                                        const float4 &dir, float near2, float &ux, float &uy, float &uz) {
     const float il = hi.w;
@@ -270,7 +272,7 @@ __device__ __forceinline__ bool pair32(float rx, float ry, float rz, const float
     const float nb2 = fmaf(bx, bx, fmaf(by, by, bz * bz));
     const float big2 = fmaxf(1.0f, fmaxf(na2, nb2));
     bool need64 = !(h2 > 1e-8f * big2) || !(big2 < 1e18f) || irc2 < 0.0f;
-    if (MODEL != 0) {
+    if (MODEL != 0 && NEAR) {
         const float seg2 = t < 0.0f ? na2 : (t > 1.0f ? nb2 : h2);  // distance^2 to the finite segment, units of L^2
         need64 = need64 || (irc2 > 0.0f && seg2 * irc2 < near2);
     }

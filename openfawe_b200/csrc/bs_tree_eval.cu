@@ -123,13 +123,22 @@ __device__ __forceinline__ void far_node(const EvalArgs &a, const Target &t, int
 // One leaf for the lanes in `walk`: the warp stages the leaf's records in shared memory 32 at a time, then every
 // walking lane evaluates its pairs (exclusions skipped through the lane's forward cursor e).
 template <int PREC, int MODEL>
-__device__ __forceinline__ void leaf_pairs(const EvalArgs &a, const Target &t, int lo, int hi, bool walk,
+__device__ __forceinline__ void leaf_pairs(const EvalArgs &a, const Target &t, const NodeRec &nr, bool walk,
                                            int64_t &e, int64_t e1, Seg64 *seg64_tile, Seg32 *seg32_tile,
                                            Acc<PREC> &acc, int &flag, long long &near_pairs,
                                            long long &fp64_pairs) {
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, lo = nr.lo, hi = nr.hi;
     if (walk) while (e < e1 && a.ex_pos[e] < lo) ++e;
     float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+    // When every walking lane is farther from the leaf's bounding sphere than sqrt(near2) of its largest core radius
+    // (with a 1% margin for rounding), no pair of the leaf can need FP64 for its core: the pairs skip that test.
+    bool clear = true;
+    if (PREC != 0 && MODEL != 0 && walk) {
+        const double rx = t.x0 - nr.cx, ry = t.x1 - nr.cy, rz = t.x2 - nr.cz;
+        const double gap = sqrt(rx * rx + ry * ry + rz * rz) - nr.bound;
+        clear = gap > 1.01 * sqrt((double)a.near2) * nr.clear_core;
+    }
+    const bool all_clear = __all_sync(0xffffffffu, clear);
     for (int base = lo; base < hi; base += 32) {
         const int cnt = min(32, hi - base);
         __syncwarp();
@@ -153,7 +162,16 @@ __device__ __forceinline__ void leaf_pairs(const EvalArgs &a, const Target &t, i
             continue;
         }
         unsigned need = 0;
-        if (excl == 0) {  // the common case: every pair of the tile counts
+        if (excl == 0 && all_clear) {  // the common case: every pair of the tile counts, none is near a core
+#pragma unroll 4
+            for (int j = 0; j < cnt; ++j) {
+                const Seg32 &r = seg32_tile[j];
+                const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
+                const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
+                const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
+                if (pair32<MODEL, false>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1u << j;
+            }
+        } else if (excl == 0) {  // every pair counts
 #pragma unroll 4
             for (int j = 0; j < cnt; ++j) {
                 const Seg32 &r = seg32_tile[j];
@@ -301,8 +319,8 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
                     running += (nr.hi - nr.lo) + 2;
                 } else {
                     int64_t ec = e;
-                    leaf_pairs<PREC, MODEL>(a, t, nr.lo, nr.hi, mine && !accept, ec, e1, seg64_tile, seg32_tile, acc,
-                                            flag, near_pairs, fp64_pairs);
+                    leaf_pairs<PREC, MODEL>(a, t, nr, mine && !accept, ec, e1, seg64_tile, seg32_tile, acc, flag,
+                                            near_pairs, fp64_pairs);
                 }
             } else {
                 if (top + 2 > a.stack_limit) {
@@ -400,7 +418,7 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
         } else {
             const NodeRec nr = a.tv.nodes[entry.x];
             int64_t ec = e;  // list entries are not in position order: each leaf scans the exclusions from the start
-            leaf_pairs<PREC, MODEL>(a, t, nr.lo, nr.hi, mine, ec, e1, seg64_tile, seg32_tile, acc, flag, near_pairs,
+            leaf_pairs<PREC, MODEL>(a, t, nr, mine, ec, e1, seg64_tile, seg32_tile, acc, flag, near_pairs,
                                     fp64_pairs);
         }
     }
