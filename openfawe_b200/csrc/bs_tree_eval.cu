@@ -432,7 +432,7 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
 }
 
 template <int PREC, int MODEL>
-__global__ void __launch_bounds__(LIST_WARPS * 32) tree_list_kernel(EvalArgs a, int64_t target_warps) {
+__global__ void __launch_bounds__(LIST_WARPS * 32, 5) tree_list_kernel(EvalArgs a, int64_t target_warps) {
     __shared__ __align__(16) unsigned char tile_mem[LIST_WARPS * 32 * sizeof(Seg64)];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Seg64 *seg64_tile = reinterpret_cast<Seg64 *>(tile_mem) + warp * 32;
