@@ -288,3 +288,33 @@ def test_morton_bottom_up_moments_against_direct_node_sums(device):
         for key, value in zip(("m0", "m1", "m2"), ref[3:]):
             assert np.abs(ex[key] - value).max() <= 1e-12 * seg_scale * len(starts), (leaf, key)
             assert node_relative(value, ex[key]).max() <= 1e-9, (leaf, key)
+
+
+def test_list_overflow_is_evaluated_by_the_walk(device):
+    """A warp whose interaction list outgrows its chunk table (4,096 entries) or the shared pool evaluates the rest in
+    the walk itself: results stay as close to the direct sum as the truncation allows."""
+    from openfawe_b200 import engine, wakes
+    case = wakes.rotor_sheet(60, seed=13, targets=2000)
+    args = wakes.backend_args(case)
+    src = engine.Sources(*args[1:6], device)
+    tgt = engine.Targets(case["points"], None, device)
+    direct, _ = engine.direct(src, tgt, 2, "raise", "fp64")
+    direct = direct.cpu().numpy()
+    tree = engine.build_tree(src, leaf_size=1, kind="morton")
+    for precision, bound in (("fp64", 1e-6), ("mixed", 1e-6)):  # truncation at theta 0.02 is ~5e-8
+        u, flags, far = engine.tree_eval(tree, tgt, 2, "raise", precision, theta=0.02)
+        # thousands of far entries per warp of targets: far beyond one warp's list
+        assert int(far.cpu().numpy().max()) > 4096
+        rel = np.linalg.norm(u.cpu().numpy() - direct) / np.linalg.norm(direct)
+        assert rel < bound and not flags.cpu().numpy().any(), (precision, rel)
+
+
+def test_upload_moves_host_bytes_exactly(device):
+    """bs_upload (pinned staging ring, threaded host copies) delivers every byte, for sizes around its chunk size."""
+    import torch
+    from openfawe_b200 import engine
+    rng = np.random.default_rng(17)
+    for count in (1 << 17, (4 << 20) // 8 + 3, (12 << 20) // 8 - 5):
+        host = rng.normal(size=count)
+        dev = engine.f64(host, torch.device("cuda", device))
+        assert np.array_equal(dev.cpu().numpy(), host)
