@@ -248,12 +248,13 @@ __device__ __forceinline__ int pair64_at(double px, double py, double pz, const 
     return pair64_core(ax, ay, az, t, cx, cy, cz, s, model, raise_singular, ux, uy, uz);
 }
 
-// The single-precision pair.  `rx, ry, rz` is p - s (formed from two-float coordinates); dir.w holds (L/rc)^2, 0 for
-// no core, -1 for a core too small for FP32.  Adds the velocity to (ux, uy, uz) unless the pair needs FP64, which is
-// returned as true: within sqrt(near2) core radii of the finite segment, within 1e-4 L of its axis (the reference's
-// "suspect" rule, vortex_cuda.py:123-124), a tiny core, or out of FP32's comfortable range -- the FP64 pair then
-// decides value and flags exactly.  The common path has no data-dependent branch; the core factor is computed only
-// where it differs from 1 (Lamb-Oseen past its cut-off, Rankine and Vatistas outside one core radius).  MODEL: 0..5.
+// The single-precision pair.  `rx, ry, rz` is p - s (formed from two-float coordinates); hi.w holds 1/L (NaN for a
+// core too small for FP32), dir.w (L/rc)^2, 0 for no core.  Adds the velocity to (ux, uy, uz) unless the pair needs
+// FP64, which is returned as true: within sqrt(near2) core radii of the finite segment, within 1e-4 L of its axis
+// (the reference's "suspect" rule, vortex_cuda.py:123-124; a NaN 1/L fails it too), or out of FP32's comfortable
+// range -- the FP64 pair then decides value and flags exactly.  The common path has no data-dependent branch; the core
+// factor is computed only where it differs from 1 (Lamb-Oseen past its cut-off, Rankine and Vatistas outside one core
+// radius).  MODEL: 0..5.
 // NEAR = false leaves out the "within sqrt(near2) core radii" test, for callers that know every pair of the batch lies
 // farther than that from its segment.
 template <int MODEL, bool NEAR = true>
@@ -271,7 +272,7 @@ __device__ __forceinline__ bool pair32(float rx, float ry, float rz, const float
     const float bx = ax - dx, by = ay - dy, bz = az - dz;
     const float nb2 = fmaf(bx, bx, fmaf(by, by, bz * bz));
     const float big2 = fmaxf(1.0f, fmaxf(na2, nb2));
-    bool need64 = !(h2 > 1e-8f * big2) || !(big2 < 1e18f) || irc2 < 0.0f;
+    bool need64 = !(h2 > 1e-8f * big2) || !(big2 < 1e18f);
     if (MODEL != 0 && NEAR) {
         const float seg2 = t < 0.0f ? na2 : (t > 1.0f ? nb2 : h2);  // distance^2 to the finite segment, units of L^2
         need64 = need64 || (irc2 > 0.0f && seg2 * irc2 < near2);

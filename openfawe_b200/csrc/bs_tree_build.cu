@@ -64,12 +64,13 @@ __global__ void pack_kernel(int64_t m, const double *starts, const double *direc
         split2(sx, q.hi.x, q.lo.x);
         split2(sy, q.hi.y, q.lo.y);
         split2(sz, q.hi.z, q.lo.z);
-        q.hi.w = (float)(1.0 / L);
+        // a core with rc/L below FP32's comfortable range sends all its pairs to FP64: 1/L is stored as NaN, which
+        // fails the pair's "suspect" test; (L/rc)^2 then 0, as without a core
+        const double rcl = r / L;
+        const bool tiny = r > 0.0 && rcl < 1e-15;
+        q.hi.w = tiny ? __int_as_float(0x7fc00000) : (float)(1.0 / L);
         q.lo.w = (float)((g / L) / 12.566370614359172);
-        // (L/rc)^2; 0 without a core; -1 marks rc/L below FP32's comfortable range (its pairs are done in FP64)
-        double rcl = r / L;
-        q.dir = make_float4((float)dx, (float)dy, (float)dz,
-                            r > 0.0 ? (rcl >= 1e-15 ? (float)(1.0 / (rcl * rcl)) : -1.0f) : 0.0f);
+        q.dir = make_float4((float)dx, (float)dy, (float)dz, (r > 0.0 && !tiny) ? (float)(1.0 / (rcl * rcl)) : 0.0f);
         seg32[k] = q;
     }
     if (geo) {

@@ -162,7 +162,16 @@ __device__ __forceinline__ void leaf_pairs(const EvalArgs &a, const Target &t, c
             continue;
         }
         unsigned need = 0;
-        if (excl == 0 && all_clear) {  // the common case: every pair of the tile counts, none is near a core
+        if (excl == 0 && all_clear && cnt == 32) {  // the common case: a full tile, every pair counts, none near a core
+#pragma unroll 8
+            for (int j = 0; j < 32; ++j) {
+                const Seg32 &r = seg32_tile[j];
+                const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
+                const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
+                const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
+                if (pair32<MODEL, false>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1u << j;
+            }
+        } else if (excl == 0 && all_clear) {
 #pragma unroll 4
             for (int j = 0; j < cnt; ++j) {
                 const Seg32 &r = seg32_tile[j];
