@@ -34,7 +34,8 @@ THETA, ORDER, LEAF, CLEARANCE = 0.12, 3, 256, 3.0
 REF_THETA, REF_ORDER, REF_LEAF = 0.04, 2, 32
 W_PAIR, W_VISIT = 62.0, 12.0            # algorithmic flops per near pair and per visited node
 LIST_TRAFFIC = None                     # DRAM bytes per list-kernel launch from an ncu capture (None: not captured)
-W_FAR = {0: 40.0, 1: 100.0, 2: 180.0, 3: 350.0}  # per far evaluation of order p (3: 180 + 170 for the third term)
+# per far evaluation of order p (3: 180 + 170 for the third term, 4: 350 + 300 for the fourth)
+W_FAR = {0: 40.0, 1: 100.0, 2: 180.0, 3: 350.0, 4: 650.0}
 L2_FLUSH_BYTES = 512 << 20  # larger than the 126 MB L2
 
 
@@ -47,7 +48,7 @@ def parse():
     p.add_argument("--rows", type=int, default=ROWS)
     p.add_argument("--theta", type=float, default=THETA)
     p.add_argument("--leaf", type=int, default=LEAF)
-    p.add_argument("--order", type=int, default=ORDER, choices=(0, 1, 2, 3))
+    p.add_argument("--order", type=int, default=ORDER, choices=(0, 1, 2, 3, 4))
     p.add_argument("--kind", default="morton", choices=("morton", "median"))
     p.add_argument("--cpu-sample", type=int, default=1024, help="targets in the CPU-baseline sample")
     p.add_argument("--no-extras", action="store_true", help="skip the batched-wakes and adjoint measurements")

@@ -140,6 +140,14 @@ enum { G_M3 = 0, G_T3 = 30, G_W3 = 39, G_W3V = 57 };
 // [+13, +19) W3 row, then w3 at [60, 63).
 enum { H_ROW = 20, H_M3 = 0, H_T3 = 10, H_W3 = 13, H_W3V = 60 };
 
+// Fourth-order far-field coefficients (trees built for order 4), one row of 36 per component i (nine float4), in both
+// precisions: [0, 15) m4[i] symmetric (0000,0001,0002,0011,0012,0022,0111,0112,0122,0222,1111,1112,1122,1222,2222),
+// [15, 21) T4[i][l][m] = m4[i][j][j][l][m] symmetric, [21] tau4[i] = T4[i][l][l], [22, 32) W4[i][k][l][m] =
+// eps_ibc m4[b][c][k][l][m] symmetric, [32, 35) W4T[i][m] = eps_ibc T4[b][c][m], [35] zero.
+enum { K_ROW = 36, K_M4 = 0, K_T4 = 15, K_TAU4 = 21, K_W4 = 22, K_W4T = 32 };
+struct __align__(16) Far64y { double v[112]; };
+struct __align__(16) Far32y { float v[112]; };
+
 // ---------------------------------------------------------------------------------------------------------------------
 // Arithmetic helpers.
 // ---------------------------------------------------------------------------------------------------------------------
@@ -327,12 +335,49 @@ __device__ __forceinline__ bool pair32(float rx, float ry, float rz, const float
     return need64;
 }
 
+// The fourth-order term of the expansion, R = x - c:
+//   (39.375 S4 / r^11 - 26.25 T4:RR / r^9 + 1.875 tau4 / r^7) x R - 17.5 W4:RRR / r^9 + 7.5 W4T R / r^7,
+// S4_i = m4[i] : RRRR.  It is linear in the component rows, so row i (K_ROW values) adds its own share:
+// x4_i (e_i x R) + w_i e_i.
+template <class T>
+__device__ __forceinline__ void far_term4_row(T rx, T ry, T rz, T inv7, T inv9, T inv11, const T *r, int i, T &u0,
+                                              T &u1, T &u2) {
+    const T xx = rx * rx, xy = rx * ry, xz = rx * rz, yy = ry * ry, yz = ry * rz, zz = rz * rz;
+    // monomials of the symmetric components times their multiplicities
+    const T q4[15] = {xx * xx, T(4) * xx * xy, T(4) * xx * xz, T(6) * xx * yy, T(12) * xx * yz, T(6) * xx * zz,
+                      T(4) * xy * yy, T(12) * xy * yz, T(12) * xy * zz, T(4) * xz * zz, yy * yy, T(4) * yy * yz,
+                      T(6) * yy * zz, T(4) * yz * zz, zz * zz};
+    const T q3[10] = {xx * rx, T(3) * xx * ry, T(3) * xx * rz, T(3) * xy * ry, T(6) * xy * rz, T(3) * xz * rz,
+                      yy * ry, T(3) * yy * rz, T(3) * yz * rz, zz * rz};
+    const T q2[6] = {xx, T(2) * xy, T(2) * xz, yy, T(2) * yz, zz};
+    T s4 = 0, t4 = 0, w4 = 0;
+#pragma unroll
+    for (int q = 0; q < 15; ++q) s4 += r[K_M4 + q] * q4[q];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) t4 += r[K_T4 + q] * q2[q];
+#pragma unroll
+    for (int q = 0; q < 10; ++q) w4 += r[K_W4 + q] * q3[q];
+    const T x4 = T(39.375) * inv11 * s4 - T(26.25) * inv9 * t4 + T(1.875) * inv7 * r[K_TAU4];
+    const T w = T(7.5) * inv7 * (r[K_W4T] * rx + r[K_W4T + 1] * ry + r[K_W4T + 2] * rz) - T(17.5) * inv9 * w4;
+    if (i == 0) { u0 += w; u1 -= x4 * rz; u2 += x4 * ry; }
+    else if (i == 1) { u0 += x4 * rz; u1 += w; u2 -= x4 * rx; }
+    else { u0 -= x4 * ry; u1 += x4 * rx; u2 += w; }
+}
+
+template <class T>
+__device__ __forceinline__ void far_term4(T rx, T ry, T rz, T inv7, T inv9, T inv11, const T *h, T &u0, T &u1,
+                                          T &u2) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) far_term4_row<T>(rx, ry, rz, inv7, inv9, inv11, h + K_ROW * i, i, u0, u1, u2);
+}
+
 // vortex_tree.far_velocity with the symmetric second moment; R = x - c.  Order 3 (g: the third-order record) adds
 //   (17.5 S3 / r^9 - 7.5 T3 R / r^7) x R - 7.5 (W3 : R R) / r^7 + 1.5 w3 / r^5,  S3_b = m3[b] : R R R,
-// the next term of the same Taylor series of the segments' line integrals about the node centre.
+// the next term of the same Taylor series of the segments' line integrals about the node centre; order 4 (k4: the
+// fourth-order record) adds far_term4.
 template <class T>
 __device__ __forceinline__ void far_eval(T rx, T ry, T rz, const T *f, int order, T &ux, T &uy, T &uz,
-                                         const T *g = nullptr) {
+                                         const T *g = nullptr, const T *k4 = nullptr) {
     T r2 = rx * rx + ry * ry + rz * rz;
     T inv3 = T(1) / (r2 * sqrt(r2));
     T inv5 = inv3 / r2;
@@ -393,6 +438,7 @@ __device__ __forceinline__ void far_eval(T rx, T ry, T rz, const T *f, int order
             u0 += (x3[1] * rz - x3[2] * ry) - c7 * w[0] + c5 * g[G_W3V + 0];
             u1 += (x3[2] * rx - x3[0] * rz) - c7 * w[1] + c5 * g[G_W3V + 1];
             u2 += (x3[0] * ry - x3[1] * rx) - c7 * w[2] + c5 * g[G_W3V + 2];
+            if (order >= 4) far_term4<T>(rx, ry, rz, inv7, inv9, inv9 / r2, k4, u0, u1, u2);
         }
     }
     ux += T(INV_FOUR_PI) * u0;
@@ -400,10 +446,12 @@ __device__ __forceinline__ void far_eval(T rx, T ry, T rz, const T *f, int order
     uz += T(INV_FOUR_PI) * u2;
 }
 
-// far_eval<float> reading the packed records (Far32: 12 float4, Far32x: 16 float4) in vector loads, one group at a
-// time where it is used, so that only one order's coefficients are live at once.  Same arithmetic as far_eval.
+// far_eval<float> reading the packed records (Far32: 12 float4, Far32x: 16 float4, Far32y: 28 float4) in vector
+// loads, one group at a time where it is used, so that only one order's coefficients are live at once.  Same
+// arithmetic as far_eval.
 __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const float4 *f, int order, float &ux,
-                                            float &uy, float &uz, const float4 *g = nullptr) {
+                                            float &uy, float &uz, const float4 *g = nullptr,
+                                            const float4 *k4 = nullptr) {
     const float r2 = rx * rx + ry * ry + rz * rz;
     // 1/r from the hardware estimate and one Newton-Raphson step for x^(-1/2) (y <- y (3 - x y^2) / 2), then the odd
     // inverse powers by products: no IEEE division or square root on this path
@@ -474,6 +522,20 @@ __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const 
                 u0 += (x3[1] * rz - x3[2] * ry) - c7 * w[0] + c5 * wv.x;
                 u1 += (x3[2] * rx - x3[0] * rz) - c7 * w[1] + c5 * wv.y;
                 u2 += (x3[0] * ry - x3[1] * rx) - c7 * w[2] + c5 * wv.z;
+                if (order >= 4) {
+                    // one component row at a time (nine float4), through the shared fourth-order term
+                    const float inv11 = inv9 * ir2;
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        float h[K_ROW];
+#pragma unroll
+                        for (int q = 0; q < K_ROW / 4; ++q) {
+                            const float4 x = __ldg(k4 + (K_ROW / 4) * i + q);
+                            h[4 * q] = x.x; h[4 * q + 1] = x.y; h[4 * q + 2] = x.z; h[4 * q + 3] = x.w;
+                        }
+                        far_term4_row<float>(rx, ry, rz, inv7, inv9, inv11, h, i, u0, u1, u2);
+                    }
+                }
             }
         }
     }

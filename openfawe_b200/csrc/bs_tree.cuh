@@ -31,7 +31,9 @@ struct bs_tree {
     bs::Far32 *far32 = nullptr;
     bs::Far64x *far64x = nullptr;  // third-order records (trees built for order 3 only)
     bs::Far32x *far32x = nullptr;
-    int order3 = 0;
+    bs::Far64y *far64y = nullptr;  // fourth-order records (trees built for order 4 only)
+    bs::Far32y *far32y = nullptr;
+    int order3 = 0, order4 = 0;
     bs::Seg64 *seg64 = nullptr;  // tree order
     bs::Seg32 *seg32 = nullptr;  // tree order
     uint64_t *keys = nullptr;    // Morton keys (input order), Morton trees only

@@ -25,6 +25,7 @@ constexpr int CHUNK = 2048;
 constexpr int MOM_THREADS = 256;
 constexpr int MOM_PARTS = 31;   // r2 + m0 (3) + m1 (9) + m2 symmetric (18)
 constexpr int MOM_PARTS3 = 61;  // ... + m3 symmetric (30), for third-order trees
+constexpr int MOM_PARTS4 = 106; // ... + m4 symmetric (45), for fourth-order trees
 
 __device__ __forceinline__ uint64_t ordered_bits(double x) {
     uint64_t b = (uint64_t)__double_as_longlong(x + 0.0);  // -0.0 -> +0.0 (equal keys compare equal)
@@ -852,6 +853,27 @@ __device__ __forceinline__ int sym3(int j, int k, int l) {
     return a == 0 ? (b == 0 ? c : (b == 1 ? 2 + c : 5)) : (a == 1 ? (b == 1 ? 5 + c : 8) : 9);
 }
 
+// Index of the symmetric fourth-order component (j, k, l, m) in 0000,0001,0002,0011,0012,0022,0111,0112,0122,0222,
+// 1111,1112,1122,1222,2222: the base-3 code of the sorted indices through a table (-1: not sorted).
+__constant__ signed char c_sym4[81] = {
+    0,  1,  2,  -1, 3,  4,  -1, -1, 5,  -1, -1, -1, -1, 6,  7,  -1, -1, 8,  -1, -1, -1, -1, -1, -1, -1, -1, 9,
+    -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, 10, 11, -1, -1, 12, -1, -1, -1, -1, -1, -1, -1, -1, 13,
+    -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, 14};
+__device__ __forceinline__ int sym4(int j, int k, int l, int m) {
+    int t;
+    if (j > k) { t = j; j = k; k = t; }
+    if (l > m) { t = l; l = m; m = t; }
+    if (j > l) { t = j; j = l; l = t; }
+    if (k > m) { t = k; k = m; m = t; }
+    if (k > l) { t = k; k = l; l = t; }
+    return c_sym4[27 * j + 9 * k + 3 * l + m];
+}
+
+// The symmetric index pairs (m2, T4) and triples (m3, W4) in storage order.
+__constant__ signed char c_kl[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+__constant__ signed char c_jkl[10][3] = {{0, 0, 0}, {0, 0, 1}, {0, 0, 2}, {0, 1, 1}, {0, 1, 2},
+                                         {0, 2, 2}, {1, 1, 1}, {1, 1, 2}, {1, 2, 2}, {2, 2, 2}};
+
 // The outputs of the moment pipelines for one node.
 struct NodeOut {
     const int64_t *lo, *hi, *left, *right;
@@ -862,10 +884,12 @@ struct NodeOut {
     Far32 *far32;
     Far64x *far64x;
     Far32x *far32x;
+    Far64y *far64y;
+    Far32y *far32y;
 };
 
-// Node j from its sums v (bound^2, m0, m1, symmetric m2 [, symmetric m3]) about its centre: the export arrays, the
-// contractions and the packed traversal / far records.
+// Node j from its sums v (bound^2, m0, m1, symmetric m2 [, symmetric m3 [, symmetric m4]]) about its centre: the
+// export arrays, the contractions and the packed traversal / far records.
 template <int PARTS>
 __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
     double *bound = o.bound, *m0 = o.m0, *m1 = o.m1, *m2 = o.m2, *w1 = o.w1, *t2 = o.t2, *w2 = o.w2;
@@ -911,7 +935,7 @@ __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
         far64[j].v[q] = f[q];
         far32[j].v[q] = (float)f[q];
     }
-    if (PARTS == MOM_PARTS3) {
+    if (PARTS >= MOM_PARTS3) {
         const double *M3 = v + 31;  // M3[10 b + sym3(j, k, l)]
         double g[BS_FAR3_N], T3[9];
         for (int q = 0; q < 30; ++q) g[G_M3 + q] = M3[q];
@@ -940,6 +964,42 @@ __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
         }
         for (int q = 0; q < 3; ++q) h[H_W3V + q] = (float)g[G_W3V + q];
         for (int q = 0; q < 64; ++q) far32x[j].v[q] = h[q];
+    }
+    if (PARTS == MOM_PARTS4) {
+        const double *M4 = v + 61;  // M4[15 b + sym4(j, k, l, m)]
+        double T4[3][6];            // T4[b][(l, m)] = M4[b][j][j][l][m]
+        for (int b4 = 0; b4 < 3; ++b4)
+            for (int p = 0; p < 6; ++p) {
+                const int l4 = c_kl[p][0], n4 = c_kl[p][1];
+                T4[b4][p] = M4[15 * b4 + sym4(0, 0, l4, n4)] + M4[15 * b4 + sym4(1, 1, l4, n4)] +
+                            M4[15 * b4 + sym4(2, 2, l4, n4)];
+            }
+        auto t4 = [&](int b4, int c4, int n4) {
+            const int x = c4 < n4 ? c4 : n4, y = c4 < n4 ? n4 : c4;
+            return T4[b4][x == 0 ? y : (x == 1 ? 2 + y : 5)];
+        };
+        // eps_ibc X[b][c] = X[b'][c'] - X[c'][b'] with (b', c') = (1, 2), (2, 0), (0, 1) for i = 0, 1, 2
+        for (int i = 0; i < 3; ++i) {
+            const int b4 = (i + 1) % 3, c4 = (i + 2) % 3;
+            double row[K_ROW];
+            for (int q = 0; q < K_ROW; ++q) row[q] = 0.0;
+            for (int q = 0; q < 15; ++q) row[K_M4 + q] = M4[15 * i + q];
+            for (int p = 0; p < 6; ++p) row[K_T4 + p] = T4[i][p];
+            row[K_TAU4] = T4[i][0] + T4[i][3] + T4[i][5];
+            for (int q = 0; q < 10; ++q) {
+                const int k4 = c_jkl[q][0], l4 = c_jkl[q][1], n4 = c_jkl[q][2];
+                row[K_W4 + q] = M4[15 * b4 + sym4(c4, k4, l4, n4)] - M4[15 * c4 + sym4(b4, k4, l4, n4)];
+            }
+            for (int n4 = 0; n4 < 3; ++n4) row[K_W4T + n4] = t4(b4, c4, n4) - t4(c4, b4, n4);
+            for (int q = 0; q < K_ROW; ++q) {
+                o.far64y[j].v[K_ROW * i + q] = row[q];
+                o.far32y[j].v[K_ROW * i + q] = (float)row[q];
+            }
+        }
+        for (int q = 3 * K_ROW; q < 112; ++q) {
+            o.far64y[j].v[q] = 0.0;
+            o.far32y[j].v[q] = 0.f;
+        }
     }
     NodeRec r;
     r.cx = centre[3 * j]; r.cy = centre[3 * j + 1]; r.cz = centre[3 * j + 2];
@@ -971,6 +1031,8 @@ __global__ void moment_final_kernel(int64_t count, const int64_t *first, const i
 // core from its children (exact) and its moments by translating the children's to its centre
 //   m1_ij += m0_i D_j,  m2_ijk += m1_ij D_k + m1_ik D_j + m0_i D_j D_k,
 //   m3_ijkl += D_j m2_ikl + D_k m2_ijl + D_l m2_ijk + D_j D_k m1_il + D_j D_l m1_ik + D_k D_l m1_ij + D_j D_k D_l m0_i
+// and for fourth-order trees
+//   m4_ijklm += the 4 D m3, 6 D D m2, 4 D D D m1 and D D D D m0 terms of the same binomial expansion
 // (D = child centre - node centre; left child first, then right), which equals the direct sums up to rounding.  The
 // bounding radius stays exact: one pass over the internal nodes' ranges of tree-ordered endpoints.
 // ---------------------------------------------------------------------------------------------------------------------
@@ -995,94 +1057,204 @@ __global__ void parent_kernel(int64_t count, const int64_t *left, const int64_t 
     }
 }
 
-// Adds one segment's bound^2 and moments about (c0, c1, c2) to acc (the accumulation of moment_sum_kernel).
-template <int PARTS>
-__device__ __forceinline__ void accumulate_segment(const SegGeo &g, double c0, double c1, double c2, double *acc) {
-    double a0 = g.sx - c0, a1 = g.sy - c1, a2 = g.sz - c2;
-    double b0 = g.ex - c0, b1 = g.ey - c1, b2 = g.ez - c2;
-    double ra = __dadd_rn(__dadd_rn(__dmul_rn(a0, a0), __dmul_rn(a1, a1)), __dmul_rn(a2, a2));
-    double rb = __dadd_rn(__dadd_rn(__dmul_rn(b0, b0), __dmul_rn(b1, b1)), __dmul_rn(b2, b2));
-    acc[0] = fmax(acc[0], fmax(ra, rb));
-    if (g.gamma == 0.0) return;
-    double d[3] = {0.5 * (g.sx + g.ex) - c0, 0.5 * (g.sy + g.ey) - c1, 0.5 * (g.sz + g.ez) - c2};
-    double l[3] = {g.lx, g.ly, g.lz};
-    double al[3] = {g.gamma * g.lx, g.gamma * g.ly, g.gamma * g.lz};
-    double sym[6];
-    int q = 0;
-#pragma unroll
-    for (int j = 0; j < 3; ++j)
-#pragma unroll
-        for (int k2 = j; k2 < 3; ++k2) sym[q++] = d[j] * d[k2] + l[j] * l[k2] * (1.0 / 12.0);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        acc[1 + i] += al[i];
-#pragma unroll
-        for (int j = 0; j < 3; ++j) acc[4 + 3 * i + j] += al[i] * d[j];
-#pragma unroll
-        for (int p = 0; p < 6; ++p) acc[13 + 6 * i + p] += al[i] * sym[p];
+// The symmetric index tuples of orders 0..4 in storage order (order, then lexicographic): (), 0, 1, 2, 00, 01, ..., 2222
+// -- 1 + 3 + 6 + 10 + 15 = 35.  Moment (i; tuple of order n, rank r among the order-n tuples) is stored at
+// T_BASE[n] + T_CNT[n] i + r of a node's sums (index 0 holds bound^2).  src[u][mask]: where the tuple left after
+// removing the positions in `mask` from tuple u is stored (T_BASE + rank, plus T_CNT << 8).
+constexpr int T_FIRST[5] = {0, 1, 4, 10, 20}, T_BASE[5] = {1, 4, 13, 31, 61}, T_CNT[5] = {1, 3, 6, 10, 15};
+struct TupleTables {
+    unsigned char n[35], packed[35];  // order and indices (two bits each, first index in the low bits)
+    unsigned char out0[35], cnt[35];  // moment (i; u) is stored at out0[u] + cnt[u] i
+    unsigned short src[35][16];
+};
+constexpr TupleTables make_tuple_tables() {
+    TupleTables t{};
+    int u = 0;
+    for (int n = 0; n <= 4; ++n) {
+        int codes = 1;
+        for (int k = 0; k < n; ++k) codes *= 3;
+        for (int code = 0; code < codes; ++code) {  // base-3 codes, first index most significant: lexicographic
+            int dig[4] = {0, 0, 0, 0}, c = code;
+            for (int s = n - 1; s >= 0; --s) { dig[s] = c % 3; c /= 3; }
+            bool sorted = true;
+            for (int s = 1; s < n; ++s) sorted = sorted && dig[s - 1] <= dig[s];
+            if (!sorted) continue;
+            int pk = 0;
+            for (int s = 0; s < n; ++s) pk |= dig[s] << (2 * s);
+            t.n[u] = (unsigned char)n;
+            t.packed[u] = (unsigned char)pk;
+            t.out0[u] = (unsigned char)(T_BASE[n] + u - T_FIRST[n]);
+            t.cnt[u] = (unsigned char)T_CNT[n];
+            ++u;
+        }
     }
-    if (PARTS == MOM_PARTS3) {
-        double cub[10];
-        int q3 = 0;
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-#pragma unroll
-            for (int k2 = j; k2 < 3; ++k2)
-#pragma unroll
-                for (int l2 = k2; l2 < 3; ++l2)
-                    cub[q3++] = d[j] * d[k2] * d[l2] +
-                                (d[j] * l[k2] * l[l2] + l[j] * d[k2] * l[l2] + l[j] * l[k2] * d[l2]) * (1.0 / 12.0);
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int p = 0; p < 10; ++p) acc[31 + 10 * i + p] += al[i] * cub[p];
+    for (int v = 0; v < 35; ++v) {
+        const int n = t.n[v];
+        for (int mask = 0; mask < (1 << n); ++mask) {
+            int rest = 0, m = 0;
+            for (int s = 0; s < n; ++s)
+                if (!((mask >> s) & 1)) rest |= ((t.packed[v] >> (2 * s)) & 3) << (2 * m++);
+            int w = T_FIRST[m];
+            while (t.n[w] != m || t.packed[w] != rest) ++w;
+            t.src[v][mask] = (unsigned short)((T_BASE[m] + w - T_FIRST[m]) | (T_CNT[m] << 8));
+        }
+    }
+    return t;
+}
+__constant__ TupleTables c_tt = make_tuple_tables();
+
+template <int PARTS>
+struct MomentTuples {
+    static constexpr int n = PARTS == MOM_PARTS ? 10 : (PARTS == MOM_PARTS3 ? 20 : 35);  // tuples up to the order
+    static constexpr int slots = (n + 31) / 32;                                         // tuples per lane
+};
+
+// Storage index of moment (i; tuple u).
+__device__ __forceinline__ int tuple_out(int u, int i) { return c_tt.out0[u] + c_tt.cnt[u] * i; }
+
+// The box of the leaf's segments [a, b) and their largest core radius, reduced over the warp.
+__device__ __forceinline__ void leaf_extent(int lane, int64_t a, int64_t b, const int32_t *order, const SegGeo *geo,
+                                            double *mn, double *mx, double &c) {
+    for (int x = 0; x < 3; ++x) {
+        mn[x] = INFINITY;
+        mx[x] = -INFINITY;
+    }
+    c = 0.0;
+    for (int64_t k = a + lane; k < b; k += 32) {
+        const SegGeo g = geo[order[k]];
+        mn[0] = fmin(mn[0], fmin(g.sx, g.ex)); mx[0] = fmax(mx[0], fmax(g.sx, g.ex));
+        mn[1] = fmin(mn[1], fmin(g.sy, g.ey)); mx[1] = fmax(mx[1], fmax(g.sy, g.ey));
+        mn[2] = fmin(mn[2], fmin(g.sz, g.ez)); mx[2] = fmax(mx[2], fmax(g.sz, g.ez));
+        c = fmax(c, g.radius);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int x = 0; x < 3; ++x) {
+            mn[x] = fmin(mn[x], __shfl_xor_sync(0xffffffffu, mn[x], o));
+            mx[x] = fmax(mx[x], __shfl_xor_sync(0xffffffffu, mx[x], o));
+        }
+        c = fmax(c, __shfl_xor_sync(0xffffffffu, c, o));
     }
 }
 
-// One warp per leaf: box, core and centre, then bound^2 and moments about the centre; sums[j][PARTS].
+// <rho_a1 .. rho_an> over one segment for the index tuples u < NT in storage order, rho = d + t l with t uniform on
+// [-1/2, 1/2] (<t^2> = 1/12, <t^4> = 1/80, odd moments 0): m2 takes d d + l l / 12, m3 d d d + (d l l + l d l +
+// l l d) / 12, m4 d d d d + (the six placements of two l's) / 12 + l l l l / 80.
+template <int NT>
+__device__ __forceinline__ void segment_means(const double *d, const double *l, double *g) {
+    double dd[3][3], ll[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = a; b < 3; ++b) {
+            dd[a][b] = dd[b][a] = d[a] * d[b];
+            ll[a][b] = ll[b][a] = l[a] * l[b];
+        }
+    g[0] = 1.0;
+    g[1] = d[0]; g[2] = d[1]; g[3] = d[2];
+    int u = 4;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = a; b < 3; ++b) g[u++] = fma(ll[a][b], 1.0 / 12.0, dd[a][b]);
+    if (NT > 10) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = a; b < 3; ++b)
+#pragma unroll
+                for (int c = b; c < 3; ++c)
+                    g[u++] = d[a] * dd[b][c] + (d[a] * ll[b][c] + l[a] * (d[b] * l[c] + l[b] * d[c])) * (1.0 / 12.0);
+    }
+    if (NT > 20) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = a; b < 3; ++b)
+#pragma unroll
+                for (int c = b; c < 3; ++c)
+#pragma unroll
+                    for (int e = c; e < 3; ++e) {
+                        const double pairs = ll[a][b] * dd[c][e] + ll[a][c] * dd[b][e] + ll[a][e] * dd[b][c] +
+                                             ll[b][c] * dd[a][e] + ll[b][e] * dd[a][c] + ll[c][e] * dd[a][b];
+                        g[u++] = dd[a][b] * dd[c][e] + pairs * (1.0 / 12.0) + ll[a][b] * ll[c][e] * (1.0 / 80.0);
+                    }
+    }
+}
+
+// One warp per leaf: box, core and centre, then bound^2 and the moments about the centre; sums[j][PARTS].  The warp
+// takes 32 segments at a time: each lane forms its segment's means (segment_means) and alpha = gamma l into shared
+// memory, then lane u sums, over the 32, alpha_i times the mean of index tuple u (and of u + 32) for i = 0..2.
 template <int PARTS>
 __global__ void __launch_bounds__(128) leaf_moments_kernel(int64_t count, const int64_t *lo, const int64_t *hi,
                                                            const int64_t *left, const int32_t *order,
                                                            const SegGeo *geo, double *box, double *centre,
                                                            double *core, double *sums) {
-    const int lane = threadIdx.x & 31;
+    using MT = MomentTuples<PARTS>;
+    constexpr int ROWS = MT::n + 3, STRIDE = 33;  // means, then alpha; padded rows: lanes of a column hit other banks
+    __shared__ double st[4][ROWS * STRIDE];
+    const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 3;
+    double *sw = st[w];
+    bool own[MT::slots];
+#pragma unroll
+    for (int r = 0; r < MT::slots; ++r) own[r] = lane + 32 * r < MT::n;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t j = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); j < count; j += warps) {
         if (left[j] >= 0) continue;
         const int64_t a = lo[j], b = hi[j];
-        double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY}, c = 0.0;
-        for (int64_t k = a + lane; k < b; k += 32) {
-            const SegGeo g = geo[order[k]];
-            mn[0] = fmin(mn[0], fmin(g.sx, g.ex)); mx[0] = fmax(mx[0], fmax(g.sx, g.ex));
-            mn[1] = fmin(mn[1], fmin(g.sy, g.ey)); mx[1] = fmax(mx[1], fmax(g.sy, g.ey));
-            mn[2] = fmin(mn[2], fmin(g.sz, g.ez)); mx[2] = fmax(mx[2], fmax(g.sz, g.ez));
-            c = fmax(c, g.radius);
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            for (int x = 0; x < 3; ++x) {
-                mn[x] = fmin(mn[x], __shfl_xor_sync(0xffffffffu, mn[x], o));
-                mx[x] = fmax(mx[x], __shfl_xor_sync(0xffffffffu, mx[x], o));
-            }
-            c = fmax(c, __shfl_xor_sync(0xffffffffu, c, o));
-        }
+        double mn[3], mx[3], c;
+        leaf_extent(lane, a, b, order, geo, mn, mx, c);
         const double c0 = 0.5 * (mn[0] + mx[0]), c1 = 0.5 * (mn[1] + mx[1]), c2 = 0.5 * (mn[2] + mx[2]);
-        double acc[PARTS];
+        double acc[MT::slots][3], r2 = 0.0;
 #pragma unroll
-        for (int q = 0; q < PARTS; ++q) acc[q] = 0.0;
-        for (int64_t k = a + lane; k < b; k += 32) accumulate_segment<PARTS>(geo[order[k]], c0, c1, c2, acc);
+        for (int r = 0; r < MT::slots; ++r) acc[r][0] = acc[r][1] = acc[r][2] = 0.0;
+        for (int64_t base = a; base < b; base += 32) {
+            const int64_t k = base + lane;
+            double g[MT::n], al[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-        for (int q = 0; q < PARTS; ++q) {
-            double v = acc[q];
-            for (int o = 16; o > 0; o >>= 1) {
-                double w = __shfl_xor_sync(0xffffffffu, v, o);
-                v = q == 0 ? fmax(v, w) : v + w;
+            for (int q = 0; q < MT::n; ++q) g[q] = 0.0;
+            if (k < b) {
+                const SegGeo e = geo[order[k]];
+                const double a0 = e.sx - c0, a1 = e.sy - c1, a2 = e.sz - c2;
+                const double b0 = e.ex - c0, b1 = e.ey - c1, b2 = e.ez - c2;
+                // the reference's ((x^2 + y^2) + z^2) without contraction, as in every bound of this file
+                const double ra = __dadd_rn(__dadd_rn(__dmul_rn(a0, a0), __dmul_rn(a1, a1)), __dmul_rn(a2, a2));
+                const double rb = __dadd_rn(__dadd_rn(__dmul_rn(b0, b0), __dmul_rn(b1, b1)), __dmul_rn(b2, b2));
+                r2 = fmax(r2, fmax(ra, rb));
+                if (e.gamma != 0.0) {  // a segment without circulation adds nothing (and no non-finite geometry)
+                    const double d[3] = {0.5 * (e.sx + e.ex) - c0, 0.5 * (e.sy + e.ey) - c1, 0.5 * (e.sz + e.ez) - c2};
+                    const double l[3] = {e.lx, e.ly, e.lz};
+                    segment_means<MT::n>(d, l, g);
+                    al[0] = e.gamma * e.lx; al[1] = e.gamma * e.ly; al[2] = e.gamma * e.lz;
+                }
             }
-            acc[q] = v;
-        }
 #pragma unroll
-        for (int q = 0; q < PARTS; ++q)
-            if (lane == (q & 31)) sums[(int64_t)PARTS * j + q] = acc[q];
+            for (int q = 0; q < MT::n; ++q) sw[q * STRIDE + lane] = g[q];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) sw[(MT::n + i) * STRIDE + lane] = al[i];
+            __syncwarp();
+#pragma unroll 4
+            for (int s2 = 0; s2 < 32; ++s2) {
+                const double x0 = sw[MT::n * STRIDE + s2], x1 = sw[(MT::n + 1) * STRIDE + s2],
+                             x2 = sw[(MT::n + 2) * STRIDE + s2];
+#pragma unroll
+                for (int r = 0; r < MT::slots; ++r) {
+                    if (!own[r]) continue;
+                    const double m = sw[(lane + 32 * r) * STRIDE + s2];
+                    acc[r][0] = fma(x0, m, acc[r][0]);
+                    acc[r][1] = fma(x1, m, acc[r][1]);
+                    acc[r][2] = fma(x2, m, acc[r][2]);
+                }
+            }
+            __syncwarp();
+        }
+        for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
+        double *out = sums + (int64_t)PARTS * j;
+#pragma unroll
+        for (int r = 0; r < MT::slots; ++r)
+            if (own[r])
+                for (int i = 0; i < 3; ++i) out[tuple_out(lane + 32 * r, i)] = acc[r][i];
         if (lane == 0) {
+            out[0] = r2;
             for (int x = 0; x < 3; ++x) {
                 box[6 * j + x] = mn[x];
                 box[6 * j + 3 + x] = mx[x];
@@ -1095,84 +1267,107 @@ __global__ void __launch_bounds__(128) leaf_moments_kernel(int64_t count, const 
     }
 }
 
-// Adds the child's moments (about its centre cc) translated to the centre c into v (v[0], bound^2, untouched).
+// One warp per leaf climbs towards the root; at each parent the second of the two arriving warps combines the
+// children (their results were published, and fenced by every lane, before the arrival count moved), so every
+// internal node is combined exactly once, from its left then its right child, and no warp waits for another.  Both
+// children's sums are staged in shared memory; lane u translates index tuple u by the binomial expansion
+//   m'_(i; a1..an) = sum over subsets S of the positions of prod_(s in S) D_as * m_(i; the positions not in S),
+// D = child centre - node centre, the subset products built up one factor at a time.
 template <int PARTS>
-__device__ __forceinline__ void add_translated(const double *w, const double *cc, const double *c, double *v) {
-    const double D[3] = {cc[0] - c[0], cc[1] - c[1], cc[2] - c[2]};
-    const double *M0 = w + 1, *M1 = w + 4, *S = w + 13;
-    auto S2 = [&](int i, int a, int b) -> double {
-        int x = a < b ? a : b, y = a < b ? b : a;
-        return S[6 * i + (x == 0 ? y : (x == 1 ? 2 + y : 5))];
-    };
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        v[1 + i] += M0[i];
-#pragma unroll
-        for (int j = 0; j < 3; ++j) v[4 + 3 * i + j] += M1[3 * i + j] + M0[i] * D[j];
-        int p = 0;
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-#pragma unroll
-            for (int k = j; k < 3; ++k, ++p)
-                v[13 + 6 * i + p] += S[6 * i + p] + M1[3 * i + j] * D[k] + M1[3 * i + k] * D[j] + M0[i] * D[j] * D[k];
-        if (PARTS == MOM_PARTS3) {
-            const double *M3 = w + 31;
-            int q = 0;
-#pragma unroll
-            for (int j = 0; j < 3; ++j)
-#pragma unroll
-                for (int k = j; k < 3; ++k)
-#pragma unroll
-                    for (int l = k; l < 3; ++l, ++q)
-                        v[31 + 10 * i + q] += M3[10 * i + q] + D[j] * S2(i, k, l) + D[k] * S2(i, j, l) +
-                                              D[l] * S2(i, j, k) + D[j] * D[k] * M1[3 * i + l] +
-                                              D[j] * D[l] * M1[3 * i + k] + D[k] * D[l] * M1[3 * i + j] +
-                                              D[j] * D[k] * D[l] * M0[i];
-        }
-    }
-}
-
-// One thread per leaf climbs towards the root; at each parent the second of the two arriving threads combines the
-// children (their results were published before the arrival count moved), so every internal node is combined exactly
-// once, from its left then its right child.  No thread waits for another.
-template <int PARTS>
-__global__ void bottom_up_kernel(int64_t count, const int64_t *left, const int64_t *right, const int32_t *parent,
-                                 unsigned *arrive, double *box, double *centre, double *core, double *sums) {
-    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) bottom_up_kernel(int64_t count, const int64_t *left, const int64_t *right,
+                                                        const int32_t *parent, unsigned *arrive, double *box,
+                                                        double *centre, double *core, double *sums) {
+    using MT = MomentTuples<PARTS>;
+    __shared__ double sm[4][2][PARTS];
+    __shared__ unsigned short src[16][MT::n];  // by mask, then tuple: the lanes of one mask read adjacent entries
+    for (int q = threadIdx.x; q < MT::n * 16; q += blockDim.x) src[q & 15][q >> 4] = c_tt.src[q >> 4][q & 15];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 3;
+    const int64_t j = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (j >= count || left[j] >= 0) return;
+    int tn[MT::slots], tp[MT::slots];
+#pragma unroll
+    for (int r = 0; r < MT::slots; ++r) {
+        const int u = lane + 32 * r;
+        tn[r] = u < MT::n ? c_tt.n[u] : -1;
+        tp[r] = u < MT::n ? c_tt.packed[u] : 0;
+    }
     int64_t node = j;
     for (int depth = 0; depth < 4096; ++depth) {
         const int32_t p = parent[node];
         if (p < 0) return;
         __threadfence();
-        if (atomicAdd(&arrive[p], 1u) == 0) return;
+        __syncwarp();
+        unsigned prior = 0;
+        if (lane == 0) prior = atomicAdd(&arrive[p], 1u);
+        prior = __shfl_sync(0xffffffffu, prior, 0);
+        if (prior == 0) return;
         __threadfence();
         const int64_t l = left[p], r = right[p];
-        double mn[3], mx[3];
+        for (int q = lane; q < PARTS; q += 32) {
+            sm[w][0][q] = __ldcg(sums + (int64_t)PARTS * l + q);
+            sm[w][1][q] = __ldcg(sums + (int64_t)PARTS * r + q);
+        }
+        double lo_x = 0.0, hi_x = 0.0;
+        if (lane < 3) {
+            lo_x = fmin(__ldcg(box + 6 * l + lane), __ldcg(box + 6 * r + lane));
+            hi_x = fmax(__ldcg(box + 6 * l + 3 + lane), __ldcg(box + 6 * r + 3 + lane));
+        }
+        const double mid = 0.5 * (lo_x + hi_x);
+        const double c[3] = {__shfl_sync(0xffffffffu, mid, 0), __shfl_sync(0xffffffffu, mid, 1),
+                             __shfl_sync(0xffffffffu, mid, 2)};
+        double D[2][3];
+#pragma unroll
         for (int x = 0; x < 3; ++x) {
-            mn[x] = fmin(__ldcg(box + 6 * l + x), __ldcg(box + 6 * r + x));
-            mx[x] = fmax(__ldcg(box + 6 * l + 3 + x), __ldcg(box + 6 * r + 3 + x));
+            D[0][x] = __ldcg(centre + 3 * l + x) - c[x];
+            D[1][x] = __ldcg(centre + 3 * r + x) - c[x];
         }
-        const double c[3] = {0.5 * (mn[0] + mx[0]), 0.5 * (mn[1] + mx[1]), 0.5 * (mn[2] + mx[2])};
-        double v[PARTS];
+        __syncwarp();
+        double acc[MT::slots][3];
 #pragma unroll
-        for (int q = 0; q < PARTS; ++q) v[q] = 0.0;
-        double w[PARTS], cc[3];
+        for (int q = 0; q < MT::slots; ++q) {
+            acc[q][0] = acc[q][1] = acc[q][2] = 0.0;
+            if (tn[q] < 0) continue;
+            const int u = lane + 32 * q;
 #pragma unroll
-        for (int side = 0; side < 2; ++side) {
-            const int64_t ch = side == 0 ? l : r;
+            for (int side = 0; side < 2; ++side) {
+                double Dp[4];  // D at the tuple's positions
 #pragma unroll
-            for (int q = 0; q < PARTS; ++q) w[q] = __ldcg(sums + (int64_t)PARTS * ch + q);
-            for (int x = 0; x < 3; ++x) cc[x] = __ldcg(centre + 3 * ch + x);
-            add_translated<PARTS>(w, cc, c, v);
+                for (int s2 = 0; s2 < 4; ++s2) {
+                    const int x = (tp[q] >> (2 * s2)) & 3;
+                    Dp[s2] = x == 0 ? D[side][0] : (x == 1 ? D[side][1] : D[side][2]);
+                }
+                double f[16];
+                f[0] = 1.0;
+#pragma unroll
+                for (int mask = 1; mask < 16; ++mask) {
+                    const int low = mask & -mask, pos = low == 1 ? 0 : (low == 2 ? 1 : (low == 4 ? 2 : 3));
+                    f[mask] = f[mask ^ low] * Dp[pos];
+                }
+                const double *sv = sm[w][side];
+#pragma unroll
+                for (int mask = 0; mask < 16; ++mask) {
+                    if (mask < (1 << tn[q])) {
+                        const int e = src[mask][u], o0 = e & 255, cn = e >> 8;
+                        acc[q][0] = fma(f[mask], sv[o0], acc[q][0]);
+                        acc[q][1] = fma(f[mask], sv[o0 + cn], acc[q][1]);
+                        acc[q][2] = fma(f[mask], sv[o0 + 2 * cn], acc[q][2]);
+                    }
+                }
+            }
         }
-        for (int q = 1; q < PARTS; ++q) sums[(int64_t)PARTS * p + q] = v[q];
-        for (int x = 0; x < 3; ++x) {
-            box[6 * p + x] = mn[x];
-            box[6 * p + 3 + x] = mx[x];
-            centre[3 * p + x] = c[x];
+        __syncwarp();
+        double *out = sums + (int64_t)PARTS * p;
+#pragma unroll
+        for (int q = 0; q < MT::slots; ++q)
+            if (tn[q] >= 0)
+                for (int i = 0; i < 3; ++i) out[tuple_out(lane + 32 * q, i)] = acc[q][i];
+        if (lane < 3) {
+            box[6 * p + lane] = lo_x;
+            box[6 * p + 3 + lane] = hi_x;
+            centre[3 * p + lane] = mid;
         }
-        core[p] = fmax(__ldcg(core + l), __ldcg(core + r));
+        if (lane == 0) core[p] = fmax(__ldcg(core + l), __ldcg(core + r));
         node = p;
     }
 }
@@ -1247,8 +1442,8 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
     const unsigned leaf_blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((count + 3) / 4, 148 * 16));
     leaf_moments_kernel<PARTS><<<leaf_blocks, 128, 0, s>>>(count, t->lo, t->hi, t->left, t->order32, geo, box,
                                                             t->centre, t->core, sums);
-    bottom_up_kernel<PARTS><<<blocks_for(count, 128), 128, 0, s>>>(count, t->left, t->right, parent, arrive, box,
-                                                                    t->centre, t->core, sums);
+    bottom_up_kernel<PARTS><<<blocks_for(count, 4), 128, 0, s>>>(count, t->left, t->right, parent, arrive, box,
+                                                                  t->centre, t->core, sums);
     internal_item_count_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->lo, t->hi, t->left, nitems);
     BS_CHECK_LAUNCH("bottom-up moments");
     int rc = scan_exclusive(nitems, first, count, total, scratch, s);
@@ -1265,7 +1460,8 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
         bound_chunk_kernel<<<grid, MOM_THREADS, 0, s>>>(items, n_items, ends, t->centre, partial);
     }
     const NodeOut out{t->lo, t->hi, t->left, t->right, t->centre, t->core, t->bound, t->m0, t->m1, t->m2,
-                      t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x};
+                      t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x,
+                      t->far64y, t->far32y};
     node_final_kernel<PARTS><<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, partial, sums, out);
     BS_CHECK_LAUNCH("bottom-up moments");
     return BS_OK;
@@ -1290,9 +1486,16 @@ int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_
         t->far32x = t->alloc<Far32x>(count, s);
         if (!t->far64x || !t->far32x) return BS_ERR_OOM;
     }
+    if (t->order4) {
+        t->far64y = t->alloc<Far64y>(count, s);
+        t->far32y = t->alloc<Far32y>(count, s);
+        if (!t->far64y || !t->far32y) return BS_ERR_OOM;
+    }
     if (!t->centre || !t->bound || !t->core || !t->m0 || !t->m1 || !t->m2 || !t->w1 || !t->t2 || !t->w2 ||
         !t->nodes || !t->far64 || !t->far32)
         return BS_ERR_OOM;
+    // fourth order: the bottom-up pipeline for every kind (its box, centre and bound equal the direct sums')
+    if (t->order4) return moments_bottom_up<MOM_PARTS4>(t, geo, scratch, s);
     if (t->kind == BS_TREE_MORTON) return t->order3 ? moments_bottom_up<MOM_PARTS3>(t, geo, scratch, s)
                                                    : moments_bottom_up<MOM_PARTS>(t, geo, scratch, s);
     int64_t *nitems = scratch.get<int64_t>(count), *first = scratch.get<int64_t>(count);
@@ -1314,7 +1517,8 @@ int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_
     moment_box_kernel<<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, box);
     moment_centre_kernel<<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, box, t->centre, t->core);
     const NodeOut out{t->lo, t->hi, t->left, t->right, t->centre, t->core, t->bound, t->m0, t->m1, t->m2,
-                      t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x};
+                      t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x,
+                      t->far64y, t->far32y};
     if (t->order3) {
         moment_sum_kernel<MOM_PARTS3><<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, t->centre, sums);
         moment_final_kernel<MOM_PARTS3><<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, sums, out);
@@ -1400,6 +1604,7 @@ extern "C" int bs_tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_p
     t->m = src->m;
     t->leaf_size = tp->leaf_size;
     t->order3 = tp->order >= 3;
+    t->order4 = tp->order >= 4;
     {
         Scratch scratch(ctx->pool, s);
         SegGeo *geo = scratch.get<SegGeo>(src->m);
@@ -1459,6 +1664,7 @@ extern "C" int bs_forest_build(bs_ctx *ctx, const bs_sources *src, int nwakes, c
     t->m = src->m;
     t->leaf_size = tp->leaf_size;
     t->order3 = tp->order >= 3;
+    t->order4 = tp->order >= 4;
     {
         Scratch scratch(ctx->pool, s);
         SegGeo *geo = scratch.get<SegGeo>(src->m);

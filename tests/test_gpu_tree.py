@@ -267,6 +267,38 @@ def test_third_order_expansion_converges_one_order_faster(device):
                          theta=0.1, order=3)
 
 
+def test_fourth_order_expansion_converges_one_order_faster_again(device):
+    """Order 4 (the fourth moments of the segments' line integrals, an extension beyond the reference's orders 0-2):
+    below order 3 at each opening angle, shrinking ~theta^5, on Morton and median trees (both take their fourth-order
+    moments bottom-up) and in mixed precision; an order-4 tree evaluated at order 3 matches an order-3 tree."""
+    from openfawe_b200 import engine, wakes
+    case = wakes.rotor_sheet(120, seed=9, targets=4000)
+    args = wakes.backend_args(case)
+    src = engine.Sources(*args[1:6], device)
+    tgt = engine.Targets(case["points"], None, device)
+    direct, _ = engine.direct(src, tgt, 2, "raise", "fp64")
+    direct = direct.cpu().numpy()
+    rel = lambda u: np.linalg.norm(u.cpu().numpy() - direct) / np.linalg.norm(direct)
+    for kind in ("morton", "median"):
+        err = {}
+        trees = {order: engine.build_tree(src, leaf_size=16, kind=kind, order=order) for order in (3, 4)}
+        for order in (3, 4):
+            for theta in (0.1, 0.2):
+                u, flags, _ = engine.tree_eval(trees[order], tgt, 2, "raise", "fp64", theta=theta, order=order)
+                assert not flags.cpu().numpy().any()
+                err[order, theta] = rel(u)
+        for theta in (0.1, 0.2):
+            assert err[4, theta] < 0.5 * err[3, theta], (kind, err)
+        assert err[4, 0.2] / err[4, 0.1] > 12.0, (kind, err)
+        u3, _, _ = engine.tree_eval(trees[4], tgt, 2, "raise", "fp64", theta=0.2, order=3)
+        assert abs(rel(u3) - err[3, 0.2]) <= 1e-3 * err[3, 0.2], (kind, rel(u3), err[3, 0.2])
+        um, _, _ = engine.tree_eval(trees[4], tgt, 2, "raise", "mixed", theta=0.2, order=4)
+        assert rel(um) < 1.5 * err[4, 0.2] + 2e-7, (kind, rel(um), err)
+    with pytest.raises(ValueError):
+        engine.tree_eval(engine.build_tree(src, leaf_size=16, kind="morton", order=3), tgt, 2, "raise", "fp64",
+                         theta=0.1, order=4)
+
+
 def test_morton_bottom_up_moments_against_direct_node_sums(device):
     """Morton trees and forests take their node moments bottom-up (leaves summed, parents translated from their
     children): box, centre, core and bounding radius equal the direct per-node computation bit for bit, the moments
