@@ -263,6 +263,8 @@ extern "C" int bs_incident_pairs(bs_ctx *ctx, const double *nodes, int64_t n, co
     int64_t found = 0;
     BS_CUDA(cudaMemcpyAsync(&found, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     BS_CUDA(cudaStreamSynchronize(s));
+    rc = check_sort_fault();
+    if (rc != BS_OK) return rc;
     *count = found;
     if (found == 0 || found > capacity) return BS_OK;
     incident_write_kernel<<<grid_for(entries), 256, 0, s>>>(entries, first, edges, nodes, order, run_of, run_free, cnt,
@@ -335,5 +337,5 @@ extern "C" int bs_exclusion_csr(bs_ctx *ctx, int64_t n, const int64_t *pairs, in
     if (rc != BS_OK) return rc;
     BS_CUDA(cudaMemcpyAsync(unique_count, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     BS_CUDA(cudaStreamSynchronize(s));
-    return BS_OK;
+    return check_sort_fault();
 }

@@ -1618,6 +1618,7 @@ extern "C" int bs_tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_p
         if (rc == BS_OK) {
             cudaError_t e = cudaEventSynchronize(e2);
             if (e != cudaSuccess) rc = cuda_fail(e, "tree build");
+            if (rc == BS_OK) rc = check_sort_fault();
         }
     }
     if (rc == BS_OK) {
@@ -1678,6 +1679,7 @@ extern "C" int bs_forest_build(bs_ctx *ctx, const bs_sources *src, int nwakes, c
         if (rc == BS_OK) {
             cudaError_t e = cudaEventSynchronize(e2);
             if (e != cudaSuccess) rc = cuda_fail(e, "forest build");
+            if (rc == BS_OK) rc = check_sort_fault();
         }
     }
     if (rc == BS_OK) {

@@ -616,7 +616,9 @@ int target_order(int64_t n, const double *points, int32_t *perm, Scratch &scratc
     target_box_kernel<<<std::min<unsigned>(nblocks(n, 256), 592), 256, 0, s>>>(n, points, box);
     target_keys_kernel<<<nblocks(n, 256), 256, 0, s>>>(n, points, box, keys, perm);
     BS_CHECK_LAUNCH("target keys");
-    return radix_sort(keys, perm, n, 0, 63, scratch, s);
+    // the order only groups nearby targets into warps (each target's result does not depend on it): the top 32 key
+    // bits (about 10.7 per axis) do that in four passes
+    return radix_sort(keys, perm, n, 31, 63, scratch, s);
 }
 
 // Forest targets: sorted by (wake, Morton key in the wake's own target box); each sorted target learns its root.
@@ -733,7 +735,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
         forest_target_keys_kernel<<<nblocks(n, 256), 256, 0, s>>>(n, tgt->points, target_wake_ptr, nw, box, bits,
                                                                   keys, perm);
         BS_CHECK_LAUNCH("forest target keys");
-        rc = radix_sort(keys, perm, n, 0, 64, scratch, s);
+        rc = radix_sort(keys, perm, n, 32, 64, scratch, s);  // wake, then the leading Morton bits
         if (rc != BS_OK) return rc;
         forest_roots_of_kernel<<<nblocks(n, 256), 256, 0, s>>>(n, perm, target_wake_ptr, nw, tree->wake_root,
                                                                root_of);
@@ -839,6 +841,8 @@ int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const b
     for (auto &m : marks) cudaEventDestroy(m);
     if (rc != BS_OK) return rc;
     if (le != cudaSuccess) return cuda_fail(le, "tree evaluation");
+    rc = check_sort_fault();
+    if (rc != BS_OK) return rc;
     ctx->stats.points = tgt->n;
     ctx->stats.segments = tree->m;
     ctx->stats.nodes = tree->count;
@@ -920,6 +924,7 @@ extern "C" int bs_forest_graph(bs_ctx *ctx, const bs_tree *forest, const bs_tree
         need = probe.requested;
         cudaError_t e = cudaStreamSynchronize(s);
         if (rc == BS_OK && e != cudaSuccess) rc = cuda_fail(e, "bs_forest_graph sizing run");
+        if (rc == BS_OK) rc = check_sort_fault();
     }
     bs_graph *g = new bs_graph();
     g->device = ctx->device;
@@ -970,6 +975,8 @@ extern "C" int bs_graph_status(bs_graph *g, bs_stats *stats) {
     }
     unsigned long long host[6];
     BS_CUDA(cudaMemcpy(host, g->state, sizeof host, cudaMemcpyDeviceToHost));
+    const int sorted = check_sort_fault();
+    if (sorted != BS_OK) return sorted;
     memset(stats, 0, sizeof *stats);
     stats->far_evaluations = (int64_t)host[1];
     stats->near_pairs = (int64_t)host[2];
