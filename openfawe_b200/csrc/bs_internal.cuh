@@ -111,7 +111,7 @@ struct __align__(16) Seg64 {
 struct __align__(16) Seg32 {
     float4 hi;   // sx_hi, sy_hi, sz_hi, 1/L
     float4 lo;   // sx_lo, sy_lo, sz_lo, (Gamma/L)/(4 pi)
-    float4 dir;  // dx, dy, dz, rc/L
+    float4 dir;  // dx, dy, dz, (L/rc)^2
 };
 
 // Traversal record of one node (64 bytes).
@@ -256,40 +256,42 @@ __device__ __forceinline__ int pair64_at(double px, double py, double pz, const 
     return pair64_core(ax, ay, az, t, cx, cy, cz, s, model, raise_singular, ux, uy, uz);
 }
 
-// The single-precision pair.  `rx, ry, rz` is p - s (formed from two-float coordinates); hi.w holds 1/L (NaN for a
-// core too small for FP32), dir.w (L/rc)^2, 0 for no core.  Adds the velocity to (ux, uy, uz) unless the pair needs
-// FP64, which is returned as true: within sqrt(near2) core radii of the finite segment, within 1e-4 L of its axis
-// (the reference's "suspect" rule, vortex_cuda.py:123-124; a NaN 1/L fails it too), or out of FP32's comfortable
-// range -- the FP64 pair then decides value and flags exactly.  The common path has no data-dependent branch; the core
-// factor is computed only where it differs from 1 (Lamb-Oseen past its cut-off, Rankine and Vatistas outside one core
-// radius).  MODEL: 0..5.
-// NEAR = false leaves out the "within sqrt(near2) core radii" test, for callers that know every pair of the batch lies
-// farther than that from its segment.
+// The single-precision pair, in units of the segment's length: a = (p - s)/L (from two-float coordinates), b = a - d,
+// c = d x a, h^2 = |c|^2, and the reference's (vortex_numba.pair_velocity)
+//   u = (Gamma/L)/(4 pi) factor (|a| + |b|) / (|a| |b| (|a| |b| + a.b)) c.
+// hi.w holds 1/L (NaN for a core too small for FP32), lo.w (Gamma/L)/(4 pi), dir.w (L/rc)^2, 0 for no core.  Adds
+// the velocity to (ux, uy, uz) unless the pair needs FP64, which is returned as true: within sqrt(near2) core radii of
+// the finite segment, within 1e-4 L of its axis (the reference's "suspect" rule, vortex_cuda.py:123-124; a NaN 1/L
+// fails it too), or out of FP32's comfortable range -- the FP64 pair then decides value and flags exactly.  Where
+// a.b < 0, |a||b| + a.b = h^2 / (|a||b| - a.b) (|a x b| = |c|): no cancellation.  The common path has no
+// data-dependent branch; the core factor is computed only where it differs from 1 (Lamb-Oseen inside its cut-off,
+// Rankine and Vatistas inside one core radius).  MODEL: 0..5.  NEAR = false leaves out the "within sqrt(near2) core
+// radii" test, for callers that know every pair of the batch lies farther than that from its segment.
 template <int MODEL, bool NEAR = true>
 __device__ __forceinline__ bool pair32(float rx, float ry, float rz, const float4 &hi, const float4 &lo,
                                        const float4 &dir, float near2, float &ux, float &uy, float &uz) {
     const float il = hi.w;
     const float ax = rx * il, ay = ry * il, az = rz * il;
     const float dx = dir.x, dy = dir.y, dz = dir.z, irc2 = dir.w;
-    const float t = fmaf(az, dz, fmaf(ay, dy, ax * dx));
+    const float bx = ax - dx, by = ay - dy, bz = az - dz;
     const float cx = fmaf(dy, az, -dz * ay);
     const float cy = fmaf(dz, ax, -dx * az);
     const float cz = fmaf(dx, ay, -dy * ax);
     const float h2 = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
     const float na2 = fmaf(ax, ax, fmaf(ay, ay, az * az));
-    const float bx = ax - dx, by = ay - dy, bz = az - dz;
     const float nb2 = fmaf(bx, bx, fmaf(by, by, bz * bz));
+    const float dot = fmaf(ax, bx, fmaf(ay, by, az * bz));
     const float big2 = fmaxf(1.0f, fmaxf(na2, nb2));
     bool need64 = !(h2 > 1e-8f * big2) || !(big2 < 1e18f);
     if (MODEL != 0 && NEAR) {
+        const float t = fmaf(az, dz, fmaf(ay, dy, ax * dx));
         const float seg2 = t < 0.0f ? na2 : (t > 1.0f ? nb2 : h2);  // distance^2 to the finite segment, units of L^2
         need64 = need64 || (irc2 > 0.0f && seg2 * irc2 < near2);
     }
     const float na = na2 * rsqrtf(na2), nb = nb2 * rsqrtf(nb2);
-    float product = na * nb;
-    float dot = fmaf(t, t - 1.0f, h2);
-    // coefficient = (Gamma/L)/(4 pi) * factor * (na + nb) / (product * plus) with plus = product + dot, or, when
-    // dot < 0, the rationalised h^2 / (product - dot); one reciprocal either way.
+    const float product = na * nb;
+    // coefficient = lo.w * factor * num / den: num = |a| + |b| and den = product * (product + dot), or where dot < 0
+    // num = (|a| + |b|)(product - dot) and den = product * h^2; one reciprocal either way
     float num = na + nb;
     num = dot < 0.0f ? num * (product - dot) : num;
     float den = product * (dot < 0.0f ? h2 : product + dot);
@@ -299,8 +301,7 @@ __device__ __forceinline__ bool pair32(float rx, float ry, float rz, const float
             const float rc2 = __fdividef(1.0f, irc2);
             if (MODEL == 5) {  // Rosenhead-Moore: augmented distances
                 const float pa = sqrtf(na2 + rc2), pb = sqrtf(nb2 + rc2);
-                const float pr = pa * pb, tr2 = h2 + rc2;
-                const float dt = fmaf(t, t - 1.0f, tr2);
+                const float pr = pa * pb, tr2 = h2 + rc2, dt = dot + rc2;
                 num = dt < 0.0f ? (pa + pb) * (pr - dt) : pa + pb;
                 den = pr * (dt < 0.0f ? tr2 : pr + dt);
             } else {  // offset core: denominator + rc^2
@@ -315,11 +316,9 @@ __device__ __forceinline__ bool pair32(float rx, float ry, float rz, const float
             if (MODEL == 1) {
                 factor = fminf(r2, 1.0f);
             } else if (MODEL == 2) {
-                // 1 - exp(-x), x = 1.25643 r^2, by its series where the exponential form loses digits
-                const float x = (float)LAMB_A * r2;
-                factor = x < 0.0625f
-                             ? x * (1.0f - x * (0.5f - x * (1.0f / 6.0f - x * (1.0f / 24.0f - x * (1.0f / 120.0f)))))
-                             : 1.0f - __expf(-x);
+                // 1 - exp(-x), x = 1.25643 r^2; where x is small the difference loses relative digits, but the pair
+                // is then as small as x, so its absolute error stays at FP32 rounding of the pair without the core
+                factor = 1.0f - __expf(-(float)LAMB_A * r2);
             } else {  // Vatistas n = 2
                 factor = r2 < 1.0f ? r2 * rsqrtf(fmaf(r2, r2, 1.0f))
                                    : rsqrtf(fmaf(__fdividef(1.0f, r2), __fdividef(1.0f, r2), 1.0f));

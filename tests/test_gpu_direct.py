@@ -138,3 +138,29 @@ def test_repeatable_bitwise(device):
         a, _ = cuda_sum(*wakes.backend_args(case), csr, "raise", settings(precision))
         b, _ = cuda_sum(*wakes.backend_args(case), csr, "raise", settings(precision))
         assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+def test_mixed_pairs_at_any_length_scale_and_tiny_cores(device):
+    """The mixed pair works in units of each segment's length, so the same network scaled from 1e-7 m to 1e10 m stays
+    in FP32 within the mixed bound; a core below 1e-15 of its segment's length carries a NaN 1/L in its FP32 record
+    and every pair of such a segment is evaluated in FP64 (counted in fp64_pairs)."""
+    from openfawe_b200 import engine
+    g = golden("direct_random.npz")
+    P = lambda k: g[f"s3_{k}"]  # noqa: E731
+    n, m = len(P("points")), len(P("gamma"))
+    for scale_x, core, all_fp64 in ((1e-7, 0.2, False), (1e7, 0.2, False), (1e10, 0.2, False), (1.0, 1e-17, True)):
+        args = (P("points") * scale_x, P("starts") * scale_x, P("directions"), P("lengths") * scale_x, P("gamma"),
+                np.full(m, core * scale_x), 2)
+        src = engine.Sources(*args[1:6], device)
+        tgt = engine.Targets(args[0], None, device)
+        u64, f64 = engine.direct(src, tgt, 2, "zero", "fp64")
+        um, fm = engine.direct(src, tgt, 2, "zero", "mixed")
+        stats = engine.last_stats(device)
+        assert np.array_equal(f64.cpu().numpy(), fm.cpu().numpy())
+        if all_fp64:
+            assert stats["fp64_pairs"] == n * m, (scale_x, core, stats["fp64_pairs"])
+            np.testing.assert_allclose(um.cpu().numpy(), u64.cpu().numpy(), rtol=1e-12,
+                                       atol=1e-12 * float(np.abs(u64.cpu().numpy()).max()))
+        else:
+            assert stats["fp64_pairs"] < n * m // 10, (scale_x, stats["fp64_pairs"])
+            within(um.cpu().numpy(), u64.cpu().numpy(), scale_of(*args), 1e-5)
