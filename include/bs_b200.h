@@ -99,6 +99,11 @@ int bs_version(int *major, int *minor, int *arch);
  * several host threads fill 4 MiB pinned chunks while earlier chunks transfer.  Returns once the source has been read
  * (the last transfers may still be in flight on the stream). */
 int bs_upload(bs_ctx *ctx, void *dst, const void *src, size_t bytes, bs_stream stream);
+/* bs_upload for `count` arrays in one pass of the staging ring (dst[i] <- src[i], bytes[i] each): the next array's
+ * first chunk is staged while the previous array's last chunks transfer.  Used by the drop-in backends, whose inputs
+ * arrive as several host arrays per call.  Same return rule as bs_upload. */
+int bs_upload_many(bs_ctx *ctx, int count, void *const *dst, const void *const *src, const size_t *bytes,
+                   bs_stream stream);
 /* Measures the device's FP32 FMA throughput (TFLOP/s, an FMA counted as 2) with a kernel of independent FMA chains
  * on every SM: the denominator of the pair kernels' roofline, which run on the FP32 pipe. */
 int bs_fp32_peak(bs_ctx *ctx, double *tflops);

@@ -1,10 +1,13 @@
 // Host -> device upload from ordinary (pageable) host memory through a pinned staging ring.  The caller's bytes are
-// copied into 4 MiB pinned chunks by OpenMP threads while the chunks before them cross PCIe (cudaMemcpyAsync on the
-// caller's stream), so host copying and transfer overlap and the copy runs on several cores.  The call returns when
-// the source has been read; the last transfers may still be in flight on the stream.
+// copied into 4 MiB pinned chunks by OpenMP threads (non-temporal stores where the CPU has AVX2) while the chunks
+// before them cross PCIe (cudaMemcpyAsync on the caller's stream), so host copying and transfer overlap and the copy
+// runs on several cores.  The call returns when the sources have been read; the last transfers may still be in flight
+// on the stream.  bs_upload_many keeps the ring going across several arrays.
+#include <immintrin.h>
 #include <omp.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 
@@ -52,35 +55,84 @@ void bs_upload_release(bs_ctx *ctx) {
     ctx->upload = nullptr;
 }
 
+// Copy of one staging piece: AVX2 non-temporal stores where the CPU has them (the staging buffer is then written
+// without being read into the cache first, which leaves the host's memory bandwidth to the transfers), else memcpy.
+__attribute__((target("avx2"))) static void stream_copy_avx2(char *dst, const char *src, size_t n) {
+    size_t i = 0;
+    if ((reinterpret_cast<uintptr_t>(dst) & 31) == 0) {
+        for (; i + 128 <= n; i += 128) {
+            const __m256i a = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(src + i));
+            const __m256i b = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(src + i + 32));
+            const __m256i c = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(src + i + 64));
+            const __m256i d = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(src + i + 96));
+            _mm256_stream_si256(reinterpret_cast<__m256i *>(dst + i), a);
+            _mm256_stream_si256(reinterpret_cast<__m256i *>(dst + i + 32), b);
+            _mm256_stream_si256(reinterpret_cast<__m256i *>(dst + i + 64), c);
+            _mm256_stream_si256(reinterpret_cast<__m256i *>(dst + i + 96), d);
+        }
+        _mm_sfence();
+    }
+    if (i < n) std::memcpy(dst + i, src + i, n - i);
+}
+
+static void stage_copy(char *dst, const char *src, size_t n, bool avx2) {
+    if (avx2) stream_copy_avx2(dst, src, n);
+    else std::memcpy(dst, src, n);
+}
+
+// One ring pass over several host -> device copies: the chunk counter runs on across the arrays, so the next array's
+// first chunk is staged while the previous array's last chunks transfer.
+static int upload_list(bs_ctx *ctx, int count, void *const *dst, const void *const *src, const size_t *bytes,
+                       cudaStream_t s) {
+    BS_CUDA(cudaSetDevice(ctx->device));
+    bs_upload_ring *r = nullptr;
+    int rc = ring_of(ctx, &r);
+    if (rc != BS_OK) return rc;
+    std::lock_guard<std::mutex> guard(r->lock);
+    static const bool avx2 = __builtin_cpu_supports("avx2");
+    const int threads = std::max(1, std::min(8, omp_get_max_threads()));
+    int k = 0;
+    for (int a = 0; a < count; ++a) {
+        const char *from = static_cast<const char *>(src[a]);
+        char *to = static_cast<char *>(dst[a]);
+        for (size_t off = 0; off < bytes[a]; off += bs_upload_ring::CHUNK, ++k) {
+            const int slot = k % bs_upload_ring::SLOTS;
+            BS_CUDA(cudaEventSynchronize(r->done[slot]));  // the slot's previous transfer has left it
+            const size_t len = std::min(bs_upload_ring::CHUNK, bytes[a] - off);
+            char *stage = static_cast<char *>(r->buf[slot]);
+            const size_t piece = ((len + threads - 1) / threads + 127) & ~size_t(127);  // 128-byte aligned pieces
+#pragma omp parallel for num_threads(threads) schedule(static)
+            for (int i = 0; i < threads; ++i) {
+                const size_t lo = std::min(len, (size_t)i * piece), hi = std::min(len, lo + piece);
+                if (hi > lo) stage_copy(stage + lo, from + off + lo, hi - lo, avx2);
+            }
+            BS_CUDA(cudaMemcpyAsync(to + off, stage, len, cudaMemcpyHostToDevice, s));
+            BS_CUDA(cudaEventRecord(r->done[slot], s));
+        }
+    }
+    return BS_OK;
+}
+
 extern "C" int bs_upload(bs_ctx *ctx, void *dst, const void *src, size_t bytes, bs_stream stream) {
     if (!ctx || (bytes > 0 && (!dst || !src))) {
         bs::set_error("bs_upload: null argument");
         return BS_ERR_ARG;
     }
     if (bytes == 0) return BS_OK;
-    BS_CUDA(cudaSetDevice(ctx->device));
-    bs_upload_ring *r = nullptr;
-    int rc = ring_of(ctx, &r);
-    if (rc != BS_OK) return rc;
-    std::lock_guard<std::mutex> guard(r->lock);
-    cudaStream_t s = (cudaStream_t)stream;
-    const int threads = std::max(1, std::min(8, omp_get_max_threads()));
-    const char *from = static_cast<const char *>(src);
-    char *to = static_cast<char *>(dst);
-    int k = 0;
-    for (size_t off = 0; off < bytes; off += bs_upload_ring::CHUNK, ++k) {
-        const int slot = k % bs_upload_ring::SLOTS;
-        BS_CUDA(cudaEventSynchronize(r->done[slot]));  // the slot's previous transfer has left it
-        const size_t len = std::min(bs_upload_ring::CHUNK, bytes - off);
-        char *stage = static_cast<char *>(r->buf[slot]);
-        const size_t piece = (len + threads - 1) / threads;
-#pragma omp parallel for num_threads(threads) schedule(static)
-        for (int i = 0; i < threads; ++i) {
-            const size_t a = std::min(len, (size_t)i * piece), b = std::min(len, a + piece);
-            if (b > a) std::memcpy(stage + a, from + off + a, b - a);
-        }
-        BS_CUDA(cudaMemcpyAsync(to + off, stage, len, cudaMemcpyHostToDevice, s));
-        BS_CUDA(cudaEventRecord(r->done[slot], s));
+    return upload_list(ctx, 1, &dst, &src, &bytes, (cudaStream_t)stream);
+}
+
+extern "C" int bs_upload_many(bs_ctx *ctx, int count, void *const *dst, const void *const *src, const size_t *bytes,
+                              bs_stream stream) {
+    if (!ctx || count < 0 || (count > 0 && (!dst || !src || !bytes))) {
+        bs::set_error("bs_upload_many: null argument");
+        return BS_ERR_ARG;
     }
-    return BS_OK;
+    for (int a = 0; a < count; ++a)
+        if (bytes[a] > 0 && (!dst[a] || !src[a])) {
+            bs::set_error("bs_upload_many: null pointer for copy %d", a);
+            return BS_ERR_ARG;
+        }
+    if (count == 0) return BS_OK;
+    return upload_list(ctx, count, dst, src, bytes, (cudaStream_t)stream);
 }

@@ -44,6 +44,31 @@ def _to_device(a, np_dtype, dtype, device):
     return a.to(device=device, dtype=dtype).contiguous()
 
 
+def f64_many(arrays, device):
+    """Several arrays as C-contiguous float64 tensors on `device`: the large host arrays go through one pass of the
+    library's pinned staging ring (bs_upload_many), the rest as in f64."""
+    device = _device_of(device)
+    out = [None] * len(arrays)
+    dst, src, nbytes, keep = [], [], [], []
+    for i, a in enumerate(arrays):
+        if device.type == "cuda" and not isinstance(a, torch.Tensor):
+            array = np.ascontiguousarray(a, dtype=np.float64)
+            if array.nbytes >= UPLOAD_MIN_BYTES:
+                out[i] = torch.empty(array.shape, dtype=torch.float64, device=device)
+                dst.append(out[i].data_ptr())
+                src.append(array.ctypes.data)
+                nbytes.append(array.nbytes)
+                keep.append(array)
+                continue
+        out[i] = f64(a, device)
+    if dst:
+        k = len(dst)
+        L.check(L.library().bs_upload_many(L.context(device.index), k, (ctypes.c_void_p * k)(*dst),
+                                           (ctypes.c_void_p * k)(*src), (ctypes.c_size_t * k)(*nbytes),
+                                           _stream(device)), "bs_upload_many")
+    return out
+
+
 def f64(a, device):
     """A C-contiguous float64 tensor on `device` (copies only when needed)."""
     return _to_device(a, np.float64, torch.float64, _device_of(device))
@@ -66,11 +91,12 @@ class Sources:
 
     def __init__(self, starts, directions, lengths, gamma, radius, device=None):
         self.device = _device_of(device)
-        self.starts = f64(starts, self.device).reshape(-1, 3)
-        self.directions = f64(directions, self.device).reshape(-1, 3)
-        self.lengths = f64(lengths, self.device).reshape(-1)
-        self.gamma = f64(gamma, self.device).reshape(-1)
-        self.radius = f64(radius, self.device).reshape(-1)
+        starts, directions, lengths, gamma, radius = f64_many((starts, directions, lengths, gamma, radius), self.device)
+        self.starts = starts.reshape(-1, 3)
+        self.directions = directions.reshape(-1, 3)
+        self.lengths = lengths.reshape(-1)
+        self.gamma = gamma.reshape(-1)
+        self.radius = radius.reshape(-1)
         self.m = int(self.starts.shape[0])
 
     def struct(self):

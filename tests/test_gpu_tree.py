@@ -350,3 +350,18 @@ def test_upload_moves_host_bytes_exactly(device):
         host = rng.normal(size=count)
         dev = engine.f64(host, torch.device("cuda", device))
         assert np.array_equal(dev.cpu().numpy(), host)
+
+
+def test_upload_many_moves_every_array_exactly(device):
+    """bs_upload_many (one pass of the staging ring over several arrays, non-temporal staging copies) delivers every
+    byte of each array, for sizes that end inside, at and across chunk boundaries, with small arrays in between."""
+    import torch
+    from openfawe_b200 import engine
+    rng = np.random.default_rng(19)
+    sizes = ((4 << 20) // 8, 3, (1 << 20) // 8 + 1, (9 << 20) // 8 - 7, 1 << 17, (4 << 20) // 8 + 5)
+    hosts = [rng.normal(size=c) for c in sizes]
+    hosts.append(np.asfortranarray(rng.normal(size=(70000, 3))))  # not C-contiguous: copied first
+    for _ in range(2):
+        devs = engine.f64_many(hosts, torch.device("cuda", device))
+        for h, d in zip(hosts, devs):
+            assert np.array_equal(d.cpu().numpy(), np.ascontiguousarray(h))
