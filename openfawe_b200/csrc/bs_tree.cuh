@@ -40,6 +40,7 @@ struct bs_tree {
     int32_t *wake_root = nullptr;  // forests: root node of each wake (-1 for a wake without segments)
     int nwakes = 0;
     float build_ms = 0.f, moments_ms = 0.f;
+    cudaEvent_t marks[3] = {nullptr, nullptr, nullptr};  // build start, moments start, moments end
     void *blocks[32];
     int nblocks = 0;
     template <class T> T *alloc(size_t elems, cudaStream_t s) {
@@ -50,3 +51,10 @@ struct bs_tree {
         return static_cast<T *>(p);
     }
 };
+
+// Build without waiting (bs_tree_sum): the stage times are read by tree_stage_times after the stream synchronised;
+// tree_release frees the tree's memory stream-ordered on s, after the work queued there.
+int tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_tree **out, cudaStream_t s,
+               bool wait);
+void tree_stage_times(bs_tree *t);
+void tree_release(bs_tree *tree, cudaStream_t s);

@@ -699,11 +699,11 @@ __global__ void item_count_kernel(int64_t count, const int64_t *lo, const int64_
     n[j] = size > 0 ? (size + CHUNK - 1) / CHUNK : 0;
 }
 
-// Items (chunks of CHUNK positions) of every node, or with `left` of the internal nodes only.
+// Items (chunks of CHUNK positions) of every node.
 __global__ void item_fill_kernel(int64_t count, const int64_t *lo, const int64_t *hi, const int64_t *first,
-                                 Item *items, const int64_t *left = nullptr) {
+                                 Item *items) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= count || (left && left[j] < 0)) return;
+    if (j >= count) return;
     int64_t k = first[j];
     for (int64_t c = lo[j]; c < hi[j]; c += CHUNK, ++k)
         items[k] = {(int32_t)j, (int32_t)c, (int32_t)min(hi[j], c + CHUNK), 0};
@@ -1372,16 +1372,35 @@ __global__ void __launch_bounds__(128) bottom_up_kernel(int64_t count, const int
     }
 }
 
-// Bound^2 of one chunk of an internal node's range from the tree-ordered endpoints.
-__global__ void __launch_bounds__(MOM_THREADS) bound_chunk_kernel(const Item *items, int64_t nitems,
-                                                                  const EndPts *ends, const double *centre,
-                                                                  double *partial) {
+// Bound^2 of every internal node from the tree-ordered endpoints, by CHUNK-segment chunks of the nodes' ranges: chunk c
+// belongs to the last node j with first[j] <= c (first: exclusive scan of the per-node chunk counts, *total chunks in
+// all), found by binary search, so the chunk list needs no host round trip.  A block takes one chunk at a time and
+// folds its maximum into bound2[j] with an integer atomicMax (non-negative doubles order like their bit patterns):
+// the same value in any order.
+__global__ void __launch_bounds__(MOM_THREADS) bound_chunks_kernel(int64_t count, const int64_t *first,
+                                                                   const int64_t *total, const int64_t *lo,
+                                                                   const int64_t *hi, const EndPts *ends,
+                                                                   const double *centre,
+                                                                   unsigned long long *bound2) {
     __shared__ double red[MOM_THREADS / 32];
-    for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x) {
-        Item item = items[it];
-        const double c0 = centre[3 * item.node], c1 = centre[3 * item.node + 1], c2 = centre[3 * item.node + 2];
+    __shared__ int64_t node_s;
+    const int64_t chunks = *total;
+    for (int64_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+        if (threadIdx.x == 0) {
+            int64_t l = 0, h = count;  // first[l] <= c < first[h] (first[count] taken as +inf)
+            while (h - l > 1) {
+                const int64_t mid = (l + h) >> 1;
+                if (first[mid] <= c) l = mid;
+                else h = mid;
+            }
+            node_s = l;
+        }
+        __syncthreads();
+        const int64_t j = node_s;
+        const int64_t start = lo[j] + (c - first[j]) * CHUNK, end = min(hi[j], start + CHUNK);
+        const double c0 = centre[3 * j], c1 = centre[3 * j + 1], c2 = centre[3 * j + 2];
         double r2 = 0.0;
-        for (int k = item.start + threadIdx.x; k < item.end; k += blockDim.x) {
+        for (int64_t k = start + threadIdx.x; k < end; k += blockDim.x) {
             const EndPts e = ends[k];
             const double a0 = e.sx - c0, a1 = e.sy - c1, a2 = e.sz - c2;
             const double b0 = e.ex - c0, b1 = e.ey - c1, b2 = e.ez - c2;
@@ -1395,25 +1414,20 @@ __global__ void __launch_bounds__(MOM_THREADS) bound_chunk_kernel(const Item *it
         if (threadIdx.x == 0) {
             double v = red[0];
             for (int w = 1; w < MOM_THREADS / 32; ++w) v = fmax(v, red[w]);
-            partial[it] = v;
+            atomicMax(bound2 + j, (unsigned long long)__double_as_longlong(v));
         }
         __syncthreads();
     }
 }
 
-// Internal node: bound^2 = the max of its chunks; then finalize every node from its sums.
+// Internal node: bound^2 from bound_chunks_kernel; then finalize every node from its sums.
 template <int PARTS>
-__global__ void node_final_kernel(int64_t count, const int64_t *first, const int64_t *nitems, const double *partial,
-                                  double *sums, NodeOut o) {
+__global__ void node_final_kernel(int64_t count, const unsigned long long *bound2, double *sums, NodeOut o) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= count) return;
     double v[PARTS];
     for (int q = 0; q < PARTS; ++q) v[q] = sums[(int64_t)PARTS * j + q];
-    if (o.left[j] >= 0) {
-        double r2 = 0.0;
-        for (int64_t it = first[j]; it < first[j] + nitems[j]; ++it) r2 = fmax(r2, partial[it]);
-        v[0] = r2;
-    }
+    if (o.left[j] >= 0) v[0] = __longlong_as_double((long long)bound2[j]);
     finalize_node<PARTS>(j, v, o);
 }
 
@@ -1435,8 +1449,10 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
     EndPts *ends = scratch.get<EndPts>(m);
     int64_t *nitems = scratch.get<int64_t>(count), *first = scratch.get<int64_t>(count);
     int64_t *total = scratch.get<int64_t>(1);
-    if (!box || !sums || !parent || !arrive || !ends || !nitems || !first || !total) return scratch.status;
+    unsigned long long *bound2 = scratch.get<unsigned long long>(count);
+    if (!box || !sums || !parent || !arrive || !ends || !nitems || !first || !total || !bound2) return scratch.status;
     BS_CUDA(cudaMemsetAsync(arrive, 0, count * sizeof(unsigned), s));
+    BS_CUDA(cudaMemsetAsync(bound2, 0, count * sizeof(unsigned long long), s));
     parent_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->left, t->right, parent);
     sorted_ends_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, t->order32, geo, ends);
     const unsigned leaf_blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((count + 3) / 4, 148 * 16));
@@ -1448,21 +1464,11 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
     BS_CHECK_LAUNCH("bottom-up moments");
     int rc = scan_exclusive(nitems, first, count, total, scratch, s);
     if (rc != BS_OK) return rc;
-    int64_t n_items = 0;
-    BS_CUDA(cudaMemcpyAsync(&n_items, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    BS_CUDA(cudaStreamSynchronize(s));
-    Item *items = scratch.get<Item>(std::max<int64_t>(n_items, 1));
-    double *partial = scratch.get<double>(std::max<int64_t>(n_items, 1));
-    if (!items || !partial) return scratch.status;
-    if (n_items > 0) {
-        item_fill_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->lo, t->hi, first, items, t->left);
-        unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(n_items, 8192));
-        bound_chunk_kernel<<<grid, MOM_THREADS, 0, s>>>(items, n_items, ends, t->centre, partial);
-    }
+    bound_chunks_kernel<<<148 * 8, MOM_THREADS, 0, s>>>(count, first, total, t->lo, t->hi, ends, t->centre, bound2);
     const NodeOut out{t->lo, t->hi, t->left, t->right, t->centre, t->core, t->bound, t->m0, t->m1, t->m2,
                       t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x,
                       t->far64y, t->far32y};
-    node_final_kernel<PARTS><<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, partial, sums, out);
+    node_final_kernel<PARTS><<<blocks_for(count, 128), 128, 0, s>>>(count, bound2, sums, out);
     BS_CHECK_LAUNCH("bottom-up moments");
     return BS_OK;
 }
@@ -1568,13 +1574,18 @@ extern "C" void bs_tree_free(bs_tree *tree) {
     cudaDeviceSynchronize();
     for (int i = 0; i < tree->nblocks; ++i) cudaFreeAsync(tree->blocks[i], 0);
     cudaStreamSynchronize(0);
+    for (auto &e : tree->marks)
+        if (e) cudaEventDestroy(e);
     delete tree;
 }
 
 extern "C" int64_t bs_tree_count(const bs_tree *tree) { return tree ? tree->count : -1; }
 
-extern "C" int bs_tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_tree **out,
-                             bs_stream stream) {
+// The build behind bs_tree_build (wait = true: synchronises, checks and records the stage times) and bs_tree_sum
+// (wait = false: the evaluation is queued behind the build on the same stream, and tree_stage_times reads the times
+// once the caller has synchronised).
+int tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_tree **out, cudaStream_t s,
+               bool wait) {
     if (!ctx || !tp || !out) {
         set_error("bs_tree_build: null argument");
         return BS_ERR_ARG;
@@ -1590,14 +1601,13 @@ extern "C" int bs_tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_p
         set_error("bs_tree_build: leaf size must be positive and kind median or morton");
         return BS_ERR_ARG;
     }
-    cudaStream_t s = (cudaStream_t)stream;
     BS_CUDA(cudaSetDevice(ctx->device));
-    cudaEvent_t e0, e1, e2;
+    bs_tree *t = new bs_tree();
+    cudaEvent_t &e0 = t->marks[0], &e1 = t->marks[1], &e2 = t->marks[2];
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventCreate(&e2);
     cudaEventRecord(e0, s);
-    bs_tree *t = new bs_tree();
     t->device = ctx->device;
     t->pool = ctx->pool;
     t->kind = tp->kind;
@@ -1615,15 +1625,14 @@ extern "C" int bs_tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_p
             rc = finish_tree(t, src, geo, scratch, s);
         }
         cudaEventRecord(e2, s);
-        if (rc == BS_OK) {
+        if (rc == BS_OK && wait) {
             cudaError_t e = cudaEventSynchronize(e2);
             if (e != cudaSuccess) rc = cuda_fail(e, "tree build");
             if (rc == BS_OK) rc = check_sort_fault();
         }
     }
     if (rc == BS_OK) {
-        cudaEventElapsedTime(&t->build_ms, e0, e1);
-        cudaEventElapsedTime(&t->moments_ms, e1, e2);
+        if (wait) tree_stage_times(t);
         ctx->stats.build_ms = t->build_ms;
         ctx->stats.moments_ms = t->moments_ms;
         ctx->stats.nodes = t->count;
@@ -1632,10 +1641,26 @@ extern "C" int bs_tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_p
     } else {
         bs_tree_free(t);
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaEventDestroy(e2);
     return rc;
+}
+
+void tree_stage_times(bs_tree *t) {
+    cudaEventElapsedTime(&t->build_ms, t->marks[0], t->marks[1]);
+    cudaEventElapsedTime(&t->moments_ms, t->marks[1], t->marks[2]);
+}
+
+void tree_release(bs_tree *tree, cudaStream_t s) {
+    if (!tree) return;
+    cudaSetDevice(tree->device);
+    for (int i = 0; i < tree->nblocks; ++i) cudaFreeAsync(tree->blocks[i], s);
+    for (auto &e : tree->marks)
+        if (e) cudaEventDestroy(e);
+    delete tree;
+}
+
+extern "C" int bs_tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_tree **out,
+                             bs_stream stream) {
+    return tree_build(ctx, src, tp, out, (cudaStream_t)stream, true);
 }
 
 extern "C" int bs_forest_build(bs_ctx *ctx, const bs_sources *src, int nwakes, const int64_t *wake_ptr,

@@ -1015,12 +1015,16 @@ extern "C" int bs_tree_sum(bs_ctx *ctx, const bs_sources *src, const bs_tree_par
         if (far_counts) BS_CUDA(cudaMemsetAsync(far_counts, 0, tgt->n * sizeof(int64_t), s));
         return BS_OK;
     }
+    // the evaluation queues behind the build on the same stream: no wait in between; the tree is freed in stream
+    // order after the evaluation (which synchronises before it returns)
+    cudaStream_t s = (cudaStream_t)stream;
     bs_tree *tree = nullptr;
-    int rc = bs_tree_build(ctx, src, tp, &tree, stream);
+    int rc = tree_build(ctx, src, tp, &tree, s, false);
     if (rc != BS_OK) return rc;
     rc = bs_tree_eval(ctx, tree, tp, tgt, kp, out, flags, far_counts, stream);
+    if (rc == BS_OK) tree_stage_times(tree);
     float b = tree->build_ms, mm = tree->moments_ms;
-    bs_tree_free(tree);
+    tree_release(tree, s);
     ctx->stats.build_ms = b;
     ctx->stats.moments_ms = mm;
     return rc;

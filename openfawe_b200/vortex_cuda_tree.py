@@ -75,30 +75,29 @@ def cuda_tree_sum(points, starts, directions, lengths, gamma, radius, model, csr
     sources = engine.Sources(starts, directions, lengths, gamma, radius, device)
     targets = engine.Targets(points, csr, device)
     upload_s = time.perf_counter() - tick  # host side: the last transfers overlap the build's first launches
-    tick = time.perf_counter()
-    built = engine.build_tree(sources, tree.theta, expansion, tree.leaf_size, tree.core_clearance, kind)
-    build_s = time.perf_counter() - tick
-    build_stats = engine.last_stats(device)
     limit = int(stack_size) if 0 < int(stack_size) < DEVICE_STACK else 0
     tick = time.perf_counter()
     try:
-        d_out, d_flags, d_far = engine.tree_eval(built, targets, int(model), singularity, precision, block, near,
-                                                 tree.theta, expansion, tree.core_clearance, stack_limit=limit)
+        # build, moments and evaluation in one library call: the evaluation queues behind the build
+        d_out, d_flags, d_far = engine.tree_sum(sources, targets, int(model), singularity, precision, block, near,
+                                                tree.theta, expansion, tree.leaf_size, tree.core_clearance, kind,
+                                                stack_limit=limit)
     except _lib.StackOverflow as error:
         raise RuntimeError(f"tree traversal stack overflow on the GPU (depth {min(int(stack_size), DEVICE_STACK)})") \
             from error
-    evaluate_s = time.perf_counter() - tick
+    stats = engine.last_stats(device)
+    build_s = 1e-3 * (stats["build_ms"] + stats["moments_ms"])
+    evaluate_s = max(0.0, time.perf_counter() - tick - build_s)
     tick = time.perf_counter()
     out = VC.to_host(d_out, (n, 3), np.float64)
     flags = VC.to_host(d_flags, (n,), np.int8)
     far = VC.to_host(d_far, (n,), np.int64)
     download_s = time.perf_counter() - tick
-    stats = engine.last_stats(device)
-    Statistics.last = dict(points=n, segments=m, nodes=built.count, precision=precision, launches=1,
+    Statistics.last = dict(points=n, segments=m, nodes=int(stats["nodes"]), precision=precision, launches=1,
                            targets_per_launch=n, longest_launch_s=stats["evaluate_ms"] * 1e-3, suspect=0,
                            mean_far_nodes=float(far.mean()), build_s=build_s, moments_s=0.0, upload_s=upload_s,
                            evaluate_s=evaluate_s, download_s=download_s, recompute_s=0.0, tree=kind,
-                           build_ms=build_stats["build_ms"], moments_ms=build_stats["moments_ms"],
+                           build_ms=stats["build_ms"], moments_ms=stats["moments_ms"],
                            evaluate_ms=stats["evaluate_ms"], near_pairs=int(stats["near_pairs"]),
                            far_evaluations=int(stats["far_evaluations"]), fp64_pairs=int(stats["fp64_pairs"]),
                            visits=int(stats["visits"]),
@@ -109,5 +108,4 @@ def cuda_tree_sum(points, starts, directions, lengths, gamma, radius, model, csr
     Statistics.last_far_counts = far
     Statistics.totals["calls"] += 1
     Statistics.totals["launches"] += 1
-    del built
     return out, bool(np.any(flags))
