@@ -114,6 +114,14 @@ struct __align__(16) Seg32 {
     float4 dir;  // dx, dy, dz, (L/rc)^2
 };
 
+// Two consecutive segments (tree order) for the packed-FP32 pair (128 bytes): sixteen fields, each a float2 holding the
+// two segments' values, at float offset 2f: 0-2 -s_hi, 3 1/L, 4-6 -s_lo, 7 (Gamma/L)/(4 pi), 8-10 d, 11 (L/rc)^2,
+// 12-14 -d, 15 zero.  A segment whose pairs all go to FP64 (a NaN 1/L in its Seg32, or coordinates beyond 1e30) has
+// 1/L = 0 and a zero start here, which sends its pairs to FP64 with finite intermediates.
+struct __align__(16) Seg32x2 {
+    float4 g[8];
+};
+
 // Traversal record of one node (64 bytes).
 struct __align__(16) NodeRec {
     double cx, cy, cz, bound;
@@ -332,6 +340,80 @@ __device__ __forceinline__ bool pair32(float rx, float ry, float rz, const float
         uz = fmaf(coefficient, cz, uz);
     }
     return need64;
+}
+
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// pair32 for two segments at once in packed FP32 (one f32x2 add, multiply or FMA per operation for both segments;
+// tests, selects and the special-function unit per component): the same arithmetic as pair32 for MODEL 0 (no core),
+// 1 (Rankine) and 2 (Lamb-Oseen).  The target is (t_hi + t_lo) per axis, broadcast in both halves; `rec` is the pair's
+// Seg32x2.  Accumulates into the float2 sums (one half per segment) the pairs that do not need FP64 and returns those
+// that do: bit 0 for the first segment, bit 1 for the second.  The caller's target must have finite coordinates
+// below 1e30 (an out-of-range pair's finite intermediates are multiplied by a zero coefficient).
+template <int MODEL, bool NEAR>
+__device__ __forceinline__ unsigned pair32x2(float2 txh, float2 tyh, float2 tzh, float2 txl, float2 tyl, float2 tzl,
+                                             const float4 *rec, float near2, float2 &u0, float2 &u1, float2 &u2) {
+    static_assert(MODEL >= 0 && MODEL <= 2, "packed pairs for the models without a per-pair special form");
+    const float4 g0 = rec[0], g1 = rec[1], g2 = rec[2], g3 = rec[3], g4 = rec[4], g5 = rec[5], g6 = rec[6],
+                 g7 = rec[7];
+    const float2 il = make_float2(g1.z, g1.w), gf = make_float2(g3.z, g3.w);
+    const float2 dx = make_float2(g4.x, g4.y), dy = make_float2(g4.z, g4.w), dz = make_float2(g5.x, g5.y);
+    const float2 w = make_float2(g5.z, g5.w);
+    const float2 ndx = make_float2(g6.x, g6.y), ndy = make_float2(g6.z, g6.w), ndz = make_float2(g7.x, g7.y);
+    // q = (t_hi - s_hi) + (t_lo - s_lo), a = q / L, b = a - d, c = d x a
+    const float2 ax = mul2(add2(add2(txh, make_float2(g0.x, g0.y)), add2(txl, make_float2(g2.x, g2.y))), il);
+    const float2 ay = mul2(add2(add2(tyh, make_float2(g0.z, g0.w)), add2(tyl, make_float2(g2.z, g2.w))), il);
+    const float2 az = mul2(add2(add2(tzh, make_float2(g1.x, g1.y)), add2(tzl, make_float2(g3.x, g3.y))), il);
+    const float2 bx = add2(ax, ndx), by = add2(ay, ndy), bz = add2(az, ndz);
+    const float2 cx = fma2(dy, az, mul2(ndz, ay));
+    const float2 cy = fma2(dz, ax, mul2(ndx, az));
+    const float2 cz = fma2(dx, ay, mul2(ndy, ax));
+    const float2 h2 = fma2(cx, cx, fma2(cy, cy, mul2(cz, cz)));
+    const float2 na2 = fma2(ax, ax, fma2(ay, ay, mul2(az, az)));
+    const float2 nb2 = fma2(bx, bx, fma2(by, by, mul2(bz, bz)));
+    const float2 dot = fma2(ax, bx, fma2(ay, by, mul2(az, bz)));
+    const float big0 = fmaxf(1.0f, fmaxf(na2.x, nb2.x)), big1 = fmaxf(1.0f, fmaxf(na2.y, nb2.y));
+    const float2 lim = mul2(make_float2(big0, big1), make_float2(1e-8f, 1e-8f));
+    bool n0 = !(h2.x > lim.x) || !(big0 < 1e18f);
+    bool n1 = !(h2.y > lim.y) || !(big1 < 1e18f);
+    if (MODEL != 0 && NEAR) {
+        const float2 t = fma2(az, dz, fma2(ay, dy, mul2(ax, dx)));
+        const float2 seg2 = make_float2(t.x < 0.0f ? na2.x : (t.x > 1.0f ? nb2.x : h2.x),
+                                        t.y < 0.0f ? na2.y : (t.y > 1.0f ? nb2.y : h2.y));
+        const float2 rr = mul2(seg2, w);
+        n0 = n0 || (w.x > 0.0f && rr.x < near2);
+        n1 = n1 || (w.y > 0.0f && rr.y < near2);
+    }
+    const float2 na = mul2(na2, make_float2(rsqrtf(na2.x), rsqrtf(na2.y)));
+    const float2 nb = mul2(nb2, make_float2(rsqrtf(nb2.x), rsqrtf(nb2.y)));
+    const float2 product = mul2(na, nb);
+    const float2 sum = add2(na, nb);
+    // as in pair32: where a.b < 0, |a||b| + a.b = h^2 / (|a||b| - a.b)
+    const float2 numr = mul2(sum, fma2(dot, make_float2(-1.0f, -1.0f), product));
+    const float2 plus = add2(product, dot);
+    const float2 num = make_float2(dot.x < 0.0f ? numr.x : sum.x, dot.y < 0.0f ? numr.y : sum.y);
+    const float2 den = mul2(product, make_float2(dot.x < 0.0f ? h2.x : plus.x, dot.y < 0.0f ? h2.y : plus.y));
+    float2 factor = make_float2(1.0f, 1.0f);
+    if (MODEL == 1) {
+        const float2 r2 = mul2(h2, w);
+        factor = make_float2(w.x > 0.0f ? fminf(r2.x, 1.0f) : 1.0f, w.y > 0.0f ? fminf(r2.y, 1.0f) : 1.0f);
+    } else if (MODEL == 2) {
+        const float2 r2 = mul2(h2, w);
+        const float2 x = mul2(r2, make_float2(-(float)LAMB_A, -(float)LAMB_A));
+        const float2 f = fma2(make_float2(__expf(x.x), __expf(x.y)), make_float2(-1.0f, -1.0f), make_float2(1.0f, 1.0f));
+        factor = make_float2(w.x > 0.0f && r2.x < (float)LAMB_CUT2 ? f.x : 1.0f,
+                             w.y > 0.0f && r2.y < (float)LAMB_CUT2 ? f.y : 1.0f);
+    }
+    float2 coefficient = mul2(mul2(gf, factor),
+                              mul2(num, make_float2(__fdividef(1.0f, den.x), __fdividef(1.0f, den.y))));
+    coefficient.x = n0 ? 0.0f : coefficient.x;
+    coefficient.y = n1 ? 0.0f : coefficient.y;
+    u0 = fma2(coefficient, cx, u0);
+    u1 = fma2(coefficient, cy, u1);
+    u2 = fma2(coefficient, cz, u2);
+    return (n0 ? 1u : 0u) | (n1 ? 2u : 0u);
 }
 
 // The fourth-order term of the expansion, R = x - c:

@@ -1540,6 +1540,28 @@ int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_
 
 using namespace bs;
 
+// The packed-pair records of the tree-ordered segments (one thread per segment; m rounded up to even, the padding
+// segment all zero).
+__global__ void pair_records_kernel(int64_t m, const Seg32 *seg32, Seg32x2 *pairs) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ((m + 1) & ~int64_t(1))) return;
+    float v[16];
+    for (int f = 0; f < 16; ++f) v[f] = 0.0f;
+    if (k < m) {
+        const Seg32 r = seg32[k];
+        const bool ok = r.hi.w > 0.0f && fabsf(r.hi.x) < 1e30f && fabsf(r.hi.y) < 1e30f && fabsf(r.hi.z) < 1e30f;
+        if (ok) {
+            v[0] = -r.hi.x; v[1] = -r.hi.y; v[2] = -r.hi.z; v[3] = r.hi.w;
+            v[4] = -r.lo.x; v[5] = -r.lo.y; v[6] = -r.lo.z;
+        }
+        v[7] = r.lo.w;
+        v[8] = r.dir.x; v[9] = r.dir.y; v[10] = r.dir.z; v[11] = r.dir.w;
+        v[12] = -r.dir.x; v[13] = -r.dir.y; v[14] = -r.dir.z;
+    }
+    float *out = reinterpret_cast<float *>(pairs + (k >> 1)) + (k & 1);
+    for (int f = 0; f < 16; ++f) out[2 * f] = v[f];
+}
+
 // Shared tail of both constructors: inverse permutation, int64 order, tree-ordered segment records, moments.
 static int finish_tree(bs_tree *t, const bs_sources *src, const SegGeo *geo, Scratch &scratch, cudaStream_t s) {
     const int64_t m = t->m;
@@ -1547,11 +1569,14 @@ static int finish_tree(bs_tree *t, const bs_sources *src, const SegGeo *geo, Scr
     t->inverse = t->alloc<int32_t>(m, s);
     t->seg64 = t->alloc<Seg64>(m, s);
     t->seg32 = t->alloc<Seg32>(m, s);
-    if (!t->order || !t->inverse || !t->seg64 || !t->seg32) return BS_ERR_OOM;
+    t->seg32x2 = t->alloc<Seg32x2>((m + 1) / 2, s);
+    if (!t->order || !t->inverse || !t->seg64 || !t->seg32 || !t->seg32x2) return BS_ERR_OOM;
     widen_order_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, t->order32, t->order, t->inverse);
     BS_CHECK_LAUNCH("widen_order_kernel");
     int rc = pack_segments(src, t->order32, t->seg64, t->seg32, nullptr, s);
     if (rc != BS_OK) return rc;
+    pair_records_kernel<<<blocks_for(m + 1, 256), 256, 0, s>>>(m, t->seg32, t->seg32x2);
+    BS_CHECK_LAUNCH("pair_records_kernel");
     return compute_moments(t, geo, scratch, s);
 }
 

@@ -36,6 +36,7 @@ struct TreeView {
     const Far32y *far32y;
     const Seg64 *seg64;
     const Seg32 *seg32;
+    const Seg32x2 *seg32x2;
 };
 
 struct EvalArgs {
@@ -77,6 +78,7 @@ struct Target {
     float xh0, xl0, xh1, xl1, xh2, xl2;
     int64_t p;
     bool valid;
+    bool packed;  // finite coordinates below 1e30: the packed pair may take this target
     __device__ void load(const EvalArgs &a, int64_t i) {
         valid = i < a.n;
         p = valid ? a.perm[i] : 0;
@@ -85,6 +87,7 @@ struct Target {
         split2(x0, xh0, xl0);
         split2(x1, xh1, xl1);
         split2(x2, xh2, xl2);
+        packed = fabs(x0) < 1e30 && fabs(x1) < 1e30 && fabs(x2) < 1e30;
     }
 };
 
@@ -123,6 +126,114 @@ __device__ __forceinline__ void far_node(const EvalArgs &a, const Target &t, int
     }
 }
 
+// FP64 re-evaluation of the pairs of segments base + j (bits of `need`): value added or flag recorded.
+template <int PREC, int MODEL>
+__device__ __forceinline__ void pairs_in_fp64(const EvalArgs &a, const Target &t, int base, unsigned need,
+                                              Acc<PREC> &acc, int &flag) {
+    while (need) {
+        const int j = __ffs(need) - 1;
+        need &= need - 1;
+        double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+        const int fl = pair64_at(t.x0, t.x1, t.x2, a.tv.seg64[base + j], MODEL, a.raise_singular, v0, v1, v2);
+        if (fl != BS_FLAG_OK) {
+            if (flag == BS_FLAG_OK) flag = fl;
+        } else {
+            acc.add64(v0, v1, v2);
+        }
+    }
+}
+
+// One segment for one lane in single precision, read from the tree-ordered Seg32 array (the leaf's odd ends and the
+// tiles the packed path leaves out).
+template <int PREC, int MODEL>
+__device__ __forceinline__ void single_pair(const EvalArgs &a, const Target &t, int s, float &t0, float &t1, float &t2,
+                                            Acc<PREC> &acc, int &flag, long long &fp64_pairs) {
+    const Seg32 r = a.tv.seg32[s];
+    const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
+    const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
+    const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
+    if (pair32<MODEL>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) {
+        ++fp64_pairs;
+        pairs_in_fp64<PREC, MODEL>(a, t, s, 1u, acc, flag);
+    }
+}
+
+// One leaf of a single-precision evaluation with MODEL 0..2, two segments per operation: the leaf's whole pairs of
+// consecutive segments [2 p0, 2 p1) are staged 16 pairs (32 segments) at a time as Seg32x2 records, and a walking lane
+// evaluates a tile with pair32x2 when none of its segments is excluded for it (otherwise, and for targets the packed
+// pair does not take, segment by segment with pair32); the odd ends of the leaf go through pair32.  Exclusions are
+// consumed in position order through the lane's cursor e.
+template <int PREC, int MODEL>
+__device__ __forceinline__ void leaf_pairs_packed(const EvalArgs &a, const Target &t, int lo, int hi, bool walk,
+                                                  bool all_clear, int64_t &e, int64_t e1, float4 *tile,
+                                                  Acc<PREC> &acc, int &flag, long long &near_pairs,
+                                                  long long &fp64_pairs) {
+    const int lane = threadIdx.x & 31;
+    float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+    float2 u0 = make_float2(0.f, 0.f), u1 = u0, u2 = u0;
+    const float2 txh = make_float2(t.xh0, t.xh0), tyh = make_float2(t.xh1, t.xh1), tzh = make_float2(t.xh2, t.xh2);
+    const float2 txl = make_float2(t.xl0, t.xl0), tyl = make_float2(t.xl1, t.xl1), tzl = make_float2(t.xl2, t.xl2);
+    // an excluded segment at position s: consume it and report
+    auto excluded = [&](int s) -> bool {
+        while (e < e1 && a.ex_pos[e] < s) ++e;
+        if (e < e1 && a.ex_pos[e] == s) {
+            ++e;
+            return true;
+        }
+        return false;
+    };
+    const int p0 = (lo + 1) >> 1, p1 = hi >> 1;
+    if (walk && (lo & 1)) {  // the leaf's first segment, when it starts a pair with the previous leaf's last
+        if (!excluded(lo)) {
+            ++near_pairs;
+            single_pair<PREC, MODEL>(a, t, lo, t0, t1, t2, acc, flag, fp64_pairs);
+        }
+    }
+    for (int pb = p0; pb < p1; pb += 16) {
+        const int np = min(16, p1 - pb), base = 2 * pb, cnt = 2 * np;
+        __syncwarp();
+        const float4 *src = reinterpret_cast<const float4 *>(a.tv.seg32x2 + pb);
+        for (int i = lane; i < 8 * np; i += 32) tile[i] = __ldg(src + i);
+        __syncwarp();
+        if (!walk) continue;
+        unsigned excl = 0;
+        while (e < e1 && a.ex_pos[e] < base + cnt) excl |= 1u << (a.ex_pos[e++] - base);
+        near_pairs += cnt - __popc(excl);
+        unsigned need = 0;
+        if (excl == 0 && t.packed) {
+            if (all_clear) {
+#pragma unroll 4
+                for (int q = 0; q < np; ++q)
+                    need |= pair32x2<MODEL, false>(txh, tyh, tzh, txl, tyl, tzl, tile + 8 * q, a.near2, u0, u1, u2)
+                            << (2 * q);
+            } else {
+#pragma unroll 2
+                for (int q = 0; q < np; ++q)
+                    need |= pair32x2<MODEL, true>(txh, tyh, tzh, txl, tyl, tzl, tile + 8 * q, a.near2, u0, u1, u2)
+                            << (2 * q);
+            }
+        } else {
+            for (int j = 0; j < cnt; ++j) {
+                if ((excl >> j) & 1u) continue;
+                const Seg32 r = a.tv.seg32[base + j];
+                const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
+                const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
+                const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
+                if (pair32<MODEL>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1u << j;
+            }
+        }
+        fp64_pairs += __popc(need);
+        pairs_in_fp64<PREC, MODEL>(a, t, base, need, acc, flag);
+    }
+    if (walk && (hi & 1) && hi - 1 >= lo && hi - 1 >= 2 * p1) {  // the leaf's last segment, when it ends unpaired
+        if (!excluded(hi - 1)) {
+            ++near_pairs;
+            single_pair<PREC, MODEL>(a, t, hi - 1, t0, t1, t2, acc, flag, fp64_pairs);
+        }
+    }
+    if (walk) acc.add32(t0 + (u0.x + u0.y), t1 + (u1.x + u1.y), t2 + (u2.x + u2.y));
+}
+
 // One leaf for the lanes in `walk`: the warp stages the leaf's records in shared memory 32 at a time, then every
 // walking lane evaluates its pairs (exclusions skipped through the lane's forward cursor e).
 template <int PREC, int MODEL>
@@ -142,6 +253,12 @@ __device__ __forceinline__ void leaf_pairs(const EvalArgs &a, const Target &t, c
         clear = gap > 1.01 * sqrt((double)a.near2) * nr.clear_core;
     }
     const bool all_clear = __all_sync(0xffffffffu, clear);
+    if constexpr (PREC != 0 && MODEL <= 2) {
+        // the warp's tile space is sized for 32 Seg64 (3 KB): 16 Seg32x2 (2 KB) fit
+        leaf_pairs_packed<PREC, MODEL>(a, t, lo, hi, walk, all_clear, e, e1, reinterpret_cast<float4 *>(seg64_tile),
+                                       acc, flag, near_pairs, fp64_pairs);
+        return;
+    }
     for (int base = lo; base < hi; base += 32) {
         const int cnt = min(32, hi - base);
         __syncwarp();
@@ -443,8 +560,9 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
     }
 }
 
+// Three blocks per SM (up to 168 registers a thread): the packed pairs of a tile need the registers to interleave.
 template <int PREC, int MODEL>
-__global__ void __launch_bounds__(LIST_WARPS * 32, 5) tree_list_kernel(EvalArgs a, int64_t target_warps) {
+__global__ void __launch_bounds__(LIST_WARPS * 32, 3) tree_list_kernel(EvalArgs a, int64_t target_warps) {
     __shared__ __align__(16) unsigned char tile_mem[LIST_WARPS * 32 * sizeof(Seg64)];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Seg64 *seg64_tile = reinterpret_cast<Seg64 *>(tile_mem) + warp * 32;
@@ -773,7 +891,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     args.ex_ptr = ex_pos ? tgt->ex_ptr : nullptr;
     args.ex_pos = ex_pos;
     args.tv = TreeView{tree->nodes,  tree->far64,  tree->far32, tree->far64x, tree->far32x,
-                       tree->far64y, tree->far32y, tree->seg64, tree->seg32};
+                       tree->far64y, tree->far32y, tree->seg64, tree->seg32, tree->seg32x2};
     args.theta = tp->theta;
     args.theta2 = tp->theta * tp->theta;
     args.clearance = tp->clearance;
@@ -803,7 +921,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     const unsigned walk_grid = (unsigned)((target_warps + block / 32 - 1) / (block / 32));
     const int64_t items = target_warps * chunks;
     const unsigned list_grid = (unsigned)std::max<int64_t>(
-        1, std::min<int64_t>((items + LIST_WARPS - 1) / LIST_WARPS, (int64_t)ctx->sm_count * 4));
+        1, std::min<int64_t>((items + LIST_WARPS - 1) / LIST_WARPS, (int64_t)ctx->sm_count * 3));
     launch_eval(kp->precision, kp->model, walk_grid, block, smem, list_grid, target_warps, nblocks(n, 256), s, args,
                 out, flags);
     BS_CHECK_LAUNCH("tree evaluation");
