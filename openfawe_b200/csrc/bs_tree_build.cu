@@ -1207,13 +1207,17 @@ __global__ void __launch_bounds__(128) leaf_moments_kernel(int64_t count, const 
         double acc[MT::slots][3], r2 = 0.0;
 #pragma unroll
         for (int r = 0; r < MT::slots; ++r) acc[r][0] = acc[r][1] = acc[r][2] = 0.0;
+        // the next stage's record is loaded while this stage computes
+        SegGeo next;
+        if (a + lane < b) next = geo[order[a + lane]];
         for (int64_t base = a; base < b; base += 32) {
             const int64_t k = base + lane;
+            const SegGeo e = next;
+            if (k + 32 < b) next = geo[order[k + 32]];
             double g[MT::n], al[3] = {0.0, 0.0, 0.0};
 #pragma unroll
             for (int q = 0; q < MT::n; ++q) g[q] = 0.0;
             if (k < b) {
-                const SegGeo e = geo[order[k]];
                 const double a0 = e.sx - c0, a1 = e.sy - c1, a2 = e.sz - c2;
                 const double b0 = e.ex - c0, b1 = e.ey - c1, b2 = e.ez - c2;
                 // the reference's ((x^2 + y^2) + z^2) without contraction, as in every bound of this file
@@ -1468,7 +1472,8 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
     const NodeOut out{t->lo, t->hi, t->left, t->right, t->centre, t->core, t->bound, t->m0, t->m1, t->m2,
                       t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x,
                       t->far64y, t->far32y};
-    node_final_kernel<PARTS><<<blocks_for(count, 128), 128, 0, s>>>(count, bound2, sums, out);
+    // one warp per block: the thread per node is long, so the nodes spread over every SM
+    node_final_kernel<PARTS><<<blocks_for(count, 32), 32, 0, s>>>(count, bound2, sums, out);
     BS_CHECK_LAUNCH("bottom-up moments");
     return BS_OK;
 }
