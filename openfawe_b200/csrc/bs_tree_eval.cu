@@ -257,83 +257,83 @@ __device__ __forceinline__ void leaf_pairs(const EvalArgs &a, const Target &t, c
         // the warp's tile space is sized for 32 Seg64 (3 KB): 16 Seg32x2 (2 KB) fit
         leaf_pairs_packed<PREC, MODEL>(a, t, lo, hi, walk, all_clear, e, e1, reinterpret_cast<float4 *>(seg64_tile),
                                        acc, flag, near_pairs, fp64_pairs);
-        return;
-    }
-    for (int base = lo; base < hi; base += 32) {
-        const int cnt = min(32, hi - base);
-        __syncwarp();
-        if (lane < cnt) {
-            if (PREC == 0) seg64_tile[lane] = a.tv.seg64[base + lane];
-            else seg32_tile[lane] = a.tv.seg32[base + lane];
-        }
-        __syncwarp();
-        if (!walk) continue;
-        unsigned excl = 0;
-        while (e < e1 && a.ex_pos[e] < base + cnt) excl |= 1u << (a.ex_pos[e++] - base);
-        near_pairs += cnt - __popc(excl);
-        if (PREC == 0) {
-            double u0 = 0.0, u1 = 0.0, u2 = 0.0;
-            for (int j = 0; j < cnt; ++j) {
-                if ((excl >> j) & 1u) continue;
-                int fl = pair64_at(t.x0, t.x1, t.x2, seg64_tile[j], a.model, a.raise_singular, u0, u1, u2);
-                if (fl != BS_FLAG_OK && flag == BS_FLAG_OK) flag = fl;
+    } else {
+        for (int base = lo; base < hi; base += 32) {
+            const int cnt = min(32, hi - base);
+            __syncwarp();
+            if (lane < cnt) {
+                if (PREC == 0) seg64_tile[lane] = a.tv.seg64[base + lane];
+                else seg32_tile[lane] = a.tv.seg32[base + lane];
             }
-            acc.add64(u0, u1, u2);
-            continue;
-        }
-        unsigned need = 0;
-        if (excl == 0 && all_clear && cnt == 32) {  // the common case: a full tile, every pair counts, none near a core
-#pragma unroll 8
-            for (int j = 0; j < 32; ++j) {
-                const Seg32 &r = seg32_tile[j];
-                const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
-                const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
-                const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
-                if (pair32<MODEL, false>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1u << j;
+            __syncwarp();
+            if (!walk) continue;
+            unsigned excl = 0;
+            while (e < e1 && a.ex_pos[e] < base + cnt) excl |= 1u << (a.ex_pos[e++] - base);
+            near_pairs += cnt - __popc(excl);
+            if (PREC == 0) {
+                double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+                for (int j = 0; j < cnt; ++j) {
+                    if ((excl >> j) & 1u) continue;
+                    int fl = pair64_at(t.x0, t.x1, t.x2, seg64_tile[j], a.model, a.raise_singular, u0, u1, u2);
+                    if (fl != BS_FLAG_OK && flag == BS_FLAG_OK) flag = fl;
+                }
+                acc.add64(u0, u1, u2);
+                continue;
             }
-        } else if (excl == 0 && all_clear) {
-#pragma unroll 4
-            for (int j = 0; j < cnt; ++j) {
-                const Seg32 &r = seg32_tile[j];
-                const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
-                const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
-                const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
-                if (pair32<MODEL, false>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1u << j;
-            }
-        } else if (excl == 0) {  // every pair counts
-#pragma unroll 4
-            for (int j = 0; j < cnt; ++j) {
-                const Seg32 &r = seg32_tile[j];
-                const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
-                const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
-                const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
-                if (pair32<MODEL>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1u << j;
-            }
-        } else {
-            for (int j = 0; j < cnt; ++j) {
-                if ((excl >> j) & 1u) continue;
-                const Seg32 &r = seg32_tile[j];
-                const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
-                const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
-                const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
-                if (pair32<MODEL>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1u << j;
-            }
-        }
-        // pairs near a segment, its axis or out of FP32 range: FP64 from FP64 inputs
-        fp64_pairs += __popc(need);
-        while (need) {
-            const int j = __ffs(need) - 1;
-            need &= need - 1;
-            double v0 = 0.0, v1 = 0.0, v2 = 0.0;
-            int fl = pair64_at(t.x0, t.x1, t.x2, a.tv.seg64[base + j], MODEL, a.raise_singular, v0, v1, v2);
-            if (fl != BS_FLAG_OK) {
-                if (flag == BS_FLAG_OK) flag = fl;
+            unsigned need = 0;
+            if (excl == 0 && all_clear && cnt == 32) {  // the common case: a full tile, every pair counts, none near a core
+    #pragma unroll 8
+                for (int j = 0; j < 32; ++j) {
+                    const Seg32 &r = seg32_tile[j];
+                    const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
+                    const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
+                    const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
+                    if (pair32<MODEL, false>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1u << j;
+                }
+            } else if (excl == 0 && all_clear) {
+    #pragma unroll 4
+                for (int j = 0; j < cnt; ++j) {
+                    const Seg32 &r = seg32_tile[j];
+                    const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
+                    const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
+                    const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
+                    if (pair32<MODEL, false>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1u << j;
+                }
+            } else if (excl == 0) {  // every pair counts
+    #pragma unroll 4
+                for (int j = 0; j < cnt; ++j) {
+                    const Seg32 &r = seg32_tile[j];
+                    const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
+                    const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
+                    const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
+                    if (pair32<MODEL>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1u << j;
+                }
             } else {
-                acc.add64(v0, v1, v2);
+                for (int j = 0; j < cnt; ++j) {
+                    if ((excl >> j) & 1u) continue;
+                    const Seg32 &r = seg32_tile[j];
+                    const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
+                    const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
+                    const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
+                    if (pair32<MODEL>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1u << j;
+                }
+            }
+            // pairs near a segment, its axis or out of FP32 range: FP64 from FP64 inputs
+            fp64_pairs += __popc(need);
+            while (need) {
+                const int j = __ffs(need) - 1;
+                need &= need - 1;
+                double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+                int fl = pair64_at(t.x0, t.x1, t.x2, a.tv.seg64[base + j], MODEL, a.raise_singular, v0, v1, v2);
+                if (fl != BS_FLAG_OK) {
+                    if (flag == BS_FLAG_OK) flag = fl;
+                } else {
+                    acc.add64(v0, v1, v2);
+                }
             }
         }
+        if (walk && PREC != 0) acc.add32(t0, t1, t2);
     }
-    if (walk && PREC != 0) acc.add32(t0, t1, t2);
 }
 
 // Phase 1: the traversal.  Each warp walks the tree once for its 32 targets and writes an interaction list: far
