@@ -387,13 +387,16 @@ def main():
     csr = (np.zeros(len(case["points"]) + 1, dtype=np.int64), np.zeros(0, dtype=np.int64))
     a = (case["points"], case["starts"], case["directions"], case["lengths"], case["gamma"], case["radius"], model,
          csr, "raise", tree, cuda)
-    vortex_cuda_tree.cuda_tree_sum(*a, order=args.order)
-    e2e = []
-    for _ in range(max(3, min(args.steps, 5))):
+    for _ in range(2):  # warm-up: staging ring, pools, host pages
+        vortex_cuda_tree.cuda_tree_sum(*a, order=args.order)
+    e2e, e2e_stages = [], []
+    for _ in range(max(5, min(args.steps, 10))):
         torch.cuda.synchronize()
         tick = time.perf_counter()
         vortex_cuda_tree.cuda_tree_sum(*a, order=args.order)
         e2e.append(1e3 * (time.perf_counter() - tick))
+        last = vortex_cuda_tree.Statistics.last
+        e2e_stages.append({k: 1e3 * last[k] for k in ("upload_s", "build_s", "evaluate_s", "download_s")})
     h2d = sum(np.asarray(x).nbytes for x in (case["points"], case["starts"], case["directions"], case["lengths"],
                                               case["gamma"], case["radius"]))
     d2h = len(case["points"]) * (24 + 1 + 8)
@@ -424,7 +427,8 @@ def main():
                                    "direct_equivalent": len(case["points"]) * len(case["starts"]) / (ms * 1e-3)},
             "roofline": roofline,
             "e2e": {"value": float(np.median(e2e)), "unit": "ms/call", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
+                    "d2h_bytes_per_step": int(d2h), "calls_ms": e2e,
+                    "stages_ms_of_median_call": e2e_stages[int(np.argsort(e2e)[len(e2e) // 2])]},
             "gpu_launches": gpu_launches, "clocks": clocks}
     if rank == 0 and world == 1:
         line["cpu_baseline"] = cpu_baseline(case, args)
