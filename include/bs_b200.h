@@ -104,6 +104,11 @@ int bs_upload(bs_ctx *ctx, void *dst, const void *src, size_t bytes, bs_stream s
  * arrive as several host arrays per call.  Same return rule as bs_upload. */
 int bs_upload_many(bs_ctx *ctx, int count, void *const *dst, const void *const *src, const size_t *bytes,
                    bs_stream stream);
+/* Device -> ordinary host memory for `count` arrays (dst[i] host <- src[i] device, bytes[i] each) through the same
+ * pinned ring: the transfer of one chunk overlaps the host copy of the previous one.  Ordered after the work queued
+ * on `stream`; returns when every byte has arrived. */
+int bs_download_many(bs_ctx *ctx, int count, void *const *dst, const void *const *src, const size_t *bytes,
+                     bs_stream stream);
 /* Measures the device's FP32 FMA throughput (TFLOP/s, an FMA counted as 2) with a kernel of independent FMA chains
  * on every SM: the denominator of the pair kernels' roofline, which run on the FP32 pipe. */
 int bs_fp32_peak(bs_ctx *ctx, double *tflops);

@@ -55,6 +55,7 @@ SIGNATURES = {
     "bs_fp32_peak": (ctypes.c_int, [_p, ctypes.POINTER(ctypes.c_double)]),
     "bs_upload": (ctypes.c_int, [_p, _p, _p, ctypes.c_size_t, _p]),
     "bs_upload_many": (ctypes.c_int, [_p, ctypes.c_int, _p, _p, _p, _p]),
+    "bs_download_many": (ctypes.c_int, [_p, ctypes.c_int, _p, _p, _p, _p]),
     "bs_direct": (ctypes.c_int, [_p, ctypes.POINTER(Sources), ctypes.POINTER(Targets), ctypes.POINTER(KernelParams),
                                  _p, _p, _p]),
     "bs_tree_build": (ctypes.c_int, [_p, ctypes.POINTER(Sources), ctypes.POINTER(TreeParams), ctypes.POINTER(_p),

@@ -2,7 +2,7 @@
 // copied into 4 MiB pinned chunks by OpenMP threads (non-temporal stores where the CPU has AVX2) while the chunks
 // before them cross PCIe (cudaMemcpyAsync on the caller's stream), so host copying and transfer overlap and the copy
 // runs on several cores.  The call returns when the sources have been read; the last transfers may still be in flight
-// on the stream.  bs_upload_many keeps the ring going across several arrays.
+// on the stream.  bs_upload_many keeps the ring going across several arrays; bs_download_many runs it the other way.
 #include <immintrin.h>
 #include <omp.h>
 
@@ -136,3 +136,74 @@ extern "C" int bs_upload_many(bs_ctx *ctx, int count, void *const *dst, const vo
     if (count == 0) return BS_OK;
     return upload_list(ctx, count, dst, src, bytes, (cudaStream_t)stream);
 }
+
+// Device -> host through the same ring: chunk k's transfer into a pinned slot is in flight while the host copies chunk
+// k - 1 out of its slot (OpenMP threads for large chunks).  Returns when every byte is in the host buffers.
+extern "C" int bs_download_many(bs_ctx *ctx, int count, void *const *dst, const void *const *src, const size_t *bytes,
+                                bs_stream stream) {
+    if (!ctx || count < 0 || (count > 0 && (!dst || !src || !bytes))) {
+        bs::set_error("bs_download_many: null argument");
+        return BS_ERR_ARG;
+    }
+    for (int a = 0; a < count; ++a)
+        if (bytes[a] > 0 && (!dst[a] || !src[a])) {
+            bs::set_error("bs_download_many: null pointer for copy %d", a);
+            return BS_ERR_ARG;
+        }
+    if (count == 0) return BS_OK;
+    BS_CUDA(cudaSetDevice(ctx->device));
+    bs_upload_ring *r = nullptr;
+    int rc = ring_of(ctx, &r);
+    if (rc != BS_OK) return rc;
+    std::lock_guard<std::mutex> guard(r->lock);
+    cudaStream_t s = (cudaStream_t)stream;
+    const int threads = std::max(1, std::min(8, omp_get_max_threads()));
+    struct Pending {
+        char *to;
+        int slot;
+        size_t len;
+    };
+    Pending pending[bs_upload_ring::SLOTS];
+    int head = 0, queued = 0, k = 0;
+    auto drain_one = [&]() -> int {
+        const Pending p = pending[head];
+        head = (head + 1) % bs_upload_ring::SLOTS;
+        --queued;
+        BS_CUDA(cudaEventSynchronize(r->done[p.slot]));
+        const char *stage = static_cast<const char *>(r->buf[p.slot]);
+        if (p.len >= (size_t(256) << 10) && threads > 1) {
+            const size_t piece = (p.len + threads - 1) / threads;
+#pragma omp parallel for num_threads(threads) schedule(static)
+            for (int i = 0; i < threads; ++i) {
+                const size_t lo = std::min(p.len, (size_t)i * piece), hi = std::min(p.len, lo + piece);
+                if (hi > lo) std::memcpy(p.to + lo, stage + lo, hi - lo);
+            }
+        } else {
+            std::memcpy(p.to, stage, p.len);
+        }
+        return BS_OK;
+    };
+    for (int a = 0; a < count; ++a) {
+        const char *from = static_cast<const char *>(src[a]);
+        char *to = static_cast<char *>(dst[a]);
+        for (size_t off = 0; off < bytes[a]; off += bs_upload_ring::CHUNK, ++k) {
+            if (queued == bs_upload_ring::SLOTS) {
+                rc = drain_one();
+                if (rc != BS_OK) return rc;
+            }
+            const int slot = k % bs_upload_ring::SLOTS;
+            BS_CUDA(cudaEventSynchronize(r->done[slot]));  // an upload may still be reading the slot
+            const size_t len = std::min(bs_upload_ring::CHUNK, bytes[a] - off);
+            BS_CUDA(cudaMemcpyAsync(r->buf[slot], from + off, len, cudaMemcpyDeviceToHost, s));
+            BS_CUDA(cudaEventRecord(r->done[slot], s));
+            pending[(head + queued) % bs_upload_ring::SLOTS] = Pending{to + off, slot, len};
+            ++queued;
+        }
+    }
+    while (queued > 0) {
+        rc = drain_one();
+        if (rc != BS_OK) return rc;
+    }
+    return BS_OK;
+}
+

@@ -69,6 +69,23 @@ def f64_many(arrays, device):
     return out
 
 
+def to_host_many(tensors, shapes, dtypes):
+    """Owned NumPy arrays holding device tensors, copied through the library's pinned ring in one pass
+    (bs_download_many); None entries give None."""
+    out = [None if t is None else np.empty(shape, dtype=dtype) for t, shape, dtype in zip(tensors, shapes, dtypes)]
+    pairs = [(h, t) for h, t in zip(out, tensors) if t is not None and h.size]
+    if pairs:
+        device = pairs[0][1].device
+        k = len(pairs)
+        views = [t.contiguous() for _, t in pairs]
+        L.check(L.library().bs_download_many(L.context(device.index), k,
+                                             (ctypes.c_void_p * k)(*[h.ctypes.data for h, _ in pairs]),
+                                             (ctypes.c_void_p * k)(*[v.data_ptr() for v in views]),
+                                             (ctypes.c_size_t * k)(*[h.nbytes for h, _ in pairs]), _stream(device)),
+                "bs_download_many")
+    return out
+
+
 def f64(a, device):
     """A C-contiguous float64 tensor on `device` (copies only when needed)."""
     return _to_device(a, np.float64, torch.float64, _device_of(device))

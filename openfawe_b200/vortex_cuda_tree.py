@@ -89,9 +89,8 @@ def cuda_tree_sum(points, starts, directions, lengths, gamma, radius, model, csr
     build_s = 1e-3 * (stats["build_ms"] + stats["moments_ms"])
     evaluate_s = max(0.0, time.perf_counter() - tick - build_s)
     tick = time.perf_counter()
-    out = VC.to_host(d_out, (n, 3), np.float64)
-    flags = VC.to_host(d_flags, (n,), np.int8)
-    far = VC.to_host(d_far, (n,), np.int64)
+    out, flags, far = engine.to_host_many((d_out, d_flags, d_far), ((n, 3), (n,), (n,)),
+                                          (np.float64, np.int8, np.int64))
     download_s = time.perf_counter() - tick
     Statistics.last = dict(points=n, segments=m, nodes=int(stats["nodes"]), precision=precision, launches=1,
                            targets_per_launch=n, longest_launch_s=stats["evaluate_ms"] * 1e-3, suspect=0,

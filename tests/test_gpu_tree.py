@@ -365,3 +365,21 @@ def test_upload_many_moves_every_array_exactly(device):
         devs = engine.f64_many(hosts, torch.device("cuda", device))
         for h, d in zip(hosts, devs):
             assert np.array_equal(d.cpu().numpy(), np.ascontiguousarray(h))
+
+
+def test_download_many_moves_every_array_exactly(device):
+    """bs_download_many (device -> host through the pinned ring, the next chunk in flight while the previous one is
+    copied out) returns every byte, for arrays that end inside, at and across chunk boundaries and of several types."""
+    import torch
+    from openfawe_b200 import engine
+    rng = np.random.default_rng(23)
+    dev = torch.device("cuda", device)
+    arrays = [rng.normal(size=(4 << 20) // 8), rng.normal(size=3), rng.integers(-9, 9, size=(9 << 20) + 5).astype(np.int8),
+              rng.integers(0, 1 << 40, size=(1 << 17) + 1), rng.normal(size=((17 << 20) // 24, 3))]
+    tensors = [torch.as_tensor(a, device=dev) for a in arrays]
+    for _ in range(2):
+        got = engine.to_host_many(tensors + [None], [a.shape for a in arrays] + [(1,)],
+                                  [a.dtype for a in arrays] + [np.float64])
+        assert got[-1] is None
+        for a, g in zip(arrays, got):
+            assert g.dtype == a.dtype and np.array_equal(g, a)
