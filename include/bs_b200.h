@@ -84,6 +84,7 @@ typedef struct {
     double build_ms, moments_ms, evaluate_ms;                /* device time of the last build / evaluation */
     int64_t pair_slots;  /* lane slots spent in leaf walks (32 per warp-pair); near_pairs / pair_slots = SIMT use */
     double walk_ms, list_ms; /* device time of the traversal and interaction-list kernels of the last tree evaluation */
+    double upload_ms, download_ms; /* host time of the last bs_tree_sum_host's uploads and of its result read-back */
 } bs_stats;
 
 /* Context: one per device.  bs_init makes `device` current, probes it with a one-thread kernel (the reference's
@@ -136,6 +137,14 @@ int bs_direct(bs_ctx *ctx, const bs_sources *src, const bs_targets *tgt, const b
 #define BS_NOALLOC_SCRATCH_BYTES (65536 * 144 + 256) /* 9 MiB of FP64 + FP32 segment records, 256 B of flags */
 int bs_direct_noalloc(const bs_sources *src, const bs_targets *tgt, const bs_kernel_params *kp, double *out,
                       int8_t *flags, bs_stream stream);
+
+/* bs_tree_sum from and to ordinary host memory: `src` and `tgt` hold HOST pointers (the reference backend's NumPy
+ * inputs, vortex_cuda_tree.py:439-595; tgt->ex_ptr/ex_seg a host CSR or NULL), `out`, `flags` and `far_counts` (may be
+ * NULL) are host buffers.  The uploads go through the pinned staging ring; for a Morton tree the circulations and core
+ * radii are uploaded on a second stream while the device sorts the keys and builds the topology from starts,
+ * directions and lengths.  Results equal bs_tree_sum's on the same inputs.  Blocks until the results are in `out`. */
+int bs_tree_sum_host(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, const bs_targets *tgt,
+                     const bs_kernel_params *kp, double *out, int8_t *flags, int64_t *far_counts, bs_stream stream);
 
 /* Tree build on the device (Morton keys + radix sort + binary radix tree, or the reference's median split element for
  * element).  Node moments and contractions about cell centres in FP64 (vortex_tree.node_moments semantics).  Blocks

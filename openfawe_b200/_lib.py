@@ -40,7 +40,8 @@ class Stats(ctypes.Structure):
     _fields_ = [("points", _i64), ("segments", _i64), ("nodes", _i64), ("launches", _i64),
                 ("far_evaluations", _i64), ("near_pairs", _i64), ("fp64_pairs", _i64), ("visits", _i64),
                 ("build_ms", ctypes.c_double), ("moments_ms", ctypes.c_double), ("evaluate_ms", ctypes.c_double),
-                ("pair_slots", _i64), ("walk_ms", ctypes.c_double), ("list_ms", ctypes.c_double)]
+                ("pair_slots", _i64), ("walk_ms", ctypes.c_double), ("list_ms", ctypes.c_double),
+                ("upload_ms", ctypes.c_double), ("download_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -56,6 +57,8 @@ SIGNATURES = {
     "bs_upload": (ctypes.c_int, [_p, _p, _p, ctypes.c_size_t, _p]),
     "bs_upload_many": (ctypes.c_int, [_p, ctypes.c_int, _p, _p, _p, _p]),
     "bs_download_many": (ctypes.c_int, [_p, ctypes.c_int, _p, _p, _p, _p]),
+    "bs_tree_sum_host": (ctypes.c_int, [_p, ctypes.POINTER(Sources), ctypes.POINTER(TreeParams),
+                                        ctypes.POINTER(Targets), ctypes.POINTER(KernelParams), _p, _p, _p, _p]),
     "bs_direct": (ctypes.c_int, [_p, ctypes.POINTER(Sources), ctypes.POINTER(Targets), ctypes.POINTER(KernelParams),
                                  _p, _p, _p]),
     "bs_tree_build": (ctypes.c_int, [_p, ctypes.POINTER(Sources), ctypes.POINTER(TreeParams), ctypes.POINTER(_p),

@@ -98,6 +98,7 @@ extern "C" void bs_destroy(bs_ctx *ctx) {
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
     bs_upload_release(ctx);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     cudaMemPoolDestroy(ctx->pool);
     delete ctx;
 }

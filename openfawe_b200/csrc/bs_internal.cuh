@@ -85,6 +85,11 @@ struct Scratch {
 }  // namespace bs
 
 struct bs_upload_ring;  // pinned staging of bs_upload (bs_upload.cu)
+// bs_upload_many on the context's staging thread: returns at once; bs_stage_wait returns the upload's status once the
+// sources have been read (the transfers are queued on s).  One staging at a time per context.
+int bs_stage_async(bs_ctx *ctx, int count, void *const *dst, const void *const *src, const size_t *bytes,
+                   cudaStream_t s);
+int bs_stage_wait(bs_ctx *ctx);
 
 struct bs_ctx {
     int device;
@@ -92,6 +97,7 @@ struct bs_ctx {
     cudaMemPool_t pool;
     bs_stats stats;
     bs_upload_ring *upload = nullptr;
+    cudaStream_t copy_stream = nullptr;  // host-array uploads that overlap work on the caller's stream
 };
 
 // ---------------------------------------------------------------------------------------------------------------------

@@ -1,5 +1,7 @@
 // Internal tree object shared by the build, moments and evaluation translation units.
 #pragma once
+#include <functional>
+
 #include "bs_internal.cuh"
 
 namespace bs {
@@ -54,8 +56,10 @@ struct bs_tree {
 };
 
 // Build without waiting (bs_tree_sum): the stage times are read by tree_stage_times after the stream synchronised;
+// before_geometry (may be empty) runs on the host once, before any kernel reads gamma or radius (for Morton trees
+// while the node count is read back), so that a caller can still be uploading those two arrays;
 // tree_release frees the tree's memory stream-ordered on s, after the work queued there.
 int tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_tree **out, cudaStream_t s,
-               bool wait);
+               bool wait, const std::function<int()> &before_geometry);
 void tree_stage_times(bs_tree *t);
 void tree_release(bs_tree *tree, cudaStream_t s);

@@ -14,6 +14,7 @@
 // Moments: vortex_tree.node_moments (vortex_tree.py:309-376) per node, split into chunks of CHUNK positions so that big
 // nodes use many blocks; partial sums are combined in chunk order (run-to-run repeatable).
 #include <algorithm>
+#include <functional>
 #include <vector>
 
 #include "bs_sort.cuh"
@@ -111,13 +112,26 @@ __global__ void box_init_kernel(unsigned long long *box) {
     else if (threadIdx.x < 6) box[threadIdx.x] = ordered_bits(-INFINITY);
 }
 
-__global__ void mid_box_kernel(int64_t m, const SegGeo *geo, unsigned long long *box) {
+// The midpoint midpoint() forms from a SegGeo, formed from the input arrays with the same roundings (pack_kernel's
+// end s + (d L)), so that Morton keys need only starts, directions and lengths.
+__device__ __forceinline__ void midpoint_raw(const bs_sources &src, int64_t s, double &x, double &y, double &z) {
+    const double L = src.lengths[s];
+    const double sx = src.starts[3 * s], sy = src.starts[3 * s + 1], sz = src.starts[3 * s + 2];
+    const double ex = __dadd_rn(sx, __dmul_rn(src.directions[3 * s], L));
+    const double ey = __dadd_rn(sy, __dmul_rn(src.directions[3 * s + 1], L));
+    const double ez = __dadd_rn(sz, __dmul_rn(src.directions[3 * s + 2], L));
+    x = __dmul_rn(0.5, __dadd_rn(sx, ex));
+    y = __dmul_rn(0.5, __dadd_rn(sy, ey));
+    z = __dmul_rn(0.5, __dadd_rn(sz, ez));
+}
+
+__global__ void mid_box_kernel(int64_t m, const bs_sources src, unsigned long long *box) {
     __shared__ unsigned long long sb[6];
     if (threadIdx.x < 6) sb[threadIdx.x] = threadIdx.x < 3 ? ordered_bits(INFINITY) : ordered_bits(-INFINITY);
     __syncthreads();
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < m; s += (int64_t)gridDim.x * blockDim.x) {
         double v[3];
-        midpoint(geo[s], v[0], v[1], v[2]);
+        midpoint_raw(src, s, v[0], v[1], v[2]);
         for (int a = 0; a < 3; ++a) {
             atomicMin(&sb[a], ordered_bits(v[a]));
             atomicMax(&sb[3 + a], ordered_bits(v[a]));
@@ -139,7 +153,7 @@ __device__ __forceinline__ uint64_t spread3(uint32_t v) {
 }
 
 // Keys of the spec in morton_oracle.c: q = min(2^21 - 1, trunc((mid - lo) * inv)), inv = 2^21 / max extent.
-__global__ void morton_keys_kernel(int64_t m, const SegGeo *geo, const unsigned long long *box, uint64_t *keys,
+__global__ void morton_keys_kernel(int64_t m, const bs_sources src, const unsigned long long *box, uint64_t *keys,
                                    int32_t *vals) {
     int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= m) return;
@@ -151,7 +165,7 @@ __global__ void morton_keys_kernel(int64_t m, const SegGeo *geo, const unsigned 
     }
     double inv = ext > 0.0 ? __ddiv_rn(2097152.0, ext) : 0.0;
     double v[3];
-    midpoint(geo[s], v[0], v[1], v[2]);
+    midpoint_raw(src, s, v[0], v[1], v[2]);
     uint32_t q[3];
     for (int a = 0; a < 3; ++a) {
         uint32_t u = __double2uint_rz(__dmul_rn(__dsub_rn(v[a], lo[a]), inv));
@@ -267,8 +281,9 @@ static inline unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n
 
 // Traversal tree from stably sorted keys (t->order32 holds the sorted segment ids): Karras's binary radix tree, then
 // the big internal nodes and their small children numbered by an exclusive scan.
-static int topology_from_sorted(bs_tree *t, const uint64_t *keys, int wake_shift, Scratch &scratch,
-                                cudaStream_t s) {
+// `while_counting` (may be empty) runs on the host while the node count is on its way back.
+static int topology_from_sorted(bs_tree *t, const uint64_t *keys, int wake_shift, Scratch &scratch, cudaStream_t s,
+                                const std::function<int()> &while_counting = {}) {
     const int64_t m = t->m;
     if ((m <= t->leaf_size && wake_shift == 0) || m == 1) {
         t->count = 1;
@@ -293,6 +308,10 @@ static int topology_from_sorted(bs_tree *t, const uint64_t *keys, int wake_shift
     if (rc != BS_OK) return rc;
     int64_t count = 0;
     BS_CUDA(cudaMemcpyAsync(&count, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    if (while_counting) {
+        rc = while_counting();
+        if (rc != BS_OK) return rc;
+    }
     BS_CUDA(cudaStreamSynchronize(s));
     t->count = count;
     t->lo = t->alloc<int64_t>(count, s);
@@ -306,7 +325,8 @@ static int topology_from_sorted(bs_tree *t, const uint64_t *keys, int wake_shift
     return BS_OK;
 }
 
-static int build_morton(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_t s) {
+static int build_morton(bs_tree *t, const bs_sources *src, Scratch &scratch, cudaStream_t s,
+                        const std::function<int()> &while_counting) {
     const int64_t m = t->m;
     unsigned long long *box = scratch.get<unsigned long long>(6);
     uint64_t *keys = scratch.get<uint64_t>(m);
@@ -314,13 +334,13 @@ static int build_morton(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStr
     t->order32 = t->alloc<int32_t>(m, s);
     if (!box || !keys || !t->keys || !t->order32) return scratch.status != BS_OK ? scratch.status : BS_ERR_OOM;
     box_init_kernel<<<1, 32, 0, s>>>(box);
-    mid_box_kernel<<<std::min<unsigned>(blocks_for(m, 256), 1184), 256, 0, s>>>(m, geo, box);
-    morton_keys_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, geo, box, keys, t->order32);
+    mid_box_kernel<<<std::min<unsigned>(blocks_for(m, 256), 1184), 256, 0, s>>>(m, *src, box);
+    morton_keys_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, *src, box, keys, t->order32);
     BS_CHECK_LAUNCH("morton keys");
     BS_CUDA(cudaMemcpyAsync(t->keys, keys, m * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
     int rc = radix_sort(keys, t->order32, m, 0, 63, scratch, s);
     if (rc != BS_OK) return rc;
-    return topology_from_sorted(t, keys, 0, scratch, s);
+    return topology_from_sorted(t, keys, 0, scratch, s, while_counting);
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -1615,7 +1635,7 @@ extern "C" int64_t bs_tree_count(const bs_tree *tree) { return tree ? tree->coun
 // (wait = false: the evaluation is queued behind the build on the same stream, and tree_stage_times reads the times
 // once the caller has synchronised).
 int tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_tree **out, cudaStream_t s,
-               bool wait) {
+               bool wait, const std::function<int()> &before_geometry) {
     if (!ctx || !tp || !out) {
         set_error("bs_tree_build: null argument");
         return BS_ERR_ARG;
@@ -1647,9 +1667,25 @@ int tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_
     t->order4 = tp->order >= 4;
     {
         Scratch scratch(ctx->pool, s);
+        // before_geometry (may be empty) runs once, before anything reads gamma or radius: for Morton trees while the
+        // node count travels back (keys and topology need only starts, directions and lengths)
+        bool ran = false;
+        auto gate = [&]() -> int {
+            if (ran || !before_geometry) return BS_OK;
+            ran = true;
+            return before_geometry();
+        };
         SegGeo *geo = scratch.get<SegGeo>(src->m);
-        rc = geo ? pack_segments(src, nullptr, nullptr, nullptr, geo, s) : scratch.status;
-        if (rc == BS_OK) rc = tp->kind == BS_TREE_MORTON ? build_morton(t, geo, scratch, s) : build_median(t, geo, scratch, s);
+        rc = geo ? BS_OK : scratch.status;
+        if (rc == BS_OK && tp->kind == BS_TREE_MORTON) {
+            rc = build_morton(t, src, scratch, s, gate);
+            if (rc == BS_OK) rc = gate();
+            if (rc == BS_OK) rc = pack_segments(src, nullptr, nullptr, nullptr, geo, s);
+        } else if (rc == BS_OK) {
+            rc = gate();
+            if (rc == BS_OK) rc = pack_segments(src, nullptr, nullptr, nullptr, geo, s);
+            if (rc == BS_OK) rc = build_median(t, geo, scratch, s);
+        }
         if (rc == BS_OK) {
             cudaEventRecord(e1, s);
             rc = finish_tree(t, src, geo, scratch, s);
@@ -1690,7 +1726,7 @@ void tree_release(bs_tree *tree, cudaStream_t s) {
 
 extern "C" int bs_tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_tree **out,
                              bs_stream stream) {
-    return tree_build(ctx, src, tp, out, (cudaStream_t)stream, true);
+    return tree_build(ctx, src, tp, out, (cudaStream_t)stream, true, {});
 }
 
 extern "C" int bs_forest_build(bs_ctx *ctx, const bs_sources *src, int nwakes, const int64_t *wake_ptr,

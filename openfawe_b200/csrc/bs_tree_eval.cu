@@ -10,6 +10,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
+#include <thread>
 
 #include "bs_sort.cuh"
 #include <cstdlib>
@@ -1006,6 +1008,108 @@ extern "C" int bs_forest_eval(bs_ctx *ctx, const bs_tree *forest, const bs_tree_
                     (cudaStream_t)stream);
 }
 
+extern "C" int bs_tree_sum_host(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, const bs_targets *tgt,
+                                const bs_kernel_params *kp, double *out, int8_t *flags, int64_t *far_counts,
+                                bs_stream stream) {
+    if (!ctx || !src || !tp || !tgt || !kp) {
+        set_error("bs_tree_sum_host: null argument");
+        return BS_ERR_ARG;
+    }
+    const int64_t n = tgt->n, m = src->m, e = (tgt->ex_ptr && tgt->ex_seg) ? tgt->e : 0;
+    if (n < 0 || m < 0 || e < 0 || (n > 0 && (!tgt->points || !out || !flags)) ||
+        (m > 0 && (!src->starts || !src->directions || !src->lengths || !src->gamma || !src->radius))) {
+        set_error("bs_tree_sum_host: invalid arrays");
+        return BS_ERR_ARG;
+    }
+    if (n == 0) return BS_OK;
+    BS_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    using clock = std::chrono::steady_clock;
+    const auto t0 = clock::now();
+    int rc = BS_OK;
+    {
+        Scratch scratch(ctx->pool, s);
+        double *d_points = scratch.get<double>(3 * n), *d_out = scratch.get<double>(3 * n);
+        int8_t *d_flags = scratch.get<int8_t>(n);
+        int64_t *d_far = far_counts ? scratch.get<int64_t>(n) : nullptr;
+        int64_t *d_ex_ptr = e > 0 ? scratch.get<int64_t>(n + 1) : nullptr;
+        int64_t *d_ex_seg = e > 0 ? scratch.get<int64_t>(e) : nullptr;
+        double *d_seg = m > 0 ? scratch.get<double>((size_t)9 * m) : nullptr;  // starts, directions, L, gamma, rc
+        if (!d_points || !d_out || !d_flags || (far_counts && !d_far) || (e > 0 && (!d_ex_ptr || !d_ex_seg)) ||
+            (m > 0 && !d_seg))
+            return scratch.status;
+        bs_sources dsrc{m, d_seg, d_seg + 3 * m, d_seg + 6 * m, d_seg + 7 * m, d_seg + 8 * m};
+        bs_targets dtgt{n, d_points, d_ex_ptr, d_ex_seg, e};
+        // 1. targets, exclusions and what the keys and topology need, in one pass of the staging ring
+        {
+            void *dst[6] = {d_points, d_ex_ptr, d_ex_seg, (void *)dsrc.starts, (void *)dsrc.directions,
+                            (void *)dsrc.lengths};
+            const void *from[6] = {tgt->points, tgt->ex_ptr, tgt->ex_seg, src->starts, src->directions, src->lengths};
+            size_t bytes[6] = {(size_t)3 * n * sizeof(double), e > 0 ? (size_t)(n + 1) * sizeof(int64_t) : 0,
+                               (size_t)e * sizeof(int64_t), (size_t)3 * m * sizeof(double),
+                               (size_t)3 * m * sizeof(double), (size_t)m * sizeof(double)};
+            rc = bs_upload_many(ctx, 6, dst, from, bytes, stream);
+            if (rc != BS_OK) return rc;
+        }
+        double upload_ms = 0.0;
+        if (m == 0) {
+            BS_CUDA(cudaMemsetAsync(d_out, 0, 3 * n * sizeof(double), s));
+            BS_CUDA(cudaMemsetAsync(d_flags, 0, n, s));
+            if (d_far) BS_CUDA(cudaMemsetAsync(d_far, 0, n * sizeof(int64_t), s));
+            upload_ms = std::chrono::duration<double, std::milli>(clock::now() - t0).count();
+        } else {
+            // 2. circulations and core radii: staged by the context's staging thread on the copy stream right away
+            // (the ring keeps running) while this thread queues the key sort and topology, which need neither
+            if (!ctx->copy_stream) BS_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+            cudaEvent_t landed;
+            BS_CUDA(cudaEventCreateWithFlags(&landed, cudaEventDisableTiming));
+            {
+                void *dst[2] = {(void *)dsrc.gamma, (void *)dsrc.radius};
+                const void *from[2] = {src->gamma, src->radius};
+                size_t bytes[2] = {(size_t)m * sizeof(double), (size_t)m * sizeof(double)};
+                rc = bs_stage_async(ctx, 2, dst, from, bytes, ctx->copy_stream);
+                if (rc != BS_OK) {
+                    cudaEventDestroy(landed);
+                    return rc;
+                }
+            }
+            bool joined = false;
+            auto rest = [&]() -> int {  // before any kernel reads gamma or radius
+                const int staged = bs_stage_wait(ctx);
+                joined = true;
+                upload_ms = std::chrono::duration<double, std::milli>(clock::now() - t0).count();
+                if (staged != BS_OK) return staged;
+                BS_CUDA(cudaEventRecord(landed, ctx->copy_stream));
+                BS_CUDA(cudaStreamWaitEvent(s, landed, 0));
+                return BS_OK;
+            };
+            bs_tree *tree = nullptr;
+            rc = tree_build(ctx, &dsrc, tp, &tree, s, false, rest);
+            if (rc == BS_OK) rc = check_eval_args(ctx, tree, tp, &dtgt, kp, d_out, d_flags);
+            if (rc == BS_OK) rc = eval_run(ctx, tree, tp, &dtgt, nullptr, 1, kp, d_out, d_flags, d_far, s);
+            if (tree) {
+                if (rc == BS_OK) tree_stage_times(tree);
+                ctx->stats.build_ms = tree->build_ms;
+                ctx->stats.moments_ms = tree->moments_ms;
+                tree_release(tree, s);
+            }
+            if (!joined) bs_stage_wait(ctx);
+            cudaStreamSynchronize(ctx->copy_stream);  // the staging of the rest has finished on any return
+            cudaEventDestroy(landed);
+            if (rc != BS_OK) return rc;
+        }
+        // 3. results through the ring
+        const auto t1 = clock::now();
+        void *dst[3] = {out, flags, far_counts};
+        const void *from[3] = {d_out, d_flags, d_far};
+        size_t bytes[3] = {(size_t)3 * n * sizeof(double), (size_t)n, far_counts ? (size_t)n * sizeof(int64_t) : 0};
+        rc = bs_download_many(ctx, 3, dst, from, bytes, stream);
+        ctx->stats.upload_ms = upload_ms;
+        ctx->stats.download_ms = std::chrono::duration<double, std::milli>(clock::now() - t1).count();
+    }
+    return rc;
+}
+
 struct bs_graph {
     int device;
     cudaGraphExec_t exec = nullptr;
@@ -1137,7 +1241,7 @@ extern "C" int bs_tree_sum(bs_ctx *ctx, const bs_sources *src, const bs_tree_par
     // order after the evaluation (which synchronises before it returns)
     cudaStream_t s = (cudaStream_t)stream;
     bs_tree *tree = nullptr;
-    int rc = tree_build(ctx, src, tp, &tree, s, false);
+    int rc = tree_build(ctx, src, tp, &tree, s, false, {});
     if (rc != BS_OK) return rc;
     rc = bs_tree_eval(ctx, tree, tp, tgt, kp, out, flags, far_counts, stream);
     if (rc == BS_OK) tree_stage_times(tree);

@@ -7,9 +7,13 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <condition_variable>
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <mutex>
+#include <thread>
+#include <vector>
 
 #include "bs_internal.cuh"
 
@@ -19,6 +23,13 @@ struct bs_upload_ring {
     void *buf[SLOTS] = {};
     cudaEvent_t done[SLOTS] = {};
     std::mutex lock;
+    // a persistent host thread for uploads that overlap the caller's own work (its OpenMP team stays alive)
+    std::thread worker;
+    std::mutex wm;
+    std::condition_variable wcv;
+    std::function<int()> job;
+    bool pending = false, quit = false;
+    int result = BS_OK;
 };
 
 static int ring_of(bs_ctx *ctx, bs_upload_ring **out) {
@@ -46,6 +57,14 @@ static int ring_of(bs_ctx *ctx, bs_upload_ring **out) {
 
 void bs_upload_release(bs_ctx *ctx) {
     if (!ctx || !ctx->upload) return;
+    if (ctx->upload->worker.joinable()) {
+        {
+            std::lock_guard<std::mutex> g(ctx->upload->wm);
+            ctx->upload->quit = true;
+        }
+        ctx->upload->wcv.notify_all();
+        ctx->upload->worker.join();
+    }
     for (int i = 0; i < bs_upload_ring::SLOTS; ++i) {
         cudaEventSynchronize(ctx->upload->done[i]);
         cudaEventDestroy(ctx->upload->done[i]);
@@ -205,5 +224,52 @@ extern "C" int bs_download_many(bs_ctx *ctx, int count, void *const *dst, const 
         if (rc != BS_OK) return rc;
     }
     return BS_OK;
+}
+
+// The staging thread: runs one submitted upload at a time.
+static void stage_worker(bs_upload_ring *r) {
+    for (;;) {
+        std::function<int()> job;
+        {
+            std::unique_lock<std::mutex> g(r->wm);
+            r->wcv.wait(g, [&] { return r->quit || (r->pending && r->job); });
+            if (r->quit) return;
+            job = std::move(r->job);
+            r->job = nullptr;
+        }
+        const int rc = job();
+        {
+            std::lock_guard<std::mutex> g(r->wm);
+            r->result = rc;
+            r->pending = false;
+        }
+        r->wcv.notify_all();
+    }
+}
+
+int bs_stage_async(bs_ctx *ctx, int count, void *const *dst, const void *const *src, const size_t *bytes,
+                   cudaStream_t s) {
+    bs_upload_ring *r = nullptr;
+    int rc = ring_of(ctx, &r);
+    if (rc != BS_OK) return rc;
+    std::vector<void *> d(dst, dst + count);
+    std::vector<const void *> f(src, src + count);
+    std::vector<size_t> b(bytes, bytes + count);
+    std::unique_lock<std::mutex> g(r->wm);
+    r->wcv.wait(g, [&] { return !r->pending; });
+    if (!r->worker.joinable()) r->worker = std::thread(stage_worker, r);
+    r->job = [ctx, d, f, b, s]() { return upload_list(ctx, (int)d.size(), d.data(), f.data(), b.data(), s); };
+    r->pending = true;
+    g.unlock();
+    r->wcv.notify_all();
+    return BS_OK;
+}
+
+int bs_stage_wait(bs_ctx *ctx) {
+    bs_upload_ring *r = ctx->upload;
+    if (!r) return BS_OK;
+    std::unique_lock<std::mutex> g(r->wm);
+    r->wcv.wait(g, [&] { return !r->pending; });
+    return r->result;
 }
 

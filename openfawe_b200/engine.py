@@ -261,6 +261,36 @@ def tree_sum(sources, targets, model, singularity="raise", precision="mixed", bl
     return out, flags, far
 
 
+def tree_sum_host(points, starts, directions, lengths, gamma, radius, csr, model, singularity="raise",
+                  precision="mixed", block=128, near=3.0, theta=0.5, order=2, leaf_size=32, clearance=3.0,
+                  kind="median", stack_limit=0, device=None, far_counts=True):
+    """tree_sum from and to host NumPy arrays in one library call (bs_tree_sum_host): returns (velocity [n,3] float64,
+    flags [n] int8, far counts [n] int64 or None) as NumPy arrays.  csr = (ptr [n+1], seg [e]) or None."""
+    dev = _device_of(device)
+    c = lambda a, dt: np.ascontiguousarray(a, dtype=dt)  # noqa: E731
+    points = c(points, np.float64).reshape(-1, 3)
+    starts, directions = c(starts, np.float64).reshape(-1, 3), c(directions, np.float64).reshape(-1, 3)
+    m = len(starts)
+    lengths, gamma = c(lengths, np.float64).reshape(-1), c(gamma, np.float64).reshape(-1)
+    radius = c(np.broadcast_to(np.asarray(radius, dtype=np.float64), (m,)), np.float64)
+    n = len(points)
+    ptr = seg = None
+    if csr is not None and len(csr[1]):
+        ptr, seg = c(csr[0], np.int64), c(csr[1], np.int64)
+    out = np.empty((n, 3), dtype=np.float64)
+    flags = np.empty(n, dtype=np.int8)
+    far = np.empty(n, dtype=np.int64) if far_counts else None
+    addr = lambda a: ctypes.c_void_p(a.ctypes.data if a is not None and a.size else 0)  # noqa: E731
+    src = L.Sources(m, addr(starts), addr(directions), addr(lengths), addr(gamma), addr(radius))
+    tgt = L.Targets(n, addr(points), addr(ptr), addr(seg), 0 if seg is None else len(seg))
+    tp = tree_params(theta, order, leaf_size, clearance, kind, stack_limit)
+    kp = kernel_params(model, singularity, precision, block, near)
+    L.check(L.library().bs_tree_sum_host(L.context(dev.index), ctypes.byref(src), ctypes.byref(tp),
+                                         ctypes.byref(tgt), ctypes.byref(kp), addr(out), addr(flags), addr(far),
+                                         _stream(dev)), "bs_tree_sum_host")
+    return out, flags, far
+
+
 def last_stats(device=0):
     """Counters and device times of the last call on `device` (bs_last_stats)."""
     return L.stats(device)

@@ -71,27 +71,39 @@ def cuda_tree_sum(points, starts, directions, lengths, gamma, radius, model, csr
     import torch
     from . import _lib, engine
     device = torch.cuda.current_device()
-    tick = time.perf_counter()
-    sources = engine.Sources(starts, directions, lengths, gamma, radius, device)
-    targets = engine.Targets(points, csr, device)
-    upload_s = time.perf_counter() - tick  # host side: the last transfers overlap the build's first launches
     limit = int(stack_size) if 0 < int(stack_size) < DEVICE_STACK else 0
-    tick = time.perf_counter()
     try:
-        # build, moments and evaluation in one library call: the evaluation queues behind the build
-        d_out, d_flags, d_far = engine.tree_sum(sources, targets, int(model), singularity, precision, block, near,
-                                                tree.theta, expansion, tree.leaf_size, tree.core_clearance, kind,
-                                                stack_limit=limit)
+        if any(isinstance(x, torch.Tensor) for x in (starts, directions, lengths, gamma, radius)):
+            # device-resident inputs: build, moments and evaluation in one library call, then the three results
+            tick = time.perf_counter()
+            sources = engine.Sources(starts, directions, lengths, gamma, radius, device)
+            targets = engine.Targets(points, csr, device)
+            upload_s = time.perf_counter() - tick
+            tick = time.perf_counter()
+            d_out, d_flags, d_far = engine.tree_sum(sources, targets, int(model), singularity, precision, block,
+                                                    near, tree.theta, expansion, tree.leaf_size, tree.core_clearance,
+                                                    kind, stack_limit=limit)
+            total_s = time.perf_counter() - tick
+            tick = time.perf_counter()
+            out, flags, far = engine.to_host_many((d_out, d_flags, d_far), ((n, 3), (n,), (n,)),
+                                                  (np.float64, np.int8, np.int64))
+            download_s = time.perf_counter() - tick
+            stats = engine.last_stats(device)
+        else:
+            # host arrays: one library call from the host arrays to the host results (uploads overlap the build)
+            tick = time.perf_counter()
+            out, flags, far = engine.tree_sum_host(points, starts, directions, lengths, gamma, radius, csr,
+                                                   int(model), singularity, precision, block, near, tree.theta,
+                                                   expansion, tree.leaf_size, tree.core_clearance, kind, limit,
+                                                   device)
+            stats = engine.last_stats(device)
+            upload_s, download_s = 1e-3 * stats["upload_ms"], 1e-3 * stats["download_ms"]
+            total_s = time.perf_counter() - tick - upload_s - download_s
     except _lib.StackOverflow as error:
         raise RuntimeError(f"tree traversal stack overflow on the GPU (depth {min(int(stack_size), DEVICE_STACK)})") \
             from error
-    stats = engine.last_stats(device)
     build_s = 1e-3 * (stats["build_ms"] + stats["moments_ms"])
-    evaluate_s = max(0.0, time.perf_counter() - tick - build_s)
-    tick = time.perf_counter()
-    out, flags, far = engine.to_host_many((d_out, d_flags, d_far), ((n, 3), (n,), (n,)),
-                                          (np.float64, np.int8, np.int64))
-    download_s = time.perf_counter() - tick
+    evaluate_s = max(0.0, total_s - build_s)
     Statistics.last = dict(points=n, segments=m, nodes=int(stats["nodes"]), precision=precision, launches=1,
                            targets_per_launch=n, longest_launch_s=stats["evaluate_ms"] * 1e-3, suspect=0,
                            mean_far_nodes=float(far.mean()), build_s=build_s, moments_s=0.0, upload_s=upload_s,
