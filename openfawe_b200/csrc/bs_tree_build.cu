@@ -362,17 +362,32 @@ __global__ void forest_box_init_kernel(int nw, unsigned long long *box) {
     if (i < 6 * nw) box[i] = (i % 6) < 3 ? ordered_bits(INFINITY) : ordered_bits(-INFINITY);
 }
 
-__global__ void forest_box_kernel(int64_t m, const SegGeo *geo, const int64_t *wake_ptr, int nw,
-                                  unsigned long long *box) {
-    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= m) return;
-    const int w = wake_of(wake_ptr, nw, s);
-    double v[3];
-    midpoint(geo[s], v[0], v[1], v[2]);
-    for (int a = 0; a < 3; ++a) {
-        atomicMin(&box[6 * w + a], ordered_bits(v[a]));
-        atomicMax(&box[6 * w + 3 + a], ordered_bits(v[a]));
+// Each wake's midpoint box: blockIdx.x is the wake, the blocks along y stride over its segment range; a block folds
+// its part in shared memory and adds six atomics (per-segment atomics on a few hundred words serialise).
+__global__ void forest_box_kernel(const SegGeo *geo, const int64_t *wake_ptr, unsigned long long *box) {
+    __shared__ unsigned long long sb[6];
+    const int w = blockIdx.x;
+    if (threadIdx.x < 6) sb[threadIdx.x] = threadIdx.x < 3 ? ordered_bits(INFINITY) : ordered_bits(-INFINITY);
+    __syncthreads();
+    const int64_t a = wake_ptr[w], b = wake_ptr[w + 1];
+    unsigned long long lo[3] = {ordered_bits(INFINITY), ordered_bits(INFINITY), ordered_bits(INFINITY)};
+    unsigned long long hi[3] = {ordered_bits(-INFINITY), ordered_bits(-INFINITY), ordered_bits(-INFINITY)};
+    for (int64_t s = a + (int64_t)blockIdx.y * blockDim.x + threadIdx.x; s < b; s += (int64_t)gridDim.y * blockDim.x) {
+        double v[3];
+        midpoint(geo[s], v[0], v[1], v[2]);
+        for (int x = 0; x < 3; ++x) {
+            const unsigned long long o = ordered_bits(v[x]);
+            lo[x] = o < lo[x] ? o : lo[x];
+            hi[x] = o > hi[x] ? o : hi[x];
+        }
     }
+    for (int x = 0; x < 3; ++x) {
+        atomicMin(&sb[x], lo[x]);
+        atomicMax(&sb[3 + x], hi[x]);
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) atomicMin(&box[6 * w + threadIdx.x], sb[threadIdx.x]);
+    else if (threadIdx.x < 6) atomicMax(&box[6 * w + threadIdx.x], sb[threadIdx.x]);
 }
 
 __device__ __forceinline__ uint64_t spread_bits(uint32_t v, int bits) {
@@ -429,7 +444,7 @@ static int build_forest(bs_tree *t, const SegGeo *geo, const int64_t *wake_ptr, 
         return scratch.status != BS_OK ? scratch.status : BS_ERR_OOM;
     t->nwakes = nw;
     forest_box_init_kernel<<<blocks_for(6 * (int64_t)nw, 256), 256, 0, s>>>(nw, box);
-    forest_box_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, geo, wake_ptr, nw, box);
+    forest_box_kernel<<<dim3((unsigned)nw, 16), 256, 0, s>>>(geo, wake_ptr, box);
     forest_keys_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, geo, wake_ptr, nw, box, bits, keys, t->order32);
     BS_CHECK_LAUNCH("forest keys");
     BS_CUDA(cudaMemcpyAsync(t->keys, keys, m * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));

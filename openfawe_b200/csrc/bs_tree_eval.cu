@@ -756,15 +756,30 @@ __device__ __forceinline__ unsigned long long ordered64(double x) {
     return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
 }
 
-__global__ void forest_target_box_kernel(int64_t n, const double *points, const int64_t *ptr, int nw,
-                                         unsigned long long *box) {
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    const int w = target_wake(ptr, nw, p);
-    for (int a = 0; a < 3; ++a) {
-        atomicMin(&box[6 * w + a], ordered64(points[3 * p + a]));
-        atomicMax(&box[6 * w + 3 + a], ordered64(points[3 * p + a]));
+// Each wake's target box: blockIdx.x is the wake, the blocks along y stride over its targets; a block folds its part
+// in shared memory and adds six atomics.
+__global__ void forest_target_box_kernel(const double *points, const int64_t *ptr, unsigned long long *box) {
+    __shared__ unsigned long long sb[6];
+    const int w = blockIdx.x;
+    if (threadIdx.x < 6) sb[threadIdx.x] = threadIdx.x < 3 ? ordered64(INFINITY) : ordered64(-INFINITY);
+    __syncthreads();
+    unsigned long long lo[3] = {ordered64(INFINITY), ordered64(INFINITY), ordered64(INFINITY)};
+    unsigned long long hi[3] = {ordered64(-INFINITY), ordered64(-INFINITY), ordered64(-INFINITY)};
+    for (int64_t p = ptr[w] + (int64_t)blockIdx.y * blockDim.x + threadIdx.x; p < ptr[w + 1];
+         p += (int64_t)gridDim.y * blockDim.x) {
+        for (int a = 0; a < 3; ++a) {
+            const unsigned long long o = ordered64(points[3 * p + a]);
+            lo[a] = o < lo[a] ? o : lo[a];
+            hi[a] = o > hi[a] ? o : hi[a];
+        }
     }
+    for (int a = 0; a < 3; ++a) {
+        atomicMin(&sb[a], lo[a]);
+        atomicMax(&sb[3 + a], hi[a]);
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) atomicMin(&box[6 * w + threadIdx.x], sb[threadIdx.x]);
+    else if (threadIdx.x < 6) atomicMax(&box[6 * w + threadIdx.x], sb[threadIdx.x]);
 }
 
 __global__ void forest_target_box_init_kernel(int nw, unsigned long long *box) {
@@ -851,7 +866,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
         root_of = scratch.get<int32_t>(n);
         if (!box || !keys || !root_of) return scratch.status;
         forest_target_box_init_kernel<<<nblocks(6 * (int64_t)nw, 256), 256, 0, s>>>(nw, box);
-        forest_target_box_kernel<<<nblocks(n, 256), 256, 0, s>>>(n, tgt->points, target_wake_ptr, nw, box);
+        forest_target_box_kernel<<<dim3((unsigned)nw, 4), 256, 0, s>>>(tgt->points, target_wake_ptr, box);
         forest_target_keys_kernel<<<nblocks(n, 256), 256, 0, s>>>(n, tgt->points, target_wake_ptr, nw, box, bits,
                                                                   keys, perm);
         BS_CHECK_LAUNCH("forest target keys");
