@@ -13,8 +13,9 @@ struct __align__(16) SegGeo {
     double lx, ly, lz, gamma, radius, pad;
 };
 
+// pairs (may be null): also the packed-pair records (Seg32x2) of the same order.
 int pack_segments(const bs_sources *src, const int32_t *order, Seg64 *seg64, Seg32 *seg32, SegGeo *geo,
-                  cudaStream_t s);
+                  cudaStream_t s, Seg32x2 *pairs = nullptr);
 int compute_moments(bs_tree *tree, const SegGeo *geo, Scratch &scratch, cudaStream_t s);
 
 }  // namespace bs

@@ -42,7 +42,7 @@ __device__ __forceinline__ double from_ordered(uint64_t k) {
 // ---------------------------------------------------------------------------------------------------------------------
 __global__ void pack_kernel(int64_t m, const double *starts, const double *directions, const double *lengths,
                             const double *gamma, const double *radius, const int32_t *order, Seg64 *seg64,
-                            Seg32 *seg32, SegGeo *geo) {
+                            Seg32 *seg32, SegGeo *geo, Seg32x2 *pairs) {
     int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= m) return;
     int64_t s = order ? order[k] : k;
@@ -74,6 +74,18 @@ __global__ void pack_kernel(int64_t m, const double *starts, const double *direc
         q.lo.w = (float)((g / L) / 12.566370614359172);
         q.dir = make_float4((float)dx, (float)dy, (float)dz, (r > 0.0 && !tiny) ? (float)(1.0 / (rcl * rcl)) : 0.0f);
         seg32[k] = q;
+        if (pairs) {  // the packed-pair record (Seg32x2): this segment's half of pair k / 2
+            float v[16];
+            const bool ok = !tiny && fabsf(q.hi.x) < 1e30f && fabsf(q.hi.y) < 1e30f && fabsf(q.hi.z) < 1e30f;
+            v[0] = ok ? -q.hi.x : 0.f; v[1] = ok ? -q.hi.y : 0.f; v[2] = ok ? -q.hi.z : 0.f; v[3] = ok ? q.hi.w : 0.f;
+            v[4] = ok ? -q.lo.x : 0.f; v[5] = ok ? -q.lo.y : 0.f; v[6] = ok ? -q.lo.z : 0.f; v[7] = q.lo.w;
+            v[8] = q.dir.x; v[9] = q.dir.y; v[10] = q.dir.z; v[11] = q.dir.w;
+            v[12] = -q.dir.x; v[13] = -q.dir.y; v[14] = -q.dir.z; v[15] = 0.f;
+            float *half = reinterpret_cast<float *>(pairs + (k >> 1)) + (k & 1);
+            for (int f = 0; f < 16; ++f) half[2 * f] = v[f];
+            if ((m & 1) && k == m - 1)  // the padding half of an odd count's last pair
+                for (int f = 0; f < 16; ++f) half[2 * f + 1] = 0.f;
+        }
     }
     if (geo) {
         SegGeo q;
@@ -89,10 +101,11 @@ __global__ void pack_kernel(int64_t m, const double *starts, const double *direc
 }
 
 int pack_segments(const bs_sources *src, const int32_t *order, Seg64 *seg64, Seg32 *seg32, SegGeo *geo,
-                  cudaStream_t s) {
+                  cudaStream_t s, Seg32x2 *pairs) {
     if (src->m == 0) return BS_OK;
     pack_kernel<<<(unsigned)((src->m + 255) / 256), 256, 0, s>>>(src->m, src->starts, src->directions, src->lengths,
-                                                                 src->gamma, src->radius, order, seg64, seg32, geo);
+                                                                 src->gamma, src->radius, order, seg64, seg32, geo,
+                                                                 pairs);
     BS_CHECK_LAUNCH("pack_kernel");
     return BS_OK;
 }
@@ -1082,13 +1095,15 @@ __global__ void sorted_ends_kernel(int64_t m, const int32_t *order, const SegGeo
     ends[k] = EndPts{g.sx, g.sy, g.sz, g.ex, g.ey, g.ez};
 }
 
-__global__ void parent_kernel(int64_t count, const int64_t *left, const int64_t *right, int32_t *parent) {
+// up[child] = (parent, the other child), the other child stored as -(it + 1) when `child` is the right one, so that a
+// climbing warp knows both children and their order from one load; up[0].x = -1.
+__global__ void parent_kernel(int64_t count, const int64_t *left, const int64_t *right, int2 *up) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= count) return;
-    if (j == 0) parent[0] = -1;
+    if (j == 0) up[0] = make_int2(-1, 0);
     if (left[j] >= 0) {
-        parent[left[j]] = (int32_t)j;
-        parent[right[j]] = (int32_t)j;
+        up[left[j]] = make_int2((int)j, (int)right[j]);
+        up[right[j]] = make_int2((int)j, -(int)left[j] - 1);
     }
 }
 
@@ -1313,8 +1328,8 @@ __global__ void __launch_bounds__(128) leaf_moments_kernel(int64_t count, const 
 //   m'_(i; a1..an) = sum over subsets S of the positions of prod_(s in S) D_as * m_(i; the positions not in S),
 // D = child centre - node centre, the subset products built up one factor at a time.
 template <int PARTS>
-__global__ void __launch_bounds__(128) bottom_up_kernel(int64_t count, const int64_t *left, const int64_t *right,
-                                                        const int32_t *parent, unsigned *arrive, double *box,
+__global__ void __launch_bounds__(128) bottom_up_kernel(int64_t count, const int64_t *left, const int2 *up,
+                                                        unsigned *arrive, double *box,
                                                         double *centre, double *core, double *sums) {
     using MT = MomentTuples<PARTS>;
     __shared__ double sm[4][2][PARTS];
@@ -1333,7 +1348,8 @@ __global__ void __launch_bounds__(128) bottom_up_kernel(int64_t count, const int
     }
     int64_t node = j;
     for (int depth = 0; depth < 4096; ++depth) {
-        const int32_t p = parent[node];
+        const int2 pu = up[node];
+        const int32_t p = pu.x;
         if (p < 0) return;
         __threadfence();
         __syncwarp();
@@ -1342,7 +1358,7 @@ __global__ void __launch_bounds__(128) bottom_up_kernel(int64_t count, const int
         prior = __shfl_sync(0xffffffffu, prior, 0);
         if (prior == 0) return;
         __threadfence();
-        const int64_t l = left[p], r = right[p];
+        const int64_t l = pu.y >= 0 ? node : -(int64_t)pu.y - 1, r = pu.y >= 0 ? (int64_t)pu.y : node;
         for (int q = lane; q < PARTS; q += 32) {
             sm[w][0][q] = __ldcg(sums + (int64_t)PARTS * l + q);
             sm[w][1][q] = __ldcg(sums + (int64_t)PARTS * r + q);
@@ -1483,7 +1499,7 @@ template <int PARTS>
 static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_t s) {
     const int64_t count = t->count, m = t->m;
     double *box = scratch.get<double>(6 * count), *sums = scratch.get<double>((size_t)PARTS * count);
-    int32_t *parent = scratch.get<int32_t>(count);
+    int2 *parent = scratch.get<int2>(count);
     unsigned *arrive = scratch.get<unsigned>(count);
     EndPts *ends = scratch.get<EndPts>(m);
     int64_t *nitems = scratch.get<int64_t>(count), *first = scratch.get<int64_t>(count);
@@ -1497,8 +1513,8 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
     const unsigned leaf_blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((count + 3) / 4, 148 * 16));
     leaf_moments_kernel<PARTS><<<leaf_blocks, 128, 0, s>>>(count, t->lo, t->hi, t->left, t->order32, geo, box,
                                                             t->centre, t->core, sums);
-    bottom_up_kernel<PARTS><<<blocks_for(count, 4), 128, 0, s>>>(count, t->left, t->right, parent, arrive, box,
-                                                                  t->centre, t->core, sums);
+    bottom_up_kernel<PARTS><<<blocks_for(count, 4), 128, 0, s>>>(count, t->left, parent, arrive, box, t->centre,
+                                                                  t->core, sums);
     internal_item_count_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->lo, t->hi, t->left, nitems);
     BS_CHECK_LAUNCH("bottom-up moments");
     int rc = scan_exclusive(nitems, first, count, total, scratch, s);
@@ -1580,28 +1596,6 @@ int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_
 
 using namespace bs;
 
-// The packed-pair records of the tree-ordered segments (one thread per segment; m rounded up to even, the padding
-// segment all zero).
-__global__ void pair_records_kernel(int64_t m, const Seg32 *seg32, Seg32x2 *pairs) {
-    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= ((m + 1) & ~int64_t(1))) return;
-    float v[16];
-    for (int f = 0; f < 16; ++f) v[f] = 0.0f;
-    if (k < m) {
-        const Seg32 r = seg32[k];
-        const bool ok = r.hi.w > 0.0f && fabsf(r.hi.x) < 1e30f && fabsf(r.hi.y) < 1e30f && fabsf(r.hi.z) < 1e30f;
-        if (ok) {
-            v[0] = -r.hi.x; v[1] = -r.hi.y; v[2] = -r.hi.z; v[3] = r.hi.w;
-            v[4] = -r.lo.x; v[5] = -r.lo.y; v[6] = -r.lo.z;
-        }
-        v[7] = r.lo.w;
-        v[8] = r.dir.x; v[9] = r.dir.y; v[10] = r.dir.z; v[11] = r.dir.w;
-        v[12] = -r.dir.x; v[13] = -r.dir.y; v[14] = -r.dir.z;
-    }
-    float *out = reinterpret_cast<float *>(pairs + (k >> 1)) + (k & 1);
-    for (int f = 0; f < 16; ++f) out[2 * f] = v[f];
-}
-
 // Shared tail of both constructors: inverse permutation, int64 order, tree-ordered segment records, moments.
 static int finish_tree(bs_tree *t, const bs_sources *src, const SegGeo *geo, Scratch &scratch, cudaStream_t s) {
     const int64_t m = t->m;
@@ -1613,10 +1607,8 @@ static int finish_tree(bs_tree *t, const bs_sources *src, const SegGeo *geo, Scr
     if (!t->order || !t->inverse || !t->seg64 || !t->seg32 || !t->seg32x2) return BS_ERR_OOM;
     widen_order_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, t->order32, t->order, t->inverse);
     BS_CHECK_LAUNCH("widen_order_kernel");
-    int rc = pack_segments(src, t->order32, t->seg64, t->seg32, nullptr, s);
+    int rc = pack_segments(src, t->order32, t->seg64, t->seg32, nullptr, s, t->seg32x2);
     if (rc != BS_OK) return rc;
-    pair_records_kernel<<<blocks_for(m + 1, 256), 256, 0, s>>>(m, t->seg32, t->seg32x2);
-    BS_CHECK_LAUNCH("pair_records_kernel");
     return compute_moments(t, geo, scratch, s);
 }
 
