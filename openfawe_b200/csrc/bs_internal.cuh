@@ -534,35 +534,37 @@ __device__ __forceinline__ void far_eval(T rx, T ry, T rz, const T *f, int order
 }
 
 // far_eval<float> reading the packed records (Far32: 12 float4, Far32x: 16 float4, Far32y: 28 float4) in vector
-// loads, one group at a time where it is used, so that only one order's coefficients are live at once.  Same
-// arithmetic as far_eval.
+// loads, one group at a time where it is used, so that only one order's coefficients are live at once.  The terms are
+// those of far_eval written on the unit vector n = R / r: the order-p term is r^-(p+2) times a combination of the
+// order-p coefficients and powers of n (R^k = r^k n^k), summed by Horner's rule in 1/r, so no intermediate carries a
+// power of r beyond the order's own (r^-11 at order 4 would leave FP32's range for distances below ~1e-3.5 or above
+// ~3e3 in the caller's units; here from ~1e-6 to ~1e6 every intermediate stays normal).
 __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const float4 *f, int order, float &ux,
                                             float &uy, float &uz, const float4 *g = nullptr,
                                             const float4 *k4 = nullptr) {
     const float r2 = rx * rx + ry * ry + rz * rz;
-    // 1/r from the hardware estimate and one Newton-Raphson step for x^(-1/2) (y <- y (3 - x y^2) / 2), then the odd
-    // inverse powers by products: no IEEE division or square root on this path
+    // 1/r from the hardware estimate and one Newton-Raphson step for x^(-1/2) (y <- y (3 - x y^2) / 2): no IEEE
+    // division or square root on this path
     float ir = rsqrtf(r2);
     ir = ir * fmaf(-0.5f * r2, ir * ir, 1.5f);
-    const float ir2 = ir * ir;
-    const float inv3 = ir * ir2;
-    const float inv5 = inv3 * ir2;
+    const float nx = rx * ir, ny = ry * ir, nz = rz * ir;
+    // order-p parts v_p (dimensionless in r); u = r^-2 (v0 + r^-1 (v1 + r^-1 (v2 + ...)))
+    float p0[3] = {0.f, 0.f, 0.f}, p1[3] = {0.f, 0.f, 0.f}, p2[3] = {0.f, 0.f, 0.f}, p3[3] = {0.f, 0.f, 0.f},
+          p4[3] = {0.f, 0.f, 0.f};
     const float4 q0 = __ldg(f);  // m0 x y z, m1[0]
-    float u0 = inv3 * (q0.y * rz - q0.z * ry);
-    float u1 = inv3 * (q0.z * rx - q0.x * rz);
-    float u2 = inv3 * (q0.x * ry - q0.y * rx);
+    p0[0] = q0.y * nz - q0.z * ny;
+    p0[1] = q0.z * nx - q0.x * nz;
+    p0[2] = q0.x * ny - q0.y * nx;
     if (order >= 1) {
         const float4 q1 = __ldg(f + 1), q2 = __ldg(f + 2), q3 = __ldg(f + 3);  // m1[1..8], w1, t2[0]
-        const float v0 = q0.w * rx + q1.x * ry + q1.y * rz;
-        const float v1 = q1.z * rx + q1.w * ry + q2.x * rz;
-        const float v2 = q2.y * rx + q2.z * ry + q2.w * rz;
-        const float k = 3.0f * inv5;
-        u0 += k * (v1 * rz - v2 * ry) - inv3 * q3.x;
-        u1 += k * (v2 * rx - v0 * rz) - inv3 * q3.y;
-        u2 += k * (v0 * ry - v1 * rx) - inv3 * q3.z;
+        const float v0 = q0.w * nx + q1.x * ny + q1.y * nz;
+        const float v1 = q1.z * nx + q1.w * ny + q2.x * nz;
+        const float v2 = q2.y * nx + q2.z * ny + q2.w * nz;
+        p1[0] = 3.0f * (v1 * nz - v2 * ny) - q3.x;
+        p1[1] = 3.0f * (v2 * nx - v0 * nz) - q3.y;
+        p1[2] = 3.0f * (v0 * ny - v1 * nx) - q3.z;
         if (order >= 2) {
-            const float inv7 = inv5 * ir2;
-            const float xx = rx * rx, xy = rx * ry, xz = rx * rz, yy = ry * ry, yz = ry * rz, zz = rz * rz;
+            const float xx = nx * nx, xy = nx * ny, xz = nx * nz, yy = ny * ny, yz = ny * nz, zz = nz * nz;
             const float4 q4 = __ldg(f + 4), q5 = __ldg(f + 5), q6 = __ldg(f + 6);  // t2[1..2], w2[0..8], m2 s[0]
             const float4 q7 = __ldg(f + 7), q8 = __ldg(f + 8), q9 = __ldg(f + 9), q10 = __ldg(f + 10),
                          q11 = __ldg(f + 11);  // m2 symmetric s[1..17]
@@ -573,21 +575,19 @@ __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const 
             auto quad = [&](const float *sv) {
                 return sv[0] * xx + sv[3] * yy + sv[5] * zz + 2.0f * (sv[1] * xy + sv[2] * xz + sv[4] * yz);
             };
-            const float a = 7.5f * inv7, b = 1.5f * inv5;
-            const float b0 = a * quad(s0) - b * q3.w;
-            const float b1 = a * quad(s1) - b * q4.x;
-            const float b2 = a * quad(s2) - b * q4.y;
-            const float w0 = q4.z * rx + q4.w * ry + q5.x * rz;
-            const float w1 = q5.y * rx + q5.z * ry + q5.w * rz;
-            const float w2 = q6.x * rx + q6.y * ry + q6.z * rz;
-            u0 += (b1 * rz - b2 * ry) - k * w0;
-            u1 += (b2 * rx - b0 * rz) - k * w1;
-            u2 += (b0 * ry - b1 * rx) - k * w2;
+            const float b0 = 7.5f * quad(s0) - 1.5f * q3.w;
+            const float b1 = 7.5f * quad(s1) - 1.5f * q4.x;
+            const float b2 = 7.5f * quad(s2) - 1.5f * q4.y;
+            const float w0 = q4.z * nx + q4.w * ny + q5.x * nz;
+            const float w1 = q5.y * nx + q5.z * ny + q5.w * nz;
+            const float w2 = q6.x * nx + q6.y * ny + q6.z * nz;
+            p2[0] = (b1 * nz - b2 * ny) - 3.0f * w0;
+            p2[1] = (b2 * nx - b0 * nz) - 3.0f * w1;
+            p2[2] = (b0 * ny - b1 * nx) - 3.0f * w2;
             if (order >= 3) {
-                const float inv9 = inv7 * ir2;
-                const float c000 = xx * rx, c001 = 3.0f * xx * ry, c002 = 3.0f * xx * rz, c011 = 3.0f * xy * ry;
-                const float c012 = 6.0f * xy * rz, c022 = 3.0f * xz * rz, c111 = yy * ry, c112 = 3.0f * yy * rz;
-                const float c122 = 3.0f * yz * rz, c222 = zz * rz;
+                const float c000 = xx * nx, c001 = 3.0f * xx * ny, c002 = 3.0f * xx * nz, c011 = 3.0f * xy * ny;
+                const float c012 = 6.0f * xy * nz, c022 = 3.0f * xz * nz, c111 = yy * ny, c112 = 3.0f * yy * nz;
+                const float c122 = 3.0f * yz * nz, c222 = zz * nz;
                 float x3[3], w[3];
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
@@ -600,18 +600,16 @@ __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const 
                     const float *m = h + H_M3;
                     const float s3 = m[0] * c000 + m[1] * c001 + m[2] * c002 + m[3] * c011 + m[4] * c012 +
                                      m[5] * c022 + m[6] * c111 + m[7] * c112 + m[8] * c122 + m[9] * c222;
-                    const float tr = h[H_T3] * rx + h[H_T3 + 1] * ry + h[H_T3 + 2] * rz;
-                    x3[i] = 17.5f * inv9 * s3 - 7.5f * inv7 * tr;
+                    const float tr = h[H_T3] * nx + h[H_T3 + 1] * ny + h[H_T3 + 2] * nz;
+                    x3[i] = 17.5f * s3 - 7.5f * tr;
                     w[i] = quad(h + H_W3);
                 }
                 const float4 wv = __ldg(g + H_W3V / 4);
-                const float c7 = 7.5f * inv7, c5 = 1.5f * inv5;
-                u0 += (x3[1] * rz - x3[2] * ry) - c7 * w[0] + c5 * wv.x;
-                u1 += (x3[2] * rx - x3[0] * rz) - c7 * w[1] + c5 * wv.y;
-                u2 += (x3[0] * ry - x3[1] * rx) - c7 * w[2] + c5 * wv.z;
+                p3[0] = (x3[1] * nz - x3[2] * ny) - 7.5f * w[0] + 1.5f * wv.x;
+                p3[1] = (x3[2] * nx - x3[0] * nz) - 7.5f * w[1] + 1.5f * wv.y;
+                p3[2] = (x3[0] * ny - x3[1] * nx) - 7.5f * w[2] + 1.5f * wv.z;
                 if (order >= 4) {
-                    // one component row at a time (nine float4), through the shared fourth-order term
-                    const float inv11 = inv9 * ir2;
+                    // one component row at a time (nine float4), through the shared fourth-order term at r = 1
 #pragma unroll
                     for (int i = 0; i < 3; ++i) {
                         float h[K_ROW];
@@ -620,15 +618,20 @@ __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const 
                             const float4 x = __ldg(k4 + (K_ROW / 4) * i + q);
                             h[4 * q] = x.x; h[4 * q + 1] = x.y; h[4 * q + 2] = x.z; h[4 * q + 3] = x.w;
                         }
-                        far_term4_row<float>(rx, ry, rz, inv7, inv9, inv11, h, i, u0, u1, u2);
+                        far_term4_row<float>(nx, ny, nz, 1.0f, 1.0f, 1.0f, h, i, p4[0], p4[1], p4[2]);
                     }
                 }
             }
         }
     }
-    ux += (float)INV_FOUR_PI * u0;
-    uy += (float)INV_FOUR_PI * u1;
-    uz += (float)INV_FOUR_PI * u2;
+    const float scale = (float)INV_FOUR_PI * ir * ir;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float v = p0[c] + ir * (p1[c] + ir * (p2[c] + ir * (p3[c] + ir * p4[c])));
+        if (c == 0) ux += scale * v;
+        else if (c == 1) uy += scale * v;
+        else uz += scale * v;
+    }
 }
 
 // Two-float split of an FP64 value: hi = round(x), lo = round(x - hi).

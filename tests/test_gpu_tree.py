@@ -407,3 +407,27 @@ def test_tree_sum_from_host_arrays_equals_device_call(device):
     u, flags, far = engine.tree_sum_host(np.ones((5, 3)), np.zeros((0, 3)), np.zeros((0, 3)), np.zeros(0),
                                          np.zeros(0), np.zeros(0), None, 2, device=device, kind="morton")
     assert np.all(u == 0) and not flags.any() and not far.any()
+
+
+def test_mixed_tree_far_field_at_any_length_scale(device):
+    """The single-precision far field is formed on the unit vector with one power of 1/r per order, so the same wake
+    at 1e-4, 1 and 1e4 times its size (cores scaled with it) gives the same relative error against the FP64 direct sum
+    at orders 2 and 4 (r^-11 itself would leave FP32's range at both ends)."""
+    from openfawe_b200 import engine, wakes
+    case = wakes.rotor_sheet(40, seed=21, targets=1500)
+    args = wakes.backend_args(case)
+    errs = {}
+    for scale in (1.0, 1e-4, 1e4):
+        pts, st, dr, ln, gm, rc = args[0] * scale, args[1] * scale, args[2], args[3] * scale, args[4], args[5] * scale
+        src = engine.Sources(st, dr, ln, gm, rc, device)
+        tgt = engine.Targets(pts, None, device)
+        direct, _ = engine.direct(src, tgt, 2, "raise", "fp64")
+        direct = direct.cpu().numpy()
+        for order in (2, 4):
+            u, flags, _ = engine.tree_sum(src, tgt, 2, "raise", "mixed", 128, 3.0, 0.3, order, 32, 3.0, "morton")
+            u = u.cpu().numpy()
+            assert np.all(np.isfinite(u)) and not flags.cpu().numpy().any(), (scale, order)
+            errs[scale, order] = np.linalg.norm(u - direct) / np.linalg.norm(direct)
+    for order in (2, 4):
+        for scale in (1e-4, 1e4):
+            assert errs[scale, order] <= 1.1 * errs[1.0, order] + 1e-7, errs
