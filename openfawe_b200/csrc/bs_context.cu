@@ -99,6 +99,7 @@ extern "C" void bs_destroy(bs_ctx *ctx) {
     cudaDeviceSynchronize();
     bs_upload_release(ctx);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+    if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
     cudaMemPoolDestroy(ctx->pool);
     delete ctx;
 }

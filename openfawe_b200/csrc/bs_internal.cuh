@@ -98,6 +98,7 @@ struct bs_ctx {
     bs_stats stats;
     bs_upload_ring *upload = nullptr;
     cudaStream_t copy_stream = nullptr;  // host-array uploads that overlap work on the caller's stream
+    cudaStream_t side_stream = nullptr;  // tree sums: the target sort and the far records, beside the caller's stream
 };
 
 // ---------------------------------------------------------------------------------------------------------------------

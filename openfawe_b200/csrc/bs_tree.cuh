@@ -16,7 +16,8 @@ struct __align__(16) SegGeo {
 // pairs (may be null): also the packed-pair records (Seg32x2) of the same order.
 int pack_segments(const bs_sources *src, const int32_t *order, Seg64 *seg64, Seg32 *seg32, SegGeo *geo,
                   cudaStream_t s, Seg32x2 *pairs = nullptr);
-int compute_moments(bs_tree *tree, const SegGeo *geo, Scratch &scratch, cudaStream_t s);
+// side (may be null): the stream for the moment phase of the bottom-up pipeline (bs_tree::moments_done marks its end).
+int compute_moments(bs_tree *tree, const SegGeo *geo, Scratch &scratch, cudaStream_t s, cudaStream_t side);
 
 }  // namespace bs
 
@@ -45,10 +46,13 @@ struct bs_tree {
     int nwakes = 0;
     float build_ms = 0.f, moments_ms = 0.f;
     cudaEvent_t marks[3] = {nullptr, nullptr, nullptr};  // build start, moments start, moments end
-    void *blocks[32];
+    // marks[2] when the far records are still being computed on a side stream after the build returned (the node
+    // records are complete): work that reads them waits for it; else null
+    cudaEvent_t moments_done = nullptr;
+    void *blocks[48];
     int nblocks = 0;
     template <class T> T *alloc(size_t elems, cudaStream_t s) {
-        if (nblocks >= 32) return nullptr;
+        if (nblocks >= 48) return nullptr;
         void *p = nullptr;
         if (cudaMallocFromPoolAsync(&p, (elems ? elems : 1) * sizeof(T), pool, s) != cudaSuccess) return nullptr;
         blocks[nblocks++] = p;
@@ -59,8 +63,10 @@ struct bs_tree {
 // Build without waiting (bs_tree_sum): the stage times are read by tree_stage_times after the stream synchronised;
 // before_geometry (may be empty) runs on the host once, before any kernel reads gamma or radius (for Morton trees
 // while the node count is read back), so that a caller can still be uploading those two arrays;
-// tree_release frees the tree's memory stream-ordered on s, after the work queued there.
+// tree_release frees the tree's memory stream-ordered on s, after the work queued there.  With a side stream (not
+// waiting), the moments and far records of a bottom-up tree are computed there, concurrently with what s runs after
+// the node records (the walk): bs_tree::moments_done marks their end.
 int tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_tree **out, cudaStream_t s,
-               bool wait, const std::function<int()> &before_geometry);
+               bool wait, const std::function<int()> &before_geometry, cudaStream_t side = nullptr);
 void tree_stage_times(bs_tree *t);
 void tree_release(bs_tree *tree, cudaStream_t s);

@@ -922,6 +922,19 @@ __constant__ signed char c_kl[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {
 __constant__ signed char c_jkl[10][3] = {{0, 0, 0}, {0, 0, 1}, {0, 0, 2}, {0, 1, 1}, {0, 1, 2},
                                          {0, 2, 2}, {1, 1, 1}, {1, 1, 2}, {1, 2, 2}, {2, 2, 2}};
 
+// The traversal record of node j with bounding radius b.
+__device__ __forceinline__ NodeRec node_record(int64_t j, double b, const double *centre, const double *core,
+                                               const int64_t *lo, const int64_t *hi, const int64_t *left,
+                                               const int64_t *right) {
+    NodeRec r;
+    r.cx = centre[3 * j]; r.cy = centre[3 * j + 1]; r.cz = centre[3 * j + 2];
+    r.bound = b;
+    r.clear_core = core[j];
+    r.lo = (int)lo[j]; r.hi = (int)hi[j]; r.left = (int)left[j]; r.right = (int)right[j];
+    r.pad = 0.0;
+    return r;
+}
+
 // The outputs of the moment pipelines for one node.
 struct NodeOut {
     const int64_t *lo, *hi, *left, *right;
@@ -937,8 +950,9 @@ struct NodeOut {
 };
 
 // Node j from its sums v (bound^2, m0, m1, symmetric m2 [, symmetric m3 [, symmetric m4]]) about its centre: the
-// export arrays, the contractions and the packed traversal / far records.
-template <int PARTS>
+// export arrays, the contractions and the packed far records, and with RECORDS the bounding radius and the traversal
+// record (the bottom-up pipeline writes those two earlier, in node_rec_kernel, and leaves v[0] unused).
+template <int PARTS, bool RECORDS = true>
 __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
     double *bound = o.bound, *m0 = o.m0, *m1 = o.m1, *m2 = o.m2, *w1 = o.w1, *t2 = o.t2, *w2 = o.w2;
     Far64 *far64 = o.far64;
@@ -948,8 +962,8 @@ __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
     const double *centre = o.centre, *core = o.core;
     const int64_t *lo = o.lo, *hi = o.hi, *left = o.left, *right = o.right;
     NodeRec *nodes = o.nodes;
-    double b = sqrt(v[0]) * (1.0 + 1e-12);
-    bound[j] = b;
+    const double b = sqrt(v[0]) * (1.0 + 1e-12);
+    if (RECORDS) bound[j] = b;
     const double *M0 = v + 1, *M1 = v + 4, *S = v + 13;  // S[6 i + p], p over (00,01,02,11,12,22)
     auto M2 = [&](int i, int a, int c) -> double {
         int lo_ = a < c ? a : c, hi_ = a < c ? c : a;
@@ -1049,13 +1063,7 @@ __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
             o.far32y[j].v[q] = 0.f;
         }
     }
-    NodeRec r;
-    r.cx = centre[3 * j]; r.cy = centre[3 * j + 1]; r.cz = centre[3 * j + 2];
-    r.bound = b;
-    r.clear_core = core[j];
-    r.lo = (int)lo[j]; r.hi = (int)hi[j]; r.left = (int)left[j]; r.right = (int)right[j];
-    r.pad = 0.0;
-    nodes[j] = r;
+    if (RECORDS) nodes[j] = node_record(j, b, centre, core, lo, hi, left, right);
 }
 
 // Combine a node's chunks in order, then finalize it.
@@ -1231,14 +1239,53 @@ __device__ __forceinline__ void segment_means(const double *d, const double *l, 
     }
 }
 
-// One warp per leaf: box, core and centre, then bound^2 and the moments about the centre; sums[j][PARTS].  The warp
-// takes 32 segments at a time: each lane forms its segment's means (segment_means) and alpha = gamma l into shared
-// memory, then lane u sums, over the 32, alpha_i times the mean of index tuple u (and of u + 32) for i = 0..2.
+// One warp per leaf: box, core and centre from the leaf's segments, then bound^2 (the largest squared distance from
+// the centre to an endpoint, from the tree-ordered endpoints) into bound2 as its bit pattern.
+__global__ void __launch_bounds__(128) leaf_geometry_kernel(int64_t count, const int64_t *lo, const int64_t *hi,
+                                                            const int64_t *left, const int32_t *order,
+                                                            const SegGeo *geo, const EndPts *ends, double *box,
+                                                            double *centre, double *core,
+                                                            unsigned long long *bound2) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t j = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); j < count; j += warps) {
+        if (left[j] >= 0) continue;
+        const int64_t a = lo[j], b = hi[j];
+        double mn[3], mx[3], c;
+        leaf_extent(lane, a, b, order, geo, mn, mx, c);
+        const double c0 = 0.5 * (mn[0] + mx[0]), c1 = 0.5 * (mn[1] + mx[1]), c2 = 0.5 * (mn[2] + mx[2]);
+        double r2 = 0.0;
+        for (int64_t k = a + lane; k < b; k += 32) {
+            const EndPts e = ends[k];
+            const double a0 = e.sx - c0, a1 = e.sy - c1, a2 = e.sz - c2;
+            const double b0 = e.ex - c0, b1 = e.ey - c1, b2 = e.ez - c2;
+            // the reference's ((x^2 + y^2) + z^2) without contraction, as in every bound of this file
+            const double ra = __dadd_rn(__dadd_rn(__dmul_rn(a0, a0), __dmul_rn(a1, a1)), __dmul_rn(a2, a2));
+            const double rb = __dadd_rn(__dadd_rn(__dmul_rn(b0, b0), __dmul_rn(b1, b1)), __dmul_rn(b2, b2));
+            r2 = fmax(r2, fmax(ra, rb));
+        }
+        for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
+        if (lane == 0) {
+            for (int x = 0; x < 3; ++x) {
+                box[6 * j + x] = mn[x];
+                box[6 * j + 3 + x] = mx[x];
+            }
+            centre[3 * j] = c0;
+            centre[3 * j + 1] = c1;
+            centre[3 * j + 2] = c2;
+            core[j] = c;
+            bound2[j] = (unsigned long long)__double_as_longlong(r2);
+        }
+    }
+}
+
+// One warp per leaf: the moments about the leaf's centre; sums[j][PARTS] (sums[j][0] unused).  The warp takes 32
+// segments at a time: each lane forms its segment's means (segment_means) and alpha = gamma l into shared memory,
+// then lane u sums, over the 32, alpha_i times the mean of index tuple u (and of u + 32) for i = 0..2.
 template <int PARTS>
 __global__ void __launch_bounds__(128) leaf_moments_kernel(int64_t count, const int64_t *lo, const int64_t *hi,
                                                            const int64_t *left, const int32_t *order,
-                                                           const SegGeo *geo, double *box, double *centre,
-                                                           double *core, double *sums) {
+                                                           const SegGeo *geo, const double *centre, double *sums) {
     using MT = MomentTuples<PARTS>;
     constexpr int ROWS = MT::n + 3, STRIDE = 33;  // means, then alpha; padded rows: lanes of a column hit other banks
     __shared__ double st[4][ROWS * STRIDE];
@@ -1251,10 +1298,8 @@ __global__ void __launch_bounds__(128) leaf_moments_kernel(int64_t count, const 
     for (int64_t j = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); j < count; j += warps) {
         if (left[j] >= 0) continue;
         const int64_t a = lo[j], b = hi[j];
-        double mn[3], mx[3], c;
-        leaf_extent(lane, a, b, order, geo, mn, mx, c);
-        const double c0 = 0.5 * (mn[0] + mx[0]), c1 = 0.5 * (mn[1] + mx[1]), c2 = 0.5 * (mn[2] + mx[2]);
-        double acc[MT::slots][3], r2 = 0.0;
+        const double c0 = centre[3 * j], c1 = centre[3 * j + 1], c2 = centre[3 * j + 2];
+        double acc[MT::slots][3];
 #pragma unroll
         for (int r = 0; r < MT::slots; ++r) acc[r][0] = acc[r][1] = acc[r][2] = 0.0;
         // the next stage's record is loaded while this stage computes
@@ -1268,12 +1313,6 @@ __global__ void __launch_bounds__(128) leaf_moments_kernel(int64_t count, const 
 #pragma unroll
             for (int q = 0; q < MT::n; ++q) g[q] = 0.0;
             if (k < b) {
-                const double a0 = e.sx - c0, a1 = e.sy - c1, a2 = e.sz - c2;
-                const double b0 = e.ex - c0, b1 = e.ey - c1, b2 = e.ez - c2;
-                // the reference's ((x^2 + y^2) + z^2) without contraction, as in every bound of this file
-                const double ra = __dadd_rn(__dadd_rn(__dmul_rn(a0, a0), __dmul_rn(a1, a1)), __dmul_rn(a2, a2));
-                const double rb = __dadd_rn(__dadd_rn(__dmul_rn(b0, b0), __dmul_rn(b1, b1)), __dmul_rn(b2, b2));
-                r2 = fmax(r2, fmax(ra, rb));
                 if (e.gamma != 0.0) {  // a segment without circulation adds nothing (and no non-finite geometry)
                     const double d[3] = {0.5 * (e.sx + e.ex) - c0, 0.5 * (e.sy + e.ey) - c1, 0.5 * (e.sz + e.ez) - c2};
                     const double l[3] = {e.lx, e.ly, e.lz};
@@ -1301,36 +1340,51 @@ __global__ void __launch_bounds__(128) leaf_moments_kernel(int64_t count, const 
             }
             __syncwarp();
         }
-        for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
         double *out = sums + (int64_t)PARTS * j;
 #pragma unroll
         for (int r = 0; r < MT::slots; ++r)
             if (own[r])
                 for (int i = 0; i < 3; ++i) out[tuple_out(lane + 32 * r, i)] = acc[r][i];
-        if (lane == 0) {
-            out[0] = r2;
-            for (int x = 0; x < 3; ++x) {
-                box[6 * j + x] = mn[x];
-                box[6 * j + 3 + x] = mx[x];
-            }
-            centre[3 * j] = c0;
-            centre[3 * j + 1] = c1;
-            centre[3 * j + 2] = c2;
-            core[j] = c;
-        }
     }
 }
 
-// One warp per leaf climbs towards the root; at each parent the second of the two arriving warps combines the
-// children (their results were published, and fenced by every lane, before the arrival count moved), so every
-// internal node is combined exactly once, from its left then its right child, and no warp waits for another.  Both
+// One thread per leaf climbs towards the root; at each parent the second of the two arriving threads combines the
+// children (their results were published, and fenced, before the arrival count moved), so every internal node is
+// combined exactly once and no thread waits for another: box = the children's union, centre = its midpoint, core =
+// the larger of the two.
+__global__ void box_climb_kernel(int64_t count, const int64_t *left, const int2 *up, unsigned *arrive, double *box,
+                                 double *centre, double *core) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count || left[j] >= 0) return;
+    int64_t node = j;
+    for (int depth = 0; depth < 4096; ++depth) {
+        const int2 pu = up[node];
+        const int32_t p = pu.x;
+        if (p < 0) return;
+        __threadfence();
+        if (atomicAdd(&arrive[p], 1u) == 0) return;
+        __threadfence();
+        const int64_t l = pu.y >= 0 ? node : -(int64_t)pu.y - 1, r = pu.y >= 0 ? (int64_t)pu.y : node;
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            const double lo_x = fmin(__ldcg(box + 6 * l + x), __ldcg(box + 6 * r + x));
+            const double hi_x = fmax(__ldcg(box + 6 * l + 3 + x), __ldcg(box + 6 * r + 3 + x));
+            box[6 * p + x] = lo_x;
+            box[6 * p + 3 + x] = hi_x;
+            centre[3 * p + x] = 0.5 * (lo_x + hi_x);
+        }
+        core[p] = fmax(__ldcg(core + l), __ldcg(core + r));
+        node = p;
+    }
+}
+
+// The moments of the internal nodes, climbing like box_climb_kernel but one warp per leaf (centres known): both
 // children's sums are staged in shared memory; lane u translates index tuple u by the binomial expansion
 //   m'_(i; a1..an) = sum over subsets S of the positions of prod_(s in S) D_as * m_(i; the positions not in S),
-// D = child centre - node centre, the subset products built up one factor at a time.
+// D = child centre - node centre, the subset products built up one factor at a time; left child first, then right.
 template <int PARTS>
 __global__ void __launch_bounds__(128) bottom_up_kernel(int64_t count, const int64_t *left, const int2 *up,
-                                                        unsigned *arrive, double *box,
-                                                        double *centre, double *core, double *sums) {
+                                                        unsigned *arrive, const double *centre, double *sums) {
     using MT = MomentTuples<PARTS>;
     __shared__ double sm[4][2][PARTS];
     __shared__ unsigned short src[16][MT::n];  // by mask, then tuple: the lanes of one mask read adjacent entries
@@ -1359,23 +1413,29 @@ __global__ void __launch_bounds__(128) bottom_up_kernel(int64_t count, const int
         if (prior == 0) return;
         __threadfence();
         const int64_t l = pu.y >= 0 ? node : -(int64_t)pu.y - 1, r = pu.y >= 0 ? (int64_t)pu.y : node;
-        for (int q = lane; q < PARTS; q += 32) {
-            sm[w][0][q] = __ldcg(sums + (int64_t)PARTS * l + q);
-            sm[w][1][q] = __ldcg(sums + (int64_t)PARTS * r + q);
+        // every load first (one round trip), then the stores to shared memory
+        constexpr int PER = (PARTS + 31) / 32;
+        double vl[PER], vr[PER];
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int q = lane + 32 * k;
+            vl[k] = q < PARTS ? __ldcg(sums + (int64_t)PARTS * l + q) : 0.0;
+            vr[k] = q < PARTS ? __ldcg(sums + (int64_t)PARTS * r + q) : 0.0;
         }
-        double lo_x = 0.0, hi_x = 0.0;
-        if (lane < 3) {
-            lo_x = fmin(__ldcg(box + 6 * l + lane), __ldcg(box + 6 * r + lane));
-            hi_x = fmax(__ldcg(box + 6 * l + 3 + lane), __ldcg(box + 6 * r + 3 + lane));
-        }
-        const double mid = 0.5 * (lo_x + hi_x);
-        const double c[3] = {__shfl_sync(0xffffffffu, mid, 0), __shfl_sync(0xffffffffu, mid, 1),
-                             __shfl_sync(0xffffffffu, mid, 2)};
         double D[2][3];
 #pragma unroll
         for (int x = 0; x < 3; ++x) {
-            D[0][x] = __ldcg(centre + 3 * l + x) - c[x];
-            D[1][x] = __ldcg(centre + 3 * r + x) - c[x];
+            const double cx = centre[3 * (int64_t)p + x];
+            D[0][x] = centre[3 * l + x] - cx;
+            D[1][x] = centre[3 * r + x] - cx;
+        }
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int q = lane + 32 * k;
+            if (q < PARTS) {
+                sm[w][0][q] = vl[k];
+                sm[w][1][q] = vr[k];
+            }
         }
         __syncwarp();
         double acc[MT::slots][3];
@@ -1417,12 +1477,6 @@ __global__ void __launch_bounds__(128) bottom_up_kernel(int64_t count, const int
         for (int q = 0; q < MT::slots; ++q)
             if (tn[q] >= 0)
                 for (int i = 0; i < 3; ++i) out[tuple_out(lane + 32 * q, i)] = acc[q][i];
-        if (lane < 3) {
-            box[6 * p + lane] = lo_x;
-            box[6 * p + 3 + lane] = hi_x;
-            centre[3 * p + lane] = mid;
-        }
-        if (lane == 0) core[p] = fmax(__ldcg(core + l), __ldcg(core + r));
         node = p;
     }
 }
@@ -1475,15 +1529,27 @@ __global__ void __launch_bounds__(MOM_THREADS) bound_chunks_kernel(int64_t count
     }
 }
 
-// Internal node: bound^2 from bound_chunks_kernel; then finalize every node from its sums.
+// The bounding radius (bound^2 from leaf_geometry_kernel or bound_chunks_kernel) and the traversal record of every
+// node: all that the walk reads.
+__global__ void node_rec_kernel(int64_t count, const unsigned long long *bound2, const double *centre,
+                                const double *core, const int64_t *lo, const int64_t *hi, const int64_t *left,
+                                const int64_t *right, double *bound, NodeRec *nodes) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    const double b = sqrt(__longlong_as_double((long long)bound2[j])) * (1.0 + 1e-12);
+    bound[j] = b;
+    nodes[j] = node_record(j, b, centre, core, lo, hi, left, right);
+}
+
+// Every node's export arrays and far records from its sums.
 template <int PARTS>
-__global__ void node_final_kernel(int64_t count, const unsigned long long *bound2, double *sums, NodeOut o) {
+__global__ void node_final_kernel(int64_t count, const double *sums, NodeOut o) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= count) return;
     double v[PARTS];
-    for (int q = 0; q < PARTS; ++q) v[q] = sums[(int64_t)PARTS * j + q];
-    if (o.left[j] >= 0) v[0] = __longlong_as_double((long long)bound2[j]);
-    finalize_node<PARTS>(j, v, o);
+    v[0] = 0.0;
+    for (int q = 1; q < PARTS; ++q) v[q] = sums[(int64_t)PARTS * j + q];
+    finalize_node<PARTS, false>(j, v, o);
 }
 
 __global__ void internal_item_count_kernel(int64_t count, const int64_t *lo, const int64_t *hi, const int64_t *left,
@@ -1494,42 +1560,66 @@ __global__ void internal_item_count_kernel(int64_t count, const int64_t *lo, con
     n[j] = (left[j] >= 0 && size > 0) ? (size + CHUNK - 1) / CHUNK : 0;
 }
 
-// Bottom-up pipeline: leaves, then internal nodes from their children, then the exact bounds, then the records.
+// Bottom-up pipeline in two phases.  Geometry, on s: leaf boxes, centres, cores and bounds, the internal nodes' boxes
+// from their children, their exact bounds (one pass over the internal nodes' ranges of tree-ordered endpoints) and
+// the traversal records.  Moments, on `side` when given (after s reached the end of the geometry; t->moments_done
+// marks their end) or else on s: leaf sums, the internal nodes' translated sums, the far records.  What the moment
+// phase reads lives with the tree when it runs on the side stream (freed with the tree, after the evaluation that
+// waited for it), else in scratch.
 template <int PARTS>
-static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_t s) {
+static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_t s, cudaStream_t side) {
     const int64_t count = t->count, m = t->m;
-    double *box = scratch.get<double>(6 * count), *sums = scratch.get<double>((size_t)PARTS * count);
-    int2 *parent = scratch.get<int2>(count);
-    unsigned *arrive = scratch.get<unsigned>(count);
+    const bool defer = side != nullptr;
+    double *box = scratch.get<double>(6 * count);
+    unsigned *arrive = scratch.get<unsigned>(2 * count);
     EndPts *ends = scratch.get<EndPts>(m);
     int64_t *nitems = scratch.get<int64_t>(count), *first = scratch.get<int64_t>(count);
     int64_t *total = scratch.get<int64_t>(1);
     unsigned long long *bound2 = scratch.get<unsigned long long>(count);
-    if (!box || !sums || !parent || !arrive || !ends || !nitems || !first || !total || !bound2) return scratch.status;
+    if (!box || !arrive || !ends || !nitems || !first || !total || !bound2) return scratch.status;
+    double *sums = defer ? t->alloc<double>((size_t)PARTS * count, s) : scratch.get<double>((size_t)PARTS * count);
+    int2 *parent = defer ? t->alloc<int2>(count, s) : scratch.get<int2>(count);
+    unsigned *arrive_m = defer ? t->alloc<unsigned>(count, s) : scratch.get<unsigned>(count);
+    if (!sums || !parent || !arrive_m) return defer ? BS_ERR_OOM : scratch.status;
     BS_CUDA(cudaMemsetAsync(arrive, 0, count * sizeof(unsigned), s));
+    BS_CUDA(cudaMemsetAsync(arrive_m, 0, count * sizeof(unsigned), s));
     BS_CUDA(cudaMemsetAsync(bound2, 0, count * sizeof(unsigned long long), s));
     parent_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->left, t->right, parent);
     sorted_ends_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, t->order32, geo, ends);
     const unsigned leaf_blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((count + 3) / 4, 148 * 16));
-    leaf_moments_kernel<PARTS><<<leaf_blocks, 128, 0, s>>>(count, t->lo, t->hi, t->left, t->order32, geo, box,
-                                                            t->centre, t->core, sums);
-    bottom_up_kernel<PARTS><<<blocks_for(count, 4), 128, 0, s>>>(count, t->left, parent, arrive, box, t->centre,
-                                                                  t->core, sums);
+    leaf_geometry_kernel<<<leaf_blocks, 128, 0, s>>>(count, t->lo, t->hi, t->left, t->order32, geo, ends, box,
+                                                      t->centre, t->core, bound2);
+    box_climb_kernel<<<blocks_for(count, 128), 128, 0, s>>>(count, t->left, parent, arrive, box, t->centre, t->core);
     internal_item_count_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->lo, t->hi, t->left, nitems);
-    BS_CHECK_LAUNCH("bottom-up moments");
+    BS_CHECK_LAUNCH("node geometry");
     int rc = scan_exclusive(nitems, first, count, total, scratch, s);
     if (rc != BS_OK) return rc;
     bound_chunks_kernel<<<148 * 8, MOM_THREADS, 0, s>>>(count, first, total, t->lo, t->hi, ends, t->centre, bound2);
+    node_rec_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, bound2, t->centre, t->core, t->lo, t->hi, t->left,
+                                                            t->right, t->bound, t->nodes);
+    BS_CHECK_LAUNCH("node records");
+    cudaStream_t ms = s;
+    if (defer) {
+        cudaEvent_t geometry;
+        BS_CUDA(cudaEventCreateWithFlags(&geometry, cudaEventDisableTiming));
+        cudaEventRecord(geometry, s);
+        cudaStreamWaitEvent(side, geometry, 0);
+        cudaEventDestroy(geometry);
+        ms = side;
+    }
+    leaf_moments_kernel<PARTS><<<leaf_blocks, 128, 0, ms>>>(count, t->lo, t->hi, t->left, t->order32, geo, t->centre,
+                                                             sums);
+    bottom_up_kernel<PARTS><<<blocks_for(count, 4), 128, 0, ms>>>(count, t->left, parent, arrive_m, t->centre, sums);
     const NodeOut out{t->lo, t->hi, t->left, t->right, t->centre, t->core, t->bound, t->m0, t->m1, t->m2,
                       t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x,
                       t->far64y, t->far32y};
     // one warp per block: the thread per node is long, so the nodes spread over every SM
-    node_final_kernel<PARTS><<<blocks_for(count, 32), 32, 0, s>>>(count, bound2, sums, out);
+    node_final_kernel<PARTS><<<blocks_for(count, 32), 32, 0, ms>>>(count, sums, out);
     BS_CHECK_LAUNCH("bottom-up moments");
     return BS_OK;
 }
 
-int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_t s) {
+int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_t s, cudaStream_t side) {
     const int64_t count = t->count;
     t->centre = t->alloc<double>(3 * count, s);
     t->bound = t->alloc<double>(count, s);
@@ -1557,9 +1647,9 @@ int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_
         !t->nodes || !t->far64 || !t->far32)
         return BS_ERR_OOM;
     // fourth order: the bottom-up pipeline for every kind (its box, centre and bound equal the direct sums')
-    if (t->order4) return moments_bottom_up<MOM_PARTS4>(t, geo, scratch, s);
-    if (t->kind == BS_TREE_MORTON) return t->order3 ? moments_bottom_up<MOM_PARTS3>(t, geo, scratch, s)
-                                                   : moments_bottom_up<MOM_PARTS>(t, geo, scratch, s);
+    if (t->order4) return moments_bottom_up<MOM_PARTS4>(t, geo, scratch, s, side);
+    if (t->kind == BS_TREE_MORTON) return t->order3 ? moments_bottom_up<MOM_PARTS3>(t, geo, scratch, s, side)
+                                                   : moments_bottom_up<MOM_PARTS>(t, geo, scratch, s, side);
     int64_t *nitems = scratch.get<int64_t>(count), *first = scratch.get<int64_t>(count);
     int64_t *total = scratch.get<int64_t>(1);
     if (!nitems || !first || !total) return scratch.status;
@@ -1597,7 +1687,8 @@ int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_
 using namespace bs;
 
 // Shared tail of both constructors: inverse permutation, int64 order, tree-ordered segment records, moments.
-static int finish_tree(bs_tree *t, const bs_sources *src, const SegGeo *geo, Scratch &scratch, cudaStream_t s) {
+static int finish_tree(bs_tree *t, const bs_sources *src, const SegGeo *geo, Scratch &scratch, cudaStream_t s,
+                       cudaStream_t side = nullptr) {
     const int64_t m = t->m;
     if (!t->order) t->order = t->alloc<int64_t>(m, s);
     t->inverse = t->alloc<int32_t>(m, s);
@@ -1609,7 +1700,7 @@ static int finish_tree(bs_tree *t, const bs_sources *src, const SegGeo *geo, Scr
     BS_CHECK_LAUNCH("widen_order_kernel");
     int rc = pack_segments(src, t->order32, t->seg64, t->seg32, nullptr, s, t->seg32x2);
     if (rc != BS_OK) return rc;
-    return compute_moments(t, geo, scratch, s);
+    return compute_moments(t, geo, scratch, s, side);
 }
 
 static int check_sources(const bs_sources *src) {
@@ -1642,7 +1733,7 @@ extern "C" int64_t bs_tree_count(const bs_tree *tree) { return tree ? tree->coun
 // (wait = false: the evaluation is queued behind the build on the same stream, and tree_stage_times reads the times
 // once the caller has synchronised).
 int tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_tree **out, cudaStream_t s,
-               bool wait, const std::function<int()> &before_geometry) {
+               bool wait, const std::function<int()> &before_geometry, cudaStream_t side) {
     if (!ctx || !tp || !out) {
         set_error("bs_tree_build: null argument");
         return BS_ERR_ARG;
@@ -1672,6 +1763,8 @@ int tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_
     t->leaf_size = tp->leaf_size;
     t->order3 = tp->order >= 3;
     t->order4 = tp->order >= 4;
+    // the moment phase of the bottom-up pipeline (Morton trees, fourth-order trees) may run on the side stream
+    cudaStream_t defer = (side && (t->order4 || t->kind == BS_TREE_MORTON)) ? side : nullptr;
     {
         Scratch scratch(ctx->pool, s);
         // before_geometry (may be empty) runs once, before anything reads gamma or radius: for Morton trees while the
@@ -1682,8 +1775,8 @@ int tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_
             ran = true;
             return before_geometry();
         };
-        SegGeo *geo = scratch.get<SegGeo>(src->m);
-        rc = geo ? BS_OK : scratch.status;
+        SegGeo *geo = defer ? t->alloc<SegGeo>(src->m, s) : scratch.get<SegGeo>(src->m);
+        rc = geo ? BS_OK : (defer ? BS_ERR_OOM : scratch.status);
         if (rc == BS_OK && tp->kind == BS_TREE_MORTON) {
             rc = build_morton(t, src, scratch, s, gate);
             if (rc == BS_OK) rc = gate();
@@ -1695,9 +1788,10 @@ int tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_
         }
         if (rc == BS_OK) {
             cudaEventRecord(e1, s);
-            rc = finish_tree(t, src, geo, scratch, s);
+            rc = finish_tree(t, src, geo, scratch, s, defer);
         }
-        cudaEventRecord(e2, s);
+        cudaEventRecord(e2, defer ? defer : s);
+        if (defer) t->moments_done = e2;
         if (rc == BS_OK && wait) {
             cudaError_t e = cudaEventSynchronize(e2);
             if (e != cudaSuccess) rc = cuda_fail(e, "tree build");
@@ -1725,6 +1819,7 @@ void tree_stage_times(bs_tree *t) {
 void tree_release(bs_tree *tree, cudaStream_t s) {
     if (!tree) return;
     cudaSetDevice(tree->device);
+    if (tree->moments_done) cudaStreamWaitEvent(s, tree->moments_done, 0);  // moments still read the tree's memory
     for (int i = 0; i < tree->nblocks; ++i) cudaFreeAsync(tree->blocks[i], s);
     for (auto &e : tree->marks)
         if (e) cudaEventDestroy(e);
@@ -2015,7 +2110,7 @@ extern "C" int bs_node_quantities(bs_ctx *ctx, int64_t m, const double *starts, 
             geo_from_ends_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, starts, ends, length_vectors, gamma, radius,
                                                                     geo);
             BS_CHECK_LAUNCH("geo_from_ends_kernel");
-            rc = compute_moments(t, geo, scratch, s);
+            rc = compute_moments(t, geo, scratch, s, nullptr);
         }
         if (rc == BS_OK) {
             rc = bs_tree_export(t, nullptr, nullptr, nullptr, nullptr, nullptr, centre, bound, core, m0, m1, m2, w1,

@@ -50,6 +50,7 @@ struct EvalArgs {
     TreeView tv;
     double theta, theta2, clearance;
     int order, model, raise_singular, stack_limit;
+    int deferred;  // the far records may still be in computation while the walk runs: the walk must not read them
     float near2;
     // interaction lists: entries live in chunks of LIST_CHUNK taken from a shared pool; warp gw of targets lists its
     // chunks in unit_chunks[gw][0 .. LIST_CHUNKS)
@@ -434,7 +435,9 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
                 ++len;
                 running += FAR_COST;
             } else if (mine && accept) {
-                far_node<PREC>(a, t, node, acc);
+                // far records still in computation: the host evaluates again once they are complete
+                if (a.deferred) atomicOr(a.overflow + 1, 1);
+                else far_node<PREC>(a, t, node, acc);
             }
         }
         if (openm) {
@@ -686,8 +689,10 @@ __global__ void exclusion_positions_kernel(int64_t n, const int64_t *ex_ptr, con
 
 static inline unsigned nblocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
-// Events that eval_run records around the walk and list kernels (null while a graph is being captured).
+// Events that eval_run records around the walk and list kernels (null while a graph is being captured), and the event
+// the list kernel waits for when the far records were still in computation (null: nothing to wait for).
 static thread_local cudaEvent_t *t_marks = nullptr;
+static thread_local cudaEvent_t t_far_ready = nullptr;
 
 template <int PREC, int MODEL>
 static void launch_pair(unsigned walk_grid, int block, size_t smem, unsigned list_grid, int64_t target_warps,
@@ -700,6 +705,7 @@ static void launch_pair(unsigned walk_grid, int block, size_t smem, unsigned lis
     if (t_marks) cudaEventRecord(t_marks[0], s);
     if (pop == 2) tree_walk_kernel<PREC, MODEL, 2><<<walk_grid, block, smem, s>>>(args);
     else tree_walk_kernel<PREC, MODEL, 1><<<walk_grid, block, smem, s>>>(args);
+    if (t_far_ready) cudaStreamWaitEvent(s, t_far_ready, 0);
     if (t_marks) cudaEventRecord(t_marks[1], s);
     tree_list_kernel<PREC, MODEL><<<list_grid, LIST_WARPS * 32, 0, s>>>(args, target_warps);
     if (t_marks) cudaEventRecord(t_marks[2], s);
@@ -846,18 +852,30 @@ int check_eval_args(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params
     return BS_OK;
 }
 
+// What a tree sum prepared beside its build: the sorted target order (perm, complete at perm_ready) and the end of
+// the far records' computation (far_ready), for eval_enqueue; all may be null.
+struct EvalPre {
+    const int32_t *perm = nullptr;
+    cudaEvent_t perm_ready = nullptr;
+    cudaEvent_t far_ready = nullptr;
+};
+
 // Everything the evaluation launches, on stream s, with scratch from `scratch` (pool or arena).  No host
-// synchronisation: the counters and the overflow flag stay in `state` (device, 6 words: overflow + 5 counters).
+// synchronisation: the counters and the overflow flags stay in `state` (device, 6 words: overflow + 5 counters).
 int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const bs_targets *tgt,
                  const int64_t *target_wake_ptr, int nw, const bs_kernel_params *kp, double *out, int8_t *flags,
-                 int64_t *far_counts, unsigned long long *state, Scratch &scratch, cudaStream_t s) {
+                 int64_t *far_counts, unsigned long long *state, Scratch &scratch, cudaStream_t s,
+                 const EvalPre *pre = nullptr) {
     const int64_t n = tgt->n;
-    int32_t *perm = scratch.get<int32_t>(n);
+    const bool sorted = pre && pre->perm && !target_wake_ptr;
+    int32_t *perm = sorted ? const_cast<int32_t *>(pre->perm) : scratch.get<int32_t>(n);
     unsigned long long *queue = scratch.get<unsigned long long>(2);  // list-kernel work counter, list-pool cursor
     int32_t *ex_pos = nullptr, *root_of = nullptr;
     if (!perm || !queue) return scratch.status;
     int rc;
-    if (target_wake_ptr) {
+    if (sorted) {
+        if (pre->perm_ready) BS_CUDA(cudaStreamWaitEvent(s, pre->perm_ready, 0));
+    } else if (target_wake_ptr) {
         int wbits = 0;
         while ((1 << wbits) < nw) ++wbits;
         const int bits = (63 - wbits) / 3;
@@ -915,6 +933,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     args.order = tp->order;
     args.model = kp->model;
     args.raise_singular = kp->raise_singular ? 1 : 0;
+    args.deferred = (pre && pre->far_ready) ? 1 : 0;
     args.near2 = (float)(kp->near_cores * kp->near_cores);
     args.stack_limit = (tp->stack_limit > 0 && tp->stack_limit < STACK_DEPTH) ? tp->stack_limit : STACK_DEPTH;
     args.list = list;
@@ -939,8 +958,10 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     const int64_t items = target_warps * chunks;
     const unsigned list_grid = (unsigned)std::max<int64_t>(
         1, std::min<int64_t>((items + LIST_WARPS - 1) / LIST_WARPS, (int64_t)ctx->sm_count * 3));
+    t_far_ready = args.deferred ? pre->far_ready : nullptr;
     launch_eval(kp->precision, kp->model, walk_grid, block, smem, list_grid, target_warps, nblocks(n, 256), s, args,
                 out, flags);
+    t_far_ready = nullptr;
     BS_CHECK_LAUNCH("tree evaluation");
     return BS_OK;
 }
@@ -948,7 +969,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
 // Runs the evaluation, waits for it and reads counters and the overflow flag into the context's statistics.
 int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const bs_targets *tgt,
              const int64_t *target_wake_ptr, int nw, const bs_kernel_params *kp, double *out, int8_t *flags,
-             int64_t *far_counts, cudaStream_t s) {
+             int64_t *far_counts, cudaStream_t s, const EvalPre *pre = nullptr) {
     Scratch scratch(ctx->pool, s);
     unsigned long long *state = scratch.get<unsigned long long>(6);
     if (!state) return scratch.status;
@@ -958,7 +979,8 @@ int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const b
     for (auto &m : marks) cudaEventCreate(&m);
     cudaEventRecord(e0, s);
     t_marks = marks;
-    int rc = eval_enqueue(ctx, tree, tp, tgt, target_wake_ptr, nw, kp, out, flags, far_counts, state, scratch, s);
+    int rc = eval_enqueue(ctx, tree, tp, tgt, target_wake_ptr, nw, kp, out, flags, far_counts, state, scratch, s,
+                          pre);
     t_marks = nullptr;
     cudaEventRecord(e1, s);
     unsigned long long host[6] = {0, 0, 0, 0, 0, 0};
@@ -995,6 +1017,37 @@ int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const b
                   (tp->stack_limit > 0 && tp->stack_limit < STACK_DEPTH) ? tp->stack_limit : STACK_DEPTH);
         return BS_ERR_STACK;
     }
+    if (host[0] >> 32) {  // a full list met a far node while the far records were in computation: again, complete
+        EvalPre again;
+        if (pre) again.perm = pre->perm;
+        return eval_run(ctx, tree, tp, tgt, target_wake_ptr, nw, kp, out, flags, far_counts, s, &again);
+    }
+    return BS_OK;
+}
+
+// A tree sum's side stream: the target sort is queued there at once (the targets are on the device when s reaches
+// this point) and the far records later, so that both run beside the build and the walk on s.
+int side_stream(bs_ctx *ctx, cudaStream_t *side) {
+    if (!ctx->side_stream) BS_CUDA(cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking));
+    *side = ctx->side_stream;
+    return BS_OK;
+}
+
+int sort_targets_beside(bs_ctx *ctx, const bs_targets *tgt, int32_t *perm, cudaStream_t s, cudaStream_t side,
+                        cudaEvent_t *ready) {
+    cudaEvent_t fork;
+    BS_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    cudaEventRecord(fork, s);
+    cudaStreamWaitEvent(side, fork, 0);
+    cudaEventDestroy(fork);
+    int rc;
+    {
+        Scratch scratch(ctx->pool, side);  // allocated and freed in the side stream's order
+        rc = target_order(tgt->n, tgt->points, perm, scratch, side);
+    }
+    if (rc != BS_OK) return rc;
+    BS_CUDA(cudaEventCreateWithFlags(ready, cudaEventDisableTiming));
+    BS_CUDA(cudaEventRecord(*ready, side));
     return BS_OK;
 }
 
@@ -1098,15 +1151,30 @@ extern "C" int bs_tree_sum_host(bs_ctx *ctx, const bs_sources *src, const bs_tre
                 BS_CUDA(cudaStreamWaitEvent(s, landed, 0));
                 return BS_OK;
             };
+            // the target sort on the side stream, beside the build (the targets landed with the first upload)
+            cudaStream_t side = nullptr;
+            cudaEvent_t sorted = nullptr;
+            int32_t *perm = scratch.get<int32_t>(n);
+            rc = perm ? side_stream(ctx, &side) : scratch.status;
+            if (rc == BS_OK) rc = sort_targets_beside(ctx, &dtgt, perm, s, side, &sorted);
             bs_tree *tree = nullptr;
-            rc = tree_build(ctx, &dsrc, tp, &tree, s, false, rest);
+            if (rc == BS_OK) rc = tree_build(ctx, &dsrc, tp, &tree, s, false, rest, side);
             if (rc == BS_OK) rc = check_eval_args(ctx, tree, tp, &dtgt, kp, d_out, d_flags);
-            if (rc == BS_OK) rc = eval_run(ctx, tree, tp, &dtgt, nullptr, 1, kp, d_out, d_flags, d_far, s);
+            if (rc == BS_OK) {
+                const EvalPre pre{perm, sorted, tree->moments_done};
+                rc = eval_run(ctx, tree, tp, &dtgt, nullptr, 1, kp, d_out, d_flags, d_far, s, &pre);
+            }
             if (tree) {
                 if (rc == BS_OK) tree_stage_times(tree);
                 ctx->stats.build_ms = tree->build_ms;
                 ctx->stats.moments_ms = tree->moments_ms;
                 tree_release(tree, s);
+            }
+            if (sorted) {  // the side stream's use of perm ends before perm is freed on s
+                cudaStreamWaitEvent(s, sorted, 0);
+                cudaEventDestroy(sorted);
+            } else if (side) {
+                cudaStreamSynchronize(side);
             }
             if (!joined) bs_stage_wait(ctx);
             cudaStreamSynchronize(ctx->copy_stream);  // the staging of the rest has finished on any return
@@ -1252,16 +1320,41 @@ extern "C" int bs_tree_sum(bs_ctx *ctx, const bs_sources *src, const bs_tree_par
         if (far_counts) BS_CUDA(cudaMemsetAsync(far_counts, 0, tgt->n * sizeof(int64_t), s));
         return BS_OK;
     }
-    // the evaluation queues behind the build on the same stream: no wait in between; the tree is freed in stream
-    // order after the evaluation (which synchronises before it returns)
-    cudaStream_t s = (cudaStream_t)stream;
-    bs_tree *tree = nullptr;
-    int rc = tree_build(ctx, src, tp, &tree, s, false, {});
+    // the evaluation queues behind the build on the same stream: no wait in between; the target sort and the far
+    // records run on the side stream beside the build and the walk; the tree is freed in stream order after the
+    // evaluation (which synchronises before it returns)
+    cudaStream_t s = (cudaStream_t)stream, side = nullptr;
+    BS_CUDA(cudaSetDevice(ctx->device));
+    int rc = side_stream(ctx, &side);
     if (rc != BS_OK) return rc;
-    rc = bs_tree_eval(ctx, tree, tp, tgt, kp, out, flags, far_counts, stream);
-    if (rc == BS_OK) tree_stage_times(tree);
-    float b = tree->build_ms, mm = tree->moments_ms;
-    tree_release(tree, s);
+    float b = 0.f, mm = 0.f;
+    {
+        Scratch scratch(ctx->pool, s);
+        int32_t *perm = scratch.get<int32_t>(tgt->n);
+        if (!perm) return scratch.status;
+        cudaEvent_t sorted = nullptr;
+        rc = sort_targets_beside(ctx, tgt, perm, s, side, &sorted);
+        bs_tree *tree = nullptr;
+        if (rc == BS_OK) rc = tree_build(ctx, src, tp, &tree, s, false, {}, side);
+        if (rc == BS_OK) rc = check_eval_args(ctx, tree, tp, tgt, kp, out, flags);
+        if (rc == BS_OK) {
+            const EvalPre pre{perm, sorted, tree->moments_done};
+            rc = eval_run(ctx, tree, tp, tgt, nullptr, 1, kp, out, flags, far_counts, s, &pre);
+        }
+        if (tree) {
+            if (rc == BS_OK) tree_stage_times(tree);
+            b = tree->build_ms;
+            mm = tree->moments_ms;
+            tree_release(tree, s);
+        }
+        // on every path the side stream's use of perm ends before perm is freed on s
+        if (sorted) {
+            cudaStreamWaitEvent(s, sorted, 0);
+            cudaEventDestroy(sorted);
+        } else {
+            cudaStreamSynchronize(side);
+        }
+    }
     ctx->stats.build_ms = b;
     ctx->stats.moments_ms = mm;
     return rc;

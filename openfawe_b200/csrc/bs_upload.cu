@@ -182,7 +182,7 @@ extern "C" int bs_download_many(bs_ctx *ctx, int count, void *const *dst, const 
         int slot;
         size_t len;
     };
-    Pending pending[bs_upload_ring::SLOTS];
+    Pending pending[bs_upload_ring::SLOTS] = {};
     int head = 0, queued = 0, k = 0;
     auto drain_one = [&]() -> int {
         const Pending p = pending[head];
