@@ -38,6 +38,7 @@ struct bs_tree {
     bs::Far64y *far64y = nullptr;  // fourth-order records (trees built for order 4 only)
     bs::Far32y *far32y = nullptr;
     int order3 = 0, order4 = 0;
+    bool geo_sorted = false;  // the build's segment geometry (SegGeo) is in tree order (Morton trees)
     bs::Seg64 *seg64 = nullptr;  // tree order
     bs::Seg32 *seg32 = nullptr;  // tree order
     bs::Seg32x2 *seg32x2 = nullptr;  // tree order, consecutive pairs

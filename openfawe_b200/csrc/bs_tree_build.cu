@@ -1096,22 +1096,20 @@ struct __align__(16) EndPts {
     double sx, sy, sz, ex, ey, ez;
 };
 
-__global__ void sorted_ends_kernel(int64_t m, const int32_t *order, const SegGeo *geo, EndPts *ends) {
-    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= m) return;
-    const SegGeo g = geo[order[k]];
-    ends[k] = EndPts{g.sx, g.sy, g.sz, g.ex, g.ey, g.ez};
-}
 
 // up[child] = (parent, the other child), the other child stored as -(it + 1) when `child` is the right one, so that a
 // climbing warp knows both children and their order from one load; up[0].x = -1.
-__global__ void parent_kernel(int64_t count, const int64_t *left, const int64_t *right, int2 *up) {
+// The leaves are listed in leaves[0 .. *nleaves) in no particular order (each leaf's work is independent of which
+// thread takes it).  up[] starts as all -1 (memset), so a node without a parent reads parent -1.
+__global__ void parent_kernel(int64_t count, const int64_t *left, const int64_t *right, int2 *up, int32_t *leaves,
+                              unsigned *nleaves) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= count) return;
-    if (j == 0) up[0] = make_int2(-1, 0);
     if (left[j] >= 0) {
         up[left[j]] = make_int2((int)j, (int)right[j]);
         up[right[j]] = make_int2((int)j, -(int)left[j] - 1);
+    } else {
+        leaves[atomicAdd(nleaves, 1u)] = (int32_t)j;
     }
 }
 
@@ -1170,16 +1168,18 @@ struct MomentTuples {
 // Storage index of moment (i; tuple u).
 __device__ __forceinline__ int tuple_out(int u, int i) { return c_tt.out0[u] + c_tt.cnt[u] * i; }
 
-// The box of the leaf's segments [a, b) and their largest core radius, reduced over the warp.
+// The box of the leaf's segments [a, b) and their largest core radius, reduced over the warp; with ends, also the
+// tree-ordered endpoints of the segments.
 __device__ __forceinline__ void leaf_extent(int lane, int64_t a, int64_t b, const int32_t *order, const SegGeo *geo,
-                                            double *mn, double *mx, double &c) {
+                                            double *mn, double *mx, double &c, EndPts *ends = nullptr) {
     for (int x = 0; x < 3; ++x) {
         mn[x] = INFINITY;
         mx[x] = -INFINITY;
     }
     c = 0.0;
     for (int64_t k = a + lane; k < b; k += 32) {
-        const SegGeo g = geo[order[k]];
+        const SegGeo g = geo[order ? order[k] : k];
+        if (ends) ends[k] = EndPts{g.sx, g.sy, g.sz, g.ex, g.ey, g.ez};
         mn[0] = fmin(mn[0], fmin(g.sx, g.ex)); mx[0] = fmax(mx[0], fmax(g.sx, g.ex));
         mn[1] = fmin(mn[1], fmin(g.sy, g.ey)); mx[1] = fmax(mx[1], fmax(g.sy, g.ey));
         mn[2] = fmin(mn[2], fmin(g.sz, g.ez)); mx[2] = fmax(mx[2], fmax(g.sz, g.ez));
@@ -1191,6 +1191,46 @@ __device__ __forceinline__ void leaf_extent(int lane, int64_t a, int64_t b, cons
             mx[x] = fmax(mx[x], __shfl_xor_sync(0xffffffffu, mx[x], o));
         }
         c = fmax(c, __shfl_xor_sync(0xffffffffu, c, o));
+    }
+}
+
+// One warp per leaf: box, core and centre from the leaf's segments (and their tree-ordered endpoints into ends), then
+// bound^2 (the largest squared distance from the centre to an endpoint) into bound2 as its bit pattern.
+__global__ void __launch_bounds__(128) leaf_geometry_kernel(const int32_t *leaves, const unsigned *nleaves,
+                                                            const int64_t *lo, const int64_t *hi,
+                                                            const int32_t *order, const SegGeo *geo,
+                                                            EndPts *ends, double *box, double *centre,
+                                                            double *core, unsigned long long *bound2) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5), n = *nleaves;
+    for (int64_t w = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n; w += warps) {
+        const int64_t j = leaves[w];
+        const int64_t a = lo[j], b = hi[j];
+        double mn[3], mx[3], c;
+        leaf_extent(lane, a, b, order, geo, mn, mx, c, ends);
+        const double c0 = 0.5 * (mn[0] + mx[0]), c1 = 0.5 * (mn[1] + mx[1]), c2 = 0.5 * (mn[2] + mx[2]);
+        double r2 = 0.0;
+        for (int64_t k = a + lane; k < b; k += 32) {
+            const SegGeo e = geo[order ? order[k] : k];
+            const double a0 = e.sx - c0, a1 = e.sy - c1, a2 = e.sz - c2;
+            const double b0 = e.ex - c0, b1 = e.ey - c1, b2 = e.ez - c2;
+            // the reference's ((x^2 + y^2) + z^2) without contraction, as in every bound of this file
+            const double ra = __dadd_rn(__dadd_rn(__dmul_rn(a0, a0), __dmul_rn(a1, a1)), __dmul_rn(a2, a2));
+            const double rb = __dadd_rn(__dadd_rn(__dmul_rn(b0, b0), __dmul_rn(b1, b1)), __dmul_rn(b2, b2));
+            r2 = fmax(r2, fmax(ra, rb));
+        }
+        for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
+        if (lane == 0) {
+            for (int x = 0; x < 3; ++x) {
+                box[6 * j + x] = mn[x];
+                box[6 * j + 3 + x] = mx[x];
+            }
+            centre[3 * j] = c0;
+            centre[3 * j + 1] = c1;
+            centre[3 * j + 2] = c2;
+            core[j] = c;
+            bound2[j] = (unsigned long long)__double_as_longlong(r2);
+        }
     }
 }
 
@@ -1239,53 +1279,14 @@ __device__ __forceinline__ void segment_means(const double *d, const double *l, 
     }
 }
 
-// One warp per leaf: box, core and centre from the leaf's segments, then bound^2 (the largest squared distance from
-// the centre to an endpoint, from the tree-ordered endpoints) into bound2 as its bit pattern.
-__global__ void __launch_bounds__(128) leaf_geometry_kernel(int64_t count, const int64_t *lo, const int64_t *hi,
-                                                            const int64_t *left, const int32_t *order,
-                                                            const SegGeo *geo, const EndPts *ends, double *box,
-                                                            double *centre, double *core,
-                                                            unsigned long long *bound2) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t j = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); j < count; j += warps) {
-        if (left[j] >= 0) continue;
-        const int64_t a = lo[j], b = hi[j];
-        double mn[3], mx[3], c;
-        leaf_extent(lane, a, b, order, geo, mn, mx, c);
-        const double c0 = 0.5 * (mn[0] + mx[0]), c1 = 0.5 * (mn[1] + mx[1]), c2 = 0.5 * (mn[2] + mx[2]);
-        double r2 = 0.0;
-        for (int64_t k = a + lane; k < b; k += 32) {
-            const EndPts e = ends[k];
-            const double a0 = e.sx - c0, a1 = e.sy - c1, a2 = e.sz - c2;
-            const double b0 = e.ex - c0, b1 = e.ey - c1, b2 = e.ez - c2;
-            // the reference's ((x^2 + y^2) + z^2) without contraction, as in every bound of this file
-            const double ra = __dadd_rn(__dadd_rn(__dmul_rn(a0, a0), __dmul_rn(a1, a1)), __dmul_rn(a2, a2));
-            const double rb = __dadd_rn(__dadd_rn(__dmul_rn(b0, b0), __dmul_rn(b1, b1)), __dmul_rn(b2, b2));
-            r2 = fmax(r2, fmax(ra, rb));
-        }
-        for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
-        if (lane == 0) {
-            for (int x = 0; x < 3; ++x) {
-                box[6 * j + x] = mn[x];
-                box[6 * j + 3 + x] = mx[x];
-            }
-            centre[3 * j] = c0;
-            centre[3 * j + 1] = c1;
-            centre[3 * j + 2] = c2;
-            core[j] = c;
-            bound2[j] = (unsigned long long)__double_as_longlong(r2);
-        }
-    }
-}
-
 // One warp per leaf: the moments about the leaf's centre; sums[j][PARTS] (sums[j][0] unused).  The warp takes 32
 // segments at a time: each lane forms its segment's means (segment_means) and alpha = gamma l into shared memory,
 // then lane u sums, over the 32, alpha_i times the mean of index tuple u (and of u + 32) for i = 0..2.
 template <int PARTS>
-__global__ void __launch_bounds__(128) leaf_moments_kernel(int64_t count, const int64_t *lo, const int64_t *hi,
-                                                           const int64_t *left, const int32_t *order,
-                                                           const SegGeo *geo, const double *centre, double *sums) {
+__global__ void __launch_bounds__(128) leaf_moments_kernel(const int32_t *leaves, const unsigned *nleaves,
+                                                           const int64_t *lo, const int64_t *hi,
+                                                           const int32_t *order, const SegGeo *geo,
+                                                           const double *centre, double *sums) {
     using MT = MomentTuples<PARTS>;
     constexpr int ROWS = MT::n + 3, STRIDE = 33;  // means, then alpha; padded rows: lanes of a column hit other banks
     __shared__ double st[4][ROWS * STRIDE];
@@ -1294,9 +1295,9 @@ __global__ void __launch_bounds__(128) leaf_moments_kernel(int64_t count, const 
     bool own[MT::slots];
 #pragma unroll
     for (int r = 0; r < MT::slots; ++r) own[r] = lane + 32 * r < MT::n;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t j = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); j < count; j += warps) {
-        if (left[j] >= 0) continue;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5), n = *nleaves;
+    for (int64_t x = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); x < n; x += warps) {
+        const int64_t j = leaves[x];
         const int64_t a = lo[j], b = hi[j];
         const double c0 = centre[3 * j], c1 = centre[3 * j + 1], c2 = centre[3 * j + 2];
         double acc[MT::slots][3];
@@ -1304,11 +1305,11 @@ __global__ void __launch_bounds__(128) leaf_moments_kernel(int64_t count, const 
         for (int r = 0; r < MT::slots; ++r) acc[r][0] = acc[r][1] = acc[r][2] = 0.0;
         // the next stage's record is loaded while this stage computes
         SegGeo next;
-        if (a + lane < b) next = geo[order[a + lane]];
+        if (a + lane < b) next = geo[order ? order[a + lane] : a + lane];
         for (int64_t base = a; base < b; base += 32) {
             const int64_t k = base + lane;
             const SegGeo e = next;
-            if (k + 32 < b) next = geo[order[k + 32]];
+            if (k + 32 < b) next = geo[order ? order[k + 32] : k + 32];
             double g[MT::n], al[3] = {0.0, 0.0, 0.0};
 #pragma unroll
             for (int q = 0; q < MT::n; ++q) g[q] = 0.0;
@@ -1348,15 +1349,16 @@ __global__ void __launch_bounds__(128) leaf_moments_kernel(int64_t count, const 
     }
 }
 
+
 // One thread per leaf climbs towards the root; at each parent the second of the two arriving threads combines the
 // children (their results were published, and fenced, before the arrival count moved), so every internal node is
 // combined exactly once and no thread waits for another: box = the children's union, centre = its midpoint, core =
 // the larger of the two.
-__global__ void box_climb_kernel(int64_t count, const int64_t *left, const int2 *up, unsigned *arrive, double *box,
-                                 double *centre, double *core) {
-    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= count || left[j] >= 0) return;
-    int64_t node = j;
+__global__ void box_climb_kernel(const int32_t *leaves, const unsigned *nleaves, const int2 *up, unsigned *arrive,
+                                 double *box, double *centre, double *core) {
+    const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= (int64_t)*nleaves) return;
+    int64_t node = leaves[w];
     for (int depth = 0; depth < 4096; ++depth) {
         const int2 pu = up[node];
         const int32_t p = pu.x;
@@ -1383,34 +1385,43 @@ __global__ void box_climb_kernel(int64_t count, const int64_t *left, const int2 
 //   m'_(i; a1..an) = sum over subsets S of the positions of prod_(s in S) D_as * m_(i; the positions not in S),
 // D = child centre - node centre, the subset products built up one factor at a time; left child first, then right.
 template <int PARTS>
-__global__ void __launch_bounds__(128) bottom_up_kernel(int64_t count, const int64_t *left, const int2 *up,
-                                                        unsigned *arrive, const double *centre, double *sums) {
+__global__ void __launch_bounds__(128) bottom_up_kernel(const int32_t *leaves, const unsigned *nleaves,
+                                                        const int2 *up, unsigned *arrive, const double *centre,
+                                                        double *sums) {
     using MT = MomentTuples<PARTS>;
     __shared__ double sm[4][2][PARTS];
     __shared__ unsigned short src[16][MT::n];  // by mask, then tuple: the lanes of one mask read adjacent entries
     for (int q = threadIdx.x; q < MT::n * 16; q += blockDim.x) src[q & 15][q >> 4] = c_tt.src[q >> 4][q & 15];
     __syncthreads();
     const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 3;
-    const int64_t j = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (j >= count || left[j] >= 0) return;
-    int tn[MT::slots], tp[MT::slots];
+    // lane's tuple in each slot: with two slots (fourth-order trees) slot 0 holds the first order-1 tuple and the 31 of
+    // orders 2-4, slot 1 the order-0 tuple and the other two of order 1, so that slot 1 runs two subset masks, not 16
+    int tu[MT::slots], tn[MT::slots], tp[MT::slots];
 #pragma unroll
     for (int r = 0; r < MT::slots; ++r) {
-        const int u = lane + 32 * r;
-        tn[r] = u < MT::n ? c_tt.n[u] : -1;
-        tp[r] = u < MT::n ? c_tt.packed[u] : 0;
+        const int u = MT::slots == 1 ? lane : (r == 0 ? (lane == 0 ? 1 : lane + 3) : (lane == 0 ? 0 : lane + 1));
+        const bool ok = MT::slots == 1 ? u < MT::n : (r == 0 || lane < 3);
+        tu[r] = u;
+        tn[r] = ok ? c_tt.n[u] : -1;
+        tp[r] = ok ? c_tt.packed[u] : 0;
     }
-    int64_t node = j;
+    // subset masks of a slot: 2^(largest order in it)
+    constexpr int MAXM = PARTS >= MOM_PARTS4 ? 16 : (PARTS >= MOM_PARTS3 ? 8 : 4);
+    // a grid that stays resident, so that every leaf's climb starts at once (more leaves than resident warps: a warp
+    // takes them one after another)
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5), n = *nleaves;
+    for (int64_t x = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); x < n; x += warps) {
+    int64_t node = leaves[x];
     for (int depth = 0; depth < 4096; ++depth) {
         const int2 pu = up[node];
         const int32_t p = pu.x;
-        if (p < 0) return;
+        if (p < 0) break;
         __threadfence();
         __syncwarp();
         unsigned prior = 0;
         if (lane == 0) prior = atomicAdd(&arrive[p], 1u);
         prior = __shfl_sync(0xffffffffu, prior, 0);
-        if (prior == 0) return;
+        if (prior == 0) break;
         __threadfence();
         const int64_t l = pu.y >= 0 ? node : -(int64_t)pu.y - 1, r = pu.y >= 0 ? (int64_t)pu.y : node;
         // every load first (one round trip), then the stores to shared memory
@@ -1443,7 +1454,7 @@ __global__ void __launch_bounds__(128) bottom_up_kernel(int64_t count, const int
         for (int q = 0; q < MT::slots; ++q) {
             acc[q][0] = acc[q][1] = acc[q][2] = 0.0;
             if (tn[q] < 0) continue;
-            const int u = lane + 32 * q;
+            const int u = tu[q], masks = (MT::slots == 2 && q == 1) ? 2 : MAXM;
 #pragma unroll
             for (int side = 0; side < 2; ++side) {
                 double Dp[4];  // D at the tuple's positions
@@ -1462,7 +1473,7 @@ __global__ void __launch_bounds__(128) bottom_up_kernel(int64_t count, const int
                 const double *sv = sm[w][side];
 #pragma unroll
                 for (int mask = 0; mask < 16; ++mask) {
-                    if (mask < (1 << tn[q])) {
+                    if (mask < masks && mask < (1 << tn[q])) {
                         const int e = src[mask][u], o0 = e & 255, cn = e >> 8;
                         acc[q][0] = fma(f[mask], sv[o0], acc[q][0]);
                         acc[q][1] = fma(f[mask], sv[o0 + cn], acc[q][1]);
@@ -1476,8 +1487,9 @@ __global__ void __launch_bounds__(128) bottom_up_kernel(int64_t count, const int
 #pragma unroll
         for (int q = 0; q < MT::slots; ++q)
             if (tn[q] >= 0)
-                for (int i = 0; i < 3; ++i) out[tuple_out(lane + 32 * q, i)] = acc[q][i];
+                for (int i = 0; i < 3; ++i) out[tuple_out(tu[q], i)] = acc[q][i];
         node = p;
+    }
     }
 }
 
@@ -1579,17 +1591,22 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
     if (!box || !arrive || !ends || !nitems || !first || !total || !bound2) return scratch.status;
     double *sums = defer ? t->alloc<double>((size_t)PARTS * count, s) : scratch.get<double>((size_t)PARTS * count);
     int2 *parent = defer ? t->alloc<int2>(count, s) : scratch.get<int2>(count);
-    unsigned *arrive_m = defer ? t->alloc<unsigned>(count, s) : scratch.get<unsigned>(count);
-    if (!sums || !parent || !arrive_m) return defer ? BS_ERR_OOM : scratch.status;
+    unsigned *arrive_m = defer ? t->alloc<unsigned>(count + 1, s) : scratch.get<unsigned>(count + 1);
+    int32_t *leaves = defer ? t->alloc<int32_t>(count, s) : scratch.get<int32_t>(count);
+    if (!sums || !parent || !arrive_m || !leaves) return defer ? BS_ERR_OOM : scratch.status;
+    unsigned *nleaves = arrive_m + count;
     BS_CUDA(cudaMemsetAsync(arrive, 0, count * sizeof(unsigned), s));
-    BS_CUDA(cudaMemsetAsync(arrive_m, 0, count * sizeof(unsigned), s));
+    BS_CUDA(cudaMemsetAsync(arrive_m, 0, (count + 1) * sizeof(unsigned), s));
     BS_CUDA(cudaMemsetAsync(bound2, 0, count * sizeof(unsigned long long), s));
-    parent_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->left, t->right, parent);
-    sorted_ends_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, t->order32, geo, ends);
-    const unsigned leaf_blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((count + 3) / 4, 148 * 16));
-    leaf_geometry_kernel<<<leaf_blocks, 128, 0, s>>>(count, t->lo, t->hi, t->left, t->order32, geo, ends, box,
+    BS_CUDA(cudaMemsetAsync(parent, 0xff, count * sizeof(int2), s));
+    parent_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->left, t->right, parent, leaves, nleaves);
+    const int32_t *geo_order = t->geo_sorted ? nullptr : t->order32;  // geo in input order: read through the order
+    int sms = 0;
+    BS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, t->device));
+    const unsigned leaf_blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((count + 3) / 4, (int64_t)sms * 16));
+    leaf_geometry_kernel<<<leaf_blocks, 128, 0, s>>>(leaves, nleaves, t->lo, t->hi, geo_order, geo, ends, box,
                                                       t->centre, t->core, bound2);
-    box_climb_kernel<<<blocks_for(count, 128), 128, 0, s>>>(count, t->left, parent, arrive, box, t->centre, t->core);
+    box_climb_kernel<<<blocks_for(count, 128), 128, 0, s>>>(leaves, nleaves, parent, arrive, box, t->centre, t->core);
     internal_item_count_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->lo, t->hi, t->left, nitems);
     BS_CHECK_LAUNCH("node geometry");
     int rc = scan_exclusive(nitems, first, count, total, scratch, s);
@@ -1607,9 +1624,17 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
         cudaEventDestroy(geometry);
         ms = side;
     }
-    leaf_moments_kernel<PARTS><<<leaf_blocks, 128, 0, ms>>>(count, t->lo, t->hi, t->left, t->order32, geo, t->centre,
-                                                             sums);
-    bottom_up_kernel<PARTS><<<blocks_for(count, 4), 128, 0, ms>>>(count, t->left, parent, arrive_m, t->centre, sums);
+    int leaf_resident = 0;  // resident blocks: one wave takes as many leaves as fit
+    BS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&leaf_resident, leaf_moments_kernel<PARTS>, 128, 0));
+    const unsigned moment_blocks = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>((count + 3) / 4, (int64_t)std::max(1, leaf_resident) * sms));
+    leaf_moments_kernel<PARTS><<<moment_blocks, 128, 0, ms>>>(leaves, nleaves, t->lo, t->hi, geo_order, geo, t->centre,
+                                                              sums);
+    int climb_blocks = 0;  // resident blocks: one wave holds every climbing warp
+    BS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&climb_blocks, bottom_up_kernel<PARTS>, 128, 0));
+    const unsigned climb_grid = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>(blocks_for(count, 4), (int64_t)std::max(1, climb_blocks) * sms));
+    bottom_up_kernel<PARTS><<<climb_grid, 128, 0, ms>>>(leaves, nleaves, parent, arrive_m, t->centre, sums);
     const NodeOut out{t->lo, t->hi, t->left, t->right, t->centre, t->core, t->bound, t->m0, t->m1, t->m2,
                       t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x,
                       t->far64y, t->far32y};
@@ -1698,9 +1723,20 @@ static int finish_tree(bs_tree *t, const bs_sources *src, const SegGeo *geo, Scr
     if (!t->order || !t->inverse || !t->seg64 || !t->seg32 || !t->seg32x2) return BS_ERR_OOM;
     widen_order_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, t->order32, t->order, t->inverse);
     BS_CHECK_LAUNCH("widen_order_kernel");
-    int rc = pack_segments(src, t->order32, t->seg64, t->seg32, nullptr, s, t->seg32x2);
+    // with a side stream (bottom-up trees of a tree sum) the segment records are packed there, beside the node
+    // geometry and the walk, which do not read them
+    const bool bottom_up = t->order4 || t->kind == BS_TREE_MORTON;
+    cudaStream_t ps = (side && bottom_up) ? side : s;
+    if (ps != s) {
+        cudaEvent_t ready;
+        BS_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+        cudaEventRecord(ready, s);
+        cudaStreamWaitEvent(ps, ready, 0);
+        cudaEventDestroy(ready);
+    }
+    int rc = pack_segments(src, t->order32, t->seg64, t->seg32, nullptr, ps, t->seg32x2);
     if (rc != BS_OK) return rc;
-    return compute_moments(t, geo, scratch, s, side);
+    return compute_moments(t, geo, scratch, s, bottom_up ? side : nullptr);
 }
 
 static int check_sources(const bs_sources *src) {
@@ -1780,7 +1816,9 @@ int tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_
         if (rc == BS_OK && tp->kind == BS_TREE_MORTON) {
             rc = build_morton(t, src, scratch, s, gate);
             if (rc == BS_OK) rc = gate();
-            if (rc == BS_OK) rc = pack_segments(src, nullptr, nullptr, nullptr, geo, s);
+            // the moment pipeline's geometry in tree order: every leaf reads a contiguous range
+            if (rc == BS_OK) rc = pack_segments(src, t->order32, nullptr, nullptr, geo, s);
+            t->geo_sorted = true;
         } else if (rc == BS_OK) {
             rc = gate();
             if (rc == BS_OK) rc = pack_segments(src, nullptr, nullptr, nullptr, geo, s);

@@ -50,7 +50,7 @@ struct EvalArgs {
     TreeView tv;
     double theta, theta2, clearance;
     int order, model, raise_singular, stack_limit;
-    int deferred;  // the far records may still be in computation while the walk runs: the walk must not read them
+    int deferred;  // the segment and far records may still be in computation while the walk runs: it must not read them
     float near2;
     // interaction lists: entries live in chunks of LIST_CHUNK taken from a shared pool; warp gw of targets lists its
     // chunks in unit_chunks[gw][0 .. LIST_CHUNKS)
@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
                 ++len;
                 running += FAR_COST;
             } else if (mine && accept) {
-                // far records still in computation: the host evaluates again once they are complete
+                // far records still being computed: evaluated again by the host once they are complete
                 if (a.deferred) atomicOr(a.overflow + 1, 1);
                 else far_node<PREC>(a, t, node, acc);
             }
@@ -451,6 +451,8 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
                     }
                     ++len;
                     running += (nr.hi - nr.lo) + 2;
+                } else if (a.deferred) {  // segment records still being written: evaluated again by the host
+                    if (mine && !accept) atomicOr(a.overflow + 1, 1);
                 } else {
                     int64_t ec = e;
                     leaf_pairs<PREC, MODEL>(a, t, nr, mine && !accept, ec, e1, seg64_tile, seg32_tile, acc, flag,
@@ -1017,7 +1019,7 @@ int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const b
                   (tp->stack_limit > 0 && tp->stack_limit < STACK_DEPTH) ? tp->stack_limit : STACK_DEPTH);
         return BS_ERR_STACK;
     }
-    if (host[0] >> 32) {  // a full list met a far node while the far records were in computation: again, complete
+    if (host[0] >> 32) {  // a full list met a node whose records were still being computed: again, with them complete
         EvalPre again;
         if (pre) again.perm = pre->perm;
         return eval_run(ctx, tree, tp, tgt, target_wake_ptr, nw, kp, out, flags, far_counts, s, &again);

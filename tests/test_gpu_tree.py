@@ -341,6 +341,27 @@ def test_list_overflow_is_evaluated_by_the_walk(device):
         assert rel < bound and not flags.cpu().numpy().any(), (precision, rel)
 
 
+def test_list_overflow_while_far_records_are_pending(device):
+    """A tree sum computes the far records on a side stream beside the walk; a walk whose list overflowed onto a far
+    node before they were complete is evaluated again once they are: device and host tree sums equal a separate build
+    and evaluation bit for bit, with thousands of far entries per warp (far beyond one list)."""
+    from openfawe_b200 import engine, wakes
+    case = wakes.rotor_sheet(60, seed=13, targets=2000)
+    args = wakes.backend_args(case)
+    src = engine.Sources(*args[1:6], device)
+    tgt = engine.Targets(case["points"], None, device)
+    for kind, order in (("morton", 2), ("median", 4)):
+        tree = engine.build_tree(src, leaf_size=1, kind=kind, order=order)
+        ref, ref_flags, far = engine.tree_eval(tree, tgt, 2, "raise", "mixed", theta=0.02, order=order)
+        assert int(far.cpu().numpy().max()) > 4096
+        u, flags, _ = engine.tree_sum(src, tgt, 2, "raise", "mixed", 128, 3.0, 0.02, order, 1, 3.0, kind)
+        assert np.array_equal(u.cpu().numpy(), ref.cpu().numpy()), (kind, order)
+        assert np.array_equal(flags.cpu().numpy(), ref_flags.cpu().numpy())
+        uh, _, _ = engine.tree_sum_host(case["points"], *args[1:6], None, 2, "raise", "mixed", 128, 3.0, 0.02, order,
+                                        1, 3.0, kind, device=device)
+        assert np.array_equal(uh, ref.cpu().numpy()), (kind, order)
+
+
 def test_upload_moves_host_bytes_exactly(device):
     """bs_upload (pinned staging ring, threaded host copies) delivers every byte, for sizes around its chunk size."""
     import torch
