@@ -69,9 +69,9 @@ typedef struct {
 
 typedef struct {
     double theta;      /* opening ratio, 0 < theta < 1 (TreeSettings.theta) */
-    int order;         /* expansion order 0, 1 or 2 (the reference's); 3 and 4 add the third- and fourth-order terms
-                          (a tree evaluated at order 3 or 4 must be built with at least that order, which computes
-                          the higher moments) */
+    int order;         /* expansion order 0, 1 or 2 (the reference's); 3, 4 and 5 add the third- to fifth-order
+                          terms (a tree evaluated at order 3, 4 or 5 must be built with at least that order, which
+                          computes the higher moments) */
     int64_t leaf_size; /* maximum segments per leaf */
     double clearance;  /* core clearance in largest core radii */
     int kind;          /* bs_tree_kind */

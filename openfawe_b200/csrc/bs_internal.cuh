@@ -163,6 +163,15 @@ enum { K_ROW = 36, K_M4 = 0, K_T4 = 15, K_TAU4 = 21, K_W4 = 22, K_W4T = 32 };
 struct __align__(16) Far64y { double v[112]; };
 struct __align__(16) Far32y { float v[112]; };
 
+// Fifth-order far-field coefficients (trees built for order 5), one row of 56 per component i (fourteen float4), in
+// both precisions: [0, 21) m5[i] symmetric in its five indices (lexicographic a <= b <= c <= d <= e), [21, 31)
+// T5[i][k][l][m] = m5[i][j][j][k][l][m] symmetric, [31, 34) TT5[i][m] = T5[i][j][j][m], [34, 49) W5[i][k][l][m][n] =
+// eps_ibc m5[b][c][k][l][m][n] symmetric, [49, 55) W5T[i][l][m] = eps_ibc T5[b][c][l][m] symmetric, [55] W5TT[i] =
+// eps_ibc TT5[b][c].
+enum { Z_ROW = 56, Z_M5 = 0, Z_T5 = 21, Z_TT5 = 31, Z_W5 = 34, Z_W5T = 49, Z_W5TT = 55 };
+struct __align__(16) Far64z { double v[3 * Z_ROW]; };
+struct __align__(16) Far32z { float v[3 * Z_ROW]; };
+
 // ---------------------------------------------------------------------------------------------------------------------
 // Arithmetic helpers.
 // ---------------------------------------------------------------------------------------------------------------------
@@ -459,13 +468,54 @@ __device__ __forceinline__ void far_term4(T rx, T ry, T rz, T inv7, T inv9, T in
     for (int i = 0; i < 3; ++i) far_term4_row<T>(rx, ry, rz, inv7, inv9, inv11, h + K_ROW * i, i, u0, u1, u2);
 }
 
+// The fifth-order term, R = x - c (the general order-p term of the same series at p = 5):
+//   (86.625 S5 / r^13 - 78.75 T5:RRR / r^11 + 13.125 TT5.R / r^9) x R
+//     - 39.375 W5:RRRR / r^11 + 26.25 W5T:RR / r^9 - 1.875 W5TT / r^7,
+// S5_i = m5[i] : RRRRR; row i (Z_ROW values) adds x5_i (e_i x R) + w_i e_i.
+template <class T>
+__device__ __forceinline__ void far_term5_row(T rx, T ry, T rz, T inv7, T inv9, T inv11, T inv13, const T *r, int i,
+                                              T &u0, T &u1, T &u2) {
+    const T xx = rx * rx, xy = rx * ry, xz = rx * rz, yy = ry * ry, yz = ry * rz, zz = rz * rz;
+    // monomials of the symmetric components (lexicographic index tuples) times their multiplicities
+    const T q2[6] = {xx, T(2) * xy, T(2) * xz, yy, T(2) * yz, zz};
+    const T c3[10] = {xx * rx, xx * ry, xx * rz, xy * ry, xy * rz, xz * rz, yy * ry, yy * rz, yz * rz, zz * rz};
+    const T q3[10] = {c3[0], T(3) * c3[1], T(3) * c3[2], T(3) * c3[3], T(6) * c3[4], T(3) * c3[5], c3[6],
+                      T(3) * c3[7], T(3) * c3[8], c3[9]};
+    const T q4[15] = {xx * xx, T(4) * xx * xy, T(4) * xx * xz, T(6) * xx * yy, T(12) * xx * yz, T(6) * xx * zz,
+                      T(4) * xy * yy, T(12) * xy * yz, T(12) * xy * zz, T(4) * xz * zz, yy * yy, T(4) * yy * yz,
+                      T(6) * yy * zz, T(4) * yz * zz, zz * zz};
+    // degree 5: (c0, c1, c2) = (5,0,0), (4,1,0), (4,0,1), (3,2,0), (3,1,1), (3,0,2), (2,3,0), (2,2,1), (2,1,2),
+    // (2,0,3), (1,4,0), (1,3,1), (1,2,2), (1,1,3), (1,0,4), (0,5,0), (0,4,1), (0,3,2), (0,2,3), (0,1,4), (0,0,5)
+    const T q5[21] = {xx * c3[0],          T(5) * xx * c3[1],   T(5) * xx * c3[2],   T(10) * xx * c3[3],
+                      T(20) * xx * c3[4],  T(10) * xx * c3[5],  T(10) * xx * c3[6],  T(30) * xx * c3[7],
+                      T(30) * xx * c3[8],  T(10) * xx * c3[9],  T(5) * xy * c3[6],   T(20) * xy * c3[7],
+                      T(30) * xy * c3[8],  T(20) * xy * c3[9],  T(5) * xz * c3[9],   yy * c3[6],
+                      T(5) * yy * c3[7],   T(10) * yy * c3[8],  T(10) * yy * c3[9],  T(5) * yz * c3[9],
+                      zz * c3[9]};
+    T s5 = 0, t5 = 0, w5 = 0, w5t = 0;
+#pragma unroll
+    for (int q = 0; q < 21; ++q) s5 += r[Z_M5 + q] * q5[q];
+#pragma unroll
+    for (int q = 0; q < 10; ++q) t5 += r[Z_T5 + q] * q3[q];
+#pragma unroll
+    for (int q = 0; q < 15; ++q) w5 += r[Z_W5 + q] * q4[q];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) w5t += r[Z_W5T + q] * q2[q];
+    const T tt5 = r[Z_TT5] * rx + r[Z_TT5 + 1] * ry + r[Z_TT5 + 2] * rz;
+    const T x5 = T(86.625) * inv13 * s5 - T(78.75) * inv11 * t5 + T(13.125) * inv9 * tt5;
+    const T w = T(26.25) * inv9 * w5t - T(39.375) * inv11 * w5 - T(1.875) * inv7 * r[Z_W5TT];
+    if (i == 0) { u0 += w; u1 -= x5 * rz; u2 += x5 * ry; }
+    else if (i == 1) { u0 += x5 * rz; u1 += w; u2 -= x5 * rx; }
+    else { u0 -= x5 * ry; u1 += x5 * rx; u2 += w; }
+}
+
 // vortex_tree.far_velocity with the symmetric second moment; R = x - c.  Order 3 (g: the third-order record) adds
 //   (17.5 S3 / r^9 - 7.5 T3 R / r^7) x R - 7.5 (W3 : R R) / r^7 + 1.5 w3 / r^5,  S3_b = m3[b] : R R R,
 // the next term of the same Taylor series of the segments' line integrals about the node centre; order 4 (k4: the
 // fourth-order record) adds far_term4.
 template <class T>
 __device__ __forceinline__ void far_eval(T rx, T ry, T rz, const T *f, int order, T &ux, T &uy, T &uz,
-                                         const T *g = nullptr, const T *k4 = nullptr) {
+                                         const T *g = nullptr, const T *k4 = nullptr, const T *z5 = nullptr) {
     T r2 = rx * rx + ry * ry + rz * rz;
     T inv3 = T(1) / (r2 * sqrt(r2));
     T inv5 = inv3 / r2;
@@ -527,6 +577,12 @@ __device__ __forceinline__ void far_eval(T rx, T ry, T rz, const T *f, int order
             u1 += (x3[2] * rx - x3[0] * rz) - c7 * w[1] + c5 * g[G_W3V + 1];
             u2 += (x3[0] * ry - x3[1] * rx) - c7 * w[2] + c5 * g[G_W3V + 2];
             if (order >= 4) far_term4<T>(rx, ry, rz, inv7, inv9, inv9 / r2, k4, u0, u1, u2);
+            if (order >= 5) {
+                const T inv11 = inv9 / r2;
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    far_term5_row<T>(rx, ry, rz, inv7, inv9, inv11, inv11 / r2, z5 + Z_ROW * i, i, u0, u1, u2);
+            }
         }
     }
     ux += T(INV_FOUR_PI) * u0;
@@ -534,7 +590,27 @@ __device__ __forceinline__ void far_eval(T rx, T ry, T rz, const T *f, int order
     uz += T(INV_FOUR_PI) * u2;
 }
 
-// far_eval<float> reading the packed records (Far32: 12 float4, Far32x: 16 float4, Far32y: 28 float4) in vector
+// The fifth-order part on the unit vector n (FP32, record z5 of 42 float4), added to p5: a call of its own, so that its
+// 56-float rows do not raise the register count of the kernels that inline far_eval32v.
+static __device__ __noinline__ void far_order5_unit(float nx, float ny, float nz, const float4 *z5, float *p5) {
+    float u0 = 0.f, u1 = 0.f, u2 = 0.f;
+#pragma unroll 1
+    for (int i = 0; i < 3; ++i) {
+        float h[Z_ROW];
+#pragma unroll
+        for (int q = 0; q < Z_ROW / 4; ++q) {
+            const float4 x = __ldg(z5 + (Z_ROW / 4) * i + q);
+            h[4 * q] = x.x; h[4 * q + 1] = x.y; h[4 * q + 2] = x.z; h[4 * q + 3] = x.w;
+        }
+        far_term5_row<float>(nx, ny, nz, 1.0f, 1.0f, 1.0f, 1.0f, h, i, u0, u1, u2);
+    }
+    p5[0] += u0;
+    p5[1] += u1;
+    p5[2] += u2;
+}
+
+// far_eval<float> reading the packed records (Far32: 12 float4, Far32x: 16 float4, Far32y: 28 float4, Far32z: 42
+// float4) in vector
 // loads, one group at a time where it is used, so that only one order's coefficients are live at once.  The terms are
 // those of far_eval written on the unit vector n = R / r: the order-p term is r^-(p+2) times a combination of the
 // order-p coefficients and powers of n (R^k = r^k n^k), summed by Horner's rule in 1/r, so no intermediate carries a
@@ -542,7 +618,7 @@ __device__ __forceinline__ void far_eval(T rx, T ry, T rz, const T *f, int order
 // ~3e3 in the caller's units; here from ~1e-6 to ~1e6 every intermediate stays normal).
 __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const float4 *f, int order, float &ux,
                                             float &uy, float &uz, const float4 *g = nullptr,
-                                            const float4 *k4 = nullptr) {
+                                            const float4 *k4 = nullptr, const float4 *z5 = nullptr) {
     const float r2 = rx * rx + ry * ry + rz * rz;
     // 1/r from the hardware estimate and one Newton-Raphson step for x^(-1/2) (y <- y (3 - x y^2) / 2): no IEEE
     // division or square root on this path
@@ -551,7 +627,7 @@ __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const 
     const float nx = rx * ir, ny = ry * ir, nz = rz * ir;
     // order-p parts v_p (dimensionless in r); u = r^-2 (v0 + r^-1 (v1 + r^-1 (v2 + ...)))
     float p0[3] = {0.f, 0.f, 0.f}, p1[3] = {0.f, 0.f, 0.f}, p2[3] = {0.f, 0.f, 0.f}, p3[3] = {0.f, 0.f, 0.f},
-          p4[3] = {0.f, 0.f, 0.f};
+          p4[3] = {0.f, 0.f, 0.f}, p5[3] = {0.f, 0.f, 0.f};
     const float4 q0 = __ldg(f);  // m0 x y z, m1[0]
     p0[0] = q0.y * nz - q0.z * ny;
     p0[1] = q0.z * nx - q0.x * nz;
@@ -621,6 +697,7 @@ __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const 
                         }
                         far_term4_row<float>(nx, ny, nz, 1.0f, 1.0f, 1.0f, h, i, p4[0], p4[1], p4[2]);
                     }
+                    if (order >= 5) far_order5_unit(nx, ny, nz, z5, p5);
                 }
             }
         }
@@ -628,7 +705,7 @@ __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const 
     const float scale = (float)INV_FOUR_PI * ir * ir;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const float v = p0[c] + ir * (p1[c] + ir * (p2[c] + ir * (p3[c] + ir * p4[c])));
+        const float v = p0[c] + ir * (p1[c] + ir * (p2[c] + ir * (p3[c] + ir * (p4[c] + ir * p5[c]))));
         if (c == 0) ux += scale * v;
         else if (c == 1) uy += scale * v;
         else uz += scale * v;

@@ -35,9 +35,11 @@ struct bs_tree {
     bs::Far32 *far32 = nullptr;
     bs::Far64x *far64x = nullptr;  // third-order records (trees built for order 3 only)
     bs::Far32x *far32x = nullptr;
-    bs::Far64y *far64y = nullptr;  // fourth-order records (trees built for order 4 only)
+    bs::Far64y *far64y = nullptr;  // fourth-order records (trees built for order 4 or 5 only)
     bs::Far32y *far32y = nullptr;
-    int order3 = 0, order4 = 0;
+    bs::Far64z *far64z = nullptr;  // fifth-order records (trees built for order 5 only)
+    bs::Far32z *far32z = nullptr;
+    int order3 = 0, order4 = 0, order5 = 0;
     bool geo_sorted = false;  // the build's segment geometry (SegGeo) is in tree order (Morton trees)
     bs::Seg64 *seg64 = nullptr;  // tree order
     bs::Seg32 *seg32 = nullptr;  // tree order

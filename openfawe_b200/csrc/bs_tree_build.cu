@@ -27,6 +27,7 @@ constexpr int MOM_THREADS = 256;
 constexpr int MOM_PARTS = 31;   // r2 + m0 (3) + m1 (9) + m2 symmetric (18)
 constexpr int MOM_PARTS3 = 61;  // ... + m3 symmetric (30), for third-order trees
 constexpr int MOM_PARTS4 = 106; // ... + m4 symmetric (45), for fourth-order trees
+constexpr int MOM_PARTS5 = 169; // ... + m5 symmetric (63), for fifth-order trees
 
 __device__ __forceinline__ uint64_t ordered_bits(double x) {
     uint64_t b = (uint64_t)__double_as_longlong(x + 0.0);  // -0.0 -> +0.0 (equal keys compare equal)
@@ -947,6 +948,8 @@ struct NodeOut {
     Far32x *far32x;
     Far64y *far64y;
     Far32y *far32y;
+    Far64z *far64z;
+    Far32z *far32z;
 };
 
 // Node j from its sums v (bound^2, m0, m1, symmetric m2 [, symmetric m3 [, symmetric m4]]) about its centre: the
@@ -1027,7 +1030,7 @@ __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
         for (int q = 0; q < 3; ++q) h[H_W3V + q] = (float)g[G_W3V + q];
         for (int q = 0; q < 64; ++q) far32x[j].v[q] = h[q];
     }
-    if (PARTS == MOM_PARTS4) {
+    if (PARTS >= MOM_PARTS4) {
         const double *M4 = v + 61;  // M4[15 b + sym4(j, k, l, m)]
         double T4[3][6];            // T4[b][(l, m)] = M4[b][j][j][l][m]
         for (int b4 = 0; b4 < 3; ++b4)
@@ -1061,6 +1064,47 @@ __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
         for (int q = 3 * K_ROW; q < 112; ++q) {
             o.far64y[j].v[q] = 0.0;
             o.far32y[j].v[q] = 0.f;
+        }
+    }
+    if (PARTS == MOM_PARTS5) {
+        // symmetric tensors by index counts (c0, c1, c2): rank among the order-n tuples in storage order
+        auto rank = [](int n, int c0, int c1) { return (n - c0) * (n - c0 + 1) / 2 + (n - c0 - c1); };
+        const double *M5 = v + 106;  // M5[21 b + rank(5, ...)]
+        auto m5 = [&](int b5, int c0, int c1) { return M5[21 * b5 + rank(5, c0, c1)]; };
+        // T5[b][3-tuple] = sum_j M5[b][j j + tuple]; TT5[b][k] = sum_j T5[b][j j k]
+        double T5[3][10], TT5[3][3];
+        for (int b5 = 0; b5 < 3; ++b5) {
+            int q = 0;
+            for (int c0 = 3; c0 >= 0; --c0)
+                for (int c1 = 3 - c0; c1 >= 0; --c1, ++q)
+                    T5[b5][q] = m5(b5, c0 + 2, c1) + m5(b5, c0, c1 + 2) + m5(b5, c0, c1);
+            for (int k = 0; k < 3; ++k) {
+                const int k0 = k == 0, k1 = k == 1;
+                // T5 tuple with counts (2 + k0, k1, ...), (k0, 2 + k1, ...), (k0, k1, ...) + 2 on z
+                TT5[b5][k] = T5[b5][rank(3, 2 + k0, k1)] + T5[b5][rank(3, k0, 2 + k1)] + T5[b5][rank(3, k0, k1)];
+            }
+        }
+        auto t5 = [&](int b5, int c0, int c1) { return T5[b5][rank(3, c0, c1)]; };
+        for (int i = 0; i < 3; ++i) {
+            const int b5 = (i + 1) % 3, c5 = (i + 2) % 3;  // eps_ibc X[b][c] = X[b5][c5] - X[c5][b5]
+            const int e0b = c5 == 0, e1b = c5 == 1, e0c = b5 == 0, e1c = b5 == 1;  // count shifts of index c5 / b5
+            double row[Z_ROW];
+            for (int q = 0; q < 21; ++q) row[Z_M5 + q] = M5[21 * i + q];
+            for (int q = 0; q < 10; ++q) row[Z_T5 + q] = T5[i][q];
+            for (int k = 0; k < 3; ++k) row[Z_TT5 + k] = TT5[i][k];
+            int q = 0;
+            for (int c0 = 4; c0 >= 0; --c0)  // W5 over the 4-tuples
+                for (int c1 = 4 - c0; c1 >= 0; --c1, ++q)
+                    row[Z_W5 + q] = m5(b5, c0 + e0b, c1 + e1b) - m5(c5, c0 + e0c, c1 + e1c);
+            q = 0;
+            for (int c0 = 2; c0 >= 0; --c0)  // W5T over the 2-tuples
+                for (int c1 = 2 - c0; c1 >= 0; --c1, ++q)
+                    row[Z_W5T + q] = t5(b5, c0 + e0b, c1 + e1b) - t5(c5, c0 + e0c, c1 + e1c);
+            row[Z_W5TT] = TT5[b5][c5] - TT5[c5][b5];
+            for (int k = 0; k < Z_ROW; ++k) {
+                o.far64z[j].v[Z_ROW * i + k] = row[k];
+                o.far32z[j].v[Z_ROW * i + k] = (float)row[k];
+            }
         }
     }
     if (RECORDS) nodes[j] = node_record(j, b, centre, core, lo, hi, left, right);
@@ -1113,24 +1157,27 @@ __global__ void parent_kernel(int64_t count, const int64_t *left, const int64_t 
     }
 }
 
-// The symmetric index tuples of orders 0..4 in storage order (order, then lexicographic): (), 0, 1, 2, 00, 01, ..., 2222
-// -- 1 + 3 + 6 + 10 + 15 = 35.  Moment (i; tuple of order n, rank r among the order-n tuples) is stored at
+// The symmetric index tuples of orders 0..5 in storage order (order, then lexicographic): (), 0, 1, 2, 00, 01, ...,
+// 22222 -- 1 + 3 + 6 + 10 + 15 + 21 = 56.  Moment (i; tuple of order n, rank r among the order-n tuples) is stored at
 // T_BASE[n] + T_CNT[n] i + r of a node's sums (index 0 holds bound^2).  src[u][mask]: where the tuple left after
 // removing the positions in `mask` from tuple u is stored (T_BASE + rank, plus T_CNT << 8).
-constexpr int T_FIRST[5] = {0, 1, 4, 10, 20}, T_BASE[5] = {1, 4, 13, 31, 61}, T_CNT[5] = {1, 3, 6, 10, 15};
+constexpr int N_TUPLES = 56;
+constexpr int T_FIRST[6] = {0, 1, 4, 10, 20, 35}, T_BASE[6] = {1, 4, 13, 31, 61, 106},
+              T_CNT[6] = {1, 3, 6, 10, 15, 21};
 struct TupleTables {
-    unsigned char n[35], packed[35];  // order and indices (two bits each, first index in the low bits)
-    unsigned char out0[35], cnt[35];  // moment (i; u) is stored at out0[u] + cnt[u] i
-    unsigned short src[35][16];
+    unsigned char n[N_TUPLES];
+    unsigned short packed[N_TUPLES];                // indices, two bits each, first index in the low bits
+    unsigned char out0[N_TUPLES], cnt[N_TUPLES];    // moment (i; u) is stored at out0[u] + cnt[u] i
+    unsigned short src[N_TUPLES][32];
 };
 constexpr TupleTables make_tuple_tables() {
     TupleTables t{};
     int u = 0;
-    for (int n = 0; n <= 4; ++n) {
+    for (int n = 0; n <= 5; ++n) {
         int codes = 1;
         for (int k = 0; k < n; ++k) codes *= 3;
         for (int code = 0; code < codes; ++code) {  // base-3 codes, first index most significant: lexicographic
-            int dig[4] = {0, 0, 0, 0}, c = code;
+            int dig[5] = {0, 0, 0, 0, 0}, c = code;
             for (int s = n - 1; s >= 0; --s) { dig[s] = c % 3; c /= 3; }
             bool sorted = true;
             for (int s = 1; s < n; ++s) sorted = sorted && dig[s - 1] <= dig[s];
@@ -1138,13 +1185,13 @@ constexpr TupleTables make_tuple_tables() {
             int pk = 0;
             for (int s = 0; s < n; ++s) pk |= dig[s] << (2 * s);
             t.n[u] = (unsigned char)n;
-            t.packed[u] = (unsigned char)pk;
+            t.packed[u] = (unsigned short)pk;
             t.out0[u] = (unsigned char)(T_BASE[n] + u - T_FIRST[n]);
             t.cnt[u] = (unsigned char)T_CNT[n];
             ++u;
         }
     }
-    for (int v = 0; v < 35; ++v) {
+    for (int v = 0; v < N_TUPLES; ++v) {
         const int n = t.n[v];
         for (int mask = 0; mask < (1 << n); ++mask) {
             int rest = 0, m = 0;
@@ -1161,8 +1208,9 @@ __constant__ TupleTables c_tt = make_tuple_tables();
 
 template <int PARTS>
 struct MomentTuples {
-    static constexpr int n = PARTS == MOM_PARTS ? 10 : (PARTS == MOM_PARTS3 ? 20 : 35);  // tuples up to the order
-    static constexpr int slots = (n + 31) / 32;                                         // tuples per lane
+    static constexpr int n = PARTS == MOM_PARTS ? 10 : (PARTS == MOM_PARTS3 ? 20 : (PARTS == MOM_PARTS4 ? 35 : 56));
+    static constexpr int slots = (n + 31) / 32;  // tuples per lane
+    static constexpr int order = PARTS == MOM_PARTS ? 2 : (PARTS == MOM_PARTS3 ? 3 : (PARTS == MOM_PARTS4 ? 4 : 5));
 };
 
 // Storage index of moment (i; tuple u).
@@ -1236,7 +1284,9 @@ __global__ void __launch_bounds__(128) leaf_geometry_kernel(const int32_t *leave
 
 // <rho_a1 .. rho_an> over one segment for the index tuples u < NT in storage order, rho = d + t l with t uniform on
 // [-1/2, 1/2] (<t^2> = 1/12, <t^4> = 1/80, odd moments 0): m2 takes d d + l l / 12, m3 d d d + (d l l + l d l +
-// l l d) / 12, m4 d d d d + (the six placements of two l's) / 12 + l l l l / 80.
+// l l d) / 12, m4 d d d d + (the six placements of two l's) / 12 + l l l l / 80.  The order-5 means (NT = 56) come
+// from the three-point Gauss-Legendre rule on [-1/2, 1/2] (nodes 0 and +-sqrt(3/5)/2, weights 8/18 and 5/18), exact
+// for polynomials in t of degree 5: sum over the nodes of weight times the degree-5 monomials of rho.
 template <int NT>
 __device__ __forceinline__ void segment_means(const double *d, const double *l, double *g) {
     double dd[3][3], ll[3][3];
@@ -1277,20 +1327,48 @@ __device__ __forceinline__ void segment_means(const double *d, const double *l, 
                         g[u++] = dd[a][b] * dd[c][e] + pairs * (1.0 / 12.0) + ll[a][b] * ll[c][e] * (1.0 / 80.0);
                     }
     }
+    if (NT > 35) {
+        constexpr double tg = 0.3872983346207417;  // sqrt(3/5) / 2
+        const double wt[3] = {8.0 / 18.0, 5.0 / 18.0, 5.0 / 18.0}, tt[3] = {0.0, tg, -tg};
+        double m5[21];
+#pragma unroll
+        for (int q = 0; q < 21; ++q) m5[q] = 0.0;
+#pragma unroll
+        for (int gp = 0; gp < 3; ++gp) {
+            const double r0 = fma(tt[gp], l[0], d[0]), r1 = fma(tt[gp], l[1], d[1]), r2 = fma(tt[gp], l[2], d[2]);
+            const double x2 = r0 * r0, xy = r0 * r1, xz = r0 * r2, y2 = r1 * r1, yz = r1 * r2, z2 = r2 * r2;
+            const double c3[10] = {x2 * r0, x2 * r1, x2 * r2, xy * r1, xy * r2, xz * r2, y2 * r1, y2 * r2, yz * r2,
+                                   z2 * r2};
+            // lexicographic degree-5 tuples: (c0, c1, c2) = (5,0,0), (4,1,0), ..., (0,0,5) as x^c0 y^c1 z^c2
+            const double v[21] = {x2 * c3[0], x2 * c3[1], x2 * c3[2], x2 * c3[3], x2 * c3[4], x2 * c3[5], x2 * c3[6],
+                                  x2 * c3[7], x2 * c3[8], x2 * c3[9], xy * c3[6], xy * c3[7], xy * c3[8], xy * c3[9],
+                                  xz * c3[9], y2 * c3[6], y2 * c3[7], y2 * c3[8], y2 * c3[9], yz * c3[9], z2 * c3[9]};
+#pragma unroll
+            for (int q = 0; q < 21; ++q) m5[q] = fma(wt[gp], v[q], m5[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < 21; ++q) g[u++] = m5[q];
+    }
 }
+
+// Warps per block of leaf_moments_kernel (its staging takes (tuples + 3) x 33 doubles a warp).
+template <int PARTS>
+constexpr int leaf_warps() { return PARTS == MOM_PARTS5 ? 2 : 4; }
 
 // One warp per leaf: the moments about the leaf's centre; sums[j][PARTS] (sums[j][0] unused).  The warp takes 32
 // segments at a time: each lane forms its segment's means (segment_means) and alpha = gamma l into shared memory,
 // then lane u sums, over the 32, alpha_i times the mean of index tuple u (and of u + 32) for i = 0..2.
 template <int PARTS>
-__global__ void __launch_bounds__(128) leaf_moments_kernel(const int32_t *leaves, const unsigned *nleaves,
-                                                           const int64_t *lo, const int64_t *hi,
-                                                           const int32_t *order, const SegGeo *geo,
-                                                           const double *centre, double *sums) {
+__global__ void __launch_bounds__(32 * leaf_warps<PARTS>()) leaf_moments_kernel(const int32_t *leaves,
+                                                                              const unsigned *nleaves,
+                                                                              const int64_t *lo, const int64_t *hi,
+                                                                              const int32_t *order, const SegGeo *geo,
+                                                                              const double *centre, double *sums) {
     using MT = MomentTuples<PARTS>;
     constexpr int ROWS = MT::n + 3, STRIDE = 33;  // means, then alpha; padded rows: lanes of a column hit other banks
-    __shared__ double st[4][ROWS * STRIDE];
-    const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 3;
+    constexpr int LW = leaf_warps<PARTS>();
+    __shared__ double st[LW][ROWS * STRIDE];
+    const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) % LW;
     double *sw = st[w];
     bool own[MT::slots];
 #pragma unroll
@@ -1389,24 +1467,32 @@ __global__ void __launch_bounds__(128) bottom_up_kernel(const int32_t *leaves, c
                                                         const int2 *up, unsigned *arrive, const double *centre,
                                                         double *sums) {
     using MT = MomentTuples<PARTS>;
+    constexpr int MAXM = 1 << MT::order;  // subset masks of the highest order
     __shared__ double sm[4][2][PARTS];
-    __shared__ unsigned short src[16][MT::n];  // by mask, then tuple: the lanes of one mask read adjacent entries
-    for (int q = threadIdx.x; q < MT::n * 16; q += blockDim.x) src[q & 15][q >> 4] = c_tt.src[q >> 4][q & 15];
+    __shared__ unsigned short src[MAXM][MT::n];  // by mask, then tuple: the lanes of one mask read adjacent entries
+    for (int q = threadIdx.x; q < MT::n * MAXM; q += blockDim.x) src[q % MAXM][q / MAXM] = c_tt.src[q / MAXM][q % MAXM];
     __syncthreads();
     const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 3;
-    // lane's tuple in each slot: with two slots (fourth-order trees) slot 0 holds the first order-1 tuple and the 31 of
-    // orders 2-4, slot 1 the order-0 tuple and the other two of order 1, so that slot 1 runs two subset masks, not 16
+    // lane's tuple in each slot, so that slot 1 runs few subset masks: fourth-order trees put the first order-1 tuple
+    // and the 31 of orders 2-4 in slot 0, the order-0 tuple and the other two of order 1 in slot 1 (two masks);
+    // fifth-order trees the 21 tuples of order 5 and the last 11 of order 4 in slot 0, the other 24 in slot 1 (16)
     int tu[MT::slots], tn[MT::slots], tp[MT::slots];
 #pragma unroll
     for (int r = 0; r < MT::slots; ++r) {
-        const int u = MT::slots == 1 ? lane : (r == 0 ? (lane == 0 ? 1 : lane + 3) : (lane == 0 ? 0 : lane + 1));
-        const bool ok = MT::slots == 1 ? u < MT::n : (r == 0 || lane < 3);
+        int u = lane;
+        bool ok = u < MT::n;
+        if (MT::n == 35) {
+            u = r == 0 ? (lane == 0 ? 1 : lane + 3) : (lane == 0 ? 0 : lane + 1);
+            ok = r == 0 || lane < 3;
+        } else if (MT::n == 56) {
+            u = r == 0 ? (lane < 21 ? 35 + lane : lane + 3) : lane;
+            ok = r == 0 || lane < 24;
+        }
         tu[r] = u;
         tn[r] = ok ? c_tt.n[u] : -1;
         tp[r] = ok ? c_tt.packed[u] : 0;
     }
-    // subset masks of a slot: 2^(largest order in it)
-    constexpr int MAXM = PARTS >= MOM_PARTS4 ? 16 : (PARTS >= MOM_PARTS3 ? 8 : 4);
+    constexpr int SLOT1_MASKS = MT::n == 56 ? 16 : 2;
     // a grid that stays resident, so that every leaf's climb starts at once (more leaves than resident warps: a warp
     // takes them one after another)
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5), n = *nleaves;
@@ -1454,25 +1540,27 @@ __global__ void __launch_bounds__(128) bottom_up_kernel(const int32_t *leaves, c
         for (int q = 0; q < MT::slots; ++q) {
             acc[q][0] = acc[q][1] = acc[q][2] = 0.0;
             if (tn[q] < 0) continue;
-            const int u = tu[q], masks = (MT::slots == 2 && q == 1) ? 2 : MAXM;
+            const int u = tu[q], masks = (MT::slots == 2 && q == 1) ? SLOT1_MASKS : MAXM;
 #pragma unroll
             for (int side = 0; side < 2; ++side) {
-                double Dp[4];  // D at the tuple's positions
+                constexpr int NP = MT::order;
+                double Dp[NP];  // D at the tuple's positions
 #pragma unroll
-                for (int s2 = 0; s2 < 4; ++s2) {
+                for (int s2 = 0; s2 < NP; ++s2) {
                     const int x = (tp[q] >> (2 * s2)) & 3;
                     Dp[s2] = x == 0 ? D[side][0] : (x == 1 ? D[side][1] : D[side][2]);
                 }
-                double f[16];
+                double f[MAXM];
                 f[0] = 1.0;
 #pragma unroll
-                for (int mask = 1; mask < 16; ++mask) {
-                    const int low = mask & -mask, pos = low == 1 ? 0 : (low == 2 ? 1 : (low == 4 ? 2 : 3));
+                for (int mask = 1; mask < MAXM; ++mask) {
+                    const int low = mask & -mask;
+                    const int pos = low == 1 ? 0 : (low == 2 ? 1 : (low == 4 ? 2 : (low == 8 ? 3 : 4)));
                     f[mask] = f[mask ^ low] * Dp[pos];
                 }
                 const double *sv = sm[w][side];
 #pragma unroll
-                for (int mask = 0; mask < 16; ++mask) {
+                for (int mask = 0; mask < MAXM; ++mask) {
                     if (mask < masks && mask < (1 << tn[q])) {
                         const int e = src[mask][u], o0 = e & 255, cn = e >> 8;
                         acc[q][0] = fma(f[mask], sv[o0], acc[q][0]);
@@ -1624,12 +1712,13 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
         cudaEventDestroy(geometry);
         ms = side;
     }
+    constexpr int LW = leaf_warps<PARTS>();
     int leaf_resident = 0;  // resident blocks: one wave takes as many leaves as fit
-    BS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&leaf_resident, leaf_moments_kernel<PARTS>, 128, 0));
+    BS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&leaf_resident, leaf_moments_kernel<PARTS>, 32 * LW, 0));
     const unsigned moment_blocks = (unsigned)std::max<int64_t>(
-        1, std::min<int64_t>((count + 3) / 4, (int64_t)std::max(1, leaf_resident) * sms));
-    leaf_moments_kernel<PARTS><<<moment_blocks, 128, 0, ms>>>(leaves, nleaves, t->lo, t->hi, geo_order, geo, t->centre,
-                                                              sums);
+        1, std::min<int64_t>((count + LW - 1) / LW, (int64_t)std::max(1, leaf_resident) * sms));
+    leaf_moments_kernel<PARTS><<<moment_blocks, 32 * LW, 0, ms>>>(leaves, nleaves, t->lo, t->hi, geo_order, geo,
+                                                                  t->centre, sums);
     int climb_blocks = 0;  // resident blocks: one wave holds every climbing warp
     BS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&climb_blocks, bottom_up_kernel<PARTS>, 128, 0));
     const unsigned climb_grid = (unsigned)std::max<int64_t>(
@@ -1637,7 +1726,7 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
     bottom_up_kernel<PARTS><<<climb_grid, 128, 0, ms>>>(leaves, nleaves, parent, arrive_m, t->centre, sums);
     const NodeOut out{t->lo, t->hi, t->left, t->right, t->centre, t->core, t->bound, t->m0, t->m1, t->m2,
                       t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x,
-                      t->far64y, t->far32y};
+                      t->far64y, t->far32y, t->far64z, t->far32z};
     // one warp per block: the thread per node is long, so the nodes spread over every SM
     node_final_kernel<PARTS><<<blocks_for(count, 32), 32, 0, ms>>>(count, sums, out);
     BS_CHECK_LAUNCH("bottom-up moments");
@@ -1668,10 +1757,16 @@ int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_
         t->far32y = t->alloc<Far32y>(count, s);
         if (!t->far64y || !t->far32y) return BS_ERR_OOM;
     }
+    if (t->order5) {
+        t->far64z = t->alloc<Far64z>(count, s);
+        t->far32z = t->alloc<Far32z>(count, s);
+        if (!t->far64z || !t->far32z) return BS_ERR_OOM;
+    }
     if (!t->centre || !t->bound || !t->core || !t->m0 || !t->m1 || !t->m2 || !t->w1 || !t->t2 || !t->w2 ||
         !t->nodes || !t->far64 || !t->far32)
         return BS_ERR_OOM;
     // fourth order: the bottom-up pipeline for every kind (its box, centre and bound equal the direct sums')
+    if (t->order5) return moments_bottom_up<MOM_PARTS5>(t, geo, scratch, s, side);
     if (t->order4) return moments_bottom_up<MOM_PARTS4>(t, geo, scratch, s, side);
     if (t->kind == BS_TREE_MORTON) return t->order3 ? moments_bottom_up<MOM_PARTS3>(t, geo, scratch, s, side)
                                                    : moments_bottom_up<MOM_PARTS>(t, geo, scratch, s, side);
@@ -1695,7 +1790,7 @@ int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_
     moment_centre_kernel<<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, box, t->centre, t->core);
     const NodeOut out{t->lo, t->hi, t->left, t->right, t->centre, t->core, t->bound, t->m0, t->m1, t->m2,
                       t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x,
-                      t->far64y, t->far32y};
+                      t->far64y, t->far32y, t->far64z, t->far32z};
     if (t->order3) {
         moment_sum_kernel<MOM_PARTS3><<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, t->centre, sums);
         moment_final_kernel<MOM_PARTS3><<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, sums, out);
@@ -1799,6 +1894,7 @@ int tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_
     t->leaf_size = tp->leaf_size;
     t->order3 = tp->order >= 3;
     t->order4 = tp->order >= 4;
+    t->order5 = tp->order >= 5;
     // the moment phase of the bottom-up pipeline (Morton trees, fourth-order trees) may run on the side stream
     cudaStream_t defer = (side && (t->order4 || t->kind == BS_TREE_MORTON)) ? side : nullptr;
     {
@@ -1897,6 +1993,7 @@ extern "C" int bs_forest_build(bs_ctx *ctx, const bs_sources *src, int nwakes, c
     t->leaf_size = tp->leaf_size;
     t->order3 = tp->order >= 3;
     t->order4 = tp->order >= 4;
+    t->order5 = tp->order >= 5;
     {
         Scratch scratch(ctx->pool, s);
         SegGeo *geo = scratch.get<SegGeo>(src->m);

@@ -36,6 +36,8 @@ struct TreeView {
     const Far32x *far32x;
     const Far64y *far64y;  // fourth-order records, or null
     const Far32y *far32y;
+    const Far64z *far64z;  // fifth-order records, or null
+    const Far32z *far32z;
     const Seg64 *seg64;
     const Seg32 *seg32;
     const Seg32x2 *seg32x2;
@@ -118,13 +120,15 @@ __device__ __forceinline__ void far_node(const EvalArgs &a, const Target &t, int
     if (PREC == 0) {
         double g0 = 0.0, g1 = 0.0, g2 = 0.0;
         far_eval<double>(rx, ry, rz, a.tv.far64[node].v, a.order, g0, g1, g2,
-                         a.order >= 3 ? a.tv.far64x[node].v : nullptr, a.order >= 4 ? a.tv.far64y[node].v : nullptr);
+                         a.order >= 3 ? a.tv.far64x[node].v : nullptr, a.order >= 4 ? a.tv.far64y[node].v : nullptr,
+                         a.order >= 5 ? a.tv.far64z[node].v : nullptr);
         acc.add64(g0, g1, g2);
     } else {
         float g0 = 0.f, g1 = 0.f, g2 = 0.f;
         far_eval32v((float)rx, (float)ry, (float)rz, reinterpret_cast<const float4 *>(a.tv.far32[node].v), a.order,
                     g0, g1, g2, a.order >= 3 ? reinterpret_cast<const float4 *>(a.tv.far32x[node].v) : nullptr,
-                    a.order >= 4 ? reinterpret_cast<const float4 *>(a.tv.far32y[node].v) : nullptr);
+                    a.order >= 4 ? reinterpret_cast<const float4 *>(a.tv.far32y[node].v) : nullptr,
+                    a.order >= 5 ? reinterpret_cast<const float4 *>(a.tv.far32z[node].v) : nullptr);
         acc.add32(g0, g1, g2);
     }
 }
@@ -834,11 +838,11 @@ int check_eval_args(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params
         set_error("tree evaluation: null argument");
         return BS_ERR_ARG;
     }
-    if (!(tp->theta > 0.0 && tp->theta < 1.0) || tp->order < 0 || tp->order > 4 || !(tp->clearance >= 0.0)) {
-        set_error("tree evaluation: theta must lie in (0, 1), order in 0..4, clearance >= 0");
+    if (!(tp->theta > 0.0 && tp->theta < 1.0) || tp->order < 0 || tp->order > 5 || !(tp->clearance >= 0.0)) {
+        set_error("tree evaluation: theta must lie in (0, 1), order in 0..5, clearance >= 0");
         return BS_ERR_ARG;
     }
-    if ((tp->order == 3 && !tree->order3) || (tp->order == 4 && !tree->order4)) {
+    if ((tp->order == 3 && !tree->order3) || (tp->order == 4 && !tree->order4) || (tp->order == 5 && !tree->order5)) {
         set_error("tree evaluation: order %d needs a tree built with order %d (its moments)", tp->order, tp->order);
         return BS_ERR_ARG;
     }
@@ -928,7 +932,8 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     args.ex_ptr = ex_pos ? tgt->ex_ptr : nullptr;
     args.ex_pos = ex_pos;
     args.tv = TreeView{tree->nodes,  tree->far64,  tree->far32, tree->far64x, tree->far32x,
-                       tree->far64y, tree->far32y, tree->seg64, tree->seg32, tree->seg32x2};
+                       tree->far64y, tree->far32y, tree->far64z, tree->far32z, tree->seg64, tree->seg32,
+                       tree->seg32x2};
     args.theta = tp->theta;
     args.theta2 = tp->theta * tp->theta;
     args.clearance = tp->clearance;

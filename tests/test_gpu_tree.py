@@ -299,6 +299,75 @@ def test_fourth_order_expansion_converges_one_order_faster_again(device):
                          theta=0.1, order=4)
 
 
+def test_fifth_order_expansion_converges_one_order_faster_again(device):
+    """Order 5 (the fifth moments, an extension beyond the reference's orders 0-2; its means come from the three-point
+    Gauss-Legendre rule, exact for degree 5).  One cluster of segments seen from b/r = 0.3, 0.2, 1/4, 1/8 (the root
+    accepted): from order 1 on, each order's relative error falls by about b/r (at most 1.5 b/r), the mixed far field
+    agrees with FP64 to 1e-6 of the field, and a tree of 3-segment leaves (the root's moments translated up from ten leaves) gives the same field as a single leaf.  On the
+    rotor sheet without cores (a far node's expansion is that of singular segments: with cores, the far field differs
+    from the regularised pairs by an order-independent amount that would hide the comparison): below order 4 at each
+    opening angle, shrinking ~theta^6, Morton and median; a fifth-order tree evaluated at order 4 matches a
+    fourth-order tree."""
+    from openfawe_b200 import engine, wakes
+    rng = np.random.default_rng(3)
+    m = 30
+    starts = rng.normal(scale=0.3, size=(m, 3))
+    d = rng.normal(size=(m, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    lengths, gamma, radius = 0.05 + 0.2 * rng.random(m), rng.normal(size=m), np.zeros(m)
+    ends = starts + d * lengths[:, None]
+    c = 0.5 * (np.minimum(starts, ends).min(0) + np.maximum(starts, ends).max(0))
+    b = np.sqrt(np.max(np.sum((np.vstack([starts, ends]) - c) ** 2, axis=1)))
+    direction = np.array([0.3, -0.7, 0.5]) / np.linalg.norm([0.3, -0.7, 0.5])
+    ratios = np.array([0.3, 0.2, 0.25, 0.125])
+    pts = c + (b / ratios)[:, None] * direction
+    exact = np.array([(O.pair_matrix(p[None], starts, d, lengths, radius, 0, False)[0][0] * gamma[:, None]).sum(0)
+                      for p in pts])
+    src = engine.Sources(starts, d, lengths, gamma, radius, device)
+    tgt = engine.Targets(pts, None, device)
+    for kind in ("morton", "median"):
+        fields = {}
+        for leaf in (64, 3):
+            tree = engine.build_tree(src, leaf_size=leaf, kind=kind, order=5)
+            err = []
+            for order in range(6):
+                u, _, far = engine.tree_eval(tree, tgt, 0, "zero", "fp64", theta=0.5, order=order, clearance=0.0)
+                assert np.array_equal(far.cpu().numpy(), np.ones(4)), (kind, leaf)
+                fields[leaf, order] = u.cpu().numpy()
+                err.append(np.linalg.norm(fields[leaf, order] - exact, axis=1) / np.linalg.norm(exact, axis=1))
+                # the single-precision far field (on the unit vector) agrees with FP64 to FP32 rounding
+                um, _, _ = engine.tree_eval(tree, tgt, 0, "zero", "mixed", theta=0.5, order=order, clearance=0.0)
+                gap = np.linalg.norm(um.cpu().numpy() - fields[leaf, order], axis=1) / np.linalg.norm(exact, axis=1)
+                assert np.all(gap < 1e-6), (kind, leaf, order, gap)
+            assert np.all(err[1] < err[0]), (kind, leaf, err)
+            for order in range(1, 5):
+                assert np.all(err[order + 1] < 1.5 * ratios * err[order]), (kind, leaf, order, err)
+        for order in range(6):
+            np.testing.assert_allclose(fields[3, order], fields[64, order], rtol=1e-10, atol=0)
+    case = wakes.rotor_sheet(120, seed=9, targets=4000)
+    args = wakes.backend_args(case)
+    src = engine.Sources(*args[1:5], np.zeros(len(args[4])), device)
+    tgt = engine.Targets(case["points"], None, device)
+    direct, _ = engine.direct(src, tgt, 0, "zero", "fp64")
+    direct = direct.cpu().numpy()
+    rel = lambda u: np.linalg.norm(u.cpu().numpy() - direct) / np.linalg.norm(direct)
+    for kind in ("morton", "median"):
+        err = {}
+        trees = {order: engine.build_tree(src, leaf_size=16, kind=kind, order=order) for order in (4, 5)}
+        for order in (4, 5):
+            for theta in (0.1, 0.2):
+                u, _, _ = engine.tree_eval(trees[order], tgt, 0, "zero", "fp64", theta=theta, order=order)
+                err[order, theta] = rel(u)
+        for theta in (0.1, 0.2):
+            assert err[5, theta] < 0.5 * err[4, theta], (kind, err)
+        assert err[5, 0.2] / err[5, 0.1] > 20.0, (kind, err)
+        u4, _, _ = engine.tree_eval(trees[5], tgt, 0, "zero", "fp64", theta=0.2, order=4)
+        assert abs(rel(u4) - err[4, 0.2]) <= 1e-3 * err[4, 0.2], (kind, rel(u4), err[4, 0.2])
+    with pytest.raises(ValueError):
+        engine.tree_eval(engine.build_tree(src, leaf_size=16, kind="morton", order=4), tgt, 2, "raise", "fp64",
+                         theta=0.1, order=5)
+
+
 def test_morton_bottom_up_moments_against_direct_node_sums(device):
     """Morton trees and forests take their node moments bottom-up (leaves summed, parents translated from their
     children): box, centre, core and bounding radius equal the direct per-node computation bit for bit, the moments
@@ -433,7 +502,7 @@ def test_tree_sum_from_host_arrays_equals_device_call(device):
 def test_mixed_tree_far_field_at_any_length_scale(device):
     """The single-precision far field is formed on the unit vector with one power of 1/r per order, so the same wake
     at 1e-4, 1 and 1e4 times its size (cores scaled with it) gives the same relative error against the FP64 direct sum
-    at orders 2 and 4 (r^-11 itself would leave FP32's range at both ends)."""
+    at orders 2, 4 and 5 (r^-13 itself would leave FP32's range at both ends)."""
     from openfawe_b200 import engine, wakes
     case = wakes.rotor_sheet(40, seed=21, targets=1500)
     args = wakes.backend_args(case)
@@ -444,11 +513,11 @@ def test_mixed_tree_far_field_at_any_length_scale(device):
         tgt = engine.Targets(pts, None, device)
         direct, _ = engine.direct(src, tgt, 2, "raise", "fp64")
         direct = direct.cpu().numpy()
-        for order in (2, 4):
+        for order in (2, 4, 5):
             u, flags, _ = engine.tree_sum(src, tgt, 2, "raise", "mixed", 128, 3.0, 0.3, order, 32, 3.0, "morton")
             u = u.cpu().numpy()
             assert np.all(np.isfinite(u)) and not flags.cpu().numpy().any(), (scale, order)
             errs[scale, order] = np.linalg.norm(u - direct) / np.linalg.norm(direct)
-    for order in (2, 4):
+    for order in (2, 4, 5):
         for scale in (1e-4, 1e4):
             assert errs[scale, order] <= 1.1 * errs[1.0, order] + 1e-7, errs
