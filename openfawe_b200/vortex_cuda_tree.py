@@ -43,8 +43,8 @@ def cuda_tree_sum(points, starts, directions, lengths, gamma, radius, model, csr
                   targets_per_launch=None, stack_size=STACK, block=None, order=None):
     """Return (velocity, any_flag) like ``vortex_tree.tree_sum`` for the same inputs, evaluated on the GPU.
 
-    ``order`` (keyword, not in the reference) overrides ``tree.order``; 3 and 4 select the third- and fourth-order far
-    fields, which reach the accuracy of order 2 at larger opening angles."""
+    ``order`` (keyword, not in the reference) overrides ``tree.order``; 3, 4 and 5 select the third- to fifth-order
+    far fields, which reach the accuracy of order 2 at larger opening angles."""
     if not VC.available():
         raise ValueError(f"the cuda tree evaluation needs a CUDA device ({VC.probe_error()})")
     if int(model) not in SUPPORTED_MODELS and np.any(np.asarray(radius) > 0):
@@ -57,8 +57,8 @@ def cuda_tree_sum(points, starts, directions, lengths, gamma, radius, model, csr
         raise ValueError("suspect='gpu64' is for the single precisions only")
     block = int(settings.block if block is None else block)
     expansion = int(tree.order if order is None else order)
-    if expansion not in (0, 1, 2, 3, 4):
-        raise ValueError("tree order must be 0, 1, 2, 3 or 4")
+    if expansion not in (0, 1, 2, 3, 4, 5):
+        raise ValueError("tree order must be 0, 1, 2, 3, 4 or 5")
     _, _, near = VC._check_settings(settings)
     kind = getattr(settings, "tree", "median")
     points = np.ascontiguousarray(points, dtype=np.float64)
