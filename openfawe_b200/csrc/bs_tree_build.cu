@@ -952,19 +952,29 @@ struct NodeOut {
     Far32z *far32z;
 };
 
-// Node j from its sums v (bound^2, m0, m1, symmetric m2 [, symmetric m3 [, symmetric m4]]) about its centre: the
-// export arrays, the contractions and the packed far records, and with RECORDS the bounding radius and the traversal
-// record (the bottom-up pipeline writes those two earlier, in node_rec_kernel, and leaves v[0] unused).
-template <int PARTS, bool RECORDS = true>
-__device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
+// A record's n values (n even; 16-byte aligned destinations) in FP64 and FP32: 16-byte stores, so that a thread
+// writing one node's records issues a quarter to a half of the scalar stores.
+__device__ __forceinline__ void store_pair(double *d64, float *d32, const double *v, int n) {
+    for (int q = 0; q < n; q += 2) reinterpret_cast<double2 *>(d64)[q / 2] = make_double2(v[q], v[q + 1]);
+    int q = 0;
+    for (; q + 4 <= n; q += 4)
+        reinterpret_cast<float4 *>(d32)[q / 4] = make_float4((float)v[q], (float)v[q + 1], (float)v[q + 2], (float)v[q + 3]);
+    for (; q < n; ++q) d32[q] = (float)v[q];
+}
+
+// Node j from its sums v (bound^2, m0, m1, symmetric m2 [, symmetric m3 [, symmetric m4 [, symmetric m5]]]) about
+// its centre: the export arrays, the contractions and the packed far records, and with RECORDS the bounding radius and
+// the traversal record (the bottom-up pipeline writes those two earlier, in node_rec_kernel, and leaves v[0] unused).
+// PART -1 does all of it; PART 0 the records of orders 0-3 (and the export arrays and traversal record), PART 1-3 the
+// order-4 and order-5 rows of component PART - 1, so that four threads can share a node.
+template <int PARTS, bool RECORDS = true, int PART = -1>
+__device__ void finalize_node(int64_t j, const double *__restrict__ v, const NodeOut &o) {
     double *bound = o.bound, *m0 = o.m0, *m1 = o.m1, *m2 = o.m2, *w1 = o.w1, *t2 = o.t2, *w2 = o.w2;
     Far64 *far64 = o.far64;
     Far32 *far32 = o.far32;
     Far64x *far64x = o.far64x;
     Far32x *far32x = o.far32x;
-    const double *centre = o.centre, *core = o.core;
-    const int64_t *lo = o.lo, *hi = o.hi, *left = o.left, *right = o.right;
-    NodeRec *nodes = o.nodes;
+    if (PART <= 0) {
     const double b = sqrt(v[0]) * (1.0 + 1e-12);
     if (RECORDS) bound[j] = b;
     const double *M0 = v + 1, *M1 = v + 4, *S = v + 13;  // S[6 i + p], p over (00,01,02,11,12,22)
@@ -996,9 +1006,14 @@ __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
     for (int i = 0; i < 3; ++i) { f[F_W1 + i] = W1[i]; f[F_T2 + i] = T2[i]; }
     for (int q = 0; q < 9; ++q) f[F_W2 + q] = W2[q];
     for (int q = 0; q < 18; ++q) f[F_M2 + q] = S[q];
-    for (int q = 0; q < BS_FAR_N; ++q) {
-        far64[j].v[q] = f[q];
-        far32[j].v[q] = (float)f[q];
+    {
+        double fp[BS_FAR_N + 3];  // the records' padding as zeros (Far64: 46 doubles, Far32: 48 floats)
+        for (int q = 0; q < BS_FAR_N + 3; ++q) fp[q] = q < BS_FAR_N ? f[q] : 0.0;
+        for (int q = 0; q < BS_FAR_N + 1; q += 2)
+            reinterpret_cast<double2 *>(far64[j].v)[q / 2] = make_double2(fp[q], fp[q + 1]);
+        for (int q = 0; q < BS_FAR_N + 3; q += 4)
+            reinterpret_cast<float4 *>(far32[j].v)[q / 4] =
+                make_float4((float)fp[q], (float)fp[q + 1], (float)fp[q + 2], (float)fp[q + 3]);
     }
     if (PARTS >= MOM_PARTS3) {
         const double *M3 = v + 31;  // M3[10 b + sym3(j, k, l)]
@@ -1019,7 +1034,9 @@ __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
         g[G_W3V + 0] = T3[3 * 1 + 2] - T3[3 * 2 + 1];
         g[G_W3V + 1] = T3[3 * 2 + 0] - T3[3 * 0 + 2];
         g[G_W3V + 2] = T3[3 * 0 + 1] - T3[3 * 1 + 0];
-        for (int q = 0; q < 64; ++q) far64x[j].v[q] = q < BS_FAR3_N ? g[q] : 0.0;
+        for (int q = 0; q < 64; q += 2)
+            reinterpret_cast<double2 *>(far64x[j].v)[q / 2] =
+                make_double2(q < BS_FAR3_N ? g[q] : 0.0, q + 1 < BS_FAR3_N ? g[q + 1] : 0.0);
         float h[64];
         for (int q = 0; q < 64; ++q) h[q] = 0.f;
         for (int i = 0; i < 3; ++i) {
@@ -1028,7 +1045,9 @@ __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
             for (int q = 0; q < 6; ++q) h[H_ROW * i + H_W3 + q] = (float)g[G_W3 + 6 * i + q];
         }
         for (int q = 0; q < 3; ++q) h[H_W3V + q] = (float)g[G_W3V + q];
-        for (int q = 0; q < 64; ++q) far32x[j].v[q] = h[q];
+        for (int q = 0; q < 64; q += 4)
+            reinterpret_cast<float4 *>(far32x[j].v)[q / 4] = make_float4(h[q], h[q + 1], h[q + 2], h[q + 3]);
+    }
     }
     if (PARTS >= MOM_PARTS4) {
         const double *M4 = v + 61;  // M4[15 b + sym4(j, k, l, m)]
@@ -1045,6 +1064,7 @@ __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
         };
         // eps_ibc X[b][c] = X[b'][c'] - X[c'][b'] with (b', c') = (1, 2), (2, 0), (0, 1) for i = 0, 1, 2
         for (int i = 0; i < 3; ++i) {
+            if (PART > 0 && i != PART - 1) continue;
             const int b4 = (i + 1) % 3, c4 = (i + 2) % 3;
             double row[K_ROW];
             for (int q = 0; q < K_ROW; ++q) row[q] = 0.0;
@@ -1056,15 +1076,13 @@ __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
                 row[K_W4 + q] = M4[15 * b4 + sym4(c4, k4, l4, n4)] - M4[15 * c4 + sym4(b4, k4, l4, n4)];
             }
             for (int n4 = 0; n4 < 3; ++n4) row[K_W4T + n4] = t4(b4, c4, n4) - t4(c4, b4, n4);
-            for (int q = 0; q < K_ROW; ++q) {
-                o.far64y[j].v[K_ROW * i + q] = row[q];
-                o.far32y[j].v[K_ROW * i + q] = (float)row[q];
+            store_pair(o.far64y[j].v + K_ROW * i, o.far32y[j].v + K_ROW * i, row, K_ROW);
+        }
+        if (PART <= 1)
+            for (int q = 3 * K_ROW; q < 112; ++q) {
+                o.far64y[j].v[q] = 0.0;
+                o.far32y[j].v[q] = 0.f;
             }
-        }
-        for (int q = 3 * K_ROW; q < 112; ++q) {
-            o.far64y[j].v[q] = 0.0;
-            o.far32y[j].v[q] = 0.f;
-        }
     }
     if (PARTS == MOM_PARTS5) {
         // symmetric tensors by index counts (c0, c1, c2): rank among the order-n tuples in storage order
@@ -1086,6 +1104,7 @@ __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
         }
         auto t5 = [&](int b5, int c0, int c1) { return T5[b5][rank(3, c0, c1)]; };
         for (int i = 0; i < 3; ++i) {
+            if (PART > 0 && i != PART - 1) continue;
             const int b5 = (i + 1) % 3, c5 = (i + 2) % 3;  // eps_ibc X[b][c] = X[b5][c5] - X[c5][b5]
             const int e0b = c5 == 0, e1b = c5 == 1, e0c = b5 == 0, e1c = b5 == 1;  // count shifts of index c5 / b5
             double row[Z_ROW];
@@ -1101,13 +1120,13 @@ __device__ void finalize_node(int64_t j, const double *v, const NodeOut &o) {
                 for (int c1 = 2 - c0; c1 >= 0; --c1, ++q)
                     row[Z_W5T + q] = t5(b5, c0 + e0b, c1 + e1b) - t5(c5, c0 + e0c, c1 + e1c);
             row[Z_W5TT] = TT5[b5][c5] - TT5[c5][b5];
-            for (int k = 0; k < Z_ROW; ++k) {
-                o.far64z[j].v[Z_ROW * i + k] = row[k];
-                o.far32z[j].v[Z_ROW * i + k] = (float)row[k];
-            }
+            store_pair(o.far64z[j].v + Z_ROW * i, o.far32z[j].v + Z_ROW * i, row, Z_ROW);
         }
     }
-    if (RECORDS) nodes[j] = node_record(j, b, centre, core, lo, hi, left, right);
+    if (PART <= 0 && RECORDS) {
+        const double b = sqrt(v[0]) * (1.0 + 1e-12);
+        o.nodes[j] = node_record(j, b, o.centre, o.core, o.lo, o.hi, o.left, o.right);
+    }
 }
 
 // Combine a node's chunks in order, then finalize it.
@@ -1204,7 +1223,45 @@ constexpr TupleTables make_tuple_tables() {
     }
     return t;
 }
-__constant__ TupleTables c_tt = make_tuple_tables();
+// in global memory, not constant: the lanes of a warp read different entries
+__device__ TupleTables g_tt = make_tuple_tables();
+
+// Translation terms by index counts.  Tuple u with counts (c0, c1, c2) of the indices 0, 1, 2 translates as
+//   m'_(i; u) = sum over k <= c (componentwise) of C(c0,k0) C(c1,k1) C(c2,k2) D0^k0 D1^k1 D2^k2 m_(i; c - k),
+// the subset expansion with equal subsets merged (at order 5: 252 terms instead of 672).  term[u][t], t < n[u]:
+// binomial product (bits 0-3), the monomial D^k as a tuple index (bits 4-9), storage offset T_BASE + rank of c - k
+// (bits 10-16) and its T_CNT (bits 17-21).  rank(n, c0, c1) is the place of counts (c0, c1, n - c0 - c1) among the
+// order-n tuples in storage order.
+constexpr int TERMS_MAX = 18;
+constexpr int tuple_rank(int n, int c0, int c1) { return (n - c0) * (n - c0 + 1) / 2 + (n - c0 - c1); }
+struct TermTables {
+    unsigned char n[N_TUPLES];
+    unsigned term[N_TUPLES][TERMS_MAX];
+};
+constexpr TermTables make_term_tables() {
+    TermTables t{};
+    const TupleTables tt = make_tuple_tables();
+    const int binom[6][6] = {{1, 0, 0, 0, 0, 0}, {1, 1, 0, 0, 0, 0}, {1, 2, 1, 0, 0, 0},
+                             {1, 3, 3, 1, 0, 0}, {1, 4, 6, 4, 1, 0}, {1, 5, 10, 10, 5, 1}};
+    for (int u = 0; u < N_TUPLES; ++u) {
+        int c[3] = {0, 0, 0};
+        for (int s = 0; s < tt.n[u]; ++s) ++c[(tt.packed[u] >> (2 * s)) & 3];
+        int q = 0;
+        for (int k0 = 0; k0 <= c[0]; ++k0)
+            for (int k1 = 0; k1 <= c[1]; ++k1)
+                for (int k2 = 0; k2 <= c[2]; ++k2) {
+                    const int coef = binom[c[0]][k0] * binom[c[1]][k1] * binom[c[2]][k2];
+                    const int nk = k0 + k1 + k2, nv = tt.n[u] - nk;
+                    const int mono = T_FIRST[nk] + tuple_rank(nk, k0, k1);
+                    const int off = T_BASE[nv] + tuple_rank(nv, c[0] - k0, c[1] - k1);
+                    t.term[u][q++] = (unsigned)coef | ((unsigned)mono << 4) | ((unsigned)off << 10) |
+                                     ((unsigned)T_CNT[nv] << 17);
+                }
+        t.n[u] = (unsigned char)q;
+    }
+    return t;
+}
+__device__ TermTables g_terms = make_term_tables();
 
 template <int PARTS>
 struct MomentTuples {
@@ -1214,7 +1271,7 @@ struct MomentTuples {
 };
 
 // Storage index of moment (i; tuple u).
-__device__ __forceinline__ int tuple_out(int u, int i) { return c_tt.out0[u] + c_tt.cnt[u] * i; }
+__device__ __forceinline__ int tuple_out(int u, int i) { return g_tt.out0[u] + g_tt.cnt[u] * i; }
 
 // The box of the leaf's segments [a, b) and their largest core radius, reduced over the warp; with ends, also the
 // tree-ordered endpoints of the segments.
@@ -1463,20 +1520,21 @@ __global__ void box_climb_kernel(const int32_t *leaves, const unsigned *nleaves,
 //   m'_(i; a1..an) = sum over subsets S of the positions of prod_(s in S) D_as * m_(i; the positions not in S),
 // D = child centre - node centre, the subset products built up one factor at a time; left child first, then right.
 template <int PARTS>
-__global__ void __launch_bounds__(128) bottom_up_kernel(const int32_t *leaves, const unsigned *nleaves,
+__global__ void __launch_bounds__(128, 6) bottom_up_kernel(const int32_t *leaves, const unsigned *nleaves,
                                                         const int2 *up, unsigned *arrive, const double *centre,
                                                         double *sums) {
     using MT = MomentTuples<PARTS>;
-    constexpr int MAXM = 1 << MT::order;  // subset masks of the highest order
+    // lane's tuple in each slot, so that slot 1 runs few terms: fourth-order trees put the first order-1 tuple and the
+    // 31 of orders 2-4 in slot 0 (at most 12 terms), the order-0 tuple and the other two of order 1 in slot 1 (2);
+    // fifth-order trees the 21 tuples of order 5 and the last 11 of order 4 in slot 0 (18), the other 24 in slot 1 (9)
+    constexpr int T0 = MT::n == 56 ? 18 : (MT::n == 35 ? 12 : (MT::n == 20 ? 8 : 4));  // terms a slot runs
+    constexpr int T1 = MT::n == 56 ? 9 : 2;
     __shared__ double sm[4][2][PARTS];
-    __shared__ unsigned short src[MAXM][MT::n];  // by mask, then tuple: the lanes of one mask read adjacent entries
-    for (int q = threadIdx.x; q < MT::n * MAXM; q += blockDim.x) src[q % MAXM][q / MAXM] = c_tt.src[q / MAXM][q % MAXM];
-    __syncthreads();
+    __shared__ double mono[4][2][MT::n];        // D^k per warp and side, by tuple index
+    __shared__ unsigned term[2][T0 > T1 ? T0 : T1][32];  // by slot, term, lane: a warp reads adjacent words
     const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 3;
-    // lane's tuple in each slot, so that slot 1 runs few subset masks: fourth-order trees put the first order-1 tuple
-    // and the 31 of orders 2-4 in slot 0, the order-0 tuple and the other two of order 1 in slot 1 (two masks);
-    // fifth-order trees the 21 tuples of order 5 and the last 11 of order 4 in slot 0, the other 24 in slot 1 (16)
-    int tu[MT::slots], tn[MT::slots], tp[MT::slots];
+    int tu[MT::slots], tp[MT::slots];
+    bool tok[MT::slots];
 #pragma unroll
     for (int r = 0; r < MT::slots; ++r) {
         int u = lane;
@@ -1489,10 +1547,27 @@ __global__ void __launch_bounds__(128) bottom_up_kernel(const int32_t *leaves, c
             ok = r == 0 || lane < 24;
         }
         tu[r] = u;
-        tn[r] = ok ? c_tt.n[u] : -1;
-        tp[r] = ok ? c_tt.packed[u] : 0;
+        tok[r] = ok;
+        tp[r] = ok ? g_tt.packed[u] : 0;
     }
-    constexpr int SLOT1_MASKS = MT::n == 56 ? 16 : 2;
+    // the term table in the slot layout; unused places add zero (coefficient 0, offset 1)
+    if (w == 0) {
+#pragma unroll
+        for (int r = 0; r < MT::slots; ++r) {
+            const int tmax = r == 0 ? T0 : T1;
+            for (int q = 0; q < tmax; ++q)
+                term[r][q][lane] = (tok[r] && q < g_terms.n[tu[r]]) ? g_terms.term[tu[r]][q] : (1u << 10);
+        }
+    }
+    __syncthreads();
+    // lane's monomials of D: tuples lane and lane + 32, by their packed indices
+    int mn_[2], mp_[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const int u = lane + 32 * r;
+        mn_[r] = u < MT::n ? g_tt.n[u] : -1;
+        mp_[r] = u < MT::n ? g_tt.packed[u] : 0;
+    }
     // a grid that stays resident, so that every leaf's climb starts at once (more leaves than resident warps: a warp
     // takes them one after another)
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5), n = *nleaves;
@@ -1535,38 +1610,39 @@ __global__ void __launch_bounds__(128) bottom_up_kernel(const int32_t *leaves, c
             }
         }
         __syncwarp();
+        // D^k for every tuple k of order <= the tree's, both sides
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            if (mn_[r] < 0) continue;
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                double f = 1.0;
+#pragma unroll
+                for (int s2 = 0; s2 < MT::order; ++s2) {
+                    const int xi = (mp_[r] >> (2 * s2)) & 3;
+                    const double dx = xi == 0 ? D[side][0] : (xi == 1 ? D[side][1] : D[side][2]);
+                    f = s2 < mn_[r] ? f * dx : f;
+                }
+                mono[w][side][lane + 32 * r] = f;
+            }
+        }
+        __syncwarp();
         double acc[MT::slots][3];
 #pragma unroll
         for (int q = 0; q < MT::slots; ++q) {
             acc[q][0] = acc[q][1] = acc[q][2] = 0.0;
-            if (tn[q] < 0) continue;
-            const int u = tu[q], masks = (MT::slots == 2 && q == 1) ? SLOT1_MASKS : MAXM;
+            if (!tok[q]) continue;
 #pragma unroll
             for (int side = 0; side < 2; ++side) {
-                constexpr int NP = MT::order;
-                double Dp[NP];  // D at the tuple's positions
-#pragma unroll
-                for (int s2 = 0; s2 < NP; ++s2) {
-                    const int x = (tp[q] >> (2 * s2)) & 3;
-                    Dp[s2] = x == 0 ? D[side][0] : (x == 1 ? D[side][1] : D[side][2]);
-                }
-                double f[MAXM];
-                f[0] = 1.0;
-#pragma unroll
-                for (int mask = 1; mask < MAXM; ++mask) {
-                    const int low = mask & -mask;
-                    const int pos = low == 1 ? 0 : (low == 2 ? 1 : (low == 4 ? 2 : (low == 8 ? 3 : 4)));
-                    f[mask] = f[mask ^ low] * Dp[pos];
-                }
-                const double *sv = sm[w][side];
-#pragma unroll
-                for (int mask = 0; mask < MAXM; ++mask) {
-                    if (mask < masks && mask < (1 << tn[q])) {
-                        const int e = src[mask][u], o0 = e & 255, cn = e >> 8;
-                        acc[q][0] = fma(f[mask], sv[o0], acc[q][0]);
-                        acc[q][1] = fma(f[mask], sv[o0 + cn], acc[q][1]);
-                        acc[q][2] = fma(f[mask], sv[o0 + 2 * cn], acc[q][2]);
-                    }
+                const double *sv = sm[w][side], *mo = mono[w][side];
+#pragma unroll 3
+                for (int t = 0; t < (q == 0 ? T0 : T1); ++t) {
+                    const unsigned e = term[q][t][lane];
+                    const double f = (double)(e & 15u) * mo[(e >> 4) & 63u];
+                    const int o0 = (int)((e >> 10) & 127u), cn = (int)(e >> 17);
+                    acc[q][0] = fma(f, sv[o0], acc[q][0]);
+                    acc[q][1] = fma(f, sv[o0 + cn], acc[q][1]);
+                    acc[q][2] = fma(f, sv[o0 + 2 * cn], acc[q][2]);
                 }
             }
         }
@@ -1574,7 +1650,7 @@ __global__ void __launch_bounds__(128) bottom_up_kernel(const int32_t *leaves, c
         double *out = sums + (int64_t)PARTS * p;
 #pragma unroll
         for (int q = 0; q < MT::slots; ++q)
-            if (tn[q] >= 0)
+            if (tok[q])
                 for (int i = 0; i < 3; ++i) out[tuple_out(tu[q], i)] = acc[q][i];
         node = p;
     }
@@ -1641,15 +1717,23 @@ __global__ void node_rec_kernel(int64_t count, const unsigned long long *bound2,
     nodes[j] = node_record(j, b, centre, core, lo, hi, left, right);
 }
 
-// Every node's export arrays and far records from its sums.
+// Every node's export arrays and far records from its sums (read in place); for fourth- and fifth-order trees
+// blockIdx.y picks the part (0: orders 0-3, 1-3: the order-4 and order-5 rows of one component).
 template <int PARTS>
 __global__ void node_final_kernel(int64_t count, const double *sums, NodeOut o) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= count) return;
-    double v[PARTS];
-    v[0] = 0.0;
-    for (int q = 1; q < PARTS; ++q) v[q] = sums[(int64_t)PARTS * j + q];
-    finalize_node<PARTS, false>(j, v, o);
+    const double *v = sums + (int64_t)PARTS * j;
+    if (PARTS < MOM_PARTS4) {
+        finalize_node<PARTS, false, -1>(j, v, o);
+        return;
+    }
+    switch (blockIdx.y) {
+        case 0: finalize_node<PARTS, false, 0>(j, v, o); break;
+        case 1: finalize_node<PARTS, false, 1>(j, v, o); break;
+        case 2: finalize_node<PARTS, false, 2>(j, v, o); break;
+        default: finalize_node<PARTS, false, 3>(j, v, o); break;
+    }
 }
 
 __global__ void internal_item_count_kernel(int64_t count, const int64_t *lo, const int64_t *hi, const int64_t *left,
@@ -1728,7 +1812,7 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
                       t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x,
                       t->far64y, t->far32y, t->far64z, t->far32z};
     // one warp per block: the thread per node is long, so the nodes spread over every SM
-    node_final_kernel<PARTS><<<blocks_for(count, 32), 32, 0, ms>>>(count, sums, out);
+    node_final_kernel<PARTS><<<dim3(blocks_for(count, 32), PARTS >= MOM_PARTS4 ? 4 : 1), 32, 0, ms>>>(count, sums, out);
     BS_CHECK_LAUNCH("bottom-up moments");
     return BS_OK;
 }
