@@ -550,11 +550,23 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
     if (t.valid && a.ex_ptr) { e = a.ex_ptr[t.p]; e1 = a.ex_ptr[t.p + 1]; }
     Acc<PREC> acc;
     int flag = BS_FLAG_OK;
+    // Far entries whose lane masks do not overlap are evaluated together, each lane at its own node: a far entry
+    // holds about a third of the warp's lanes, and a group of disjoint ones fills the warp (their records are a few
+    // distinct addresses a load).  The group is evaluated when an entry overlaps it and at the end.
+    int my_far = -1;
+    unsigned group = 0;
+    auto flush = [&]() {
+        if (my_far >= 0) far_node<PREC>(a, t, my_far, acc);
+        my_far = -1;
+        group = 0;
+    };
     for (int k = first; k < last; ++k) {
         const int2 entry = a.list[at(k)];
         const bool mine = ((unsigned)entry.y >> lane) & 1u;
         if (entry.x & FAR_BIT) {
-            if (mine) far_node<PREC>(a, t, entry.x & ~FAR_BIT, acc);
+            if (group & (unsigned)entry.y) flush();
+            group |= (unsigned)entry.y;
+            if (mine) my_far = entry.x & ~FAR_BIT;
         } else {
             const NodeRec nr = a.tv.nodes[entry.x];
             int64_t ec = e;  // list entries are not in position order: each leaf scans the exclusions from the start
@@ -562,6 +574,7 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
                                     fp64_pairs);
         }
     }
+    flush();
     if (t.valid) {
         const int64_t o = (int64_t)c * a.n + t.p;
         a.partial[3 * o] = acc.x();
