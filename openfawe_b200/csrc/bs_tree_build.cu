@@ -1152,8 +1152,9 @@ __global__ void moment_final_kernel(int64_t count, const int64_t *first, const i
 //   m3_ijkl += D_j m2_ikl + D_k m2_ijl + D_l m2_ijk + D_j D_k m1_il + D_j D_l m1_ik + D_k D_l m1_ij + D_j D_k D_l m0_i
 // and for fourth-order trees
 //   m4_ijklm += the 4 D m3, 6 D D m2, 4 D D D m1 and D D D D m0 terms of the same binomial expansion
-// (D = child centre - node centre; left child first, then right), which equals the direct sums up to rounding.  The
-// bounding radius stays exact: one pass over the internal nodes' ranges of tree-ordered endpoints.
+// (D = child centre - node centre; left child first, then right), which equals the direct sums up to rounding.  Boxes
+// and cores are unions over the leaves (exact); the bounding radius stays exact: every leaf's endpoints against each
+// of its ancestors' centres.
 // ---------------------------------------------------------------------------------------------------------------------
 struct __align__(16) EndPts {
     double sx, sy, sz, ex, ey, ez;
@@ -1161,13 +1162,18 @@ struct __align__(16) EndPts {
 
 
 // up[child] = (parent, the other child), the other child stored as -(it + 1) when `child` is the right one, so that a
-// climbing warp knows both children and their order from one load; up[0].x = -1.
+// climbing warp knows both children and their order from one load; a root's up[].x = -1 (up[] starts as all -1).
 // The leaves are listed in leaves[0 .. *nleaves) in no particular order (each leaf's work is independent of which
-// thread takes it).  up[] starts as all -1 (memset), so a node without a parent reads parent -1.
+// thread takes it).  Every node's box (ordered bits, for atomicMin / atomicMax) starts empty and its core at zero.
 __global__ void parent_kernel(int64_t count, const int64_t *left, const int64_t *right, int2 *up, int32_t *leaves,
-                              unsigned *nleaves) {
+                              unsigned *nleaves, unsigned long long *boxbits, unsigned long long *corebits) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= count) return;
+    for (int x = 0; x < 3; ++x) {
+        boxbits[6 * j + x] = ordered_bits(INFINITY);
+        boxbits[6 * j + 3 + x] = ordered_bits(-INFINITY);
+    }
+    corebits[j] = 0ull;
     if (left[j] >= 0) {
         up[left[j]] = make_int2((int)j, (int)right[j]);
         up[right[j]] = make_int2((int)j, -(int)left[j] - 1);
@@ -1300,11 +1306,14 @@ __device__ __forceinline__ void leaf_extent(int lane, int64_t a, int64_t b, cons
 }
 
 // One warp per leaf: box, core and centre from the leaf's segments (and their tree-ordered endpoints into ends), then
-// bound^2 (the largest squared distance from the centre to an endpoint) into bound2 as its bit pattern.
+// bound^2 (the largest squared distance from the centre to an endpoint) into bound2 as its bit pattern.  Seven lanes
+// then fold the box's six bounds and the core into every ancestor (atomicMin / atomicMax on ordered bits: the union
+// of the leaves' boxes and the largest core, the same in any order), so that no climb is needed for the boxes.
 __global__ void __launch_bounds__(128) leaf_geometry_kernel(const int32_t *leaves, const unsigned *nleaves,
                                                             const int64_t *lo, const int64_t *hi,
-                                                            const int32_t *order, const SegGeo *geo,
-                                                            EndPts *ends, double *box, double *centre,
+                                                            const int32_t *order, const SegGeo *geo, const int2 *up,
+                                                            EndPts *ends, unsigned long long *boxbits,
+                                                            unsigned long long *corebits, double *centre,
                                                             double *core, unsigned long long *bound2) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5), n = *nleaves;
@@ -1326,15 +1335,23 @@ __global__ void __launch_bounds__(128) leaf_geometry_kernel(const int32_t *leave
         }
         for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
         if (lane == 0) {
-            for (int x = 0; x < 3; ++x) {
-                box[6 * j + x] = mn[x];
-                box[6 * j + 3 + x] = mx[x];
-            }
             centre[3 * j] = c0;
             centre[3 * j + 1] = c1;
             centre[3 * j + 2] = c2;
             core[j] = c;
             bound2[j] = (unsigned long long)__double_as_longlong(r2);
+        }
+        if (lane < 7) {
+            const double m0 = mn[0], m1 = mn[1], m2 = mn[2], x0 = mx[0], x1 = mx[1], x2 = mx[2];
+            const double bv = lane == 0 ? m0 : lane == 1 ? m1 : lane == 2 ? m2 : lane == 3 ? x0 : lane == 4 ? x1 : x2;
+            const unsigned long long v = lane < 6 ? ordered_bits(bv) : (unsigned long long)__double_as_longlong(c);
+            if (lane < 6) boxbits[6 * j + lane] = v;
+            else corebits[j] = v;
+            for (int node = up[j].x, depth = 0; node >= 0 && depth < 4096; node = up[node].x, ++depth) {
+                if (lane < 3) atomicMin(boxbits + 6 * (int64_t)node + lane, v);
+                else if (lane < 6) atomicMax(boxbits + 6 * (int64_t)node + lane, v);
+                else atomicMax(corebits + node, v);
+            }
         }
     }
 }
@@ -1485,40 +1502,11 @@ __global__ void __launch_bounds__(32 * leaf_warps<PARTS>()) leaf_moments_kernel(
 }
 
 
-// One thread per leaf climbs towards the root; at each parent the second of the two arriving threads combines the
-// children (their results were published, and fenced, before the arrival count moved), so every internal node is
-// combined exactly once and no thread waits for another: box = the children's union, centre = its midpoint, core =
-// the larger of the two.
-__global__ void box_climb_kernel(const int32_t *leaves, const unsigned *nleaves, const int2 *up, unsigned *arrive,
-                                 double *box, double *centre, double *core) {
-    const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= (int64_t)*nleaves) return;
-    int64_t node = leaves[w];
-    for (int depth = 0; depth < 4096; ++depth) {
-        const int2 pu = up[node];
-        const int32_t p = pu.x;
-        if (p < 0) return;
-        __threadfence();
-        if (atomicAdd(&arrive[p], 1u) == 0) return;
-        __threadfence();
-        const int64_t l = pu.y >= 0 ? node : -(int64_t)pu.y - 1, r = pu.y >= 0 ? (int64_t)pu.y : node;
-#pragma unroll
-        for (int x = 0; x < 3; ++x) {
-            const double lo_x = fmin(__ldcg(box + 6 * l + x), __ldcg(box + 6 * r + x));
-            const double hi_x = fmax(__ldcg(box + 6 * l + 3 + x), __ldcg(box + 6 * r + 3 + x));
-            box[6 * p + x] = lo_x;
-            box[6 * p + 3 + x] = hi_x;
-            centre[3 * p + x] = 0.5 * (lo_x + hi_x);
-        }
-        core[p] = fmax(__ldcg(core + l), __ldcg(core + r));
-        node = p;
-    }
-}
-
-// The moments of the internal nodes, climbing like box_climb_kernel but one warp per leaf (centres known): both
-// children's sums are staged in shared memory; lane u translates index tuple u by the binomial expansion
-//   m'_(i; a1..an) = sum over subsets S of the positions of prod_(s in S) D_as * m_(i; the positions not in S),
-// D = child centre - node centre, the subset products built up one factor at a time; left child first, then right.
+// The moments of the internal nodes: one warp per leaf climbs towards the root; at each parent the second of the
+// two arriving warps combines the children (their results were published, and fenced, before the arrival count
+// moved), so every internal node is combined exactly once and no warp waits for another (centres known): both
+// children's sums are staged in shared memory; lane u translates index tuple u over its distinct sub-tuples with
+// binomial weights (g_terms), D = child centre - node centre; left child first, then right.
 template <int PARTS>
 __global__ void __launch_bounds__(128, 6) bottom_up_kernel(const int32_t *leaves, const unsigned *nleaves,
                                                         const int2 *up, unsigned *arrive, const double *centre,
@@ -1657,61 +1645,69 @@ __global__ void __launch_bounds__(128, 6) bottom_up_kernel(const int32_t *leaves
     }
 }
 
-// Bound^2 of every internal node from the tree-ordered endpoints, by CHUNK-segment chunks of the nodes' ranges: chunk c
-// belongs to the last node j with first[j] <= c (first: exclusive scan of the per-node chunk counts, *total chunks in
-// all), found by binary search, so the chunk list needs no host round trip.  A block takes one chunk at a time and
-// folds its maximum into bound2[j] with an integer atomicMax (non-negative doubles order like their bit patterns):
-// the same value in any order.
-__global__ void __launch_bounds__(MOM_THREADS) bound_chunks_kernel(int64_t count, const int64_t *first,
-                                                                   const int64_t *total, const int64_t *lo,
-                                                                   const int64_t *hi, const EndPts *ends,
-                                                                   const double *centre,
-                                                                   unsigned long long *bound2) {
-    __shared__ double red[MOM_THREADS / 32];
-    __shared__ int64_t node_s;
-    const int64_t chunks = *total;
-    for (int64_t c = blockIdx.x; c < chunks; c += gridDim.x) {
-        if (threadIdx.x == 0) {
-            int64_t l = 0, h = count;  // first[l] <= c < first[h] (first[count] taken as +inf)
-            while (h - l > 1) {
-                const int64_t mid = (l + h) >> 1;
-                if (first[mid] <= c) l = mid;
-                else h = mid;
+// Bound^2 of every internal node, exactly: one warp per leaf folds the largest squared distance from each of the
+// leaf's ancestors' centres (the midpoints of their boxes) to the leaf's tree-ordered endpoints into that ancestor's
+// bound2 with an integer atomicMax (non-negative doubles order like their bit patterns: the same value in any order).
+// The ancestors go eight at a time, their centres in registers, so that the leaf's endpoints are read once a group.
+constexpr int BOUND_GROUP = 8;
+__global__ void __launch_bounds__(128) bound_up_kernel(const int32_t *leaves, const unsigned *nleaves,
+                                                       const int64_t *lo, const int64_t *hi, const int2 *up,
+                                                       const EndPts *ends, const unsigned long long *boxbits,
+                                                       unsigned long long *bound2) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5), n = *nleaves;
+    for (int64_t x = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); x < n; x += warps) {
+        const int64_t j = leaves[x], a = lo[j], b = hi[j];
+        if (b <= a) continue;
+        int node = up[j].x;
+        for (int group = 0; node >= 0 && group < 512; ++group) {
+            int anc[BOUND_GROUP];
+            double c[BOUND_GROUP][3], r2[BOUND_GROUP];
+#pragma unroll
+            for (int g = 0; g < BOUND_GROUP; ++g) {
+                anc[g] = node;
+                r2[g] = 0.0;
+                const int64_t q = node >= 0 ? node : 0;
+#pragma unroll
+                for (int xx = 0; xx < 3; ++xx)
+                    c[g][xx] = 0.5 * (from_ordered(boxbits[6 * q + xx]) + from_ordered(boxbits[6 * q + 3 + xx]));
+                if (node >= 0) node = up[node].x;
             }
-            node_s = l;
+            for (int64_t k = a + lane; k < b; k += 32) {
+                const EndPts e = ends[k];
+#pragma unroll
+                for (int g = 0; g < BOUND_GROUP; ++g) {
+                    const double a0 = e.sx - c[g][0], a1 = e.sy - c[g][1], a2 = e.sz - c[g][2];
+                    const double b0 = e.ex - c[g][0], b1 = e.ey - c[g][1], b2 = e.ez - c[g][2];
+                    // the reference's ((x^2 + y^2) + z^2) without contraction, as in every bound of this file
+                    const double ra = __dadd_rn(__dadd_rn(__dmul_rn(a0, a0), __dmul_rn(a1, a1)), __dmul_rn(a2, a2));
+                    const double rb = __dadd_rn(__dadd_rn(__dmul_rn(b0, b0), __dmul_rn(b1, b1)), __dmul_rn(b2, b2));
+                    r2[g] = fmax(r2[g], fmax(ra, rb));
+                }
+            }
+#pragma unroll
+            for (int g = 0; g < BOUND_GROUP; ++g) {
+                for (int o = 16; o > 0; o >>= 1) r2[g] = fmax(r2[g], __shfl_xor_sync(0xffffffffu, r2[g], o));
+                if (lane == 0 && anc[g] >= 0)
+                    atomicMax(bound2 + anc[g], (unsigned long long)__double_as_longlong(r2[g]));
+            }
         }
-        __syncthreads();
-        const int64_t j = node_s;
-        const int64_t start = lo[j] + (c - first[j]) * CHUNK, end = min(hi[j], start + CHUNK);
-        const double c0 = centre[3 * j], c1 = centre[3 * j + 1], c2 = centre[3 * j + 2];
-        double r2 = 0.0;
-        for (int64_t k = start + threadIdx.x; k < end; k += blockDim.x) {
-            const EndPts e = ends[k];
-            const double a0 = e.sx - c0, a1 = e.sy - c1, a2 = e.sz - c2;
-            const double b0 = e.ex - c0, b1 = e.ey - c1, b2 = e.ez - c2;
-            const double ra = __dadd_rn(__dadd_rn(__dmul_rn(a0, a0), __dmul_rn(a1, a1)), __dmul_rn(a2, a2));
-            const double rb = __dadd_rn(__dadd_rn(__dmul_rn(b0, b0), __dmul_rn(b1, b1)), __dmul_rn(b2, b2));
-            r2 = fmax(r2, fmax(ra, rb));
-        }
-        for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r2;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double v = red[0];
-            for (int w = 1; w < MOM_THREADS / 32; ++w) v = fmax(v, red[w]);
-            atomicMax(bound2 + j, (unsigned long long)__double_as_longlong(v));
-        }
-        __syncthreads();
     }
 }
 
-// The bounding radius (bound^2 from leaf_geometry_kernel or bound_chunks_kernel) and the traversal record of every
-// node: all that the walk reads.
-__global__ void node_rec_kernel(int64_t count, const unsigned long long *bound2, const double *centre,
-                                const double *core, const int64_t *lo, const int64_t *hi, const int64_t *left,
-                                const int64_t *right, double *bound, NodeRec *nodes) {
+// The bounding radius (bound^2 from leaf_geometry_kernel or bound_up_kernel), the centre and core of the internal
+// nodes (from their boxes and cores) and the traversal record of every node: all that the walk reads.
+__global__ void node_rec_kernel(int64_t count, const unsigned long long *bound2,
+                                const unsigned long long *boxbits, const unsigned long long *corebits,
+                                double *centre, double *core, const int64_t *lo, const int64_t *hi,
+                                const int64_t *left, const int64_t *right, double *bound, NodeRec *nodes) {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= count) return;
+    if (left[j] >= 0) {
+        for (int x = 0; x < 3; ++x)
+            centre[3 * j + x] = 0.5 * (from_ordered(boxbits[6 * j + x]) + from_ordered(boxbits[6 * j + 3 + x]));
+        core[j] = __longlong_as_double((long long)corebits[j]);
+    }
     const double b = sqrt(__longlong_as_double((long long)bound2[j])) * (1.0 + 1e-12);
     bound[j] = b;
     nodes[j] = node_record(j, b, centre, core, lo, hi, left, right);
@@ -1736,17 +1732,9 @@ __global__ void node_final_kernel(int64_t count, const double *sums, NodeOut o) 
     }
 }
 
-__global__ void internal_item_count_kernel(int64_t count, const int64_t *lo, const int64_t *hi, const int64_t *left,
-                                           int64_t *n) {
-    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= count) return;
-    int64_t size = hi[j] - lo[j];
-    n[j] = (left[j] >= 0 && size > 0) ? (size + CHUNK - 1) / CHUNK : 0;
-}
-
-// Bottom-up pipeline in two phases.  Geometry, on s: leaf boxes, centres, cores and bounds, the internal nodes' boxes
-// from their children, their exact bounds (one pass over the internal nodes' ranges of tree-ordered endpoints) and
-// the traversal records.  Moments, on `side` when given (after s reached the end of the geometry; t->moments_done
+// Bottom-up pipeline in two phases.  Geometry, on s: leaf boxes, centres, cores and bounds, each leaf folding its box
+// and core into its ancestors, the internal nodes' exact bounds (every leaf's endpoints against its ancestors'
+// centres) and the traversal records.  Moments, on `side` when given (after s reached the end of the geometry; t->moments_done
 // marks their end) or else on s: leaf sums, the internal nodes' translated sums, the far records.  What the moment
 // phase reads lives with the tree when it runs on the side stream (freed with the tree, after the evaluation that
 // waited for it), else in scratch.
@@ -1754,38 +1742,31 @@ template <int PARTS>
 static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_t s, cudaStream_t side) {
     const int64_t count = t->count, m = t->m;
     const bool defer = side != nullptr;
-    double *box = scratch.get<double>(6 * count);
-    unsigned *arrive = scratch.get<unsigned>(2 * count);
+    unsigned long long *boxbits = scratch.get<unsigned long long>(7 * count);  // six bounds a node, then the cores
     EndPts *ends = scratch.get<EndPts>(m);
-    int64_t *nitems = scratch.get<int64_t>(count), *first = scratch.get<int64_t>(count);
-    int64_t *total = scratch.get<int64_t>(1);
     unsigned long long *bound2 = scratch.get<unsigned long long>(count);
-    if (!box || !arrive || !ends || !nitems || !first || !total || !bound2) return scratch.status;
+    if (!boxbits || !ends || !bound2) return scratch.status;
+    unsigned long long *corebits = boxbits + 6 * count;
     double *sums = defer ? t->alloc<double>((size_t)PARTS * count, s) : scratch.get<double>((size_t)PARTS * count);
     int2 *parent = defer ? t->alloc<int2>(count, s) : scratch.get<int2>(count);
     unsigned *arrive_m = defer ? t->alloc<unsigned>(count + 1, s) : scratch.get<unsigned>(count + 1);
     int32_t *leaves = defer ? t->alloc<int32_t>(count, s) : scratch.get<int32_t>(count);
     if (!sums || !parent || !arrive_m || !leaves) return defer ? BS_ERR_OOM : scratch.status;
     unsigned *nleaves = arrive_m + count;
-    BS_CUDA(cudaMemsetAsync(arrive, 0, count * sizeof(unsigned), s));
     BS_CUDA(cudaMemsetAsync(arrive_m, 0, (count + 1) * sizeof(unsigned), s));
     BS_CUDA(cudaMemsetAsync(bound2, 0, count * sizeof(unsigned long long), s));
     BS_CUDA(cudaMemsetAsync(parent, 0xff, count * sizeof(int2), s));
-    parent_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->left, t->right, parent, leaves, nleaves);
+    parent_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->left, t->right, parent, leaves, nleaves, boxbits,
+                                                         corebits);
     const int32_t *geo_order = t->geo_sorted ? nullptr : t->order32;  // geo in input order: read through the order
     int sms = 0;
     BS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, t->device));
     const unsigned leaf_blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((count + 3) / 4, (int64_t)sms * 16));
-    leaf_geometry_kernel<<<leaf_blocks, 128, 0, s>>>(leaves, nleaves, t->lo, t->hi, geo_order, geo, ends, box,
-                                                      t->centre, t->core, bound2);
-    box_climb_kernel<<<blocks_for(count, 128), 128, 0, s>>>(leaves, nleaves, parent, arrive, box, t->centre, t->core);
-    internal_item_count_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->lo, t->hi, t->left, nitems);
-    BS_CHECK_LAUNCH("node geometry");
-    int rc = scan_exclusive(nitems, first, count, total, scratch, s);
-    if (rc != BS_OK) return rc;
-    bound_chunks_kernel<<<148 * 8, MOM_THREADS, 0, s>>>(count, first, total, t->lo, t->hi, ends, t->centre, bound2);
-    node_rec_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, bound2, t->centre, t->core, t->lo, t->hi, t->left,
-                                                            t->right, t->bound, t->nodes);
+    leaf_geometry_kernel<<<leaf_blocks, 128, 0, s>>>(leaves, nleaves, t->lo, t->hi, geo_order, geo, parent, ends,
+                                                      boxbits, corebits, t->centre, t->core, bound2);
+    bound_up_kernel<<<leaf_blocks, 128, 0, s>>>(leaves, nleaves, t->lo, t->hi, parent, ends, boxbits, bound2);
+    node_rec_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, bound2, boxbits, corebits, t->centre, t->core, t->lo,
+                                                            t->hi, t->left, t->right, t->bound, t->nodes);
     BS_CHECK_LAUNCH("node records");
     cudaStream_t ms = s;
     if (defer) {
