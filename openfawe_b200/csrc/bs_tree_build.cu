@@ -1778,14 +1778,21 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
         ms = side;
     }
     constexpr int LW = leaf_warps<PARTS>();
-    int leaf_resident = 0;  // resident blocks: one wave takes as many leaves as fit
-    BS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&leaf_resident, leaf_moments_kernel<PARTS>, 32 * LW, 0));
+    // resident blocks a SM (one wave takes as many leaves as fit), asked once: a property of the compiled kernel
+    static const int leaf_resident = [] {
+        int r = 0;
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, leaf_moments_kernel<PARTS>, 32 * LW, 0) ==
+                       cudaSuccess ? r : 1;
+    }();
     const unsigned moment_blocks = (unsigned)std::max<int64_t>(
         1, std::min<int64_t>((count + LW - 1) / LW, (int64_t)std::max(1, leaf_resident) * sms));
     leaf_moments_kernel<PARTS><<<moment_blocks, 32 * LW, 0, ms>>>(leaves, nleaves, t->lo, t->hi, geo_order, geo,
                                                                   t->centre, sums);
-    int climb_blocks = 0;  // resident blocks: one wave holds every climbing warp
-    BS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&climb_blocks, bottom_up_kernel<PARTS>, 128, 0));
+    static const int climb_blocks = [] {  // resident blocks: one wave holds every climbing warp
+        int r = 0;
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, bottom_up_kernel<PARTS>, 128, 0) == cudaSuccess ? r
+                                                                                                        : 1;
+    }();
     const unsigned climb_grid = (unsigned)std::max<int64_t>(
         1, std::min<int64_t>(blocks_for(count, 4), (int64_t)std::max(1, climb_blocks) * sms));
     bottom_up_kernel<PARTS><<<climb_grid, 128, 0, ms>>>(leaves, nleaves, parent, arrive_m, t->centre, sums);
@@ -1798,38 +1805,44 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
     return BS_OK;
 }
 
+// The next n elements of T in a carved block (256-byte aligned pieces); with base null only the size is counted.
+template <class T>
+static T *carve(char *base, size_t &off, size_t n) {
+    T *p = base ? reinterpret_cast<T *>(base + off) : nullptr;
+    off += ((n ? n : 1) * sizeof(T) + 255) / 256 * 256;
+    return p;
+}
+
 int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_t s, cudaStream_t side) {
-    const int64_t count = t->count;
-    t->centre = t->alloc<double>(3 * count, s);
-    t->bound = t->alloc<double>(count, s);
-    t->core = t->alloc<double>(count, s);
-    t->m0 = t->alloc<double>(3 * count, s);
-    t->m1 = t->alloc<double>(9 * count, s);
-    t->m2 = t->alloc<double>(27 * count, s);
-    t->w1 = t->alloc<double>(3 * count, s);
-    t->t2 = t->alloc<double>(3 * count, s);
-    t->w2 = t->alloc<double>(9 * count, s);
-    t->nodes = t->alloc<NodeRec>(count, s);
-    t->far64 = t->alloc<Far64>(count, s);
-    t->far32 = t->alloc<Far32>(count, s);
-    if (t->order3) {
-        t->far64x = t->alloc<Far64x>(count, s);
-        t->far32x = t->alloc<Far32x>(count, s);
-        if (!t->far64x || !t->far32x) return BS_ERR_OOM;
+    const size_t count = (size_t)t->count;
+    // every per-node array of the tree in one pool allocation (the host enqueues no allocation per array while the
+    // device waits for the node count's consumers): one pass to size the block, one to hand out its pieces
+    char *base = nullptr;
+    for (int pass = 0; pass < 2; ++pass) {
+        size_t off = 0;
+        t->centre = carve<double>(base, off, 3 * count);
+        t->bound = carve<double>(base, off, count);
+        t->core = carve<double>(base, off, count);
+        t->m0 = carve<double>(base, off, 3 * count);
+        t->m1 = carve<double>(base, off, 9 * count);
+        t->m2 = carve<double>(base, off, 27 * count);
+        t->w1 = carve<double>(base, off, 3 * count);
+        t->t2 = carve<double>(base, off, 3 * count);
+        t->w2 = carve<double>(base, off, 9 * count);
+        t->nodes = carve<NodeRec>(base, off, count);
+        t->far64 = carve<Far64>(base, off, count);
+        t->far32 = carve<Far32>(base, off, count);
+        t->far64x = t->order3 ? carve<Far64x>(base, off, count) : nullptr;
+        t->far32x = t->order3 ? carve<Far32x>(base, off, count) : nullptr;
+        t->far64y = t->order4 ? carve<Far64y>(base, off, count) : nullptr;
+        t->far32y = t->order4 ? carve<Far32y>(base, off, count) : nullptr;
+        t->far64z = t->order5 ? carve<Far64z>(base, off, count) : nullptr;
+        t->far32z = t->order5 ? carve<Far32z>(base, off, count) : nullptr;
+        if (pass == 0) {
+            base = t->alloc<char>(off, s);
+            if (!base) return BS_ERR_OOM;
+        }
     }
-    if (t->order4) {
-        t->far64y = t->alloc<Far64y>(count, s);
-        t->far32y = t->alloc<Far32y>(count, s);
-        if (!t->far64y || !t->far32y) return BS_ERR_OOM;
-    }
-    if (t->order5) {
-        t->far64z = t->alloc<Far64z>(count, s);
-        t->far32z = t->alloc<Far32z>(count, s);
-        if (!t->far64z || !t->far32z) return BS_ERR_OOM;
-    }
-    if (!t->centre || !t->bound || !t->core || !t->m0 || !t->m1 || !t->m2 || !t->w1 || !t->t2 || !t->w2 ||
-        !t->nodes || !t->far64 || !t->far32)
-        return BS_ERR_OOM;
     // fourth order: the bottom-up pipeline for every kind (its box, centre and bound equal the direct sums')
     if (t->order5) return moments_bottom_up<MOM_PARTS5>(t, geo, scratch, s, side);
     if (t->order4) return moments_bottom_up<MOM_PARTS4>(t, geo, scratch, s, side);
