@@ -7,7 +7,7 @@
 // order exactly as numpy's mergesort does.  The host walks the levels (reading one flag per node per level back), as the
 // reference's own GPU build does (src/openfawe/aero/vortex_cuda_build.py:234-275).
 //
-// Morton tree: 21-bit quantisation per axis in IEEE FP64 (no contraction), 63-bit interleaved keys, stable radix sort,
+// Morton tree: 16-bit quantisation per axis in IEEE FP64 (no contraction), 48-bit interleaved keys, stable radix sort,
 // Karras's binary radix tree (ties broken by position), and a traversal tree made of the internal nodes holding more
 // than leaf_size segments plus their small children as leaves.  oracle/morton_oracle.c restates it on the CPU.
 //
@@ -166,7 +166,8 @@ __device__ __forceinline__ uint64_t spread3(uint32_t v) {
     return x;
 }
 
-// Keys of the spec in morton_oracle.c: q = min(2^21 - 1, trunc((mid - lo) * inv)), inv = 2^21 / max extent.
+// Keys of the spec in morton_oracle.c: q = min(2^16 - 1, trunc((mid - lo) * inv)), inv = 2^16 / max extent; 48-bit
+// keys sort in six 8-bit passes.
 __global__ void morton_keys_kernel(int64_t m, const bs_sources src, const unsigned long long *box, uint64_t *keys,
                                    int32_t *vals) {
     int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -177,13 +178,13 @@ __global__ void morton_keys_kernel(int64_t m, const bs_sources src, const unsign
         double e = __dsub_rn(from_ordered(box[3 + a]), lo[a]);
         if (e > ext) ext = e;
     }
-    double inv = ext > 0.0 ? __ddiv_rn(2097152.0, ext) : 0.0;
+    double inv = ext > 0.0 ? __ddiv_rn(65536.0, ext) : 0.0;
     double v[3];
     midpoint_raw(src, s, v[0], v[1], v[2]);
     uint32_t q[3];
     for (int a = 0; a < 3; ++a) {
         uint32_t u = __double2uint_rz(__dmul_rn(__dsub_rn(v[a], lo[a]), inv));
-        q[a] = u > 2097151u ? 2097151u : u;
+        q[a] = u > 65535u ? 65535u : u;
     }
     keys[s] = (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
     vals[s] = (int32_t)s;
@@ -352,7 +353,7 @@ static int build_morton(bs_tree *t, const bs_sources *src, Scratch &scratch, cud
     morton_keys_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, *src, box, keys, t->order32);
     BS_CHECK_LAUNCH("morton keys");
     BS_CUDA(cudaMemcpyAsync(t->keys, keys, m * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
-    int rc = radix_sort(keys, t->order32, m, 0, 63, scratch, s);
+    int rc = radix_sort(keys, t->order32, m, 0, 48, scratch, s);
     if (rc != BS_OK) return rc;
     return topology_from_sorted(t, keys, 0, scratch, s, while_counting);
 }

@@ -9,9 +9,9 @@
  * Specification (shared with openfawe_b200/csrc/bs_tree_build.cu):
  *   mid    = 0.5 * (s + (s + d*L))                       per axis, IEEE round-to-nearest, no fused multiply-add
  *   box    = [min mid, max mid] per axis;  extent = max over axes of (max - min)
- *   inv    = 2097152 / extent   (0 when extent == 0)
- *   q      = min(2^21 - 1, (uint32)((mid - min) * inv))  truncation toward zero
- *   key    = bit-interleave(qx, qy, qz): bit i of x -> 3i+2, of y -> 3i+1, of z -> 3i    (63 bits)
+ *   inv    = 65536 / extent   (0 when extent == 0)
+ *   q      = min(2^16 - 1, (uint32)((mid - min) * inv))  truncation toward zero
+ *   key    = bit-interleave(qx, qy, qz): bit i of x -> 3i+2, of y -> 3i+1, of z -> 3i    (48 bits)
  *   sort   = stable by key (ties keep segment index order)
  *   topology: the binary radix tree of Karras (HPG 2012) over the sorted keys, ties broken by position;
  *   traversal tree: internal nodes holding more than leaf_size segments ("big") plus their non-big children as leaves,
@@ -23,12 +23,12 @@
 #include <stdlib.h>
 #include <string.h>
 
-#define MORTON_BITS 21
-#define MORTON_SCALE 2097152.0
+#define MORTON_BITS 16
+#define MORTON_SCALE 65536.0
 
 static uint64_t spread3(uint32_t v)
 {
-    uint64_t x = v & 0x1fffff;
+    uint64_t x = v & 0xffff;
     uint64_t out = 0;
     for (int i = 0; i < MORTON_BITS; ++i) out |= ((x >> i) & 1ull) << (3 * i);
     return out;
@@ -61,7 +61,7 @@ void orc_morton_keys(int64_t m, const double *mid, const double *box, double inv
         for (int a = 0; a < 3; ++a) {
             double v = (mid[3 * s + a] - box[a]) * inv;
             uint32_t u = (uint32_t)v;
-            q[a] = u > 2097151u ? 2097151u : u;
+            q[a] = u > 65535u ? 65535u : u;
         }
         keys[s] = (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
     }
