@@ -1171,15 +1171,20 @@ extern "C" int bs_tree_sum_host(bs_ctx *ctx, const bs_sources *src, const bs_tre
                 BS_CUDA(cudaStreamWaitEvent(s, landed, 0));
                 return BS_OK;
             };
-            // the target sort on the side stream, beside the build (the targets landed with the first upload)
+            // the target sort on the side stream, queued while the node count travels back (the device starts on
+            // the keys at once; the sort runs beside the packing and the node geometry)
             cudaStream_t side = nullptr;
             cudaEvent_t sorted = nullptr;
             int32_t *perm = scratch.get<int32_t>(n);
             rc = perm ? side_stream(ctx, &side) : scratch.status;
-            if (rc == BS_OK) rc = sort_targets_beside(ctx, &dtgt, perm, s, side, &sorted);
+            auto rest_and_sort = [&]() -> int {
+                const int r = rest();
+                return r != BS_OK ? r : sort_targets_beside(ctx, &dtgt, perm, s, side, &sorted);
+            };
             bs_tree *tree = nullptr;
-            if (rc == BS_OK) rc = tree_build(ctx, &dsrc, tp, &tree, s, false, rest, side);
+            if (rc == BS_OK) rc = tree_build(ctx, &dsrc, tp, &tree, s, false, rest_and_sort, side);
             if (rc == BS_OK) rc = check_eval_args(ctx, tree, tp, &dtgt, kp, d_out, d_flags);
+            if (rc == BS_OK && !sorted) rc = sort_targets_beside(ctx, &dtgt, perm, s, side, &sorted);
             if (rc == BS_OK) {
                 const EvalPre pre{perm, sorted, tree->moments_done};
                 rc = eval_run(ctx, tree, tp, &dtgt, nullptr, 1, kp, d_out, d_flags, d_far, s, &pre);
@@ -1353,10 +1358,13 @@ extern "C" int bs_tree_sum(bs_ctx *ctx, const bs_sources *src, const bs_tree_par
         int32_t *perm = scratch.get<int32_t>(tgt->n);
         if (!perm) return scratch.status;
         cudaEvent_t sorted = nullptr;
-        rc = sort_targets_beside(ctx, tgt, perm, s, side, &sorted);
+        // the target sort is queued on the side stream while the node count travels back, so that the device
+        // starts on the segments' keys at once
+        auto sort_hook = [&]() -> int { return sort_targets_beside(ctx, tgt, perm, s, side, &sorted); };
         bs_tree *tree = nullptr;
-        if (rc == BS_OK) rc = tree_build(ctx, src, tp, &tree, s, false, {}, side);
+        rc = tree_build(ctx, src, tp, &tree, s, false, sort_hook, side);
         if (rc == BS_OK) rc = check_eval_args(ctx, tree, tp, tgt, kp, out, flags);
+        if (rc == BS_OK && !sorted) rc = sort_hook();  // (a build that returned before its hook ran)
         if (rc == BS_OK) {
             const EvalPre pre{perm, sorted, tree->moments_done};
             rc = eval_run(ctx, tree, tp, tgt, nullptr, 1, kp, out, flags, far_counts, s, &pre);
