@@ -1696,19 +1696,23 @@ __global__ void __launch_bounds__(128) bound_up_kernel(const int32_t *leaves, co
     }
 }
 
-// The bounding radius (bound^2 from leaf_geometry_kernel or bound_up_kernel), the centre and core of the internal
-// nodes (from their boxes and cores) and the traversal record of every node: all that the walk reads.
-__global__ void node_rec_kernel(int64_t count, const unsigned long long *bound2,
-                                const unsigned long long *boxbits, const unsigned long long *corebits,
-                                double *centre, double *core, const int64_t *lo, const int64_t *hi,
-                                const int64_t *left, const int64_t *right, double *bound, NodeRec *nodes) {
+// The centre (box midpoint) and core of every internal node, from the boxes and cores the leaves folded in.
+__global__ void node_centre_kernel(int64_t count, const int64_t *left, const unsigned long long *boxbits,
+                                   const unsigned long long *corebits, double *centre, double *core) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count || left[j] < 0) return;
+    for (int x = 0; x < 3; ++x)
+        centre[3 * j + x] = 0.5 * (from_ordered(boxbits[6 * j + x]) + from_ordered(boxbits[6 * j + 3 + x]));
+    core[j] = __longlong_as_double((long long)corebits[j]);
+}
+
+// The bounding radius (bound^2 from leaf_geometry_kernel or bound_up_kernel) and the traversal record of every node:
+// all that the walk reads.
+__global__ void node_rec_kernel(int64_t count, const unsigned long long *bound2, const double *centre,
+                                const double *core, const int64_t *lo, const int64_t *hi, const int64_t *left,
+                                const int64_t *right, double *bound, NodeRec *nodes) {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= count) return;
-    if (left[j] >= 0) {
-        for (int x = 0; x < 3; ++x)
-            centre[3 * j + x] = 0.5 * (from_ordered(boxbits[6 * j + x]) + from_ordered(boxbits[6 * j + 3 + x]));
-        core[j] = __longlong_as_double((long long)corebits[j]);
-    }
     const double b = sqrt(__longlong_as_double((long long)bound2[j])) * (1.0 + 1e-12);
     bound[j] = b;
     nodes[j] = node_record(j, b, centre, core, lo, hi, left, right);
@@ -1734,9 +1738,10 @@ __global__ void node_final_kernel(int64_t count, const double *sums, NodeOut o) 
 }
 
 // Bottom-up pipeline in two phases.  Geometry, on s: leaf boxes, centres, cores and bounds, each leaf folding its box
-// and core into its ancestors, the internal nodes' exact bounds (every leaf's endpoints against its ancestors'
-// centres) and the traversal records.  Moments, on `side` when given (after s reached the end of the geometry; t->moments_done
-// marks their end) or else on s: leaf sums, the internal nodes' translated sums, the far records.  What the moment
+// and core into its ancestors, the internal centres and cores, then (after the moment phase is queued) the internal
+// nodes' exact bounds (every leaf's endpoints against its ancestors' centres) and the traversal records.  Moments, on
+// `side` when given (once s has the centres, beside the bounds and records; t->moments_done marks their end) or else
+// on s: leaf sums, the internal nodes' translated sums, the far records.  What the moment
 // phase reads lives with the tree when it runs on the side stream (freed with the tree, after the evaluation that
 // waited for it), else in scratch.
 template <int PARTS>
@@ -1765,17 +1770,16 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
     const unsigned leaf_blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((count + 3) / 4, (int64_t)sms * 16));
     leaf_geometry_kernel<<<leaf_blocks, 128, 0, s>>>(leaves, nleaves, t->lo, t->hi, geo_order, geo, parent, ends,
                                                       boxbits, corebits, t->centre, t->core, bound2);
-    bound_up_kernel<<<leaf_blocks, 128, 0, s>>>(leaves, nleaves, t->lo, t->hi, parent, ends, boxbits, bound2);
-    node_rec_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, bound2, boxbits, corebits, t->centre, t->core, t->lo,
-                                                            t->hi, t->left, t->right, t->bound, t->nodes);
-    BS_CHECK_LAUNCH("node records");
+    node_centre_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->left, boxbits, corebits, t->centre, t->core);
+    BS_CHECK_LAUNCH("node geometry");
+    // the moments need the centres only: they start here, beside the exact bounds and the node records
     cudaStream_t ms = s;
     if (defer) {
-        cudaEvent_t geometry;
-        BS_CUDA(cudaEventCreateWithFlags(&geometry, cudaEventDisableTiming));
-        cudaEventRecord(geometry, s);
-        cudaStreamWaitEvent(side, geometry, 0);
-        cudaEventDestroy(geometry);
+        cudaEvent_t centres;
+        BS_CUDA(cudaEventCreateWithFlags(&centres, cudaEventDisableTiming));
+        cudaEventRecord(centres, s);
+        cudaStreamWaitEvent(side, centres, 0);
+        cudaEventDestroy(centres);
         ms = side;
     }
     constexpr int LW = leaf_warps<PARTS>();
@@ -1803,6 +1807,10 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
     // one warp per block: the thread per node is long, so the nodes spread over every SM
     node_final_kernel<PARTS><<<dim3(blocks_for(count, 32), PARTS >= MOM_PARTS4 ? 4 : 1), 32, 0, ms>>>(count, sums, out);
     BS_CHECK_LAUNCH("bottom-up moments");
+    bound_up_kernel<<<leaf_blocks, 128, 0, s>>>(leaves, nleaves, t->lo, t->hi, parent, ends, boxbits, bound2);
+    node_rec_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, bound2, t->centre, t->core, t->lo, t->hi, t->left,
+                                                            t->right, t->bound, t->nodes);
+    BS_CHECK_LAUNCH("node records");
     return BS_OK;
 }
 
