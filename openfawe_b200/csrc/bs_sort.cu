@@ -302,6 +302,27 @@ int radix_sort(uint64_t *keys, int32_t *vals, int64_t n, int begin_bit, int end_
     return BS_OK;
 }
 
+const int *sort_fault_flag() {
+    // the flag's device address, asked once per device
+    static const int *addr[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    if (!addr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_sort_fault) != cudaSuccess) return nullptr;
+        addr[dev] = static_cast<const int *>(p);
+    }
+    return addr[dev];
+}
+
+int sort_fault_seen(int fault) {
+    if (!fault) return BS_OK;
+    const int zero = 0;
+    cudaMemcpyToSymbol(g_sort_fault, &zero, sizeof(int));
+    set_error("radix sort: a look-back wait ran out (the sorted order is not valid)");
+    return BS_ERR_TIMEOUT;
+}
+
 int check_sort_fault() {
     int fault = 0;
     BS_CUDA(cudaMemcpyFromSymbol(&fault, g_sort_fault, sizeof(int)));

@@ -15,5 +15,9 @@ int radix_sort(uint64_t *keys, int32_t *vals, int64_t n, int begin_bit, int end_
 // After the stream has synchronised: BS_OK, or an error if a sort since the last check gave up waiting on the
 // look-back of an earlier tile (its order is then invalid).  Clears the record.
 int check_sort_fault();
+// The fault flag's device address (null if it cannot be had), for a copy queued with a call's other results; and the
+// check of a flag value read that way (clears the flag and reports the fault, as check_sort_fault).
+const int *sort_fault_flag();
+int sort_fault_seen(int fault);
 
 }  // namespace bs

@@ -993,7 +993,7 @@ int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const b
              const int64_t *target_wake_ptr, int nw, const bs_kernel_params *kp, double *out, int8_t *flags,
              int64_t *far_counts, cudaStream_t s, const EvalPre *pre = nullptr) {
     Scratch scratch(ctx->pool, s);
-    unsigned long long *state = scratch.get<unsigned long long>(6);
+    unsigned long long *state = scratch.get<unsigned long long>(7);  // flags, 5 counters, sort fault
     if (!state) return scratch.status;
     cudaEvent_t e0, e1, marks[3];
     cudaEventCreate(&e0);
@@ -1005,9 +1005,12 @@ int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const b
                           pre);
     t_marks = nullptr;
     cudaEventRecord(e1, s);
-    unsigned long long host[6] = {0, 0, 0, 0, 0, 0};
+    unsigned long long host[7] = {0, 0, 0, 0, 0, 0, 0};
     cudaError_t le = cudaSuccess;
-    if (rc == BS_OK) le = cudaMemcpyAsync(host, state, sizeof host, cudaMemcpyDeviceToHost, s);
+    // the sort-fault flag travels back with the counters: one round trip
+    const int *fault = sort_fault_flag();
+    if (rc == BS_OK && fault) le = cudaMemcpyAsync(state + 6, fault, sizeof(int), cudaMemcpyDeviceToDevice, s);
+    if (rc == BS_OK && le == cudaSuccess) le = cudaMemcpyAsync(host, state, sizeof host, cudaMemcpyDeviceToHost, s);
     if (le == cudaSuccess) le = cudaStreamSynchronize(s);
     float ms = 0.f, walk_ms = 0.f, list_ms = 0.f;
     if (rc == BS_OK && le == cudaSuccess) {
@@ -1020,7 +1023,7 @@ int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const b
     for (auto &m : marks) cudaEventDestroy(m);
     if (rc != BS_OK) return rc;
     if (le != cudaSuccess) return cuda_fail(le, "tree evaluation");
-    rc = check_sort_fault();
+    rc = fault ? sort_fault_seen((int)(host[6] & 0xffffffffull)) : check_sort_fault();
     if (rc != BS_OK) return rc;
     ctx->stats.points = tgt->n;
     ctx->stats.segments = tree->m;
