@@ -1306,6 +1306,9 @@ __device__ __forceinline__ void leaf_extent(int lane, int64_t a, int64_t b, cons
     }
 }
 
+// Ancestors a leaf lists for bound_up_kernel (the nearest first, -1 after the root when fewer).
+constexpr int ANC_LIST = 16;
+
 // One warp per leaf: box, core and centre from the leaf's segments (and their tree-ordered endpoints into ends), then
 // bound^2 (the largest squared distance from the centre to an endpoint) into bound2 as its bit pattern.  Seven lanes
 // then fold the box's six bounds and the core into every ancestor (atomicMin / atomicMax on ordered bits: the union
@@ -1315,7 +1318,8 @@ __global__ void __launch_bounds__(128) leaf_geometry_kernel(const int32_t *leave
                                                             const int32_t *order, const SegGeo *geo, const int2 *up,
                                                             EndPts *ends, unsigned long long *boxbits,
                                                             unsigned long long *corebits, double *centre,
-                                                            double *core, unsigned long long *bound2) {
+                                                            double *core, unsigned long long *bound2,
+                                                            int32_t *anc_list) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5), n = *nleaves;
     for (int64_t w = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n; w += warps) {
@@ -1348,11 +1352,14 @@ __global__ void __launch_bounds__(128) leaf_geometry_kernel(const int32_t *leave
             const unsigned long long v = lane < 6 ? ordered_bits(bv) : (unsigned long long)__double_as_longlong(c);
             if (lane < 6) boxbits[6 * j + lane] = v;
             else corebits[j] = v;
-            for (int node = up[j].x, depth = 0; node >= 0 && depth < 4096; node = up[node].x, ++depth) {
+            int depth = 0;
+            for (int node = up[j].x; node >= 0 && depth < 4096; node = up[node].x, ++depth) {
                 if (lane < 3) atomicMin(boxbits + 6 * (int64_t)node + lane, v);
                 else if (lane < 6) atomicMax(boxbits + 6 * (int64_t)node + lane, v);
                 else atomicMax(corebits + node, v);
+                if (lane == 6 && depth < ANC_LIST) anc_list[(int64_t)ANC_LIST * w + depth] = node;
             }
+            if (lane == 6 && depth < ANC_LIST) anc_list[(int64_t)ANC_LIST * w + depth] = -1;
         }
     }
 }
@@ -1649,30 +1656,39 @@ __global__ void __launch_bounds__(128, 6) bottom_up_kernel(const int32_t *leaves
 // Bound^2 of every internal node, exactly: one warp per leaf folds the largest squared distance from each of the
 // leaf's ancestors' centres (the midpoints of their boxes) to the leaf's tree-ordered endpoints into that ancestor's
 // bound2 with an integer atomicMax (non-negative doubles order like their bit patterns: the same value in any order).
-// The ancestors go eight at a time, their centres in registers, so that the leaf's endpoints are read once a group.
+// The ancestors go eight at a time, their centres in registers, so that the leaf's endpoints are read once a group;
+// the first ANC_LIST come from the leaf pass's list (no chain of dependent loads), deeper ones from up[].
 constexpr int BOUND_GROUP = 8;
 __global__ void __launch_bounds__(128) bound_up_kernel(const int32_t *leaves, const unsigned *nleaves,
                                                        const int64_t *lo, const int64_t *hi, const int2 *up,
-                                                       const EndPts *ends, const unsigned long long *boxbits,
-                                                       unsigned long long *bound2) {
+                                                       const EndPts *ends, const double *centre,
+                                                       const int32_t *anc_list, unsigned long long *bound2) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5), n = *nleaves;
     for (int64_t x = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); x < n; x += warps) {
         const int64_t j = leaves[x], a = lo[j], b = hi[j];
         if (b <= a) continue;
-        int node = up[j].x;
-        for (int group = 0; node >= 0 && group < 512; ++group) {
+        const int32_t *al = anc_list + (int64_t)ANC_LIST * x;
+        int next = -1;
+        bool done = false;
+        for (int depth0 = 0; !done && depth0 < 4096; depth0 += BOUND_GROUP) {
             int anc[BOUND_GROUP];
             double c[BOUND_GROUP][3], r2[BOUND_GROUP];
 #pragma unroll
             for (int g = 0; g < BOUND_GROUP; ++g) {
-                anc[g] = node;
+                const int d = depth0 + g;
+                int nd = -1;
+                if (!done) {
+                    nd = d < ANC_LIST ? al[d] : next;
+                    if (nd < 0) done = true;
+                    else if (d >= ANC_LIST - 1) next = up[nd].x;
+                }
+                anc[g] = nd;
                 r2[g] = 0.0;
-                const int64_t q = node >= 0 ? node : 0;
-#pragma unroll
-                for (int xx = 0; xx < 3; ++xx)
-                    c[g][xx] = 0.5 * (from_ordered(boxbits[6 * q + xx]) + from_ordered(boxbits[6 * q + 3 + xx]));
-                if (node >= 0) node = up[node].x;
+                const int64_t q = nd >= 0 ? nd : 0;
+                c[g][0] = centre[3 * q];
+                c[g][1] = centre[3 * q + 1];
+                c[g][2] = centre[3 * q + 2];
             }
             for (int64_t k = a + lane; k < b; k += 32) {
                 const EndPts e = ends[k];
@@ -1751,7 +1767,8 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
     unsigned long long *boxbits = scratch.get<unsigned long long>(7 * count);  // six bounds a node, then the cores
     EndPts *ends = scratch.get<EndPts>(m);
     unsigned long long *bound2 = scratch.get<unsigned long long>(count);
-    if (!boxbits || !ends || !bound2) return scratch.status;
+    int32_t *anc_list = scratch.get<int32_t>((size_t)ANC_LIST * count);
+    if (!boxbits || !ends || !bound2 || !anc_list) return scratch.status;
     unsigned long long *corebits = boxbits + 6 * count;
     double *sums = defer ? t->alloc<double>((size_t)PARTS * count, s) : scratch.get<double>((size_t)PARTS * count);
     int2 *parent = defer ? t->alloc<int2>(count, s) : scratch.get<int2>(count);
@@ -1769,7 +1786,7 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
     BS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, t->device));
     const unsigned leaf_blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((count + 3) / 4, (int64_t)sms * 16));
     leaf_geometry_kernel<<<leaf_blocks, 128, 0, s>>>(leaves, nleaves, t->lo, t->hi, geo_order, geo, parent, ends,
-                                                      boxbits, corebits, t->centre, t->core, bound2);
+                                                      boxbits, corebits, t->centre, t->core, bound2, anc_list);
     node_centre_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->left, boxbits, corebits, t->centre, t->core);
     BS_CHECK_LAUNCH("node geometry");
     // the moments need the centres only: they start here, beside the exact bounds and the node records
@@ -1807,7 +1824,8 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
     // one warp per block: the thread per node is long, so the nodes spread over every SM
     node_final_kernel<PARTS><<<dim3(blocks_for(count, 32), PARTS >= MOM_PARTS4 ? 4 : 1), 32, 0, ms>>>(count, sums, out);
     BS_CHECK_LAUNCH("bottom-up moments");
-    bound_up_kernel<<<leaf_blocks, 128, 0, s>>>(leaves, nleaves, t->lo, t->hi, parent, ends, boxbits, bound2);
+    bound_up_kernel<<<leaf_blocks, 128, 0, s>>>(leaves, nleaves, t->lo, t->hi, parent, ends, t->centre, anc_list,
+                                                 bound2);
     node_rec_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, bound2, t->centre, t->core, t->lo, t->hi, t->left,
                                                             t->right, t->bound, t->nodes);
     BS_CHECK_LAUNCH("node records");
