@@ -128,8 +128,12 @@ int bs_direct(bs_ctx *ctx, const bs_sources *src, const bs_targets *tgt, const b
  * library routine.  Limits and caveats:
  *   - at most BS_NOALLOC_MAX_SEGMENTS segments (BS_ERR_ARG beyond); targets are not limited;
  *   - every GPU that loads the library holds the BS_NOALLOC_SCRATCH_BYTES array until the process exits;
- *   - the first call on a device looks up the array's device address (cudaGetSymbolAddress) with that device current;
- *     make that first call before any stream capture;
+ *   - it runs on the current device; every pointer argument must be device memory of that device (or memory the
+ *     device can address), BS_ERR_ARG otherwise;
+ *   - the first call on a device looks up the array's device address (cudaGetSymbolAddress) with that device current
+ *     and keeps it for the life of the process; make that first call before any stream capture, and make no call on a
+ *     device after cudaDeviceReset (or any reset of its primary context) in the same process, since the kept address
+ *     then no longer maps the array;
  *   - all calls share the one array: calls that overlap on the GPU (other streams, other host threads) race and must
  *     be serialised by the caller;
  *   - blocks the host until the result is ready, like bs_direct. */

@@ -7,10 +7,11 @@ reference's module names so that ``segments_velocity(..., backend='cuda'|'cuda_t
 from .settings import CoreModel, CudaSettings, TreeSettings  # noqa: F401
 
 
-def install(package="openfawe.aero"):
-    """Register the drop-in modules as ``<package>.vortex_cuda`` and ``<package>.vortex_cuda_tree``."""
+def install(package="openfawe.aero", **options):
+    """Register the drop-in modules as ``<package>.vortex_cuda`` and ``<package>.vortex_cuda_tree``; keyword options
+    (tree, order, theta, leaf_size) as in ``openfawe_b200.dropin.install``."""
     from .dropin import install as _install
-    return _install(package)
+    return _install(package, **options)
 
 
 def uninstall(package="openfawe.aero"):

@@ -388,6 +388,23 @@ extern "C" int bs_direct_noalloc(const bs_sources *src, const bs_targets *tgt, c
         set_error("bs_direct_noalloc: device %d out of range", device);
         return BS_ERR_ARG;
     }
+    // every device pointer must belong to the current device, whose copy of the array the call uses
+    const void *device_pointers[] = {tgt->points, out, flags, src->starts, src->directions, src->lengths, src->gamma,
+                                     src->radius};
+    for (const void *ptr : device_pointers) {
+        if (!ptr) continue;
+        cudaPointerAttributes attr;
+        if (cudaPointerGetAttributes(&attr, ptr) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("bs_direct_noalloc: an argument is not a CUDA pointer");
+            return BS_ERR_ARG;
+        }
+        if (attr.type == cudaMemoryTypeDevice && attr.device != device) {
+            set_error("bs_direct_noalloc: an argument lives on device %d, the current device is %d", attr.device,
+                      device);
+            return BS_ERR_ARG;
+        }
+    }
     void *base = nullptr;
     {
         std::lock_guard<std::mutex> guard(g_noalloc_lock);

@@ -1,6 +1,8 @@
 // Exclusive scan and stable least-significant-digit radix sort for the tree builds.
 //
 // Radix sort: 8-bit digits, one kernel per digit with decoupled look-back across tiles (below).
+#include <mutex>
+
 #include "bs_sort.cuh"
 
 namespace bs {
@@ -302,11 +304,16 @@ int radix_sort(uint64_t *keys, int32_t *vals, int64_t n, int begin_bit, int end_
     return BS_OK;
 }
 
+// The fault word is one per device, shared by every context, stream and host thread of the process: a look-back
+// timeout in one sort is reported by (and cleared by) the next call on that device that checks it, which may be
+// another thread's.  A timeout is a broken-device condition, not a per-call result, so that is acceptable here.
 const int *sort_fault_flag() {
-    // the flag's device address, asked once per device
+    // the flag's device address, asked once per device under a lock (host threads may sort at the same time)
+    static std::mutex lock;
     static const int *addr[64] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> guard(lock);
     if (!addr[dev]) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_sort_fault) != cudaSuccess) return nullptr;

@@ -9,13 +9,22 @@ registering this package's modules under the reference's names swaps the backend
 import sys
 
 
-def install(package="openfawe.aero"):
+def install(package="openfawe.aero", *, tree=None, order=None, theta=None, leaf_size=None):
     """Register ``openfawe_b200.vortex_cuda`` / ``vortex_cuda_tree`` / ``vortex_cuda_moments`` / ``vortex_cuda_build``
     under ``<package>``.
 
     Returns the two modules.  Call it before the first GPU-backend call of the process (or after, since the reference
-    imports them inside each call)."""
+    imports them inside each call).
+
+    The keyword options reach the tree path through settings objects the caller cannot change (the reference's
+    TreeSettings refuses orders above 2, its CudaSettings has no tree field): ``tree`` ('median' or 'morton'),
+    ``order`` (0-5), ``theta`` (a number, a dict {caller's theta: theta} or a callable) and ``leaf_size`` apply to
+    every later ``cuda_tree_sum`` call (``vortex_cuda_tree.configure``).  They change the approximation the caller
+    asked for -- for example ``install(tree='morton', order=5, theta={0.04: 0.215}, leaf_size=384)`` swaps the
+    order-2 tree at theta 0.04 for the fifth-order tree at the same error level -- and each call records what it
+    ran in ``Statistics.last['effective']``.  Without options nothing changes."""
     from . import vortex_cuda, vortex_cuda_build, vortex_cuda_moments, vortex_cuda_tree
+    vortex_cuda_tree.configure(tree=tree, order=order, theta=theta, leaf_size=leaf_size)
     modules = dict(vortex_cuda=vortex_cuda, vortex_cuda_tree=vortex_cuda_tree, vortex_cuda_moments=vortex_cuda_moments,
                    vortex_cuda_build=vortex_cuda_build)
     parent = sys.modules.get(package)
@@ -27,7 +36,9 @@ def install(package="openfawe.aero"):
 
 
 def uninstall(package="openfawe.aero"):
-    """Remove the registrations made by ``install``."""
+    """Remove the registrations made by ``install`` and clear its options."""
+    from . import vortex_cuda_tree
+    vortex_cuda_tree.configure()
     for name in ("vortex_cuda", "vortex_cuda_tree", "vortex_cuda_moments", "vortex_cuda_build"):
         module = sys.modules.get(f"{package}.{name}")
         if module is not None and module.__name__.startswith("openfawe_b200."):

@@ -29,6 +29,53 @@ SUPPORTED_MODELS = (0, 1, 2)  # NONE, RANKINE, LAMB_OSEEN (vortex_tree.py:46)
 DEVICE_STACK = 128
 
 
+# Options set by ``configure`` (or ``openfawe_b200.install(...)``) for callers that pass the reference's own settings
+# objects, which cannot express them: its TreeSettings refuses orders above 2 and its CudaSettings has no tree field
+# (vortex.py:30-116).  Each one changes the approximation the caller asked for, and ``Statistics.last['effective']``
+# records what a call ran.
+OPTIONS = {}
+_OPTION_NAMES = ("tree", "order", "theta", "leaf_size")
+
+
+def configure(tree=None, order=None, theta=None, leaf_size=None):
+    """Set (or, with no arguments, clear) the options every later ``cuda_tree_sum`` call applies.
+
+    * ``tree``: 'median' or 'morton', for calls whose settings have no ``tree`` field (an explicit field wins);
+    * ``order``: expansion order 0-5 in place of ``TreeSettings.order`` (the ``order=`` keyword of a call wins);
+    * ``theta``: the opening ratio in place of ``TreeSettings.theta``: a number, a dict {caller's theta: theta}
+      (thetas not in it are kept), or a callable of the caller's theta;
+    * ``leaf_size``: in place of ``TreeSettings.leaf_size``.
+    Returns the previous options."""
+    if tree is not None and tree not in ("median", "morton"):
+        raise ValueError("tree must be 'median' or 'morton'")
+    if order is not None and order not in (0, 1, 2, 3, 4, 5):
+        raise ValueError("tree order must be 0, 1, 2, 3, 4 or 5")
+    if leaf_size is not None and (isinstance(leaf_size, bool) or int(leaf_size) < 1):
+        raise ValueError("leaf size must be a positive integer")
+    if theta is not None and not (callable(theta) or isinstance(theta, dict)) and not 0 < float(theta) < 1:
+        raise ValueError("tree theta must lie strictly between 0 and 1")
+    previous = dict(OPTIONS)
+    OPTIONS.clear()
+    OPTIONS.update({k: v for k, v in zip(_OPTION_NAMES, (tree, order, theta, leaf_size)) if v is not None})
+    return previous
+
+
+def effective(tree, settings, order=None):
+    """(kind, order, theta, leaf_size) that a call with these settings runs under the configured options."""
+    kind = getattr(settings, "tree", None) or OPTIONS.get("tree", "median")
+    expansion = int(order if order is not None else OPTIONS.get("order", tree.order))
+    theta = float(tree.theta)
+    mapped = OPTIONS.get("theta")
+    if callable(mapped):
+        theta = float(mapped(theta))
+    elif isinstance(mapped, dict):
+        theta = float(mapped.get(theta, theta))
+    elif mapped is not None:
+        theta = float(mapped)
+    leaf = int(OPTIONS.get("leaf_size", tree.leaf_size))
+    return kind, expansion, theta, leaf
+
+
 class Statistics:
     last = {}
     last_far_counts = None
@@ -44,23 +91,25 @@ def cuda_tree_sum(points, starts, directions, lengths, gamma, radius, model, csr
     """Return (velocity, any_flag) like ``vortex_tree.tree_sum`` for the same inputs, evaluated on the GPU.
 
     ``order`` (keyword, not in the reference) overrides ``tree.order``; 3, 4 and 5 select the third- to fifth-order
-    far fields, which reach the accuracy of order 2 at larger opening angles."""
+    far fields, which reach the accuracy of order 2 at larger opening angles.  Options set by ``configure`` apply to
+    every call (see there)."""
     if not VC.available():
         raise ValueError(f"the cuda tree evaluation needs a CUDA device ({VC.probe_error()})")
     if int(model) not in SUPPORTED_MODELS and np.any(np.asarray(radius) > 0):
         raise ValueError("tree backend supports core models NONE, RANKINE and LAMB_OSEEN only")
     if tree.theta >= 1.0:
         raise ValueError("tree theta must be below one")
+    kind, expansion, theta, leaf_size = effective(tree, settings, order)
+    if not 0.0 < theta < 1.0:
+        raise ValueError("tree theta must lie strictly between 0 and 1 (after the configured mapping)")
     precision = settings.precision
     gpu64 = getattr(settings, "suspect", "cpu") == "gpu64"
     if gpu64 and precision == "fp64":
         raise ValueError("suspect='gpu64' is for the single precisions only")
     block = int(settings.block if block is None else block)
-    expansion = int(tree.order if order is None else order)
     if expansion not in (0, 1, 2, 3, 4, 5):
         raise ValueError("tree order must be 0, 1, 2, 3, 4 or 5")
     _, _, near = VC._check_settings(settings)
-    kind = getattr(settings, "tree", "median")
     points = np.ascontiguousarray(points, dtype=np.float64)
     n, m = len(points), len(starts)
     if n == 0 or m == 0:
@@ -81,8 +130,8 @@ def cuda_tree_sum(points, starts, directions, lengths, gamma, radius, model, csr
             upload_s = time.perf_counter() - tick
             tick = time.perf_counter()
             d_out, d_flags, d_far = engine.tree_sum(sources, targets, int(model), singularity, precision, block,
-                                                    near, tree.theta, expansion, tree.leaf_size, tree.core_clearance,
-                                                    kind, stack_limit=limit)
+                                                    near, theta, expansion, leaf_size, tree.core_clearance, kind,
+                                                    stack_limit=limit)
             total_s = time.perf_counter() - tick
             tick = time.perf_counter()
             out, flags, far = engine.to_host_many((d_out, d_flags, d_far), ((n, 3), (n,), (n,)),
@@ -93,9 +142,8 @@ def cuda_tree_sum(points, starts, directions, lengths, gamma, radius, model, csr
             # host arrays: one library call from the host arrays to the host results (uploads overlap the build)
             tick = time.perf_counter()
             out, flags, far = engine.tree_sum_host(points, starts, directions, lengths, gamma, radius, csr,
-                                                   int(model), singularity, precision, block, near, tree.theta,
-                                                   expansion, tree.leaf_size, tree.core_clearance, kind, limit,
-                                                   device)
+                                                   int(model), singularity, precision, block, near, theta,
+                                                   expansion, leaf_size, tree.core_clearance, kind, limit, device)
             stats = engine.last_stats(device)
             upload_s, download_s = 1e-3 * stats["upload_ms"], 1e-3 * stats["download_ms"]
             total_s = time.perf_counter() - tick - upload_s - download_s
@@ -112,6 +160,7 @@ def cuda_tree_sum(points, starts, directions, lengths, gamma, radius, model, csr
                            evaluate_ms=stats["evaluate_ms"], near_pairs=int(stats["near_pairs"]),
                            far_evaluations=int(stats["far_evaluations"]), fp64_pairs=int(stats["fp64_pairs"]),
                            visits=int(stats["visits"]),
+                           effective=dict(tree=kind, order=expansion, theta=theta, leaf_size=leaf_size),
                            **({"moments": "gpu"} if getattr(settings, "moments", "cpu") == "gpu" else {}),
                            **({"build": "gpu"} if getattr(settings, "build", "cpu") == "gpu" else {}))
     if gpu64:

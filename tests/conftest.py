@@ -1,6 +1,7 @@
 """Shared fixtures.  ``-m gpu`` tests need a CUDA device and the built libbs_b200.so; the rest run on CPU."""
 import os
 import sys
+from dataclasses import dataclass
 
 import numpy as np
 import pytest
@@ -30,3 +31,28 @@ def device():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     return torch.cuda.current_device()
+
+
+# The reference's own settings types as a caller holds them (src/openfawe/aero/vortex.py:30-116): the same field names
+# and defaults and nothing more (no ``tree`` field, orders 0-2), for tests of what an unchanged caller reaches.
+@dataclass(frozen=True)
+class ReferenceTreeSettings:
+    theta: float = 0.5
+    order: int = 2
+    leaf_size: int = 32
+    core_clearance: float = 3.0
+
+    def __post_init__(self):
+        if self.order not in (0, 1, 2):
+            raise ValueError("tree order must be 0, 1 or 2")
+
+
+@dataclass(frozen=True)
+class ReferenceCudaSettings:
+    precision: str = "mixed"
+    block: int = 128
+    suspect: str = "cpu"
+    control: str = "cpu"
+    moments: str = "cpu"
+    build: str = "cpu"
+    rings: str = "cpu"

@@ -1,8 +1,9 @@
 """Generate the golden fixtures of tests/golden/ by running the reference's own code.
 
-Run in a container that holds the reference project (read-only) at REFERENCE (default /root/reference):
+Run in a container that holds the reference project (read-only); give its location with --reference or the
+OPENFAWE_REFERENCE environment variable:
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <path of the reference project> [--only NAME]
 
 It imports the reference's numba backends (src/openfawe/aero/vortex_numba.py, vortex_tree.py) with the numba cache
 redirected outside the reference tree, evaluates them on small seeded cases and writes compressed ``.npz`` files beside
@@ -51,6 +52,15 @@ def segment_arrays(nodes, edges):
     delta = nodes[edges[:, 1]] - starts
     lengths = np.hypot(np.hypot(delta[..., 0], delta[..., 1]), delta[..., 2])
     return starts, delta / lengths[:, None], lengths
+
+
+def input_digest(case):
+    """SHA-256 over the bytes of a case's backend inputs (points, starts, directions, lengths, gamma, radius)."""
+    import hashlib
+    h = hashlib.sha256()
+    for key in ("points", "starts", "directions", "lengths", "gamma", "radius"):
+        h.update(np.ascontiguousarray(case[key], dtype=np.float64).tobytes())
+    return h.hexdigest()
 
 
 def ring_lattice(seed=11, rows=24, span=17):
@@ -108,9 +118,12 @@ def exclusion_cases(seed):
 
 def main():
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--reference", default=os.environ.get("OPENFAWE_REFERENCE"),
+                        help="the reference project's root (default: $OPENFAWE_REFERENCE)")
     parser.add_argument("--only", default=None, help="write only this fixture (e.g. network.npz)")
     args = parser.parse_args()
+    if not args.reference:
+        parser.error("give the reference project's root with --reference or OPENFAWE_REFERENCE")
     os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(tempfile.gettempdir(), "numba_reference_cache"))
     sys.path.insert(0, os.path.join(args.reference, "src"))
     sys.path.insert(0, REPO)
@@ -194,6 +207,36 @@ def main():
         save("operators.npz", **out)
         if args.only:
             return
+
+    for name, make in (("c2_sheet.npz", lambda: wakes.selftest_sheet(468, seed=468)),
+                       ("c2_rotor.npz", lambda: wakes.rotor_sheet(468, seed=468, targets=20570))):
+        if args.only not in (name, None):
+            continue
+        # Full-size C2 wakes (102k segments x 20,570 targets): the reference's numba direct sum and its CPU tree code
+        # at the reference default (theta 0.5) and the production setting (theta 0.2), order 2, leaf 32, clearance 3
+        # (vortex.py:30-55; apps/studio/openfawe_studio/selftest.py:35).  The inputs come from this repository's
+        # generators; their SHA-256 is stored so that a test can check it regenerated the same arrays.
+        import time
+        import numba
+        case = make()
+        args_ = wakes.backend_args(case)
+        csr = vn.exclusion_csr(len(case["points"]), np.zeros((0, 2), dtype=np.int64))
+        out = dict(inputs_sha256=np.array(input_digest(case)), threads=np.array(numba.get_num_threads()))
+        vn.direct_sum(args_[0][:64], *args_[1:], (csr[0][:65], csr[1]), "raise")   # compile
+        tick = time.perf_counter()
+        out["direct"], flagged = vn.direct_sum(*args_, csr, "raise")
+        out["direct_s"], out["direct_flag"] = np.array(time.perf_counter() - tick), np.array(flagged)
+        for theta in (0.5, 0.2):
+            settings = type("S", (), dict(theta=theta, order=2, leaf_size=32, core_clearance=3.0))()
+            vt.tree_sum(*args_, csr, "raise", settings)                          # compile, warm
+            tick = time.perf_counter()
+            u, flagged = vt.tree_sum(*args_, csr, "raise", settings)
+            key = f"t{int(round(theta * 100))}"
+            out[key], out[key + "_s"], out[key + "_flag"] = u, np.array(time.perf_counter() - tick), np.array(flagged)
+            out[key + "_mean_far"] = np.array(vt.TreeStatistics.last["mean_far_nodes"])
+        save(name, **out)
+    if args.only in ("c2_sheet.npz", "c2_rotor.npz"):
+        return
 
     if args.only == "network.npz" or args.only is None:
         from openfawe.aero import network_numba as nn

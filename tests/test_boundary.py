@@ -145,3 +145,29 @@ def test_install_registers_build_and_moments_modules_and_patches_functions():
     finally:
         for name in fakes:
             del sys.modules[name]
+
+
+def test_install_options_map_reference_settings():
+    """install(...) options reach calls whose settings cannot express them, and record what they change."""
+    from conftest import ReferenceCudaSettings, ReferenceTreeSettings
+    import openfawe_b200
+    from openfawe_b200 import vortex_cuda_tree as VCT
+    from openfawe_b200.settings import CudaSettings
+    tree, cuda = ReferenceTreeSettings(theta=0.04), ReferenceCudaSettings()
+    try:
+        assert VCT.effective(tree, cuda) == ("median", 2, 0.04, 32)
+        openfawe_b200.install("openfawe_b200_test_pkg", tree="morton", order=5, theta={0.04: 0.215}, leaf_size=384)
+        assert VCT.effective(tree, cuda) == ("morton", 5, 0.215, 384)
+        # thetas outside the dict are kept; an explicit tree field and the order= keyword win
+        assert VCT.effective(ReferenceTreeSettings(theta=0.2), cuda) == ("morton", 5, 0.2, 384)
+        assert VCT.effective(tree, CudaSettings(tree="median"), order=3) == ("median", 3, 0.215, 384)
+        VCT.configure(theta=lambda t: 5 * t)
+        assert VCT.effective(tree, cuda) == ("median", 2, 0.2, 32)
+        VCT.configure(theta=0.3)
+        assert VCT.effective(tree, cuda)[2] == 0.3
+        for bad in (dict(tree="octree"), dict(order=6), dict(leaf_size=0), dict(theta=1.5)):
+            with pytest.raises(ValueError):
+                VCT.configure(**bad)
+    finally:
+        openfawe_b200.uninstall("openfawe_b200_test_pkg")
+    assert VCT.OPTIONS == {} and VCT.effective(tree, cuda) == ("median", 2, 0.04, 32)

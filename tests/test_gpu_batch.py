@@ -1,14 +1,17 @@
-"""Batched wakes: one forest over many wakes (bs_forest_build / bs_forest_eval / bs_forest_graph) against per-wake
-evaluation.
+"""Batched wakes: one forest over many wakes (bs_forest_build / bs_forest_eval / bs_forest_graph) against each wake's
+exact direct sum from the CPU oracle (oracle/bs_oracle.c, pinned to the reference's numba direct sum).
 
 * A forest at a vanishing opening angle accepts no cell: every wake's velocity equals that wake's own FP64 direct sum
   within 1e-12 * max|u| (no cross-wake interaction, far counts all zero).
-* Mixed precision at the bench's opening angle: each wake within 1e-5 relative L2 of its FP64 direct sum.
+* Mixed precision at a small opening angle: each wake within 1e-5 relative L2 of its FP64 direct sum.
 * The captured graph replays to the same bits as a fresh evaluation, also after the targets moved in place.
 * The autotuned batch and the one-call-per-wake path agree.
 """
 import numpy as np
 import pytest
+
+from conftest import no_exclusions
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -26,14 +29,14 @@ def small_cases():
     return cases + [tiny, one]
 
 
-def per_wake_direct(cases, device):
-    from openfawe_b200 import engine
+def per_wake_direct(cases, device=None):
+    """Each wake's FP64 direct sum from the CPU oracle."""
+    from openfawe_b200 import wakes
     out = []
     for c in cases:
-        src = engine.Sources(c["starts"], c["directions"], c["lengths"], c["gamma"], c["radius"], device)
-        u, flags = engine.direct(src, engine.Targets(c["points"], None, device), c["model"], "raise", "fp64")
-        assert not flags.any()
-        out.append(u.cpu().numpy())
+        u, flagged = O.direct_sum(*wakes.backend_args(c), no_exclusions(len(c["points"])), "raise")
+        assert not flagged
+        out.append(u)
     return out
 
 
@@ -90,6 +93,7 @@ def test_autotune_and_sequential_agree(device):
     u, _, _ = b.evaluate(theta=0.05, block=tuned["choice"][1])
     times, outs = batch.sequential(cases, device, theta=0.05)
     assert len(times) == 4 and np.all(times > 0)
-    for got, ref in zip(b.split(u.cpu().numpy()), outs):
-        ref = ref.cpu().numpy()
-        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-4
+    for got, seq, ref in zip(b.split(u.cpu().numpy()), outs, per_wake_direct(cases)):
+        seq = seq.cpu().numpy()
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-5
+        assert np.linalg.norm(seq - ref) / np.linalg.norm(ref) < 1e-5

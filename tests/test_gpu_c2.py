@@ -1,0 +1,139 @@
+"""Full-size C2 wakes (102k segments x 20,570 targets) against the reference's own outputs at that size.
+
+tests/golden/c2_sheet.npz (the reference self-test's sheet, 468 rows, seed 468: 102,382 segments, Lamb-Oseen core
+0.075 m) and c2_rotor.npz (the 468-row rotor-ring + wing-sheet wake: 102,446 segments, core 0.05 m) hold the
+reference's numba direct sum and its CPU tree code at theta 0.5 (its default) and 0.2 (the production setting), order
+2, leaf 32, clearance 3 (tests/golden/make_golden.py).  Bounds:
+
+* FP64 direct sum: the reference's A1, |u - u_ref| <= 1e-12 * sum_s |u_s| per target (tests/test_vortex_numba.py:3-5).
+* FP64 median tree: the self-test's 1e-10 * max|u| against the CPU tree (apps/studio/openfawe_studio/selftest.py:413).
+* Mixed median tree: max and rms error against the CPU tree within 0.1 x the CPU tree's own max and rms error against
+  the direct sum (selftest.py:415-417).
+* The bench's configuration (fifth-order Morton tree, theta 0.215, leaf 384, mixed): <= 1e-6 relative L2 against the
+  reference's direct sum, and at most 1e-6 * max|u| at any target.
+"""
+import numpy as np
+import pytest
+
+from conftest import ReferenceCudaSettings, ReferenceTreeSettings, golden, no_exclusions
+
+pytestmark = pytest.mark.gpu
+
+CASES = ("c2_sheet", "c2_rotor")
+
+
+def make_case(name):
+    from openfawe_b200 import wakes
+    if name == "c2_sheet":
+        return wakes.selftest_sheet(468, seed=468)
+    return wakes.rotor_sheet(468, seed=468, targets=20570)
+
+
+def digest(case):
+    import hashlib
+    h = hashlib.sha256()
+    for key in ("points", "starts", "directions", "lengths", "gamma", "radius"):
+        h.update(np.ascontiguousarray(case[key], dtype=np.float64).tobytes())
+    return h.hexdigest()
+
+
+def sum_of_magnitudes(case, device, chunk=512):
+    """sum_s |u_s| per target from the library's FP64 pair matrix (one chunk of targets at a time)."""
+    import torch
+    from openfawe_b200 import engine, operators
+    src = engine.Sources(case["starts"], case["directions"], case["lengths"], case["gamma"], case["radius"], device)
+    g = torch.as_tensor(np.abs(case["gamma"]), device=device)
+    out = np.zeros(len(case["points"]))
+    for a in range(0, len(case["points"]), chunk):
+        pairs, _ = operators.pair_matrix_device(case["points"][a:a + chunk], src, case["model"], False)
+        out[a:a + chunk] = (torch.linalg.vector_norm(pairs, dim=2) * g[None, :]).sum(dim=1).cpu().numpy()
+        del pairs
+    return out
+
+
+@pytest.fixture(scope="module", params=CASES)
+def c2(request):
+    case = make_case(request.param)
+    g = golden(f"{request.param}.npz")
+    assert digest(case) == str(g["inputs_sha256"]), "the wake generator no longer reproduces the fixture's inputs"
+    return request.param, case, g
+
+
+def test_c2_fp64_direct_within_a1(c2, device):
+    from openfawe_b200.settings import CudaSettings
+    from openfawe_b200.vortex_cuda import cuda_sum
+    from openfawe_b200.wakes import backend_args
+    name, case, g = c2
+    args = (*backend_args(case), no_exclusions(len(case["points"])), "raise")
+    u, flag = cuda_sum(*args, CudaSettings("fp64"))
+    assert flag == bool(g["direct_flag"])
+    err = np.linalg.norm(u - g["direct"], axis=1)
+    bound = 1e-12 * sum_of_magnitudes(case, device)
+    assert np.all(err <= bound), (name, float((err / bound).max()))
+
+
+@pytest.mark.parametrize("theta", [0.5, 0.2])
+def test_c2_median_tree_within_selftest_bounds(c2, device, theta):
+    from openfawe_b200.settings import CudaSettings, TreeSettings
+    from openfawe_b200.vortex_cuda_tree import Statistics, cuda_tree_sum
+    from openfawe_b200.wakes import backend_args
+    name, case, g = c2
+    key = f"t{int(round(theta * 100))}"
+    cpu, direct = g[key], g["direct"]
+    args = (*backend_args(case), no_exclusions(len(case["points"])), "raise", TreeSettings(theta, 2, 32, 3.0))
+    norm = lambda v: np.linalg.norm(v, axis=1)  # noqa: E731
+    tree_err = norm(cpu - direct)
+    scale = norm(cpu).max()
+    u64, flag = cuda_tree_sum(*args, CudaSettings("fp64"))
+    assert flag == bool(g[key + "_flag"])
+    assert norm(u64 - cpu).max() <= 1e-10 * scale, (name, theta, float(norm(u64 - cpu).max() / scale))
+    # the accepted nodes are the CPU's: the mean far count per target is the reference's
+    assert Statistics.last["mean_far_nodes"] == pytest.approx(float(g[key + "_mean_far"]), rel=0, abs=1e-9)
+    for suspect in ("cpu", "gpu64"):
+        um, flag = cuda_tree_sum(*args, CudaSettings("mixed", 128, suspect))
+        e = norm(um - cpu)
+        assert flag == bool(g[key + "_flag"])
+        assert e.max() <= 0.1 * tree_err.max(), (name, theta, float(e.max() / tree_err.max()))
+        assert np.sqrt(np.mean(e ** 2)) <= 0.1 * np.sqrt(np.mean(tree_err ** 2)), (name, theta)
+
+
+def test_c2_bench_configuration_within_1e6(c2, device):
+    """The configuration the benchmark times, through the engine: <= 1e-6 relative L2 and max error."""
+    from openfawe_b200 import engine
+    name, case, g = c2
+    src = engine.Sources(case["starts"], case["directions"], case["lengths"], case["gamma"], case["radius"], device)
+    tgt = engine.Targets(case["points"], None, device)
+    u, flags, _ = engine.tree_sum(src, tgt, case["model"], "raise", "mixed", 128, 3.0, 0.215, 5, 384, 3.0, "morton")
+    u = u.cpu().numpy()
+    direct = g["direct"]
+    assert not flags.cpu().numpy().any()
+    rel = np.linalg.norm(u - direct) / np.linalg.norm(direct)
+    worst = np.linalg.norm(u - direct, axis=1).max() / np.linalg.norm(direct, axis=1).max()
+    assert rel <= 1e-6 and worst <= 1e-6, (name, rel, worst)
+
+
+def test_unchanged_caller_reaches_the_fifth_order_path(c2, device):
+    """A caller that passes the reference's own TreeSettings(theta=0.04) and CudaSettings() gets the fifth-order Morton
+    tree once install(...) maps them, with the same result as the engine call of that configuration."""
+    import openfawe_b200
+    from openfawe_b200 import engine, vortex_cuda_tree as VCT
+    from openfawe_b200.wakes import backend_args
+    name, case, g = c2
+    if name != "c2_rotor":
+        pytest.skip("one wake is enough")
+    args = (*backend_args(case), no_exclusions(len(case["points"])), "raise")
+    try:
+        openfawe_b200.install("openfawe_b200_test_pkg", tree="morton", order=5, theta={0.04: 0.215}, leaf_size=384)
+        u, flag = VCT.cuda_tree_sum(*args, ReferenceTreeSettings(theta=0.04), ReferenceCudaSettings("mixed", 128))
+        assert VCT.Statistics.last["effective"] == dict(tree="morton", order=5, theta=0.215, leaf_size=384)
+        pairs = VCT.Statistics.last["near_pairs"]
+    finally:
+        openfawe_b200.uninstall("openfawe_b200_test_pkg")
+    src = engine.Sources(case["starts"], case["directions"], case["lengths"], case["gamma"], case["radius"], device)
+    tgt = engine.Targets(case["points"], None, device)
+    ref, _, _ = engine.tree_sum(src, tgt, case["model"], "raise", "mixed", 128, 3.0, 0.215, 5, 384, 3.0, "morton")
+    assert not flag and engine.last_stats(device)["near_pairs"] == pairs
+    assert np.array_equal(u, ref.cpu().numpy())
+    # without options the same caller gets the reference's median order-2 tree
+    VCT.cuda_tree_sum(*args, ReferenceTreeSettings(theta=0.5), ReferenceCudaSettings("mixed", 128))
+    assert VCT.Statistics.last["effective"] == dict(tree="median", order=2, theta=0.5, leaf_size=32)
