@@ -13,6 +13,7 @@ the reference's CPU tree code (its CPU restatement in oracle/) on the host's cor
 """
 import argparse
 import ctypes
+import hashlib
 import json
 import os
 import statistics
@@ -20,6 +21,7 @@ import subprocess
 import sys
 import tempfile
 import time
+from dataclasses import dataclass
 
 import numpy as np
 
@@ -37,6 +39,33 @@ LIST_TRAFFIC = 8.56e6                   # DRAM bytes per list-kernel launch (ncu
 # per far evaluation of order p (3: 180 + 170 for the third term, 4: 350 + 300 for the fourth)
 W_FAR = {0: 40.0, 1: 100.0, 2: 180.0, 3: 350.0, 4: 650.0, 5: 1100.0}
 L2_FLUSH_BYTES = 512 << 20  # larger than the 126 MB L2
+GOLDEN = os.path.join(HERE, "tests", "golden")
+ACCURACY_SAMPLE = 256  # targets at which the reference arm's CPU tree is checked against the oracle's FP64 direct sum
+# The reference's published figures for the 468-row self-test sheet at theta 0.2, order 2, leaf 32 (README.md:88;
+# RTX 4090 D and 22 CPU threads, median of five calls), seconds.
+README_468 = {"cpu_1_thread_s": 2.07, "cpu_22_threads_s": 0.16, "gpu_double_s": 0.14, "gpu_mixed_s": 0.07,
+              "hardware": "NVIDIA RTX 4090 D, 22 CPU threads"}
+
+
+@dataclass(frozen=True)
+class CallerTreeSettings:
+    """The reference's TreeSettings as a caller holds it (vortex.py:30-55): these fields and no others."""
+    theta: float = 0.5
+    order: int = 2
+    leaf_size: int = 32
+    core_clearance: float = 3.0
+
+
+@dataclass(frozen=True)
+class CallerCudaSettings:
+    """The reference's CudaSettings as a caller holds it (vortex.py:58-116): no tree field."""
+    precision: str = "mixed"
+    block: int = 128
+    suspect: str = "cpu"
+    control: str = "cpu"
+    moments: str = "cpu"
+    build: str = "cpu"
+    rings: str = "cpu"
 
 
 def parse():
@@ -50,10 +79,12 @@ def parse():
     p.add_argument("--leaf", type=int, default=LEAF)
     p.add_argument("--order", type=int, default=ORDER, choices=(0, 1, 2, 3, 4, 5))
     p.add_argument("--kind", default="morton", choices=("morton", "median"))
-    p.add_argument("--cpu-sample", type=int, default=1024, help="targets in the CPU-baseline sample")
-    p.add_argument("--no-extras", action="store_true", help="skip the batched-wakes and adjoint measurements")
-    p.add_argument("--tree-only", action="store_true",
-                   help="time the tree path alone (no FP64 direct sum, end-to-end, baselines): for profiler runs")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the batched-wakes, adjoint, C1, C2 and default-path measurements")
+    p.add_argument("--only", default=None, choices=("tree", "direct-fp64", "direct-mixed", "adjoint",
+                                                    "tree-adjoint"),
+                   help="run one call kind alone, warmup + steps times, and print its counters (for profiler runs)")
+    p.add_argument("--tree-only", action="store_const", const="tree", dest="only", help="the same as --only tree")
     return p.parse_args()
 
 
@@ -67,7 +98,8 @@ def config(case, args, extra=None):
                      f"targets, Lamb-Oseen rc 0.05 m",
          "segments": len(case["starts"]), "targets": len(case["points"]), "theta": args.theta, "order": args.order,
          "leaf_size": args.leaf, "tree": args.kind, "precision": "mixed", "l2": "flushed between timed steps (512 MB write)",
-         "parallelism": f"replicas x{args.gpus}"}
+         "parallelism": ("one GPU" if args.gpus <= 1 else
+                         f"one call shared by segments over {args.gpus} GPUs (Morton ranges, all-reduce of the result)")}
     if extra:
         c.update(extra)
     return c
@@ -124,56 +156,91 @@ def measured_peaks():
         return {}
 
 
-def cpu_baseline(case, args, threads=0):
-    """The reference's CPU tree code (vortex_tree.tree_sum, restated in oracle/) on the host cores: the full tree
-    build + moments, and the traversal for a sample of targets, scaled to the whole call."""
-    from oracle import oracle as O
-    n = len(case["points"])
-    sample = min(args.cpu_sample, n)
-    pick = np.linspace(0, n - 1, sample).astype(np.int64)
-    points = case["points"][pick]
-    a = (case["starts"], case["directions"], case["lengths"], case["gamma"], case["radius"])
-    tick = time.perf_counter()
-    lv, ends, alpha, mid = O.segment_geometry(*a[:4])
-    tree = O.build_tree(mid, REF_LEAF)[:5]
-    q = O.node_moments(tree[0], tree[1], tree[2], a[0], ends, alpha, lv, a[4], a[3], threads)
-    w = O.node_contractions(q[4], q[5])
-    build_s = time.perf_counter() - tick
-    tick = time.perf_counter()
-    O.tree_velocity(points, *a, case["model"], "raise", tree, (*q, *w), REF_THETA, REF_ORDER, CLEARANCE,
-                    np.zeros(sample + 1, dtype=np.int64), np.zeros(0, dtype=np.int64), threads)
-    eval_s = time.perf_counter() - tick
-    cores = threads if threads > 0 else (os.cpu_count() or 1)
+def host_cores():
     try:
-        cores = len(os.sched_getaffinity(0)) if threads <= 0 else threads
+        return len(os.sched_getaffinity(0))
     except AttributeError:
-        pass
-    ms = 1e3 * (build_s + eval_s * n / sample)
-    return {"value": ms, "unit": "ms/call", "cores": cores, "kind": "port",
-            "sample": f"full median-split build + moments ({1e3 * build_s:.0f} ms) and the traversal of {sample} of "
-                      f"{n} targets ({1e3 * eval_s:.0f} ms) scaled to all targets; theta {REF_THETA}, order {REF_ORDER} "
-                      f"(the reference's orders stop at 2; this is its setting for the same <= 1e-6 error), "
-                      f"leaf {REF_LEAF}"}
+        return os.cpu_count() or 1
+
+
+def no_exclusions(n):
+    return np.zeros(n + 1, dtype=np.int64), np.zeros(0, dtype=np.int64)
+
+
+def cpu_tree_call(case, theta, order=REF_ORDER, leaf=REF_LEAF, points=None):
+    """One full call of the reference's CPU tree code (vortex_tree.tree_sum, restated in oracle/) on every host core:
+    median-split build, moments, contractions and the traversal of every target.  Returns (seconds, velocity)."""
+    from oracle import oracle as O
+    from openfawe_b200 import wakes
+    args = wakes.backend_args(case)
+    if points is not None:
+        args = (points, *args[1:])
+    tick = time.perf_counter()
+    u, _ = O.tree_sum(*args, no_exclusions(len(args[0])), "raise", theta, order, leaf, CLEARANCE, "median")
+    return time.perf_counter() - tick, u
+
+
+def sample_accuracy(case, u):
+    """Relative L2 and max error of `u` against the oracle's FP64 direct sum at ACCURACY_SAMPLE evenly spaced targets."""
+    from oracle import oracle as O
+    from openfawe_b200 import wakes
+    n = len(case["points"])
+    pick = np.linspace(0, n - 1, min(ACCURACY_SAMPLE, n)).astype(np.int64)
+    args = wakes.backend_args(case)
+    ref, _ = O.direct_sum(case["points"][pick], *args[1:], no_exclusions(len(pick)), "raise")
+    err = np.linalg.norm(u[pick] - ref, axis=1)
+    return {"rel_l2": float(np.linalg.norm(u[pick] - ref) / np.linalg.norm(ref)),
+            "max_err_over_max_speed": float(err.max() / np.linalg.norm(ref, axis=1).max()),
+            "sample": f"{len(pick)} evenly spaced targets against the oracle's FP64 direct sum"}
+
+
+def errors(u, ref):
+    err = np.linalg.norm(u - ref, axis=1)
+    return {"rel_l2": float(np.linalg.norm(u - ref) / np.linalg.norm(ref)),
+            "max_err_over_max_speed": float(err.max() / np.linalg.norm(ref, axis=1).max())}
+
+
+def cpu_baseline(case, direct_host=None):
+    """The reference's CPU tree code (oracle port) timed on the host's cores: one full call at its setting for the same
+    <= 1e-6 accuracy (order 2, theta 0.04), every target."""
+    seconds, u = cpu_tree_call(case, REF_THETA)
+    base = {"value": 1e3 * seconds, "unit": "ms/call", "cores": host_cores(), "kind": "port",
+            "sample": f"one full call, all {len(case['points'])} targets: median-split build, moments and traversal at "
+                      f"theta {REF_THETA}, order {REF_ORDER}, leaf {REF_LEAF} (the reference's orders stop at 2; "
+                      f"this is its setting for the same <= 1e-6 error)"}
+    if direct_host is not None:
+        base["accuracy_vs_fp64_direct"] = errors(u, direct_host)
+    return base
 
 
 def reference_arm(args):
+    """The reference's CPU tree code (its restatement in oracle/, C with OpenMP on every host core) on the same wake
+    and metric: each step is one full call (build, moments, traversal of every target), timed whole."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     case = workload(args.rows)
-    times = []
-    base = None
+    times, u = [], None
     for step in range(args.warmup + args.steps):
-        base = cpu_baseline(case, args)
+        seconds, u = cpu_tree_call(case, REF_THETA)
         if step >= args.warmup:
-            times.append(base["value"])
+            times.append(1e3 * seconds)
     value = statistics.median(times)
-    base["value"] = value
+    rows = {}
+    for theta, label in ((0.5, "reference default"), (0.2, "production setting")):
+        runs = [cpu_tree_call(case, theta) for _ in range(3)]
+        rows[f"theta_{theta}"] = {"setting": label, "ms_per_call": 1e3 * statistics.median(r[0] for r in runs),
+                                  "accuracy": sample_accuracy(case, runs[-1][1])}
+    base = {"value": value, "unit": "ms/call", "cores": host_cores(), "kind": "port",
+            "sample": f"full calls on all {len(case['points'])} targets, median of {args.steps} after {args.warmup} "
+                      f"warm-up calls; theta {REF_THETA}, order {REF_ORDER}, leaf {REF_LEAF}, median-split tree",
+            "accuracy": sample_accuracy(case, u), "other_settings": rows}
     line = {"metric": METRIC, "value": value, "unit": "ms/call", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config(case, args, {"precision": "fp64 (CPU tree code)", "tree": "median", "theta": REF_THETA,
-                                          "order": REF_ORDER, "leaf_size": REF_LEAF}),
+                                          "order": REF_ORDER, "leaf_size": REF_LEAF,
+                                          "l2": "not applicable (CPU)"}),
             "cpu_baseline": base, "e2e": {"value": value, "unit": "ms/call", "h2d_bytes_per_step": 0,
                                           "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -275,13 +342,185 @@ def sharded_measure(src, case, rank, world, device, args, dist):
             "targets_per_rank": len(case["points"]) // world}
 
 
+def _median_ms(fn, repeat, flush=None):
+    """Median CUDA-event time of `fn` over `repeat` calls after one warm-up call (L2 flushed before each if given)."""
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(repeat):
+        if flush is not None:
+            flush.zero_()
+        times.append(_event_ms(fn))
+    return float(statistics.median(times))
+
+
+def _golden(name):
+    try:
+        return np.load(os.path.join(GOLDEN, name))
+    except OSError:
+        return None
+
+
+def _digest(case):
+    h = hashlib.sha256()
+    for key in ("points", "starts", "directions", "lengths", "gamma", "radius"):
+        h.update(np.ascontiguousarray(case[key], dtype=np.float64).tobytes())
+    return h.hexdigest()
+
+
+def _dropin_ms(case, tree, cuda, repeat=5):
+    """Median wall time of the drop-in cuda_tree_sum from host arrays to host results (the call a caller makes)."""
+    from openfawe_b200 import vortex_cuda_tree, wakes
+    a = (*wakes.backend_args(case), no_exclusions(len(case["points"])), "raise", tree, cuda)
+    vortex_cuda_tree.cuda_tree_sum(*a)
+    times = []
+    for _ in range(repeat):
+        tick = time.perf_counter()
+        vortex_cuda_tree.cuda_tree_sum(*a)
+        times.append(1e3 * (time.perf_counter() - tick))
+    return float(statistics.median(times))
+
+
+def c1_measure(device, flush):
+    """C1: the 16 x 128 lattice (4,207 segments, Rosenhead-Moore 0.05 m) on 1,024 wing points, FP64 direct sum, against
+    the reference's own numba result (tests/golden/direct_lattice.npz) and the oracle's CPU direct sum."""
+    from oracle import oracle as O
+    from openfawe_b200 import engine, vortex_cuda, wakes
+    from openfawe_b200.settings import CudaSettings
+    case = wakes.lattice()
+    args = wakes.backend_args(case)
+    src = engine.Sources(*args[1:6], device)
+    tgt = engine.Targets(case["points"], None, device)
+    u, _ = engine.direct(src, tgt, case["model"], "raise", "fp64")
+    device_ms = _median_ms(lambda: engine.direct(src, tgt, case["model"], "raise", "fp64"), 20, flush)
+    csr = no_exclusions(len(case["points"]))
+    e2e = []
+    for _ in range(12):
+        tick = time.perf_counter()
+        vortex_cuda.cuda_sum(*args, csr, "raise", CudaSettings("fp64"))
+        e2e.append(1e3 * (time.perf_counter() - tick))
+    cpu = []
+    for _ in range(5):
+        tick = time.perf_counter()
+        O.direct_sum(*args, csr, "raise")
+        cpu.append(1e3 * (time.perf_counter() - tick))
+    out = {"workload": f"lattice 16 x 128, {src.m} segments x {tgt.n} targets, Rosenhead-Moore rc 0.05 m, FP64 "
+                       f"direct sum", "device_ms": device_ms, "e2e_ms": float(statistics.median(e2e[2:])),
+           "cpu_port_ms": float(statistics.median(cpu)), "cpu_cores": host_cores()}
+    g = _golden("direct_lattice.npz")
+    if g is not None:
+        out["vs_reference_numba"] = errors(u.cpu().numpy(), g["u"])
+    return out
+
+
+def c2_measure(device, flush):
+    """C2: the README-shape 468-row wakes (102k segments x 20,570 targets), both variants: the reference's self-test
+    sheet and the rotor-ring + wing-sheet mix.  The reference's own tree settings (median tree, order 2, leaf 32, theta
+    0.5 and 0.2) in FP64 and mixed, the fifth-order Morton tree at the bench setting, the FP64 direct sum, and the
+    reference's CPU tree code (oracle port) on the host cores; errors against the reference's numba direct sum and CPU
+    tree (tests/golden/c2_*.npz) where the fixture's inputs match."""
+    from openfawe_b200 import engine, wakes
+    out = {"readme_468_rows_theta_0.2": README_468}
+    for name, make in (("sheet", lambda: wakes.selftest_sheet(468, seed=468)),
+                       ("rotor", lambda: wakes.rotor_sheet(468, seed=468, targets=TARGETS))):
+        case = make()
+        g = _golden(f"c2_{name}.npz")
+        if g is not None and str(g["inputs_sha256"]) != _digest(case):
+            g = None
+        model = case["model"]
+        src = engine.Sources(case["starts"], case["directions"], case["lengths"], case["gamma"], case["radius"], device)
+        tgt = engine.Targets(case["points"], None, device)
+        direct, _ = engine.direct(src, tgt, model, "raise", "fp64")
+        direct = direct.cpu().numpy()
+        ref_direct = g["direct"] if g is not None else direct
+        row = {"segments": src.m, "targets": tgt.n, "core_m": float(case["radius"][0]),
+               "fp64_direct_ms": _median_ms(lambda: engine.direct(src, tgt, model, "raise", "fp64"), 3, flush),
+               "fp64_direct_vs_reference": errors(direct, ref_direct) if g is not None else None,
+               "reference_fixture": g is not None}
+        for theta in (0.5, 0.2):
+            key = f"t{int(round(theta * 100))}"
+            cell = {}
+            for precision in ("fp64", "mixed"):
+                call = lambda: engine.tree_sum(src, tgt, model, "raise", precision, 128, 3.0, theta, 2, 32,  # noqa
+                                               CLEARANCE, "median", far_counts=False)
+                u = call()[0].cpu().numpy()
+                cell[precision] = {"ms": _median_ms(call, 5, flush), "vs_fp64_direct": errors(u, ref_direct),
+                                   "e2e_ms": _dropin_ms(case, CallerTreeSettings(theta, 2, 32, CLEARANCE),
+                                                        CallerCudaSettings(precision, 128))}
+                if g is not None:
+                    cpu = g[key]
+                    e, te = np.linalg.norm(u - cpu, axis=1), np.linalg.norm(cpu - ref_direct, axis=1)
+                    cell[precision]["vs_reference_cpu_tree"] = {
+                        "max_over_max_speed": float(e.max() / np.linalg.norm(cpu, axis=1).max()),
+                        "max_over_tree_error_max": float(e.max() / te.max()),
+                        "rms_over_tree_error_rms": float(np.sqrt(np.mean(e ** 2)) / np.sqrt(np.mean(te ** 2)))}
+            runs = [cpu_tree_call(case, theta) for _ in range(3)]
+            cell["cpu_port"] = {"ms": 1e3 * statistics.median(r[0] for r in runs), "cores": host_cores(),
+                                "vs_fp64_direct": errors(runs[-1][1], ref_direct)}
+            if g is not None:
+                cell["reference_numba_tree"] = {"ms_in_fixture_run": 1e3 * float(g[key + "_s"]),
+                                                "threads": int(g["threads"]),
+                                                "vs_fp64_direct": errors(g[key], ref_direct)}
+            row[f"median_order2_theta_{theta}"] = cell
+        call = lambda: engine.tree_sum(src, tgt, model, "raise", "mixed", 128, 3.0, THETA, ORDER, LEAF,  # noqa: E731
+                                       CLEARANCE, "morton", far_counts=False)
+        u = call()[0].cpu().numpy()
+        row[f"morton_order{ORDER}_theta_{THETA}_leaf_{LEAF}_mixed"] = {"ms": _median_ms(call, 5, flush),
+                                                                         "vs_fp64_direct": errors(u, ref_direct)}
+        out[name] = row
+    return out
+
+
+def default_path_measure(src, tgt, model, direct_host, flush):
+    """The bench wake through the path an unchanged caller of the reference reaches: the median tree at order 2 (leaf
+    32, mixed), at the equal-accuracy theta 0.04 and the production theta 0.2."""
+    from openfawe_b200 import engine
+    out = {}
+    for theta in (REF_THETA, 0.2):
+        call = lambda: engine.tree_sum(src, tgt, model, "raise", "mixed", 128, 3.0, theta, 2, 32, CLEARANCE,  # noqa
+                                       "median", far_counts=False)
+        u = call()[0].cpu().numpy()
+        out[f"theta_{theta}"] = {"ms": _median_ms(call, 3, flush), "vs_fp64_direct": errors(u, direct_host),
+                                 "near_pairs": engine.last_stats(src.device.index)["near_pairs"]}
+    return out
+
+
+def only_run(args, case, src, tgt, device):
+    """--only: one call kind, warmup + steps times, for profiler runs; prints its counters."""
+    import torch
+    from openfawe_b200 import adjoint, engine
+    model = case["model"]
+    if args.only == "tree":
+        fn = lambda: engine.tree_sum(src, tgt, model, "raise", "mixed", 128, 3.0, args.theta, args.order,  # noqa
+                                     args.leaf, CLEARANCE, args.kind, far_counts=False)
+    elif args.only in ("direct-fp64", "direct-mixed"):
+        precision = "fp64" if args.only == "direct-fp64" else "mixed"
+        fn = lambda: engine.direct(src, tgt, model, "raise", precision)  # noqa: E731
+    else:
+        ends = case["nodes"][case["edges"][:, 1]]
+        pts, a = torch.as_tensor(case["points"], device=device), torch.as_tensor(case["starts"], device=device)
+        bb, gam = torch.as_tensor(ends, device=device), torch.as_tensor(case["gamma"], device=device)
+        rad = torch.as_tensor(case["radius"], device=device)
+        w = torch.as_tensor(np.random.default_rng(5).standard_normal((len(case["points"]), 3)), device=device)
+        if args.only == "adjoint":
+            fn = lambda: adjoint.adjoint_direct(pts, a, bb, gam, rad, model, w)  # noqa: E731
+        else:
+            fn = lambda: adjoint.adjoint_tree(pts, a, bb, gam, rad, model, w, precision="mixed",  # noqa: E731
+                                              theta=args.theta, order=args.order, leaf_size=args.leaf,
+                                              kind=args.kind)
+    for _ in range(args.warmup + args.steps):
+        fn()
+    torch.cuda.synchronize()
+    print(json.dumps({"only": args.only, "stats": engine.last_stats(device), "config": config(case, args)}))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
     import torch
     from openfawe_b200 import engine, vortex_cuda_tree
-    from openfawe_b200.settings import CudaSettings, TreeSettings
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -296,21 +535,33 @@ def main():
 
     case = workload(args.rows)
     model = case["model"]
-    src = engine.Sources(case["starts"], case["directions"], case["lengths"], case["gamma"], case["radius"], device)
+    segments = tuple(case[k] for k in ("starts", "directions", "lengths", "gamma", "radius"))
+    src = engine.Sources(*segments, device)
     tgt = engine.Targets(case["points"], None, device)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    # On N GPUs one call is shared by sources (openfawe_b200.shard): this rank holds its Morton range of the segments,
+    # builds its own tree over them, evaluates every target, and the partial velocities are summed over the ranks.
+    src_step = src
+    if world > 1:
+        from openfawe_b200 import shard
+        mine = shard.source_shards(case["starts"], case["directions"], case["lengths"], world)[rank]
+        src_step = engine.Sources(*(a[mine] for a in segments), device)
 
     def step():
-        return engine.tree_sum(src, tgt, model, "raise", "mixed", 128, 3.0, args.theta, args.order, args.leaf, CLEARANCE,
-                               args.kind, far_counts=False)
+        u, flags, far = engine.tree_sum(src_step, tgt, model, "raise", "mixed", 128, 3.0, args.theta, args.order,
+                                        args.leaf, CLEARANCE, args.kind, far_counts=False)
+        if world > 1:
+            f = flags.to(torch.int32)
+            dist.all_reduce(u, op=dist.ReduceOp.SUM)
+            dist.all_reduce(f, op=dist.ReduceOp.MAX)
+            flags = f.to(torch.int8)
+        return u, flags, far
 
-    if args.tree_only:
-        for _ in range(args.warmup + args.steps):
-            step()
-        torch.cuda.synchronize()
+    if args.only:
         if rank == 0:
-            print(json.dumps({"tree_only": True, "stats": engine.last_stats(device), "config": config(case, args)}))
+            only_run(args, case, src, tgt, device)
         if dist:
+            dist.barrier()
             dist.destroy_process_group()
         return 0
 
@@ -381,39 +632,72 @@ def main():
                 "peak_note": "FP32 FMA throughput measured in this run (bs_fp32_peak); the pair and far-field "
                              "arithmetic runs on the FP32 pipe, neither HBM- nor tensor-core-bound"}
 
-    # end to end through the drop-in: host NumPy in, host NumPy out
-    tree = TreeSettings(args.theta, min(args.order, 2), args.leaf, CLEARANCE)
-    cuda = CudaSettings("mixed", 128, "gpu64", tree=args.kind)
-    csr = (np.zeros(len(case["points"]) + 1, dtype=np.int64), np.zeros(0, dtype=np.int64))
-    a = (case["points"], case["starts"], case["directions"], case["lengths"], case["gamma"], case["radius"], model,
-         csr, "raise", tree, cuda)
-    for _ in range(2):  # warm-up: staging ring, pools, host pages
-        vortex_cuda_tree.cuda_tree_sum(*a, order=args.order)
-    e2e, e2e_stages = [], []
-    for _ in range(max(5, min(args.steps, 10))):
-        torch.cuda.synchronize()
-        tick = time.perf_counter()
-        vortex_cuda_tree.cuda_tree_sum(*a, order=args.order)
-        e2e.append(1e3 * (time.perf_counter() - tick))
-        last = vortex_cuda_tree.Statistics.last
-        e2e_stages.append({k: 1e3 * last[k] for k in ("upload_s", "build_s", "evaluate_s", "download_s")})
-    h2d = sum(np.asarray(x).nbytes for x in (case["points"], case["starts"], case["directions"], case["lengths"],
-                                              case["gamma"], case["radius"]))
+    # End to end, as an unchanged caller of the reference makes the call: host NumPy in, host NumPy out, the
+    # reference's own settings objects (here their field-for-field mirrors) at its equal-accuracy setting (order 2,
+    # theta 0.04), mapped by install-time options to the benchmarked fifth-order Morton tree.
+    e2e, e2e_stages, e2e_effective = [], [], None
+    h2d = sum(np.asarray(x).nbytes for x in (case["points"], *segments))
     d2h = len(case["points"]) * (24 + 1 + 8)
+    if world == 1:
+        import openfawe_b200
+        openfawe_b200.install(tree=args.kind, order=args.order, theta={REF_THETA: args.theta}, leaf_size=args.leaf)
+        tree = CallerTreeSettings(REF_THETA, REF_ORDER, REF_LEAF, CLEARANCE)
+        cuda = CallerCudaSettings("mixed", 128, "gpu64")
+        a = (case["points"], *segments, model, no_exclusions(len(case["points"])), "raise", tree, cuda)
+        for _ in range(2):  # warm-up: staging ring, pools, host pages
+            vortex_cuda_tree.cuda_tree_sum(*a)
+        for _ in range(max(5, min(args.steps, 10))):
+            torch.cuda.synchronize()
+            tick = time.perf_counter()
+            vortex_cuda_tree.cuda_tree_sum(*a)
+            e2e.append(1e3 * (time.perf_counter() - tick))
+            last = vortex_cuda_tree.Statistics.last
+            e2e_stages.append({k: 1e3 * last[k] for k in ("upload_s", "build_s", "evaluate_s", "download_s")})
+        e2e_effective = dict(vortex_cuda_tree.Statistics.last["effective"])
+        openfawe_b200.uninstall()
+        e2e_call = ("cuda_tree_sum from host arrays with the reference's TreeSettings(theta=0.04, order=2, "
+                    "leaf_size=32) and CudaSettings('mixed', 128, 'gpu64'); install-time options map them to the "
+                    "effective tree below")
+    else:
+        # every rank uploads its share of the segments and all targets, evaluates, and reads the summed result back
+        from openfawe_b200 import shard
+        evaluate = shard.tree_evaluator(model, device, "mixed", args.theta, args.order, args.leaf, kind=args.kind)
+        for k in range(2 + max(5, min(args.steps, 10))):
+            torch.cuda.synchronize()
+            dist.barrier()
+            tick = time.perf_counter()
+            shard.sharded_sum(evaluate, case["points"], segments, rank, world, "sources")[0].cpu()
+            elapsed = torch.tensor([1e3 * (time.perf_counter() - tick)], dtype=torch.float64, device=device)
+            dist.all_reduce(elapsed, op=dist.ReduceOp.MAX)
+            if k >= 2:
+                e2e.append(float(elapsed.item()))
+        e2e_effective = dict(tree=args.kind, order=args.order, theta=args.theta, leaf_size=args.leaf)
+        e2e_call = (f"openfawe_b200.shard.sharded_sum over {world} ranks from host arrays (each rank uploads its "
+                    f"Morton range of the segments and every target), result read back on every rank; wall time, "
+                    f"max over ranks")
+        h2d = h2d + (world - 1) * case["points"].nbytes
+        d2h = world * len(case["points"]) * (24 + 1)
 
-    # launches of this library's kernels inside one step (CUPTI through the torch profiler)
-    gpu_launches = None
+    # launches of this library's kernels inside one step (CUPTI through the torch profiler); the step itself runs on
+    # every rank whatever the profiler does, so the ranks' collectives stay matched
+    gpu_launches, prof = None, None
     try:
         from torch.profiler import ProfilerActivity, profile
-        with profile(activities=[ProfilerActivity.CUDA]) as prof:
-            step()
-            torch.cuda.synchronize()
-        gpu_launches = sum(1 for e in prof.events() if e.device_type.name == "CUDA" and "bs::" in e.name)
+        prof = profile(activities=[ProfilerActivity.CUDA])
+        prof.__enter__()
     except Exception:  # noqa: BLE001 - profiler unavailable: leave the count out rather than guess
-        gpu_launches = None
+        prof = None
+    step()
+    torch.cuda.synchronize()
+    if prof is not None:
+        try:
+            prof.__exit__(None, None, None)
+            gpu_launches = sum(1 for e in prof.events() if e.device_type.name == "CUDA" and "bs::" in e.name)
+        except Exception:  # noqa: BLE001
+            gpu_launches = None
 
-    line = {"metric": METRIC, "value": ms / world, "unit": "ms/call", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+    line = {"metric": METRIC, "value": ms, "unit": "ms/call", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "strong",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
             "config": config(case, args),
             "accuracy": {"rel_l2_vs_fp64_direct": rel_l2, "max_err_over_max_speed": max_err},
@@ -428,16 +712,21 @@ def main():
             "roofline": roofline,
             "e2e": {"value": float(np.median(e2e)), "unit": "ms/call", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "calls_ms": e2e,
-                    "stages_ms_of_median_call": e2e_stages[int(np.argsort(e2e)[len(e2e) // 2])]},
+                    "stages_ms_of_median_call": (e2e_stages[int(np.argsort(e2e)[len(e2e) // 2])]
+                                                 if e2e_stages else None),
+                    "call": e2e_call, "effective": e2e_effective},
             "gpu_launches": gpu_launches, "clocks": clocks}
     if rank == 0 and world == 1:
-        line["cpu_baseline"] = cpu_baseline(case, args)
+        line["cpu_baseline"] = cpu_baseline(case, direct_host)
         if not args.no_extras:
+            line["default_path"] = default_path_measure(src, tgt, model, direct_host, flush)
+            line["c1"] = c1_measure(device, flush)
+            line["c2"] = c2_measure(device, flush)
             line["batch"] = batch_measure(device, args.theta, args.order)
             line["adjoint"] = adjoint_measure(device, args.theta)
             line["adjoint_fwd_ratio"] = line["adjoint"]["ratio_to_fp64_direct"]
     if dist:
-        line["sharded"] = sharded_measure(src, case, rank, world, device, args, dist)
+        line["target_sharded"] = sharded_measure(src, case, rank, world, device, args, dist)
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
