@@ -285,37 +285,72 @@ def batch_measure(device, theta, order=ORDER):
             "batched_per_wake_ms": total / len(cases), "speedup_vs_sequential": float(seq.sum()) / total}
 
 
-def adjoint_measure(device, theta):
-    """The hand-written adjoint (grads w.r.t. targets, both endpoints and circulations) on a 468-row rotor sheet
-    against the forward it differentiates (FP64 direct) and the mixed tree forward."""
+def adjoint_measure(device, theta, bench_case=None):
+    """The hand-written adjoints (grads w.r.t. targets, both endpoints and circulations) against the forwards they
+    differentiate: on the 468-row rotor sheet (C5) the exact FP64 adjoint against the FP64 direct sum, and the tree
+    adjoint against the mixed fifth-order tree forward (with its error against the exact gradient); on the bench wake
+    the tree adjoint against the bench's tree forward."""
     import torch
     from openfawe_b200 import adjoint, engine, wakes
+
+    def setup(case):
+        ends = case["nodes"][case["edges"][:, 1]]
+        pts = torch.as_tensor(case["points"], device=device)
+        a = torch.as_tensor(case["starts"], device=device)
+        bb = torch.as_tensor(ends, device=device)
+        gam = torch.as_tensor(case["gamma"], device=device)
+        rad = torch.as_tensor(case["radius"], device=device)
+        rng = np.random.default_rng(5)
+        w = torch.as_tensor(rng.standard_normal((len(case["points"]), 3)).astype(np.float32).astype(np.float64),
+                            device=device)
+        src = engine.Sources(case["starts"], case["directions"], case["lengths"], case["gamma"], case["radius"],
+                             device)
+        tgt = engine.Targets(case["points"], None, device)
+        return pts, a, bb, gam, rad, w, src, tgt
+
     case = wakes.rotor_sheet(468, seed=468, targets=20570)
-    ends = case["nodes"][case["edges"][:, 1]]
-    pts = torch.as_tensor(case["points"], device=device)
-    a = torch.as_tensor(case["starts"], device=device)
-    bb = torch.as_tensor(ends, device=device)
-    gam = torch.as_tensor(case["gamma"], device=device)
-    rad = torch.as_tensor(case["radius"], device=device)
-    rng = np.random.default_rng(5)
-    w = torch.as_tensor(rng.standard_normal((len(case["points"]), 3)).astype(np.float32).astype(np.float64),
-                        device=device)
-    src = engine.Sources(case["starts"], case["directions"], case["lengths"], case["gamma"], case["radius"], device)
-    tgt = engine.Targets(case["points"], None, device)
+    pts, a, bb, gam, rad, w, src, tgt = setup(case)
     model = case["model"]
     run_adj = lambda: adjoint.adjoint_direct(pts, a, bb, gam, rad, model, w)  # noqa: E731
     run_direct = lambda: engine.direct(src, tgt, model, "raise", "fp64")  # noqa: E731
     run_tree = lambda: engine.tree_sum(src, tgt, model, "raise", "mixed", 128, 3.0, theta, ORDER, LEAF,  # noqa: E731
                                        CLEARANCE, "morton", far_counts=False)
-    for fn in (run_adj, run_direct, run_tree):
+    run_tree_adj = lambda: adjoint.adjoint_tree(pts, a, bb, gam, rad, model, w, precision="mixed",  # noqa: E731
+                                                theta=theta, order=ORDER, leaf_size=LEAF, kind="morton")
+    for fn in (run_adj, run_direct, run_tree, run_tree_adj):
         fn()
     torch.cuda.synchronize()
     adj = min(_event_ms(run_adj) for _ in range(3))
     fwd = min(_event_ms(run_direct) for _ in range(3))
-    tree = min(_event_ms(run_tree) for _ in range(3))
-    return {"workload": f"rotor-sheet wake 468 rows, {src.m} segments x {tgt.n} targets, cotangent N(0,1) seed 5",
-            "adjoint_ms": adj, "fp64_direct_forward_ms": fwd, "mixed_tree_forward_ms": tree,
-            "ratio_to_fp64_direct": adj / fwd, "ratio_to_tree_forward": adj / tree}
+    tree = min(_event_ms(run_tree) for _ in range(5))
+    tree_adj = min(_event_ms(run_tree_adj) for _ in range(5))
+    stats = engine.last_stats(device)
+    exact = [t.cpu().numpy() for t in run_adj()]
+    approx = [t.cpu().numpy() for t in run_tree_adj()]
+    err = {name: float(np.linalg.norm(u - v) / np.linalg.norm(v))
+           for name, u, v in zip(("points", "starts", "ends", "gamma"), approx, exact)}
+    out = {"workload": f"rotor-sheet wake 468 rows, {src.m} segments x {tgt.n} targets, cotangent N(0,1) seed 5",
+           "adjoint_ms": adj, "fp64_direct_forward_ms": fwd, "mixed_tree_forward_ms": tree,
+           "ratio_to_fp64_direct": adj / fwd, "ratio_to_tree_forward": adj / tree,
+           "tree_adjoint": {"ms": tree_adj, "ratio_to_tree_forward": tree_adj / tree,
+                            "stages_ms": {"build_walk_transpose": stats["walk_ms"], "near_pairs": stats["list_ms"],
+                                          "far_pushdown_segments": stats["moments_ms"]},
+                            "rel_l2_vs_exact_adjoint": err,
+                            "setting": f"Morton tree, order {ORDER}, theta {theta}, leaf {LEAF}, mixed near pairs"}}
+    if bench_case is not None:
+        pts, a, bb, gam, rad, w, src, tgt = setup(bench_case)
+        run_tree = lambda: engine.tree_sum(src, tgt, model, "raise", "mixed", 128, 3.0, theta, ORDER,  # noqa: E731
+                                           LEAF, CLEARANCE, "morton", far_counts=False)
+        run_tree_adj = lambda: adjoint.adjoint_tree(pts, a, bb, gam, rad, model, w, precision="mixed",  # noqa: E731
+                                                    theta=theta, order=ORDER, leaf_size=LEAF, kind="morton")
+        run_tree()
+        run_tree_adj()
+        torch.cuda.synchronize()
+        tree = min(_event_ms(run_tree) for _ in range(5))
+        tree_adj = min(_event_ms(run_tree_adj) for _ in range(5))
+        out["bench_wake"] = {"workload": f"{src.m} segments x {tgt.n} targets", "tree_forward_ms": tree,
+                             "tree_adjoint_ms": tree_adj, "ratio_to_tree_forward": tree_adj / tree}
+    return out
 
 
 def sharded_measure(src, case, rank, world, device, args, dist):
@@ -723,8 +758,8 @@ def main():
             line["c1"] = c1_measure(device, flush)
             line["c2"] = c2_measure(device, flush)
             line["batch"] = batch_measure(device, args.theta, args.order)
-            line["adjoint"] = adjoint_measure(device, args.theta)
-            line["adjoint_fwd_ratio"] = line["adjoint"]["ratio_to_fp64_direct"]
+            line["adjoint"] = adjoint_measure(device, args.theta, case)
+            line["adjoint_fwd_ratio"] = line["adjoint"]["tree_adjoint"]["ratio_to_tree_forward"]
     if dist:
         line["target_sharded"] = sharded_measure(src, case, rank, world, device, args, dist)
         dist.barrier()

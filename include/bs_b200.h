@@ -211,6 +211,19 @@ int bs_adjoint_direct(bs_ctx *ctx, int64_t n, const double *points, int64_t m, c
                       int64_t e, int model, const double *cotangent, double *grad_points, double *grad_A,
                       double *grad_B, double *grad_gamma, bs_stream stream);
 
+/* Adjoint of the tree sum (no counterpart in the reference, which has no adjoint): for the cotangent w [n,3] of the
+ * velocities bs_tree_sum returns with the same arguments, d(sum_p w_p . u_p) with respect to the targets [n,3], the
+ * segment starts A and ends B = A + L d [m,3] and the circulations [m] (any output may be NULL), as the derivative of
+ * the forward the tree code evaluates: the same tree (built again), the same accepted nodes and near pairs (the walk
+ * runs again), pair terms and expansions recomputed; node centres and acceptance decisions are held fixed.  Near pairs
+ * in FP32 (kp->precision BS_MIXED or BS_FP32) with FP64 where the forward takes FP64, or all in FP64 (BS_FP64); the
+ * far field's derivatives in FP64.  Core models NONE, RANKINE and LAMB_OSEEN; orders 0..5.  Gradients are summed with
+ * atomics (repeatable to rounding).  BS_ERR_OOM if a warp's interaction list exceeds the list pool.  Blocks until
+ * the gradients are written. */
+int bs_tree_adjoint(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, const bs_targets *tgt,
+                    const bs_kernel_params *kp, const double *cotangent, double *grad_points, double *grad_starts,
+                    double *grad_ends, double *grad_gamma, bs_stream stream);
+
 /* The reference's median-split tree from midpoints alone (replaces vortex_cuda_build.device_build_tree,
  * src/openfawe/aero/vortex_cuda_build.py:234-275, and vortex_tree.build_tree, vortex_tree.py:208-241): order [m] and,
  * when *count <= capacity, lo/hi/left/right [count] in depth-first numbering, element for element equal to

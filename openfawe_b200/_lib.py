@@ -87,6 +87,8 @@ SIGNATURES = {
                                          ctypes.POINTER(ctypes.c_int64), _p]),
     "bs_exclusion_csr": (ctypes.c_int, [_p, ctypes.c_int64, _p, ctypes.c_int64, _p, _p, ctypes.POINTER(ctypes.c_int64),
                                         _p]),
+    "bs_tree_adjoint": (ctypes.c_int, [_p, ctypes.POINTER(Sources), ctypes.POINTER(TreeParams),
+                                       ctypes.POINTER(Targets), ctypes.POINTER(KernelParams)] + [_p] * 6),
     "bs_median_topology": (ctypes.c_int, [_p, ctypes.c_int64, _p, ctypes.c_int, _p, _p, _p, _p, _p, ctypes.c_int64,
                                           ctypes.POINTER(ctypes.c_int64), _p]),
     "bs_node_quantities": (ctypes.c_int, [_p, ctypes.c_int64, _p, _p, _p, _p, _p, ctypes.c_int64, _p, _p, _p]

@@ -10,13 +10,13 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBRARY = os.path.join(HERE, "libbs_b200.so")
-SOURCES = ["bs_context.cu", "bs_sort.cu", "bs_tree_build.cu", "bs_tree_eval.cu", "bs_direct.cu", "bs_adjoint.cu", "bs_network.cu", "bs_operators.cu",
-           "bs_upload.cu"]
+SOURCES = ["bs_context.cu", "bs_sort.cu", "bs_tree_build.cu", "bs_tree_eval.cu", "bs_direct.cu", "bs_adjoint.cu",
+           "bs_tree_adjoint.cu", "bs_network.cu", "bs_operators.cu", "bs_upload.cu"]
 OPENMP = {"bs_upload.cu"}  # host-threaded sources
 # Sources whose FP32 pair and far-field arithmetic flushes single-precision subnormals to zero: the special-function
 # results then need no subnormal handling (7% fewer instructions in the interaction-list kernel); FP64 is unaffected,
 # and an FP32 value below 1.2e-38 m/s is no part of a velocity here (out-of-range pairs are evaluated in FP64).
-FTZ = {"bs_tree_eval.cu", "bs_direct.cu"}
+FTZ = {"bs_tree_eval.cu", "bs_direct.cu", "bs_tree_adjoint.cu"}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 

@@ -14,90 +14,9 @@
 // partials in chunk order.  Deterministic.
 #include <algorithm>
 
-#include "bs_internal.cuh"
+#include "bs_pair_vjp.cuh"
 
 namespace bs {
-
-// A segment as the adjoint reads it: endpoints, circulation and the per-segment invariants of the pair.
-struct AdjSeg {
-    double ax, ay, az, bx, by, bz, gamma;
-    double irc2L2;  // 1 / (L^2 rc^2) for a cored model with rc > 0, else 0 (no core factor)
-    double invL2;   // 1 / L^2
-    double pad;
-};
-struct AdjTgt {
-    double x, y, z, wx, wy, wz;
-};
-
-static constexpr double AXIS_EPS64_SQ = AXIS_EPS64 * AXIS_EPS64;
-
-// d(w . u)/dr1 and d(w . u)/dr2 of one pair (r1 = x - A, r2 = x - B) and d(w . u)/dGamma; false for a pair that
-// contributes nothing (the roundoff axis guard).  Then d/dx = g1 + g2, d/dA = -g1, d/dB = -g2.
-__device__ __forceinline__ bool pair_vjp64(double x0, double x1, double x2, const AdjSeg &s, int model, double w0,
-                                           double w1, double w2, double *g1, double *g2, double &gg) {
-    const double r10 = x0 - s.ax, r11 = x1 - s.ay, r12 = x2 - s.az;
-    const double r20 = x0 - s.bx, r21 = x1 - s.by, r22 = x2 - s.bz;
-    const double c0 = r11 * r22 - r12 * r21, c1 = r12 * r20 - r10 * r22, c2v = r10 * r21 - r11 * r20;
-    const double cc = c0 * c0 + c1 * c1 + c2v * c2v;
-    const double q1 = r10 * r10 + r11 * r11 + r12 * r12, q2 = r20 * r20 + r21 * r21 + r22 * r22;
-    // the reference's roundoff axis guard h <= eps max(1, na, nb) in its scaled units (h = |c|/L^2,
-    // na = |r1|/L, nb = |r2|/L), squared
-    if (cc * s.invL2 * s.invL2 <= AXIS_EPS64_SQ * fmax(1.0, fmax(q1, q2) * s.invL2)) return false;
-    const double in1 = rsqrt(q1), in2 = rsqrt(q2);
-    const double n1 = q1 * in1, n2 = q2 * in2;
-    const double d = r10 * r20 + r11 * r21 + r12 * r22;
-    const double P = n1 * n2;
-    double D, dD_dP, dD_dd, dD_dcc;
-    if (d >= 0.0) {
-        D = P * (P + d);
-        dD_dP = 2.0 * P + d;
-        dD_dd = P;
-        dD_dcc = 0.0;
-    } else {  // the rationalised denominator P (P + d) = P |c|^2 / (P - d)
-        const double iq = 1.0 / (P - d);
-        D = P * cc * iq;
-        dD_dP = -cc * d * iq * iq;
-        dD_dd = P * cc * iq * iq;
-        dD_dcc = P * iq;
-    }
-    double f = 1.0, df = 0.0, rho2 = 0.0;  // core factor f(rho2), df/drho2 with rho2 = |c|^2 / (L^2 rc^2)
-    if (s.irc2L2 > 0.0) {
-        rho2 = cc * s.irc2L2;
-        if (model == 1) {
-            if (rho2 < 1.0) { f = rho2; df = 1.0; }
-        } else if (rho2 <= LAMB_CUT2) {
-            const double em1 = expm1(-LAMB_A * rho2);
-            f = -em1;
-            df = LAMB_A * (1.0 + em1);
-        }
-    }
-    const double S = n1 + n2;
-    const double iD = 1.0 / D;
-    const double coefG = INV_FOUR_PI * f * S * iD;  // u = Gamma * coefG * c
-    const double wc = w0 * c0 + w1 * c1 + w2 * c2v;
-    gg = coefG * wc;
-    const double G = s.gamma;
-    const double h = G * wc * INV_FOUR_PI * iD;  // common factor of the scalar adjoints
-    const double g_f = h * S;
-    const double g_S = h * f;
-    const double g_D = -h * f * S * iD;
-    const double g_rho2 = g_f * df;
-    const double g_cc = g_rho2 * s.irc2L2 + g_D * dD_dcc;
-    const double g_L2 = -g_rho2 * rho2 * s.invL2;
-    const double g_P = g_D * dD_dP, g_d = g_D * dD_dd;
-    const double k = G * coefG;
-    const double gc0 = k * w0 + 2.0 * c0 * g_cc, gc1 = k * w1 + 2.0 * c1 * g_cc, gc2 = k * w2 + 2.0 * c2v * g_cc;
-    // c = r1 x r2: dL/dr1 += r2 x g_c, dL/dr2 += g_c x r1; |B - A|^2 = |r1 - r2|^2: dL2/dr1 = 2 l = -dL2/dr2
-    const double a1 = (g_S + g_P * n2) * in1, a2 = (g_S + g_P * n1) * in2, b = 2.0 * g_L2;
-    const double l0 = s.bx - s.ax, l1 = s.by - s.ay, l2 = s.bz - s.az;
-    g1[0] = a1 * r10 + g_d * r20 + (r21 * gc2 - r22 * gc1) + b * l0;
-    g1[1] = a1 * r11 + g_d * r21 + (r22 * gc0 - r20 * gc2) + b * l1;
-    g1[2] = a1 * r12 + g_d * r22 + (r20 * gc1 - r21 * gc0) + b * l2;
-    g2[0] = a2 * r20 + g_d * r10 + (gc1 * r12 - gc2 * r11) - b * l0;
-    g2[1] = a2 * r21 + g_d * r11 + (gc2 * r10 - gc0 * r12) - b * l1;
-    g2[2] = a2 * r22 + g_d * r12 + (gc0 * r11 - gc1 * r10) - b * l2;
-    return true;
-}
 
 __device__ __forceinline__ bool excluded(const int64_t *ex_ptr, const int64_t *ex_seg, int64_t p, int64_t s) {
     if (!ex_ptr) return false;

@@ -73,3 +73,33 @@ int tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_
                bool wait, const std::function<int()> &before_geometry, cudaStream_t side = nullptr);
 void tree_stage_times(bs_tree *t);
 void tree_release(bs_tree *tree, cudaStream_t s);
+
+namespace bs {
+
+// Interaction lists of the traversal (the walk of bs_tree_eval), shared with the adjoint.  Warp gw of the sorted
+// targets owns list_len[gw] entries, entry k at list[unit_chunks[gw * LIST_CHUNKS + k / LIST_CHUNK] * LIST_CHUNK +
+// k % LIST_CHUNK]: (node, lane mask) for a near leaf, (node | FAR_BIT, lane mask) for an accepted far node; lane l of
+// warp gw is sorted target gw * 32 + l, target perm[gw * 32 + l].
+constexpr int LIST_CHUNK = 128;  // list entries per chunk of the shared list pool
+constexpr int LIST_CHUNKS = 32;  // chunks a warp's list may hold (4096 entries)
+constexpr int LIST_POOL = 4096;  // pool entries per warp of targets
+constexpr int FAR_BIT = int(0x80000000u);
+
+struct TreeLists {
+    int64_t n = 0, target_warps = 0;
+    const int32_t *perm = nullptr;    // sorted target -> target
+    const int32_t *ex_pos = nullptr;  // excluded tree positions per target (ranges ex_ptr[p] .. ex_ptr[p + 1]), or null
+    const int64_t *ex_ptr = nullptr;
+    const int2 *list = nullptr;
+    const int *unit_chunks = nullptr;
+    const int *list_len = nullptr;
+    unsigned long long *state = nullptr;  // device: overflow word (low: stack, high: list full), 5 counters
+};
+
+// The walk alone, on s, every interaction going into the lists (none is evaluated): sorts the targets, maps their
+// exclusions to tree positions and fills `lists`.  A warp whose list does not fit sets the overflow word's high half;
+// a stack overflow sets its low half (the caller reads `state` back).  MODEL 0..2.
+int tree_lists(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const bs_targets *tgt,
+               const bs_kernel_params *kp, Scratch &scratch, cudaStream_t s, TreeLists *lists);
+
+}  // namespace bs

@@ -21,10 +21,6 @@
 namespace bs {
 
 constexpr int STACK_DEPTH = 128;
-constexpr int LIST_CHUNK = 128;           // list entries per chunk of the shared list pool
-constexpr int LIST_CHUNKS = 32;           // chunks a unit's list may hold (4096 entries)
-constexpr int LIST_POOL = 4096;           // pool entries per warp of targets
-constexpr int FAR_BIT = int(0x80000000u);
 constexpr int FAR_COST = 16;              // list cost units: one far evaluation ~ sixteen near pairs (measured)
 constexpr int LIST_WARPS = 4;             // warps per block of the list kernel
 
@@ -987,6 +983,98 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     BS_CHECK_LAUNCH("tree evaluation");
     return BS_OK;
 }
+
+}  // namespace
+
+namespace bs {
+
+int tree_lists(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const bs_targets *tgt,
+               const bs_kernel_params *kp, Scratch &scratch, cudaStream_t s, TreeLists *lists) {
+    const int64_t n = tgt->n;
+    int32_t *perm = scratch.get<int32_t>(n);
+    unsigned long long *queue = scratch.get<unsigned long long>(2);
+    unsigned long long *state = scratch.get<unsigned long long>(6);
+    if (!perm || !queue || !state) return scratch.status;
+    int rc = target_order(n, tgt->points, perm, scratch, s);
+    if (rc != BS_OK) return rc;
+    int32_t *ex_pos = nullptr;
+    if (tgt->ex_ptr && tgt->e > 0) {
+        ex_pos = scratch.get<int32_t>(tgt->e);
+        if (!ex_pos) return scratch.status;
+        exclusion_positions_kernel<<<nblocks(n, 128), 128, 0, s>>>(n, tgt->ex_ptr, tgt->ex_seg, tree->inverse,
+                                                                    ex_pos);
+        BS_CHECK_LAUNCH("exclusion_positions_kernel");
+    }
+    BS_CUDA(cudaMemsetAsync(state, 0, 6 * sizeof(unsigned long long), s));
+    BS_CUDA(cudaMemsetAsync(queue, 0, 2 * sizeof(unsigned long long), s));
+    const int block = std::min(kp->block, 128);
+    const int64_t target_warps = (n + 31) / 32;
+    const size_t slots = (size_t)target_warps, pool = (size_t)target_warps * LIST_POOL;
+    int2 *list = scratch.get<int2>(pool);
+    int *list_cost = scratch.get<int>(pool);
+    int *unit_chunks = scratch.get<int>(slots * LIST_CHUNKS);
+    int *list_len = scratch.get<int>(slots), *list_total = scratch.get<int>(slots);
+    double *walk_u = scratch.get<double>((size_t)3 * n);
+    int8_t *walk_flag = scratch.get<int8_t>((size_t)n);
+    if (!list || !list_cost || !unit_chunks || !list_len || !list_total || !walk_u || !walk_flag)
+        return scratch.status;
+    EvalArgs args{};
+    args.n = n;
+    args.points = tgt->points;
+    args.perm = perm;
+    args.ex_ptr = ex_pos ? tgt->ex_ptr : nullptr;
+    args.ex_pos = ex_pos;
+    args.tv = TreeView{tree->nodes,  tree->far64,  tree->far32, tree->far64x, tree->far32x,
+                       tree->far64y, tree->far32y, tree->far64z, tree->far32z, tree->seg64, tree->seg32,
+                       tree->seg32x2};
+    args.theta = tp->theta;
+    args.theta2 = tp->theta * tp->theta;
+    args.clearance = tp->clearance;
+    args.order = tp->order;
+    args.model = kp->model;
+    args.raise_singular = kp->raise_singular ? 1 : 0;
+    args.deferred = 1;  // nothing is evaluated in the walk: what does not fit in the lists is reported
+    args.near2 = (float)(kp->near_cores * kp->near_cores);
+    args.stack_limit = (tp->stack_limit > 0 && tp->stack_limit < STACK_DEPTH) ? tp->stack_limit : STACK_DEPTH;
+    args.list = list;
+    args.list_cost = list_cost;
+    args.list_len = list_len;
+    args.list_total = list_total;
+    args.walk_u = walk_u;
+    args.walk_flag = walk_flag;
+    args.overflow = reinterpret_cast<int *>(state);
+    args.counters = state + 1;
+    args.chunks = 1;
+    args.unit_chunks = unit_chunks;
+    args.pool_cursor = queue + 1;
+    args.pool_chunks = pool / LIST_CHUNK;
+    args.queue = queue;
+    const size_t smem = (size_t)(block / 32) * (STACK_DEPTH * sizeof(int2) + 32 * sizeof(Seg64));
+    const unsigned walk_grid = (unsigned)((target_warps + block / 32 - 1) / (block / 32));
+    switch (kp->model) {
+        case 0: tree_walk_kernel<1, 0, 2><<<walk_grid, block, smem, s>>>(args); break;
+        case 1: tree_walk_kernel<1, 1, 2><<<walk_grid, block, smem, s>>>(args); break;
+        case 2: tree_walk_kernel<1, 2, 2><<<walk_grid, block, smem, s>>>(args); break;
+        default:
+            set_error("tree lists: core models 0..2 only");
+            return BS_ERR_ARG;
+    }
+    BS_CHECK_LAUNCH("tree_walk_kernel (lists)");
+    lists->n = n;
+    lists->target_warps = target_warps;
+    lists->perm = perm;
+    lists->ex_pos = ex_pos;
+    lists->ex_ptr = ex_pos ? tgt->ex_ptr : nullptr;
+    lists->list = list;
+    lists->unit_chunks = unit_chunks;
+    lists->list_len = list_len;
+    lists->state = state;
+    return BS_OK;
+}
+
+}  // namespace bs
+
+namespace {
 
 // Runs the evaluation, waits for it and reads counters and the overflow flag into the context's statistics.
 int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const bs_targets *tgt,

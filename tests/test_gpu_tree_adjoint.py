@@ -1,0 +1,154 @@
+"""The adjoint of the tree sum (bs_tree_adjoint) against the exact adjoint and against finite differences of the tree
+forward it differentiates.
+
+* No far field (theta 1e-9: every node is opened): the tree adjoint is the exact adjoint, so it equals
+  bs_adjoint_direct (itself checked against central differences and the VSM columns) within 1e-12 relative in FP64
+  and 1e-5 in mixed precision (FP32 pair terms).
+* Central differences (h = 1e-4 m, FP64 forward) of the tree sum at theta 0.3, orders 2 and 5: the tree adjoint holds
+  node centres and acceptance decisions fixed, so coordinates are taken only where the forward's tree, accepted nodes
+  and near pairs stay the same under the perturbation (identical counters at x - h, x and x + h) and where the
+  perturbed endpoint is interior to every node box that holds it (a box's extreme endpoints move its centre); there
+  the difference quotient equals the adjoint to 1e-6 of the gradient's scale.  Circulations enter linearly: exact.
+* The benchmark's setting (fifth-order Morton tree, theta 0.215, leaf 384, mixed) on the 468-row rotor wake (102k
+  segments x 20,570 targets): every gradient within 2e-5 relative L2 of the exact adjoint.
+* The autograd function's backward on a tree forward is the tree adjoint.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def small_wake(rows=14, targets=700, seed=9):
+    from openfawe_b200 import wakes
+    case = wakes.rotor_sheet(rows, seed=seed, targets=targets)
+    a = case["starts"]
+    b = case["nodes"][case["edges"][:, 1]]
+    rng = np.random.default_rng(seed)
+    w = rng.normal(size=case["points"].shape)
+    return case["points"], a, b, case["gamma"], case["radius"], w
+
+
+def tree_forward(device, x, a, b, g, r, theta, order, leaf, kind, precision="fp64", model=2):
+    import torch
+    from openfawe_b200 import adjoint, engine
+    s, d, length = adjoint.segments_from_endpoints(torch.as_tensor(a, device=device), torch.as_tensor(b, device=device))
+    src = engine.Sources(s, d, length, g, r, device)
+    u, _, far = engine.tree_sum(src, engine.Targets(x, None, device), model, "zero", precision, 128, 3.0, theta, order,
+                                leaf, 3.0, kind)
+    st = engine.last_stats(device)
+    return u.cpu().numpy(), (st["near_pairs"], st["far_evaluations"], st["nodes"], int(far.sum().item()))
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.mark.parametrize("kind", ["morton", "median"])
+def test_tree_adjoint_without_far_field_is_the_exact_adjoint(device, kind):
+    import torch
+    from openfawe_b200 import adjoint
+    x, a, b, g, r, w = small_wake()
+    pts = torch.as_tensor(x, device=device)
+    exact = [t.cpu().numpy() for t in adjoint.adjoint_direct(pts, a, b, g, r, 2, w)]
+    for precision, tol in (("fp64", 1e-12), ("mixed", 1e-5)):
+        got = [t.cpu().numpy() for t in adjoint.adjoint_tree(pts, a, b, g, r, 2, w, precision=precision, theta=1e-9,
+                                                             order=2, leaf_size=32, kind=kind)]
+        for name, u, v in zip(("points", "starts", "ends", "gamma"), got, exact):
+            assert rel(u, v) <= tol, (kind, precision, name, rel(u, v))
+
+
+def interior_endpoints(x, a, b, g, r, leaf, kind, device):
+    """(segment, end, axis) triples whose coordinate is strictly inside the endpoint box of every node holding the
+    segment (moving it moves no node centre)."""
+    import torch
+    from openfawe_b200 import adjoint, engine
+    s, d, length = adjoint.segments_from_endpoints(torch.as_tensor(a, device=device), torch.as_tensor(b, device=device))
+    tree = engine.build_tree(engine.Sources(s, d, length, g, r, device), leaf_size=leaf, kind=kind, order=2)
+    arr = tree.export()
+    ends = np.stack((a, b), axis=1)  # [m, 2, 3]
+    extreme = np.zeros((len(a), 2, 3), dtype=bool)
+    for lo, hi in zip(arr["lo"], arr["hi"]):
+        segs = arr["order"][lo:hi]
+        e = ends[segs]
+        for axis in range(3):
+            vals = e[:, :, axis]
+            extreme[segs, :, axis] |= (vals == vals.min()) | (vals == vals.max())
+    return [(i, k, axis) for i in range(len(a)) for k in range(2) for axis in range(3) if not extreme[i, k, axis]]
+
+
+@pytest.mark.parametrize("order,kind", [(2, "median"), (5, "morton")])
+def test_tree_adjoint_against_central_differences(device, order, kind):
+    import torch
+    from openfawe_b200 import adjoint
+    theta, leaf, h = 0.3, 16, 1e-4
+    x, a, b, g, r, w = small_wake(rows=10, targets=400, seed=order)
+    pts = torch.as_tensor(x, device=device)
+    gx, ga, gb, gg = [t.cpu().numpy() for t in adjoint.adjoint_tree(pts, a, b, g, r, 2, w, precision="fp64",
+                                                                    theta=theta, order=order, leaf_size=leaf,
+                                                                    kind=kind)]
+    base_u, base_c = tree_forward(device, x, a, b, g, r, theta, order, leaf, kind)
+    assert base_c[1] > 0  # the far field takes part
+    loss = lambda u: float(np.sum(w * u))  # noqa: E731
+    scale = max(np.abs(gx).max(), np.abs(ga).max(), np.abs(gb).max())
+    rng = np.random.default_rng(order)
+    candidates = interior_endpoints(x, a, b, g, r, leaf, kind, device)
+    checked = 0
+    trials = [("point", int(i), 0, int(k)) for i, k in zip(rng.integers(len(x), size=24), rng.integers(3, size=24))]
+    trials += [("end",) + candidates[int(j)] for j in rng.choice(len(candidates), size=48, replace=False)]
+    for trial in trials:
+        plus, minus = [x.copy(), a.copy(), b.copy()], [x.copy(), a.copy(), b.copy()]
+        if trial[0] == "point":
+            _, i, _, k = trial
+            which, grad = 0, gx[i, k]
+        else:
+            _, i, end, k = trial
+            which, grad = 1 + end, (ga if end == 0 else gb)[i, k]
+        plus[which][i, k] += h
+        minus[which][i, k] -= h
+        up, cp = tree_forward(device, *plus, g, r, theta, order, leaf, kind)
+        um, cm = tree_forward(device, *minus, g, r, theta, order, leaf, kind)
+        if cp != base_c or cm != base_c:
+            continue  # the tree or its decisions changed: the forward is not differentiable across that step
+        fd = (loss(up) - loss(um)) / (2 * h)
+        assert abs(fd - grad) <= 1e-6 * scale, (order, kind, trial, fd, grad)
+        checked += 1
+    assert checked >= 40, checked
+    # circulations enter linearly: the derivative is exact
+    for s_ in rng.integers(len(g), size=6):
+        gp = g.copy()
+        gp[s_] += 1.0
+        u1, _ = tree_forward(device, x, a, b, gp, r, theta, order, leaf, kind)
+        assert abs(loss(u1) - loss(base_u) - gg[s_]) <= 1e-10 * max(1.0, np.abs(gg).max())
+
+
+def test_tree_adjoint_at_the_bench_setting_matches_the_exact_gradient(device):
+    import torch
+    from openfawe_b200 import adjoint, wakes
+    case = wakes.rotor_sheet(468, seed=468, targets=20570)
+    x, a, g, r = case["points"], case["starts"], case["gamma"], case["radius"]
+    b = case["nodes"][case["edges"][:, 1]]
+    w = np.random.default_rng(5).standard_normal(x.shape).astype(np.float32).astype(np.float64)
+    pts = torch.as_tensor(x, device=device)
+    exact = [t.cpu().numpy() for t in adjoint.adjoint_direct(pts, a, b, g, r, 2, w)]
+    got = [t.cpu().numpy() for t in adjoint.adjoint_tree(pts, a, b, g, r, 2, w, precision="mixed", theta=0.215,
+                                                         order=5, leaf_size=384, kind="morton")]
+    for name, u, v in zip(("points", "starts", "ends", "gamma"), got, exact):
+        assert rel(u, v) <= 2e-5, (name, rel(u, v))
+
+
+def test_autograd_backward_of_a_tree_forward_is_the_tree_adjoint(device):
+    import torch
+    from openfawe_b200 import adjoint
+    x, a, b, g, r, w = small_wake(rows=8, targets=300, seed=4)
+    tensors = [torch.tensor(v, device=device, requires_grad=True) for v in (x, a, b, g)]
+    radius = torch.tensor(r, device=device)
+    opts = dict(model=2, method="tree", precision="mixed", theta=0.3, order=5, leaf_size=16, kind="morton",
+                singularity="zero")
+    u = adjoint.induced_velocity(*tensors, radius, **opts)
+    wt = torch.tensor(w, device=device)
+    (u * wt).sum().backward()
+    ref = adjoint.adjoint_tree(tensors[0].detach(), a, b, g, r, 2, wt, precision="mixed", theta=0.3, order=5,
+                               leaf_size=16, kind="morton")
+    for t, gref in zip(tensors, ref):
+        assert rel(t.grad.cpu().numpy(), gref.cpu().numpy()) <= 1e-6
