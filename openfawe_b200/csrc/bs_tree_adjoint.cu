@@ -27,6 +27,7 @@
 // the expansion's dependence on its centre is of the truncation order).  Gradients are summed with atomics: the
 // result is repeatable to rounding, not bit for bit.
 #include <algorithm>
+#include <type_traits>
 
 #include "bs_pair_vjp.cuh"
 #include "bs_sort.cuh"
@@ -238,9 +239,10 @@ __device__ __forceinline__ bool position_excluded(const int32_t *ex_pos, int64_t
 // target gets one shared-memory add per warp and group.
 template <int PREC, int MODEL>
 __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
+    using T = typename std::conditional<PREC == 0, double, float>::type;  // the sums' type: FP64 in FP64 mode
     __shared__ float sx[6][NEAR_TARGETS];  // two-float target coordinates: hi x, y, z, lo x, y, z
     __shared__ float sw[3][NEAR_TARGETS];
-    __shared__ float sacc[3][NEAR_TARGETS];
+    __shared__ T sacc[3][NEAR_TARGETS];
     __shared__ int sp[NEAR_TARGETS];
     __shared__ long long se0[NEAR_TARGETS], se1[NEAR_TARGETS];
     __shared__ long long s_item;
@@ -262,7 +264,7 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
                 sx[k][tid] = hi;
                 sx[3 + k][tid] = lo;
                 sw[k][tid] = (float)a.cot[3 * (int64_t)p + k];
-                sacc[k][tid] = 0.f;
+                sacc[k][tid] = T(0);
             }
             se0[tid] = a.ex_ptr ? a.ex_ptr[p] : 0;
             se1[tid] = a.ex_ptr ? a.ex_ptr[p + 1] : 0;
@@ -274,17 +276,23 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
             const bool valid = s < nr.hi;
             Seg32 r{};
             if (valid && PREC != 0) r = a.seg32[s];
-            float sg[7] = {0, 0, 0, 0, 0, 0, 0};
+            T sg[7] = {0, 0, 0, 0, 0, 0, 0};
             for (int g0 = 0; g0 < nt; g0 += 32) {
-                float tacc0 = 0.f, tacc1 = 0.f, tacc2 = 0.f;
+                T tacc0 = 0, tacc1 = 0, tacc2 = 0;
                 for (int j = 0; j < 32; ++j) {
                     const int t = g0 + ((lane + j) & 31);
-                    float g1[3] = {0.f, 0.f, 0.f}, g2[3] = {0.f, 0.f, 0.f}, gg = 0.f;
+                    T g1[3] = {0, 0, 0}, g2[3] = {0, 0, 0}, gg = 0;
                     if (valid && t < nt && !(se0[t] < se1[t] && position_excluded(a.ex_pos, se0[t], se1[t], s))) {
                         bool need64 = true;
-                        if (PREC != 0)
+                        if (PREC != 0) {
+                            float f1[3], f2[3], fg = 0.f;
                             need64 = pair_vjp32<MODEL>(sx[0][t], sx[1][t], sx[2][t], sx[3][t], sx[4][t], sx[5][t], r,
-                                                       sw[0][t], sw[1][t], sw[2][t], a.near2, g1, g2, gg);
+                                                       sw[0][t], sw[1][t], sw[2][t], a.near2, f1, f2, fg);
+                            if (!need64) {
+                                for (int k = 0; k < 3; ++k) { g1[k] = (T)f1[k]; g2[k] = (T)f2[k]; }
+                                gg = (T)fg;
+                            }
+                        }
                         if (need64) {
                             const Seg64 q = a.seg64[s];
                             const double L = q.len;
@@ -300,8 +308,8 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
                             if (pair_vjp64(a.points[3 * (int64_t)p], a.points[3 * (int64_t)p + 1],
                                            a.points[3 * (int64_t)p + 2], as, MODEL, a.cot[3 * (int64_t)p],
                                            a.cot[3 * (int64_t)p + 1], a.cot[3 * (int64_t)p + 2], h1, h2, hg)) {
-                                for (int k = 0; k < 3; ++k) { g1[k] = (float)h1[k]; g2[k] = (float)h2[k]; }
-                                gg = (float)hg;
+                                for (int k = 0; k < 3; ++k) { g1[k] = (T)h1[k]; g2[k] = (T)h2[k]; }
+                                gg = (T)hg;
                             }
                         }
                     }
