@@ -4,11 +4,13 @@ forward it differentiates.
 * No far field (theta 1e-9: every node is opened): the tree adjoint is the exact adjoint, so it equals
   bs_adjoint_direct (itself checked against central differences and the VSM columns) within 1e-12 relative in FP64
   and 1e-5 in mixed precision (FP32 pair terms).
-* Central differences (h = 1e-4 m, FP64 forward) of the tree sum at theta 0.3, orders 2 and 5: the tree adjoint holds
-  node centres and acceptance decisions fixed, so coordinates are taken only where the forward's tree, accepted nodes
-  and near pairs stay the same under the perturbation (identical counters at x - h, x and x + h) and where the
-  perturbed endpoint is interior to every node box that holds it (a box's extreme endpoints move its centre); there
-  the difference quotient equals the adjoint to 1e-6 of the gradient's scale.  Circulations enter linearly: exact.
+* Central differences (h = 1e-4 m and h/2, Richardson-extrapolated, FP64 forward) of the tree sum at theta 0.3,
+  orders 2 and 5: targets sit 0.011 m above the sheet, where a plain central difference at 1e-4 m still carries a
+  truncation error of (h / 0.011 m)^2 ~ 1e-4, hence the extrapolation (error ~ h^4).  The tree adjoint holds node
+  centres and acceptance decisions fixed, so coordinates are taken only where the forward's tree, accepted nodes and
+  near pairs stay the same under the perturbations (identical counters at all of them) and where the perturbed
+  endpoint is interior to every node box that holds it (a box's extreme endpoints move its centre); there the
+  extrapolated quotient equals the adjoint to 1e-6 of the gradient's scale.  Circulations enter linearly: exact.
 * The benchmark's setting (fifth-order Morton tree, theta 0.215, leaf 384, mixed) on the 468-row rotor wake (102k
   segments x 20,570 targets): every gradient within 2e-5 relative L2 of the exact adjoint.
 * The autograd function's backward on a tree forward is the tree adjoint.
@@ -97,21 +99,26 @@ def test_tree_adjoint_against_central_differences(device, order, kind):
     trials = [("point", int(i), 0, int(k)) for i, k in zip(rng.integers(len(x), size=24), rng.integers(3, size=24))]
     trials += [("end",) + candidates[int(j)] for j in rng.choice(len(candidates), size=48, replace=False)]
     for trial in trials:
-        plus, minus = [x.copy(), a.copy(), b.copy()], [x.copy(), a.copy(), b.copy()]
         if trial[0] == "point":
             _, i, _, k = trial
             which, grad = 0, gx[i, k]
         else:
             _, i, end, k = trial
             which, grad = 1 + end, (ga if end == 0 else gb)[i, k]
-        plus[which][i, k] += h
-        minus[which][i, k] -= h
-        up, cp = tree_forward(device, *plus, g, r, theta, order, leaf, kind)
-        um, cm = tree_forward(device, *minus, g, r, theta, order, leaf, kind)
-        if cp != base_c or cm != base_c:
+        quotients, same = [], True
+        for step in (h, h / 2):
+            values = []
+            for sign in (1.0, -1.0):
+                moved = [x.copy(), a.copy(), b.copy()]
+                moved[which][i, k] += sign * step
+                u, c = tree_forward(device, *moved, g, r, theta, order, leaf, kind)
+                same = same and c == base_c
+                values.append(loss(u))
+            quotients.append((values[0] - values[1]) / (2 * step))
+        if not same:
             continue  # the tree or its decisions changed: the forward is not differentiable across that step
-        fd = (loss(up) - loss(um)) / (2 * h)
-        assert abs(fd - grad) <= 1e-6 * scale, (order, kind, trial, fd, grad)
+        fd = (4.0 * quotients[1] - quotients[0]) / 3.0
+        assert abs(fd - grad) <= 1e-6 * scale, (order, kind, trial, fd, grad, quotients)
         checked += 1
     assert checked >= 40, checked
     # circulations enter linearly: the derivative is exact
