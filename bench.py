@@ -333,8 +333,9 @@ def adjoint_measure(device, theta, bench_case=None):
            "adjoint_ms": adj, "fp64_direct_forward_ms": fwd, "mixed_tree_forward_ms": tree,
            "ratio_to_fp64_direct": adj / fwd, "ratio_to_tree_forward": adj / tree,
            "tree_adjoint": {"ms": tree_adj, "ratio_to_tree_forward": tree_adj / tree,
-                            "stages_ms": {"build_walk_transpose": stats["walk_ms"], "near_pairs": stats["list_ms"],
-                                          "far_pushdown_segments": stats["moments_ms"]},
+                            "stages_ms": {"build_walk_transpose": stats["build_ms"], "near_pairs": stats["walk_ms"],
+                                          "far_entries": stats["list_ms"],
+                                          "pushdown_segment_moments": stats["moments_ms"]},
                             "rel_l2_vs_exact_adjoint": err,
                             "setting": f"Morton tree, order {ORDER}, theta {theta}, leaf {LEAF}, mixed near pairs"}}
     if bench_case is not None:

@@ -240,8 +240,8 @@ __device__ __forceinline__ bool position_excluded(const int32_t *ex_pos, int64_t
 template <int PREC, int MODEL>
 __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
     using T = typename std::conditional<PREC == 0, double, float>::type;  // the sums' type: FP64 in FP64 mode
-    __shared__ float sx[6][NEAR_TARGETS];  // two-float target coordinates: hi x, y, z, lo x, y, z
-    __shared__ float sw[3][NEAR_TARGETS];
+    __shared__ float4 shi[NEAR_TARGETS], slo[NEAR_TARGETS];  // two-float target: (hi x, y, z, w_x), (lo x, y, z, w_y)
+    __shared__ float sw2[NEAR_TARGETS];                      // w_z
     __shared__ T sacc[3][NEAR_TARGETS];
     __shared__ int sp[NEAR_TARGETS];
     __shared__ long long se0[NEAR_TARGETS], se1[NEAR_TARGETS];
@@ -258,14 +258,14 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
         if (tid < nt) {
             const int p = a.perm[a.near_items[first + tid]];
             sp[tid] = p;
+            float hi[3], lo[3];
             for (int k = 0; k < 3; ++k) {
-                float hi, lo;
-                split2(a.points[3 * (int64_t)p + k], hi, lo);
-                sx[k][tid] = hi;
-                sx[3 + k][tid] = lo;
-                sw[k][tid] = (float)a.cot[3 * (int64_t)p + k];
+                split2(a.points[3 * (int64_t)p + k], hi[k], lo[k]);
                 sacc[k][tid] = T(0);
             }
+            shi[tid] = make_float4(hi[0], hi[1], hi[2], (float)a.cot[3 * (int64_t)p]);
+            slo[tid] = make_float4(lo[0], lo[1], lo[2], (float)a.cot[3 * (int64_t)p + 1]);
+            sw2[tid] = (float)a.cot[3 * (int64_t)p + 2];
             se0[tid] = a.ex_ptr ? a.ex_ptr[p] : 0;
             se1[tid] = a.ex_ptr ? a.ex_ptr[p + 1] : 0;
         }
@@ -282,12 +282,14 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
                 for (int j = 0; j < 32; ++j) {
                     const int t = g0 + ((lane + j) & 31);
                     T g1[3] = {0, 0, 0}, g2[3] = {0, 0, 0}, gg = 0;
-                    if (valid && t < nt && !(se0[t] < se1[t] && position_excluded(a.ex_pos, se0[t], se1[t], s))) {
+                    if (valid && t < nt &&
+                        !(a.ex_ptr && se0[t] < se1[t] && position_excluded(a.ex_pos, se0[t], se1[t], s))) {
                         bool need64 = true;
                         if (PREC != 0) {
                             float f1[3], f2[3], fg = 0.f;
-                            need64 = pair_vjp32<MODEL>(sx[0][t], sx[1][t], sx[2][t], sx[3][t], sx[4][t], sx[5][t], r,
-                                                       sw[0][t], sw[1][t], sw[2][t], a.near2, f1, f2, fg);
+                            const float4 th = shi[t], tl = slo[t];
+                            need64 = pair_vjp32<MODEL>(th.x, th.y, th.z, tl.x, tl.y, tl.z, r, th.w, tl.w, sw2[t],
+                                                       a.near2, f1, f2, fg);
                             if (!need64) {
                                 for (int k = 0; k < 3; ++k) { g1[k] = (T)f1[k]; g2[k] = (T)f2[k]; }
                                 gg = (T)fg;
@@ -345,14 +347,15 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
 constexpr int DER_ROW = N_DER + 1;  // odd row length: lanes' rows fall in different banks
 constexpr int H_SLOTS = 3;          // v of orders 1..6 per lane: 83 over 32 lanes
 
+template <int ORDER>
 __global__ void __launch_bounds__(32) far_adjoint_kernel(AdjArgs a) {
+    constexpr int NU = tuple_offset(ORDER + 1);      // moment tuples
+    constexpr int NV = tuple_offset(ORDER + 2) - 1;  // v of orders 1 .. ORDER + 1
     __shared__ double sb[32 * DER_ROW];
     __shared__ double sm[3 * N_RAW];
     __shared__ double swv[32][3];
     __shared__ long long s_item;
     const int lane = threadIdx.x;
-    const int order = a.order;
-    const int nv = tuple_offset(order + 2) - 1;  // v of orders 1 .. order + 1
     double *row = sb + lane * DER_ROW;
     for (;;) {
         if (lane == 0) s_item = (long long)atomicAdd(a.queue + 1, 1ull);
@@ -381,72 +384,86 @@ __global__ void __launch_bounds__(32) far_adjoint_kernel(AdjArgs a) {
                 swv[lane][2] = w2;
                 const double r2 = R0 * R0 + R1 * R1 + R2 * R2, ir2 = 1.0 / r2;
                 row[0] = sqrt(ir2);
-                const double R[3] = {R0, R1, R2};
-#pragma unroll 1
-                for (int n = 1; n <= order + 2; ++n) {
+#pragma unroll
+                for (int n = 1; n <= ORDER + 2; ++n) {
                     const double f1 = (double)(2 * n - 1), f2 = (double)(n - 1), fn = -ir2 / (double)n;
-                    for (int v = tuple_offset(n); v < tuple_offset(n + 1); ++v) {
-                        const int c0 = c_tc.c[v][0], c1 = c_tc.c[v][1], c2 = c_tc.c[v][2];
-                        double s1 = 0.0, s2 = 0.0;
-                        if (c0 >= 1) s1 += R[0] * row[tuple_index(c0 - 1, c1, c2)];
-                        if (c1 >= 1) s1 += R[1] * row[tuple_index(c0, c1 - 1, c2)];
-                        if (c2 >= 1) s1 += R[2] * row[tuple_index(c0, c1, c2 - 1)];
-                        if (c0 >= 2) s2 += row[tuple_index(c0 - 2, c1, c2)];
-                        if (c1 >= 2) s2 += row[tuple_index(c0, c1 - 2, c2)];
-                        if (c2 >= 2) s2 += row[tuple_index(c0, c1, c2 - 2)];
-                        row[v] = fn * (f1 * s1 + f2 * s2);
-                    }
-                }
-                // the target's gradient: -(1/4 pi) sum_u (-1)^|u| sum_(k,m) (u_k + 1)(u_m + delta_km + 1)
-                //                        (w x M_u)_k b_(u + e_k + e_m)
-                double gm0 = 0.0, gm1 = 0.0, gm2 = 0.0;
-#pragma unroll 1
-                for (int u = 0; u < tuple_offset(order + 1); ++u) {
-                    const int c[3] = {c_tc.c[u][0], c_tc.c[u][1], c_tc.c[u][2]};
-                    const double M0 = sm[u], M1 = sm[N_RAW + u], M2 = sm[2 * N_RAW + u];
-                    const double Q[3] = {w1 * M2 - w2 * M1, w2 * M0 - w0 * M2, w0 * M1 - w1 * M0};
-                    const double sign = ((c[0] + c[1] + c[2]) & 1) ? -1.0 : 1.0;
-                    double acc[3] = {0.0, 0.0, 0.0};
-                    for (int k = 0; k < 3; ++k) {
-                        for (int mm = 0; mm < 3; ++mm) {
-                            int e[3] = {c[0], c[1], c[2]};
-                            e[k] += 1;
-                            const double ck = (double)e[k];  // u_k + 1
-                            e[mm] += 1;
-                            const double cm = (double)e[mm];  // u_m + delta_km + 1
-                            acc[mm] += ck * cm * Q[k] * row[tuple_index(e[0], e[1], e[2])];
+#pragma unroll
+                    for (int c0 = n; c0 >= 0; --c0) {
+#pragma unroll
+                        for (int c1 = n - c0; c1 >= 0; --c1) {
+                            const int c2 = n - c0 - c1;
+                            double s1 = 0.0, s2 = 0.0;
+                            if (c0 >= 1) s1 = fma(R0, row[tuple_index(c0 - 1, c1, c2)], s1);
+                            if (c1 >= 1) s1 = fma(R1, row[tuple_index(c0, c1 - 1, c2)], s1);
+                            if (c2 >= 1) s1 = fma(R2, row[tuple_index(c0, c1, c2 - 1)], s1);
+                            if (c0 >= 2) s2 += row[tuple_index(c0 - 2, c1, c2)];
+                            if (c1 >= 2) s2 += row[tuple_index(c0, c1 - 2, c2)];
+                            if (c2 >= 2) s2 += row[tuple_index(c0, c1, c2 - 2)];
+                            row[tuple_index(c0, c1, c2)] = fn * fma(f1, s1, f2 * s2);
                         }
                     }
-                    gm0 += sign * acc[0];
-                    gm1 += sign * acc[1];
-                    gm2 += sign * acc[2];
                 }
-                atomicAdd(&a.gx[3 * (int64_t)p], -INV_FOUR_PI * gm0);
-                atomicAdd(&a.gx[3 * (int64_t)p + 1], -INV_FOUR_PI * gm1);
-                atomicAdd(&a.gx[3 * (int64_t)p + 2], -INV_FOUR_PI * gm2);
+                // read the row back from shared memory rather than keeping all of it in registers
+                asm volatile("" ::: "memory");
+                // the target's gradient: -(1/4 pi) sum_u (-1)^|u| sum_(k,m) (u_k + 1)(u_m + delta_km + 1)
+                //                        (w x M_u)_k b_(u + e_k + e_m)
+                double gm[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+                for (int n = 0; n <= ORDER; ++n) {
+#pragma unroll
+                    for (int c0 = n; c0 >= 0; --c0) {
+#pragma unroll
+                        for (int c1 = n - c0; c1 >= 0; --c1) {
+                            const int c[3] = {c0, c1, n - c0 - c1};
+                            const int u = tuple_index(c[0], c[1], c[2]);
+                            const double M0 = sm[u], M1 = sm[N_RAW + u], M2 = sm[2 * N_RAW + u];
+                            const double sign = (n & 1) ? -1.0 : 1.0;
+                            const double Q[3] = {sign * (w1 * M2 - w2 * M1), sign * (w2 * M0 - w0 * M2),
+                                                 sign * (w0 * M1 - w1 * M0)};
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+#pragma unroll
+                                for (int mm = 0; mm < 3; ++mm) {
+                                    int e[3] = {c[0], c[1], c[2]};
+                                    e[k] += 1;
+                                    const double ck = (double)e[k];  // u_k + 1
+                                    e[mm] += 1;
+                                    const double cm = (double)e[mm];  // u_m + delta_km + 1
+                                    gm[mm] = fma(ck * cm * Q[k], row[tuple_index(e[0], e[1], e[2])], gm[mm]);
+                                }
+                            }
+                        }
+                    }
+                }
+                atomicAdd(&a.gx[3 * (int64_t)p], -INV_FOUR_PI * gm[0]);
+                atomicAdd(&a.gx[3 * (int64_t)p + 1], -INV_FOUR_PI * gm[1]);
+                atomicAdd(&a.gx[3 * (int64_t)p + 2], -INV_FOUR_PI * gm[2]);
             }
             __syncwarp();
+#pragma unroll
             for (int q = 0; q < H_SLOTS; ++q) {
                 const int v = 1 + lane + 32 * q;
-                if (v - 1 >= nv) break;
-                for (int t = 0; t < nb; ++t) {
-                    const double b = sb[t * DER_ROW + v];
-                    H[q][0] += b * swv[t][0];
-                    H[q][1] += b * swv[t][1];
-                    H[q][2] += b * swv[t][2];
+                if (v - 1 < NV) {
+                    for (int t = 0; t < nb; ++t) {
+                        const double b = sb[t * DER_ROW + v];
+                        H[q][0] = fma(b, swv[t][0], H[q][0]);
+                        H[q][1] = fma(b, swv[t][1], H[q][1]);
+                        H[q][2] = fma(b, swv[t][2], H[q][2]);
+                    }
                 }
             }
             __syncwarp();
         }
         // H into shared (the rows are free now), then g_(i;u) = -(1/4 pi)(-1)^|u| sum_(k,j) eps_ikj (u_k + 1)
         // H_(u + e_k, j)
+#pragma unroll
         for (int q = 0; q < H_SLOTS; ++q) {
             const int v = 1 + lane + 32 * q;
-            if (v - 1 >= nv) break;
-            for (int j = 0; j < 3; ++j) sb[3 * v + j] = H[q][j];
+            if (v - 1 < NV)
+                for (int j = 0; j < 3; ++j) sb[3 * v + j] = H[q][j];
         }
         __syncwarp();
-        for (int u = lane; u < tuple_offset(order + 1); u += 32) {
+        for (int u = lane; u < NU; u += 32) {
             const int c0 = c_tc.c[u][0], c1 = c_tc.c[u][1], c2 = c_tc.c[u][2];
             const double sign = -INV_FOUR_PI * (((c0 + c1 + c2) & 1) ? -1.0 : 1.0);
             const double *H0 = sb + 3 * tuple_index(c0 + 1, c1, c2), *H1 = sb + 3 * tuple_index(c0, c1 + 1, c2),
@@ -465,10 +482,10 @@ __global__ void __launch_bounds__(32) far_adjoint_kernel(AdjArgs a) {
     }
 }
 
-// 4. One warp per leaf: the leaf's effective moment cotangent (its own plus every ancestor's, translated down), then
-// the derivative of each of its segments' moments about the leaf centre.
-__global__ void __launch_bounds__(128) leaf_adjoint_kernel(AdjArgs a) {
-    __shared__ double sg[4][3 * N_RAW];
+// 4a. One warp per leaf: the leaf's effective moment cotangent, its own plus every ancestor's translated down, written
+// over its row of G (nothing else reads a leaf's row after this); leaf_of marks the leaf's segment positions, or -1
+// when no cotangent reaches the leaf.
+__global__ void __launch_bounds__(128) pushdown_kernel(AdjArgs a, int32_t *leaf_of) {
     __shared__ double sd[4][3][6];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t leaf = (int64_t)blockIdx.x * 4 + wib;
@@ -476,9 +493,7 @@ __global__ void __launch_bounds__(128) leaf_adjoint_kernel(AdjArgs a) {
     const NodeRec nr = a.nodes[leaf];
     if (nr.left >= 0) return;  // warp-uniform
     const int order = a.order, nu = tuple_offset(order + 1);
-    double *g = sg[wib];
     bool any = a.far_count[leaf] > 0;
-    for (int q = lane; q < 3 * N_RAW; q += 32) g[q] = any ? a.G[(size_t)leaf * 3 * N_RAW + q] : 0.0;
     double acc[2][3] = {{0, 0, 0}, {0, 0, 0}};
     for (int anc = a.parent[leaf]; anc >= 0; anc = a.parent[anc]) {
         if (a.far_count[anc] == 0) continue;
@@ -511,64 +526,76 @@ __global__ void __launch_bounds__(128) leaf_adjoint_kernel(AdjArgs a) {
                     }
         }
     }
-    any = __any_sync(0xffffffffu, any);
-    if (!any) return;
-    __syncwarp();
+    double *g = a.G + (size_t)leaf * 3 * N_RAW;
     for (int h = 0; h < 2; ++h) {
         const int k = lane + 32 * h;
         if (k < nu)
-            for (int i = 0; i < 3; ++i) g[i * N_RAW + k] += acc[h][i];
+            for (int i = 0; i < 3; ++i) g[i * N_RAW + k] = (a.far_count[leaf] > 0 ? g[i * N_RAW + k] : 0.0) + acc[h][i];
     }
-    __syncwarp();
-    // three-point Gauss-Legendre rule on t in [0, 1]
+    for (int pos = nr.lo + lane; pos < nr.hi; pos += 32) leaf_of[pos] = any ? (int32_t)leaf : -1;
+}
+
+// 4b. One thread per segment: the derivative of its moments about its leaf centre against the leaf's effective
+// cotangent, by the three-point Gauss-Legendre rule on t in [0, 1] (exact for these degree <= 5 polynomials).
+template <int ORDER>
+__global__ void __launch_bounds__(128) segment_moments_adjoint_kernel(AdjArgs a, const int32_t *leaf_of) {
+    const int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= a.m) return;
+    const int leaf = leaf_of[pos];
+    if (leaf < 0) return;
+    const double *g = a.G + (size_t)leaf * 3 * N_RAW;
+    const NodeRec nr = a.nodes[leaf];
+    const int id = a.order32[pos];
+    const double A0 = a.starts[3 * (int64_t)id], A1 = a.starts[3 * (int64_t)id + 1],
+                 A2 = a.starts[3 * (int64_t)id + 2];
+    const double L = a.lengths[id];
+    const double l0 = a.directions[3 * (int64_t)id] * L, l1 = a.directions[3 * (int64_t)id + 1] * L,
+                 l2 = a.directions[3 * (int64_t)id + 2] * L;
+    const double Gm = a.gamma[id];
+    const double al[3] = {Gm * l0, Gm * l1, Gm * l2};
     const double gt[3] = {0.5 - 0.5 * 0.7745966692414834, 0.5, 0.5 + 0.5 * 0.7745966692414834};
     const double gw[3] = {5.0 / 18.0, 8.0 / 18.0, 5.0 / 18.0};
-    for (int pos = nr.lo + lane; pos < nr.hi; pos += 32) {
-        const int id = a.order32[pos];
-        const double A0 = a.starts[3 * (int64_t)id], A1 = a.starts[3 * (int64_t)id + 1],
-                     A2 = a.starts[3 * (int64_t)id + 2];
-        const double L = a.lengths[id];
-        const double l0 = a.directions[3 * (int64_t)id] * L, l1 = a.directions[3 * (int64_t)id + 1] * L,
-                     l2 = a.directions[3 * (int64_t)id + 2] * L;
-        const double Gm = a.gamma[id];
-        const double al[3] = {Gm * l0, Gm * l1, Gm * l2};
-        double dal[3] = {0, 0, 0}, drA[3] = {0, 0, 0}, drB[3] = {0, 0, 0};
-        for (int q = 0; q < 3; ++q) {
-            const double rho[3] = {A0 + gt[q] * l0 - nr.cx, A1 + gt[q] * l1 - nr.cy, A2 + gt[q] * l2 - nr.cz};
-            double pw[3][6];
-            for (int ax = 0; ax < 3; ++ax) {
-                pw[ax][0] = 1.0;
-                for (int e = 1; e < 6; ++e) pw[ax][e] = pw[ax][e - 1] * rho[ax];
-            }
-            double P[3] = {0, 0, 0}, dP[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};  // dP[i][axis]
-            for (int u = 0; u < nu; ++u) {
-                const int c0 = c_tc.c[u][0], c1 = c_tc.c[u][1], c2 = c_tc.c[u][2];
-                const double mono = pw[0][c0] * pw[1][c1] * pw[2][c2];
-                const double d0 = c0 ? c0 * pw[0][c0 - 1] * pw[1][c1] * pw[2][c2] : 0.0;
-                const double d1 = c1 ? c1 * pw[0][c0] * pw[1][c1 - 1] * pw[2][c2] : 0.0;
-                const double d2 = c2 ? c2 * pw[0][c0] * pw[1][c1] * pw[2][c2 - 1] : 0.0;
-                for (int i = 0; i < 3; ++i) {
-                    const double gv = g[i * N_RAW + u];
-                    P[i] += gv * mono;
-                    dP[i][0] += gv * d0;
-                    dP[i][1] += gv * d1;
-                    dP[i][2] += gv * d2;
-                }
-            }
-            for (int i = 0; i < 3; ++i) dal[i] += gw[q] * P[i];
-            for (int ax = 0; ax < 3; ++ax) {
-                const double dr = al[0] * dP[0][ax] + al[1] * dP[1][ax] + al[2] * dP[2][ax];
-                drA[ax] += gw[q] * (1.0 - gt[q]) * dr;
-                drB[ax] += gw[q] * gt[q] * dr;
-            }
-        }
-        double *o = a.gseg + 7 * (int64_t)pos;
+    double dal[3] = {0, 0, 0}, drA[3] = {0, 0, 0}, drB[3] = {0, 0, 0};
+#pragma unroll 1
+    for (int q = 0; q < 3; ++q) {
+        const double rho[3] = {A0 + gt[q] * l0 - nr.cx, A1 + gt[q] * l1 - nr.cy, A2 + gt[q] * l2 - nr.cz};
+        double pw[3][6];
         for (int ax = 0; ax < 3; ++ax) {
-            o[ax] += -Gm * dal[ax] + drA[ax];
-            o[3 + ax] += Gm * dal[ax] + drB[ax];
+            pw[ax][0] = 1.0;
+            for (int e = 1; e <= ORDER; ++e) pw[ax][e] = pw[ax][e - 1] * rho[ax];
         }
-        o[6] += dal[0] * l0 + dal[1] * l1 + dal[2] * l2;
+        double P[3] = {0, 0, 0}, dP[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};  // dP[i][axis]
+#pragma unroll 1
+        for (int u = 0; u < tuple_offset(ORDER + 1); ++u) {
+            const int c0 = c_tc.c[u][0], c1 = c_tc.c[u][1], c2 = c_tc.c[u][2];
+            const double p12 = pw[1][c1] * pw[2][c2];
+            const double mono = pw[0][c0] * p12;
+            const double d0 = c0 ? c0 * pw[0][c0 - 1] * p12 : 0.0;
+            const double d1 = c1 ? c1 * pw[0][c0] * pw[1][c1 - 1] * pw[2][c2] : 0.0;
+            const double d2 = c2 ? c2 * pw[0][c0] * pw[1][c1] * pw[2][c2 - 1] : 0.0;
+            for (int i = 0; i < 3; ++i) {
+                const double gv = g[i * N_RAW + u];
+                P[i] = fma(gv, mono, P[i]);
+                dP[i][0] = fma(gv, d0, dP[i][0]);
+                dP[i][1] = fma(gv, d1, dP[i][1]);
+                dP[i][2] = fma(gv, d2, dP[i][2]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) dal[i] += gw[q] * P[i];
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+            const double dr = al[0] * dP[0][ax] + al[1] * dP[1][ax] + al[2] * dP[2][ax];
+            drA[ax] += gw[q] * (1.0 - gt[q]) * dr;
+            drB[ax] += gw[q] * gt[q] * dr;
+        }
     }
+    double *o = a.gseg + 7 * pos;
+    for (int ax = 0; ax < 3; ++ax) {
+        o[ax] += -Gm * dal[ax] + drA[ax];
+        o[3 + ax] += Gm * dal[ax] + drB[ax];
+    }
+    o[6] += dal[0] * l0 + dal[1] * l1 + dal[2] * l2;
 }
 
 __global__ void adjoint_scatter_kernel(int64_t m, const int32_t *order32, const double *gseg, double *gA, double *gB,
@@ -583,6 +610,15 @@ __global__ void adjoint_scatter_kernel(int64_t m, const int32_t *order32, const 
 }
 
 unsigned blocks(int64_t n, int t) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
+
+template <int ORDER>
+void launch_far_segments(unsigned far_grid, bool far, int64_t m, cudaStream_t s, const AdjArgs &a,
+                         const int32_t *leaf_of, cudaEvent_t mid) {
+    if (far) far_adjoint_kernel<ORDER><<<far_grid, 32, 0, s>>>(a);
+    cudaEventRecord(mid, s);
+    pushdown_kernel<<<blocks(a.count, 4), 128, 0, s>>>(a, const_cast<int32_t *>(leaf_of));
+    segment_moments_adjoint_kernel<ORDER><<<blocks(m, 128), 128, 0, s>>>(a, leaf_of);
+}
 
 template <int PREC>
 void launch_near(int model, unsigned grid, cudaStream_t s, const AdjArgs &a) {
@@ -633,7 +669,7 @@ extern "C" int bs_tree_adjoint(bs_ctx *ctx, const bs_sources *src, const bs_tree
     if (grad_ends && m) BS_CUDA(cudaMemsetAsync(grad_ends, 0, 3 * m * sizeof(double), s));
     if (grad_gamma && m) BS_CUDA(cudaMemsetAsync(grad_gamma, 0, m * sizeof(double), s));
     if (n == 0 || m == 0) return BS_OK;
-    cudaEvent_t ev[5];
+    cudaEvent_t ev[6];
     for (auto &e : ev) cudaEventCreate(&e);
     cudaEventRecord(ev[0], s);
     bs_tree *tree = nullptr;
@@ -652,12 +688,13 @@ extern "C" int bs_tree_adjoint(bs_ctx *ctx, const bs_sources *src, const bs_tree
         double *raw = scratch.get<double>((size_t)K * 3 * N_RAW), *G = scratch.get<double>((size_t)K * 3 * N_RAW);
         double *gseg = scratch.get<double>((size_t)7 * m);
         double *gx = grad_points ? grad_points : scratch.get<double>((size_t)3 * n);
-        int32_t *parent = scratch.get<int32_t>(K);
+        int32_t *parent = scratch.get<int32_t>(K), *leaf_of = scratch.get<int32_t>(m);
         int *counts = scratch.get<int>((size_t)2 * K);
         int64_t *offs = scratch.get<int64_t>((size_t)4 * (K + 1));
         int64_t *d_totals = scratch.get<int64_t>(4);
         unsigned long long *queue = scratch.get<unsigned long long>(2);
-        if (rc == BS_OK && (!raw || !G || !gseg || !gx || !parent || !counts || !offs || !d_totals || !queue))
+        if (rc == BS_OK && (!raw || !G || !gseg || !gx || !parent || !leaf_of || !counts || !offs || !d_totals ||
+                            !queue))
             rc = scratch.status;
         int *far_count = counts, *near_count = counts + K;
         int64_t *far_off = offs, *near_off = offs + (K + 1), *far_item_off = offs + 2 * (K + 1),
@@ -746,7 +783,7 @@ extern "C" int bs_tree_adjoint(bs_ctx *ctx, const bs_sources *src, const bs_tree
             }();
             static const int far_resident = [] {
                 int r = 0;
-                return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, far_adjoint_kernel, 32, 0) == cudaSuccess
+                return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, far_adjoint_kernel<5>, 32, 0) == cudaSuccess
                            ? std::max(1, r) : 1;
             }();
             const unsigned near_grid = (unsigned)std::max<int64_t>(
@@ -759,22 +796,30 @@ extern "C" int bs_tree_adjoint(bs_ctx *ctx, const bs_sources *src, const bs_tree
                 else launch_near<1>(kp->model, near_grid, s, a);
             }
             cudaEventRecord(ev[3], s);
-            if (totals[2] > 0) far_adjoint_kernel<<<far_grid, 32, 0, s>>>(a);
-            leaf_adjoint_kernel<<<blocks(K, 4), 128, 0, s>>>(a);
+            const bool far = totals[2] > 0;
+            switch (tp->order) {
+                case 0: launch_far_segments<0>(far_grid, far, m, s, a, leaf_of, ev[4]); break;
+                case 1: launch_far_segments<1>(far_grid, far, m, s, a, leaf_of, ev[4]); break;
+                case 2: launch_far_segments<2>(far_grid, far, m, s, a, leaf_of, ev[4]); break;
+                case 3: launch_far_segments<3>(far_grid, far, m, s, a, leaf_of, ev[4]); break;
+                case 4: launch_far_segments<4>(far_grid, far, m, s, a, leaf_of, ev[4]); break;
+                default: launch_far_segments<5>(far_grid, far, m, s, a, leaf_of, ev[4]); break;
+            }
             adjoint_scatter_kernel<<<blocks(m, 256), 256, 0, s>>>(m, tree->order32, gseg, grad_starts, grad_ends,
                                                                   grad_gamma);
-            cudaEventRecord(ev[4], s);
+            cudaEventRecord(ev[5], s);
             cudaError_t le = cudaGetLastError();
             if (le == cudaSuccess) le = cudaStreamSynchronize(s);
             if (le != cudaSuccess) rc = cuda_fail(le, "bs_tree_adjoint");
         }
         if (rc == BS_OK) rc = check_sort_fault();
         if (rc == BS_OK) {
-            float total = 0.f, lists_ms = 0.f, near_ms = 0.f, rest_ms = 0.f;
-            cudaEventElapsedTime(&total, ev[0], ev[4]);
+            float total = 0.f, lists_ms = 0.f, near_ms = 0.f, far_ms = 0.f, seg_ms = 0.f;
+            cudaEventElapsedTime(&total, ev[0], ev[5]);
             cudaEventElapsedTime(&lists_ms, ev[0], ev[1]);
             cudaEventElapsedTime(&near_ms, ev[2], ev[3]);
-            cudaEventElapsedTime(&rest_ms, ev[3], ev[4]);
+            cudaEventElapsedTime(&far_ms, ev[3], ev[4]);
+            cudaEventElapsedTime(&seg_ms, ev[4], ev[5]);
             ctx->stats.points = n;
             ctx->stats.segments = m;
             ctx->stats.nodes = K;
@@ -782,9 +827,10 @@ extern "C" int bs_tree_adjoint(bs_ctx *ctx, const bs_sources *src, const bs_tree
             ctx->stats.far_evaluations = totals[0];
             ctx->stats.near_pairs = 0;
             ctx->stats.evaluate_ms = total;
-            ctx->stats.walk_ms = lists_ms;    // build, walk and transposition
-            ctx->stats.list_ms = near_ms;     // near pairs
-            ctx->stats.moments_ms = rest_ms;  // far entries, push-down, segment moments, scatter
+            ctx->stats.build_ms = lists_ms;  // build, walk and transposition
+            ctx->stats.walk_ms = near_ms;    // near pairs
+            ctx->stats.list_ms = far_ms;     // far entries
+            ctx->stats.moments_ms = seg_ms;  // push-down, segment moments, scatter
         }
     }
     tree_release(tree, s);
