@@ -198,6 +198,18 @@ int bs_forest_eval(bs_ctx *ctx, const bs_tree *forest, const bs_tree_params *tp,
 int bs_forest_graph(bs_ctx *ctx, const bs_tree *forest, const bs_tree_params *tp, const bs_targets *tgt,
                     const int64_t *target_wake_ptr, const bs_kernel_params *kp, double *out, int8_t *flags,
                     int64_t *far_counts, bs_graph **graph);
+/* bs_forest_eval / bs_forest_graph with targets summed exactly (the batched form of the reference's control-point
+ * induction, vsm_wake.history_vsm_induction, src/openfawe/aero/vsm_wake.py:255-300, which sums the wake exactly at a
+ * wing's control and load points): exact (device uint8 [n], input order; NULL = none) marks targets for which no far
+ * node is accepted, so their velocity is the full sum over their wake's segments (in tree order, FP64 near-field rule
+ * of the precision), evaluated in the same traversal and persistent list launch as the other targets; their far
+ * counts are zero. */
+int bs_forest_eval_exact(bs_ctx *ctx, const bs_tree *forest, const bs_tree_params *tp, const bs_targets *tgt,
+                         const int64_t *target_wake_ptr, const uint8_t *exact, const bs_kernel_params *kp,
+                         double *out, int8_t *flags, int64_t *far_counts, bs_stream stream);
+int bs_forest_graph_exact(bs_ctx *ctx, const bs_tree *forest, const bs_tree_params *tp, const bs_targets *tgt,
+                          const int64_t *target_wake_ptr, const uint8_t *exact, const bs_kernel_params *kp,
+                          double *out, int8_t *flags, int64_t *far_counts, bs_graph **graph);
 int bs_graph_launch(bs_graph *graph, bs_stream stream);
 int bs_graph_status(bs_graph *graph, bs_stats *stats);
 void bs_graph_free(bs_graph *graph);

@@ -80,6 +80,10 @@ SIGNATURES = {
                                       ctypes.POINTER(KernelParams), _p, _p, _p, _p]),
     "bs_forest_graph": (ctypes.c_int, [_p, _p, ctypes.POINTER(TreeParams), ctypes.POINTER(Targets), _p,
                                        ctypes.POINTER(KernelParams), _p, _p, _p, ctypes.POINTER(_p)]),
+    "bs_forest_eval_exact": (ctypes.c_int, [_p, _p, ctypes.POINTER(TreeParams), ctypes.POINTER(Targets), _p, _p,
+                                            ctypes.POINTER(KernelParams), _p, _p, _p, _p]),
+    "bs_forest_graph_exact": (ctypes.c_int, [_p, _p, ctypes.POINTER(TreeParams), ctypes.POINTER(Targets), _p, _p,
+                                             ctypes.POINTER(KernelParams), _p, _p, _p, ctypes.POINTER(_p)]),
     "bs_graph_launch": (ctypes.c_int, [_p, _p]),
     "bs_graph_status": (ctypes.c_int, [_p, ctypes.POINTER(Stats)]),
     "bs_graph_free": (None, [_p]),

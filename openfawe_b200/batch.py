@@ -8,6 +8,11 @@ evaluates one wake per call; ``sequential`` times that pattern on the same wakes
 
 ``autotune`` is the project's tuner of the launch shapes: it times candidate leaf sizes and traversal block sizes on
 the batch itself with CUDA events and keeps the fastest per size class of batch.
+
+Control points: the reference's VSM free wake also sums every wake exactly at its wing's control and load points
+(vsm_wake.history_vsm_induction, src/openfawe/aero/vsm_wake.py:255-300).  ``WakeBatch(cases, control=[points of wake
+0, ...])`` appends those points to each wake's targets, marked exact (no far node is accepted for them), so both
+sums of every wake run in the one traversal and persistent list launch (and graph); ``split_control`` returns them.
 """
 import numpy as np
 import torch
@@ -21,20 +26,31 @@ class WakeBatch:
     """Wakes given as backend-argument dicts (``wakes.rotor_sheet`` and friends: points, starts, directions, lengths,
     gamma, radius, model); all wakes share the core model."""
 
-    def __init__(self, cases, device=0, leaf_size=32):
+    def __init__(self, cases, device=0, leaf_size=32, control=None):
         self.device = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
         models = {int(c["model"]) for c in cases}
         if len(models) != 1:
             raise ValueError("all wakes of a batch must use one core model")
         self.model = models.pop()
+        if control is not None and len(control) != len(cases):
+            raise ValueError("control: one point array per wake (or None)")
+        ctrl = [np.zeros((0, 3)) if control is None or control[w] is None
+                else np.asarray(control[w], dtype=np.float64).reshape(-1, 3) for w in range(len(cases))]
         seg_counts = [len(c["starts"]) for c in cases]
-        tgt_counts = [len(c["points"]) for c in cases]
+        own_counts = [len(c["points"]) for c in cases]
+        tgt_counts = [a + len(b) for a, b in zip(own_counts, ctrl)]
         self.wake_ptr = np.concatenate(([0], np.cumsum(seg_counts))).astype(np.int64)
         self.target_ptr = np.concatenate(([0], np.cumsum(tgt_counts))).astype(np.int64)
+        self.own_counts = own_counts
         cat = lambda key: np.concatenate([c[key] for c in cases])  # noqa: E731
         self.sources = engine.Sources(cat("starts"), cat("directions"), cat("lengths"), cat("gamma"), cat("radius"),
                                       self.device)
-        self.targets = engine.Targets(cat("points"), None, self.device)
+        points = np.concatenate([np.concatenate((c["points"], q)) for c, q in zip(cases, ctrl)])
+        self.exact = None
+        if control is not None:
+            self.exact = np.concatenate([np.concatenate((np.zeros(len(c["points"]), np.uint8),
+                                                         np.ones(len(q), np.uint8))) for c, q in zip(cases, ctrl)])
+        self.targets = engine.Targets(points, None, self.device)
         self.leaf_size = leaf_size
         self.order = 2
         self.forest = None
@@ -58,19 +74,23 @@ class WakeBatch:
         if self.forest is None:
             self.build()
         return engine.forest_eval(self.forest, self.targets, self.target_ptr, self.model, singularity, precision,
-                                  block, near, theta, order)
+                                  block, near, theta, order, exact=self.exact)
 
     def capture(self, theta=0.04, order=2, precision="mixed", block=128, singularity="raise", near=3.0):
         """Capture the evaluation as a CUDA graph (``launch()`` replays it)."""
         if self.forest is None:
             self.build()
         self.graph = engine.Graph(self.forest, self.targets, self.target_ptr, self.model, singularity, precision, block,
-                                  near, theta, order)
+                                  near, theta, order, exact=self.exact)
         return self.graph
 
     def split(self, array):
-        """Per-wake views of a concatenated per-target array."""
-        return [array[a:b] for a, b in zip(self.target_ptr[:-1], self.target_ptr[1:])]
+        """Per-wake views of a concatenated per-target array (each wake's own targets; control points left out)."""
+        return [array[a:a + k] for a, k in zip(self.target_ptr[:-1], self.own_counts)]
+
+    def split_control(self, array):
+        """Per-wake views of the control points' rows of a concatenated per-target array."""
+        return [array[a + k:b] for a, k, b in zip(self.target_ptr[:-1], self.own_counts, self.target_ptr[1:])]
 
 
 def device_ms(fn, repeats=3):

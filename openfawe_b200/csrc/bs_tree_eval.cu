@@ -71,6 +71,8 @@ struct EvalArgs {
     int chunks;
     const int32_t *root_of;       // forests: root node of each (sorted) target's wake, -1 for none; null: node 0
     unsigned long long *queue;    // work counter of the persistent list kernel
+    const uint8_t *exact;         // per target (input order), or null: nonzero = no far node is accepted for it (its
+                                  // velocity is the exact sum over every segment, in tree order)
 };
 
 // Per-lane state of a target.
@@ -356,6 +358,7 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
     t.load(a, gw * 32 + lane);
     int64_t e = 0, e1 = 0;
     if (t.valid && a.ex_ptr) { e = a.ex_ptr[t.p]; e1 = a.ex_ptr[t.p + 1]; }
+    const bool exact = a.exact && t.valid && a.exact[t.p];
     Acc<PREC> acc;
     int flag = BS_FLAG_OK;
     long long far = 0, far_total = 0, near_pairs = 0, fp64_pairs = 0, visits = 0, pair_slots = 0;
@@ -420,6 +423,7 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
                 while (q < e1 && a.ex_pos[q] < nr.lo) ++q;
                 if (q < e1 && a.ex_pos[q] < nr.hi) accept = false;
             }
+            if (exact) accept = false;  // a target summed exactly opens every node
         }
         const unsigned farm = __ballot_sync(0xffffffffu, mine && accept);
         const unsigned openm = mask & ~farm;
@@ -873,6 +877,7 @@ struct EvalPre {
     const int32_t *perm = nullptr;
     cudaEvent_t perm_ready = nullptr;
     cudaEvent_t far_ready = nullptr;
+    const uint8_t *exact = nullptr;  // EvalArgs::exact
 };
 
 // Everything the evaluation launches, on stream s, with scratch from `scratch` (pool or arena).  No host
@@ -967,6 +972,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     args.pflag = pflag;
     args.chunks = chunks;
     args.root_of = root_of;
+    args.exact = pre ? pre->exact : nullptr;
     args.unit_chunks = unit_chunks;
     args.pool_cursor = queue + 1;
     args.pool_chunks = pool / LIST_CHUNK;
@@ -1132,7 +1138,10 @@ int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const b
     }
     if (host[0] >> 32) {  // a full list met a node whose records were still being computed: again, with them complete
         EvalPre again;
-        if (pre) again.perm = pre->perm;
+        if (pre) {
+            again.perm = pre->perm;
+            again.exact = pre->exact;
+        }
         return eval_run(ctx, tree, tp, tgt, target_wake_ptr, nw, kp, out, flags, far_counts, s, &again);
     }
     return BS_OK;
@@ -1187,6 +1196,23 @@ extern "C" int bs_forest_eval(bs_ctx *ctx, const bs_tree *forest, const bs_tree_
     BS_CUDA(cudaSetDevice(ctx->device));
     return eval_run(ctx, forest, tp, tgt, target_wake_ptr, forest->nwakes, kp, out, flags, far_counts,
                     (cudaStream_t)stream);
+}
+
+extern "C" int bs_forest_eval_exact(bs_ctx *ctx, const bs_tree *forest, const bs_tree_params *tp,
+                                    const bs_targets *tgt, const int64_t *target_wake_ptr, const uint8_t *exact,
+                                    const bs_kernel_params *kp, double *out, int8_t *flags, int64_t *far_counts,
+                                    bs_stream stream) {
+    int rc = check_eval_args(ctx, forest, tp, tgt, kp, out, flags);
+    if (rc != BS_OK || tgt->n == 0) return rc;
+    if (!forest->wake_root || !target_wake_ptr) {
+        set_error("bs_forest_eval_exact: not a forest, or no target ranges");
+        return BS_ERR_ARG;
+    }
+    BS_CUDA(cudaSetDevice(ctx->device));
+    EvalPre pre;
+    pre.exact = exact;
+    return eval_run(ctx, forest, tp, tgt, target_wake_ptr, forest->nwakes, kp, out, flags, far_counts,
+                    (cudaStream_t)stream, &pre);
 }
 
 extern "C" int bs_tree_sum_host(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, const bs_targets *tgt,
@@ -1318,9 +1344,9 @@ struct bs_graph {
     unsigned long long *state = nullptr;
 };
 
-extern "C" int bs_forest_graph(bs_ctx *ctx, const bs_tree *forest, const bs_tree_params *tp, const bs_targets *tgt,
-                               const int64_t *target_wake_ptr, const bs_kernel_params *kp, double *out,
-                               int8_t *flags, int64_t *far_counts, bs_graph **graph) {
+static int forest_graph(bs_ctx *ctx, const bs_tree *forest, const bs_tree_params *tp, const bs_targets *tgt,
+                        const int64_t *target_wake_ptr, const uint8_t *exact, const bs_kernel_params *kp,
+                        double *out, int8_t *flags, int64_t *far_counts, bs_graph **graph) {
     if (!graph) {
         set_error("bs_forest_graph: null output");
         return BS_ERR_ARG;
@@ -1341,8 +1367,10 @@ extern "C" int bs_forest_graph(bs_ctx *ctx, const bs_tree *forest, const bs_tree
     {
         Scratch probe(ctx->pool, s);
         unsigned long long *state = probe.get<unsigned long long>(6);
+        EvalPre pre;
+        pre.exact = exact;
         rc = state ? eval_enqueue(ctx, forest, tp, tgt, target_wake_ptr, nw, kp, out, flags, far_counts, state, probe,
-                                  s)
+                                  s, &pre)
                    : probe.status;
         need = probe.requested;
         cudaError_t e = cudaStreamSynchronize(s);
@@ -1362,8 +1390,10 @@ extern "C" int bs_forest_graph(bs_ctx *ctx, const bs_tree *forest, const bs_tree
     }
     if (rc == BS_OK) {
         Scratch arena(g->arena, need + 4096, s);
+        EvalPre pre;
+        pre.exact = exact;
         int rc2 = eval_enqueue(ctx, forest, tp, tgt, target_wake_ptr, nw, kp, out, flags, far_counts, g->state,
-                               arena, s);
+                               arena, s, &pre);
         e = cudaStreamEndCapture(s, &cg);
         if (rc2 != BS_OK) rc = rc2;
         else if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamEndCapture");
@@ -1380,6 +1410,19 @@ extern "C" int bs_forest_graph(bs_ctx *ctx, const bs_tree *forest, const bs_tree
     }
     *graph = g;
     return BS_OK;
+}
+
+extern "C" int bs_forest_graph(bs_ctx *ctx, const bs_tree *forest, const bs_tree_params *tp, const bs_targets *tgt,
+                               const int64_t *target_wake_ptr, const bs_kernel_params *kp, double *out,
+                               int8_t *flags, int64_t *far_counts, bs_graph **graph) {
+    return forest_graph(ctx, forest, tp, tgt, target_wake_ptr, nullptr, kp, out, flags, far_counts, graph);
+}
+
+extern "C" int bs_forest_graph_exact(bs_ctx *ctx, const bs_tree *forest, const bs_tree_params *tp,
+                                     const bs_targets *tgt, const int64_t *target_wake_ptr, const uint8_t *exact,
+                                     const bs_kernel_params *kp, double *out, int8_t *flags, int64_t *far_counts,
+                                     bs_graph **graph) {
+    return forest_graph(ctx, forest, tp, tgt, target_wake_ptr, exact, kp, out, flags, far_counts, graph);
 }
 
 extern "C" int bs_graph_launch(bs_graph *g, bs_stream stream) {

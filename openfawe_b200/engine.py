@@ -321,8 +321,11 @@ def forest_roots(tree):
 
 
 def forest_eval(tree, targets, target_wake_ptr, model, singularity="raise", precision="mixed", block=128, near=3.0,
-                theta=0.5, order=2, clearance=3.0, stack_limit=0, far_counts=True):
-    """Evaluate every wake of a forest at its own targets (targets of wake w: [target_wake_ptr[w], ...[w+1]))."""
+                theta=0.5, order=2, clearance=3.0, stack_limit=0, far_counts=True, exact=None):
+    """Evaluate every wake of a forest at its own targets (targets of wake w: [target_wake_ptr[w], ...[w+1])).
+
+    ``exact`` (bool per target, or None): targets summed exactly over their wake's segments (no far node accepted), in
+    the same launch -- the batched form of the control-point induction (bs_forest_eval_exact)."""
     dev = tree.sources.device
     ptr = i64(target_wake_ptr, dev)
     out = torch.empty((targets.n, 3), dtype=torch.float64, device=dev)
@@ -331,20 +334,35 @@ def forest_eval(tree, targets, target_wake_ptr, model, singularity="raise", prec
     tp = tree_params(theta, order, tree.params.leaf_size, clearance, "morton", stack_limit)
     kp = kernel_params(model, singularity, precision, block, near)
     tgt = targets.struct()
-    L.check(L.library().bs_forest_eval(L.context(dev.index), tree.handle, ctypes.byref(tp), ctypes.byref(tgt),
-                                       _ptr(ptr), ctypes.byref(kp), _ptr(out), _ptr(flags), _ptr(far), _stream(dev)),
-            "bs_forest_eval")
+    if exact is None:
+        L.check(L.library().bs_forest_eval(L.context(dev.index), tree.handle, ctypes.byref(tp), ctypes.byref(tgt),
+                                           _ptr(ptr), ctypes.byref(kp), _ptr(out), _ptr(flags), _ptr(far),
+                                           _stream(dev)), "bs_forest_eval")
+    else:
+        mask = _exact_mask(exact, targets.n, dev)
+        L.check(L.library().bs_forest_eval_exact(L.context(dev.index), tree.handle, ctypes.byref(tp),
+                                                 ctypes.byref(tgt), _ptr(ptr), _ptr(mask), ctypes.byref(kp), _ptr(out),
+                                                 _ptr(flags), _ptr(far), _stream(dev)), "bs_forest_eval_exact")
     return out, flags, far
+
+
+def _exact_mask(exact, n, dev):
+    mask = exact if isinstance(exact, torch.Tensor) else torch.as_tensor(np.asarray(exact, dtype=np.uint8))
+    mask = mask.to(device=dev, dtype=torch.uint8).reshape(-1).contiguous()
+    if mask.numel() != n:
+        raise ValueError("exact mask: one entry per target")
+    return mask
 
 
 class Graph:
     """A captured forest (or tree) evaluation; ``launch()`` replays it on the current stream."""
 
     def __init__(self, tree, targets, target_wake_ptr, model, singularity="raise", precision="mixed", block=128,
-                 near=3.0, theta=0.5, order=2, clearance=3.0):
+                 near=3.0, theta=0.5, order=2, clearance=3.0, exact=None):
         dev = tree.sources.device
         self.tree, self.targets, self.device = tree, targets, dev
         self.ptr = None if target_wake_ptr is None else i64(target_wake_ptr, dev)
+        self.exact = None if exact is None else _exact_mask(exact, targets.n, dev)
         self.out = torch.empty((targets.n, 3), dtype=torch.float64, device=dev)
         self.flags = torch.empty(targets.n, dtype=torch.int8, device=dev)
         self.far = torch.empty(targets.n, dtype=torch.int64, device=dev)
@@ -353,9 +371,15 @@ class Graph:
         tgt = targets.struct()
         handle = ctypes.c_void_p()
         torch.cuda.current_stream(dev).synchronize()
-        L.check(L.library().bs_forest_graph(L.context(dev.index), tree.handle, ctypes.byref(tp), ctypes.byref(tgt),
-                                            _ptr(self.ptr), ctypes.byref(kp), _ptr(self.out), _ptr(self.flags),
-                                            _ptr(self.far), ctypes.byref(handle)), "bs_forest_graph")
+        if self.exact is None:
+            L.check(L.library().bs_forest_graph(L.context(dev.index), tree.handle, ctypes.byref(tp), ctypes.byref(tgt),
+                                                _ptr(self.ptr), ctypes.byref(kp), _ptr(self.out), _ptr(self.flags),
+                                                _ptr(self.far), ctypes.byref(handle)), "bs_forest_graph")
+        else:
+            L.check(L.library().bs_forest_graph_exact(L.context(dev.index), tree.handle, ctypes.byref(tp),
+                                                      ctypes.byref(tgt), _ptr(self.ptr), _ptr(self.exact),
+                                                      ctypes.byref(kp), _ptr(self.out), _ptr(self.flags),
+                                                      _ptr(self.far), ctypes.byref(handle)), "bs_forest_graph_exact")
         self._handle = handle
 
     def launch(self):

@@ -97,3 +97,41 @@ def test_autotune_and_sequential_agree(device):
         seq = seq.cpu().numpy()
         assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-5
         assert np.linalg.norm(seq - ref) / np.linalg.norm(ref) < 1e-5
+
+
+def _scale(points, case):
+    """sum_s |u_s| per point from the oracle's per-pair velocities."""
+    pairs, _ = O.pair_matrix(points, case["starts"], case["directions"], case["lengths"], case["radius"],
+                             case["model"], False)
+    return (np.linalg.norm(pairs, axis=2) * np.abs(case["gamma"])[None, :]).sum(axis=1)
+
+
+def test_control_points_summed_exactly_in_the_same_launch(device):
+    """Each wake's wing control points ride in the batch marked exact: no far node is accepted for them (far count 0),
+    so they equal the oracle's direct sum over their own wake (A1 bound in FP64, 1e-5 of sum |u_s| mixed), while the
+    wake's own targets keep their tree result; the captured graph replays the same bits."""
+    from openfawe_b200 import batch, wakes
+    cases = small_cases()[:4]
+    control = [wakes.ring_wing(64)["points"] + [0.1 * w, 0.0, 0.0] for w in range(len(cases))]
+    with_control = batch.WakeBatch(cases, device, control=control)
+    plain = batch.WakeBatch(cases, device)
+    for precision, tol in (("fp64", 1e-12), ("mixed", 1e-5)):
+        u, flags, far = with_control.evaluate(theta=0.3, precision=precision)
+        u0, _, far0 = plain.evaluate(theta=0.3, precision=precision)
+        assert not flags.any()
+        u, far, u0 = u.cpu().numpy(), far.cpu().numpy(), u0.cpu().numpy()
+        for w, (c, q) in enumerate(zip(cases, control)):
+            got = with_control.split_control(u)[w]
+            assert np.all(with_control.split_control(far)[w] == 0)
+            ref, flagged = O.direct_sum(q, *wakes.backend_args(c)[1:], no_exclusions(len(q)), "raise")
+            assert not flagged
+            err = np.linalg.norm(got - ref, axis=1)
+            assert np.all(err <= tol * _scale(q, c)), (precision, w, float(err.max()))
+            own, own0 = with_control.split(u)[w], plain.split(u0)[w]
+            assert np.linalg.norm(own - own0) / np.linalg.norm(own0) <= (1e-13 if precision == "fp64" else 1e-6)
+        assert int(far.sum()) == int(far0.sum().item()) and int(far.sum()) > 0
+    g = with_control.capture(theta=0.3, precision="mixed")
+    gu, _, gfar = g.launch()
+    fresh, _, ffar = with_control.evaluate(theta=0.3, precision="mixed")
+    assert np.array_equal(gu.cpu().numpy(), fresh.cpu().numpy())
+    assert np.array_equal(gfar.cpu().numpy(), ffar.cpu().numpy())
