@@ -65,10 +65,12 @@ struct EvalArgs {
     int64_t *far_counts;
     int *overflow;
     unsigned long long *counters;  // far evaluations, near pairs, fp64 pairs, visits, lane slots of leaf walks
-    // list kernel outputs
-    double *partial;     // [chunks][n][3]
-    int8_t *pflag;       // [chunks][n]
-    int chunks;
+    // list kernel: work items by warp of targets, each warp's list cut into a number of items proportional to its cost
+    // (item_off [target_warps + 1], from item_plan_kernel), and the items' partial sums
+    int *item_off;
+    int item_want;       // items wanted in all (about 96 a SM); the capacity is item_want + target warps
+    double *partial;     // [items][32 lanes][3]
+    int8_t *pflag;       // [items][32 lanes]
     const int32_t *root_of;       // forests: root node of each (sorted) target's wake, -1 for none; null: node 0
     unsigned long long *queue;    // work counter of the persistent list kernel
     const uint8_t *exact;         // per target (input order), or null: nonzero = no far node is accepted for it (its
@@ -524,10 +526,10 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
 // evaluates the item's far nodes and near leaves.  Partial sums per (chunk, target) are combined in chunk order by the
 // reduce kernel.
 template <int PREC, int MODEL>
-__device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, Seg64 *seg64_tile, Seg32 *seg32_tile,
-                                          long long &near_pairs, long long &fp64_pairs) {
+__device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, int chunks, int64_t item,
+                                          Seg64 *seg64_tile, Seg32 *seg32_tile, long long &near_pairs,
+                                          long long &fp64_pairs) {
     const int lane = threadIdx.x & 31;
-    const int chunks = a.chunks;
     // chunk c is the c-th slice of this warp's list by cost
     const int len = a.list_len[gw];
     const int64_t total = a.list_total[gw];
@@ -576,7 +578,7 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
     }
     flush();
     if (t.valid) {
-        const int64_t o = (int64_t)c * a.n + t.p;
+        const int64_t o = item * 32 + lane;
         a.partial[3 * o] = acc.x();
         a.partial[3 * o + 1] = acc.y();
         a.partial[3 * o + 2] = acc.z();
@@ -591,15 +593,22 @@ __global__ void __launch_bounds__(LIST_WARPS * 32, 3) tree_list_kernel(EvalArgs 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Seg64 *seg64_tile = reinterpret_cast<Seg64 *>(tile_mem) + warp * 32;
     Seg32 *seg32_tile = reinterpret_cast<Seg32 *>(tile_mem) + warp * 32;
-    const unsigned long long items = (unsigned long long)target_warps * a.chunks;
+    const unsigned long long items = (unsigned long long)a.item_off[target_warps];
     long long near_pairs = 0, fp64_pairs = 0;
     for (;;) {
         unsigned long long item = 0;
         if (lane == 0) item = atomicAdd(a.queue, 1ull);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= items) break;
-        list_item<PREC, MODEL>(a, (int64_t)(item / a.chunks), (int)(item % a.chunks), seg64_tile, seg32_tile,
-                               near_pairs, fp64_pairs);
+        // the warp of targets whose items hold this one: the last gw with item_off[gw] <= item
+        int64_t lo = 0, hi = target_warps;
+        while (hi - lo > 1) {
+            const int64_t mid = (lo + hi) >> 1;
+            if ((unsigned long long)a.item_off[mid] <= item) lo = mid; else hi = mid;
+        }
+        const int first = a.item_off[lo];
+        list_item<PREC, MODEL>(a, lo, (int)(item - first), a.item_off[lo + 1] - first, (int64_t)item, seg64_tile,
+                               seg32_tile, near_pairs, fp64_pairs);
     }
     for (int o = 16; o > 0; o >>= 1) {
         near_pairs += __shfl_xor_sync(0xffffffffu, near_pairs, o);
@@ -611,15 +620,58 @@ __global__ void __launch_bounds__(LIST_WARPS * 32, 3) tree_list_kernel(EvalArgs 
     }
 }
 
-// Chunks in order, then what the walk evaluated itself (later in depth-first order); first flag wins.
+// Work items of the list kernel: warp gw gets max(1, ceil(cost / unit)) items (at most 64), unit = total cost / want,
+// so every item costs about the same whatever its warp; item_off is their exclusive scan (one block).  The sum of the
+// items stays below want + target_warps, the capacity the caller allocates.
+__global__ void __launch_bounds__(1024) item_plan_kernel(int64_t target_warps, const int *list_total, int want,
+                                                         int *item_off) {
+    __shared__ long long part[1024];
+    const int t = threadIdx.x;
+    const int64_t per = (target_warps + 1023) / 1024, a0 = min(target_warps, t * per),
+                  a1 = min(target_warps, a0 + per);
+    long long cost = 0;
+    for (int64_t w = a0; w < a1; ++w) cost += list_total[w];
+    part[t] = cost;
+    __syncthreads();
+    for (int o = 512; o > 0; o >>= 1) {
+        if (t < o) part[t] += part[t + o];
+        __syncthreads();
+    }
+    const long long total = part[0];
+    __syncthreads();
+    const long long unit = max(1ll, (total + want - 1) / want);
+    long long items = 0;
+    for (int64_t w = a0; w < a1; ++w) items += min(64ll, max(1ll, ((long long)list_total[w] + unit - 1) / unit));
+    part[t] = items;
+    __syncthreads();
+    if (t == 0) {
+        long long run = 0;
+        for (int k = 0; k < 1024; ++k) {
+            const long long v = part[k];
+            part[k] = run;
+            run += v;
+        }
+        item_off[target_warps] = (int)run;
+    }
+    __syncthreads();
+    long long run = part[t];
+    for (int64_t w = a0; w < a1; ++w) {
+        item_off[w] = (int)run;
+        run += min(64ll, max(1ll, ((long long)list_total[w] + unit - 1) / unit));
+    }
+}
+
+// A target's items in order, then what the walk evaluated itself (later in depth-first order); first flag wins.
 template <int PREC>
 __global__ void tree_reduce_kernel(EvalArgs a, double *out, int8_t *flags) {
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= a.n) return;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;  // sorted target
+    if (i >= a.n) return;
+    const int64_t p = a.perm[i], gw = i >> 5;
+    const int lane = (int)(i & 31);
     Acc<PREC> acc;
     int flag = BS_FLAG_OK;
-    for (int c = 0; c < a.chunks; ++c) {
-        const int64_t o = (int64_t)c * a.n + p;
+    for (int item = a.item_off[gw]; item < a.item_off[gw + 1]; ++item) {
+        const int64_t o = (int64_t)item * 32 + lane;
         acc.add64(a.partial[3 * o], a.partial[3 * o + 1], a.partial[3 * o + 2]);
         if (flag == BS_FLAG_OK) flag = a.pflag[o];
     }
@@ -724,6 +776,7 @@ static void launch_pair(unsigned walk_grid, int block, size_t smem, unsigned lis
     if (t_marks) cudaEventRecord(t_marks[0], s);
     if (pop == 2) tree_walk_kernel<PREC, MODEL, 2><<<walk_grid, block, smem, s>>>(args);
     else tree_walk_kernel<PREC, MODEL, 1><<<walk_grid, block, smem, s>>>(args);
+    item_plan_kernel<<<1, 1024, 0, s>>>(target_warps, args.list_total, args.item_want, args.item_off);
     if (t_far_ready) cudaStreamWaitEvent(s, t_far_ready, 0);
     if (t_marks) cudaEventRecord(t_marks[1], s);
     tree_list_kernel<PREC, MODEL><<<list_grid, LIST_WARPS * 32, 0, s>>>(args, target_warps);
@@ -928,18 +981,21 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     BS_CUDA(cudaMemsetAsync(queue, 0, 2 * sizeof(unsigned long long), s));
     const int block = std::min(kp->block, 128);
     const int64_t target_warps = (n + 31) / 32;
-    // each warp's list is cut into `chunks` cost-balanced work items, ~96 items a SM in all: the persistent list
-    // kernel's last items then end close together (32 a SM left a 3-4% tail on the bench workload, 192 more partials)
-    const int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(64, ((int64_t)ctx->sm_count * 96 + target_warps - 1)
-                                                                       / target_warps));
+    // ~96 cost-balanced work items a SM in all, each warp's list cut in proportion to its cost (item_plan_kernel): the
+    // persistent list kernel's last items then end close together, whatever the spread of the warps' costs (32 a SM
+    // left a 3-4% tail on the bench workload)
+    const int want = ctx->sm_count * 96;
+    const size_t capacity = (size_t)want + (size_t)target_warps;
     const size_t slots = (size_t)target_warps, pool = (size_t)target_warps * LIST_POOL;
     int2 *list = scratch.get<int2>(pool);
     int *list_cost = scratch.get<int>(pool);
     int *unit_chunks = scratch.get<int>(slots * LIST_CHUNKS);
     int *list_len = scratch.get<int>(slots), *list_total = scratch.get<int>(slots);
-    double *walk_u = scratch.get<double>((size_t)3 * n), *partial = scratch.get<double>((size_t)3 * n * chunks);
-    int8_t *walk_flag = scratch.get<int8_t>((size_t)n), *pflag = scratch.get<int8_t>((size_t)n * chunks);
-    if (!list || !list_cost || !unit_chunks || !list_len || !list_total || !walk_u || !partial || !walk_flag || !pflag)
+    double *walk_u = scratch.get<double>((size_t)3 * n), *partial = scratch.get<double>(capacity * 32 * 3);
+    int8_t *walk_flag = scratch.get<int8_t>((size_t)n), *pflag = scratch.get<int8_t>(capacity * 32);
+    int *item_off = scratch.get<int>(slots + 1);
+    if (!list || !list_cost || !unit_chunks || !list_len || !list_total || !walk_u || !partial || !walk_flag || !pflag ||
+        !item_off)
         return scratch.status;
     EvalArgs args;
     args.n = n;
@@ -970,7 +1026,8 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     args.counters = state + 1;
     args.partial = partial;
     args.pflag = pflag;
-    args.chunks = chunks;
+    args.item_off = item_off;
+    args.item_want = want;
     args.root_of = root_of;
     args.exact = pre ? pre->exact : nullptr;
     args.unit_chunks = unit_chunks;
@@ -979,9 +1036,8 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     args.queue = queue;
     const size_t smem = (size_t)(block / 32) * (STACK_DEPTH * sizeof(int2) + 32 * sizeof(Seg64));
     const unsigned walk_grid = (unsigned)((target_warps + block / 32 - 1) / (block / 32));
-    const int64_t items = target_warps * chunks;
     const unsigned list_grid = (unsigned)std::max<int64_t>(
-        1, std::min<int64_t>((items + LIST_WARPS - 1) / LIST_WARPS, (int64_t)ctx->sm_count * 3));
+        1, std::min<int64_t>(((int64_t)capacity + LIST_WARPS - 1) / LIST_WARPS, (int64_t)ctx->sm_count * 3));
     t_far_ready = args.deferred ? pre->far_ready : nullptr;
     launch_eval(kp->precision, kp->model, walk_grid, block, smem, list_grid, target_warps, nblocks(n, 256), s, args,
                 out, flags);
@@ -1050,7 +1106,6 @@ int tree_lists(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp,
     args.walk_flag = walk_flag;
     args.overflow = reinterpret_cast<int *>(state);
     args.counters = state + 1;
-    args.chunks = 1;
     args.unit_chunks = unit_chunks;
     args.pool_cursor = queue + 1;
     args.pool_chunks = pool / LIST_CHUNK;
