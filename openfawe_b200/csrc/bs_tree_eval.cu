@@ -68,6 +68,7 @@ struct EvalArgs {
     // list kernel: work items by warp of targets, each warp's list cut into a number of items proportional to its cost
     // (item_off [target_warps + 1], from item_plan_kernel), and the items' partial sums
     int *item_off;
+    int *item_warp;      // [capacity]: the warp of targets of each item
     int item_want;       // items wanted in all (about 96 a SM); the capacity is item_want + target warps
     double *partial;     // [items][32 lanes][3]
     int8_t *pflag;       // [items][32 lanes]
@@ -600,12 +601,7 @@ __global__ void __launch_bounds__(LIST_WARPS * 32, 3) tree_list_kernel(EvalArgs 
         if (lane == 0) item = atomicAdd(a.queue, 1ull);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= items) break;
-        // the warp of targets whose items hold this one: the last gw with item_off[gw] <= item
-        int64_t lo = 0, hi = target_warps;
-        while (hi - lo > 1) {
-            const int64_t mid = (lo + hi) >> 1;
-            if ((unsigned long long)a.item_off[mid] <= item) lo = mid; else hi = mid;
-        }
+        const int64_t lo = a.item_warp[item];  // the warp of targets whose list this item slices
         const int first = a.item_off[lo];
         list_item<PREC, MODEL>(a, lo, (int)(item - first), a.item_off[lo + 1] - first, (int64_t)item, seg64_tile,
                                seg32_tile, near_pairs, fp64_pairs);
@@ -624,7 +620,7 @@ __global__ void __launch_bounds__(LIST_WARPS * 32, 3) tree_list_kernel(EvalArgs 
 // so every item costs about the same whatever its warp; item_off is their exclusive scan (one block).  The sum of the
 // items stays below want + target_warps, the capacity the caller allocates.
 __global__ void __launch_bounds__(1024) item_plan_kernel(int64_t target_warps, const int *list_total, int want,
-                                                         int *item_off) {
+                                                         int *item_off, int *item_warp) {
     __shared__ long long part[1024];
     const int t = threadIdx.x;
     const int64_t per = (target_warps + 1023) / 1024, a0 = min(target_warps, t * per),
@@ -657,7 +653,9 @@ __global__ void __launch_bounds__(1024) item_plan_kernel(int64_t target_warps, c
     long long run = part[t];
     for (int64_t w = a0; w < a1; ++w) {
         item_off[w] = (int)run;
-        run += min(64ll, max(1ll, ((long long)list_total[w] + unit - 1) / unit));
+        const long long k = min(64ll, max(1ll, ((long long)list_total[w] + unit - 1) / unit));
+        for (long long q = 0; q < k; ++q) item_warp[run + q] = (int)w;
+        run += k;
     }
 }
 
@@ -776,7 +774,8 @@ static void launch_pair(unsigned walk_grid, int block, size_t smem, unsigned lis
     if (t_marks) cudaEventRecord(t_marks[0], s);
     if (pop == 2) tree_walk_kernel<PREC, MODEL, 2><<<walk_grid, block, smem, s>>>(args);
     else tree_walk_kernel<PREC, MODEL, 1><<<walk_grid, block, smem, s>>>(args);
-    item_plan_kernel<<<1, 1024, 0, s>>>(target_warps, args.list_total, args.item_want, args.item_off);
+    item_plan_kernel<<<1, 1024, 0, s>>>(target_warps, args.list_total, args.item_want, args.item_off,
+                                        args.item_warp);
     if (t_far_ready) cudaStreamWaitEvent(s, t_far_ready, 0);
     if (t_marks) cudaEventRecord(t_marks[1], s);
     tree_list_kernel<PREC, MODEL><<<list_grid, LIST_WARPS * 32, 0, s>>>(args, target_warps);
@@ -993,9 +992,9 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     int *list_len = scratch.get<int>(slots), *list_total = scratch.get<int>(slots);
     double *walk_u = scratch.get<double>((size_t)3 * n), *partial = scratch.get<double>(capacity * 32 * 3);
     int8_t *walk_flag = scratch.get<int8_t>((size_t)n), *pflag = scratch.get<int8_t>(capacity * 32);
-    int *item_off = scratch.get<int>(slots + 1);
+    int *item_off = scratch.get<int>(slots + 1), *item_warp = scratch.get<int>(capacity);
     if (!list || !list_cost || !unit_chunks || !list_len || !list_total || !walk_u || !partial || !walk_flag || !pflag ||
-        !item_off)
+        !item_off || !item_warp)
         return scratch.status;
     EvalArgs args;
     args.n = n;
@@ -1027,6 +1026,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     args.partial = partial;
     args.pflag = pflag;
     args.item_off = item_off;
+    args.item_warp = item_warp;
     args.item_want = want;
     args.root_of = root_of;
     args.exact = pre ? pre->exact : nullptr;
