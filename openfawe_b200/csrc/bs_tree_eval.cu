@@ -69,6 +69,7 @@ struct EvalArgs {
     // (item_off [target_warps + 1], from item_plan_kernel), and the items' partial sums
     int *item_off;
     int *item_warp;      // [capacity]: the warp of targets of each item
+    int *item_first;     // [capacity]: the first list entry of each item (item_bounds_kernel)
     int item_want;       // items wanted in all (about 96 a SM); the capacity is item_want + target warps
     double *partial;     // [items][32 lanes][3]
     int8_t *pflag;       // [items][32 lanes]
@@ -531,22 +532,14 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
                                           Seg64 *seg64_tile, Seg32 *seg32_tile, long long &near_pairs,
                                           long long &fp64_pairs) {
     const int lane = threadIdx.x & 31;
-    // chunk c is the c-th slice of this warp's list by cost
+    // chunk c is the c-th slice of this warp's list by cost: entries [item_first[item], item_first[item + 1]), the
+    // last slice ending at the list's end
     const int len = a.list_len[gw];
-    const int64_t total = a.list_total[gw];
     const int *chunks_of = a.unit_chunks + gw * LIST_CHUNKS;
     auto at = [&](int k) -> int64_t {  // pool index of the list's k-th entry
         return (int64_t)chunks_of[k / LIST_CHUNK] * LIST_CHUNK + (k & (LIST_CHUNK - 1));
     };
-    auto lower = [&](int64_t v) {  // first entry whose cost start is >= v
-        int l = 0, h = len;
-        while (l < h) {
-            int m = (l + h) >> 1;
-            if (a.list_cost[at(m)] < v) l = m + 1; else h = m;
-        }
-        return l;
-    };
-    const int first = lower(total * c / chunks), last = lower(total * (c + 1) / chunks);
+    const int first = a.item_first[item], last = c + 1 < chunks ? a.item_first[item + 1] : len;
     Target t;
     t.load(a, gw * 32 + lane);
     int64_t e = 0, e1 = 0;
@@ -656,6 +649,36 @@ __global__ void __launch_bounds__(1024) item_plan_kernel(int64_t target_warps, c
         const long long k = min(64ll, max(1ll, ((long long)list_total[w] + unit - 1) / unit));
         for (long long q = 0; q < k; ++q) item_warp[run + q] = (int)w;
         run += k;
+    }
+}
+
+// The first list entry of every work item, one warp per warp of targets, its lanes reading the list's cost starts in
+// order: item c of warp gw (of `chunks`) begins at the first entry whose cost start reaches floor(total c / chunks).
+// The cost starts rise strictly (every entry costs at least 1), so entry k begins the items whose threshold lies in
+// (cost[k - 1], cost[k]], and the items whose threshold lies past the last start are empty (they begin at len).
+__global__ void item_bounds_kernel(EvalArgs a, int64_t target_warps) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (gw >= target_warps) return;
+    const int base = a.item_off[gw], chunks = a.item_off[gw + 1] - base, len = a.list_len[gw];
+    const long long total = a.list_total[gw];
+    const int *chunks_of = a.unit_chunks + gw * LIST_CHUNKS;
+    if (len == 0 || total <= 0) {
+        for (int c = lane; c < chunks; c += 32) a.item_first[base + c] = 0;
+        return;
+    }
+    auto cost = [&](int k) -> long long {
+        return a.list_cost[(int64_t)chunks_of[k / LIST_CHUNK] * LIST_CHUNK + (k & (LIST_CHUNK - 1))];
+    };
+    for (int k = lane; k < len; k += 32) {
+        const long long ck = cost(k), cp = k ? cost(k - 1) : -1;
+        // floor(total c / chunks) > cp  <=>  c >= ceil((cp + 1) chunks / total);
+        // floor(total c / chunks) <= ck <=>  c <= ceil((ck + 1) chunks / total) - 1
+        const long long c0 = ((cp + 1) * chunks + total - 1) / total;
+        const long long c1 = min((long long)chunks - 1, ((ck + 1) * chunks + total - 1) / total - 1);
+        for (long long c = c0; c <= c1; ++c) a.item_first[base + c] = k;
+        if (k == len - 1)
+            for (long long c = max(c0, c1 + 1); c < chunks; ++c) a.item_first[base + c] = len;
     }
 }
 
@@ -776,6 +799,7 @@ static void launch_pair(unsigned walk_grid, int block, size_t smem, unsigned lis
     else tree_walk_kernel<PREC, MODEL, 1><<<walk_grid, block, smem, s>>>(args);
     item_plan_kernel<<<1, 1024, 0, s>>>(target_warps, args.list_total, args.item_want, args.item_off,
                                         args.item_warp);
+    item_bounds_kernel<<<(unsigned)((target_warps * 32 + 255) / 256), 256, 0, s>>>(args, target_warps);
     if (t_far_ready) cudaStreamWaitEvent(s, t_far_ready, 0);
     if (t_marks) cudaEventRecord(t_marks[1], s);
     tree_list_kernel<PREC, MODEL><<<list_grid, LIST_WARPS * 32, 0, s>>>(args, target_warps);
@@ -993,8 +1017,9 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     double *walk_u = scratch.get<double>((size_t)3 * n), *partial = scratch.get<double>(capacity * 32 * 3);
     int8_t *walk_flag = scratch.get<int8_t>((size_t)n), *pflag = scratch.get<int8_t>(capacity * 32);
     int *item_off = scratch.get<int>(slots + 1), *item_warp = scratch.get<int>(capacity);
+    int *item_first = scratch.get<int>(capacity);
     if (!list || !list_cost || !unit_chunks || !list_len || !list_total || !walk_u || !partial || !walk_flag || !pflag ||
-        !item_off || !item_warp)
+        !item_off || !item_warp || !item_first)
         return scratch.status;
     EvalArgs args;
     args.n = n;
@@ -1027,6 +1052,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     args.pflag = pflag;
     args.item_off = item_off;
     args.item_warp = item_warp;
+    args.item_first = item_first;
     args.item_want = want;
     args.root_of = root_of;
     args.exact = pre ? pre->exact : nullptr;
