@@ -653,7 +653,7 @@ def main():
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    times, eval_ms, walk_ms, list_ms, counters = [], [], [], [], []
+    times, eval_ms, walk_ms, list_ms, far_ms, counters = [], [], [], [], [], []
     with Clocks(torch.cuda.current_device()) as clk:
         torch.cuda.synchronize()
         for _ in range(args.steps):
@@ -668,6 +668,7 @@ def main():
             eval_ms.append(s["evaluate_ms"])
             walk_ms.append(s["walk_ms"])
             list_ms.append(s["list_ms"])
+            far_ms.append(s["far_ms"])
             counters.append(s)
         torch.cuda.synchronize()
     if dist:
@@ -684,19 +685,24 @@ def main():
     max_err = float(np.max(np.linalg.norm(u - direct_host, axis=1)) / np.max(np.linalg.norm(direct_host, axis=1)))
     s = counters[-1]
 
-    # roofline of the dominant kernel, the interaction-list kernel (near pairs and far evaluations on the FP32 pipe):
-    # algorithmic flops per launch (W_PAIR per near pair, W_FAR per far evaluation) over its CUDA-event time, against
-    # the FP32 FMA rate measured on this device in this run
+    # roofline of the dominant kernel, the near-leaf list kernel (near pairs on the FP32 pipe): algorithmic flops per
+    # launch (W_PAIR per near pair) over its CUDA-event time, against the FP32 FMA rate measured on this device in
+    # this run; the far-node list kernel (W_FAR per far evaluation) beside it
     kernel_ms = float(np.mean(list_ms))
-    flops = W_PAIR * s["near_pairs"] + W_FAR[args.order] * s["far_evaluations"]
+    far_kernel_ms = float(np.mean(far_ms))
+    flops = W_PAIR * s["near_pairs"]
+    far_flops = W_FAR[args.order] * s["far_evaluations"]
     achieved = flops / (kernel_ms * 1e-3) / 1e12
     from openfawe_b200 import _lib
     peak_t = ctypes.c_double(0.0)
     _lib.check(_lib.library().bs_fp32_peak(_lib.context(device), ctypes.byref(peak_t)), "bs_fp32_peak")
     peak = float(peak_t.value)
     roofline = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": LIST_TRAFFIC, "kernel": f"tree_list_kernel<mixed, Lamb-Oseen>", "kernel_ms": kernel_ms,
-                "flops_per_launch": flops,
+                "traffic": LIST_TRAFFIC, "kernel": "tree_list_kernel<mixed, Lamb-Oseen, near leaves>",
+                "kernel_ms": kernel_ms, "flops_per_launch": flops,
+                "far_kernel": {"kernel": "tree_list_kernel<mixed, Lamb-Oseen, far nodes>", "kernel_ms": far_kernel_ms,
+                               "flops_per_launch": far_flops,
+                               "achieved": far_flops / (far_kernel_ms * 1e-3) / 1e12 if far_kernel_ms > 0 else None},
                 "peak_note": "FP32 FMA throughput measured in this run (bs_fp32_peak); the pair and far-field "
                              "arithmetic runs on the FP32 pipe, neither HBM- nor tensor-core-bound"}
 
@@ -772,7 +778,7 @@ def main():
             "fp64_direct_ms": fp64_ms, "speedup_vs_fp64_direct": fp64_ms / ms,
             "stages": {"build_ms": s["build_ms"], "moments_ms": s["moments_ms"],
                        "evaluate_ms": float(np.mean(eval_ms)), "walk_ms": float(np.mean(walk_ms)),
-                       "list_ms": kernel_ms,
+                       "list_ms": kernel_ms, "far_ms": far_kernel_ms,
                        "nodes": s["nodes"], "near_pairs": s["near_pairs"], "far_evaluations": s["far_evaluations"],
                        "fp64_pairs": s["fp64_pairs"], "visits": s["visits"]},
             "interactions_per_s": {"executed": (s["near_pairs"] + s["far_evaluations"]) / (ms * 1e-3),

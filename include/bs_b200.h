@@ -83,8 +83,9 @@ typedef struct {
     int64_t far_evaluations, near_pairs, fp64_pairs, visits; /* counters of the last tree evaluation */
     double build_ms, moments_ms, evaluate_ms;                /* device time of the last build / evaluation */
     int64_t pair_slots;  /* lane slots spent in leaf walks (32 per warp-pair); near_pairs / pair_slots = SIMT use */
-    double walk_ms, list_ms; /* device time of the traversal and interaction-list kernels of the last tree evaluation */
+    double walk_ms, list_ms; /* device time of the traversal and of the near-leaf list kernel of the last tree evaluation */
     double upload_ms, download_ms; /* host time of the last bs_tree_sum_host's uploads and of its result read-back */
+    double far_ms;       /* device time of the far-node list kernel of the last tree evaluation */
 } bs_stats;
 
 /* Context: one per device.  bs_init makes `device` current, probes it with a one-thread kernel (the reference's

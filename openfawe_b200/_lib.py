@@ -41,7 +41,7 @@ class Stats(ctypes.Structure):
                 ("far_evaluations", _i64), ("near_pairs", _i64), ("fp64_pairs", _i64), ("visits", _i64),
                 ("build_ms", ctypes.c_double), ("moments_ms", ctypes.c_double), ("evaluate_ms", ctypes.c_double),
                 ("pair_slots", _i64), ("walk_ms", ctypes.c_double), ("list_ms", ctypes.c_double),
-                ("upload_ms", ctypes.c_double), ("download_ms", ctypes.c_double)]
+                ("upload_ms", ctypes.c_double), ("download_ms", ctypes.c_double), ("far_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -129,6 +129,15 @@ struct __align__(16) Seg32x2 {
     float4 g[8];
 };
 
+// Two consecutive segments (tree order) of one leaf for the clear-leaf packed pair (96 bytes), in physical units
+// relative to the leaf's centre O, each field a float2 of the two segments' values, at float offset 2f: 0-2 O - s
+// (the start, relative and negated), 3 Gamma/(4 pi), 4-6 l = L d, 7 1/(L rc)^2 (+inf without a core), 8-10 -l,
+// 11 zero.  Only pairs that lie inside one leaf are read (a pair across two leaves holds halves of different
+// centres).
+struct __align__(16) Seg32c2 {
+    float4 g[6];
+};
+
 // Traversal record of one node (64 bytes).
 struct __align__(16) NodeRec {
     double cx, cy, cz, bound;
@@ -430,6 +439,66 @@ __device__ __forceinline__ unsigned pair32x2(float2 txh, float2 tyh, float2 tzh,
     u1 = fma2(coefficient, cy, u1);
     u2 = fma2(coefficient, cz, u2);
     return (n0 ? 1u : 0u) | (n1 ? 2u : 0u);
+}
+
+// 2^x from the special-function unit (ex2.approx, flushing subnormal results to zero); e^-y = 2^(-y log2 e).
+__device__ __forceinline__ float exp2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// -LAMB_A log2(e): the Lamb-Oseen exponent for exp2_approx.
+static constexpr float LAMB_A_LOG2E_NEG = (float)(-LAMB_A * 1.4426950408889634);
+
+// The pair of two segments of a leaf (a Seg32c2 record) for a target `clear` of the leaf: at least 1.5 times its
+// bounding radius from its centre (every segment is then seen under less than 84 degrees, so r1.r2 >= 0.1 |r1||r2|
+// and |r1||r2| + r1.r2 has no cancellation), outside the reach of the core test (no pair needs FP64 for its core) and
+// within the FP32 range the caller checks (1e-8 < |x - O| < 1e9, bound < 1e9, so that |r1|^4 stays a normal float).
+// (tx, ty, tz) is x - O in FP32, broadcast in both halves.  In physical units, r1 = x - s, r2 = r1 - l and
+// c = l x r1 (= r1 x r2):
+//   u = Gamma/(4 pi) factor (|r1| + |r2|) / (|r1| |r2| (|r1| |r2| + r1.r2)) c,
+// the reference's pair (vortex_numba.pair_velocity) with numerator and denominator multiplied by L^3, the core
+// factor from (h / rc)^2 = |c|^2 / (L rc)^2.  No pair of a clear target needs FP64: none lies on its segment, and
+// the leaf-relative FP32 offsets carry at most about 3 ulp of |r1|, as the two-float path's rounded difference does.
+// MODEL 0..2.  Adds the two segments' velocities to the float2 sums (one half each).
+template <int MODEL>
+__device__ __forceinline__ void pair32x2_clear(float2 tx, float2 ty, float2 tz, const float4 *rec, float2 &u0,
+                                               float2 &u1, float2 &u2) {
+    static_assert(MODEL >= 0 && MODEL <= 2, "clear packed pairs for the models without a per-pair special form");
+    const float4 g0 = rec[0], g1 = rec[1], g2 = rec[2], g3 = rec[3], g4 = rec[4], g5 = rec[5];
+    const float2 r1x = add2(tx, make_float2(g0.x, g0.y)), r1y = add2(ty, make_float2(g0.z, g0.w));
+    const float2 r1z = add2(tz, make_float2(g1.x, g1.y)), gf = make_float2(g1.z, g1.w);
+    const float2 lx = make_float2(g2.x, g2.y), ly = make_float2(g2.z, g2.w), lz = make_float2(g3.x, g3.y);
+    const float2 w = make_float2(g3.z, g3.w);
+    const float2 nlx = make_float2(g4.x, g4.y), nly = make_float2(g4.z, g4.w), nlz = make_float2(g5.x, g5.y);
+    const float2 r2x = add2(r1x, nlx), r2y = add2(r1y, nly), r2z = add2(r1z, nlz);
+    const float2 cx = fma2(ly, r1z, mul2(nlz, r1y));
+    const float2 cy = fma2(lz, r1x, mul2(nlx, r1z));
+    const float2 cz = fma2(lx, r1y, mul2(nly, r1x));
+    const float2 h2 = fma2(cx, cx, fma2(cy, cy, mul2(cz, cz)));
+    const float2 n12 = fma2(r1x, r1x, fma2(r1y, r1y, mul2(r1z, r1z)));
+    const float2 n22 = fma2(r2x, r2x, fma2(r2y, r2y, mul2(r2z, r2z)));
+    const float2 dot = fma2(r1x, r2x, fma2(r1y, r2y, mul2(r1z, r2z)));
+    const float2 n1 = mul2(n12, make_float2(rsqrtf(n12.x), rsqrtf(n12.y)));
+    const float2 n2 = mul2(n22, make_float2(rsqrtf(n22.x), rsqrtf(n22.y)));
+    const float2 product = mul2(n1, n2);
+    const float2 den = mul2(product, add2(product, dot));
+    float2 k = mul2(gf, add2(n1, n2));
+    if (MODEL == 1) {  // Rankine: min((h / rc)^2, 1); +inf (no core) and NaN (h = 0 without a core) give 1
+        const float2 r2 = mul2(h2, w);
+        k = mul2(k, make_float2(fminf(r2.x, 1.0f), fminf(r2.y, 1.0f)));
+    } else if (MODEL == 2) {  // Lamb-Oseen inside its cut-off: 1 - exp(-1.25643 (h / rc)^2)
+        const float2 r2 = mul2(h2, w);
+        const float2 x = mul2(r2, make_float2(LAMB_A_LOG2E_NEG, LAMB_A_LOG2E_NEG));
+        const float2 f = fma2(make_float2(exp2_approx(x.x), exp2_approx(x.y)), make_float2(-1.0f, -1.0f),
+                              make_float2(1.0f, 1.0f));
+        k = mul2(k, make_float2(r2.x < (float)LAMB_CUT2 ? f.x : 1.0f, r2.y < (float)LAMB_CUT2 ? f.y : 1.0f));
+    }
+    const float2 coefficient = mul2(k, make_float2(__fdividef(1.0f, den.x), __fdividef(1.0f, den.y)));
+    u0 = fma2(coefficient, cx, u0);
+    u1 = fma2(coefficient, cy, u1);
+    u2 = fma2(coefficient, cz, u2);
 }
 
 // The fourth-order term of the expansion, R = x - c:

@@ -44,6 +44,7 @@ struct bs_tree {
     bs::Seg64 *seg64 = nullptr;  // tree order
     bs::Seg32 *seg32 = nullptr;  // tree order
     bs::Seg32x2 *seg32x2 = nullptr;  // tree order, consecutive pairs
+    bs::Seg32c2 *seg32c2 = nullptr;  // tree order, consecutive pairs relative to their leaf's centre
     uint64_t *keys = nullptr;    // Morton keys (input order), Morton trees only
     int32_t *wake_root = nullptr;  // forests: root node of each wake (-1 for a wake without segments)
     int nwakes = 0;

@@ -830,6 +830,7 @@ extern "C" int bs_tree_adjoint(bs_ctx *ctx, const bs_sources *src, const bs_tree
             ctx->stats.build_ms = lists_ms;  // build, walk and transposition
             ctx->stats.walk_ms = near_ms;    // near pairs
             ctx->stats.list_ms = far_ms;     // far entries
+            ctx->stats.far_ms = 0.0;
             ctx->stats.moments_ms = seg_ms;  // push-down, segment moments, scatter
         }
     }

@@ -1734,6 +1734,42 @@ __global__ void node_rec_kernel(int64_t count, const unsigned long long *bound2,
     nodes[j] = node_record(j, b, centre, core, lo, hi, left, right);
 }
 
+// The clear-leaf pair records (Seg32c2) of every leaf, one warp per node (internal nodes return): each segment of
+// leaf j relative to the leaf's centre, from its FP64 record (start, L, d, (Gamma/L)/(4 pi), rc).
+__global__ void clear_pairs_kernel(int64_t count, const int64_t *lo, const int64_t *hi, const int64_t *left,
+                                   const double *centre, const Seg64 *seg64, Seg32c2 *out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (j >= count || left[j] >= 0) return;
+    const double ox = centre[3 * j], oy = centre[3 * j + 1], oz = centre[3 * j + 2];
+    for (int64_t k = lo[j] + lane; k < hi[j]; k += 32) {
+        const Seg64 q = seg64[k];
+        float v[12];
+        v[0] = (float)(ox - q.sx);
+        v[1] = (float)(oy - q.sy);
+        v[2] = (float)(oz - q.sz);
+        v[3] = (float)(q.gfac * q.len);  // Gamma / (4 pi)
+        v[4] = (float)(q.dx * q.len);
+        v[5] = (float)(q.dy * q.len);
+        v[6] = (float)(q.dz * q.len);
+        const double lrc = q.len * q.radius;
+        v[7] = q.radius > 0.0 ? (float)(1.0 / (lrc * lrc)) : __int_as_float(0x7f800000);
+        v[8] = -v[4];
+        v[9] = -v[5];
+        v[10] = -v[6];
+        v[11] = 0.0f;
+        float *half = reinterpret_cast<float *>(out + (k >> 1)) + (k & 1);
+        for (int f = 0; f < 12; ++f) half[2 * f] = v[f];
+    }
+}
+
+// Trees without segment records (bs_node_quantities: node quantities only) have none to write.
+static void clear_pairs(const bs_tree *t, cudaStream_t s) {
+    if (!t->seg64 || !t->seg32c2) return;
+    clear_pairs_kernel<<<blocks_for(t->count * 32, 256), 256, 0, s>>>(t->count, t->lo, t->hi, t->left, t->centre,
+                                                                     t->seg64, t->seg32c2);
+}
+
 // Every node's export arrays and far records from its sums (read in place); for fourth- and fifth-order trees
 // blockIdx.y picks the part (0: orders 0-3, 1-3: the order-4 and order-5 rows of one component).
 template <int PARTS>
@@ -1823,6 +1859,7 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
                       t->far64y, t->far32y, t->far64z, t->far32z};
     // one warp per block: the thread per node is long, so the nodes spread over every SM
     node_final_kernel<PARTS><<<dim3(blocks_for(count, 32), PARTS >= MOM_PARTS4 ? 4 : 1), 32, 0, ms>>>(count, sums, out);
+    clear_pairs(t, ms);  // the segment records were packed on this stream, the centres are known
     BS_CHECK_LAUNCH("bottom-up moments");
     bound_up_kernel<<<leaf_blocks, 128, 0, s>>>(leaves, nleaves, t->lo, t->hi, parent, ends, t->centre, anc_list,
                                                  bound2);
@@ -1903,6 +1940,7 @@ int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_
         moment_sum_kernel<MOM_PARTS><<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, t->centre, sums);
         moment_final_kernel<MOM_PARTS><<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, sums, out);
     }
+    clear_pairs(t, s);
     BS_CHECK_LAUNCH("moments");
     return BS_OK;
 }
@@ -1920,7 +1958,8 @@ static int finish_tree(bs_tree *t, const bs_sources *src, const SegGeo *geo, Scr
     t->seg64 = t->alloc<Seg64>(m, s);
     t->seg32 = t->alloc<Seg32>(m, s);
     t->seg32x2 = t->alloc<Seg32x2>((m + 1) / 2, s);
-    if (!t->order || !t->inverse || !t->seg64 || !t->seg32 || !t->seg32x2) return BS_ERR_OOM;
+    t->seg32c2 = t->alloc<Seg32c2>((m + 1) / 2, s);
+    if (!t->order || !t->inverse || !t->seg64 || !t->seg32 || !t->seg32x2 || !t->seg32c2) return BS_ERR_OOM;
     widen_order_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, t->order32, t->order, t->inverse);
     BS_CHECK_LAUNCH("widen_order_kernel");
     // with a side stream (bottom-up trees of a tree sum) the segment records are packed there, beside the node

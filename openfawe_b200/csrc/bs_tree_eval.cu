@@ -23,6 +23,7 @@ namespace bs {
 constexpr int STACK_DEPTH = 128;
 constexpr int FAR_COST = 16;              // list cost units: one far evaluation ~ sixteen near pairs (measured)
 constexpr int LIST_WARPS = 4;             // warps per block of the list kernel
+constexpr int FAR_GROUPS = 4;             // open groups of disjoint far entries in the far list kernel
 
 struct TreeView {
     const NodeRec *nodes;
@@ -37,6 +38,7 @@ struct TreeView {
     const Seg64 *seg64;
     const Seg32 *seg32;
     const Seg32x2 *seg32x2;
+    const Seg32c2 *seg32c2;
 };
 
 struct EvalArgs {
@@ -71,7 +73,8 @@ struct EvalArgs {
     int *item_warp;      // [capacity]: the warp of targets of each item
     int *item_first;     // [capacity]: the first list entry of each item (item_bounds_kernel)
     int item_want;       // items wanted in all (about 96 a SM); the capacity is item_want + target warps
-    double *partial;     // [items][32 lanes][3]
+    double *partial;     // [items][32 lanes][3]: the near leaves of each item (tree_list_kernel<.., 0>)
+    double *partial_far; // [items][32 lanes][3]: the far nodes of each item (tree_list_kernel<.., 1>)
     int8_t *pflag;       // [items][32 lanes]
     const int32_t *root_of;       // forests: root node of each (sorted) target's wake, -1 for none; null: node 0
     unsigned long long *queue;    // work counter of the persistent list kernel
@@ -168,20 +171,23 @@ __device__ __forceinline__ void single_pair(const EvalArgs &a, const Target &t, 
 }
 
 // One leaf of a single-precision evaluation with MODEL 0..2, two segments per operation: the leaf's whole pairs of
-// consecutive segments [2 p0, 2 p1) are staged 16 pairs (32 segments) at a time as Seg32x2 records, and a walking lane
-// evaluates a tile with pair32x2 when none of its segments is excluded for it (otherwise, and for targets the packed
-// pair does not take, segment by segment with pair32); the odd ends of the leaf go through pair32.  Exclusions are
-// consumed in position order through the lane's cursor e.
+// consecutive segments [2 p0, 2 p1) are staged a tile at a time, and a walking lane evaluates a tile
+// two segments per operation when none of its segments is excluded for it (otherwise, and for targets the packed
+// pair does not take, segment by segment with pair32); the odd ends of the leaf go through pair32.  When every
+// walking lane is clear of the leaf (`wide`: see pair32x2_clear) the tiles are 32 Seg32c2 records and the pairs
+// pair32x2_clear, from the lane's offset `rel` to the leaf's centre; otherwise 16 Seg32x2 records and pair32x2.
+// Exclusions are consumed in position order through the lane's cursor e.
 template <int PREC, int MODEL>
 __device__ __forceinline__ void leaf_pairs_packed(const EvalArgs &a, const Target &t, int lo, int hi, bool walk,
-                                                  bool all_clear, int64_t &e, int64_t e1, float4 *tile,
-                                                  Acc<PREC> &acc, int &flag, long long &near_pairs,
+                                                  bool all_clear, bool wide, float3 rel, int64_t &e, int64_t e1,
+                                                  float4 *tile, Acc<PREC> &acc, int &flag, long long &near_pairs,
                                                   long long &fp64_pairs) {
     const int lane = threadIdx.x & 31;
     float t0 = 0.f, t1 = 0.f, t2 = 0.f;
     float2 u0 = make_float2(0.f, 0.f), u1 = u0, u2 = u0;
     const float2 txh = make_float2(t.xh0, t.xh0), tyh = make_float2(t.xh1, t.xh1), tzh = make_float2(t.xh2, t.xh2);
     const float2 txl = make_float2(t.xl0, t.xl0), tyl = make_float2(t.xl1, t.xl1), tzl = make_float2(t.xl2, t.xl2);
+    const float2 rx = make_float2(rel.x, rel.x), ry = make_float2(rel.y, rel.y), rz = make_float2(rel.z, rel.z);
     // an excluded segment at position s: consume it and report
     auto excluded = [&](int s) -> bool {
         while (e < e1 && a.ex_pos[e] < s) ++e;
@@ -198,7 +204,36 @@ __device__ __forceinline__ void leaf_pairs_packed(const EvalArgs &a, const Targe
             single_pair<PREC, MODEL>(a, t, lo, t0, t1, t2, acc, flag, fp64_pairs);
         }
     }
-    for (int pb = p0; pb < p1; pb += 16) {
+    // clear leaves: tiles of 32 Seg32c2 records (the warp's 3 KB), 64 segments
+    for (int pb = p0; wide && pb < p1; pb += 32) {
+        const int np = min(32, p1 - pb), base = 2 * pb, cnt = 2 * np;
+        __syncwarp();
+        const float4 *src = reinterpret_cast<const float4 *>(a.tv.seg32c2 + pb);
+        for (int i = lane; i < 6 * np; i += 32) tile[i] = __ldg(src + i);
+        __syncwarp();
+        if (!walk) continue;
+        unsigned long long excl = 0;
+        while (e < e1 && a.ex_pos[e] < base + cnt) excl |= 1ull << (a.ex_pos[e++] - base);
+        near_pairs += cnt - __popcll(excl);
+        if (excl == 0 && t.packed) {
+#pragma unroll 4
+            for (int q = 0; q < np; ++q) pair32x2_clear<MODEL>(rx, ry, rz, tile + 6 * q, u0, u1, u2);
+        } else {
+            unsigned long long need = 0;
+            for (int j = 0; j < cnt; ++j) {
+                if ((excl >> j) & 1ull) continue;
+                const Seg32 r = a.tv.seg32[base + j];
+                const float q0 = (t.xh0 - r.hi.x) + (t.xl0 - r.lo.x);
+                const float q1 = (t.xh1 - r.hi.y) + (t.xl1 - r.lo.y);
+                const float q2 = (t.xh2 - r.hi.z) + (t.xl2 - r.lo.z);
+                if (pair32<MODEL>(q0, q1, q2, r.hi, r.lo, r.dir, a.near2, t0, t1, t2)) need |= 1ull << j;
+            }
+            fp64_pairs += __popcll(need);
+            pairs_in_fp64<PREC, MODEL>(a, t, base, (unsigned)need, acc, flag);
+            pairs_in_fp64<PREC, MODEL>(a, t, base + 32, (unsigned)(need >> 32), acc, flag);
+        }
+    }
+    for (int pb = p0; !wide && pb < p1; pb += 16) {
         const int np = min(16, p1 - pb), base = 2 * pb, cnt = 2 * np;
         __syncwarp();
         const float4 *src = reinterpret_cast<const float4 *>(a.tv.seg32x2 + pb);
@@ -254,18 +289,24 @@ __device__ __forceinline__ void leaf_pairs(const EvalArgs &a, const Target &t, c
     if (walk) while (e < e1 && a.ex_pos[e] < lo) ++e;
     float t0 = 0.f, t1 = 0.f, t2 = 0.f;
     // When every walking lane is farther from the leaf's bounding sphere than sqrt(near2) of its largest core radius
-    // (with a 1% margin for rounding), no pair of the leaf can need FP64 for its core: the pairs skip that test.
-    bool clear = true;
-    if (PREC != 0 && MODEL != 0 && walk) {
+    // (with a 1% margin for rounding), no pair of the leaf can need FP64 for its core: the pairs skip that test.  When
+    // moreover every walking lane lies at least 1.5 bounding radii from the leaf's centre (within FP32's range),
+    // the packed pairs take the clear-leaf form (pair32x2_clear).
+    bool clear = true, wide = true;
+    float3 rel = make_float3(0.f, 0.f, 0.f);
+    if (PREC != 0 && walk) {
         const double rx = t.x0 - nr.cx, ry = t.x1 - nr.cy, rz = t.x2 - nr.cz;
-        const double gap = sqrt(rx * rx + ry * ry + rz * rz) - nr.bound;
-        clear = gap > 1.01 * sqrt((double)a.near2) * nr.clear_core;
+        const double r2 = rx * rx + ry * ry + rz * rz;
+        if (MODEL != 0) clear = sqrt(r2) - nr.bound > 1.01 * sqrt((double)a.near2) * nr.clear_core;
+        wide = clear && r2 >= 2.25 * nr.bound * nr.bound && r2 > 1e-16 && r2 < 1e18 && nr.bound < 1e9;
+        rel = make_float3((float)rx, (float)ry, (float)rz);
     }
     const bool all_clear = __all_sync(0xffffffffu, clear);
     if constexpr (PREC != 0 && MODEL <= 2) {
-        // the warp's tile space is sized for 32 Seg64 (3 KB): 16 Seg32x2 (2 KB) fit
-        leaf_pairs_packed<PREC, MODEL>(a, t, lo, hi, walk, all_clear, e, e1, reinterpret_cast<float4 *>(seg64_tile),
-                                       acc, flag, near_pairs, fp64_pairs);
+        // the warp's tile space is sized for 32 Seg64 (3 KB): 16 Seg32x2 (2 KB) or 32 Seg32c2 (3 KB) fit
+        const bool all_wide = __all_sync(0xffffffffu, wide);
+        leaf_pairs_packed<PREC, MODEL>(a, t, lo, hi, walk, all_clear, all_wide, rel, e, e1,
+                                       reinterpret_cast<float4 *>(seg64_tile), acc, flag, near_pairs, fp64_pairs);
     } else {
         for (int base = lo; base < hi; base += 32) {
             const int cnt = min(32, hi - base);
@@ -343,6 +384,34 @@ __device__ __forceinline__ void leaf_pairs(const EvalArgs &a, const Target &t, c
         }
         if (walk && PREC != 0) acc.add32(t0, t1, t2);
     }
+}
+
+// The walk's own evaluations of what does not fit in its list (rare): out of line, with their inputs by value, so
+// that the traversal loop keeps the code and registers of the walk alone.
+struct LeafSum {
+    double u0, u1, u2;
+    long long near_pairs, fp64_pairs;
+    int flag;
+};
+
+template <int PREC, int MODEL>
+__device__ __noinline__ LeafSum walk_leaf(const EvalArgs a, const Target t, const NodeRec nr, bool walk, int64_t e,
+                                         int64_t e1, Seg64 *seg64_tile, Seg32 *seg32_tile) {
+    Acc<PREC> acc;
+    LeafSum r{};
+    r.flag = BS_FLAG_OK;
+    leaf_pairs<PREC, MODEL>(a, t, nr, walk, e, e1, seg64_tile, seg32_tile, acc, r.flag, r.near_pairs, r.fp64_pairs);
+    r.u0 = acc.x();
+    r.u1 = acc.y();
+    r.u2 = acc.z();
+    return r;
+}
+
+template <int PREC>
+__device__ __noinline__ double3 walk_far(const EvalArgs a, const Target t, int node) {
+    Acc<PREC> acc;
+    far_node<PREC>(a, t, node, acc);
+    return make_double3(acc.x(), acc.y(), acc.z());
 }
 
 // Phase 1: the traversal.  Each warp walks the tree once for its 32 targets and writes an interaction list: far
@@ -444,8 +513,12 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
                 running += FAR_COST;
             } else if (mine && accept) {
                 // far records still being computed: evaluated again by the host once they are complete
-                if (a.deferred) atomicOr(a.overflow + 1, 1);
-                else far_node<PREC>(a, t, node, acc);
+                if (a.deferred) {
+                    atomicOr(a.overflow + 1, 1);
+                } else {
+                    const double3 v = walk_far<PREC>(a, t, node);
+                    acc.add64(v.x, v.y, v.z);
+                }
             }
         }
         if (openm) {
@@ -462,9 +535,11 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
                 } else if (a.deferred) {  // segment records still being written: evaluated again by the host
                     if (mine && !accept) atomicOr(a.overflow + 1, 1);
                 } else {
-                    int64_t ec = e;
-                    leaf_pairs<PREC, MODEL>(a, t, nr, mine && !accept, ec, e1, seg64_tile, seg32_tile, acc, flag,
-                                            near_pairs, fp64_pairs);
+                    const LeafSum r = walk_leaf<PREC, MODEL>(a, t, nr, mine && !accept, e, e1, seg64_tile, seg32_tile);
+                    acc.add64(r.u0, r.u1, r.u2);
+                    near_pairs += r.near_pairs;
+                    fp64_pairs += r.fp64_pairs;
+                    if (flag == BS_FLAG_OK) flag = r.flag;
                 }
             } else {
                 if (top + 2 > a.stack_limit) {
@@ -523,11 +598,11 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
     }
 }
 
-// Phase 2: a persistent kernel.  Work items are (warp of targets, chunk) pairs, chunk c holding the c-th slice (by
-// cost) of that warp's list; each warp of the kernel takes items from a device counter until none is left and
-// evaluates the item's far nodes and near leaves.  Partial sums per (chunk, target) are combined in chunk order by the
-// reduce kernel.
-template <int PREC, int MODEL>
+// Phase 2: two persistent kernels over the same work items, (warp of targets, chunk) pairs, chunk c holding the c-th
+// slice (by cost) of that warp's list; each warp of a kernel takes items from its own device counter until none is
+// left.  PART 0 evaluates the item's near leaves, PART 1 its far nodes (apart, each kernel holds only its own code and
+// registers).  Partial sums per (chunk, target) are combined in chunk order by the reduce kernel.
+template <int PREC, int MODEL, int PART>
 __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, int chunks, int64_t item,
                                           Seg64 *seg64_tile, Seg32 *seg32_tile, long long &near_pairs,
                                           long long &fp64_pairs) {
@@ -546,44 +621,93 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
     if (t.valid && a.ex_ptr) { e = a.ex_ptr[t.p]; e1 = a.ex_ptr[t.p + 1]; }
     Acc<PREC> acc;
     int flag = BS_FLAG_OK;
-    // Far entries whose lane masks do not overlap are evaluated together, each lane at its own node: a far entry
-    // holds about a third of the warp's lanes, and a group of disjoint ones fills the warp (their records are a few
-    // distinct addresses a load).  The group is evaluated when an entry overlaps it and at the end.
-    int my_far = -1;
-    unsigned group = 0;
-    auto flush = [&]() {
-        if (my_far >= 0) far_node<PREC>(a, t, my_far, acc);
-        my_far = -1;
-        group = 0;
-    };
-    for (int k = first; k < last; ++k) {
-        const int2 entry = a.list[at(k)];
-        const bool mine = ((unsigned)entry.y >> lane) & 1u;
-        if (entry.x & FAR_BIT) {
-            if (group & (unsigned)entry.y) flush();
-            group |= (unsigned)entry.y;
-            if (mine) my_far = entry.x & ~FAR_BIT;
-        } else {
+    if constexpr (PART == 0) {
+        for (int k = first; k < last; ++k) {
+            const int2 entry = a.list[at(k)];
+            if (entry.x & FAR_BIT) continue;
+            const bool mine = ((unsigned)entry.y >> lane) & 1u;
             const NodeRec nr = a.tv.nodes[entry.x];
             int64_t ec = e;  // list entries are not in position order: each leaf scans the exclusions from the start
             leaf_pairs<PREC, MODEL>(a, t, nr, mine, ec, e1, seg64_tile, seg32_tile, acc, flag, near_pairs,
                                     fp64_pairs);
         }
+    } else {
+        // Far entries are packed first-fit into FAR_GROUPS open groups of disjoint lane masks, each lane of a group at
+        // its own node; a group is evaluated (every lane at its node at once) when an entry fits none -- the fullest
+        // group goes -- and, one by one, at the end.  A far entry holds about a third of the warp's lanes, so a group
+        // fills the warp from a few entries, and a load of its records touches a few distinct addresses.  One call
+        // site evaluates every group.
+        int my_far[FAR_GROUPS];
+        unsigned group[FAR_GROUPS];
+#pragma unroll
+        for (int q = 0; q < FAR_GROUPS; ++q) {
+            my_far[q] = -1;
+            group[q] = 0u;
+        }
+        int k = first;
+        for (;;) {
+            int go = -1;  // the group to evaluate next
+            while (k < last) {
+                const int2 entry = a.list[at(k)];
+                if (!(entry.x & FAR_BIT)) {
+                    ++k;
+                    continue;
+                }
+                const unsigned m = (unsigned)entry.y;
+                int fit = -1;
+#pragma unroll
+                for (int q = 0; q < FAR_GROUPS; ++q)
+                    if (fit < 0 && !(group[q] & m)) fit = q;
+                if (fit < 0) {
+                    int most = -1;
+#pragma unroll
+                    for (int q = 0; q < FAR_GROUPS; ++q)
+                        if (__popc(group[q]) > most) {
+                            most = __popc(group[q]);
+                            go = q;
+                        }
+                    break;
+                }
+#pragma unroll
+                for (int q = 0; q < FAR_GROUPS; ++q)
+                    if (q == fit) {
+                        group[q] |= m;
+                        if ((m >> lane) & 1u) my_far[q] = entry.x & ~FAR_BIT;
+                    }
+                ++k;
+            }
+            if (go < 0) {  // the list is done: the groups that hold entries, one by one
+#pragma unroll
+                for (int q = 0; q < FAR_GROUPS; ++q)
+                    if (go < 0 && group[q]) go = q;
+                if (go < 0) break;
+            }
+            int node = -1;
+#pragma unroll
+            for (int q = 0; q < FAR_GROUPS; ++q)
+                if (q == go) {
+                    node = my_far[q];
+                    my_far[q] = -1;
+                    group[q] = 0u;
+                }
+            if (node >= 0) far_node<PREC>(a, t, node, acc);
+        }
     }
-    flush();
     if (t.valid) {
         const int64_t o = item * 32 + lane;
-        a.partial[3 * o] = acc.x();
-        a.partial[3 * o + 1] = acc.y();
-        a.partial[3 * o + 2] = acc.z();
-        a.pflag[o] = (int8_t)flag;
+        double *dst = PART == 0 ? a.partial : a.partial_far;
+        dst[3 * o] = acc.x();
+        dst[3 * o + 1] = acc.y();
+        dst[3 * o + 2] = acc.z();
+        if (PART == 0) a.pflag[o] = (int8_t)flag;
     }
 }
 
 // Three blocks per SM (up to 168 registers a thread): the packed pairs of a tile need the registers to interleave.
-template <int PREC, int MODEL>
+// PART 0: near leaves (counter a.queue[0]); PART 1: far nodes (counter a.queue[2]; no tiles).
+template <int PREC, int MODEL, int PART>
 __global__ void __launch_bounds__(LIST_WARPS * 32, 3) tree_list_kernel(EvalArgs a, int64_t target_warps) {
-    __shared__ __align__(16) unsigned char tile_mem[LIST_WARPS * 32 * sizeof(Seg64)];
+    __shared__ __align__(16) unsigned char tile_mem[PART == 0 ? LIST_WARPS * 32 * sizeof(Seg64) : 16];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Seg64 *seg64_tile = reinterpret_cast<Seg64 *>(tile_mem) + warp * 32;
     Seg32 *seg32_tile = reinterpret_cast<Seg32 *>(tile_mem) + warp * 32;
@@ -591,21 +715,23 @@ __global__ void __launch_bounds__(LIST_WARPS * 32, 3) tree_list_kernel(EvalArgs 
     long long near_pairs = 0, fp64_pairs = 0;
     for (;;) {
         unsigned long long item = 0;
-        if (lane == 0) item = atomicAdd(a.queue, 1ull);
+        if (lane == 0) item = atomicAdd(a.queue + (PART == 0 ? 0 : 2), 1ull);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= items) break;
         const int64_t lo = a.item_warp[item];  // the warp of targets whose list this item slices
         const int first = a.item_off[lo];
-        list_item<PREC, MODEL>(a, lo, (int)(item - first), a.item_off[lo + 1] - first, (int64_t)item, seg64_tile,
-                               seg32_tile, near_pairs, fp64_pairs);
+        list_item<PREC, MODEL, PART>(a, lo, (int)(item - first), a.item_off[lo + 1] - first, (int64_t)item,
+                                     seg64_tile, seg32_tile, near_pairs, fp64_pairs);
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        near_pairs += __shfl_xor_sync(0xffffffffu, near_pairs, o);
-        fp64_pairs += __shfl_xor_sync(0xffffffffu, fp64_pairs, o);
-    }
-    if (lane == 0) {
-        atomicAdd(&a.counters[1], (unsigned long long)near_pairs);
-        atomicAdd(&a.counters[2], (unsigned long long)fp64_pairs);
+    if constexpr (PART == 0) {
+        for (int o = 16; o > 0; o >>= 1) {
+            near_pairs += __shfl_xor_sync(0xffffffffu, near_pairs, o);
+            fp64_pairs += __shfl_xor_sync(0xffffffffu, fp64_pairs, o);
+        }
+        if (lane == 0) {
+            atomicAdd(&a.counters[1], (unsigned long long)near_pairs);
+            atomicAdd(&a.counters[2], (unsigned long long)fp64_pairs);
+        }
     }
 }
 
@@ -694,6 +820,7 @@ __global__ void tree_reduce_kernel(EvalArgs a, double *out, int8_t *flags) {
     for (int item = a.item_off[gw]; item < a.item_off[gw + 1]; ++item) {
         const int64_t o = (int64_t)item * 32 + lane;
         acc.add64(a.partial[3 * o], a.partial[3 * o + 1], a.partial[3 * o + 2]);
+        acc.add64(a.partial_far[3 * o], a.partial_far[3 * o + 1], a.partial_far[3 * o + 2]);
         if (flag == BS_FLAG_OK) flag = a.pflag[o];
     }
     acc.add64(a.walk_u[3 * p], a.walk_u[3 * p + 1], a.walk_u[3 * p + 2]);
@@ -802,8 +929,10 @@ static void launch_pair(unsigned walk_grid, int block, size_t smem, unsigned lis
     item_bounds_kernel<<<(unsigned)((target_warps * 32 + 255) / 256), 256, 0, s>>>(args, target_warps);
     if (t_far_ready) cudaStreamWaitEvent(s, t_far_ready, 0);
     if (t_marks) cudaEventRecord(t_marks[1], s);
-    tree_list_kernel<PREC, MODEL><<<list_grid, LIST_WARPS * 32, 0, s>>>(args, target_warps);
+    tree_list_kernel<PREC, MODEL, 0><<<list_grid, LIST_WARPS * 32, 0, s>>>(args, target_warps);
     if (t_marks) cudaEventRecord(t_marks[2], s);
+    tree_list_kernel<PREC, MODEL, 1><<<list_grid, LIST_WARPS * 32, 0, s>>>(args, target_warps);
+    if (t_marks) cudaEventRecord(t_marks[3], s);
     tree_reduce_kernel<PREC><<<reduce_grid, 256, 0, s>>>(args, out, flags);
 }
 
@@ -965,7 +1094,8 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     const int64_t n = tgt->n;
     const bool sorted = pre && pre->perm && !target_wake_ptr;
     int32_t *perm = sorted ? const_cast<int32_t *>(pre->perm) : scratch.get<int32_t>(n);
-    unsigned long long *queue = scratch.get<unsigned long long>(2);  // list-kernel work counter, list-pool cursor
+    // near list-kernel work counter, list-pool cursor, far list-kernel work counter
+    unsigned long long *queue = scratch.get<unsigned long long>(3);
     int32_t *ex_pos = nullptr, *root_of = nullptr;
     if (!perm || !queue) return scratch.status;
     int rc;
@@ -1001,7 +1131,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
         BS_CHECK_LAUNCH("exclusion_positions_kernel");
     }
     BS_CUDA(cudaMemsetAsync(state, 0, 6 * sizeof(unsigned long long), s));
-    BS_CUDA(cudaMemsetAsync(queue, 0, 2 * sizeof(unsigned long long), s));
+    BS_CUDA(cudaMemsetAsync(queue, 0, 3 * sizeof(unsigned long long), s));
     const int block = std::min(kp->block, 128);
     const int64_t target_warps = (n + 31) / 32;
     // ~96 cost-balanced work items a SM in all, each warp's list cut in proportion to its cost (item_plan_kernel): the
@@ -1015,11 +1145,12 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     int *unit_chunks = scratch.get<int>(slots * LIST_CHUNKS);
     int *list_len = scratch.get<int>(slots), *list_total = scratch.get<int>(slots);
     double *walk_u = scratch.get<double>((size_t)3 * n), *partial = scratch.get<double>(capacity * 32 * 3);
+    double *partial_far = scratch.get<double>(capacity * 32 * 3);
     int8_t *walk_flag = scratch.get<int8_t>((size_t)n), *pflag = scratch.get<int8_t>(capacity * 32);
     int *item_off = scratch.get<int>(slots + 1), *item_warp = scratch.get<int>(capacity);
     int *item_first = scratch.get<int>(capacity);
-    if (!list || !list_cost || !unit_chunks || !list_len || !list_total || !walk_u || !partial || !walk_flag || !pflag ||
-        !item_off || !item_warp || !item_first)
+    if (!list || !list_cost || !unit_chunks || !list_len || !list_total || !walk_u || !partial || !partial_far ||
+        !walk_flag || !pflag || !item_off || !item_warp || !item_first)
         return scratch.status;
     EvalArgs args;
     args.n = n;
@@ -1029,7 +1160,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     args.ex_pos = ex_pos;
     args.tv = TreeView{tree->nodes,  tree->far64,  tree->far32, tree->far64x, tree->far32x,
                        tree->far64y, tree->far32y, tree->far64z, tree->far32z, tree->seg64, tree->seg32,
-                       tree->seg32x2};
+                       tree->seg32x2, tree->seg32c2};
     args.theta = tp->theta;
     args.theta2 = tp->theta * tp->theta;
     args.clearance = tp->clearance;
@@ -1049,6 +1180,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     args.overflow = reinterpret_cast<int *>(state);
     args.counters = state + 1;
     args.partial = partial;
+    args.partial_far = partial_far;
     args.pflag = pflag;
     args.item_off = item_off;
     args.item_warp = item_warp;
@@ -1114,7 +1246,7 @@ int tree_lists(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp,
     args.ex_pos = ex_pos;
     args.tv = TreeView{tree->nodes,  tree->far64,  tree->far32, tree->far64x, tree->far32x,
                        tree->far64y, tree->far32y, tree->far64z, tree->far32z, tree->seg64, tree->seg32,
-                       tree->seg32x2};
+                       tree->seg32x2, tree->seg32c2};
     args.theta = tp->theta;
     args.theta2 = tp->theta * tp->theta;
     args.clearance = tp->clearance;
@@ -1170,7 +1302,7 @@ int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const b
     Scratch scratch(ctx->pool, s);
     unsigned long long *state = scratch.get<unsigned long long>(7);  // flags, 5 counters, sort fault
     if (!state) return scratch.status;
-    cudaEvent_t e0, e1, marks[3];
+    cudaEvent_t e0, e1, marks[4];
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     for (auto &m : marks) cudaEventCreate(&m);
@@ -1187,11 +1319,12 @@ int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const b
     if (rc == BS_OK && fault) le = cudaMemcpyAsync(state + 6, fault, sizeof(int), cudaMemcpyDeviceToDevice, s);
     if (rc == BS_OK && le == cudaSuccess) le = cudaMemcpyAsync(host, state, sizeof host, cudaMemcpyDeviceToHost, s);
     if (le == cudaSuccess) le = cudaStreamSynchronize(s);
-    float ms = 0.f, walk_ms = 0.f, list_ms = 0.f;
+    float ms = 0.f, walk_ms = 0.f, list_ms = 0.f, far_ms = 0.f;
     if (rc == BS_OK && le == cudaSuccess) {
         cudaEventElapsedTime(&ms, e0, e1);
         cudaEventElapsedTime(&walk_ms, marks[0], marks[1]);
         cudaEventElapsedTime(&list_ms, marks[1], marks[2]);
+        cudaEventElapsedTime(&far_ms, marks[2], marks[3]);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1212,6 +1345,7 @@ int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const b
     ctx->stats.evaluate_ms = ms;
     ctx->stats.walk_ms = walk_ms;
     ctx->stats.list_ms = list_ms;
+    ctx->stats.far_ms = far_ms;
     if (host[0] & 0xffffffffull) {
         set_error("tree traversal stack overflow on the GPU (depth %d)",
                   (tp->stack_limit > 0 && tp->stack_limit < STACK_DEPTH) ? tp->stack_limit : STACK_DEPTH);
