@@ -659,8 +659,17 @@ __device__ __forceinline__ void far_eval(T rx, T ry, T rz, const T *f, int order
     uz += T(INV_FOUR_PI) * u2;
 }
 
+// A far-record float4: through the read-only path from global memory, or (STAGED) a plain load from a copy the
+// caller staged (in shared memory).
+template <bool STAGED>
+__device__ __forceinline__ float4 rec_ld(const float4 *p) {
+    if constexpr (STAGED) return *p;
+    else return __ldg(p);
+}
+
 // The fifth-order part on the unit vector n (FP32, record z5 of 42 float4), added to p5: a call of its own, so that its
 // 56-float rows do not raise the register count of the kernels that inline far_eval32v.
+template <bool STAGED>
 static __device__ __noinline__ void far_order5_unit(float nx, float ny, float nz, const float4 *z5, float *p5) {
     float u0 = 0.f, u1 = 0.f, u2 = 0.f;
 #pragma unroll 1
@@ -668,7 +677,7 @@ static __device__ __noinline__ void far_order5_unit(float nx, float ny, float nz
         float h[Z_ROW];
 #pragma unroll
         for (int q = 0; q < Z_ROW / 4; ++q) {
-            const float4 x = __ldg(z5 + (Z_ROW / 4) * i + q);
+            const float4 x = rec_ld<STAGED>(z5 + (Z_ROW / 4) * i + q);
             h[4 * q] = x.x; h[4 * q + 1] = x.y; h[4 * q + 2] = x.z; h[4 * q + 3] = x.w;
         }
         far_term5_row<float>(nx, ny, nz, 1.0f, 1.0f, 1.0f, 1.0f, h, i, u0, u1, u2);
@@ -685,6 +694,7 @@ static __device__ __noinline__ void far_order5_unit(float nx, float ny, float nz
 // order-p coefficients and powers of n (R^k = r^k n^k), summed by Horner's rule in 1/r, so no intermediate carries a
 // power of r beyond the order's own (r^-11 at order 4 would leave FP32's range for distances below ~1e-3.5 or above
 // ~3e3 in the caller's units; here from ~1e-6 to ~1e6 every intermediate stays normal).
+template <bool STAGED = false>
 __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const float4 *f, int order, float &ux,
                                             float &uy, float &uz, const float4 *g = nullptr,
                                             const float4 *k4 = nullptr, const float4 *z5 = nullptr) {
@@ -697,12 +707,12 @@ __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const 
     // order-p parts v_p (dimensionless in r); u = r^-2 (v0 + r^-1 (v1 + r^-1 (v2 + ...)))
     float p0[3] = {0.f, 0.f, 0.f}, p1[3] = {0.f, 0.f, 0.f}, p2[3] = {0.f, 0.f, 0.f}, p3[3] = {0.f, 0.f, 0.f},
           p4[3] = {0.f, 0.f, 0.f}, p5[3] = {0.f, 0.f, 0.f};
-    const float4 q0 = __ldg(f);  // m0 x y z, m1[0]
+    const float4 q0 = rec_ld<STAGED>(f);  // m0 x y z, m1[0]
     p0[0] = q0.y * nz - q0.z * ny;
     p0[1] = q0.z * nx - q0.x * nz;
     p0[2] = q0.x * ny - q0.y * nx;
     if (order >= 1) {
-        const float4 q1 = __ldg(f + 1), q2 = __ldg(f + 2), q3 = __ldg(f + 3);  // m1[1..8], w1, t2[0]
+        const float4 q1 = rec_ld<STAGED>(f + 1), q2 = rec_ld<STAGED>(f + 2), q3 = rec_ld<STAGED>(f + 3);  // m1[1..8], w1, t2[0]
         const float v0 = q0.w * nx + q1.x * ny + q1.y * nz;
         const float v1 = q1.z * nx + q1.w * ny + q2.x * nz;
         const float v2 = q2.y * nx + q2.z * ny + q2.w * nz;
@@ -711,9 +721,9 @@ __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const 
         p1[2] = 3.0f * (v0 * ny - v1 * nx) - q3.z;
         if (order >= 2) {
             const float xx = nx * nx, xy = nx * ny, xz = nx * nz, yy = ny * ny, yz = ny * nz, zz = nz * nz;
-            const float4 q4 = __ldg(f + 4), q5 = __ldg(f + 5), q6 = __ldg(f + 6);  // t2[1..2], w2[0..8], m2 s[0]
-            const float4 q7 = __ldg(f + 7), q8 = __ldg(f + 8), q9 = __ldg(f + 9), q10 = __ldg(f + 10),
-                         q11 = __ldg(f + 11);  // m2 symmetric s[1..17]
+            const float4 q4 = rec_ld<STAGED>(f + 4), q5 = rec_ld<STAGED>(f + 5), q6 = rec_ld<STAGED>(f + 6);  // t2[1..2], w2[0..8], m2 s[0]
+            const float4 q7 = rec_ld<STAGED>(f + 7), q8 = rec_ld<STAGED>(f + 8), q9 = rec_ld<STAGED>(f + 9), q10 = rec_ld<STAGED>(f + 10),
+                         q11 = rec_ld<STAGED>(f + 11);  // m2 symmetric s[1..17]
             // m2 symmetric rows (00,01,02,11,12,22) of i = 0, 1, 2 at floats 27..44
             const float s0[6] = {q6.w, q7.x, q7.y, q7.z, q7.w, q8.x};
             const float s1[6] = {q8.y, q8.z, q8.w, q9.x, q9.y, q9.z};
@@ -740,7 +750,7 @@ __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const 
                     float h[H_ROW];  // component i's row: m3 (10), T3 (3), W3 (6), pad
 #pragma unroll
                     for (int q = 0; q < H_ROW / 4; ++q) {
-                        const float4 x = __ldg(g + (H_ROW / 4) * i + q);
+                        const float4 x = rec_ld<STAGED>(g + (H_ROW / 4) * i + q);
                         h[4 * q] = x.x; h[4 * q + 1] = x.y; h[4 * q + 2] = x.z; h[4 * q + 3] = x.w;
                     }
                     const float *m = h + H_M3;
@@ -750,7 +760,7 @@ __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const 
                     x3[i] = 17.5f * s3 - 7.5f * tr;
                     w[i] = quad(h + H_W3);
                 }
-                const float4 wv = __ldg(g + H_W3V / 4);
+                const float4 wv = rec_ld<STAGED>(g + H_W3V / 4);
                 p3[0] = (x3[1] * nz - x3[2] * ny) - 7.5f * w[0] + 1.5f * wv.x;
                 p3[1] = (x3[2] * nx - x3[0] * nz) - 7.5f * w[1] + 1.5f * wv.y;
                 p3[2] = (x3[0] * ny - x3[1] * nx) - 7.5f * w[2] + 1.5f * wv.z;
@@ -761,12 +771,12 @@ __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const 
                         float h[K_ROW];
 #pragma unroll
                         for (int q = 0; q < K_ROW / 4; ++q) {
-                            const float4 x = __ldg(k4 + (K_ROW / 4) * i + q);
+                            const float4 x = rec_ld<STAGED>(k4 + (K_ROW / 4) * i + q);
                             h[4 * q] = x.x; h[4 * q + 1] = x.y; h[4 * q + 2] = x.z; h[4 * q + 3] = x.w;
                         }
                         far_term4_row<float>(nx, ny, nz, 1.0f, 1.0f, 1.0f, h, i, p4[0], p4[1], p4[2]);
                     }
-                    if (order >= 5) far_order5_unit(nx, ny, nz, z5, p5);
+                    if (order >= 5) far_order5_unit<STAGED>(nx, ny, nz, z5, p5);
                 }
             }
         }
@@ -792,6 +802,16 @@ __device__ __forceinline__ void split2(double x, float &hi, float &lo) {
 // ---------------------------------------------------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+// Asynchronous 16-byte copies global -> shared (both addresses 16-byte aligned), committed in groups; a thread waits
+// for its own copies (all but the newest N groups) and then __syncwarp()s before other lanes read them.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");

@@ -33,9 +33,9 @@ struct bs_tree {
     bs::NodeRec *nodes = nullptr;
     bs::Far64 *far64 = nullptr;
     bs::Far32 *far32 = nullptr;
-    bs::Far64x *far64x = nullptr;  // third-order records (trees built for order 3 only)
+    bs::Far64x *far64x = nullptr;  // third-order records (trees built for order 3 or more)
     bs::Far32x *far32x = nullptr;
-    bs::Far64y *far64y = nullptr;  // fourth-order records (trees built for order 4 or 5 only)
+    bs::Far64y *far64y = nullptr;  // fourth-order records (trees built for order 4 or 5)
     bs::Far32y *far32y = nullptr;
     bs::Far64z *far64z = nullptr;  // fifth-order records (trees built for order 5 only)
     bs::Far32z *far32z = nullptr;

@@ -1433,19 +1433,44 @@ __device__ __forceinline__ void segment_means(const double *d, const double *l, 
     }
 }
 
+// Segment k's half of its clear-leaf pair record (Seg32c2): start s relative to its leaf's centre o, negated;
+// Gamma/(4 pi); l = L d and -l; 1/(L rc)^2 from l2 = |l|^2 (+inf without a core).
+__device__ __forceinline__ void clear_half(Seg32c2 *out, int64_t k, double ox, double oy, double oz, double sx,
+                                           double sy, double sz, double lx, double ly, double lz, double l2,
+                                           double g4pi, double radius) {
+    float v[12];
+    v[0] = (float)(ox - sx);
+    v[1] = (float)(oy - sy);
+    v[2] = (float)(oz - sz);
+    v[3] = (float)g4pi;
+    v[4] = (float)lx;
+    v[5] = (float)ly;
+    v[6] = (float)lz;
+    v[7] = radius > 0.0 ? (float)(1.0 / (l2 * radius * radius)) : __int_as_float(0x7f800000);
+    v[8] = -v[4];
+    v[9] = -v[5];
+    v[10] = -v[6];
+    v[11] = 0.0f;
+    float *half = reinterpret_cast<float *>(out + (k >> 1)) + (k & 1);
+#pragma unroll
+    for (int f = 0; f < 12; ++f) half[2 * f] = v[f];
+}
+
 // Warps per block of leaf_moments_kernel (its staging takes (tuples + 3) x 33 doubles a warp).
 template <int PARTS>
 constexpr int leaf_warps() { return PARTS == MOM_PARTS5 ? 2 : 4; }
 
 // One warp per leaf: the moments about the leaf's centre; sums[j][PARTS] (sums[j][0] unused).  The warp takes 32
 // segments at a time: each lane forms its segment's means (segment_means) and alpha = gamma l into shared memory,
-// then lane u sums, over the 32, alpha_i times the mean of index tuple u (and of u + 32) for i = 0..2.
+// then lane u sums, over the 32, alpha_i times the mean of index tuple u (and of u + 32) for i = 0..2.  With `clear`
+// each lane also writes its segment's clear-leaf pair record, relative to the same centre.
 template <int PARTS>
 __global__ void __launch_bounds__(32 * leaf_warps<PARTS>()) leaf_moments_kernel(const int32_t *leaves,
                                                                               const unsigned *nleaves,
                                                                               const int64_t *lo, const int64_t *hi,
                                                                               const int32_t *order, const SegGeo *geo,
-                                                                              const double *centre, double *sums) {
+                                                                              const double *centre, double *sums,
+                                                                              Seg32c2 *clear) {
     using MT = MomentTuples<PARTS>;
     constexpr int ROWS = MT::n + 3, STRIDE = 33;  // means, then alpha; padded rows: lanes of a column hit other banks
     constexpr int LW = leaf_warps<PARTS>();
@@ -1474,6 +1499,9 @@ __global__ void __launch_bounds__(32 * leaf_warps<PARTS>()) leaf_moments_kernel(
 #pragma unroll
             for (int q = 0; q < MT::n; ++q) g[q] = 0.0;
             if (k < b) {
+                if (clear)
+                    clear_half(clear, k, c0, c1, c2, e.sx, e.sy, e.sz, e.lx, e.ly, e.lz,
+                               e.lx * e.lx + e.ly * e.ly + e.lz * e.lz, e.gamma * INV_FOUR_PI, e.radius);
                 if (e.gamma != 0.0) {  // a segment without circulation adds nothing (and no non-finite geometry)
                     const double d[3] = {0.5 * (e.sx + e.ex) - c0, 0.5 * (e.sy + e.ey) - c1, 0.5 * (e.sz + e.ez) - c2};
                     const double l[3] = {e.lx, e.ly, e.lz};
@@ -1744,22 +1772,8 @@ __global__ void clear_pairs_kernel(int64_t count, const int64_t *lo, const int64
     const double ox = centre[3 * j], oy = centre[3 * j + 1], oz = centre[3 * j + 2];
     for (int64_t k = lo[j] + lane; k < hi[j]; k += 32) {
         const Seg64 q = seg64[k];
-        float v[12];
-        v[0] = (float)(ox - q.sx);
-        v[1] = (float)(oy - q.sy);
-        v[2] = (float)(oz - q.sz);
-        v[3] = (float)(q.gfac * q.len);  // Gamma / (4 pi)
-        v[4] = (float)(q.dx * q.len);
-        v[5] = (float)(q.dy * q.len);
-        v[6] = (float)(q.dz * q.len);
-        const double lrc = q.len * q.radius;
-        v[7] = q.radius > 0.0 ? (float)(1.0 / (lrc * lrc)) : __int_as_float(0x7f800000);
-        v[8] = -v[4];
-        v[9] = -v[5];
-        v[10] = -v[6];
-        v[11] = 0.0f;
-        float *half = reinterpret_cast<float *>(out + (k >> 1)) + (k & 1);
-        for (int f = 0; f < 12; ++f) half[2 * f] = v[f];
+        clear_half(out, k, ox, oy, oz, q.sx, q.sy, q.sz, q.dx * q.len, q.dy * q.len, q.dz * q.len, q.len * q.len,
+                   q.gfac * q.len, q.radius);
     }
 }
 
@@ -1845,7 +1859,7 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
     const unsigned moment_blocks = (unsigned)std::max<int64_t>(
         1, std::min<int64_t>((count + LW - 1) / LW, (int64_t)std::max(1, leaf_resident) * sms));
     leaf_moments_kernel<PARTS><<<moment_blocks, 32 * LW, 0, ms>>>(leaves, nleaves, t->lo, t->hi, geo_order, geo,
-                                                                  t->centre, sums);
+                                                                  t->centre, sums, t->seg64 ? t->seg32c2 : nullptr);
     static const int climb_blocks = [] {  // resident blocks: one wave holds every climbing warp
         int r = 0;
         return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, bottom_up_kernel<PARTS>, 128, 0) == cudaSuccess ? r
@@ -1859,7 +1873,6 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
                       t->far64y, t->far32y, t->far64z, t->far32z};
     // one warp per block: the thread per node is long, so the nodes spread over every SM
     node_final_kernel<PARTS><<<dim3(blocks_for(count, 32), PARTS >= MOM_PARTS4 ? 4 : 1), 32, 0, ms>>>(count, sums, out);
-    clear_pairs(t, ms);  // the segment records were packed on this stream, the centres are known
     BS_CHECK_LAUNCH("bottom-up moments");
     bound_up_kernel<<<leaf_blocks, 128, 0, s>>>(leaves, nleaves, t->lo, t->hi, parent, ends, t->centre, anc_list,
                                                  bound2);

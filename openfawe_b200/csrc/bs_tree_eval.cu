@@ -24,6 +24,14 @@ constexpr int STACK_DEPTH = 128;
 constexpr int FAR_COST = 16;              // list cost units: one far evaluation ~ sixteen near pairs (measured)
 constexpr int LIST_WARPS = 4;             // warps per block of the list kernel
 constexpr int FAR_GROUPS = 4;             // open groups of disjoint far entries in the far list kernel
+constexpr int FAR_STAGE = 4;              // distinct nodes a group holds: their FP32 records are staged together
+constexpr int FAR_REC4 = 100;             // float4 of a staged node: FP32 far records to fifth order (12 + 16 + 28 +
+                                          // 42), then its centre (three doubles and a pad)
+constexpr int ENTRY_BUF = 64;             // list entries a warp of the list kernels reads ahead into shared memory
+constexpr int FAR_QUEUE = 32;             // closed far groups a warp queues before it evaluates them
+// dynamic shared memory a warp of the far list kernel uses: two staging buffers, the group queue, the entry buffer
+constexpr size_t FAR_WARP_SMEM = 2 * FAR_STAGE * FAR_REC4 * sizeof(float4) +
+                                 FAR_QUEUE * (2 * FAR_STAGE + 1) * sizeof(int) + ENTRY_BUF * sizeof(int2);
 
 struct TreeView {
     const NodeRec *nodes;
@@ -73,8 +81,8 @@ struct EvalArgs {
     int *item_warp;      // [capacity]: the warp of targets of each item
     int *item_first;     // [capacity]: the first list entry of each item (item_bounds_kernel)
     int item_want;       // items wanted in all (about 96 a SM); the capacity is item_want + target warps
-    double *partial;     // [items][32 lanes][3]: the near leaves of each item (tree_list_kernel<.., 0>)
-    double *partial_far; // [items][32 lanes][3]: the far nodes of each item (tree_list_kernel<.., 1>)
+    double *partial;     // [items][32 lanes][3]: each item's near leaves (tree_list_kernel<.., 0>), then its far
+                         // nodes added (tree_list_kernel<.., 1>, which runs after it)
     int8_t *pflag;       // [items][32 lanes]
     const int32_t *root_of;       // forests: root node of each (sorted) target's wake, -1 for none; null: node 0
     unsigned long long *queue;    // work counter of the persistent list kernel
@@ -136,6 +144,31 @@ __device__ __forceinline__ void far_node(const EvalArgs &a, const Target &t, int
                     a.order >= 5 ? reinterpret_cast<const float4 *>(a.tv.far32z[node].v) : nullptr);
         acc.add32(g0, g1, g2);
     }
+}
+
+// float4 i of node j's FP32 far records in staging order (Far32, then Far32x, Far32y, Far32z as the order has them).
+__device__ __forceinline__ const float4 *far_rec4(const TreeView &tv, int j, int i) {
+    if (i < 12) return reinterpret_cast<const float4 *>(tv.far32[j].v) + i;
+    if (i < 28) return reinterpret_cast<const float4 *>(tv.far32x[j].v) + (i - 12);
+    if (i < 56) return reinterpret_cast<const float4 *>(tv.far32y[j].v) + (i - 28);
+    return reinterpret_cast<const float4 *>(tv.far32z[j].v) + (i - 56);
+}
+
+// float4 of FP32 far records a node carries at `order`.
+__device__ __forceinline__ int far_rec4_count(int order) {
+    return 12 + (order >= 3 ? 16 : 0) + (order >= 4 ? 28 : 0) + (order >= 5 ? 42 : 0);
+}
+
+// far_node (single precision) from a staged copy of the node's records (far_rec4 order).
+template <int PREC>
+__device__ __forceinline__ void far_node_staged(const EvalArgs &a, const Target &t, int node, const float4 *st,
+                                                Acc<PREC> &acc) {
+    const double *c = reinterpret_cast<const double *>(st + FAR_REC4 - 2);  // the staged centre
+    const double rx = t.x0 - c[0], ry = t.x1 - c[1], rz = t.x2 - c[2];
+    float g0 = 0.f, g1 = 0.f, g2 = 0.f;
+    far_eval32v<true>((float)rx, (float)ry, (float)rz, st, a.order, g0, g1, g2, a.order >= 3 ? st + 12 : nullptr,
+                      a.order >= 4 ? st + 28 : nullptr, a.order >= 5 ? st + 56 : nullptr);
+    acc.add32(g0, g1, g2);
 }
 
 // FP64 re-evaluation of the pairs of segments base + j (bits of `need`): value added or flag recorded.
@@ -604,8 +637,8 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
 // registers).  Partial sums per (chunk, target) are combined in chunk order by the reduce kernel.
 template <int PREC, int MODEL, int PART>
 __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, int chunks, int64_t item,
-                                          Seg64 *seg64_tile, Seg32 *seg32_tile, long long &near_pairs,
-                                          long long &fp64_pairs) {
+                                          Seg64 *seg64_tile, Seg32 *seg32_tile, float4 *stage, int2 *ebuf,
+                                          long long &near_pairs, long long &fp64_pairs) {
     const int lane = threadIdx.x & 31;
     // chunk c is the c-th slice of this warp's list by cost: entries [item_first[item], item_first[item + 1]), the
     // last slice ending at the list's end
@@ -615,6 +648,19 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
         return (int64_t)chunks_of[k / LIST_CHUNK] * LIST_CHUNK + (k & (LIST_CHUNK - 1));
     };
     const int first = a.item_first[item], last = c + 1 < chunks ? a.item_first[item + 1] : len;
+    // entry k of the list (warp-uniform k): read ahead ENTRY_BUF entries at a time into the warp's buffer, so that
+    // the entries cost one coalesced load a block instead of two dependent loads each
+    int buf_lo = first, buf_hi = first;
+    auto entry_at = [&](int k) -> int2 {
+        if (k >= buf_hi) {
+            __syncwarp();
+            buf_lo = k;
+            buf_hi = min(last, k + ENTRY_BUF);
+            for (int i = lane; i < buf_hi - buf_lo; i += 32) ebuf[i] = a.list[at(buf_lo + i)];
+            __syncwarp();
+        }
+        return ebuf[k - buf_lo];
+    };
     Target t;
     t.load(a, gw * 32 + lane);
     int64_t e = 0, e1 = 0;
@@ -623,7 +669,7 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
     int flag = BS_FLAG_OK;
     if constexpr (PART == 0) {
         for (int k = first; k < last; ++k) {
-            const int2 entry = a.list[at(k)];
+            const int2 entry = entry_at(k);
             if (entry.x & FAR_BIT) continue;
             const bool mine = ((unsigned)entry.y >> lane) & 1u;
             const NodeRec nr = a.tv.nodes[entry.x];
@@ -632,23 +678,70 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
                                     fp64_pairs);
         }
     } else {
-        // Far entries are packed first-fit into FAR_GROUPS open groups of disjoint lane masks, each lane of a group at
-        // its own node; a group is evaluated (every lane at its node at once) when an entry fits none -- the fullest
-        // group goes -- and, one by one, at the end.  A far entry holds about a third of the warp's lanes, so a group
-        // fills the warp from a few entries, and a load of its records touches a few distinct addresses.  One call
-        // site evaluates every group.
-        int my_far[FAR_GROUPS];
-        unsigned group[FAR_GROUPS];
+        // Far entries are packed first-fit into FAR_GROUPS open groups of disjoint lane masks and at most FAR_STAGE
+        // entries, each lane of a group at its own node.  A group closes when an entry fits none (the fullest one
+        // closes) or when the list ends; closed groups queue (up to FAR_QUEUE) and are then evaluated in order, every
+        // lane at its node at once.  A far entry holds about a third of the warp's lanes, so a group fills the warp
+        // from a few entries.  In single precision the records of the next group's nodes are copied into the warp's
+        // other staging buffer (cp.async) while the current group is evaluated from its copy.
+        int *q_node = reinterpret_cast<int *>(stage + 2 * FAR_STAGE * FAR_REC4);  // [FAR_QUEUE][FAR_STAGE]
+        unsigned *q_mask = reinterpret_cast<unsigned *>(q_node + FAR_QUEUE * FAR_STAGE);
+        int *q_cnt = reinterpret_cast<int *>(q_mask + FAR_QUEUE * FAR_STAGE);
+        unsigned group[FAR_GROUPS], gmask[FAR_GROUPS][FAR_STAGE];
+        int gnode[FAR_GROUPS][FAR_STAGE], gcount[FAR_GROUPS];
 #pragma unroll
         for (int q = 0; q < FAR_GROUPS; ++q) {
-            my_far[q] = -1;
             group[q] = 0u;
+            gcount[q] = 0;
+#pragma unroll
+            for (int r = 0; r < FAR_STAGE; ++r) {
+                gnode[q][r] = -1;
+                gmask[q][r] = 0u;
+            }
         }
+        const int n4 = far_rec4_count(a.order);
+        int nq = 0;  // closed groups queued
+        auto close = [&](int go) {
+#pragma unroll
+            for (int q = 0; q < FAR_GROUPS; ++q)
+                if (q == go) {
+                    if (lane < FAR_STAGE) {
+                        int nd = -1;
+                        unsigned mk = 0u;
+#pragma unroll
+                        for (int r = 0; r < FAR_STAGE; ++r)
+                            if (r == lane) {
+                                nd = gnode[q][r];
+                                mk = gmask[q][r];
+                            }
+                        q_node[nq * FAR_STAGE + lane] = nd;
+                        q_mask[nq * FAR_STAGE + lane] = mk;
+                    }
+                    if (lane == 0) q_cnt[nq] = gcount[q];
+                    group[q] = 0u;
+                    gcount[q] = 0;
+                }
+            ++nq;
+        };
+        // the records of queued group g into staging buffer b: every lane copies its share, then commits
+        auto issue = [&](int g, int b) {
+            if (PREC != 0 && g < nq) {
+                float4 *buf = stage + b * FAR_STAGE * FAR_REC4;
+                const int cnt = q_cnt[g];
+                for (int r = 0; r < cnt; ++r) {
+                    const int nd = q_node[g * FAR_STAGE + r];
+                    for (int i = lane; i < n4; i += 32) cp_async16(buf + r * FAR_REC4 + i, far_rec4(a.tv, nd, i));
+                    if (lane < 2)  // the centre: cx, cy, cz of the node's traversal record
+                        cp_async16(buf + r * FAR_REC4 + FAR_REC4 - 2 + lane,
+                                   reinterpret_cast<const float4 *>(a.tv.nodes + nd) + lane);
+                }
+            }
+            cp_async_commit();
+        };
         int k = first;
         for (;;) {
-            int go = -1;  // the group to evaluate next
-            while (k < last) {
-                const int2 entry = a.list[at(k)];
+            while (k < last && nq < FAR_QUEUE - FAR_GROUPS) {  // room left to close every open group at the end
+                const int2 entry = entry_at(k);
                 if (!(entry.x & FAR_BIT)) {
                     ++k;
                     continue;
@@ -657,49 +750,75 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
                 int fit = -1;
 #pragma unroll
                 for (int q = 0; q < FAR_GROUPS; ++q)
-                    if (fit < 0 && !(group[q] & m)) fit = q;
+                    if (fit < 0 && !(group[q] & m) && gcount[q] < FAR_STAGE) fit = q;
                 if (fit < 0) {
-                    int most = -1;
+                    int most = -1, go = 0;
 #pragma unroll
                     for (int q = 0; q < FAR_GROUPS; ++q)
                         if (__popc(group[q]) > most) {
                             most = __popc(group[q]);
                             go = q;
                         }
-                    break;
+                    close(go);
+                    continue;  // the entry is placed again, into the emptied group at least
                 }
+                const int node = entry.x & ~FAR_BIT;
 #pragma unroll
                 for (int q = 0; q < FAR_GROUPS; ++q)
                     if (q == fit) {
                         group[q] |= m;
-                        if ((m >> lane) & 1u) my_far[q] = entry.x & ~FAR_BIT;
+#pragma unroll
+                        for (int r = 0; r < FAR_STAGE; ++r)
+                            if (r == gcount[q]) {
+                                gnode[q][r] = node;
+                                gmask[q][r] = m;
+                            }
+                        ++gcount[q];
                     }
                 ++k;
             }
-            if (go < 0) {  // the list is done: the groups that hold entries, one by one
+            const bool done = k >= last;
+            if (done) {
 #pragma unroll
                 for (int q = 0; q < FAR_GROUPS; ++q)
-                    if (go < 0 && group[q]) go = q;
-                if (go < 0) break;
+                    if (group[q]) close(q);
             }
-            int node = -1;
-#pragma unroll
-            for (int q = 0; q < FAR_GROUPS; ++q)
-                if (q == go) {
-                    node = my_far[q];
-                    my_far[q] = -1;
-                    group[q] = 0u;
+            __syncwarp();  // the queue is written
+            issue(0, 0);
+            for (int g = 0; g < nq; ++g) {
+                issue(g + 1, (g + 1) & 1);
+                cp_async_wait<1>();
+                __syncwarp();  // group g's records are in its buffer
+                int slot = -1;
+                for (int r = 0; r < q_cnt[g]; ++r)
+                    if ((q_mask[g * FAR_STAGE + r] >> lane) & 1u) slot = r;
+                if (slot >= 0) {
+                    const int node = q_node[g * FAR_STAGE + slot];
+                    if constexpr (PREC != 0)
+                        far_node_staged<PREC>(a, t, node, stage + (g & 1) * FAR_STAGE * FAR_REC4 + slot * FAR_REC4,
+                                              acc);
+                    else
+                        far_node<PREC>(a, t, node, acc);
                 }
-            if (node >= 0) far_node<PREC>(a, t, node, acc);
+                __syncwarp();  // buffer g & 1 is free for group g + 2
+            }
+            cp_async_wait<0>();
+            nq = 0;
+            if (done) break;
         }
     }
     if (t.valid) {
         const int64_t o = item * 32 + lane;
-        double *dst = PART == 0 ? a.partial : a.partial_far;
-        dst[3 * o] = acc.x();
-        dst[3 * o + 1] = acc.y();
-        dst[3 * o + 2] = acc.z();
-        if (PART == 0) a.pflag[o] = (int8_t)flag;
+        if (PART == 0) {
+            a.partial[3 * o] = acc.x();
+            a.partial[3 * o + 1] = acc.y();
+            a.partial[3 * o + 2] = acc.z();
+            a.pflag[o] = (int8_t)flag;
+        } else {
+            a.partial[3 * o] += acc.x();
+            a.partial[3 * o + 1] += acc.y();
+            a.partial[3 * o + 2] += acc.z();
+        }
     }
 }
 
@@ -707,10 +826,16 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
 // PART 0: near leaves (counter a.queue[0]); PART 1: far nodes (counter a.queue[2]; no tiles).
 template <int PREC, int MODEL, int PART>
 __global__ void __launch_bounds__(LIST_WARPS * 32, 3) tree_list_kernel(EvalArgs a, int64_t target_warps) {
+    // near kernel: static tiles and entry buffers; far kernel: FAR_WARP_SMEM of dynamic shared memory a warp
     __shared__ __align__(16) unsigned char tile_mem[PART == 0 ? LIST_WARPS * 32 * sizeof(Seg64) : 16];
+    __shared__ int2 entry_mem[PART == 0 ? LIST_WARPS * ENTRY_BUF : 1];
+    extern __shared__ __align__(16) unsigned char list_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Seg64 *seg64_tile = reinterpret_cast<Seg64 *>(tile_mem) + warp * 32;
     Seg32 *seg32_tile = reinterpret_cast<Seg32 *>(tile_mem) + warp * 32;
+    float4 *stage = reinterpret_cast<float4 *>(list_smem + warp * FAR_WARP_SMEM);  // far kernel only
+    int2 *ebuf = PART == 0 ? entry_mem + warp * ENTRY_BUF
+                           : reinterpret_cast<int2 *>(list_smem + (warp + 1) * FAR_WARP_SMEM) - ENTRY_BUF;
     const unsigned long long items = (unsigned long long)a.item_off[target_warps];
     long long near_pairs = 0, fp64_pairs = 0;
     for (;;) {
@@ -721,7 +846,7 @@ __global__ void __launch_bounds__(LIST_WARPS * 32, 3) tree_list_kernel(EvalArgs 
         const int64_t lo = a.item_warp[item];  // the warp of targets whose list this item slices
         const int first = a.item_off[lo];
         list_item<PREC, MODEL, PART>(a, lo, (int)(item - first), a.item_off[lo + 1] - first, (int64_t)item,
-                                     seg64_tile, seg32_tile, near_pairs, fp64_pairs);
+                                     seg64_tile, seg32_tile, stage, ebuf, near_pairs, fp64_pairs);
     }
     if constexpr (PART == 0) {
         for (int o = 16; o > 0; o >>= 1) {
@@ -757,19 +882,28 @@ __global__ void __launch_bounds__(1024) item_plan_kernel(int64_t target_warps, c
     const long long unit = max(1ll, (total + want - 1) / want);
     long long items = 0;
     for (int64_t w = a0; w < a1; ++w) items += min(64ll, max(1ll, ((long long)list_total[w] + unit - 1) / unit));
-    part[t] = items;
+    // exclusive scan of the threads' item counts: within each warp by shuffles, then over the 32 warp totals
+    const int lane = t & 31, wid = t >> 5;
+    long long inc = items;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+    }
+    if (lane == 31) part[wid] = inc;
     __syncthreads();
-    if (t == 0) {
-        long long run = 0;
-        for (int k = 0; k < 1024; ++k) {
-            const long long v = part[k];
-            part[k] = run;
-            run += v;
+    if (wid == 0) {
+        long long w = part[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long v = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += v;
         }
-        item_off[target_warps] = (int)run;
+        part[lane] = w;  // inclusive over the warps
+        if (lane == 31) item_off[target_warps] = (int)w;
     }
     __syncthreads();
-    long long run = part[t];
+    long long run = inc - items + (wid ? part[wid - 1] : 0);
     for (int64_t w = a0; w < a1; ++w) {
         item_off[w] = (int)run;
         const long long k = min(64ll, max(1ll, ((long long)list_total[w] + unit - 1) / unit));
@@ -793,11 +927,17 @@ __global__ void item_bounds_kernel(EvalArgs a, int64_t target_warps) {
         for (int c = lane; c < chunks; c += 32) a.item_first[base + c] = 0;
         return;
     }
-    auto cost = [&](int k) -> long long {
-        return a.list_cost[(int64_t)chunks_of[k / LIST_CHUNK] * LIST_CHUNK + (k & (LIST_CHUNK - 1))];
-    };
-    for (int k = lane; k < len; k += 32) {
-        const long long ck = cost(k), cp = k ? cost(k - 1) : -1;
+    // the chunk table (at most 32 chunks) one entry a lane; entry k's chunk is then a shuffle away
+    const int my_chunk = lane < LIST_CHUNKS && lane * LIST_CHUNK < len ? chunks_of[lane] : 0;
+    long long carry = -1;  // cost start of the entry before this round's first
+    for (int k0 = 0; k0 < len; k0 += 32) {
+        const int k = k0 + lane;
+        const int ch = __shfl_sync(0xffffffffu, my_chunk, (k < len ? k : len - 1) / LIST_CHUNK);
+        const long long ck = k < len ? a.list_cost[(int64_t)ch * LIST_CHUNK + (k & (LIST_CHUNK - 1))] : 0;
+        const long long up = __shfl_up_sync(0xffffffffu, ck, 1);
+        const long long cp = lane == 0 ? carry : up;
+        carry = __shfl_sync(0xffffffffu, ck, 31);
+        if (k >= len) continue;
         // floor(total c / chunks) > cp  <=>  c >= ceil((cp + 1) chunks / total);
         // floor(total c / chunks) <= ck <=>  c <= ceil((ck + 1) chunks / total) - 1
         const long long c0 = ((cp + 1) * chunks + total - 1) / total;
@@ -820,7 +960,6 @@ __global__ void tree_reduce_kernel(EvalArgs a, double *out, int8_t *flags) {
     for (int item = a.item_off[gw]; item < a.item_off[gw + 1]; ++item) {
         const int64_t o = (int64_t)item * 32 + lane;
         acc.add64(a.partial[3 * o], a.partial[3 * o + 1], a.partial[3 * o + 2]);
-        acc.add64(a.partial_far[3 * o], a.partial_far[3 * o + 1], a.partial_far[3 * o + 2]);
         if (flag == BS_FLAG_OK) flag = a.pflag[o];
     }
     acc.add64(a.walk_u[3 * p], a.walk_u[3 * p + 1], a.walk_u[3 * p + 2]);
@@ -931,7 +1070,12 @@ static void launch_pair(unsigned walk_grid, int block, size_t smem, unsigned lis
     if (t_marks) cudaEventRecord(t_marks[1], s);
     tree_list_kernel<PREC, MODEL, 0><<<list_grid, LIST_WARPS * 32, 0, s>>>(args, target_warps);
     if (t_marks) cudaEventRecord(t_marks[2], s);
-    tree_list_kernel<PREC, MODEL, 1><<<list_grid, LIST_WARPS * 32, 0, s>>>(args, target_warps);
+    static const bool far_smem = cudaFuncSetAttribute(tree_list_kernel<PREC, MODEL, 1>,
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      (int)(LIST_WARPS * FAR_WARP_SMEM)) == cudaSuccess;
+    (void)far_smem;  // a refusal shows as the launch's error
+    tree_list_kernel<PREC, MODEL, 1><<<list_grid, LIST_WARPS * 32, LIST_WARPS * FAR_WARP_SMEM, s>>>(args,
+                                                                                                   target_warps);
     if (t_marks) cudaEventRecord(t_marks[3], s);
     tree_reduce_kernel<PREC><<<reduce_grid, 256, 0, s>>>(args, out, flags);
 }
@@ -1145,12 +1289,11 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     int *unit_chunks = scratch.get<int>(slots * LIST_CHUNKS);
     int *list_len = scratch.get<int>(slots), *list_total = scratch.get<int>(slots);
     double *walk_u = scratch.get<double>((size_t)3 * n), *partial = scratch.get<double>(capacity * 32 * 3);
-    double *partial_far = scratch.get<double>(capacity * 32 * 3);
     int8_t *walk_flag = scratch.get<int8_t>((size_t)n), *pflag = scratch.get<int8_t>(capacity * 32);
     int *item_off = scratch.get<int>(slots + 1), *item_warp = scratch.get<int>(capacity);
     int *item_first = scratch.get<int>(capacity);
-    if (!list || !list_cost || !unit_chunks || !list_len || !list_total || !walk_u || !partial || !partial_far ||
-        !walk_flag || !pflag || !item_off || !item_warp || !item_first)
+    if (!list || !list_cost || !unit_chunks || !list_len || !list_total || !walk_u || !partial || !walk_flag || !pflag ||
+        !item_off || !item_warp || !item_first)
         return scratch.status;
     EvalArgs args;
     args.n = n;
@@ -1180,7 +1323,6 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     args.overflow = reinterpret_cast<int *>(state);
     args.counters = state + 1;
     args.partial = partial;
-    args.partial_far = partial_far;
     args.pflag = pflag;
     args.item_off = item_off;
     args.item_warp = item_warp;
