@@ -59,6 +59,7 @@ struct EvalArgs {
     double theta, theta2, clearance;
     int order, model, raise_singular, stack_limit;
     int deferred;  // the segment and far records may still be in computation while the walk runs: it must not read them
+    int fill;      // a leaf opened for a lane is summed exactly for every lane of the warp that reached it (below)
     float near2;
     // interaction lists: entries live in chunks of LIST_CHUNK taken from a shared pool; warp gw of targets lists its
     // chunks in unit_chunks[gw][0 .. LIST_CHUNKS)
@@ -531,8 +532,19 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
             }
             if (exact) accept = false;  // a target summed exactly opens every node
         }
-        const unsigned farm = __ballot_sync(0xffffffffu, mine && accept);
-        const unsigned openm = mask & ~farm;
+        unsigned farm = __ballot_sync(0xffffffffu, mine && accept);
+        unsigned openm = mask & ~farm;
+        const unsigned openers = __ballot_sync(0xffffffffu, mine && !accept && !exact);
+        // Fill: a leaf that some lane opens is evaluated by the warp anyway, and the lanes that accepted it as far
+        // would idle beside its pairs: they sum it exactly instead of through its expansion (same time, no far
+        // evaluation, more exact).  Morton trees in single precision only: median trees and FP64 keep each
+        // target's own decisions, the reference's.  Exact targets (which open every leaf) do not count, so that
+        // they leave the others' results as they are.
+        if (a.fill && nr.left < 0 && openers && farm) {
+            openm = mask;
+            farm = 0u;
+            accept = false;
+        }
         if (farm) {
             if (mine && accept) ++far;
             far_total += __popc(farm);
@@ -1015,8 +1027,8 @@ __device__ __forceinline__ uint64_t spread3_t(uint32_t v) {
     return x;
 }
 
-__global__ void target_keys_kernel(int64_t n, const double *points, const unsigned long long *box, uint64_t *keys,
-                                   int32_t *vals) {
+__global__ void target_keys_kernel(int64_t n, const double *points, const unsigned long long *box,
+                                   const uint8_t *exact, uint64_t *keys, int32_t *vals) {
     int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     double ext = 0.0, lo[3];
@@ -1027,7 +1039,8 @@ __global__ void target_keys_kernel(int64_t n, const double *points, const unsign
     double inv = ext > 0.0 ? 2097152.0 / ext : 0.0;
     uint32_t q[3];
     for (int a = 0; a < 3; ++a) q[a] = min(2097151u, (uint32_t)((points[3 * p + a] - lo[a]) * inv));
-    keys[p] = (spread3_t(q[0]) << 2) | (spread3_t(q[1]) << 1) | spread3_t(q[2]);
+    keys[p] = (spread3_t(q[0]) << 2) | (spread3_t(q[1]) << 1) | spread3_t(q[2]) |
+              ((exact && exact[p]) ? 1ull << 63 : 0ull);  // exact targets after the others
     vals[p] = (int32_t)p;
 }
 
@@ -1102,17 +1115,20 @@ static void launch_eval(int precision, int model, unsigned walk_grid, int block,
     else launch_model<2>(model, walk_grid, block, smem, list_grid, tw, reduce_grid, s, args, out, flags);
 }
 
-int target_order(int64_t n, const double *points, int32_t *perm, Scratch &scratch, cudaStream_t s) {
+// exact (may be null): targets marked exact sort after all the others (the key's top bit), in their own warps but
+// for one, so that the other targets keep the warps, and with fill the results, they have without them.
+int target_order(int64_t n, const double *points, int32_t *perm, Scratch &scratch, cudaStream_t s,
+                 const uint8_t *exact = nullptr) {
     unsigned long long *box = scratch.get<unsigned long long>(6);
     uint64_t *keys = scratch.get<uint64_t>(n);
     if (!box || !keys) return scratch.status;
     target_box_init_kernel<<<1, 32, 0, s>>>(box);
     target_box_kernel<<<std::min<unsigned>(nblocks(n, 256), 592), 256, 0, s>>>(n, points, box);
-    target_keys_kernel<<<nblocks(n, 256), 256, 0, s>>>(n, points, box, keys, perm);
+    target_keys_kernel<<<nblocks(n, 256), 256, 0, s>>>(n, points, box, exact, keys, perm);
     BS_CHECK_LAUNCH("target keys");
-    // the order only groups nearby targets into warps (each target's result does not depend on it): the top 32 key
-    // bits (about 10.7 per axis) do that in four passes
-    return radix_sort(keys, perm, n, 31, 63, scratch, s);
+    // the order groups nearby targets into warps: the top 32 Morton bits (about 10.7 per axis) do that in four passes
+    // (a fifth for the exact bit)
+    return radix_sort(keys, perm, n, 31, exact ? 64 : 63, scratch, s);
 }
 
 // Forest targets: sorted by (wake, Morton key in the wake's own target box); each sorted target learns its root.
@@ -1162,7 +1178,8 @@ __global__ void forest_target_box_init_kernel(int nw, unsigned long long *box) {
 }
 
 __global__ void forest_target_keys_kernel(int64_t n, const double *points, const int64_t *ptr, int nw,
-                                          const unsigned long long *box, int bits, uint64_t *keys, int32_t *vals) {
+                                          const unsigned long long *box, int bits, const uint8_t *exact,
+                                          uint64_t *keys, int32_t *vals) {
     int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     const int w = target_wake(ptr, nw, p);
@@ -1177,7 +1194,8 @@ __global__ void forest_target_keys_kernel(int64_t n, const double *points, const
         uint32_t q = min((1u << bits) - 1u, (uint32_t)((points[3 * p + a] - lo[a]) * inv));
         for (int b = 0; b < bits; ++b) key |= (uint64_t)((q >> b) & 1u) << (3 * b + 2 - a);
     }
-    keys[p] = ((uint64_t)w << (3 * bits)) | key;
+    // wake and key use at most 63 bits: the top bit puts exact targets after all the others (see target_order)
+    keys[p] = ((uint64_t)w << (3 * bits)) | key | ((exact && exact[p]) ? 1ull << 63 : 0ull);
     vals[p] = (int32_t)p;
 }
 
@@ -1256,7 +1274,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
         forest_target_box_init_kernel<<<nblocks(6 * (int64_t)nw, 256), 256, 0, s>>>(nw, box);
         forest_target_box_kernel<<<dim3((unsigned)nw, 4), 256, 0, s>>>(tgt->points, target_wake_ptr, box);
         forest_target_keys_kernel<<<nblocks(n, 256), 256, 0, s>>>(n, tgt->points, target_wake_ptr, nw, box, bits,
-                                                                  keys, perm);
+                                                                  pre ? pre->exact : nullptr, keys, perm);
         BS_CHECK_LAUNCH("forest target keys");
         rc = radix_sort(keys, perm, n, 32, 64, scratch, s);  // wake, then the leading Morton bits
         if (rc != BS_OK) return rc;
@@ -1264,7 +1282,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
                                                                root_of);
         BS_CHECK_LAUNCH("forest_roots_of_kernel");
     } else {
-        rc = target_order(n, tgt->points, perm, scratch, s);
+        rc = target_order(n, tgt->points, perm, scratch, s, pre ? pre->exact : nullptr);
         if (rc != BS_OK) return rc;
     }
     if (tgt->ex_ptr && tgt->e > 0) {
@@ -1311,6 +1329,7 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     args.model = kp->model;
     args.raise_singular = kp->raise_singular ? 1 : 0;
     args.deferred = (pre && pre->far_ready) ? 1 : 0;
+    args.fill = (tree->kind == BS_TREE_MORTON && kp->precision != BS_FP64) ? 1 : 0;
     args.near2 = (float)(kp->near_cores * kp->near_cores);
     args.stack_limit = (tp->stack_limit > 0 && tp->stack_limit < STACK_DEPTH) ? tp->stack_limit : STACK_DEPTH;
     args.list = list;
@@ -1396,6 +1415,7 @@ int tree_lists(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp,
     args.model = kp->model;
     args.raise_singular = kp->raise_singular ? 1 : 0;
     args.deferred = 1;  // nothing is evaluated in the walk: what does not fit in the lists is reported
+    args.fill = (tree->kind == BS_TREE_MORTON && kp->precision != BS_FP64) ? 1 : 0;  // the forward's lists
     args.near2 = (float)(kp->near_cores * kp->near_cores);
     args.stack_limit = (tp->stack_limit > 0 && tp->stack_limit < STACK_DEPTH) ? tp->stack_limit : STACK_DEPTH;
     args.list = list;
