@@ -171,4 +171,62 @@ __device__ __forceinline__ bool pair_vjp32(float xh0, float xh1, float xh2, floa
     return false;
 }
 
+// One segment of a leaf for the tree adjoint, from its half of the clear-leaf pair record (Seg32c2): start relative
+// to the leaf's centre O, negated; Gamma/(4 pi); l = L d; 1/(L rc)^2 (+inf without a core).
+struct ClearSeg {
+    float nsx, nsy, nsz, gf, lx, ly, lz, w;
+};
+
+// pair_vjp32 for a target clear of the segment's leaf (the conditions of pair32x2_clear: at least 1.5 bounding radii
+// from the leaf's centre, outside the core test's reach, within FP32's range), in physical units from the target's
+// offset (rx, ry, rz) = x - O: r1 = x - A, r2 = x - B, l = B - A = r1 - r2, c = r1 x r2, and the forward's
+//   u = Gamma/(4 pi) f S c / D,  S = |r1| + |r2|,  P = |r1||r2|,  D = P (P + r1.r2),  rho^2 = |c|^2 / (L rc)^2.
+// No FP64 fallback: no pair of a clear target needs one.  g1 = d(w.u)/dr1, g2 = d(w.u)/dr2, gg = d(w.u)/dGamma; the
+// dependence of rho^2 on L = |l| gives the -/+ 2 g_rho2 rho2 l / L^2 terms.  MODEL 0..2.
+template <int MODEL>
+__device__ __forceinline__ void pair_vjp32_clear(float rx, float ry, float rz, const ClearSeg &q, float w0, float w1,
+                                                 float w2, float *g1, float *g2, float &gg) {
+    const float a0 = rx + q.nsx, a1 = ry + q.nsy, a2 = rz + q.nsz;  // r1
+    const float b0 = a0 - q.lx, b1 = a1 - q.ly, b2 = a2 - q.lz;     // r2
+    // c = l x r1 = r1 x r2
+    const float c0 = fmaf(q.ly, a2, -q.lz * a1), c1 = fmaf(q.lz, a0, -q.lx * a2), c2 = fmaf(q.lx, a1, -q.ly * a0);
+    const float cc = fmaf(c0, c0, fmaf(c1, c1, c2 * c2));
+    const float q1 = fmaf(a0, a0, fmaf(a1, a1, a2 * a2)), q2 = fmaf(b0, b0, fmaf(b1, b1, b2 * b2));
+    const float in1 = rsqrtf(q1), in2 = rsqrtf(q2);
+    const float n1 = q1 * in1, n2 = q2 * in2;
+    const float dt = fmaf(a0, b0, fmaf(a1, b1, a2 * b2));
+    const float P = n1 * n2, D = P * (P + dt), iD = __fdividef(1.0f, D);
+    float f = 1.0f, df = 0.0f, rho2 = 0.0f;
+    if (MODEL != 0) {
+        rho2 = cc * q.w;  // +inf or NaN without a core: f stays 1, df 0
+        if (MODEL == 1) {
+            if (rho2 < 1.0f) { f = rho2; df = 1.0f; }
+        } else if (rho2 <= (float)LAMB_CUT2) {
+            const float e = exp2_approx(rho2 * LAMB_A_LOG2E_NEG);
+            f = 1.0f - e;
+            df = (float)LAMB_A * e;
+        }
+    }
+    const float S = n1 + n2;
+    const float wc = fmaf(w0, c0, fmaf(w1, c1, w2 * c2));
+    const float h = q.gf * wc * iD;
+    gg = (float)INV_FOUR_PI * f * S * wc * iD;
+    const float g_S = h * f, g_D = -h * f * S * iD;
+    const float g_rho2 = h * S * df;
+    const float g_cc = df != 0.0f ? g_rho2 * q.w : 0.0f;
+    const float g_P = g_D * (2.0f * P + dt), g_dt = g_D * P;
+    const float k = q.gf * f * S * iD;
+    const float gc0 = fmaf(2.0f * c0, g_cc, k * w0), gc1 = fmaf(2.0f * c1, g_cc, k * w1),
+                gc2 = fmaf(2.0f * c2, g_cc, k * w2);
+    const float s1 = (g_S + g_P * n2) * in1, s2 = (g_S + g_P * n1) * in2;
+    const float L2 = fmaf(q.lx, q.lx, fmaf(q.ly, q.ly, q.lz * q.lz));
+    const float bb = df != 0.0f ? 2.0f * g_rho2 * rho2 * __fdividef(1.0f, L2) : 0.0f;
+    g1[0] = s1 * a0 + g_dt * b0 + (b1 * gc2 - b2 * gc1) - bb * q.lx;
+    g1[1] = s1 * a1 + g_dt * b1 + (b2 * gc0 - b0 * gc2) - bb * q.ly;
+    g1[2] = s1 * a2 + g_dt * b2 + (b0 * gc1 - b1 * gc0) - bb * q.lz;
+    g2[0] = s2 * b0 + g_dt * a0 + (gc1 * a2 - gc2 * a1) + bb * q.lx;
+    g2[1] = s2 * b1 + g_dt * a1 + (gc2 * a0 - gc0 * a2) + bb * q.ly;
+    g2[2] = s2 * b2 + g_dt * a2 + (gc0 * a1 - gc1 * a0) + bb * q.lz;
+}
+
 }  // namespace bs

@@ -76,6 +76,7 @@ struct AdjArgs {
     float near2;
     const NodeRec *nodes;
     const Seg32 *seg32;
+    const Seg32c2 *seg32c2;  // clear-leaf records: the forward's (tree order, relative to each leaf's centre)
     const Seg64 *seg64;
     const int32_t *order32;  // tree position -> segment
     const double *starts, *directions, *lengths, *gamma;
@@ -134,10 +135,23 @@ __global__ void parent_of_kernel(int64_t count, const int64_t *left, const int64
     if (right[j] >= 0) parent[right[j]] = (int32_t)j;
 }
 
-// 1. Transposition: one warp per warp of targets walks its list.  Counting pass (FILL = false) and filling pass.
+// A target at x clear of leaf nr (the forward's pair32x2_clear conditions): at least 1.5 bounding radii from its
+// centre, outside the core test's reach (MODEL != 0), within FP32's range.
+__device__ __forceinline__ bool adj_clear(double x0, double x1, double x2, const NodeRec &nr, int model, float near2) {
+    const double rx = x0 - nr.cx, ry = x1 - nr.cy, rz = x2 - nr.cz;
+    const double r2 = rx * rx + ry * ry + rz * rz;
+    const bool core = model == 0 || sqrt(r2) - nr.bound > 1.01 * sqrt((double)near2) * nr.clear_core;
+    return core && r2 >= 2.25 * nr.bound * nr.bound && r2 > 1e-16 && r2 < 1e18 && nr.bound < 1e9 &&
+           fabs(x0) < 1e30 && fabs(x1) < 1e30 && fabs(x2) < 1e30;
+}
+
+// 1. Transposition: one warp per warp of targets walks its list.  Counting pass (FILL = false) and filling pass; in
+// the filling pass a near leaf's clear targets (adj_clear) fill its list from the front and the others from the back,
+// so that its work items of NEAR_TARGETS are all clear but one.
 template <bool FILL>
-__global__ void transpose_kernel(TreeLists L, int *far_count, int *near_count, const int64_t *far_off,
-                                 const int64_t *near_off, int32_t *far_items, int32_t *near_items) {
+__global__ void transpose_kernel(TreeLists L, int *far_count, int *near_count, int *near_back, const int64_t *far_off,
+                                 const int64_t *near_off, int32_t *far_items, int32_t *near_items,
+                                 const NodeRec *nodes, const double *points, int model, float near2) {
     const int lane = threadIdx.x & 31;
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (gw >= L.target_warps) return;
@@ -149,10 +163,25 @@ __global__ void transpose_kernel(TreeLists L, int *far_count, int *near_count, c
         const int node = e.x & ~FAR_BIT;
         unsigned mask = (unsigned)e.y;
         const int c = __popc(mask);
+        if (FILL && !far) {
+            const NodeRec nr = nodes[node];
+            int32_t *dst = near_items + near_off[node];
+            const int64_t total = near_off[node + 1] - near_off[node];
+            while (mask) {
+                const int l = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const int64_t p = L.perm[gw * 32 + l];
+                const bool clear = adj_clear(points[3 * p], points[3 * p + 1], points[3 * p + 2], nr, model, near2);
+                const int64_t at = clear ? atomicAdd(near_count + node, 1)
+                                         : total - 1 - atomicAdd(near_back + node, 1);
+                dst[at] = (int32_t)(gw * 32 + l);
+            }
+            continue;
+        }
         int *cnt = far ? far_count + node : near_count + node;
         const int base = atomicAdd(cnt, c);
         if (FILL) {
-            int32_t *dst = far ? far_items + far_off[node] : near_items + near_off[node];
+            int32_t *dst = far_items + far_off[node];
             for (int q = 0; mask; ++q) {
                 const int l = __ffs(mask) - 1;
                 mask &= mask - 1;
@@ -242,6 +271,7 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
     using T = typename std::conditional<PREC == 0, double, float>::type;  // the sums' type: FP64 in FP64 mode
     __shared__ float4 shi[NEAR_TARGETS], slo[NEAR_TARGETS];  // two-float target: (hi x, y, z, w_x), (lo x, y, z, w_y)
     __shared__ float sw2[NEAR_TARGETS];                      // w_z
+    __shared__ float4 srel[NEAR_TARGETS];                    // x - O (leaf centre), FP32
     __shared__ T sacc[3][NEAR_TARGETS];
     __shared__ int sp[NEAR_TARGETS];
     __shared__ long long se0[NEAR_TARGETS], se1[NEAR_TARGETS];
@@ -255,6 +285,8 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
         const int64_t leaf = item_node(a.near_item_off, a.count, item);
         const int64_t first = a.near_off[leaf] + (item - a.near_item_off[leaf]) * NEAR_TARGETS;
         const int nt = (int)std::min<int64_t>(NEAR_TARGETS, a.near_off[leaf + 1] - first);
+        const NodeRec nr = a.nodes[leaf];
+        bool wide = true;  // this target is clear of the leaf: its pairs take pair_vjp32_clear (pair32x2_clear's test)
         if (tid < nt) {
             const int p = a.perm[a.near_items[first + tid]];
             sp[tid] = p;
@@ -268,14 +300,28 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
             sw2[tid] = (float)a.cot[3 * (int64_t)p + 2];
             se0[tid] = a.ex_ptr ? a.ex_ptr[p] : 0;
             se1[tid] = a.ex_ptr ? a.ex_ptr[p + 1] : 0;
+            const double x0 = a.points[3 * (int64_t)p], x1 = a.points[3 * (int64_t)p + 1],
+                         x2 = a.points[3 * (int64_t)p + 2];
+            wide = adj_clear(x0, x1, x2, nr, MODEL, a.near2);
+            srel[tid] = make_float4((float)(x0 - nr.cx), (float)(x1 - nr.cy), (float)(x2 - nr.cz), 0.0f);
         }
-        __syncthreads();
-        const NodeRec nr = a.nodes[leaf];
+        // every target of the item clear: the item's pairs take the clear form (uniform over the block); the barrier
+        // also publishes the targets staged above
+        const int all_wide = __syncthreads_and(wide);
+        const bool clear_all = PREC != 0 && a.seg32c2 && all_wide;
         for (int base = nr.lo; base < nr.hi; base += NEAR_THREADS) {
             const int s = base + tid;
             const bool valid = s < nr.hi;
             Seg32 r{};
-            if (valid && PREC != 0) r = a.seg32[s];
+            ClearSeg cq{};
+            if (valid && PREC != 0) {
+                if (clear_all) {
+                    const float *half = reinterpret_cast<const float *>(a.seg32c2 + (s >> 1)) + (s & 1);
+                    cq = ClearSeg{half[0], half[2], half[4], half[6], half[8], half[10], half[12], half[14]};
+                } else {
+                    r = a.seg32[s];
+                }
+            }
             T sg[7] = {0, 0, 0, 0, 0, 0, 0};
             for (int g0 = 0; g0 < nt; g0 += 32) {
                 T tacc0 = 0, tacc1 = 0, tacc2 = 0;
@@ -288,8 +334,14 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
                         if (PREC != 0) {
                             float f1[3], f2[3], fg = 0.f;
                             const float4 th = shi[t], tl = slo[t];
-                            need64 = pair_vjp32<MODEL>(th.x, th.y, th.z, tl.x, tl.y, tl.z, r, th.w, tl.w, sw2[t],
-                                                       a.near2, f1, f2, fg);
+                            if (clear_all) {
+                                const float4 tr = srel[t];
+                                pair_vjp32_clear<MODEL>(tr.x, tr.y, tr.z, cq, th.w, tl.w, sw2[t], f1, f2, fg);
+                                need64 = false;
+                            } else {
+                                need64 = pair_vjp32<MODEL>(th.x, th.y, th.z, tl.x, tl.y, tl.z, r, th.w, tl.w, sw2[t],
+                                                           a.near2, f1, f2, fg);
+                            }
                             if (!need64) {
                                 for (int k = 0; k < 3; ++k) { g1[k] = (T)f1[k]; g2[k] = (T)f2[k]; }
                                 gg = (T)fg;
@@ -689,14 +741,14 @@ extern "C" int bs_tree_adjoint(bs_ctx *ctx, const bs_sources *src, const bs_tree
         double *gseg = scratch.get<double>((size_t)7 * m);
         double *gx = grad_points ? grad_points : scratch.get<double>((size_t)3 * n);
         int32_t *parent = scratch.get<int32_t>(K), *leaf_of = scratch.get<int32_t>(m);
-        int *counts = scratch.get<int>((size_t)2 * K);
+        int *counts = scratch.get<int>((size_t)3 * K);  // far, near (front), near (back)
         int64_t *offs = scratch.get<int64_t>((size_t)4 * (K + 1));
         int64_t *d_totals = scratch.get<int64_t>(4);
         unsigned long long *queue = scratch.get<unsigned long long>(2);
         if (rc == BS_OK && (!raw || !G || !gseg || !gx || !parent || !leaf_of || !counts || !offs || !d_totals ||
                             !queue))
             rc = scratch.status;
-        int *far_count = counts, *near_count = counts + K;
+        int *far_count = counts, *near_count = counts + K, *near_back = counts + 2 * K;
         int64_t *far_off = offs, *near_off = offs + (K + 1), *far_item_off = offs + 2 * (K + 1),
                 *near_item_off = offs + 3 * (K + 1);
         AdjArgs a{};
@@ -715,6 +767,7 @@ extern "C" int bs_tree_adjoint(bs_ctx *ctx, const bs_sources *src, const bs_tree
             a.near2 = (float)(kp->near_cores * kp->near_cores);
             a.nodes = tree->nodes;
             a.seg32 = tree->seg32;
+            a.seg32c2 = tree->seg32c2;
             a.seg64 = tree->seg64;
             a.order32 = tree->order32;
             a.starts = src->starts;
@@ -742,7 +795,8 @@ extern "C" int bs_tree_adjoint(bs_ctx *ctx, const bs_sources *src, const bs_tree
             parent_of_kernel<<<blocks(K, 256), 256, 0, s>>>(K, tree->left, tree->right, parent);
             const unsigned tgrid = blocks(lists.target_warps * 32, 256);
             transpose_kernel<false><<<tgrid, 256, 0, s>>>(lists, far_count, near_count, nullptr, nullptr, nullptr,
-                                                          nullptr);
+                                                          nullptr, nullptr, tree->nodes, tgt->points, kp->model,
+                                                          (float)(kp->near_cores * kp->near_cores));
             transpose_scan_kernel<<<1, 1024, 0, s>>>(K, far_count, near_count, far_off, near_off, far_item_off,
                                                      near_item_off, d_totals);
             cudaError_t le = cudaGetLastError();
@@ -774,8 +828,10 @@ extern "C" int bs_tree_adjoint(bs_ctx *ctx, const bs_sources *src, const bs_tree
             a.near_total = totals[3];
             const unsigned tgrid = blocks(lists.target_warps * 32, 256);
             // the counts come back to the filled lengths: the far counts then mark the nodes with cotangents
-            transpose_kernel<true><<<tgrid, 256, 0, s>>>(lists, far_count, near_count, far_off, near_off, far_items,
-                                                         near_items);
+            cudaMemsetAsync(near_back, 0, (size_t)K * sizeof(int), s);
+            transpose_kernel<true><<<tgrid, 256, 0, s>>>(lists, far_count, near_count, near_back, far_off, near_off,
+                                                         far_items, near_items, tree->nodes, tgt->points, kp->model,
+                                                         (float)(kp->near_cores * kp->near_cores));
             static const int near_resident = [] {
                 int r = 0;
                 return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, near_adjoint_kernel<1, 2>, NEAR_THREADS,
