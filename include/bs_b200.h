@@ -173,7 +173,10 @@ int bs_tree_export(const bs_tree *tree, int64_t *order, int64_t *lo, int64_t *hi
 int bs_tree_keys(const bs_tree *tree, uint64_t *keys, int64_t *sorted_order, bs_stream stream);
 
 /* Tree evaluation (vortex_tree.tree_velocity semantics, vortex_tree.py:508-568): per-target acceptance, DFS order,
- * exclusions force nodes open, leaves use the exact pair kernel.  far_counts (int64 [n]) may be NULL. */
+ * exclusions force nodes open, leaves use the exact pair kernel.  far_counts (int64 [n]) may be NULL.  On Morton trees
+ * in BS_MIXED or BS_FP32 a leaf opened for one target of a warp (32 sorted targets) is also summed exactly for the
+ * targets of that warp that accepted it as far (their far counts exclude it); median trees and BS_FP64 keep each
+ * target's own decisions. */
 int bs_tree_eval(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const bs_targets *tgt,
                  const bs_kernel_params *kp, double *out, int8_t *flags, int64_t *far_counts, bs_stream stream);
 
