@@ -504,7 +504,9 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
     __syncwarp();
     // One node for the lanes of `mask`: per-lane acceptance, then a far entry, a near-leaf entry or two pushed
     // children.  Returns false when the stack would overflow.
-    auto visit = [&](const int node, const unsigned mask, const NodeRec &nr) -> bool {
+    // This lane's decision at a node of `mask`: accept it as far (true) or open it.  Kept apart from the visit so that
+    // a step's two decisions (independent FP64 chains) overlap.
+    auto decide = [&](const unsigned mask, const NodeRec &nr) -> bool {
         const bool mine = (mask >> lane) & 1u;
         bool accept = false;
         if (mine) {
@@ -532,6 +534,10 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
             }
             if (exact) accept = false;  // a target summed exactly opens every node
         }
+        return accept;
+    };
+    auto visit = [&](const int node, const unsigned mask, const NodeRec &nr, bool accept) -> bool {
+        const bool mine = (mask >> lane) & 1u;
         unsigned farm = __ballot_sync(0xffffffffu, mine && accept);
         unsigned openm = mask & ~farm;
         const unsigned openers = __ballot_sync(0xffffffffu, mine && !accept && !exact);
@@ -608,13 +614,14 @@ __global__ void __launch_bounds__(128) tree_walk_kernel(EvalArgs a) {
             top -= 2;
             const NodeRec nx = a.tv.nodes[x.x], ny = a.tv.nodes[y.x];
             __syncwarp();
-            if (!visit(x.x, (unsigned)x.y, nx)) break;
-            if (!visit(y.x, (unsigned)y.y, ny)) break;
+            const bool ax = decide((unsigned)x.y, nx), ay = decide((unsigned)y.y, ny);
+            if (!visit(x.x, (unsigned)x.y, nx, ax)) break;
+            if (!visit(y.x, (unsigned)y.y, ny, ay)) break;
         } else {
             const int2 x = stack[--top];
             const NodeRec nx = a.tv.nodes[x.x];
             __syncwarp();
-            if (!visit(x.x, (unsigned)x.y, nx)) break;
+            if (!visit(x.x, (unsigned)x.y, nx, decide((unsigned)x.y, nx))) break;
         }
         __syncwarp();
     }
