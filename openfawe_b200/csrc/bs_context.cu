@@ -100,6 +100,7 @@ extern "C" void bs_destroy(bs_ctx *ctx) {
     bs_upload_release(ctx);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
     cudaMemPoolDestroy(ctx->pool);
     delete ctx;
 }

@@ -99,7 +99,21 @@ struct bs_ctx {
     bs_upload_ring *upload = nullptr;
     cudaStream_t copy_stream = nullptr;  // host-array uploads that overlap work on the caller's stream
     cudaStream_t side_stream = nullptr;  // tree sums: the target sort and the far records, beside the caller's stream
+    // 64 words of pinned host memory for small read-backs (words 0-7: a build's node count, 8-15: an evaluation's
+    // counters), so that those copies are asynchronous: one call at a time per context
+    unsigned long long *pinned = nullptr;
 };
+
+// The context's pinned words (allocated on first use; null if the allocation failed: callers then copy through
+// pageable memory, synchronously).
+inline unsigned long long *ctx_pinned(bs_ctx *ctx) {
+    if (!ctx->pinned) {
+        void *p = nullptr;
+        if (cudaHostAlloc(&p, 64 * sizeof(unsigned long long), cudaHostAllocDefault) == cudaSuccess)
+            ctx->pinned = static_cast<unsigned long long *>(p);
+    }
+    return ctx->pinned;
+}
 
 // ---------------------------------------------------------------------------------------------------------------------
 // Device records.

@@ -41,6 +41,8 @@ struct bs_tree {
     bs::Far32z *far32z = nullptr;
     int order3 = 0, order4 = 0, order5 = 0;
     bool geo_sorted = false;  // the build's segment geometry (SegGeo) is in tree order (Morton trees)
+    bool records_done = false;  // the tree-ordered segment records are queued (segment_records)
+    int64_t *host_count = nullptr;  // pinned word the node count is read back into (null: a pageable word)
     bs::Seg64 *seg64 = nullptr;  // tree order
     bs::Seg32 *seg32 = nullptr;  // tree order
     bs::Seg32x2 *seg32x2 = nullptr;  // tree order, consecutive pairs

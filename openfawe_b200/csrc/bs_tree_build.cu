@@ -321,13 +321,20 @@ static int topology_from_sorted(bs_tree *t, const uint64_t *keys, int wake_shift
     BS_CHECK_LAUNCH("karras");
     int rc = scan_exclusive(slot, slot, m - 1, total, scratch, s);
     if (rc != BS_OK) return rc;
-    int64_t count = 0;
-    BS_CUDA(cudaMemcpyAsync(&count, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    if (while_counting) {
-        rc = while_counting();
-        if (rc != BS_OK) return rc;
-    }
-    BS_CUDA(cudaStreamSynchronize(s));
+    // the count travels back into a pinned word (asynchronously) while the hook queues work that does not need it;
+    // the host then waits for the count alone, not for what the hook queued behind it
+    int64_t local = 0;
+    int64_t *dst = t->host_count ? t->host_count : &local;
+    BS_CUDA(cudaMemcpyAsync(dst, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    cudaEvent_t counted = nullptr;
+    BS_CUDA(cudaEventCreateWithFlags(&counted, cudaEventDisableTiming));
+    cudaError_t ce = cudaEventRecord(counted, s);
+    if (ce == cudaSuccess && while_counting) rc = while_counting();
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(counted);
+    cudaEventDestroy(counted);
+    if (ce != cudaSuccess) return cuda_fail(ce, "node count");
+    if (rc != BS_OK) return rc;
+    const int64_t count = *dst;
     t->count = count;
     t->lo = t->alloc<int64_t>(count, s);
     t->hi = t->alloc<int64_t>(count, s);
@@ -1962,9 +1969,11 @@ int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_
 
 using namespace bs;
 
-// Shared tail of both constructors: inverse permutation, int64 order, tree-ordered segment records, moments.
-static int finish_tree(bs_tree *t, const bs_sources *src, const SegGeo *geo, Scratch &scratch, cudaStream_t s,
-                       cudaStream_t side = nullptr) {
+// The inverse permutation, the int64 order and the tree-ordered segment records: everything of a tree sized by its
+// segments, not its nodes (queued while a Morton tree's node count travels back).  Once.
+static int segment_records(bs_tree *t, const bs_sources *src, cudaStream_t s, cudaStream_t side) {
+    if (t->records_done) return BS_OK;
+    t->records_done = true;
     const int64_t m = t->m;
     if (!t->order) t->order = t->alloc<int64_t>(m, s);
     t->inverse = t->alloc<int32_t>(m, s);
@@ -1986,8 +1995,15 @@ static int finish_tree(bs_tree *t, const bs_sources *src, const SegGeo *geo, Scr
         cudaStreamWaitEvent(ps, ready, 0);
         cudaEventDestroy(ready);
     }
-    int rc = pack_segments(src, t->order32, t->seg64, t->seg32, nullptr, ps, t->seg32x2);
+    return pack_segments(src, t->order32, t->seg64, t->seg32, nullptr, ps, t->seg32x2);
+}
+
+// Shared tail of both constructors: the segment records (unless already queued), then the moments.
+static int finish_tree(bs_tree *t, const bs_sources *src, const SegGeo *geo, Scratch &scratch, cudaStream_t s,
+                       cudaStream_t side = nullptr) {
+    int rc = segment_records(t, src, s, side);
     if (rc != BS_OK) return rc;
+    const bool bottom_up = t->order4 || t->kind == BS_TREE_MORTON;
     return compute_moments(t, geo, scratch, s, bottom_up ? side : nullptr);
 }
 
@@ -2067,11 +2083,21 @@ int tree_build(bs_ctx *ctx, const bs_sources *src, const bs_tree_params *tp, bs_
         SegGeo *geo = defer ? t->alloc<SegGeo>(src->m, s) : scratch.get<SegGeo>(src->m);
         rc = geo ? BS_OK : (defer ? BS_ERR_OOM : scratch.status);
         if (rc == BS_OK && tp->kind == BS_TREE_MORTON) {
-            rc = build_morton(t, src, scratch, s, gate);
-            if (rc == BS_OK) rc = gate();
-            // the moment pipeline's geometry in tree order: every leaf reads a contiguous range
-            if (rc == BS_OK) rc = pack_segments(src, t->order32, nullptr, nullptr, geo, s);
-            t->geo_sorted = true;
+            // while the node count travels back: the caller's hook, the moment pipeline's geometry in tree order
+            // (every leaf reads a contiguous range) and the segment records, none of which needs the count
+            bool early_ran = false;
+            auto early = [&]() -> int {
+                if (early_ran) return BS_OK;
+                early_ran = true;
+                int r = gate();
+                if (r == BS_OK) r = pack_segments(src, t->order32, nullptr, nullptr, geo, s);
+                t->geo_sorted = true;
+                if (r == BS_OK) r = segment_records(t, src, s, defer);
+                return r;
+            };
+            t->host_count = reinterpret_cast<int64_t *>(ctx_pinned(ctx));
+            rc = build_morton(t, src, scratch, s, early);
+            if (rc == BS_OK) rc = early();  // (a tree of one leaf has no count to wait for)
         } else if (rc == BS_OK) {
             rc = gate();
             if (rc == BS_OK) rc = pack_segments(src, nullptr, nullptr, nullptr, geo, s);

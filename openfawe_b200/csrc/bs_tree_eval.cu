@@ -1483,11 +1483,15 @@ int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const b
     cudaEventRecord(e1, s);
     unsigned long long host[7] = {0, 0, 0, 0, 0, 0, 0};
     cudaError_t le = cudaSuccess;
-    // the sort-fault flag travels back with the counters: one round trip
+    // the sort-fault flag travels back with the counters: one round trip, into the context's pinned words when it has
+    // them (an asynchronous copy), copied out at once (a retry below runs this function again)
     const int *fault = sort_fault_flag();
+    unsigned long long *pinned = ctx_pinned(ctx);
+    unsigned long long *landing = pinned ? pinned + 8 : host;
     if (rc == BS_OK && fault) le = cudaMemcpyAsync(state + 6, fault, sizeof(int), cudaMemcpyDeviceToDevice, s);
-    if (rc == BS_OK && le == cudaSuccess) le = cudaMemcpyAsync(host, state, sizeof host, cudaMemcpyDeviceToHost, s);
+    if (rc == BS_OK && le == cudaSuccess) le = cudaMemcpyAsync(landing, state, sizeof host, cudaMemcpyDeviceToHost, s);
     if (le == cudaSuccess) le = cudaStreamSynchronize(s);
+    if (rc == BS_OK && le == cudaSuccess && landing != host) memcpy(host, landing, sizeof host);
     float ms = 0.f, walk_ms = 0.f, list_ms = 0.f, far_ms = 0.f;
     if (rc == BS_OK && le == cudaSuccess) {
         cudaEventElapsedTime(&ms, e0, e1);
