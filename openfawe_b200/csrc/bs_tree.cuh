@@ -51,7 +51,9 @@ struct bs_tree {
     int32_t *wake_root = nullptr;  // forests: root node of each wake (-1 for a wake without segments)
     int nwakes = 0;
     float build_ms = 0.f, moments_ms = 0.f;
-    cudaEvent_t marks[3] = {nullptr, nullptr, nullptr};  // build start, moments start, moments end
+    // build start, moments start, moments end; with the moments on a side stream also the end of the leaf pass (the
+    // segment and clear-leaf records complete: what the near-leaf list kernel reads)
+    cudaEvent_t marks[4] = {nullptr, nullptr, nullptr, nullptr}; 
     // marks[2] when the far records are still being computed on a side stream after the build returned (the node
     // records are complete): work that reads them waits for it; else null
     cudaEvent_t moments_done = nullptr;

@@ -1867,6 +1867,8 @@ static int moments_bottom_up(bs_tree *t, const SegGeo *geo, Scratch &scratch, cu
         1, std::min<int64_t>((count + LW - 1) / LW, (int64_t)std::max(1, leaf_resident) * sms));
     leaf_moments_kernel<PARTS><<<moment_blocks, 32 * LW, 0, ms>>>(leaves, nleaves, t->lo, t->hi, geo_order, geo,
                                                                   t->centre, sums, t->seg64 ? t->seg32c2 : nullptr);
+    if (defer && cudaEventCreateWithFlags(&t->marks[3], cudaEventDisableTiming) == cudaSuccess)
+        cudaEventRecord(t->marks[3], ms);  // the records the near-leaf kernel reads are complete
     static const int climb_blocks = [] {  // resident blocks: one wave holds every climbing warp
         int r = 0;
         return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, bottom_up_kernel<PARTS>, 128, 0) == cudaSuccess ? r

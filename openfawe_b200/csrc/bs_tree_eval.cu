@@ -1071,6 +1071,7 @@ static inline unsigned nblocks(int64_t n, int t) { return (unsigned)((n + t - 1)
 // the list kernel waits for when the far records were still in computation (null: nothing to wait for).
 static thread_local cudaEvent_t *t_marks = nullptr;
 static thread_local cudaEvent_t t_far_ready = nullptr;
+static thread_local cudaEvent_t t_records_ready = nullptr;
 
 template <int PREC, int MODEL>
 static void launch_pair(unsigned walk_grid, int block, size_t smem, unsigned list_grid, int64_t target_warps,
@@ -1086,10 +1087,14 @@ static void launch_pair(unsigned walk_grid, int block, size_t smem, unsigned lis
     item_plan_kernel<<<1, 1024, 0, s>>>(target_warps, args.list_total, args.item_want, args.item_off,
                                         args.item_warp);
     item_bounds_kernel<<<(unsigned)((target_warps * 32 + 255) / 256), 256, 0, s>>>(args, target_warps);
-    if (t_far_ready) cudaStreamWaitEvent(s, t_far_ready, 0);
+    // the near-leaf kernel reads the segment and clear-leaf records, the far-node kernel the far records: each waits
+    // for its own (with a side stream the leaf pass ends before the climb and the far records)
+    if (t_records_ready) cudaStreamWaitEvent(s, t_records_ready, 0);
+    else if (t_far_ready) cudaStreamWaitEvent(s, t_far_ready, 0);
     if (t_marks) cudaEventRecord(t_marks[1], s);
     tree_list_kernel<PREC, MODEL, 0><<<list_grid, LIST_WARPS * 32, 0, s>>>(args, target_warps);
     if (t_marks) cudaEventRecord(t_marks[2], s);
+    if (t_records_ready && t_far_ready) cudaStreamWaitEvent(s, t_far_ready, 0);
     static const bool far_smem = cudaFuncSetAttribute(tree_list_kernel<PREC, MODEL, 1>,
                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                       (int)(LIST_WARPS * FAR_WARP_SMEM)) == cudaSuccess;
@@ -1252,6 +1257,7 @@ struct EvalPre {
     cudaEvent_t perm_ready = nullptr;
     cudaEvent_t far_ready = nullptr;
     const uint8_t *exact = nullptr;  // EvalArgs::exact
+    cudaEvent_t records_ready = nullptr;  // the segment and clear-leaf records complete (before far_ready), or null
 };
 
 // Everything the evaluation launches, on stream s, with scratch from `scratch` (pool or arena).  No host
@@ -1365,9 +1371,11 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     const unsigned list_grid = (unsigned)std::max<int64_t>(
         1, std::min<int64_t>(((int64_t)capacity + LIST_WARPS - 1) / LIST_WARPS, (int64_t)ctx->sm_count * 3));
     t_far_ready = args.deferred ? pre->far_ready : nullptr;
+    t_records_ready = args.deferred ? pre->records_ready : nullptr;
     launch_eval(kp->precision, kp->model, walk_grid, block, smem, list_grid, target_warps, nblocks(n, 256), s, args,
                 out, flags);
     t_far_ready = nullptr;
+    t_records_ready = nullptr;
     BS_CHECK_LAUNCH("tree evaluation");
     return BS_OK;
 }
@@ -1693,7 +1701,7 @@ extern "C" int bs_tree_sum_host(bs_ctx *ctx, const bs_sources *src, const bs_tre
             if (rc == BS_OK) rc = check_eval_args(ctx, tree, tp, &dtgt, kp, d_out, d_flags);
             if (rc == BS_OK && !sorted) rc = sort_targets_beside(ctx, &dtgt, perm, s, side, &sorted);
             if (rc == BS_OK) {
-                const EvalPre pre{perm, sorted, tree->moments_done};
+                const EvalPre pre{perm, sorted, tree->moments_done, nullptr, tree->marks[3]};
                 rc = eval_run(ctx, tree, tp, &dtgt, nullptr, 1, kp, d_out, d_flags, d_far, s, &pre);
             }
             if (tree) {
@@ -1890,7 +1898,7 @@ extern "C" int bs_tree_sum(bs_ctx *ctx, const bs_sources *src, const bs_tree_par
         if (rc == BS_OK) rc = check_eval_args(ctx, tree, tp, tgt, kp, out, flags);
         if (rc == BS_OK && !sorted) rc = sort_hook();  // (a build that returned before its hook ran)
         if (rc == BS_OK) {
-            const EvalPre pre{perm, sorted, tree->moments_done};
+            const EvalPre pre{perm, sorted, tree->moments_done, nullptr, tree->marks[3]};
             rc = eval_run(ctx, tree, tp, tgt, nullptr, 1, kp, out, flags, far_counts, s, &pre);
         }
         if (tree) {
