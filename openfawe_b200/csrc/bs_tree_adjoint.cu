@@ -323,6 +323,56 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
                 }
             }
             T sg[7] = {0, 0, 0, 0, 0, 0, 0};
+            if (PREC != 0 && clear_all) {
+                // the clear form, packed: two groups of 32 targets a pass (.x: g0 + .., .y: g0 + 32 + ..); a target
+                // past the item's end or excluded for this segment takes zero cotangent at a valid target's offset
+                const float L2 = cq.lx * cq.lx + cq.ly * cq.ly + cq.lz * cq.lz;
+                const float iL2 = valid && L2 > 0.0f ? 1.0f / L2 : 0.0f;
+                float sgf[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                for (int g0 = 0; g0 < nt; g0 += 64) {
+                    float2 tacc0 = make_float2(0.f, 0.f), tacc1 = tacc0, tacc2 = tacc0;
+                    for (int j = 0; j < 32; ++j) {
+                        const int tA = g0 + ((lane + j) & 31), tB = tA + 32;
+                        auto live = [&](int t) {
+                            return valid && t < nt &&
+                                   !(a.ex_ptr && se0[t] < se1[t] && position_excluded(a.ex_pos, se0[t], se1[t], s));
+                        };
+                        const bool okA = live(tA), okB = live(tB);
+                        const int iA = tA < nt ? tA : 0, iB = tB < nt ? tB : 0;
+                        const float4 rA = srel[iA], rB = srel[iB];
+                        const float2 w0 = make_float2(okA ? shi[iA].w : 0.f, okB ? shi[iB].w : 0.f);
+                        const float2 w1 = make_float2(okA ? slo[iA].w : 0.f, okB ? slo[iB].w : 0.f);
+                        const float2 w2 = make_float2(okA ? sw2[iA] : 0.f, okB ? sw2[iB] : 0.f);
+                        float2 f1[3], f2[3], fg;
+                        pair_vjp32_clear2<MODEL>(make_float2(rA.x, rB.x), make_float2(rA.y, rB.y),
+                                                 make_float2(rA.z, rB.z), cq, iL2, w0, w1, w2, f1, f2, fg);
+                        sgf[0] -= f1[0].x + f1[0].y; sgf[1] -= f1[1].x + f1[1].y; sgf[2] -= f1[2].x + f1[2].y;
+                        sgf[3] -= f2[0].x + f2[0].y; sgf[4] -= f2[1].x + f2[1].y; sgf[5] -= f2[2].x + f2[2].y;
+                        sgf[6] += fg.x + fg.y;
+                        // lane q owns targets g0 + q and g0 + 32 + q and receives their terms from lane (q - j) mod 32
+                        const int from = (lane - j) & 31;
+                        tacc0.x += __shfl_sync(0xffffffffu, f1[0].x + f2[0].x, from);
+                        tacc1.x += __shfl_sync(0xffffffffu, f1[1].x + f2[1].x, from);
+                        tacc2.x += __shfl_sync(0xffffffffu, f1[2].x + f2[2].x, from);
+                        tacc0.y += __shfl_sync(0xffffffffu, f1[0].y + f2[0].y, from);
+                        tacc1.y += __shfl_sync(0xffffffffu, f1[1].y + f2[1].y, from);
+                        tacc2.y += __shfl_sync(0xffffffffu, f1[2].y + f2[2].y, from);
+                    }
+                    if (g0 + lane < nt) {
+                        atomicAdd(&sacc[0][g0 + lane], (T)tacc0.x);
+                        atomicAdd(&sacc[1][g0 + lane], (T)tacc1.x);
+                        atomicAdd(&sacc[2][g0 + lane], (T)tacc2.x);
+                    }
+                    if (g0 + 32 + lane < nt) {
+                        atomicAdd(&sacc[0][g0 + 32 + lane], (T)tacc0.y);
+                        atomicAdd(&sacc[1][g0 + 32 + lane], (T)tacc1.y);
+                        atomicAdd(&sacc[2][g0 + 32 + lane], (T)tacc2.y);
+                    }
+                }
+                if (valid)
+                    for (int k = 0; k < 7; ++k) atomicAdd(&a.gseg[7 * (int64_t)s + k], (double)sgf[k]);
+                continue;
+            }
             for (int g0 = 0; g0 < nt; g0 += 32) {
                 T tacc0 = 0, tacc1 = 0, tacc2 = 0;
                 for (int j = 0; j < 32; ++j) {
@@ -725,7 +775,10 @@ extern "C" int bs_tree_adjoint(bs_ctx *ctx, const bs_sources *src, const bs_tree
     for (auto &e : ev) cudaEventCreate(&e);
     cudaEventRecord(ev[0], s);
     bs_tree *tree = nullptr;
-    int rc = tree_build(ctx, src, tp, &tree, s, false, {});
+    // the moment phase (and the segment records) on the side stream, beside the walk and the list transposition,
+    // which read neither; the kernels that do wait for them below
+    if (!ctx->side_stream) BS_CUDA(cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking));
+    int rc = tree_build(ctx, src, tp, &tree, s, false, {}, ctx->side_stream);
     if (rc != BS_OK) {
         for (auto &e : ev) cudaEventDestroy(e);
         return rc;
@@ -790,8 +843,6 @@ extern "C" int bs_tree_adjoint(bs_ctx *ctx, const bs_sources *src, const bs_tree
             a.gx = gx;
             a.gseg = gseg;
             a.queue = queue;
-            raw_moments_kernel<<<blocks(K, 128), 128, 0, s>>>(a, tree->m0, tree->m1, tree->m2, tree->far64x,
-                                                              tree->far64y, tree->far64z, raw);
             parent_of_kernel<<<blocks(K, 256), 256, 0, s>>>(K, tree->left, tree->right, parent);
             const unsigned tgrid = blocks(lists.target_warps * 32, 256);
             transpose_kernel<false><<<tgrid, 256, 0, s>>>(lists, far_count, near_count, nullptr, nullptr, nullptr,
@@ -846,6 +897,9 @@ extern "C" int bs_tree_adjoint(bs_ctx *ctx, const bs_sources *src, const bs_tree
                 1, std::min<int64_t>(totals[3], (int64_t)ctx->sm_count * near_resident));
             const unsigned far_grid = (unsigned)std::max<int64_t>(
                 1, std::min<int64_t>(totals[2], (int64_t)ctx->sm_count * far_resident));
+            if (tree->moments_done) cudaStreamWaitEvent(s, tree->moments_done, 0);  // moments and segment records
+            raw_moments_kernel<<<blocks(K, 128), 128, 0, s>>>(a, tree->m0, tree->m1, tree->m2, tree->far64x,
+                                                              tree->far64y, tree->far64z, raw);
             cudaEventRecord(ev[2], s);
             if (totals[3] > 0) {
                 if (kp->precision == BS_FP64) launch_near<0>(kp->model, near_grid, s, a);
