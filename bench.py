@@ -85,7 +85,60 @@ def parse():
                                                     "tree-adjoint"),
                    help="run one call kind alone, warmup + steps times, and print its counters (for profiler runs)")
     p.add_argument("--tree-only", action="store_const", const="tree", dest="only", help="the same as --only tree")
+    p.add_argument("--reference-gpu-leg", action="store_true", help=argparse.SUPPRESS)
     return p.parse_args()
+
+
+REF_INSTALL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "baseline", "_ref")
+
+
+def reference_gpu_leg(args):
+    """(Subprocess) the reference's own numba.cuda tree code (vortex_cuda_tree.cuda_tree_sum with the GPU build and
+    moments, vortex.py:58-116), installed under baseline/_ref, on the bench wake from host arrays, as its callers use
+    it: its production setting (theta 0.2, order 2, leaf 32; mixed with the GPU FP64 suspect pairs, and FP64) and
+    its equal-accuracy setting (theta 0.04); the first call of each compiles its kernels, the next three are timed."""
+    sys.path.insert(0, REF_INSTALL)
+    import torch
+    from openfawe.aero import vortex as RV, vortex_cuda_tree as RVCT
+    from openfawe_b200 import engine
+    case = workload(args.rows)
+    segments = [case[k] for k in ("starts", "directions", "lengths", "gamma", "radius")]
+    n = len(case["points"])
+    csr = (np.zeros(n + 1, dtype=np.int64), np.zeros(0, dtype=np.int64))
+    device = torch.device("cuda", 0)
+    src = engine.Sources(*segments, device)
+    tgt = engine.Targets(case["points"], None, device)
+    direct = engine.direct(src, tgt, case["model"], "raise", "fp64")[0].cpu().numpy()
+    out = {"implementation": "the reference's numba.cuda cuda_tree_sum (baseline/_ref), build='gpu', moments='gpu'",
+           "workload": config(case, args)["workload"]}
+    for theta, precision, suspect in ((0.2, "mixed", "gpu64"), (0.2, "fp64", "cpu"), (0.04, "mixed", "gpu64")):
+        tree = RV.TreeSettings(theta=theta, order=2, leaf_size=32, core_clearance=CLEARANCE)
+        cuda = RV.CudaSettings(precision, 128, suspect, moments="gpu", build="gpu")
+        times, u = [], None
+        for rep in range(4):
+            torch.cuda.synchronize()
+            tick = time.perf_counter()
+            u, _ = RVCT.cuda_tree_sum(case["points"], *segments, case["model"], csr, "raise", tree, cuda)
+            times.append((time.perf_counter() - tick) * 1e3)
+        out[f"theta_{theta}_{precision}"] = {
+            "ms_per_call": float(np.median(times[1:])), "first_call_ms": times[0],
+            "rel_l2_vs_fp64_direct": float(np.linalg.norm(u - direct) / np.linalg.norm(direct))}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def reference_gpu_measure():
+    """The reference's own GPU tree code on this GPU (reference_gpu_leg, in a process of its own so that nothing of
+    this library's drop-in touches its modules), when it is installed under baseline/_ref."""
+    if not os.path.isdir(os.path.join(REF_INSTALL, "openfawe")):
+        return {"unavailable": "the reference is not installed under baseline/_ref"}
+    try:
+        r = subprocess.run([sys.executable, os.path.abspath(__file__), "--reference-gpu-leg"], capture_output=True,
+                           text=True, timeout=900)
+        return json.loads(r.stdout.strip().splitlines()[-1]) if r.returncode == 0 else {
+            "unavailable": f"exit {r.returncode}: {r.stderr.strip().splitlines()[-1] if r.stderr.strip() else ''}"}
+    except Exception as exc:  # a failed leg is reported, not fatal
+        return {"unavailable": repr(exc)}
 
 
 def workload(rows):
@@ -587,6 +640,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.reference_gpu_leg:
+        return reference_gpu_leg(args)
     import torch
     from openfawe_b200 import engine, vortex_cuda_tree
 
@@ -799,6 +854,7 @@ def main():
             line["batch"] = batch_measure(device, args.theta, args.order)
             line["adjoint"] = adjoint_measure(device, args.theta, case)
             line["adjoint_fwd_ratio"] = line["adjoint"]["tree_adjoint"]["ratio_to_tree_forward"]
+            line["reference_gpu"] = reference_gpu_measure()
     if dist:
         line["target_sharded"] = sharded_measure(src, case, rank, world, device, args, dist)
         dist.barrier()
