@@ -701,6 +701,25 @@ static __device__ __noinline__ void far_order5_unit(float nx, float ny, float nz
     p5[2] += u2;
 }
 
+// far_order5_unit inlined: for records staged in shared memory, whose loads then stay shared-memory loads.
+template <bool STAGED>
+__device__ __forceinline__ void far_order5_unit_inline(float nx, float ny, float nz, const float4 *z5, float *p5) {
+    float u0 = 0.f, u1 = 0.f, u2 = 0.f;
+#pragma unroll 1
+    for (int i = 0; i < 3; ++i) {
+        float h[Z_ROW];
+#pragma unroll
+        for (int q = 0; q < Z_ROW / 4; ++q) {
+            const float4 x = rec_ld<STAGED>(z5 + (Z_ROW / 4) * i + q);
+            h[4 * q] = x.x; h[4 * q + 1] = x.y; h[4 * q + 2] = x.z; h[4 * q + 3] = x.w;
+        }
+        far_term5_row<float>(nx, ny, nz, 1.0f, 1.0f, 1.0f, 1.0f, h, i, u0, u1, u2);
+    }
+    p5[0] += u0;
+    p5[1] += u1;
+    p5[2] += u2;
+}
+
 // far_eval<float> reading the packed records (Far32: 12 float4, Far32x: 16 float4, Far32y: 28 float4, Far32z: 42
 // float4) in vector
 // loads, one group at a time where it is used, so that only one order's coefficients are live at once.  The terms are
@@ -790,7 +809,10 @@ __device__ __forceinline__ void far_eval32v(float rx, float ry, float rz, const 
                         }
                         far_term4_row<float>(nx, ny, nz, 1.0f, 1.0f, 1.0f, h, i, p4[0], p4[1], p4[2]);
                     }
-                    if (order >= 5) far_order5_unit<STAGED>(nx, ny, nz, z5, p5);
+                    if (order >= 5) {
+                        if constexpr (STAGED) far_order5_unit_inline<true>(nx, ny, nz, z5, p5);
+                        else far_order5_unit<false>(nx, ny, nz, z5, p5);
+                    }
                 }
             }
         }
