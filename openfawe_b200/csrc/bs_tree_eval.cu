@@ -1498,6 +1498,7 @@ int eval_run(bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp, const b
     unsigned long long *landing = pinned ? pinned + 8 : host;
     if (rc == BS_OK && fault) le = cudaMemcpyAsync(state + 6, fault, sizeof(int), cudaMemcpyDeviceToDevice, s);
     if (rc == BS_OK && le == cudaSuccess) le = cudaMemcpyAsync(landing, state, sizeof host, cudaMemcpyDeviceToHost, s);
+    scratch.release();  // stream-ordered frees, queued while the device still works (a retry takes its own scratch)
     if (le == cudaSuccess) le = cudaStreamSynchronize(s);
     if (rc == BS_OK && le == cudaSuccess && landing != host) memcpy(host, landing, sizeof host);
     float ms = 0.f, walk_ms = 0.f, list_ms = 0.f, far_ms = 0.f;
