@@ -89,7 +89,9 @@ typedef struct {
 } bs_stats;
 
 /* Context: one per device.  bs_init makes `device` current, probes it with a one-thread kernel (the reference's
- * available(), vortex_cuda.py:58-77) and creates the memory pool. */
+ * available(), vortex_cuda.py:58-77) and creates the memory pool.  A context serves one call at a time: its
+ * statistics, side stream, upload ring and pinned read-back words belong to the call in progress (host threads that
+ * call concurrently use a context each). */
 int bs_init(int device, bs_ctx **ctx);
 void bs_destroy(bs_ctx *ctx);
 /* Text of the last error on this thread (never NULL). */
