@@ -211,6 +211,10 @@ static constexpr double LAMB_A = 1.25643;
 static constexpr double LAMB_CUT = 2.821180356260211;   // sqrt(10 / 1.25643), OLAF's exponent cut-off
 static constexpr double LAMB_CUT2 = 7.959058602548491;  // 10 / 1.25643
 static constexpr double INV_FOUR_PI = 0.07957747154594767;  // 1 / (4 pi)
+// Without a core (MODEL 0) the single-precision pairs take FP64 within a quarter of the segment's length of the finite
+// segment: their offsets a = (x - s)/L carry ~1 ulp of |a|, and b = a - d inherits that absolute error, so near an
+// end point (or near the axis) the pair's relative error grows as eps / distance; beyond L/4 it stays below ~5 eps.
+static constexpr float NOCORE_NEAR2 = 0.0625f;  // (1/4)^2, units of L^2
 
 // The reference pair (vortex_numba.pair_velocity) on an FP64 record from the scaled offset a = (p - s)/L, t = a.d and
 // c = d x a.  Returns the flag; adds the velocity to (ux, uy, uz) only when the flag is ok.
@@ -308,12 +312,13 @@ __device__ __forceinline__ int pair64_at(double px, double py, double pz, const 
 //   u = (Gamma/L)/(4 pi) factor (|a| + |b|) / (|a| |b| (|a| |b| + a.b)) c.
 // hi.w holds 1/L (NaN for a core too small for FP32), lo.w (Gamma/L)/(4 pi), dir.w (L/rc)^2, 0 for no core.  Adds
 // the velocity to (ux, uy, uz) unless the pair needs FP64, which is returned as true: within sqrt(near2) core radii of
-// the finite segment, within 1e-4 L of its axis (the reference's "suspect" rule, vortex_cuda.py:123-124; a NaN 1/L
-// fails it too), or out of FP32's comfortable range -- the FP64 pair then decides value and flags exactly.  Where
-// a.b < 0, |a||b| + a.b = h^2 / (|a||b| - a.b) (|a x b| = |c|): no cancellation.  The common path has no
-// data-dependent branch; the core factor is computed only where it differs from 1 (Lamb-Oseen inside its cut-off,
-// Rankine and Vatistas inside one core radius).  MODEL: 0..5.  NEAR = false leaves out the "within sqrt(near2) core
-// radii" test, for callers that know every pair of the batch lies farther than that from its segment.
+// the finite segment (MODEL 0: within L/4 of it, NOCORE_NEAR2), within 1e-4 L of its axis (the reference's "suspect"
+// rule, vortex_cuda.py:123-124; a NaN 1/L fails it too), or out of FP32's comfortable range -- the FP64 pair then
+// decides value and flags exactly.  Where a.b < 0, |a||b| + a.b = h^2 / (|a||b| - a.b) (|a x b| = |c|): no
+// cancellation.  The common path has no data-dependent branch; the core factor is computed only where it differs
+// from 1 (Lamb-Oseen inside its cut-off, Rankine and Vatistas inside one core radius).  MODEL: 0..5.  NEAR = false
+// leaves out the "within sqrt(near2) core radii" (MODEL 0: "within L/4") test, for callers that know every pair of the
+// batch lies farther than that from its segment.
 template <int MODEL, bool NEAR = true>
 __device__ __forceinline__ bool pair32(float rx, float ry, float rz, const float4 &hi, const float4 &lo,
                                        const float4 &dir, float near2, float &ux, float &uy, float &uz) {
@@ -330,10 +335,10 @@ __device__ __forceinline__ bool pair32(float rx, float ry, float rz, const float
     const float dot = fmaf(ax, bx, fmaf(ay, by, az * bz));
     const float big2 = fmaxf(1.0f, fmaxf(na2, nb2));
     bool need64 = !(h2 > 1e-8f * big2) || !(big2 < 1e18f);
-    if (MODEL != 0 && NEAR) {
+    if (NEAR) {
         const float t = fmaf(az, dz, fmaf(ay, dy, ax * dx));
         const float seg2 = t < 0.0f ? na2 : (t > 1.0f ? nb2 : h2);  // distance^2 to the finite segment, units of L^2
-        need64 = need64 || (irc2 > 0.0f && seg2 * irc2 < near2);
+        need64 = need64 || (MODEL == 0 ? seg2 < NOCORE_NEAR2 : (irc2 > 0.0f && seg2 * irc2 < near2));
     }
     const float na = na2 * rsqrtf(na2), nb = nb2 * rsqrtf(nb2);
     const float product = na * nb;
@@ -417,13 +422,18 @@ __device__ __forceinline__ unsigned pair32x2(float2 txh, float2 tyh, float2 tzh,
     const float2 lim = mul2(make_float2(big0, big1), make_float2(1e-8f, 1e-8f));
     bool n0 = !(h2.x > lim.x) || !(big0 < 1e18f);
     bool n1 = !(h2.y > lim.y) || !(big1 < 1e18f);
-    if (MODEL != 0 && NEAR) {
+    if (NEAR) {
         const float2 t = fma2(az, dz, fma2(ay, dy, mul2(ax, dx)));
         const float2 seg2 = make_float2(t.x < 0.0f ? na2.x : (t.x > 1.0f ? nb2.x : h2.x),
                                         t.y < 0.0f ? na2.y : (t.y > 1.0f ? nb2.y : h2.y));
-        const float2 rr = mul2(seg2, w);
-        n0 = n0 || (w.x > 0.0f && rr.x < near2);
-        n1 = n1 || (w.y > 0.0f && rr.y < near2);
+        if (MODEL == 0) {
+            n0 = n0 || seg2.x < NOCORE_NEAR2;
+            n1 = n1 || seg2.y < NOCORE_NEAR2;
+        } else {
+            const float2 rr = mul2(seg2, w);
+            n0 = n0 || (w.x > 0.0f && rr.x < near2);
+            n1 = n1 || (w.y > 0.0f && rr.y < near2);
+        }
     }
     const float2 na = mul2(na2, make_float2(rsqrtf(na2.x), rsqrtf(na2.y)));
     const float2 nb = mul2(nb2, make_float2(rsqrtf(nb2.x), rsqrtf(nb2.y)));

@@ -94,10 +94,10 @@ __device__ __forceinline__ bool pair_vjp64(double x0, double x1, double x2, cons
 // length (a1 = r1 / L, a2 = r2 / L = a1 - d, as the forward's single-precision pair forms it, so that any length scale
 // stays in range), from the forward's Seg32 record (two-float start, 1/L, (Gamma/L)/(4 pi), direction, (L/rc)^2) and a
 // two-float target.  Returns true, and computes nothing, where the forward evaluates the pair in FP64: within
-// sqrt(near2) core radii of the finite segment, within 1e-4 L of its axis, or out of FP32's comfortable range (the
-// caller then takes pair_vjp64).  Otherwise g1 = d(w . u)/dr1, g2 = d(w . u)/dr2 and gg = d(w . u)/dGamma.  In units of
-// L the pair is u = (Gamma/L)/(4 pi) f S c / D with rho^2 = |c|^2 (L/rc)^2, and the one explicit dependence on L
-// through rho^2 gives the bb d terms (d(|B - A|^2)/dr1 = 2 (B - A)).
+// sqrt(near2) core radii of the finite segment (MODEL 0: within L/4 of it), within 1e-4 L of its axis, or out of
+// FP32's comfortable range (the caller then takes pair_vjp64).  Otherwise g1 = d(w . u)/dr1, g2 = d(w . u)/dr2 and
+// gg = d(w . u)/dGamma.  In units of L the pair is u = (Gamma/L)/(4 pi) f S c / D with rho^2 = |c|^2 (L/rc)^2, and
+// the one explicit dependence on L through rho^2 gives the bb d terms (d(|B - A|^2)/dr1 = 2 (B - A)).
 template <int MODEL>
 __device__ __forceinline__ bool pair_vjp32(float xh0, float xh1, float xh2, float xl0, float xl1, float xl2,
                                            const Seg32 &r, float w0, float w1, float w2, float near2, float *g1,
@@ -114,10 +114,10 @@ __device__ __forceinline__ bool pair_vjp32(float xh0, float xh1, float xh2, floa
     const float q1 = fmaf(a0, a0, fmaf(a1, a1, a2 * a2)), q2 = fmaf(b0, b0, fmaf(b1, b1, b2 * b2));
     const float big2 = fmaxf(1.0f, fmaxf(q1, q2));
     bool need64 = !(cc > 1e-8f * big2) || !(big2 < 1e18f);
-    if (MODEL != 0) {
+    {
         const float t = fmaf(a2, dz, fmaf(a1, dy, a0 * dx));
         const float seg2 = t < 0.0f ? q1 : (t > 1.0f ? q2 : cc);
-        need64 = need64 || (lrc2 > 0.0f && seg2 * lrc2 < near2);
+        need64 = need64 || (MODEL == 0 ? seg2 < NOCORE_NEAR2 : (lrc2 > 0.0f && seg2 * lrc2 < near2));
     }
     if (need64) return true;
     const float in1 = rsqrtf(q1), in2 = rsqrtf(q2);

@@ -323,15 +323,18 @@ __device__ __forceinline__ void leaf_pairs(const EvalArgs &a, const Target &t, c
     if (walk) while (e < e1 && a.ex_pos[e] < lo) ++e;
     float t0 = 0.f, t1 = 0.f, t2 = 0.f;
     // When every walking lane is farther from the leaf's bounding sphere than sqrt(near2) of its largest core radius
-    // (with a 1% margin for rounding), no pair of the leaf can need FP64 for its core: the pairs skip that test.  When
-    // moreover every walking lane lies at least 1.5 bounding radii from the leaf's centre (within FP32's range),
-    // the packed pairs take the clear-leaf form (pair32x2_clear).
+    // (with a 1% margin for rounding), no pair of the leaf can need FP64 for its core: the pairs skip that test.
+    // Without a core (MODEL 0) the test is "within L/4 of the segment", and a lane 1.5 bounding radii from the centre
+    // is at least half a radius, so L/4 (L <= 2 radii), from every segment.  When moreover every walking lane lies at
+    // least 1.5 bounding radii from the leaf's centre (within FP32's range), the packed pairs take the clear-leaf form
+    // (pair32x2_clear).
     bool clear = true, wide = true;
     float3 rel = make_float3(0.f, 0.f, 0.f);
     if (PREC != 0 && walk) {
         const double rx = t.x0 - nr.cx, ry = t.x1 - nr.cy, rz = t.x2 - nr.cz;
         const double r2 = rx * rx + ry * ry + rz * rz;
-        if (MODEL != 0) clear = sqrt(r2) - nr.bound > 1.01 * sqrt((double)a.near2) * nr.clear_core;
+        clear = MODEL != 0 ? sqrt(r2) - nr.bound > 1.01 * sqrt((double)a.near2) * nr.clear_core
+                           : r2 >= 2.25 * nr.bound * nr.bound;
         wide = clear && r2 >= 2.25 * nr.bound * nr.bound && r2 > 1e-16 && r2 < 1e18 && nr.bound < 1e9;
         rel = make_float3((float)rx, (float)ry, (float)rz);
     }

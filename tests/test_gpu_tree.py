@@ -594,3 +594,26 @@ def test_mixed_tree_far_field_at_any_length_scale(device):
     for order in (2, 4, 5):
         for scale in (1e-4, 1e4):
             assert errs[scale, order] <= 1.1 * errs[1.0, order] + 1e-7, errs
+
+
+@pytest.mark.parametrize("model", [0, 1, 2])
+def test_single_precision_near_field_every_packed_model(device, model):
+    """The packed near-field forms (the clear-leaf pair for targets 1.5 bounding radii out, pair32x2 nearer, the
+    scalar pair at the leaves' odd ends) for the no-core, Rankine and Lamb-Oseen models: a fifth-order Morton tree at
+    theta 0.1 and leaf 128 in mixed and FP32 against the FP64 direct sum.  The targets sit 0.011 m above the sheet's
+    nodes, 0.05 segment lengths from the nodes' segments: the cores' FP64 rule (3 core radii) covers them for models 1
+    and 2, the no-core rule (within L/4 of the segment) for model 0, which without it erred by 2.3e-6."""
+    from openfawe_b200 import engine, wakes
+    case = wakes.rotor_sheet(40, seed=21 + model, targets=2000)
+    args = wakes.backend_args(case)
+    src = engine.Sources(*args[1:6], device)
+    tgt = engine.Targets(case["points"], None, device)
+    ref, rflags = engine.direct(src, tgt, model, "zero", "fp64")
+    ref = ref.cpu().numpy()
+    assert not rflags.cpu().numpy().any()
+    tree = engine.build_tree(src, theta=0.1, order=5, leaf_size=128, kind="morton")
+    for precision, bound in (("mixed", 2e-8 if model == 0 else 3e-7), ("fp32", 5e-7)):
+        u, flags, _ = engine.tree_eval(tree, tgt, model, "zero", precision, theta=0.1, order=5)
+        rel = np.linalg.norm(u.cpu().numpy() - ref) / np.linalg.norm(ref)
+        assert rel <= bound and not flags.cpu().numpy().any(), (model, precision, rel)
+        assert engine.last_stats(device)["fp64_pairs"] > 0
