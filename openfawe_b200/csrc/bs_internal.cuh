@@ -513,11 +513,15 @@ __device__ __forceinline__ void pair32x2_clear(float2 tx, float2 ty, float2 tz, 
         const float2 r2 = mul2(h2, w);
         k = mul2(k, make_float2(fminf(r2.x, 1.0f), fminf(r2.y, 1.0f)));
     } else if (MODEL == 2) {  // Lamb-Oseen inside its cut-off: 1 - exp(-1.25643 (h / rc)^2)
+        // a clear target is seldom within the cut-off of a segment's line: the exponent is formed only when some
+        // lane of those evaluating the pair needs it (a vote over the active lanes; each lane's own test is in it)
         const float2 r2 = mul2(h2, w);
-        const float2 x = mul2(r2, make_float2(LAMB_A_LOG2E_NEG, LAMB_A_LOG2E_NEG));
-        const float2 f = fma2(make_float2(exp2_approx(x.x), exp2_approx(x.y)), make_float2(-1.0f, -1.0f),
-                              make_float2(1.0f, 1.0f));
-        k = mul2(k, make_float2(r2.x < (float)LAMB_CUT2 ? f.x : 1.0f, r2.y < (float)LAMB_CUT2 ? f.y : 1.0f));
+        if (__any_sync(__activemask(), r2.x < (float)LAMB_CUT2 || r2.y < (float)LAMB_CUT2)) {
+            const float2 x = mul2(r2, make_float2(LAMB_A_LOG2E_NEG, LAMB_A_LOG2E_NEG));
+            const float2 f = fma2(make_float2(exp2_approx(x.x), exp2_approx(x.y)), make_float2(-1.0f, -1.0f),
+                                  make_float2(1.0f, 1.0f));
+            k = mul2(k, make_float2(r2.x < (float)LAMB_CUT2 ? f.x : 1.0f, r2.y < (float)LAMB_CUT2 ? f.y : 1.0f));
+        }
     }
     const float2 coefficient = mul2(k, make_float2(__fdividef(1.0f, den.x), __fdividef(1.0f, den.y)));
     u0 = fma2(coefficient, cx, u0);

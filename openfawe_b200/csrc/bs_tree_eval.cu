@@ -23,6 +23,8 @@ namespace bs {
 constexpr int STACK_DEPTH = 128;
 constexpr int FAR_COST = 16;              // list cost units: one far evaluation ~ sixteen near pairs (measured)
 constexpr int LIST_WARPS = 4;             // warps per block of the list kernel
+constexpr int LIST_NEAR_BLOCKS = 4;       // near-leaf kernel blocks a SM (128 registers a thread)
+constexpr int LIST_FAR_BLOCKS = 3;        // far-node kernel blocks a SM (57.9 KB of shared memory each)
 constexpr int FAR_GROUPS = 4;             // open groups of disjoint far entries in the far list kernel
 constexpr int FAR_STAGE = 4;              // distinct nodes a group holds: their FP32 records are staged together
 constexpr int FAR_REC4 = 100;             // float4 of a staged node: FP32 far records to fifth order (12 + 16 + 28 +
@@ -847,7 +849,7 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
 // Three blocks per SM (up to 168 registers a thread): the packed pairs of a tile need the registers to interleave.
 // PART 0: near leaves (counter a.queue[0]); PART 1: far nodes (counter a.queue[2]; no tiles).
 template <int PREC, int MODEL, int PART>
-__global__ void __launch_bounds__(LIST_WARPS * 32, 3) tree_list_kernel(EvalArgs a, int64_t target_warps) {
+__global__ void __launch_bounds__(LIST_WARPS * 32, PART == 0 ? LIST_NEAR_BLOCKS : LIST_FAR_BLOCKS) tree_list_kernel(EvalArgs a, int64_t target_warps) {
     // near kernel: static tiles and entry buffers; far kernel: FAR_WARP_SMEM of dynamic shared memory a warp
     __shared__ __align__(16) unsigned char tile_mem[PART == 0 ? LIST_WARPS * 32 * sizeof(Seg64) : 16];
     __shared__ int2 entry_mem[PART == 0 ? LIST_WARPS * ENTRY_BUF : 1];
@@ -1077,7 +1079,7 @@ static thread_local cudaEvent_t t_far_ready = nullptr;
 static thread_local cudaEvent_t t_records_ready = nullptr;
 
 template <int PREC, int MODEL>
-static void launch_pair(unsigned walk_grid, int block, size_t smem, unsigned list_grid, int64_t target_warps,
+static void launch_pair(unsigned walk_grid, int block, size_t smem, uint2 list_grid, int64_t target_warps,
                         unsigned reduce_grid, cudaStream_t s, const EvalArgs &args, double *out, int8_t *flags) {
     // BS_WALK_POP=1 takes one stack entry per walk step (for comparisons); the default takes two
     static const int pop = [] {
@@ -1095,21 +1097,21 @@ static void launch_pair(unsigned walk_grid, int block, size_t smem, unsigned lis
     if (t_records_ready) cudaStreamWaitEvent(s, t_records_ready, 0);
     else if (t_far_ready) cudaStreamWaitEvent(s, t_far_ready, 0);
     if (t_marks) cudaEventRecord(t_marks[1], s);
-    tree_list_kernel<PREC, MODEL, 0><<<list_grid, LIST_WARPS * 32, 0, s>>>(args, target_warps);
+    tree_list_kernel<PREC, MODEL, 0><<<list_grid.x, LIST_WARPS * 32, 0, s>>>(args, target_warps);
     if (t_marks) cudaEventRecord(t_marks[2], s);
     if (t_records_ready && t_far_ready) cudaStreamWaitEvent(s, t_far_ready, 0);
     static const bool far_smem = cudaFuncSetAttribute(tree_list_kernel<PREC, MODEL, 1>,
                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                       (int)(LIST_WARPS * FAR_WARP_SMEM)) == cudaSuccess;
     (void)far_smem;  // a refusal shows as the launch's error
-    tree_list_kernel<PREC, MODEL, 1><<<list_grid, LIST_WARPS * 32, LIST_WARPS * FAR_WARP_SMEM, s>>>(args,
-                                                                                                   target_warps);
+    tree_list_kernel<PREC, MODEL, 1><<<list_grid.y, LIST_WARPS * 32, LIST_WARPS * FAR_WARP_SMEM, s>>>(args,
+                                                                                                     target_warps);
     if (t_marks) cudaEventRecord(t_marks[3], s);
     tree_reduce_kernel<PREC><<<reduce_grid, 256, 0, s>>>(args, out, flags);
 }
 
 template <int PREC>
-static void launch_model(int model, unsigned walk_grid, int block, size_t smem, unsigned list_grid, int64_t tw,
+static void launch_model(int model, unsigned walk_grid, int block, size_t smem, uint2 list_grid, int64_t tw,
                          unsigned reduce_grid, cudaStream_t s, const EvalArgs &args, double *out, int8_t *flags) {
     switch (model) {
         case 0: launch_pair<PREC, 0>(walk_grid, block, smem, list_grid, tw, reduce_grid, s, args, out, flags); break;
@@ -1122,7 +1124,7 @@ static void launch_model(int model, unsigned walk_grid, int block, size_t smem, 
 }
 
 // FP64 evaluates the core model at run time (one instantiation); the single precisions are specialised per model.
-static void launch_eval(int precision, int model, unsigned walk_grid, int block, size_t smem, unsigned list_grid,
+static void launch_eval(int precision, int model, unsigned walk_grid, int block, size_t smem, uint2 list_grid,
                         int64_t tw, unsigned reduce_grid, cudaStream_t s, const EvalArgs &args, double *out,
                         int8_t *flags) {
     if (precision == BS_FP64) launch_pair<0, 0>(walk_grid, block, smem, list_grid, tw, reduce_grid, s, args, out, flags);
@@ -1371,8 +1373,11 @@ int eval_enqueue(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *t
     args.queue = queue;
     const size_t smem = (size_t)(block / 32) * (STACK_DEPTH * sizeof(int2) + 32 * sizeof(Seg64));
     const unsigned walk_grid = (unsigned)((target_warps + block / 32 - 1) / (block / 32));
-    const unsigned list_grid = (unsigned)std::max<int64_t>(
-        1, std::min<int64_t>(((int64_t)capacity + LIST_WARPS - 1) / LIST_WARPS, (int64_t)ctx->sm_count * 3));
+    // persistent blocks (they take items from a counter): one wave of each list kernel, no more than the items need
+    const int64_t list_cap = ((int64_t)capacity + LIST_WARPS - 1) / LIST_WARPS;
+    const uint2 list_grid = make_uint2(
+        (unsigned)std::max<int64_t>(1, std::min<int64_t>(list_cap, (int64_t)ctx->sm_count * LIST_NEAR_BLOCKS)),
+        (unsigned)std::max<int64_t>(1, std::min<int64_t>(list_cap, (int64_t)ctx->sm_count * LIST_FAR_BLOCKS)));
     t_far_ready = args.deferred ? pre->far_ready : nullptr;
     t_records_ready = args.deferred ? pre->records_ready : nullptr;
     launch_eval(kp->precision, kp->model, walk_grid, block, smem, list_grid, target_warps, nblocks(n, 256), s, args,
