@@ -232,12 +232,15 @@ __device__ __forceinline__ void pair_vjp32_clear(float rx, float ry, float rz, c
 // pair_vjp32_clear for two targets of the same segment at once (f32x2: .x and .y), one packed operation for both in
 // every add, multiply and FMA; special functions and the core factor's branches per half.  iL2 = 1/|l|^2 from the
 // caller (0 for a thread without a segment, whose targets carry zero cotangents).  A half with zero cotangent gives
-// zero gradients as long as its offset is a clear target's.
+// zero gradients as long as its offset is a clear target's.  The lanes evaluating the call vote on whether any of
+// their pairs lies inside the core factor's range ((h/rc)^2 below 1 for Rankine, below the cut-off for Lamb-Oseen);
+// a clear target seldom does, and then f = 1, df = 0 leave out the core terms (the same values, to the sign of a zero).
 template <int MODEL>
 __device__ __forceinline__ void pair_vjp32_clear2(float2 rx, float2 ry, float2 rz, const ClearSeg &q, float iL2,
                                                   float2 w0, float2 w1, float2 w2, float2 *g1, float2 *g2,
                                                   float2 &gg) {
     auto bc = [](float v) { return make_float2(v, v); };
+    auto neg = [](float2 v) { return make_float2(-v.x, -v.y); };
     const float2 lx = bc(q.lx), ly = bc(q.ly), lz = bc(q.lz), nlx = bc(-q.lx), nly = bc(-q.ly), nlz = bc(-q.lz);
     const float2 a0 = add2(rx, bc(q.nsx)), a1 = add2(ry, bc(q.nsy)), a2 = add2(rz, bc(q.nsz));  // r1
     const float2 b0 = add2(a0, nlx), b1 = add2(a1, nly), b2 = add2(a2, nlz);                     // r2
@@ -249,28 +252,48 @@ __device__ __forceinline__ void pair_vjp32_clear2(float2 rx, float2 ry, float2 r
     const float2 dt = fma2(a0, b0, fma2(a1, b1, mul2(a2, b2)));
     const float2 P = mul2(n1, n2), D = mul2(P, add2(P, dt));
     const float2 iD = make_float2(__fdividef(1.0f, D.x), __fdividef(1.0f, D.y));
-    float2 f = bc(1.0f), df = bc(0.0f), rho2 = bc(0.0f);
-    if (MODEL != 0) {
-        rho2 = mul2(cc, bc(q.w));  // +inf or NaN without a core: f stays 1, df 0
-        auto core = [&](float r2, float &fo, float &dfo) {
-            if (MODEL == 1) {
-                if (r2 < 1.0f) { fo = r2; dfo = 1.0f; }
-            } else if (r2 <= (float)LAMB_CUT2) {
-                const float e = exp2_approx(r2 * LAMB_A_LOG2E_NEG);
-                fo = 1.0f - e;
-                dfo = (float)LAMB_A * e;
-            }
-        };
-        core(rho2.x, f.x, df.x);
-        core(rho2.y, f.y, df.y);
-    }
     const float2 S = add2(n1, n2);
     const float2 wc = fma2(w0, c0, fma2(w1, c1, mul2(w2, c2)));
     const float2 wciD = mul2(wc, iD);
     const float2 h = mul2(bc(q.gf), wciD);
+    float2 rho2 = bc(0.0f);  // +inf or NaN without a core: outside every range
+    bool inside = false;
+    if (MODEL != 0) {
+        rho2 = mul2(cc, bc(q.w));
+        const float lim = MODEL == 1 ? 1.0f : (float)LAMB_CUT2;
+        inside = __any_sync(__activemask(), MODEL == 1 ? (rho2.x < lim || rho2.y < lim)
+                                                       : (rho2.x <= lim || rho2.y <= lim));
+    }
+    if (!inside) {  // f = 1, df = 0
+        gg = mul2(bc((float)INV_FOUR_PI), mul2(S, wciD));
+        const float2 g_D = mul2(mul2(h, S), neg(iD));
+        const float2 g_P = mul2(g_D, fma2(bc(2.0f), P, dt)), g_dt = mul2(g_D, P);
+        const float2 k = mul2(bc(q.gf), mul2(S, iD));
+        const float2 gc0 = mul2(k, w0), gc1 = mul2(k, w1), gc2 = mul2(k, w2);
+        const float2 s1 = mul2(fma2(g_P, n2, h), in1), s2 = mul2(fma2(g_P, n1, h), in2);
+        g1[0] = fma2(s1, a0, fma2(g_dt, b0, fma2(b1, gc2, mul2(neg(b2), gc1))));
+        g1[1] = fma2(s1, a1, fma2(g_dt, b1, fma2(b2, gc0, mul2(neg(b0), gc2))));
+        g1[2] = fma2(s1, a2, fma2(g_dt, b2, fma2(b0, gc1, mul2(neg(b1), gc0))));
+        g2[0] = fma2(s2, b0, fma2(g_dt, a0, fma2(gc1, a2, mul2(neg(gc2), a1))));
+        g2[1] = fma2(s2, b1, fma2(g_dt, a1, fma2(gc2, a0, mul2(neg(gc0), a2))));
+        g2[2] = fma2(s2, b2, fma2(g_dt, a2, fma2(gc0, a1, mul2(neg(gc1), a0))));
+        return;
+    }
+    float2 f = bc(1.0f), df = bc(0.0f);
+    auto core = [&](float r2, float &fo, float &dfo) {
+        if (MODEL == 1) {
+            if (r2 < 1.0f) { fo = r2; dfo = 1.0f; }
+        } else if (r2 <= (float)LAMB_CUT2) {
+            const float e = exp2_approx(r2 * LAMB_A_LOG2E_NEG);
+            fo = 1.0f - e;
+            dfo = (float)LAMB_A * e;
+        }
+    };
+    core(rho2.x, f.x, df.x);
+    core(rho2.y, f.y, df.y);
     gg = mul2(mul2(bc((float)INV_FOUR_PI), f), mul2(S, wciD));
     const float2 hf = mul2(h, f);
-    const float2 g_S = hf, g_D = mul2(mul2(hf, S), make_float2(-iD.x, -iD.y));
+    const float2 g_S = hf, g_D = mul2(mul2(hf, S), neg(iD));
     const float2 g_rho2 = mul2(mul2(h, S), df);
     const float2 g_cc = make_float2(df.x != 0.0f ? g_rho2.x * q.w : 0.0f, df.y != 0.0f ? g_rho2.y * q.w : 0.0f);
     const float2 g_P = mul2(g_D, fma2(bc(2.0f), P, dt)), g_dt = mul2(g_D, P);
@@ -280,14 +303,14 @@ __device__ __forceinline__ void pair_vjp32_clear2(float2 rx, float2 ry, float2 r
     const float2 s1 = mul2(fma2(g_P, n2, g_S), in1), s2 = mul2(fma2(g_P, n1, g_S), in2);
     const float2 bb = make_float2(df.x != 0.0f ? 2.0f * g_rho2.x * rho2.x * iL2 : 0.0f,
                                   df.y != 0.0f ? 2.0f * g_rho2.y * rho2.y * iL2 : 0.0f);
-    const float2 nbb = make_float2(-bb.x, -bb.y);
+    const float2 nbb = neg(bb);
     // g1 = s1 r1 + g_dt r2 + r2 x gc - bb l;  g2 = s2 r2 + g_dt r1 + gc x r1 + bb l
-    g1[0] = fma2(s1, a0, fma2(g_dt, b0, fma2(b1, gc2, fma2(make_float2(-b2.x, -b2.y), gc1, mul2(nbb, lx)))));
-    g1[1] = fma2(s1, a1, fma2(g_dt, b1, fma2(b2, gc0, fma2(make_float2(-b0.x, -b0.y), gc2, mul2(nbb, ly)))));
-    g1[2] = fma2(s1, a2, fma2(g_dt, b2, fma2(b0, gc1, fma2(make_float2(-b1.x, -b1.y), gc0, mul2(nbb, lz)))));
-    g2[0] = fma2(s2, b0, fma2(g_dt, a0, fma2(gc1, a2, fma2(make_float2(-gc2.x, -gc2.y), a1, mul2(bb, lx)))));
-    g2[1] = fma2(s2, b1, fma2(g_dt, a1, fma2(gc2, a0, fma2(make_float2(-gc0.x, -gc0.y), a2, mul2(bb, ly)))));
-    g2[2] = fma2(s2, b2, fma2(g_dt, a2, fma2(gc0, a1, fma2(make_float2(-gc1.x, -gc1.y), a0, mul2(bb, lz)))));
+    g1[0] = fma2(s1, a0, fma2(g_dt, b0, fma2(b1, gc2, fma2(neg(b2), gc1, mul2(nbb, lx)))));
+    g1[1] = fma2(s1, a1, fma2(g_dt, b1, fma2(b2, gc0, fma2(neg(b0), gc2, mul2(nbb, ly)))));
+    g1[2] = fma2(s1, a2, fma2(g_dt, b2, fma2(b0, gc1, fma2(neg(b1), gc0, mul2(nbb, lz)))));
+    g2[0] = fma2(s2, b0, fma2(g_dt, a0, fma2(gc1, a2, fma2(neg(gc2), a1, mul2(bb, lx)))));
+    g2[1] = fma2(s2, b1, fma2(g_dt, a1, fma2(gc2, a0, fma2(neg(gc0), a2, mul2(bb, ly)))));
+    g2[2] = fma2(s2, b2, fma2(g_dt, a2, fma2(gc0, a1, fma2(neg(gc1), a0, mul2(bb, lz)))));
 }
 
 }  // namespace bs

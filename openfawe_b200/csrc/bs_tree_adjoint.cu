@@ -271,7 +271,8 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
     using T = typename std::conditional<PREC == 0, double, float>::type;  // the sums' type: FP64 in FP64 mode
     __shared__ float4 shi[NEAR_TARGETS], slo[NEAR_TARGETS];  // two-float target: (hi x, y, z, w_x), (lo x, y, z, w_y)
     __shared__ float sw2[NEAR_TARGETS];                      // w_z
-    __shared__ float4 srel[NEAR_TARGETS];                    // x - O (leaf centre), FP32
+    __shared__ float4 srel[NEAR_TARGETS];                    // x - O (leaf centre), FP32, and w_x
+    __shared__ float2 sw12[NEAR_TARGETS];                    // w_y, w_z (zero past the item's targets)
     __shared__ T sacc[3][NEAR_TARGETS];
     __shared__ int sp[NEAR_TARGETS];
     __shared__ long long se0[NEAR_TARGETS], se1[NEAR_TARGETS];
@@ -303,11 +304,20 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
             const double x0 = a.points[3 * (int64_t)p], x1 = a.points[3 * (int64_t)p + 1],
                          x2 = a.points[3 * (int64_t)p + 2];
             wide = adj_clear(x0, x1, x2, nr, MODEL, a.near2);
-            srel[tid] = make_float4((float)(x0 - nr.cx), (float)(x1 - nr.cy), (float)(x2 - nr.cz), 0.0f);
+            srel[tid] = make_float4((float)(x0 - nr.cx), (float)(x1 - nr.cy), (float)(x2 - nr.cz),
+                                    (float)a.cot[3 * (int64_t)p]);
+            sw12[tid] = make_float2((float)a.cot[3 * (int64_t)p + 1], (float)a.cot[3 * (int64_t)p + 2]);
+        } else if (tid < NEAR_TARGETS) {  // past the item's targets: the first target's offset, zero cotangent
+            const int p = a.perm[a.near_items[first]];
+            srel[tid] = make_float4((float)(a.points[3 * (int64_t)p] - nr.cx),
+                                    (float)(a.points[3 * (int64_t)p + 1] - nr.cy),
+                                    (float)(a.points[3 * (int64_t)p + 2] - nr.cz), 0.0f);
+            sw12[tid] = make_float2(0.0f, 0.0f);
         }
-        // every target of the item clear: the item's pairs take the clear form (uniform over the block); the barrier
-        // also publishes the targets staged above
+        // every target of the item clear: the item's pairs take the clear form (uniform over the block); the barriers
+        // also publish the targets staged above
         const int all_wide = __syncthreads_and(wide);
+        const int any_excl = __syncthreads_or(tid < nt && se0[tid] < se1[tid]);
         const bool clear_all = PREC != 0 && a.seg32c2 && all_wide;
         for (int base = nr.lo; base < nr.hi; base += NEAR_THREADS) {
             const int s = base + tid;
@@ -328,8 +338,51 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
                 // past the item's end or excluded for this segment takes zero cotangent at a valid target's offset
                 const float L2 = cq.lx * cq.lx + cq.ly * cq.ly + cq.lz * cq.lz;
                 const float iL2 = valid && L2 > 0.0f ? 1.0f / L2 : 0.0f;
+                if (!valid) cq.w = INFINITY;  // no segment: zero Gamma, and outside every core range
                 float sgf[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                for (int g0 = 0; g0 < nt; g0 += 64) {
+                if (!any_excl) {
+                    // no exclusions: the padded offsets and zero cotangents past the item's end need no tests; the
+                    // sums stay packed until the end of the item
+                    float2 sg2[7];
+                    for (int k = 0; k < 7; ++k) sg2[k] = make_float2(0.f, 0.f);
+                    for (int g0 = 0; g0 < nt; g0 += 64) {
+                        float2 tacc0 = make_float2(0.f, 0.f), tacc1 = tacc0, tacc2 = tacc0;
+                        for (int j = 0; j < 32; ++j) {
+                            const int tA = g0 + ((lane + j) & 31), tB = tA + 32;
+                            const float4 rA = srel[tA], rB = srel[tB];
+                            const float2 wA = sw12[tA], wB = sw12[tB];
+                            float2 f1[3], f2[3], fg;
+                            pair_vjp32_clear2<MODEL>(make_float2(rA.x, rB.x), make_float2(rA.y, rB.y),
+                                                     make_float2(rA.z, rB.z), cq, iL2, make_float2(rA.w, rB.w),
+                                                     make_float2(wA.x, wB.x), make_float2(wA.y, wB.y), f1, f2, fg);
+                            sg2[0] = add2(sg2[0], f1[0]); sg2[1] = add2(sg2[1], f1[1]); sg2[2] = add2(sg2[2], f1[2]);
+                            sg2[3] = add2(sg2[3], f2[0]); sg2[4] = add2(sg2[4], f2[1]); sg2[5] = add2(sg2[5], f2[2]);
+                            sg2[6] = add2(sg2[6], fg);
+                            // lane q owns targets g0 + q and g0 + 32 + q; it receives their terms from lane q - j
+                            const int from = (lane - j) & 31;
+                            const float2 d0 = add2(f1[0], f2[0]), d1 = add2(f1[1], f2[1]), d2 = add2(f1[2], f2[2]);
+                            tacc0 = add2(tacc0, make_float2(__shfl_sync(0xffffffffu, d0.x, from),
+                                                            __shfl_sync(0xffffffffu, d0.y, from)));
+                            tacc1 = add2(tacc1, make_float2(__shfl_sync(0xffffffffu, d1.x, from),
+                                                            __shfl_sync(0xffffffffu, d1.y, from)));
+                            tacc2 = add2(tacc2, make_float2(__shfl_sync(0xffffffffu, d2.x, from),
+                                                            __shfl_sync(0xffffffffu, d2.y, from)));
+                        }
+                        if (g0 + lane < nt) {
+                            atomicAdd(&sacc[0][g0 + lane], (T)tacc0.x);
+                            atomicAdd(&sacc[1][g0 + lane], (T)tacc1.x);
+                            atomicAdd(&sacc[2][g0 + lane], (T)tacc2.x);
+                        }
+                        if (g0 + 32 + lane < nt) {
+                            atomicAdd(&sacc[0][g0 + 32 + lane], (T)tacc0.y);
+                            atomicAdd(&sacc[1][g0 + 32 + lane], (T)tacc1.y);
+                            atomicAdd(&sacc[2][g0 + 32 + lane], (T)tacc2.y);
+                        }
+                    }
+                    for (int k = 0; k < 6; ++k) sgf[k] = -(sg2[k].x + sg2[k].y);
+                    sgf[6] = sg2[6].x + sg2[6].y;
+                }
+                for (int g0 = 0; any_excl && g0 < nt; g0 += 64) {
                     float2 tacc0 = make_float2(0.f, 0.f), tacc1 = tacc0, tacc2 = tacc0;
                     for (int j = 0; j < 32; ++j) {
                         const int tA = g0 + ((lane + j) & 31), tB = tA + 32;
