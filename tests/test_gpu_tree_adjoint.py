@@ -13,6 +13,8 @@ forward it differentiates.
   extrapolated quotient equals the adjoint to 1e-6 of the gradient's scale.  Circulations enter linearly: exact.
 * The benchmark's setting (fifth-order Morton tree, theta 0.215, leaf 384, mixed) on the 468-row rotor wake (102k
   segments x 20,570 targets): every gradient within 2e-5 relative L2 of the exact adjoint.
+* Excluded (target, segment) pairs: with no far field the mixed tree adjoint with exclusions is the exact adjoint
+  with the same exclusions.
 * The autograd function's backward on a tree forward is the tree adjoint.
 """
 import numpy as np
@@ -58,6 +60,31 @@ def test_tree_adjoint_without_far_field_is_the_exact_adjoint(device, kind):
                                                              order=2, leaf_size=32, kind=kind)]
         for name, u, v in zip(("points", "starts", "ends", "gamma"), got, exact):
             assert rel(u, v) <= tol, (kind, precision, name, rel(u, v))
+
+
+def test_tree_adjoint_with_exclusions_is_the_exact_adjoint(device):
+    """Excluded (target, segment) pairs in the near pairs: with no far field the mixed tree adjoint equals the exact
+    adjoint with the same exclusions.  The targets on one side of the wake exclude three segments each, spread over
+    the wake, so that work items with excluding targets, without them, and with both occur (the near kernel's clear
+    paths with and without the per-pair exclusion test); each also excludes the segment nearest to it."""
+    import torch
+    from openfawe_b200 import adjoint
+    x, a, b, g, r, w = small_wake()
+    n, m = len(x), len(a)
+    left = x[:, 0] < np.median(x[:, 0])
+    mid = 0.5 * (a + b)
+    nearest = np.argmin(((x[:, None, :] - mid[None, :, :]) ** 2).sum(axis=2), axis=1)
+    rows = [sorted({int(nearest[p]), p % m, (7 * p + 3) % m, (13 * p + 5) % m}) if left[p] else [] for p in range(n)]
+    csr = (np.concatenate(([0], np.cumsum([len(q) for q in rows]))).astype(np.int64),
+           np.array([s_ for q in rows for s_ in q], dtype=np.int64))
+    pts = torch.as_tensor(x, device=device)
+    exact = [t.cpu().numpy() for t in adjoint.adjoint_direct(pts, a, b, g, r, 2, w, csr=csr)]
+    plain = [t.cpu().numpy() for t in adjoint.adjoint_direct(pts, a, b, g, r, 2, w)]
+    assert min(rel(u, v) for u, v in zip(plain, exact)) > 1e-3  # the exclusions matter
+    got = [t.cpu().numpy() for t in adjoint.adjoint_tree(pts, a, b, g, r, 2, w, csr=csr, precision="mixed",
+                                                         theta=1e-9, order=2, leaf_size=32, kind="morton")]
+    for name, u, v in zip(("points", "starts", "ends", "gamma"), got, exact):
+        assert rel(u, v) <= 1e-5, (name, rel(u, v))
 
 
 def interior_endpoints(x, a, b, g, r, leaf, kind, device):
