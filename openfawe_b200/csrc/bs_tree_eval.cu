@@ -846,10 +846,13 @@ __device__ __forceinline__ void list_item(const EvalArgs &a, int64_t gw, int c, 
     }
 }
 
-// Three blocks per SM (up to 168 registers a thread): the packed pairs of a tile need the registers to interleave.
+// The near-leaf kernel at four blocks a SM (128 registers a thread: more warps to hide the packed pairs' dependent
+// chains, measured faster than three blocks at 160 registers); the far-node kernel at three (57.9 KB of shared memory
+// a block, up to 168 registers).
 // PART 0: near leaves (counter a.queue[0]); PART 1: far nodes (counter a.queue[2]; no tiles).
 template <int PREC, int MODEL, int PART>
-__global__ void __launch_bounds__(LIST_WARPS * 32, PART == 0 ? LIST_NEAR_BLOCKS : LIST_FAR_BLOCKS) tree_list_kernel(EvalArgs a, int64_t target_warps) {
+__global__ void __launch_bounds__(LIST_WARPS * 32, PART == 0 ? LIST_NEAR_BLOCKS : LIST_FAR_BLOCKS)
+    tree_list_kernel(EvalArgs a, int64_t target_warps) {
     // near kernel: static tiles and entry buffers; far kernel: FAR_WARP_SMEM of dynamic shared memory a warp
     __shared__ __align__(16) unsigned char tile_mem[PART == 0 ? LIST_WARPS * 32 * sizeof(Seg64) : 16];
     __shared__ int2 entry_mem[PART == 0 ? LIST_WARPS * ENTRY_BUF : 1];
