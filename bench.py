@@ -35,7 +35,8 @@ THETA, ORDER, LEAF, CLEARANCE = 0.215, 5, 384, 3.0
 # the FP64 direct sum at order 2 and theta 0.04 (7.5e-7), which is the setting its baseline is timed at.
 REF_THETA, REF_ORDER, REF_LEAF = 0.04, 2, 32
 W_PAIR, W_VISIT = 62.0, 12.0            # algorithmic flops per near pair and per visited node
-LIST_TRAFFIC = 8.56e6                   # DRAM bytes per list-kernel launch (ncu capture of the default step)
+LIST_TRAFFIC = 8.57e6                   # DRAM bytes read + written by one near-leaf kernel launch of the default
+                                        # step (ncu dram__bytes_read.sum + dram__bytes_write.sum; records L2-resident)
 # per far evaluation of order p (3: 180 + 170 for the third term, 4: 350 + 300 for the fourth)
 W_FAR = {0: 40.0, 1: 100.0, 2: 180.0, 3: 350.0, 4: 650.0, 5: 1100.0}
 L2_FLUSH_BYTES = 512 << 20  # larger than the 126 MB L2
