@@ -64,7 +64,8 @@ typedef struct {
     int raise_singular; /* 1 for singularity='raise' */
     int precision;      /* bs_precision */
     int block;          /* threads per block: 32, 64, 128 or 256 (CudaSettings.block) */
-    double near_cores;  /* single precisions: pairs within near_cores core radii of a segment are done in FP64 */
+    double near_cores;  /* single precisions: pairs within near_cores core radii of a segment are done in FP64
+                           (model 0, which has no core: pairs within a quarter of the segment's length of it) */
 } bs_kernel_params;
 
 typedef struct {
