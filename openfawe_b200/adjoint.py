@@ -1,4 +1,4 @@
-"""Differentiation of the induced velocity (north star pattern 3): hand-written adjoints behind torch.autograd.
+"""Differentiation of the induced velocity: hand-written adjoints behind torch.autograd.
 
 ``InducedVelocity.apply(points, starts, ends, gamma, radius, ...)`` returns the induced velocity [n,3] of directed
 segments A->B; its backward returns d(w . u) with respect to the targets, both endpoints and the circulations for the

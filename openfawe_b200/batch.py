@@ -1,4 +1,4 @@
-"""Batched evaluation of many independent wakes (north star pattern 2).
+"""Batched evaluation of many independent wakes of uneven sizes in one persistent launch.
 
 A ``WakeBatch`` concatenates the segments and targets of many wakes of uneven sizes (a wind-speed sweep, several time
 steps), builds one forest on the device (``bs_forest_build``: one key sort and one radix tree whose upper splits fall
