@@ -165,6 +165,46 @@ def main():
         if args.only:
             return
 
+    if args.only == "convection_rings.npz" or args.only is None:
+        # one stage of wake._network_convection (wake.py:404-491) on a network with rotor rings after its wing rows:
+        # the rotor-sheet network reordered so that every ring node follows every wing node, the first wing row
+        # bound; four settings: rows and rings; the leading ring nodes free, the ring targets with their own cores;
+        # the far-wake row limit with frozen rows at the ambient flow; the same with the frozen rows drifting with
+        # the rings' induction
+        import types
+        from openfawe.aero import wake as W
+        from openfawe.aero.vortex import CoreModel
+        case = wakes.rotor_sheet(6, seed=12, targets=1)
+        per_row, wing = 46 + 8 * 16, 46
+        index = np.arange(len(case["nodes"]))
+        is_wing = (index % per_row) < wing
+        order = np.concatenate((index[is_wing], index[~is_wing]))
+        position = np.empty_like(order)
+        position[order] = np.arange(len(order))
+        nodes = case["nodes"][order]
+        edges = position[case["edges"]]
+        first, ring_first = wing, int(is_wing.sum())
+        rng = np.random.default_rng(12)
+        gamma = rng.uniform(0.0, 8.0, len(edges))
+        radii = np.full(len(edges), 0.05)
+        ring_radii = np.full(len(edges), 0.08)
+        inflow = np.array([10.0, 0.0, 0.5])
+        out = dict(nodes=nodes, edges=edges, gamma=gamma, radii=radii, ring_radii=ring_radii, first=np.array(first),
+                   ring_first=np.array(ring_first), inflow=inflow)
+        settings = {"rings": dict(), "ring_free": dict(ring_free=200, ring_radii=ring_radii),
+                    "row_limit": dict(rows=3, drift="ambient"), "row_limit_rings": dict(rows=3, drift="ambient_rings")}
+        for name, opt in settings.items():
+            config = types.SimpleNamespace(free_wake=True, velocity_backend="numba", core_model=CoreModel.LAMB_OSEEN)
+            if "rows" in opt:
+                config.free_convection_rows = opt["rows"]
+                config.frozen_rows_drift = opt["drift"]
+            out[name] = W._network_convection(nodes, edges, gamma, first, radii, config, inflow, 0.0,
+                                              ring_first=ring_first, ring_free=opt.get("ring_free"),
+                                              ring_radii=opt.get("ring_radii"))
+        save("convection_rings.npz", **out)
+        if args.only:
+            return
+
     if args.only == "frozen_state.npz" or args.only is None:
         # a frozen state in the benchmark's format and the reference's own segments_velocity on it (the numba direct
         # sum the benchmark takes as its reference, local_benchmark.py:56-66)

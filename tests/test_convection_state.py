@@ -59,6 +59,53 @@ def test_oracle_convection_stages_match_reference():
         assert np.array_equal(got.view(np.uint64), g[integrator].view(np.uint64)), integrator
 
 
+# the four settings of convection_rings.npz (tests/golden/make_golden.py)
+RING_SETTINGS = {"rings": {}, "ring_free": {"ring_free": 200, "ring_radii": True},
+                 "row_limit": {"free_rows": 3, "frozen_drift": "ambient"},
+                 "row_limit_rings": {"free_rows": 3, "frozen_drift": "ambient_rings"}}
+
+
+def ring_options(g, name, to_tensor):
+    opt = dict(RING_SETTINGS[name])
+    opt["ring_radii"] = to_tensor(g["ring_radii"]) if opt.get("ring_radii") else None
+    return dict(ring_first=int(g["ring_first"]), **opt)
+
+
+def oracle_ring_stage(g, name):
+    """One stage of wake._network_convection with rotor rings: the sums convection.stage_parts plans, each by the
+    oracle's ordered FP64 direct sum, added to the ambient flow (test infrastructure)."""
+    import torch
+    from openfawe_b200 import convection
+    nodes, edges, gamma, radii = g["nodes"], g["edges"], g["gamma"], g["radii"]
+    first = int(g["first"])
+    points = nodes[first:]
+    pairs = O.incident_pairs(nodes, edges, first)
+    parts = convection.stage_parts(len(points), first, len(nodes), torch.as_tensor(edges), torch.as_tensor(pairs),
+                                   torch.as_tensor(radii), **ring_options(g, name, torch.as_tensor))
+    starts = nodes[edges[:, 0]]
+    delta = nodes[edges[:, 1]] - starts
+    lengths = np.hypot(np.hypot(delta[..., 0], delta[..., 1]), delta[..., 2])
+    directions = delta / lengths[:, None]
+    velocity = np.broadcast_to(g["inflow"], points.shape).copy()
+    for lo, hi, sub, cores, rule, excluded in parts:
+        take = slice(None) if sub is None else sub.numpy()
+        csr = O.exclusion_csr(hi - lo, excluded.numpy())
+        u, flag = O.direct_sum(points[lo:hi], starts[take], directions[take], lengths[take], gamma[take],
+                               cores.numpy(), 2, csr, rule or "raise")
+        assert not flag
+        velocity[lo:hi] += u
+    return velocity
+
+
+def test_oracle_ring_stages_match_reference():
+    """Rows and rings, the leading ring nodes free with their own cores, the far-wake row limit with frozen rows at
+    the ambient flow or drifting with the rings: the planned sums reproduce the reference's stage bit for bit."""
+    g = golden("convection_rings.npz")
+    for name in RING_SETTINGS:
+        got = oracle_ring_stage(g, name)
+        assert np.array_equal(got.view(np.uint64), g[name].view(np.uint64)), name
+
+
 def test_frozen_state_roundtrip_and_oracle(tmp_path):
     from openfawe_b200 import wakestate
     state = wakestate.load_state(os.path.join(GOLDEN, "frozen_state_input.npz"))
@@ -112,6 +159,22 @@ def test_device_convection_matches_reference_steps(device):
         tree = convection.convect(nodes, edges, gamma, radii, first, 2, dt, g["inflow"], integrator, method="tree",
                                   precision="mixed", theta=0.1, order=3, device=device).cpu().numpy()
         assert np.linalg.norm(tree - g[integrator]) / np.linalg.norm(step) < 1e-5, integrator
+
+
+@pytest.mark.gpu
+def test_device_ring_stages_match_reference(device):
+    """The device stage with the ring and far-wake options, FP64 direct sums, within the A1 bound of the reference's."""
+    import torch
+    from openfawe_b200 import convection
+    g = golden("convection_rings.npz")
+    nodes, edges, gamma, radii, first = g["nodes"], g["edges"], g["gamma"], g["radii"], int(g["first"])
+    scale = _a1_scale(nodes, edges, gamma, np.maximum(radii, g["ring_radii"]), first)
+    dev = lambda a: torch.as_tensor(a, device=device)  # noqa: E731
+    for name in RING_SETTINGS:
+        v = convection.network_velocity(dev(nodes), dev(edges), dev(gamma), dev(radii), first, 2, g["inflow"],
+                                        method="direct", precision="fp64", **ring_options(g, name, dev))
+        err = np.linalg.norm(v.cpu().numpy() - g[name], axis=1)
+        assert np.all(err <= 1e-12 * scale), (name, float((err / scale).max()))
 
 
 @pytest.mark.gpu
