@@ -135,11 +135,12 @@ def network_velocity(nodes, edges, gamma, radii, first, model, ambient=(0.0, 0.0
 
 
 def convect(nodes, edges, gamma, radii, first, model, dt, ambient=(0.0, 0.0, 0.0), integrator="rk4", substeps=1,
-            time=0.0, next_bound=None, **options):
+            time=0.0, next_bound=None, drift=None, **options):
     """Advance the free nodes nodes[first:] by dt (substeps explicit steps of the integrator) on the frozen graph;
     returns their new positions (device tensor [n - first, 3]).  The bound nodes nodes[:first] stay put, or move
-    linearly to ``next_bound`` over the step (the reference's stage interpolation).  ``options`` go to
-    ``network_velocity`` (method, precision, theta, order, ...)."""
+    linearly to ``next_bound`` over the step (the reference's stage interpolation).  ``drift`` ([n - first, 3], or
+    None) is added to every stage's velocity, as the reference adds its frozen rings' sheet drift (wake.py:584-592).
+    ``options`` go to ``network_velocity`` (method, precision, theta, order, the ring and far-wake options)."""
     if integrator not in INTEGRATORS:
         raise ValueError(f"integrator must be one of {INTEGRATORS}")
     dev = nodes.device if isinstance(nodes, torch.Tensor) else engine._device_of(options.pop("device", None))
@@ -151,14 +152,16 @@ def convect(nodes, edges, gamma, radii, first, model, dt, ambient=(0.0, 0.0, 0.0
         radii = radii.expand(edges.shape[0]).contiguous()
     bound = nodes[:first]
     displacement = None if next_bound is None else engine.f64(next_bound, dev).reshape(-1, 3) - bound
+    drift = None if drift is None else engine.f64(drift, dev).reshape(-1, 3)
     points = nodes[first:].clone()
     h = float(dt) / int(substeps)
     t0 = float(time)
 
     def rhs(current, t):
         stage_bound = bound if displacement is None or t == t0 else bound + ((t - t0) / float(dt)) * displacement
-        return network_velocity(torch.cat((stage_bound, current)), edges, gamma, radii, first, model, ambient, t,
-                                **options)
+        velocity = network_velocity(torch.cat((stage_bound, current)), edges, gamma, radii, first, model, ambient, t,
+                                    **options)
+        return velocity if drift is None else velocity + drift
 
     for k in range(int(substeps)):
         t = t0 + k * h

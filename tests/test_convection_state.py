@@ -71,12 +71,13 @@ def ring_options(g, name, to_tensor):
     return dict(ring_first=int(g["ring_first"]), **opt)
 
 
-def oracle_ring_stage(g, name):
+def oracle_ring_stage(g, name, nodes=None):
     """One stage of wake._network_convection with rotor rings: the sums convection.stage_parts plans, each by the
     oracle's ordered FP64 direct sum, added to the ambient flow (test infrastructure)."""
     import torch
     from openfawe_b200 import convection
-    nodes, edges, gamma, radii = g["nodes"], g["edges"], g["gamma"], g["radii"]
+    nodes = g["nodes"] if nodes is None else nodes
+    edges, gamma, radii = g["edges"], g["gamma"], g["radii"]
     first = int(g["first"])
     points = nodes[first:]
     pairs = O.incident_pairs(nodes, edges, first)
@@ -175,6 +176,38 @@ def test_device_ring_stages_match_reference(device):
                                         method="direct", precision="fp64", **ring_options(g, name, dev))
         err = np.linalg.norm(v.cpu().numpy() - g[name], axis=1)
         assert np.all(err <= 1e-12 * scale), (name, float((err / scale).max()))
+
+
+@pytest.mark.gpu
+def test_device_ring_rk4_step_with_drift(device):
+    """An RK4 step with the ring and far-wake options and a constant drift of the frozen ring nodes (the reference's
+    sheet drift): the device step against the oracle's composition of the planned stages (itself pinned stage by stage
+    and integrator by integrator to the reference), within the A1 bound times dt."""
+    from openfawe_b200 import convection
+    g = golden("convection_rings.npz")
+    name = "ring_free"
+    nodes, edges, gamma, radii, first = g["nodes"], g["edges"], g["gamma"], g["radii"], int(g["first"])
+    dt = 0.02
+    drift = np.zeros((len(nodes) - first, 3))
+    drift[int(g["ring_first"]) - first + 200:] = [0.4, -0.1, 0.2]
+
+    def rhs(points):
+        return oracle_ring_stage(g, name, np.concatenate((nodes[:first], points))) + drift
+    points = nodes[first:]
+    k1 = rhs(points)
+    k2 = rhs(points + dt * k1 / 2)
+    k3 = rhs(points + dt * k2 / 2)
+    k4 = rhs(points + dt * k3)
+    want = points + dt * (k1 + 2 * k2 + 2 * k3 + k4) / 6
+    import torch
+    got = convection.convect(nodes, edges, gamma, radii, first, 2, dt, g["inflow"], "rk4", method="direct",
+                             precision="fp64", device=device, drift=drift,
+                             **ring_options(g, name, lambda a: torch.as_tensor(a, device=device))).cpu().numpy()
+    scale = _a1_scale(nodes, edges, gamma, np.maximum(radii, g["ring_radii"]), first)
+    err = np.linalg.norm(got - want, axis=1)
+    assert np.all(err <= 4e-12 * scale * dt + 1e-15), float((err / (scale * dt)).max())
+    moved = np.linalg.norm(got - points, axis=1)
+    assert np.all(moved > 0)
 
 
 @pytest.mark.gpu
