@@ -223,8 +223,8 @@ void bs_graph_free(bs_graph *graph);
 
 /* Adjoint of the exact direct sum (no counterpart in the reference, which has no adjoint): given the cotangent w
  * [n,3] of the induced velocity, writes d(sum_p w_p . u_p) with respect to the targets [n,3], the segment starts A and
- * ends B [m,3] and the circulations [m]; any output may be NULL.  Segments are given by their endpoints; core models
- * NONE, RANKINE and LAMB_OSEEN; excluded and on-axis pairs contribute nothing.  FP64, pair terms recomputed. */
+ * ends B [m,3] and the circulations [m]; any output may be NULL.  Segments are given by their endpoints; every core
+ * model (0..5); excluded and on-axis pairs contribute nothing.  FP64, pair terms recomputed. */
 int bs_adjoint_direct(bs_ctx *ctx, int64_t n, const double *points, int64_t m, const double *A, const double *B,
                       const double *gamma, const double *radius, const int64_t *ex_ptr, const int64_t *ex_seg,
                       int64_t e, int model, const double *cotangent, double *grad_points, double *grad_A,

@@ -9,7 +9,8 @@ incoming cotangent w, recomputing every pair term rather than storing it:
   tree, accepted nodes and near pairs, with the far field differentiated through the node moments down to the segments
   (node centres and acceptance decisions held fixed).
 
-Core models NONE, RANKINE and LAMB_OSEEN (the models the reference's tree code accepts).  The reference has no adjoint.
+Core models: all six for the exact adjoint; NONE, RANKINE and LAMB_OSEEN for the tree adjoint (the models the
+reference's tree code accepts).  The reference has no adjoint.
 """
 import ctypes
 

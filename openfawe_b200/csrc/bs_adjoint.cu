@@ -5,7 +5,8 @@
 //   r1 = x - A, r2 = x - B, c = r1 x r2, P = |r1||r2|, d = r1.r2,
 //   D = P (P + d), or P |c|^2 / (P - d) when d < 0 (the reference's rationalised branch),
 //   u = Gamma/(4 pi) f(|c|^2 / (|B - A|^2 rc^2)) (|r1| + |r2|) c / D,
-// with the core factor f of models 0 (none), 1 (Rankine) and 2 (Lamb-Oseen with its exponent cut-off), and reverse-mode
+// with the core factor f of models 0 (none), 1 (Rankine), 2 (Lamb-Oseen with its exponent cut-off) and 3 (Vatistas),
+// the offset (4) and Rosenhead-Moore (5) cores in D and the distances (bs_pair_vjp.cuh), and reverse-mode
 // differentiation of that expression by hand.  Pairs on a segment's axis (the reference's roundoff guard) contribute
 // nothing, as in the forward sum.
 //
@@ -117,9 +118,10 @@ __global__ void adjoint_pack_kernel(int64_t n, int64_t m, int model, const doubl
     if (i < m) {
         const double l0 = B[3 * i] - A[3 * i], l1 = B[3 * i + 1] - A[3 * i + 1], l2 = B[3 * i + 2] - A[3 * i + 2];
         const double L2 = l0 * l0 + l1 * l1 + l2 * l2, rc = radius[i];
-        const double irc2L2 = (model != 0 && rc > 0.0) ? 1.0 / (L2 * rc * rc) : 0.0;
+        const double irc2L2 = (model >= 1 && model <= 3 && rc > 0.0) ? 1.0 / (L2 * rc * rc) : 0.0;
+        const double rc2 = (model >= 4 && rc > 0.0) ? rc * rc : 0.0;
         seg[i] = AdjSeg{A[3 * i], A[3 * i + 1], A[3 * i + 2], B[3 * i], B[3 * i + 1], B[3 * i + 2], gamma[i], irc2L2,
-                        1.0 / L2, 0.0};
+                        1.0 / L2, rc2};
     }
 }
 
@@ -166,8 +168,8 @@ extern "C" int bs_adjoint_direct(bs_ctx *ctx, int64_t n, const double *points, i
         set_error("bs_adjoint_direct: null argument");
         return BS_ERR_ARG;
     }
-    if (model < 0 || model > 2) {
-        set_error("bs_adjoint_direct: the adjoint supports core models NONE, RANKINE and LAMB_OSEEN");
+    if (model < 0 || model > 5) {
+        set_error("bs_adjoint_direct: core model must be 0..5");
         return BS_ERR_ARG;
     }
     cudaStream_t s = (cudaStream_t)stream;

@@ -3,7 +3,10 @@
 // in its two-endpoint form, r1 = x - A, r2 = x - B, c = r1 x r2, P = |r1||r2|, d = r1.r2,
 //   D = P (P + d), or P |c|^2 / (P - d) when d < 0 (the reference's rationalised branch),
 //   u = Gamma/(4 pi) f(|c|^2 / (|B - A|^2 rc^2)) (|r1| + |r2|) c / D,
-// with the core factor f of models 0 (none), 1 (Rankine) and 2 (Lamb-Oseen with its exponent cut-off).
+// with the core factor f of models 0 (none), 1 (Rankine), 2 (Lamb-Oseen with its exponent cut-off) and 3 (Vatistas
+// n = 2: f = rho^2 / sqrt(1 + rho^4)); model 4 (offset core) adds rc^2 |B - A|^2 to D, model 5 (Rosenhead-Moore) takes
+// |r1|, |r2| as sqrt(|r1|^2 + rc^2), sqrt(|r2|^2 + rc^2) and d as r1.r2 + rc^2 (P^2 - d^2 = |c|^2 + rc^2 |B - A|^2),
+// which is the FP64 pair's form (pair64_core) in physical units.
 #pragma once
 #include "bs_internal.cuh"
 
@@ -12,9 +15,9 @@ namespace bs {
 // A segment as the adjoint reads it: endpoints, circulation and the per-segment invariants of the pair.
 struct AdjSeg {
     double ax, ay, az, bx, by, bz, gamma;
-    double irc2L2;  // 1 / (L^2 rc^2) for a cored model with rc > 0, else 0 (no core factor)
+    double irc2L2;  // 1 / (L^2 rc^2) for a core-factor model (1, 2, 3) with rc > 0, else 0 (no core factor)
     double invL2;   // 1 / L^2
-    double pad;
+    double rc2;     // rc^2 for the offset and Rosenhead-Moore models (4, 5), else 0
 };
 struct AdjTgt {
     double x, y, z, wx, wy, wz;
@@ -34,28 +37,41 @@ __device__ __forceinline__ bool pair_vjp64(double x0, double x1, double x2, cons
     // the reference's roundoff axis guard h <= eps max(1, na, nb) in its scaled units (h = |c|/L^2,
     // na = |r1|/L, nb = |r2|/L), squared
     if (cc * s.invL2 * s.invL2 <= AXIS_EPS64_SQ * fmax(1.0, fmax(q1, q2) * s.invL2)) return false;
-    const double in1 = rsqrt(q1), in2 = rsqrt(q2);
-    const double n1 = q1 * in1, n2 = q2 * in2;
-    const double d = r10 * r20 + r11 * r21 + r12 * r22;
+    // |r1|, |r2| (Rosenhead-Moore: augmented by the core) and their reciprocals
+    const bool rm = model == 5 && s.rc2 > 0.0;
+    const double in1 = rm ? 1.0 / sqrt(q1 + s.rc2) : rsqrt(q1), in2 = rm ? 1.0 / sqrt(q2 + s.rc2) : rsqrt(q2);
+    const double n1 = rm ? sqrt(q1 + s.rc2) : q1 * in1, n2 = rm ? sqrt(q2 + s.rc2) : q2 * in2;
+    const double d = r10 * r20 + r11 * r21 + r12 * r22 + (rm ? s.rc2 : 0.0);
     const double P = n1 * n2;
-    double D, dD_dP, dD_dd, dD_dcc;
+    const double L2 = 1.0 / s.invL2;
+    const double Q = rm ? cc + s.rc2 * L2 : cc;  // P^2 - d^2
+    double D, dD_dP, dD_dd, dD_dcc, dD_dL2 = 0.0;
     if (d >= 0.0) {
         D = P * (P + d);
         dD_dP = 2.0 * P + d;
         dD_dd = P;
         dD_dcc = 0.0;
-    } else {  // the rationalised denominator P (P + d) = P |c|^2 / (P - d)
+    } else {  // the rationalised denominator P (P + d) = P Q / (P - d)
         const double iq = 1.0 / (P - d);
-        D = P * cc * iq;
-        dD_dP = -cc * d * iq * iq;
-        dD_dd = P * cc * iq * iq;
+        D = P * Q * iq;
+        dD_dP = -Q * d * iq * iq;
+        dD_dd = P * Q * iq * iq;
         dD_dcc = P * iq;
+        if (rm) dD_dL2 = s.rc2 * P * iq;
+    }
+    if (model == 4 && s.rc2 > 0.0) {  // offset core
+        D += s.rc2 * L2;
+        dD_dL2 = s.rc2;
     }
     double f = 1.0, df = 0.0, rho2 = 0.0;  // core factor f(rho2), df/drho2 with rho2 = |c|^2 / (L^2 rc^2)
     if (s.irc2L2 > 0.0) {
         rho2 = cc * s.irc2L2;
         if (model == 1) {
             if (rho2 < 1.0) { f = rho2; df = 1.0; }
+        } else if (model == 3) {  // Vatistas n = 2: f = x / sqrt(1 + x^2), f' = (1 + x^2)^(-3/2)
+            f = rho2 < 1.0 ? rho2 / hypot(1.0, rho2) : 1.0 / hypot(1.0, 1.0 / rho2);
+            const double g = rho2 < 1.0 ? 1.0 / hypot(1.0, rho2) : (1.0 / rho2) / hypot(1.0, 1.0 / rho2);
+            df = g * g * g;  // (1 + x^2)^(-3/2), as (1/x)^3 / (1 + 1/x^2)^(3/2) for large x
         } else if (rho2 <= LAMB_CUT2) {
             const double em1 = expm1(-LAMB_A * rho2);
             f = -em1;
@@ -74,7 +90,7 @@ __device__ __forceinline__ bool pair_vjp64(double x0, double x1, double x2, cons
     const double g_D = -h * f * S * iD;
     const double g_rho2 = g_f * df;
     const double g_cc = g_rho2 * s.irc2L2 + g_D * dD_dcc;
-    const double g_L2 = -g_rho2 * rho2 * s.invL2;
+    const double g_L2 = -g_rho2 * rho2 * s.invL2 + g_D * dD_dL2;
     const double g_P = g_D * dD_dP, g_d = g_D * dD_dd;
     const double k = G * coefG;
     const double gc0 = k * w0 + 2.0 * c0 * g_cc, gc1 = k * w1 + 2.0 * c1 * g_cc, gc2 = k * w2 + 2.0 * c2v * g_cc;

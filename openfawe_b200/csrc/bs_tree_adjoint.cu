@@ -459,7 +459,7 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
                             as.gamma = a.gamma[a.order32[s]];
                             as.irc2L2 = (MODEL != 0 && q.radius > 0.0) ? 1.0 / (L * L * q.radius * q.radius) : 0.0;
                             as.invL2 = q.inv_len * q.inv_len;
-                            as.pad = 0.0;
+                            as.rc2 = 0.0;
                             const int p = sp[t];
                             double h1[3], h2[3], hg = 0.0;
                             if (pair_vjp64(a.points[3 * (int64_t)p], a.points[3 * (int64_t)p + 1],

@@ -2,7 +2,8 @@
 the unit-circulation pair velocities of the reference's VSM operators.
 
 * Finite differences: central, h = 1e-4 m, on the FP64 direct sum, for a random subset of target and endpoint
-  coordinates; geometry kept away from the Lamb-Oseen cut-off band (the core factor jumps there by e^-10).
+  coordinates, every core model (none, Rankine, Lamb-Oseen, Vatistas, offset, Rosenhead-Moore); geometry kept away
+  from the Lamb-Oseen cut-off band (the core factor jumps there by e^-10).
 * Circulation gradients: d(w.u)/dGamma_s = sum_p w_p . g_ps with g the unit-circulation pair velocity, which is what the
   reference's ``vortex_numba.pair_matrix`` (src/openfawe/aero/vortex_numba.py:271-287) computes for its VSM influence
   operators; checked on a 64-panel wing's rings assembled into panel columns the way ``assemble_columns`` (:290-308)
@@ -46,7 +47,7 @@ def direct_u(device, x, a, b, g, r, model=2):
     return u.cpu().numpy()
 
 
-@pytest.mark.parametrize("model", [0, 1, 2])
+@pytest.mark.parametrize("model", [0, 1, 2, 3, 4, 5])
 def test_adjoint_against_central_differences(device, model):
     import torch
     from openfawe_b200 import adjoint
