@@ -236,7 +236,8 @@ int bs_adjoint_direct(bs_ctx *ctx, int64_t n, const double *points, int64_t m, c
  * the forward the tree code evaluates: the same tree (built again), the same accepted nodes and near pairs (the walk
  * runs again), pair terms and expansions recomputed; node centres and acceptance decisions are held fixed.  Near pairs
  * in FP32 (kp->precision BS_MIXED or BS_FP32) with FP64 where the forward takes FP64, or all in FP64 (BS_FP64); the
- * far field's derivatives in FP64.  Core models NONE, RANKINE and LAMB_OSEEN; orders 0..5.  Gradients are summed with
+ * far field's derivatives in FP64.  Every core model (0..5; the Vatistas, offset and Rosenhead-Moore cores with FP64
+ * near pairs in either precision); orders 0..5.  Gradients are summed with
  * atomics (repeatable to rounding).  BS_ERR_OOM if a warp's interaction list exceeds the list pool.  Blocks until
  * the gradients are written.  Afterwards bs_last_stats holds its stage times: build_ms the build, walk and list
  * transposition, walk_ms the near pairs, list_ms the far entries, moments_ms the push-down and segment moments. */

@@ -9,8 +9,8 @@ incoming cotangent w, recomputing every pair term rather than storing it:
   tree, accepted nodes and near pairs, with the far field differentiated through the node moments down to the segments
   (node centres and acceptance decisions held fixed).
 
-Core models: all six for the exact adjoint; NONE, RANKINE and LAMB_OSEEN for the tree adjoint (the models the
-reference's tree code accepts).  The reference has no adjoint.
+Every core model (0..5) in both adjoints; the tree adjoint takes the models the reference's tree code does not accept
+(Vatistas, offset, Rosenhead-Moore) with FP64 near pairs.  The reference has no adjoint.
 """
 import ctypes
 

@@ -457,9 +457,10 @@ __global__ void __launch_bounds__(NEAR_THREADS) near_adjoint_kernel(AdjArgs a) {
                             as.ax = q.sx; as.ay = q.sy; as.az = q.sz;
                             as.bx = q.sx + L * q.dx; as.by = q.sy + L * q.dy; as.bz = q.sz + L * q.dz;
                             as.gamma = a.gamma[a.order32[s]];
-                            as.irc2L2 = (MODEL != 0 && q.radius > 0.0) ? 1.0 / (L * L * q.radius * q.radius) : 0.0;
+                            as.irc2L2 = (MODEL >= 1 && MODEL <= 3 && q.radius > 0.0)
+                                            ? 1.0 / (L * L * q.radius * q.radius) : 0.0;
                             as.invL2 = q.inv_len * q.inv_len;
-                            as.rc2 = 0.0;
+                            as.rc2 = (MODEL >= 4 && q.radius > 0.0) ? q.radius * q.radius : 0.0;
                             const int p = sp[t];
                             double h1[3], h2[3], hg = 0.0;
                             if (pair_vjp64(a.points[3 * (int64_t)p], a.points[3 * (int64_t)p + 1],
@@ -775,12 +776,17 @@ void launch_far_segments(unsigned far_grid, bool far, int64_t m, cudaStream_t s,
     segment_moments_adjoint_kernel<ORDER><<<blocks(m, 128), 128, 0, s>>>(a, leaf_of);
 }
 
+// Models 0-2 in the requested precision; the Vatistas, offset and Rosenhead-Moore cores (3-5, which the reference's
+// tree code does not take) with FP64 near pairs (pair_vjp64) in either precision.
 template <int PREC>
 void launch_near(int model, unsigned grid, cudaStream_t s, const AdjArgs &a) {
     switch (model) {
         case 0: near_adjoint_kernel<PREC, 0><<<grid, NEAR_THREADS, 0, s>>>(a); break;
         case 1: near_adjoint_kernel<PREC, 1><<<grid, NEAR_THREADS, 0, s>>>(a); break;
-        default: near_adjoint_kernel<PREC, 2><<<grid, NEAR_THREADS, 0, s>>>(a); break;
+        case 2: near_adjoint_kernel<PREC, 2><<<grid, NEAR_THREADS, 0, s>>>(a); break;
+        case 3: near_adjoint_kernel<0, 3><<<grid, NEAR_THREADS, 0, s>>>(a); break;
+        case 4: near_adjoint_kernel<0, 4><<<grid, NEAR_THREADS, 0, s>>>(a); break;
+        default: near_adjoint_kernel<0, 5><<<grid, NEAR_THREADS, 0, s>>>(a); break;
     }
 }
 
@@ -802,8 +808,8 @@ extern "C" int bs_tree_adjoint(bs_ctx *ctx, const bs_sources *src, const bs_tree
         set_error("bs_tree_adjoint: invalid arrays");
         return BS_ERR_ARG;
     }
-    if (kp->model < 0 || kp->model > 2) {
-        set_error("bs_tree_adjoint: the adjoint supports core models NONE, RANKINE and LAMB_OSEEN");
+    if (kp->model < 0 || kp->model > 5) {
+        set_error("bs_tree_adjoint: core model must be 0..5");
         return BS_ERR_ARG;
     }
     if (!(tp->theta > 0.0 && tp->theta < 1.0) || tp->order < 0 || tp->order > ADJ_ORDER_MAX ||

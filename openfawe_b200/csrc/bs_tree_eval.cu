@@ -1462,8 +1462,11 @@ int tree_lists(const bs_ctx *ctx, const bs_tree *tree, const bs_tree_params *tp,
         case 0: tree_walk_kernel<1, 0, 2><<<walk_grid, block, smem, s>>>(args); break;
         case 1: tree_walk_kernel<1, 1, 2><<<walk_grid, block, smem, s>>>(args); break;
         case 2: tree_walk_kernel<1, 2, 2><<<walk_grid, block, smem, s>>>(args); break;
+        case 3: tree_walk_kernel<1, 3, 2><<<walk_grid, block, smem, s>>>(args); break;
+        case 4: tree_walk_kernel<1, 4, 2><<<walk_grid, block, smem, s>>>(args); break;
+        case 5: tree_walk_kernel<1, 5, 2><<<walk_grid, block, smem, s>>>(args); break;
         default:
-            set_error("tree lists: core models 0..2 only");
+            set_error("tree lists: core model must be 0..5");
             return BS_ERR_ARG;
     }
     BS_CHECK_LAUNCH("tree_walk_kernel (lists)");

@@ -14,7 +14,7 @@ forward it differentiates.
 * The benchmark's setting (fifth-order Morton tree, theta 0.215, leaf 384, mixed) on the 468-row rotor wake (102k
   segments x 20,570 targets): every gradient within 2e-5 relative L2 of the exact adjoint.
 * Excluded (target, segment) pairs: with no far field the mixed tree adjoint with exclusions is the exact adjoint
-  with the same exclusions.
+  with the same exclusions; so are the Vatistas, offset and Rosenhead-Moore cores' tree adjoints (FP64 near pairs).
 * The autograd function's backward on a tree forward is the tree adjoint.
 """
 import numpy as np
@@ -60,6 +60,22 @@ def test_tree_adjoint_without_far_field_is_the_exact_adjoint(device, kind):
                                                              order=2, leaf_size=32, kind=kind)]
         for name, u, v in zip(("points", "starts", "ends", "gamma"), got, exact):
             assert rel(u, v) <= tol, (kind, precision, name, rel(u, v))
+
+
+@pytest.mark.parametrize("model", [3, 4, 5])
+def test_tree_adjoint_of_the_other_core_models_is_the_exact_adjoint(device, model):
+    """Vatistas, offset and Rosenhead-Moore cores (FP64 near pairs in either precision): with no far field the tree
+    adjoint equals the exact adjoint."""
+    import torch
+    from openfawe_b200 import adjoint
+    x, a, b, g, r, w = small_wake()
+    pts = torch.as_tensor(x, device=device)
+    exact = [t.cpu().numpy() for t in adjoint.adjoint_direct(pts, a, b, g, r, model, w)]
+    for precision in ("fp64", "mixed"):
+        got = [t.cpu().numpy() for t in adjoint.adjoint_tree(pts, a, b, g, r, model, w, precision=precision,
+                                                             theta=1e-9, order=2, leaf_size=32, kind="morton")]
+        for name, u, v in zip(("points", "starts", "ends", "gamma"), got, exact):
+            assert rel(u, v) <= 1e-12, (model, precision, name, rel(u, v))
 
 
 def test_tree_adjoint_with_exclusions_is_the_exact_adjoint(device):
