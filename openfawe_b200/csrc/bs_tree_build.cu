@@ -749,158 +749,6 @@ static int build_median(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStr
 // ---------------------------------------------------------------------------------------------------------------------
 // Moments.
 // ---------------------------------------------------------------------------------------------------------------------
-__global__ void item_count_kernel(int64_t count, const int64_t *lo, const int64_t *hi, int64_t *n) {
-    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= count) return;
-    int64_t size = hi[j] - lo[j];
-    n[j] = size > 0 ? (size + CHUNK - 1) / CHUNK : 0;
-}
-
-// Items (chunks of CHUNK positions) of every node.
-__global__ void item_fill_kernel(int64_t count, const int64_t *lo, const int64_t *hi, const int64_t *first,
-                                 Item *items) {
-    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= count) return;
-    int64_t k = first[j];
-    for (int64_t c = lo[j]; c < hi[j]; c += CHUNK, ++k)
-        items[k] = {(int32_t)j, (int32_t)c, (int32_t)min(hi[j], c + CHUNK), 0};
-}
-
-// Endpoint box and largest core of one chunk.
-__global__ void __launch_bounds__(MOM_THREADS) moment_box_kernel(const Item *items, int64_t nitems,
-                                                                 const int32_t *order, const SegGeo *geo,
-                                                                 double *partial) {
-    __shared__ double red[7][MOM_THREADS / 32];
-    for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x) {
-        Item item = items[it];
-        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY}, core = 0.0;
-        for (int k = item.start + threadIdx.x; k < item.end; k += blockDim.x) {
-            SegGeo g = geo[order[k]];
-            double a[3] = {g.sx, g.sy, g.sz}, b[3] = {g.ex, g.ey, g.ez};
-            for (int x = 0; x < 3; ++x) {
-                lo[x] = fmin(lo[x], fmin(a[x], b[x]));
-                hi[x] = fmax(hi[x], fmax(a[x], b[x]));
-            }
-            core = fmax(core, g.radius);
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            for (int x = 0; x < 3; ++x) {
-                lo[x] = fmin(lo[x], __shfl_xor_sync(0xffffffffu, lo[x], o));
-                hi[x] = fmax(hi[x], __shfl_xor_sync(0xffffffffu, hi[x], o));
-            }
-            core = fmax(core, __shfl_xor_sync(0xffffffffu, core, o));
-        }
-        int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        if (lane == 0) {
-            for (int x = 0; x < 3; ++x) { red[x][warp] = lo[x]; red[3 + x][warp] = hi[x]; }
-            red[6][warp] = core;
-        }
-        __syncthreads();
-        if (threadIdx.x < 7) {
-            double v = red[threadIdx.x][0];
-            for (int w = 1; w < MOM_THREADS / 32; ++w)
-                v = threadIdx.x < 3 ? fmin(v, red[threadIdx.x][w]) : fmax(v, red[threadIdx.x][w]);
-            partial[7 * it + threadIdx.x] = v;
-        }
-        __syncthreads();
-    }
-}
-
-__global__ void moment_centre_kernel(int64_t count, const int64_t *first, const int64_t *nitems,
-                                     const double *partial, double *centre, double *core) {
-    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= count) return;
-    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY}, c = 0.0;
-    for (int64_t it = first[j]; it < first[j] + nitems[j]; ++it) {
-        for (int x = 0; x < 3; ++x) {
-            lo[x] = fmin(lo[x], partial[7 * it + x]);
-            hi[x] = fmax(hi[x], partial[7 * it + 3 + x]);
-        }
-        c = fmax(c, partial[7 * it + 6]);
-    }
-    for (int x = 0; x < 3; ++x) centre[3 * j + x] = 0.5 * (lo[x] + hi[x]);
-    core[j] = c;
-}
-
-// Bounding radius^2 and moments (m0, m1, symmetric m2, and for PARTS == MOM_PARTS3 symmetric m3) of one chunk about
-// its node's centre.
-template <int PARTS>
-__global__ void __launch_bounds__(MOM_THREADS) moment_sum_kernel(const Item *items, int64_t nitems,
-                                                                 const int32_t *order, const SegGeo *geo,
-                                                                 const double *centre, double *partial) {
-    __shared__ double red[PARTS][MOM_THREADS / 32];
-    for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x) {
-        Item item = items[it];
-        const double c0 = centre[3 * item.node], c1 = centre[3 * item.node + 1], c2 = centre[3 * item.node + 2];
-        double acc[PARTS];
-#pragma unroll
-        for (int q = 0; q < PARTS; ++q) acc[q] = 0.0;
-        for (int k = item.start + threadIdx.x; k < item.end; k += blockDim.x) {
-            SegGeo g = geo[order[k]];
-            double a0 = g.sx - c0, a1 = g.sy - c1, a2 = g.sz - c2;
-            double b0 = g.ex - c0, b1 = g.ey - c1, b2 = g.ez - c2;
-            // the reference's ((x^2 + y^2) + z^2) without contraction: the bound is then bit-identical to the CPU's
-            double ra = __dadd_rn(__dadd_rn(__dmul_rn(a0, a0), __dmul_rn(a1, a1)), __dmul_rn(a2, a2));
-            double rb = __dadd_rn(__dadd_rn(__dmul_rn(b0, b0), __dmul_rn(b1, b1)), __dmul_rn(b2, b2));
-            acc[0] = fmax(acc[0], fmax(ra, rb));
-            if (g.gamma == 0.0) continue;
-            double d[3] = {0.5 * (g.sx + g.ex) - c0, 0.5 * (g.sy + g.ey) - c1, 0.5 * (g.sz + g.ez) - c2};
-            double l[3] = {g.lx, g.ly, g.lz};
-            double al[3] = {g.gamma * g.lx, g.gamma * g.ly, g.gamma * g.lz};
-            double sym[6];
-            int q = 0;
-#pragma unroll
-            for (int j = 0; j < 3; ++j)
-#pragma unroll
-                for (int k2 = j; k2 < 3; ++k2) sym[q++] = d[j] * d[k2] + l[j] * l[k2] * (1.0 / 12.0);
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                acc[1 + i] += al[i];
-#pragma unroll
-                for (int j = 0; j < 3; ++j) acc[4 + 3 * i + j] += al[i] * d[j];
-#pragma unroll
-                for (int p = 0; p < 6; ++p) acc[13 + 6 * i + p] += al[i] * sym[p];
-            }
-            if (PARTS == MOM_PARTS3) {
-                // <rho_j rho_k rho_l> over the segment: d_j d_k d_l + (d_j l_k l_l + l_j d_k l_l + l_j l_k d_l) / 12
-                double cub[10];
-                int q3 = 0;
-#pragma unroll
-                for (int j = 0; j < 3; ++j)
-#pragma unroll
-                    for (int k2 = j; k2 < 3; ++k2)
-#pragma unroll
-                        for (int l2 = k2; l2 < 3; ++l2)
-                            cub[q3++] = d[j] * d[k2] * d[l2] +
-                                        (d[j] * l[k2] * l[l2] + l[j] * d[k2] * l[l2] + l[j] * l[k2] * d[l2]) *
-                                            (1.0 / 12.0);
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int p = 0; p < 10; ++p) acc[31 + 10 * i + p] += al[i] * cub[p];
-            }
-        }
-        int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-#pragma unroll
-        for (int q = 0; q < PARTS; ++q) {
-            double v = acc[q];
-            for (int o = 16; o > 0; o >>= 1) {
-                double w = __shfl_xor_sync(0xffffffffu, v, o);
-                v = q == 0 ? fmax(v, w) : v + w;
-            }
-            if (lane == 0) red[q][warp] = v;
-        }
-        __syncthreads();
-        if (threadIdx.x < PARTS) {
-            double v = red[threadIdx.x][0];
-            for (int w = 1; w < MOM_THREADS / 32; ++w)
-                v = threadIdx.x == 0 ? fmax(v, red[0][w]) : v + red[threadIdx.x][w];
-            partial[(int64_t)PARTS * it + threadIdx.x] = v;
-        }
-        __syncthreads();
-    }
-}
-
 // Index of the symmetric third-order component (j, k, l) in 000,001,002,011,012,022,111,112,122,222.
 __device__ __forceinline__ int sym3(int j, int k, int l) {
     int a = j, b = k, c = l, t;
@@ -1135,22 +983,6 @@ __device__ void finalize_node(int64_t j, const double *__restrict__ v, const Nod
         const double b = sqrt(v[0]) * (1.0 + 1e-12);
         o.nodes[j] = node_record(j, b, o.centre, o.core, o.lo, o.hi, o.left, o.right);
     }
-}
-
-// Combine a node's chunks in order, then finalize it.
-template <int PARTS>
-__global__ void moment_final_kernel(int64_t count, const int64_t *first, const int64_t *nitems,
-                                    const double *partial, NodeOut o) {
-    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= count) return;
-    double v[PARTS];
-    for (int q = 0; q < PARTS; ++q) v[q] = 0.0;
-    for (int64_t it = first[j]; it < first[j] + nitems[j]; ++it)
-        for (int q = 0; q < PARTS; ++q) {
-            double p = partial[(int64_t)PARTS * it + q];
-            v[q] = q == 0 ? fmax(v[q], p) : v[q] + p;
-        }
-    finalize_node<PARTS>(j, v, o);
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -1769,28 +1601,6 @@ __global__ void node_rec_kernel(int64_t count, const unsigned long long *bound2,
     nodes[j] = node_record(j, b, centre, core, lo, hi, left, right);
 }
 
-// The clear-leaf pair records (Seg32c2) of every leaf, one warp per node (internal nodes return): each segment of
-// leaf j relative to the leaf's centre, from its FP64 record (start, L, d, (Gamma/L)/(4 pi), rc).
-__global__ void clear_pairs_kernel(int64_t count, const int64_t *lo, const int64_t *hi, const int64_t *left,
-                                   const double *centre, const Seg64 *seg64, Seg32c2 *out) {
-    const int lane = threadIdx.x & 31;
-    const int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (j >= count || left[j] >= 0) return;
-    const double ox = centre[3 * j], oy = centre[3 * j + 1], oz = centre[3 * j + 2];
-    for (int64_t k = lo[j] + lane; k < hi[j]; k += 32) {
-        const Seg64 q = seg64[k];
-        clear_half(out, k, ox, oy, oz, q.sx, q.sy, q.sz, q.dx * q.len, q.dy * q.len, q.dz * q.len, q.len * q.len,
-                   q.gfac * q.len, q.radius);
-    }
-}
-
-// Trees without segment records (bs_node_quantities: node quantities only) have none to write.
-static void clear_pairs(const bs_tree *t, cudaStream_t s) {
-    if (!t->seg64 || !t->seg32c2) return;
-    clear_pairs_kernel<<<blocks_for(t->count * 32, 256), 256, 0, s>>>(t->count, t->lo, t->hi, t->left, t->centre,
-                                                                     t->seg64, t->seg32c2);
-}
-
 // Every node's export arrays and far records from its sums (read in place); for fourth- and fifth-order trees
 // blockIdx.y picks the part (0: orders 0-3, 1-3: the order-4 and order-5 rows of one component).
 template <int PARTS>
@@ -1929,42 +1739,12 @@ int compute_moments(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStream_
             if (!base) return BS_ERR_OOM;
         }
     }
-    // fourth order: the bottom-up pipeline for every kind (its box, centre and bound equal the direct sums')
+    // the bottom-up pipeline for every kind and order: its box, centre and bound equal the direct sums', its moments
+    // equal them up to rounding (the translations of the children's moments), at O(m) work instead of O(m depth)
     if (t->order5) return moments_bottom_up<MOM_PARTS5>(t, geo, scratch, s, side);
     if (t->order4) return moments_bottom_up<MOM_PARTS4>(t, geo, scratch, s, side);
-    if (t->kind == BS_TREE_MORTON) return t->order3 ? moments_bottom_up<MOM_PARTS3>(t, geo, scratch, s, side)
-                                                   : moments_bottom_up<MOM_PARTS>(t, geo, scratch, s, side);
-    int64_t *nitems = scratch.get<int64_t>(count), *first = scratch.get<int64_t>(count);
-    int64_t *total = scratch.get<int64_t>(1);
-    if (!nitems || !first || !total) return scratch.status;
-    item_count_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->lo, t->hi, nitems);
-    BS_CHECK_LAUNCH("item_count_kernel");
-    int rc = scan_exclusive(nitems, first, count, total, scratch, s);
-    if (rc != BS_OK) return rc;
-    int64_t n_items = 0;
-    BS_CUDA(cudaMemcpyAsync(&n_items, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    BS_CUDA(cudaStreamSynchronize(s));
-    Item *items = scratch.get<Item>(n_items);
-    const int parts = t->order3 ? MOM_PARTS3 : MOM_PARTS;
-    double *box = scratch.get<double>(7 * n_items), *sums = scratch.get<double>((size_t)parts * n_items);
-    if (!items || !box || !sums) return scratch.status;
-    item_fill_kernel<<<blocks_for(count, 256), 256, 0, s>>>(count, t->lo, t->hi, first, items);
-    unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(n_items, 8192));
-    moment_box_kernel<<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, box);
-    moment_centre_kernel<<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, box, t->centre, t->core);
-    const NodeOut out{t->lo, t->hi, t->left, t->right, t->centre, t->core, t->bound, t->m0, t->m1, t->m2,
-                      t->w1, t->t2, t->w2, t->nodes, t->far64, t->far32, t->far64x, t->far32x,
-                      t->far64y, t->far32y, t->far64z, t->far32z};
-    if (t->order3) {
-        moment_sum_kernel<MOM_PARTS3><<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, t->centre, sums);
-        moment_final_kernel<MOM_PARTS3><<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, sums, out);
-    } else {
-        moment_sum_kernel<MOM_PARTS><<<grid, MOM_THREADS, 0, s>>>(items, n_items, t->order32, geo, t->centre, sums);
-        moment_final_kernel<MOM_PARTS><<<blocks_for(count, 128), 128, 0, s>>>(count, first, nitems, sums, out);
-    }
-    clear_pairs(t, s);
-    BS_CHECK_LAUNCH("moments");
-    return BS_OK;
+    return t->order3 ? moments_bottom_up<MOM_PARTS3>(t, geo, scratch, s, side)
+                     : moments_bottom_up<MOM_PARTS>(t, geo, scratch, s, side);
 }
 
 }  // namespace bs
