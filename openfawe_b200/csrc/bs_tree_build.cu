@@ -544,8 +544,9 @@ __global__ void level_box_kernel(const Item *items, int64_t nitems, const int32_
 }
 
 // Per level node: combine its chunks, longest axis (lowest on ties), split flag.
+// degenerate (may be null): set when a node large enough to split has a box of zero extent and so does not split.
 __global__ void level_split_kernel(int64_t nodes, const int64_t *first_item, const int64_t *item_count,
-                                   const double *partial, int8_t *split, int8_t *axis_of) {
+                                   const double *partial, int8_t *split, int8_t *axis_of, int *degenerate) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nodes) return;
     if (item_count[j] == 0) {
@@ -565,6 +566,13 @@ __global__ void level_split_kernel(int64_t nodes, const int64_t *first_item, con
         if (hi[c] - lo[c] > extent) { extent = hi[c] - lo[c]; axis = c; }
     split[j] = extent > 0.0 ? 1 : 0;
     axis_of[j] = (int8_t)axis;
+    if (degenerate && !(extent > 0.0)) atomicOr(degenerate, 1);
+}
+
+// The axis of every node of the sort list: axis_of[map[r]].
+__global__ void sort_axis_kernel(int64_t count, const int64_t *map, const int8_t *axis_of, int8_t *sort_axis) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < count) sort_axis[r] = axis_of[map[r]];
 }
 
 // Keys (node rank in the sort list, dense coordinate rank on its axis) for the elements of splitting nodes.
@@ -638,6 +646,85 @@ static int build_median(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStr
     lo[0] = 0;
     hi[0] = m;
     int64_t count = 1;
+    // Planned levels: a node larger than a leaf splits at its middle unless its box has no extent, so the topology
+    // follows from m and the leaf size alone unless some node is degenerate.  Every level is queued at once on that
+    // plan (the axes are chosen and used on the device, no read-back between levels); one read-back at the end says
+    // whether a degenerate node occurred, and then the levels below are run again one at a time with their decisions
+    // read back.
+    if (needs_sort) {
+        int *degenerate = scratch.get<int>(1);
+        if (!degenerate) return scratch.status;
+        BS_CUDA(cudaMemsetAsync(degenerate, 0, sizeof(int), s));
+        std::vector<int64_t> level{0};
+        while (!level.empty()) {
+            Scratch ls(t->pool, s);  // this level's temporaries, freed in stream order
+            std::vector<Item> items, sort_items;
+            std::vector<int64_t> first_item(level.size()), item_count(level.size()), dest, map, following;
+            int64_t total = 0;
+            for (size_t j = 0; j < level.size(); ++j) {
+                const int64_t node = level[j], a = lo[node], b = hi[node];
+                first_item[j] = (int64_t)items.size();
+                if (b - a > leaf) {
+                    for (int64_t c = a; c < b; c += CHUNK)
+                        items.push_back({(int32_t)j, (int32_t)c, (int32_t)std::min(b, c + CHUNK), 0});
+                    const int64_t middle = (a + b) / 2, f = count, g = count + 1;
+                    count += 2;
+                    lo[f] = a; hi[f] = middle; lo[g] = middle; hi[g] = b;
+                    left[node] = f; right[node] = g;
+                    following.push_back(f);
+                    following.push_back(g);
+                    const int32_t r = (int32_t)dest.size();
+                    dest.push_back(total);
+                    map.push_back((int64_t)j);
+                    for (int64_t c = a; c < b; c += CHUNK)
+                        sort_items.push_back({r, (int32_t)c, (int32_t)std::min(b, c + CHUNK), (int32_t)a});
+                    total += b - a;
+                }
+                item_count[j] = (int64_t)items.size() - first_item[j];
+            }
+            if (items.empty()) break;
+            Item *d_items, *d_sort_items;
+            int64_t *d_first, *d_count, *d_dest, *d_map;
+            double *partial = ls.get<double>(6 * items.size());
+            int8_t *d_split = ls.get<int8_t>(level.size()), *d_axis = ls.get<int8_t>(level.size());
+            int8_t *d_sort_axis = ls.get<int8_t>(dest.size());
+            int rc = upload(ls, items, &d_items, s);
+            if (rc == BS_OK) rc = upload(ls, first_item, &d_first, s);
+            if (rc == BS_OK) rc = upload(ls, item_count, &d_count, s);
+            if (rc == BS_OK) rc = upload(ls, sort_items, &d_sort_items, s);
+            if (rc == BS_OK) rc = upload(ls, dest, &d_dest, s);
+            if (rc == BS_OK) rc = upload(ls, map, &d_map, s);
+            if (rc != BS_OK || !partial || !d_split || !d_axis || !d_sort_axis) return rc != BS_OK ? rc : ls.status;
+            level_box_kernel<<<(unsigned)std::min<size_t>(items.size(), 4096), MOM_THREADS, 0, s>>>(
+                d_items, (int64_t)items.size(), t->order32, geo, partial);
+            level_split_kernel<<<blocks_for((int64_t)level.size(), 128), 128, 0, s>>>(
+                (int64_t)level.size(), d_first, d_count, partial, d_split, d_axis, degenerate);
+            sort_axis_kernel<<<blocks_for((int64_t)dest.size(), 128), 128, 0, s>>>((int64_t)dest.size(), d_map, d_axis,
+                                                                                   d_sort_axis);
+            const unsigned grid = (unsigned)std::min<size_t>(sort_items.size(), 4096);
+            level_gather_kernel<<<grid, 256, 0, s>>>(d_sort_items, (int64_t)sort_items.size(), d_dest, d_sort_axis,
+                                                     t->order32, rank[0], rank[1], rank[2], rank_bits, keys, vals);
+            BS_CHECK_LAUNCH("planned median level");
+            rc = radix_sort(keys, vals, total, 0, rank_bits + bits_for((int64_t)dest.size() - 1), ls, s);
+            if (rc != BS_OK) return rc;
+            level_scatter_kernel<<<grid, 256, 0, s>>>(d_sort_items, (int64_t)sort_items.size(), d_dest, vals,
+                                                      t->order32);
+            BS_CHECK_LAUNCH("level_scatter_kernel");
+            level.swap(following);
+        }
+        int found = 0;
+        BS_CUDA(cudaMemcpyAsync(&found, degenerate, sizeof(int), cudaMemcpyDeviceToHost, s));
+        BS_CUDA(cudaStreamSynchronize(s));
+        if (!found) {
+            needs_sort = false;  // the planned levels are the tree
+        } else {  // start again, one level at a time
+            iota_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, t->order32);
+            BS_CHECK_LAUNCH("iota_kernel");
+            std::fill(left.begin(), left.end(), -1);
+            std::fill(right.begin(), right.end(), -1);
+            count = 1;
+        }
+    }
     std::vector<int64_t> level{0};
     while (!level.empty() && needs_sort) {
         Scratch scratch(t->pool, s);  // this level's temporaries (shadows the call's scratch)
@@ -664,7 +751,7 @@ static int build_median(bs_tree *t, const SegGeo *geo, Scratch &scratch, cudaStr
             level_box_kernel<<<(unsigned)std::min<size_t>(items.size(), 4096), MOM_THREADS, 0, s>>>(
                 d_items, (int64_t)items.size(), t->order32, geo, partial);
             level_split_kernel<<<blocks_for((int64_t)level.size(), 128), 128, 0, s>>>(
-                (int64_t)level.size(), d_first, d_count, partial, d_split, d_axis);
+                (int64_t)level.size(), d_first, d_count, partial, d_split, d_axis, nullptr);
             BS_CHECK_LAUNCH("level box/split");
             BS_CUDA(cudaMemcpyAsync(split.data(), d_split, level.size(), cudaMemcpyDeviceToHost, s));
             BS_CUDA(cudaMemcpyAsync(axis_of.data(), d_axis, level.size(), cudaMemcpyDeviceToHost, s));

@@ -59,6 +59,11 @@ def test_median_build_element_for_element(device):
     cases = [("random", *random_segments(11, 600)[:3], 8), ("grid", *grid_segments(), 32),
              ("grid-leaf-1", *[a[:200] for a in grid_segments()], 1),
              ("coincident", np.ones((40, 3)), np.tile([0.0, 1.0, 0.0], (40, 1)), np.full(40, 0.5), 4),
+             # a cluster of 40 identical segments among 600 others: a node of no extent several levels down (the
+             # planned levels are then run again one at a time)
+             ("coincident-cluster", *[np.concatenate((x, y)) for x, y in zip(
+                 random_segments(12, 600)[:3],
+                 (np.full((40, 3), 5.0), np.tile([0.0, 0.0, 1.0], (40, 1)), np.full(40, 0.25)))], 4),
              ("fewer-than-a-leaf", *[a[:5] for a in random_segments(3, 5)[:3]], 32),
              ("longer-than-a-chunk", *random_segments(4, 5000)[:3], 16)]
     for name, starts, directions, lengths, leaf in cases:
