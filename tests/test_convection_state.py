@@ -107,6 +107,35 @@ def test_oracle_ring_stages_match_reference():
         assert np.array_equal(got.view(np.uint64), g[name].view(np.uint64)), name
 
 
+def test_stage_plan_edge_cases():
+    """The plan's edge cases, by the reference's rules (wake.py:431-491): ring_first past the last node is a network
+    without rings; ring_free 0 leaves every ring node at the ambient flow; a row limit that covers every row is no
+    limit; no ring edge means no frozen-row drift."""
+    import torch
+    from openfawe_b200 import convection
+    g = golden("convection_rings.npz")
+    nodes, edges, radii = g["nodes"], torch.as_tensor(g["edges"]), torch.as_tensor(g["radii"])
+    first, ring_first = int(g["first"]), int(g["ring_first"])
+    n = len(nodes) - first
+    pairs = torch.as_tensor(O.incident_pairs(nodes, g["edges"], first))
+    plan = lambda **kw: convection.stage_parts(n, first, len(nodes), edges, pairs, radii, **kw)  # noqa: E731
+    spans = lambda parts: [(lo, hi, rule) for lo, hi, _, _, rule, _ in parts]  # noqa: E731
+    assert spans(plan(ring_first=len(nodes))) == spans(plan()) == [(0, n, None)]
+    assert spans(plan(ring_first=ring_first, ring_free=0)) == [(0, ring_first - first, None)]
+    rows = ring_first - first
+    assert spans(plan(ring_first=ring_first, free_rows=rows // first + 1)) == \
+        [(0, rows, None), (rows, n, "zero")]
+    no_rings = plan(free_rows=2, frozen_drift="ambient_rings")
+    assert spans(no_rings) == [(0, 2 * first, None)]
+    # every planned exclusion names a point of its part and an edge of its subset
+    for lo, hi, sub, cores, rule, excluded in plan(ring_first=ring_first, free_rows=3, frozen_drift="ambient_rings"):
+        width = len(edges) if sub is None else len(sub)
+        assert len(cores) == width
+        if len(excluded):
+            assert int(excluded[:, 0].min()) >= 0 and int(excluded[:, 0].max()) < hi - lo
+            assert int(excluded[:, 1].min()) >= 0 and int(excluded[:, 1].max()) < width
+
+
 def test_frozen_state_roundtrip_and_oracle(tmp_path):
     from openfawe_b200 import wakestate
     state = wakestate.load_state(os.path.join(GOLDEN, "frozen_state_input.npz"))
