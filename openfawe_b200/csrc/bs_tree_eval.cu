@@ -1084,14 +1084,8 @@ static thread_local cudaEvent_t t_records_ready = nullptr;
 template <int PREC, int MODEL>
 static void launch_pair(unsigned walk_grid, int block, size_t smem, uint2 list_grid, int64_t target_warps,
                         unsigned reduce_grid, cudaStream_t s, const EvalArgs &args, double *out, int8_t *flags) {
-    // BS_WALK_POP=1 takes one stack entry per walk step (for comparisons); the default takes two
-    static const int pop = [] {
-        const char *v = getenv("BS_WALK_POP");
-        return (v && v[0] == '1') ? 1 : 2;
-    }();
     if (t_marks) cudaEventRecord(t_marks[0], s);
-    if (pop == 2) tree_walk_kernel<PREC, MODEL, 2><<<walk_grid, block, smem, s>>>(args);
-    else tree_walk_kernel<PREC, MODEL, 1><<<walk_grid, block, smem, s>>>(args);
+    tree_walk_kernel<PREC, MODEL, 2><<<walk_grid, block, smem, s>>>(args);  // two stack entries a step
     item_plan_kernel<<<1, 1024, 0, s>>>(target_warps, args.list_total, args.item_want, args.item_off,
                                         args.item_warp);
     item_bounds_kernel<<<(unsigned)((target_warps * 32 + 255) / 256), 256, 0, s>>>(args, target_warps);
