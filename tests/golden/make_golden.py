@@ -168,9 +168,9 @@ def main():
     if args.only == "convection_rings.npz" or args.only is None:
         # one stage of wake._network_convection (wake.py:404-491) on a network with rotor rings after its wing rows:
         # the rotor-sheet network reordered so that every ring node follows every wing node, the first wing row
-        # bound; four settings: rows and rings; the leading ring nodes free, the ring targets with their own cores;
+        # bound; five settings: rows and rings; the leading ring nodes free, the ring targets with their own cores;
         # the far-wake row limit with frozen rows at the ambient flow; the same with the frozen rows drifting with
-        # the rings' induction
+        # the rings' induction; all of these at once
         import types
         from openfawe.aero import wake as W
         from openfawe.aero.vortex import CoreModel
@@ -192,7 +192,8 @@ def main():
         out = dict(nodes=nodes, edges=edges, gamma=gamma, radii=radii, ring_radii=ring_radii, first=np.array(first),
                    ring_first=np.array(ring_first), inflow=inflow)
         settings = {"rings": dict(), "ring_free": dict(ring_free=200, ring_radii=ring_radii),
-                    "row_limit": dict(rows=3, drift="ambient"), "row_limit_rings": dict(rows=3, drift="ambient_rings")}
+                    "row_limit": dict(rows=3, drift="ambient"), "row_limit_rings": dict(rows=3, drift="ambient_rings"),
+                    "all": dict(ring_free=200, ring_radii=ring_radii, rows=3, drift="ambient_rings")}
         for name, opt in settings.items():
             config = types.SimpleNamespace(free_wake=True, velocity_backend="numba", core_model=CoreModel.LAMB_OSEEN)
             if "rows" in opt:

@@ -59,10 +59,11 @@ def test_oracle_convection_stages_match_reference():
         assert np.array_equal(got.view(np.uint64), g[integrator].view(np.uint64)), integrator
 
 
-# the four settings of convection_rings.npz (tests/golden/make_golden.py)
+# the five settings of convection_rings.npz (tests/golden/make_golden.py)
 RING_SETTINGS = {"rings": {}, "ring_free": {"ring_free": 200, "ring_radii": True},
                  "row_limit": {"free_rows": 3, "frozen_drift": "ambient"},
-                 "row_limit_rings": {"free_rows": 3, "frozen_drift": "ambient_rings"}}
+                 "row_limit_rings": {"free_rows": 3, "frozen_drift": "ambient_rings"},
+                 "all": {"ring_free": 200, "ring_radii": True, "free_rows": 3, "frozen_drift": "ambient_rings"}}
 
 
 def ring_options(g, name, to_tensor):
